@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the RBF-FD hot path on B200.
+
+Workload (the configuration the headline metric is quoted on): heat equation
+on the unit sphere, u_t = Laplace-Beltrami(u), N = 163842 seeded Fibonacci
+nodes, n = 50 nearest-neighbour stencils, Gaussian RBF-FD Laplace-Beltrami
+weights with degree-3 polynomial augmentation computed in FP64 on the device,
+eps = 0.044 sqrt(N) - 0.14 (the reference's rule for n = 50,
+RBFFD::setEpsilonByStencilSize), initial condition a sum of spherical
+harmonics of degree <= 20 with N(0,1) seeded coefficients, 500 RK4 steps of
+dt = 1e-6 per benchmark step, FP32 state/weights/accumulation (FP64 reported
+beside it).  Metric: RK4 node-updates/s (one node advanced one full RK4
+step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs its own replica of the workload on its
+own GPU (the path does not shard: one GPU per solve); the value is all ranks'
+node-updates divided by the slowest rank's device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="heat_sphere_N163842_n50_deg3_500steps", N=163842, n=50, deg=3, steps=500, dt=1e-6, lmax=20,
+                seed=2)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], None, set()
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if r[3 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def setup_problem():
+    import rbffd_gpu_b200 as R
+    W = WORKLOAD
+    xyz = R.fibonacci_nodes(W["N"], W["seed"])
+    st = R.knn_stencils(xyz, W["n"])
+    c = np.random.default_rng(W["seed"]).standard_normal((W["lmax"] + 1) ** 2)
+    u0 = R.exact_sph_heat(xyz, W["lmax"], c, 0.0)
+    eps = 0.044 * np.sqrt(W["N"]) - 0.14
+    return xyz, st, u0, eps, c
+
+
+def stage_bytes(n, wbytes, sbytes):
+    """Algorithmic bytes per node per RK4 stage: n weights + n int32 indices
+    + the state terms (one gathered read of the stage input, read u_n, read and
+    write of the accumulator, write of the next stage input)."""
+    return n * wbytes + 4 * n + 4 * sbytes
+
+
+def cpu_baseline_heat(st, w_lsfc, u0, steps):
+    import oracle as O
+    nth = O.max_threads()
+    t = time.perf_counter()
+    O.rk4_heat(st, None, w_lsfc, u0, WORKLOAD["dt"], steps, nthreads=nth)
+    dt = time.perf_counter() - t
+    return WORKLOAD["N"] * steps / dt, nth, dt
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if ws > 1 and rank != 0:
+        return
+    import oracle as O
+    xyz, st, u0, eps, _ = setup_problem()
+    nth = O.max_threads()
+    t0 = time.perf_counter()
+    W = O.weights(xyz, st, None, eps, O.LSFC, dim=2, poly_deg=WORKLOAD["deg"], nthreads=nth)[O.LSFC]
+    t_w = time.perf_counter() - t0
+    sample = 10  # RK4 steps per benchmark step: a bounded sample of the 500-step workload
+    u = u0
+    for _ in range(args.warmup):
+        O.rk4_heat(st, None, W, u, WORKLOAD["dt"], 1, nthreads=nth)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        O.rk4_heat(st, None, W, u, WORKLOAD["dt"], sample, nthreads=nth)
+        times.append(time.perf_counter() - t)
+    tot = sum(times)
+    value = WORKLOAD["N"] * sample * args.steps / tot
+    line = {
+        "impl": "reference", "metric": "rk4_node_updates_per_s", "value": value, "unit": "node-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD["name"], "nodes": WORKLOAD["N"], "stencil": WORKLOAD["n"],
+                   "poly_deg": WORKLOAD["deg"], "l2_flush": "working set re-read from host memory"},
+        "cpu_baseline": {"value": value, "unit": "node-updates/s", "cores": nth, "kind": "port",
+                         "sample": "%d of the 500 RK4 steps per benchmark step on the full N=%d grid; FP64 oracle "
+                                   "restatement of TimeDependentPDE::advanceRungeKutta4 + applyWeightsForDeriv, "
+                                   "OpenMP over stencil rows (weights setup %.1f s, untimed)" % (
+                                       sample, WORKLOAD["N"], t_w)},
+        "e2e": {"value": value, "unit": "node-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import rbffd_gpu_b200 as R
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    W = WORKLOAD
+    N, n, steps, dt = W["N"], W["n"], W["steps"], W["dt"]
+    xyz, st, u0, eps, coeffs = setup_problem()
+    ctx = R.Context(local)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(R.LSFC, grid, 2)
+    der.setEpsilon(eps)
+    der.setPolynomialDegree(W["deg"])
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    der.computeAllWeightsForAllStencils()
+    t_weights = time.perf_counter() - t
+    t = time.perf_counter()
+    der.computeAllWeightsForAllStencils()  # second call: tuned shapes, warm caches
+    t_weights2 = time.perf_counter() - t
+    pde = R.HeatSphere(grid, der, 1.0, dtype=R.F32)
+    pde.fillInitialConditions(u0)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def one_step():
+        pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
+
+    for _ in range(max(3, args.warmup)):
+        one_step()
+    ctx.synchronize()
+    # ---- timed region (device time, CUDA events on the library's stream) ----
+    clocks = ClockSampler(local)
+    clocks.start()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    evs = []
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.fill_(1.0)  # write a buffer larger than L2 between timed steps
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            one_step()
+            e1.record(stream)
+            evs.append((e0, e1))
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    clk = clocks.stop()
+    tot_ms = float(sum(step_ms))
+    if ws > 1:
+        tt = torch.tensor([tot_ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        tot_ms = float(tt.item())
+    node_updates = float(N) * steps * args.steps * ws
+    value = node_updates / (tot_ms * 1e-3)
+    launches = 4 * steps * args.steps  # one fused stage kernel per RK4 stage
+    per_launch_s = tot_ms * 1e-3 / launches
+    bytes_launch = N * stage_bytes(n, 4, 4)
+    achieved = bytes_launch / per_launch_s / 1e9
+    peak, peak_kind = load_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("heat_f32_dram_bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+    # ---- end to end through the C ABI with host buffers ----
+    u_host = torch.from_numpy(u0.copy()).pin_memory()
+    out_host = torch.empty(N, dtype=torch.float64).pin_memory()
+    uh = u_host.numpy()
+    oh = out_host.numpy()
+    pde_e2e = R.HeatSphere(grid, der, 1.0, dtype=R.F32)
+    pde_e2e.fillInitialConditions(uh)
+    pde_e2e.advance(R.RK4, dt, steps, graph=True)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        pde_e2e.fillInitialConditions(uh)  # host -> device (pinned)
+        pde_e2e.advance(R.RK4, dt, steps, graph=True)
+        pde_e2e.ctx.check(0)
+        import ctypes
+        pde_e2e.ctx.check(pde_e2e.ctx.L.rbffd_pde_get_state(pde_e2e.h, oh.ctypes.data_as(ctypes.POINTER(
+            ctypes.c_double))), "get_state")  # device -> host (pinned)
+    e2e_s = time.perf_counter() - t
+    if ws > 1:
+        tt = torch.tensor([e2e_s], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_value = node_updates / e2e_s
+    extras = {}
+    if not args.no_extras and rank == 0:
+        extras = bench_extras(R, torch, ctx, grid, der, pde, u0, xyz, st, coeffs)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        w64 = der.getWeights(R.LSFC)
+        cps, nth, secs = cpu_baseline_heat(st, w64, u0, 12)
+        cpu = {"value": cps, "unit": "node-updates/s", "cores": nth, "kind": "port",
+               "sample": "12 RK4 steps of the N=%d, n=%d heat workload (%.1f s), FP64 oracle restatement of "
+                         "advanceRungeKutta4 + applyWeightsForDeriv, OpenMP over rows" % (N, n, secs)}
+    if rank == 0:
+        line = {
+            "metric": "rk4_node_updates_per_s", "value": value, "unit": "node-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": tot_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": W["name"], "nodes": N, "stencil": n, "poly_deg": W["deg"], "rk4_steps_per_step": steps,
+                       "dt": dt, "eps": eps, "parallelism": "replicas" if ws > 1 else "single",
+                       "l2_flush": "256 MiB buffer written between timed steps"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_stage_scalar<float,HEAT> (fused SpMV + RHS + RK4 stage)",
+                         "algorithmic_bytes_per_launch": bytes_launch,
+                         "note": "per-launch time = timed region / launches (includes graph launch gaps); "
+                                 "FP32 weights+indices (65.5 MB) fit the 126 MB L2"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "node-updates/s", "h2d_bytes_per_step": N * 8,
+                    "d2h_bytes_per_step": N * 8},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "weights_setup_s": {"first_call": t_weights, "tuned": t_weights2},
+            "extras": extras,
+        }
+        print(json.dumps(line), flush=True)
+    pde.close()
+    pde_e2e.close()
+    grid.close()
+    ctx.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
+    """FP64 and plain-path variants of the same workload, and errors."""
+    W = WORKLOAD
+    N, steps, dt = W["N"], W["steps"], W["dt"]
+    out = {}
+    stream = torch.cuda.ExternalStream(ctx.stream())
+
+    def timed(pde, reps=2, **kw):
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, dt, steps, **kw)
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            pde.advance(R.RK4, dt, steps, **kw)
+        e1.record(stream)
+        ctx.synchronize()
+        return N * steps * reps / (e0.elapsed_time(e1) * 1e-3)
+
+    p64 = R.HeatSphere(grid, der, 1.0, dtype=R.F64)
+    out["fp64_fused_graph"] = timed(p64, graph=True, asynchronous=True)
+    pplain = R.HeatSphere(grid, der, 1.0, dtype=R.F64)
+    out["fp64_plain_unfused"] = timed(pplain, reps=1, unfused=True)
+    out["fp32_fused_graph"] = timed(pde32, graph=True, asynchronous=True)
+    out["fused_fp32_over_plain_fp64"] = out["fp32_fused_graph"] / out["fp64_plain_unfused"]
+    # accuracy after the full 500 steps: FP32 vs FP64 (same weights), FP64 vs exact
+    p64.fillInitialConditions(u0)
+    p64.advance(R.RK4, dt, steps, graph=True)
+    pde32.fillInitialConditions(u0)
+    pde32.advance(R.RK4, dt, steps, graph=True)
+    u64, u32 = p64.getLocalSolution(), pde32.getLocalSolution()
+    ex = R.exact_sph_heat(xyz, W["lmax"], coeffs, steps * dt)
+    out["rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64))
+    out["rel_l2_fp64_vs_exact"] = float(np.linalg.norm(u64 - ex) / np.linalg.norm(ex))
+    out["shape_fp32"] = pde32.getShape()
+    p64.close()
+    pplain.close()
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

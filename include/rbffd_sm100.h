@@ -1,0 +1,217 @@
+/*
+ * rbffd_sm100.h -- C ABI of librbffd_sm100.so, the B200 (sm_100a) RBF-FD hot path.
+ *
+ * The path: per-stencil RBF-FD weights (batched FP64 solves of the
+ * RBF + polynomial saddle-point systems), ELL application of derivative and
+ * hyperviscosity operators (applyWeightsForDeriv), and the classical RK4
+ * update with the PDE right-hand side fused into each stage.
+ *
+ * Every entry point returns an int status (RBFFD_OK = 0, negative on error),
+ * never exits and never traps; the message of the last failure on a context
+ * is available from rbffd_ctx_last_error().  Host pointers are plain C arrays;
+ * device pointers appear only in the *_dev variants and are typed void*.
+ * Handles are not reentrant: one host thread per handle at a time.
+ *
+ * Layout conventions: node coordinates xyz are [N][3] doubles (unit sphere);
+ * stencils are [N][n_pad] int32 row-major, row i listing the st_len[i] node
+ * indices of stencil i with the centre i first (the reference's StencilType,
+ * src/common_typedefs.h:16; centre check rbffd.cpp:916-928); weights on the
+ * host are [N][n_pad] doubles in the same order; solution vectors with T
+ * tracers are [N][T] (tracer fastest).
+ */
+#ifndef RBFFD_SM100_H
+#define RBFFD_SM100_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+enum rbffd_status {
+    RBFFD_OK = 0,
+    RBFFD_ERR_INVALID = -1,     /* bad argument, size or handle */
+    RBFFD_ERR_OOM = -2,         /* device or host allocation failed */
+    RBFFD_ERR_CUDA = -3,        /* CUDA runtime error (message in last_error) */
+    RBFFD_ERR_TIMEOUT = -4,     /* a bounded wait expired */
+    RBFFD_ERR_UNSUPPORTED = -5, /* combination not implemented */
+    RBFFD_ERR_STATE = -6,       /* call out of order (e.g. weights missing) */
+    RBFFD_ERR_SINGULAR = -7,    /* a stencil system had an exactly zero pivot */
+    RBFFD_ERR_BUDGET = -8,      /* admission refused: over the HBM budget */
+    RBFFD_ERR_NO_DEVICE = -9    /* no CUDA device / driver */
+};
+
+/* Arithmetic type of a kernel path. */
+enum rbffd_dtype { RBFFD_F32 = 0, RBFFD_F64 = 1 };
+
+/* Derivative operator flags; identical values to RBFFD::DerType
+ * (src/rbffd/rbffd.h:43-60). */
+enum rbffd_der_type {
+    RBFFD_X = 0x1, RBFFD_Y = 0x2, RBFFD_Z = 0x4, RBFFD_LAPL = 0x8, RBFFD_R = 0x10, RBFFD_HV = 0x20,
+    RBFFD_LAMBDA = 0x40, RBFFD_THETA = 0x80, RBFFD_LSFC = 0x100, RBFFD_XSFC = 0x200, RBFFD_YSFC = 0x400,
+    RBFFD_ZSFC = 0x800, RBFFD_INTERP = 0x8000
+};
+
+typedef struct rbffd_ctx rbffd_ctx;
+typedef struct rbffd_grid rbffd_grid;
+typedef struct rbffd_pde rbffd_pde;
+
+/* ---- library / context ------------------------------------------------ */
+const char* rbffd_version(void);
+const char* rbffd_status_string(int status);
+int rbffd_device_count(int* count);
+
+/* One context per device; owns a CUDA stream and all device memory of the
+ * grids and PDEs created from it.  Replaces the OpenCL context/queue the
+ * reference GPU classes set up (src/utils/opencl/cl_base_class.cpp:16-66). */
+int rbffd_ctx_create(int device, rbffd_ctx** out);
+int rbffd_ctx_destroy(rbffd_ctx* ctx);
+const char* rbffd_ctx_last_error(const rbffd_ctx* ctx);
+int rbffd_ctx_synchronize(rbffd_ctx* ctx);
+/* Bytes this context holds on the device, and the device's free/total bytes. */
+int rbffd_ctx_mem_info(rbffd_ctx* ctx, size_t* held, size_t* free_bytes, size_t* total_bytes);
+/* The context's CUDA stream (cudaStream_t), for callers that order their own work after ours. */
+int rbffd_ctx_stream(rbffd_ctx* ctx, void** stream);
+
+/* ---- host-side inputs (no GPU) ----------------------------------------- */
+/* N Fibonacci-spiral points on the unit sphere under a seeded uniform random
+ * rotation; xyz[N][3].  Stands in for the reference's node files. */
+int rbffd_nodes_fibonacci(int N, uint64_t seed, double* xyz);
+/* n nearest neighbours of every node, closest first, centre at [0]:
+ * Grid::generateStencilsKDTree (src/grids/grid_interface.cpp:688-725) with the
+ * k-d tree of external/kdtree/KDTree.h:407-433.  st[N][n].  *ties (optional)
+ * receives the number of stencils whose distance list had an exact tie. */
+int rbffd_stencils_knn(const double* xyz, int N, int n, int* st, int* ties, int nthreads);
+/* Cosine bell ExactAdvection::operator() (tests/experiments/cosine_bell_on_sphere/exact_advection.h:37-53). */
+int rbffd_exact_cosine_bell(int N, const double* xyz, double sphere_radius, double* h);
+/* Heat on the unit sphere: u = sum_{l<=lmax,m} c_lm exp(-kappa l(l+1) t) Y_lm (real orthonormal Y_lm). */
+int rbffd_exact_sph_heat(int N, const double* xyz, int lmax, const double* coeffs, double kappa, double t, double* u);
+
+/* ---- grid (nodes + stencils resident on the device) -------------------- */
+/* Uploads nodes and stencils; replaces RBFFD_CL::updateStencilsOnGPU /
+ * updateNodesOnGPU (src/rbffd/rbffd_cl.cpp:186-257).  st_len may be NULL
+ * (every stencil has n_pad nodes).  Padding slots hold the centre index and
+ * weight 0, as the reference's ELL packing does (rbffd_cl.cpp:238-242). */
+int rbffd_grid_create(rbffd_ctx* ctx, int N, const double* xyz, int n_pad, const int* stencils, const int* st_len,
+                      rbffd_grid** out);
+int rbffd_grid_destroy(rbffd_grid* grid);
+/* Device bytes held by the grid (nodes, stencils, all weights). */
+int rbffd_grid_nbytes(const rbffd_grid* grid, size_t* bytes);
+
+/* ---- weights ------------------------------------------------------------ */
+typedef struct rbffd_weight_params {
+    unsigned der_types; /* OR of rbffd_der_type */
+    int dim;            /* RBF dimension used by LAPL and HV (RBFFD ctor dim_num, rbffd.h:192) */
+    int poly_deg;       /* -1 none; 0 constant (the reference build, rbffd.cpp:1,230-234);
+                           1 {1,x,y,z} (rbffd.cpp:150-172); 2..4 tangent-plane polynomials
+                           of total degree <= d, (d+1)(d+2)/2 terms (beyond the reference) */
+    int hv_k;           /* hyperviscosity power (RBFFD::setHVScalars, rbffd.h:241-245) */
+    double hv_gamma;    /* HV scale = -hv_gamma * hv_nodes^-hv_k (RBFFD::getHVScalar, rbffd.h:227-238) */
+    double hv_nodes;    /* global node count for the HV scale; <= 0 means the grid's N */
+} rbffd_weight_params;
+
+/* Batched FP64 weight computation on the device, all stencils, all selected
+ * operators: replaces RBFFD::computeAllWeightsForAllStencils
+ * (src/rbffd/rbffd.cpp:90-103) and computeAllWeightsForStencil_Direct
+ * (rbffd.cpp:225-352).  eps is per node (var_epsilon, the stencil uses
+ * eps[centre], rbffd.cpp:395-400) or NULL to use eps_uniform (setEpsilon,
+ * rbffd.h:352-362).  deg_per_row (optional) overrides poly_deg per stencil
+ * for mixed-size batches.  Returns RBFFD_ERR_SINGULAR if any system had a
+ * zero pivot (first failing row in last_error). */
+int rbffd_weights_compute(rbffd_grid* grid, const rbffd_weight_params* params, const double* eps, double eps_uniform,
+                          const int* deg_per_row);
+/* The assembled augmented systems [A | B] (m x (m+K), row-major, K = number
+ * of selected operators) of the listed stencils, as the weight solver builds
+ * them before elimination: RBFFD::getStencilLHS + getStencilMultiRHS
+ * (rbffd.cpp:106-191), for inspection and parity checks.  All listed rows
+ * must have the same system size m.  out: host [count][m][m+K]. */
+int rbffd_weights_assemble(rbffd_grid* grid, const rbffd_weight_params* params, const double* eps, double eps_uniform,
+                           const int* deg_per_row, const int* rows, int count, double* out);
+/* Install host FP64 weights of one operator, [N][n_pad] (e.g. computed by the
+ * reference CPU path): RBFFD_CL::updateWeightsDouble (rbffd_cl.cpp:306-385). */
+int rbffd_weights_set(rbffd_grid* grid, unsigned der_type, const double* w);
+/* Read one operator's FP64 weights back, [N][n_pad]; padding slots are 0.
+ * RBFFD::getStencilWeights (rbffd.h:395). */
+int rbffd_weights_get(rbffd_grid* grid, unsigned der_type, double* w);
+
+/* ---- apply (derivative evaluation) ------------------------------------- */
+/* deriv[i] = sum_s w[i][s] * u[st_i[s]] for i in [start, start+count):
+ * RBFFD::applyWeightsForDeriv(which, start_indx, nb_stencils, u, deriv)
+ * (src/rbffd/rbffd.cpp:669-688; GPU form RBFFD_CL::applyWeightsForDerivDouble/
+ * Single, rbffd_cl.cpp:526-694).  u has all N values; deriv is written only on
+ * [start, start+count).  Host buffers; dtype selects the FP64 or FP32 kernel
+ * (FP32 casts u to float and returns doubles, as rbffd_cl.cpp:669-682). */
+int rbffd_apply(rbffd_grid* grid, unsigned der_type, int dtype, unsigned start, unsigned count, const double* u,
+                double* deriv);
+/* Device-pointer form on the context stream: u_dev and deriv_dev hold N*ntracers
+ * values of the dtype ([N][ntracers]). */
+int rbffd_apply_dev(rbffd_grid* grid, unsigned der_type, int dtype, int ntracers, const void* u_dev, void* deriv_dev);
+
+/* ---- batched dense FP64 solves (the weight solver's core) ------------- */
+/* Solves batch independent systems A_b X_b = B_b in place, A_b m x m and B_b
+ * m x nrhs, both row-major and contiguous per system on the device
+ * (A_dev[batch][m][m], B_dev[batch][m][nrhs]); X overwrites B; A is destroyed.
+ * Gaussian elimination with partial pivoting (first maximal |pivot|), the
+ * arithmetic of LAPACK dgesv that arma::solve calls (rbffd.cpp:259).
+ * info_dev[b] = 0 or k+1 for an exactly zero pivot at step k.  m <= 160. */
+int rbffd_batched_gesv_dev(rbffd_ctx* ctx, int m, int nrhs, int batch, void* A_dev, void* B_dev, void* info_dev);
+
+/* ---- time-dependent PDE (RK4 with fused right-hand side) --------------- */
+enum rbffd_rhs_kind {
+    /* CosineBell::solve (src/pdes/hyperbolic/cosine_bell.cpp:23-70):
+     * f = -(vel_u/a * D_lambda h + vel_v/a * D_theta h) [+ D_hv h]  */
+    RBFFD_RHS_COSINE_BELL = 1,
+    /* heat on the sphere: f = kappa * D_lsfc u (one Laplace-Beltrami operator, rbffd.cpp:458-464) */
+    RBFFD_RHS_HEAT = 2,
+    /* advection with caller-given per-node coefficients cu, cv:
+     * f = -(cu * D_lambda h + cv * D_theta h) [+ D_hv h] */
+    RBFFD_RHS_ADVECTION = 3
+};
+
+typedef struct rbffd_pde_params {
+    int rhs_kind;         /* rbffd_rhs_kind */
+    int ntracers;         /* T >= 1 right-hand sides sharing the operators */
+    int dtype;            /* RBFFD_F32 or RBFFD_F64 state, weights and accumulation */
+    int use_hv;           /* add the HV operator's output to f (advection kinds) */
+    double sphere_radius; /* a (cosine bell) */
+    double alpha;         /* advection angle (cosine bell) */
+    double u0;            /* cosine bell speed 2*pi*a / (one revolution) */
+    double kappa;         /* heat diffusivity */
+    const double* cu;     /* RBFFD_RHS_ADVECTION: host [N] coefficients */
+    const double* cv;
+} rbffd_pde_params;
+
+/* Creates the device-resident state of a TimeDependentPDE
+ * (src/pdes/time_dependent_pde.h:9-126) on a grid whose weights are ready:
+ * replaces TimeDependentPDE_CL's buffers (time_dependent_pde_cl.cpp:677-708). */
+int rbffd_pde_create(rbffd_grid* grid, const rbffd_pde_params* params, rbffd_pde** out);
+int rbffd_pde_destroy(rbffd_pde* pde);
+/* Copy the solution [N][T] host <-> device (PDE::syncCPUtoGPU, pde.h:166). */
+int rbffd_pde_set_state(rbffd_pde* pde, const double* u);
+int rbffd_pde_get_state(rbffd_pde* pde, double* u);
+int rbffd_pde_set_time(rbffd_pde* pde, double t);
+int rbffd_pde_get_time(rbffd_pde* pde, double* t);
+
+enum rbffd_advance_flags {
+    RBFFD_ADVANCE_GRAPH = 0x1,   /* capture the steps in a CUDA graph and replay it */
+    RBFFD_ADVANCE_UNFUSED = 0x2, /* plain path: one SpMV launch per operator, separate RHS/axpy
+                                    launches and a host synchronisation after every step,
+                                    the structure of TimeDependentPDE_CL::advanceRK4
+                                    (time_dependent_pde_cl.cpp:496-537) */
+    RBFFD_ADVANCE_ASYNC = 0x4    /* return without waiting for the device */
+};
+/* nsteps classical RK4 steps of size dt: TimeDependentPDE::advance(RK4, dt)
+ * (src/pdes/time_dependent_pde.cpp:53-73,172-304), nsteps times.
+ * scheme must be 2 (TimeDependentPDE::RK4). */
+int rbffd_pde_advance(rbffd_pde* pde, int scheme, double dt, int nsteps, int flags);
+/* Kernel-shape choice for this PDE's stage kernel (lanes per stencil row and
+ * threads per block); 0 = autotuned. */
+int rbffd_pde_set_shape(rbffd_pde* pde, int lanes_per_row, int block_threads);
+int rbffd_pde_get_shape(rbffd_pde* pde, int* lanes_per_row, int* block_threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RBFFD_SM100_H */

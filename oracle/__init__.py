@@ -1,0 +1,199 @@
+"""ctypes bindings for the oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg (and its ``--impl reference`` arm) may import this package, and only as
+the checker or the timed CPU baseline.  The product package never imports it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = {}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+# DerType bit values (src/rbffd/rbffd.h:43-60)
+X, Y, Z, LAPL, R, HV, LAMBDA, THETA = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20, 0x40, 0x80
+LSFC, XSFC, YSFC, ZSFC, INTERP = 0x100, 0x200, 0x400, 0x800, 0x8000
+
+
+def _p(a, t=_dp):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "_build", "liboracle.so")
+        if not os.path.exists(path):
+            from . import build as _b
+            _b.build_oracle()
+        L = ctypes.CDLL(path)
+        L.orc_rbf.restype = ctypes.c_double
+        L.orc_rbf.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                              ctypes.c_double, ctypes.c_int]
+        L.orc_lu_solve.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp]
+        L.orc_poly_size.argtypes = [ctypes.c_int]
+        L.orc_cart2sph.argtypes = [ctypes.c_double] * 3 + [_dp, _dp]
+        L.orc_cart2sph.restype = None
+        L.orc_weights.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _dp, ctypes.c_uint, ctypes.c_int,
+                                  ctypes.c_int, _ip, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int]
+        L.orc_assemble.argtypes = [_dp, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_uint,
+                                   ctypes.c_int, ctypes.c_int, _dp]
+        L.orc_apply.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_int]
+        L.orc_apply.restype = None
+        L.orc_cosine_bell_coeffs.argtypes = [ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             _dp, _dp]
+        L.orc_cosine_bell_coeffs.restype = None
+        L.orc_rk4_advect.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _dp, _dp, _dp, _dp, ctypes.c_int,
+                                     _dp, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.orc_rk4_heat.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, ctypes.c_double, ctypes.c_int, _dp,
+                                   ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        _LIB = L
+    return _LIB
+
+
+def ref_lib(name):
+    """Reference code compiled from its own sources (oracle/_ref), or None if absent."""
+    if name not in _REF:
+        path = os.path.join(HERE, "_ref", "lib%s.so" % name)
+        _REF[name] = ctypes.CDLL(path) if os.path.exists(path) else None
+        L = _REF[name]
+        if L is not None and name == "ref_rbf":
+            L.ref_rbf.restype = ctypes.c_double
+            L.ref_rbf.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_int]
+            L.ref_cart2sph.argtypes = [ctypes.c_double] * 3 + [_dp] * 3
+            L.ref_cart2sph.restype = None
+        if L is not None and name == "ref_kdtree":
+            L.ref_knn.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _ip, _dp]
+    return _REF[name]
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def popcount(v):
+    return bin(v & 0xFFFF).count("1")
+
+
+def types_in_order(der_types):
+    return [1 << b for b in range(16) if der_types & (1 << b)]
+
+
+def weights(xyz, st, st_len, eps, der_types, dim=2, poly_deg=0, hv_k=4, hv_scale=1.0, deg_per_row=None,
+            nthreads=0):
+    """FP64 weights for every stencil: returns {der_type: array [N, n_pad]}."""
+    xyz = _c(xyz, np.float64)
+    st = _c(st, np.int32)
+    N, n_pad = st.shape
+    st_len = None if st_len is None else _c(st_len, np.int32)
+    eps = np.full(N, float(eps)) if np.isscalar(eps) else _c(eps, np.float64)
+    dpr = None if deg_per_row is None else _c(deg_per_row, np.int32)
+    K = popcount(der_types)
+    out = np.zeros((K, N, n_pad))
+    rc = lib().orc_weights(N, _p(xyz), n_pad, _p(st, _ip), _p(st_len, _ip), _p(eps), der_types, dim, poly_deg,
+                           _p(dpr, _ip), hv_k, hv_scale, _p(out), nthreads)
+    if rc != 0:
+        raise RuntimeError("oracle weight solve hit a zero pivot at row %d" % (-rc - 1))
+    return {t: out[k] for k, t in enumerate(types_in_order(der_types))}
+
+
+def assemble(xyz, stencil, deg, eps, der_types, dim=2, hv_k=4):
+    stencil = _c(stencil, np.int32)
+    n = len(stencil)
+    m = n + lib().orc_poly_size(deg)
+    K = popcount(der_types)
+    a = np.zeros((m, m + K))
+    lib().orc_assemble(_p(_c(xyz, np.float64)), _p(stencil, _ip), n, deg, eps, der_types, dim, hv_k, _p(a))
+    return a
+
+
+def lu_solve(A, B):
+    A = _c(A, np.float64)
+    B = _c(B, np.float64)
+    if B.ndim == 1:
+        B = B[:, None]
+    m, nrhs = B.shape
+    X = np.zeros((m, nrhs))
+    info = lib().orc_lu_solve(m, nrhs, _p(A), _p(B), _p(X))
+    if info:
+        raise np.linalg.LinAlgError("singular at %d" % info)
+    return X
+
+
+def apply(st, st_len, w, u, nthreads=0):
+    st = _c(st, np.int32)
+    N, n_pad = st.shape
+    u = _c(u, np.float64)
+    T = 1 if u.ndim == 1 else u.shape[1]
+    out = np.zeros_like(u)
+    lib().orc_apply(N, n_pad, _p(st, _ip), _p(None if st_len is None else _c(st_len, np.int32), _ip),
+                    _p(_c(w, np.float64)), T, _p(u), _p(out), 0, N, nthreads)
+    return out
+
+
+def cosine_bell_coeffs(xyz, a=1.0, alpha=np.pi / 2, u0=None, revolution=1.0):
+    xyz = _c(xyz, np.float64)
+    N = xyz.shape[0]
+    if u0 is None:
+        u0 = 2.0 * np.pi * a / revolution
+    cu = np.zeros(N)
+    cv = np.zeros(N)
+    lib().orc_cosine_bell_coeffs(N, _p(xyz), a, alpha, u0, _p(cu), _p(cv))
+    return cu, cv
+
+
+def rk4_advect(st, st_len, w_lambda, w_theta, w_hv, cu, cv, u, dt, nsteps, nthreads=0):
+    st = _c(st, np.int32)
+    N, n_pad = st.shape
+    u = np.array(u, dtype=np.float64, order="C", copy=True)
+    T = 1 if u.ndim == 1 else u.shape[1]
+    hv = None if w_hv is None else _c(w_hv, np.float64)
+    rc = lib().orc_rk4_advect(N, n_pad, _p(st, _ip), _p(None if st_len is None else _c(st_len, np.int32), _ip),
+                              _p(_c(w_lambda, np.float64)), _p(_c(w_theta, np.float64)), _p(hv),
+                              _p(_c(cu, np.float64)), _p(_c(cv, np.float64)), T, _p(u), dt, nsteps, nthreads)
+    if rc:
+        raise MemoryError("oracle rk4")
+    return u
+
+
+def rk4_heat(st, st_len, w_lsfc, u, dt, nsteps, kappa=1.0, nthreads=0):
+    st = _c(st, np.int32)
+    N, n_pad = st.shape
+    u = np.array(u, dtype=np.float64, order="C", copy=True)
+    T = 1 if u.ndim == 1 else u.shape[1]
+    rc = lib().orc_rk4_heat(N, n_pad, _p(st, _ip), _p(None if st_len is None else _c(st_len, np.int32), _ip),
+                            _p(_c(w_lsfc, np.float64)), kappa, T, _p(u), dt, nsteps, nthreads)
+    if rc:
+        raise MemoryError("oracle rk4")
+    return u
+
+
+def ref_knn(xyz, k):
+    L = ref_lib("ref_kdtree")
+    if L is None:
+        return None
+    xyz = _c(xyz, np.float64)
+    N = xyz.shape[0]
+    idx = np.zeros((N, k), dtype=np.int32)
+    d = np.zeros((N, k))
+    if L.ref_knn(_p(xyz), N, k, _p(idx, _ip), _p(d)) != 0:
+        raise RuntimeError("reference kd-tree returned a short list")
+    return idx, d
+
+
+def cart2sph(x, y, z):
+    t, p = ctypes.c_double(), ctypes.c_double()
+    lib().orc_cart2sph(x, y, z, ctypes.byref(t), ctypes.byref(p))
+    return t.value, p.value
+
+
+def max_threads():
+    return lib().orc_max_threads()

@@ -1,0 +1,88 @@
+"""Build recipe for the oracle (test infrastructure, never shipped).
+
+* ``oracle/_build/liboracle.so`` -- the C restatement in ``oracle.c``
+  (gcc, FP64, ``-ffp-contract=off``, OpenMP for the CPU baseline).
+* ``oracle/_ref/libref_kdtree.so`` -- the reference's own ``external/kdtree/KDTree.h``
+  compiled from its sources where they lie (plus ``external/timers/timer_eb.cpp`` and
+  ``external/graphics_lib/utilities/Vec3d.cpp``).
+* ``oracle/_ref/libref_rbf.so`` -- the reference's own ``src/rbffd/rbfs/rbf_gaussian.h``
+  and ``src/utils/geom/cart2sph.cpp``, with ``oracle/shim/armadillo`` standing in
+  for the Armadillo header that ``rbf.h`` includes.
+
+The reference's full RBFFD class (``src/rbffd/rbffd.cpp``) needs Armadillo,
+LAPACK, MPI and Boost, none of which exist here, so it is treated as
+unbuildable; ``oracle.c`` restates it instead.  The ``_ref`` libraries are
+built only where the reference tree exists and travel prebuilt elsewhere.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("RBFFD_REFERENCE_ROOT", "/root/reference")
+
+
+def _newer(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources if os.path.exists(s))
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("oracle build failed: " + " ".join(cmd))
+
+
+def build_oracle(force=False):
+    out = os.path.join(HERE, "_build", "liboracle.so")
+    src = os.path.join(HERE, "oracle.c")
+    if force or _newer(out, [src]):
+        os.makedirs(os.path.dirname(out), exist_ok=True)
+        _run(["gcc", "-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-std=c11",
+              src, "-o", out, "-lm"])
+    return out
+
+
+def build_ref(force=False):
+    """Compile the reference pieces; returns the list of built paths ([] if no reference tree)."""
+    if not os.path.isdir(os.path.join(REF, "external", "kdtree")):
+        return []
+    outdir = os.path.join(HERE, "_ref")
+    os.makedirs(outdir, exist_ok=True)
+    util = os.path.join(REF, "external", "graphics_lib", "utilities")
+    # KDTree's MyHeaps.h uses dynamic exception specifications, so it needs
+    # C++98; the RBF header builds with the compiler's default standard, where
+    # pow(double, int) is pow(double, double) as in C (under C++98 libstdc++
+    # would use repeated multiplication instead, a 1-ulp difference in HV).
+    common = ["g++", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-w",
+              "-DUSE_DOUBLE_VEC3", "-include", "ctime", "-include", "cstdio"]
+    built = []
+    kd = os.path.join(outdir, "libref_kdtree.so")
+    kd_src = [os.path.join(HERE, "ref_kdtree.cpp"), os.path.join(REF, "external/kdtree/KDTree.h"),
+              os.path.join(REF, "external/kdtree/MyHeaps.h")]
+    if force or _newer(kd, kd_src):
+        _run(common + ["-std=c++98", "-I" + os.path.join(REF, "external/kdtree"), "-I" + os.path.join(REF, "external/timers"),
+                       "-I" + util, kd_src[0], os.path.join(REF, "external/timers/timer_eb.cpp"),
+                       os.path.join(util, "Vec3d.cpp"), "-o", kd])
+    built.append(kd)
+    rb = os.path.join(outdir, "libref_rbf.so")
+    rb_src = [os.path.join(HERE, "ref_rbf.cpp"), os.path.join(REF, "src/rbffd/rbfs/rbf_gaussian.h"),
+              os.path.join(REF, "src/utils/geom/cart2sph.cpp")]
+    if force or _newer(rb, rb_src):
+        _run(common + ["-I" + os.path.join(HERE, "shim"), "-I" + os.path.join(REF, "src/rbffd"),
+                       "-I" + os.path.join(REF, "src"), "-I" + util, rb_src[0], rb_src[2],
+                       os.path.join(util, "Vec3d.cpp"), os.path.join(util, "CVec3.cpp"), "-o", rb])
+    built.append(rb)
+    return built
+
+
+def build(force=False):
+    return [build_oracle(force)] + build_ref(force)
+
+
+if __name__ == "__main__":
+    for p in build(force="--force" in sys.argv):
+        print(p)

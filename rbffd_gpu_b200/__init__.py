@@ -1,0 +1,14 @@
+"""B200 (sm_100a) RBF-FD hot path: batched FP64 stencil weights, fused ELL
+derivative / hyperviscosity application and RK4, behind the reference's
+RBFFD / TimeDependentPDE interface (src/rbffd/rbffd.h, src/pdes/time_dependent_pde.h).
+
+The compute lives in librbffd_sm100.so (CUDA C++ for sm_100a, C ABI in
+include/rbffd_sm100.h); this package is a thin Python view of that ABI used
+by the tests and the benchmark.  The C++ view for drop-in use is in
+rbffd_gpu_b200/cpp/.
+"""
+from .api import (  # noqa: F401
+    F32, F64, X, Y, Z, LAPL, R, HV, LAMBDA, THETA, LSFC, XSFC, YSFC, ZSFC, INTERP, RK4,
+    RbffdError, Context, Grid, RBFFD, TimeDependentPDE, CosineBell, HeatSphere, Advection,
+    fibonacci_nodes, knn_stencils, exact_cosine_bell, exact_sph_heat, device_count, version,
+)

@@ -1,0 +1,83 @@
+"""ctypes binding of librbffd_sm100.so (the C ABI in include/rbffd_sm100.h).
+
+Loading fails loudly when the shared library has not been built: there is no
+CPU fallback for any product entry point.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "librbffd_sm100.so")
+
+c_int, c_uint, c_double, c_size_t, c_void_p, c_char_p = (ctypes.c_int, ctypes.c_uint, ctypes.c_double, ctypes.c_size_t,
+                                                          ctypes.c_void_p, ctypes.c_char_p)
+c_uint64 = ctypes.c_uint64
+P = ctypes.POINTER
+dp = P(c_double)
+ip = P(c_int)
+
+
+class WeightParams(ctypes.Structure):
+    _fields_ = [("der_types", c_uint), ("dim", c_int), ("poly_deg", c_int), ("hv_k", c_int), ("hv_gamma", c_double),
+                ("hv_nodes", c_double)]
+
+
+class PdeParams(ctypes.Structure):
+    _fields_ = [("rhs_kind", c_int), ("ntracers", c_int), ("dtype", c_int), ("use_hv", c_int),
+                ("sphere_radius", c_double), ("alpha", c_double), ("u0", c_double), ("kappa", c_double),
+                ("cu", dp), ("cv", dp)]
+
+
+# name -> (restype, argtypes)
+PROTOTYPES = {
+    "rbffd_version": (c_char_p, []),
+    "rbffd_status_string": (c_char_p, [c_int]),
+    "rbffd_device_count": (c_int, [ip]),
+    "rbffd_ctx_create": (c_int, [c_int, P(c_void_p)]),
+    "rbffd_ctx_destroy": (c_int, [c_void_p]),
+    "rbffd_ctx_last_error": (c_char_p, [c_void_p]),
+    "rbffd_ctx_synchronize": (c_int, [c_void_p]),
+    "rbffd_ctx_mem_info": (c_int, [c_void_p, P(c_size_t), P(c_size_t), P(c_size_t)]),
+    "rbffd_ctx_stream": (c_int, [c_void_p, P(c_void_p)]),
+    "rbffd_nodes_fibonacci": (c_int, [c_int, c_uint64, dp]),
+    "rbffd_stencils_knn": (c_int, [dp, c_int, c_int, ip, ip, c_int]),
+    "rbffd_exact_cosine_bell": (c_int, [c_int, dp, c_double, dp]),
+    "rbffd_exact_sph_heat": (c_int, [c_int, dp, c_int, dp, c_double, c_double, dp]),
+    "rbffd_grid_create": (c_int, [c_void_p, c_int, dp, c_int, ip, ip, P(c_void_p)]),
+    "rbffd_grid_destroy": (c_int, [c_void_p]),
+    "rbffd_grid_nbytes": (c_int, [c_void_p, P(c_size_t)]),
+    "rbffd_weights_compute": (c_int, [c_void_p, P(WeightParams), dp, c_double, ip]),
+    "rbffd_weights_assemble": (c_int, [c_void_p, P(WeightParams), dp, c_double, ip, ip, c_int, dp]),
+    "rbffd_weights_set": (c_int, [c_void_p, c_uint, dp]),
+    "rbffd_weights_get": (c_int, [c_void_p, c_uint, dp]),
+    "rbffd_apply": (c_int, [c_void_p, c_uint, c_int, c_uint, c_uint, dp, dp]),
+    "rbffd_apply_dev": (c_int, [c_void_p, c_uint, c_int, c_int, c_void_p, c_void_p]),
+    "rbffd_batched_gesv_dev": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "rbffd_pde_create": (c_int, [c_void_p, P(PdeParams), P(c_void_p)]),
+    "rbffd_pde_destroy": (c_int, [c_void_p]),
+    "rbffd_pde_set_state": (c_int, [c_void_p, dp]),
+    "rbffd_pde_get_state": (c_int, [c_void_p, dp]),
+    "rbffd_pde_set_time": (c_int, [c_void_p, c_double]),
+    "rbffd_pde_get_time": (c_int, [c_void_p, dp]),
+    "rbffd_pde_advance": (c_int, [c_void_p, c_int, c_double, c_int, c_int]),
+    "rbffd_pde_set_shape": (c_int, [c_void_p, c_int, c_int]),
+    "rbffd_pde_get_shape": (c_int, [c_void_p, ip, ip]),
+}
+
+_LIB = None
+
+
+def load():
+    """Load the built library; raises if it is missing (no fallback)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("librbffd_sm100.so is not built (run __graft_entry__.build() or "
+                              "python rbffd_gpu_b200/build.py): " + LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in PROTOTYPES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB

@@ -1,0 +1,351 @@
+"""Python view of the C ABI, shaped like the reference classes it replaces.
+
+``RBFFD`` mirrors src/rbffd/rbffd.h (DerType flags, setters,
+computeAllWeightsForAllStencils, applyWeightsForDeriv, getStencilWeights);
+``TimeDependentPDE`` / ``CosineBell`` mirror src/pdes/time_dependent_pde.h and
+src/pdes/hyperbolic/cosine_bell.h (advance(RK4, dt), fillInitialConditions,
+getTime).  Every method calls librbffd_sm100.so; errors raise RbffdError with
+the library's message.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+F32, F64 = 0, 1
+X, Y, Z, LAPL, R, HV, LAMBDA, THETA = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20, 0x40, 0x80
+LSFC, XSFC, YSFC, ZSFC, INTERP = 0x100, 0x200, 0x400, 0x800, 0x8000
+EULER, MIDPOINT, RK4 = 0, 1, 2  # TimeDependentPDE::TimeScheme (time_dependent_pde.h:20)
+
+ADVANCE_GRAPH, ADVANCE_UNFUSED, ADVANCE_ASYNC = 0x1, 0x2, 0x4
+RHS_COSINE_BELL, RHS_HEAT, RHS_ADVECTION = 1, 2, 3
+
+
+class RbffdError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s (%d): %s" % (_lib.load().rbffd_status_string(status).decode(), status, message))
+        self.status = status
+
+
+def _dp(a):
+    return a.ctypes.data_as(_lib.dp)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_lib.ip)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def version():
+    return _lib.load().rbffd_version().decode()
+
+
+def device_count():
+    n = ctypes.c_int(0)
+    rc = _lib.load().rbffd_device_count(ctypes.byref(n))
+    return n.value if rc == 0 else 0
+
+
+# ---------------------------------------------------------------------------
+# host-side inputs
+
+def fibonacci_nodes(N, seed):
+    xyz = np.zeros((N, 3))
+    rc = _lib.load().rbffd_nodes_fibonacci(N, seed, _dp(xyz))
+    if rc:
+        raise RbffdError(rc, "rbffd_nodes_fibonacci")
+    return xyz
+
+
+def knn_stencils(xyz, n, nthreads=0, return_ties=False):
+    xyz = _f64(xyz)
+    N = xyz.shape[0]
+    st = np.zeros((N, n), dtype=np.int32)
+    ties = ctypes.c_int(0)
+    rc = _lib.load().rbffd_stencils_knn(_dp(xyz), N, n, _ip(st), ctypes.byref(ties), nthreads)
+    if rc:
+        raise RbffdError(rc, "rbffd_stencils_knn")
+    return (st, ties.value) if return_ties else st
+
+
+def exact_cosine_bell(xyz, a=1.0):
+    xyz = _f64(xyz)
+    h = np.zeros(xyz.shape[0])
+    rc = _lib.load().rbffd_exact_cosine_bell(xyz.shape[0], _dp(xyz), a, _dp(h))
+    if rc:
+        raise RbffdError(rc, "rbffd_exact_cosine_bell")
+    return h
+
+
+def exact_sph_heat(xyz, lmax, coeffs, t, kappa=1.0):
+    xyz = _f64(xyz)
+    coeffs = _f64(coeffs)
+    if coeffs.size != (lmax + 1) ** 2:
+        raise ValueError("need (lmax+1)^2 coefficients")
+    u = np.zeros(xyz.shape[0])
+    rc = _lib.load().rbffd_exact_sph_heat(xyz.shape[0], _dp(xyz), lmax, _dp(coeffs), kappa, t, _dp(u))
+    if rc:
+        raise RbffdError(rc, "rbffd_exact_sph_heat")
+    return u
+
+
+# ---------------------------------------------------------------------------
+
+class Context:
+    """One CUDA device, one stream; owns every device buffer made from it."""
+
+    def __init__(self, device=0):
+        self.L = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self.L.rbffd_ctx_create(device, ctypes.byref(h))
+        if rc:
+            raise RbffdError(rc, "rbffd_ctx_create(device=%d)" % device)
+        self.h = h
+        self.device = device
+
+    def check(self, rc, what=""):
+        if rc:
+            raise RbffdError(rc, "%s: %s" % (what, self.L.rbffd_ctx_last_error(self.h).decode()))
+
+    def synchronize(self):
+        self.check(self.L.rbffd_ctx_synchronize(self.h), "synchronize")
+
+    def mem_info(self):
+        held, free, total = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t()
+        self.check(self.L.rbffd_ctx_mem_info(self.h, ctypes.byref(held), ctypes.byref(free), ctypes.byref(total)))
+        return held.value, free.value, total.value
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self.check(self.L.rbffd_ctx_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.rbffd_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Grid:
+    """Nodes and stencils (the reference Grid: getNodeList, getStencils, getMaxStencilSize)."""
+
+    def __init__(self, ctx, nodes, stencils, st_len=None, global_nodes=None):
+        self.ctx = ctx
+        self.nodes = _f64(nodes)
+        self.stencils = _i32(stencils)
+        self.N, self.n_pad = self.stencils.shape
+        self.st_len = None if st_len is None else _i32(st_len)
+        self.global_nodes = global_nodes or self.N
+        h = ctypes.c_void_p()
+        ctx.check(ctx.L.rbffd_grid_create(ctx.h, self.N, _dp(self.nodes), self.n_pad, _ip(self.stencils),
+                                          None if self.st_len is None else _ip(self.st_len), ctypes.byref(h)),
+                  "rbffd_grid_create")
+        self.h = h
+
+    def getNodeList(self):
+        return self.nodes
+
+    def getStencils(self):
+        return self.stencils
+
+    def getStencilsSize(self):
+        return self.N
+
+    def getNodeListSize(self):
+        return self.N
+
+    def getGlobalNodeListSize(self):
+        return self.global_nodes
+
+    def getMaxStencilSize(self):
+        return self.n_pad
+
+    def nbytes(self):
+        b = ctypes.c_size_t()
+        self.ctx.check(self.ctx.L.rbffd_grid_nbytes(self.h, ctypes.byref(b)))
+        return b.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.rbffd_grid_destroy(self.h)
+            self.h = None
+
+
+class RBFFD:
+    """Mirror of class RBFFD (src/rbffd/rbffd.h:29-547) on the device."""
+    X, Y, Z, LAPL, R, HV, LAMBDA, THETA = X, Y, Z, LAPL, R, HV, LAMBDA, THETA
+    LSFC, XSFC, YSFC, ZSFC, INTERP = LSFC, XSFC, YSFC, ZSFC, INTERP
+
+    def __init__(self, typesToCompute, grid, dim_num, rank=0):
+        self.computedTypes = typesToCompute
+        self.grid = grid
+        self.dim_num = dim_num
+        self.rank = rank
+        self.hv_k, self.hv_gamma = 2, 8e-4  # ctor defaults (rbffd.cpp:26)
+        self.useHyperviscosity = 0
+        self.var_epsilon = np.ones(grid.N)
+        self.poly_deg = 0  # ONE_MONOMIAL (rbffd.cpp:1)
+        self.deg_per_row = None
+
+    # -- parameters (rbffd.h:213-381) --
+    def setUseHyperviscosity(self, tf):
+        self.useHyperviscosity = int(tf)
+        self.computedTypes = (self.computedTypes | HV) if tf else (self.computedTypes & ~HV)
+
+    def appendDerTypes(self, t):
+        self.computedTypes |= t
+
+    def setHVScalars(self, k, gamma_c):
+        self.hv_k, self.hv_gamma = int(k), float(gamma_c)
+        return self.hv_gamma
+
+    def getHVScalar(self):
+        return -self.hv_gamma * float(self.grid.getGlobalNodeListSize()) ** (-self.hv_k)
+
+    def setEpsilon(self, eps):
+        if np.isscalar(eps):
+            self.var_epsilon[:] = float(eps)
+        else:
+            eps = _f64(eps)
+            if eps.shape != self.var_epsilon.shape:
+                raise ValueError("length of support params list does not match")
+            self.var_epsilon = eps.copy()
+
+    def setEpsilonByParameters(self, c1, c2):
+        self.setEpsilon(c1 * np.sqrt(self.grid.getGlobalNodeListSize()) - c2)
+
+    def setPolynomialDegree(self, deg, deg_per_row=None):
+        """Beyond the reference (which fixes np = 1): -1 none, 0 constant, 1..4."""
+        self.poly_deg = int(deg)
+        self.deg_per_row = None if deg_per_row is None else _i32(deg_per_row)
+
+    # -- weights --
+    def computeAllWeightsForAllStencils(self):
+        ctx = self.grid.ctx
+        p = _lib.WeightParams(self.computedTypes, self.dim_num, self.poly_deg, self.hv_k, self.hv_gamma,
+                              float(self.grid.getGlobalNodeListSize()))
+        ctx.check(ctx.L.rbffd_weights_compute(self.grid.h, ctypes.byref(p), _dp(self.var_epsilon), 0.0,
+                                              None if self.deg_per_row is None else _ip(self.deg_per_row)),
+                  "rbffd_weights_compute")
+
+    def setWeights(self, which, w):
+        w = _f64(w)
+        ctx = self.grid.ctx
+        ctx.check(ctx.L.rbffd_weights_set(self.grid.h, which, _dp(w)), "rbffd_weights_set")
+
+    def getWeights(self, which):
+        w = np.zeros((self.grid.N, self.grid.n_pad))
+        ctx = self.grid.ctx
+        ctx.check(ctx.L.rbffd_weights_get(self.grid.h, which, _dp(w)), "rbffd_weights_get")
+        return w
+
+    def getStencilWeights(self, which, st_indx):
+        return self.getWeights(which)[st_indx]
+
+    # -- apply (rbffd.h:257-274) --
+    def applyWeightsForDeriv(self, which, u, deriv=None, isChangedU=True, start_indx=0, nb_stencils=None, dtype=F64):
+        u = _f64(u)
+        N = self.grid.N
+        if nb_stencils is None:
+            nb_stencils = N - start_indx
+        if deriv is None:
+            deriv = np.zeros(N)
+        ctx = self.grid.ctx
+        ctx.check(ctx.L.rbffd_apply(self.grid.h, which, dtype, start_indx, nb_stencils, _dp(u), _dp(deriv)),
+                  "rbffd_apply")
+        return deriv
+
+    def applyWeightsForDerivDev(self, which, u_ptr, out_ptr, dtype=F64, ntracers=1):
+        ctx = self.grid.ctx
+        ctx.check(ctx.L.rbffd_apply_dev(self.grid.h, which, dtype, ntracers, u_ptr, out_ptr), "rbffd_apply_dev")
+
+
+class TimeDependentPDE:
+    """Device-resident TimeDependentPDE (src/pdes/time_dependent_pde.h:9-126)."""
+
+    def __init__(self, grid, der, params):
+        self.grid, self.der, self.ctx = grid, der, grid.ctx
+        self.T = params.ntracers
+        self.dtype = params.dtype
+        h = ctypes.c_void_p()
+        self.ctx.check(self.ctx.L.rbffd_pde_create(grid.h, ctypes.byref(params), ctypes.byref(h)), "rbffd_pde_create")
+        self.h = h
+
+    def fillInitialConditions(self, values):
+        u = _f64(values).reshape(self.grid.N, self.T) if self.T > 1 else _f64(values)
+        self.ctx.check(self.ctx.L.rbffd_pde_set_state(self.h, _dp(np.ascontiguousarray(u))), "set_state")
+
+    def getLocalSolution(self):
+        u = np.zeros((self.grid.N, self.T)) if self.T > 1 else np.zeros(self.grid.N)
+        self.ctx.check(self.ctx.L.rbffd_pde_get_state(self.h, _dp(u)), "get_state")
+        return u
+
+    def advance(self, which=RK4, delta_t=1.0, nsteps=1, graph=False, unfused=False, asynchronous=False):
+        flags = (ADVANCE_GRAPH if graph else 0) | (ADVANCE_UNFUSED if unfused else 0) | (
+            ADVANCE_ASYNC if asynchronous else 0)
+        self.ctx.check(self.ctx.L.rbffd_pde_advance(self.h, which, delta_t, nsteps, flags), "rbffd_pde_advance")
+
+    def setTime(self, t):
+        self.ctx.check(self.ctx.L.rbffd_pde_set_time(self.h, t))
+
+    def getTime(self):
+        t = ctypes.c_double()
+        self.ctx.check(self.ctx.L.rbffd_pde_get_time(self.h, ctypes.byref(t)))
+        return t.value
+
+    def setShape(self, lanes_per_row=0, block_threads=0):
+        self.ctx.check(self.ctx.L.rbffd_pde_set_shape(self.h, lanes_per_row, block_threads), "set_shape")
+
+    def getShape(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self.ctx.check(self.ctx.L.rbffd_pde_get_shape(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.rbffd_pde_destroy(self.h)
+            self.h = None
+
+
+class CosineBell(TimeDependentPDE):
+    """CosineBell(grid, der, earth_radius, velocity_angle, one_revolution_in_seconds, useHyperviscosity)
+    (src/pdes/hyperbolic/cosine_bell.h:31-46)."""
+
+    def __init__(self, grid, der, earth_radius, velocity_angle, one_revolution_in_seconds, useHyperviscosity,
+                 dtype=F64, ntracers=1):
+        u0 = (2.0 * np.pi * earth_radius) / one_revolution_in_seconds
+        p = _lib.PdeParams(RHS_COSINE_BELL, ntracers, dtype, int(useHyperviscosity), earth_radius, velocity_angle, u0,
+                           1.0, None, None)
+        super().__init__(grid, der, p)
+
+
+class HeatSphere(TimeDependentPDE):
+    """u_t = kappa * Laplace-Beltrami(u) with the LSFC operator (rbffd.cpp:458-464)."""
+
+    def __init__(self, grid, der, kappa=1.0, dtype=F64, ntracers=1):
+        p = _lib.PdeParams(RHS_HEAT, ntracers, dtype, 0, 1.0, 0.0, 0.0, kappa, None, None)
+        super().__init__(grid, der, p)
+
+
+class Advection(TimeDependentPDE):
+    """f = -(cu * D_lambda h + cv * D_theta h) [+ D_hv h] with caller-given per-node coefficients."""
+
+    def __init__(self, grid, der, cu, cv, useHyperviscosity, dtype=F64, ntracers=1):
+        self._cu, self._cv = _f64(cu), _f64(cv)
+        p = _lib.PdeParams(RHS_ADVECTION, ntracers, dtype, int(useHyperviscosity), 1.0, 0.0, 0.0, 1.0,
+                           _dp(self._cu), _dp(self._cv))
+        super().__init__(grid, der, p)

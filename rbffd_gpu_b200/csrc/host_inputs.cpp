@@ -1,0 +1,253 @@
+// Host-side input builders for the RBF-FD path: synthetic sphere nodes,
+// k-nearest-neighbour stencils and the exact solutions used as initial
+// conditions.  These produce the inputs the reference's Grid and ExactSolution
+// classes produce; nothing here runs on the GPU.
+//
+//   rbffd_nodes_fibonacci  -- stands in for the reference's maximum-determinant
+//                             node files (GridReader, src/grids/grid_reader.*),
+//                             which are not distributed with the reference.
+//   rbffd_stencils_knn     -- Grid::generateStencilsKDTree
+//                             (src/grids/grid_interface.cpp:688-725): the n nearest
+//                             nodes, closest first, centre at [0].
+//   rbffd_exact_cosine_bell -- ExactAdvection::operator()
+//                             (tests/experiments/cosine_bell_on_sphere/exact_advection.h:37-53)
+//   rbffd_exact_sph_heat   -- heat on the unit sphere: sum c_lm e^{-l(l+1)t} Y_lm.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "../../include/rbffd_sm100.h"
+
+namespace {
+
+uint64_t splitmix64(uint64_t& s)
+{
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+double uniform01(uint64_t& s) { return (double)(splitmix64(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+int default_threads(int nthreads)
+{
+    if (nthreads > 0) return nthreads;
+    unsigned h = std::thread::hardware_concurrency();
+    return h ? (int)h : 1;
+}
+
+template <class F>
+void parallel_for(int n, int nthreads, F&& f)
+{
+    nthreads = std::max(1, std::min(default_threads(nthreads), n));
+    if (nthreads == 1) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::atomic<int> next(0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; t++)
+        pool.emplace_back([&]() {
+            for (;;) {
+                int b = next.fetch_add(256);
+                if (b >= n) break;
+                int e = std::min(n, b + 256);
+                for (int i = b; i < e; i++) f(i);
+            }
+        });
+    for (auto& th : pool) th.join();
+}
+
+}  // namespace
+
+extern "C" int rbffd_nodes_fibonacci(int N, uint64_t seed, double* xyz)
+{
+    if (N <= 0 || !xyz) return RBFFD_ERR_INVALID;
+    // Uniform random rotation from three uniforms (Shoemake's quaternion method).
+    uint64_t s = seed;
+    double u1 = uniform01(s), u2 = uniform01(s), u3 = uniform01(s);
+    const double two_pi = 6.283185307179586476925286766559;
+    double q0 = std::sqrt(1.0 - u1) * std::sin(two_pi * u2), q1 = std::sqrt(1.0 - u1) * std::cos(two_pi * u2);
+    double q2 = std::sqrt(u1) * std::sin(two_pi * u3), q3 = std::sqrt(u1) * std::cos(two_pi * u3);
+    // rotation matrix of the unit quaternion (w=q3, x=q0, y=q1, z=q2)
+    double w = q3, x = q0, y = q1, z = q2;
+    double R[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)},
+                      {2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)},
+                      {2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)}};
+    const double golden = 3.14159265358979323846264338327950288 * (3.0 - std::sqrt(5.0));
+    for (int i = 0; i < N; i++) {
+        double zz = 1.0 - (2.0 * i + 1.0) / N;
+        double r = std::sqrt(std::max(0.0, 1.0 - zz * zz));
+        double ph = golden * (double)i;
+        double p[3] = {r * std::cos(ph), r * std::sin(ph), zz};
+        double q[3];
+        for (int a = 0; a < 3; a++) q[a] = R[a][0] * p[0] + R[a][1] * p[1] + R[a][2] * p[2];
+        double nrm = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+        for (int a = 0; a < 3; a++) xyz[3 * (size_t)i + a] = q[a] / nrm;
+    }
+    return RBFFD_OK;
+}
+
+// Squared distance with the summation order of the reference k-d tree's
+// distance_squared (external/kdtree/KDTree.h:45-51): ((0 + dx^2) + dy^2) + dz^2.
+static inline double dist2(const double* a, const double* b)
+{
+    double d = 0;
+    for (int i = 0; i < 3; i++) d += (a[i] - b[i]) * (a[i] - b[i]);
+    return d;
+}
+
+extern "C" int rbffd_stencils_knn(const double* xyz, int N, int n, int* st, int* ties, int nthreads)
+{
+    if (!xyz || !st || N <= 0 || n <= 0 || n > N) return RBFFD_ERR_INVALID;
+    // Uniform cell grid over the bounding box; cell edge ~ half the radius
+    // expected to hold n points on the unit sphere.
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < N; i++)
+        for (int a = 0; a < 3; a++) {
+            lo[a] = std::min(lo[a], xyz[3 * (size_t)i + a]);
+            hi[a] = std::max(hi[a], xyz[3 * (size_t)i + a]);
+        }
+    double rk = std::sqrt(4.0 * n / (double)N);
+    double h = std::max(rk * 0.5, 1e-12);
+    int dims[3];
+    for (int a = 0; a < 3; a++) {
+        double ext = hi[a] - lo[a];
+        dims[a] = std::max(1, std::min(400, (int)std::ceil(ext / h) + 1));
+    }
+    double hc[3];
+    for (int a = 0; a < 3; a++) hc[a] = std::max((hi[a] - lo[a]) / dims[a], 1e-300) * (1.0 + 1e-12);
+    size_t ncell = (size_t)dims[0] * dims[1] * dims[2];
+    std::vector<int> cell_of(N), start(ncell + 1, 0), order(N);
+    auto cell_coord = [&](const double* p, int a) {
+        int c = (int)std::floor((p[a] - lo[a]) / hc[a]);
+        return std::max(0, std::min(dims[a] - 1, c));
+    };
+    for (int i = 0; i < N; i++) {
+        const double* p = xyz + 3 * (size_t)i;
+        size_t c = ((size_t)cell_coord(p, 0) * dims[1] + cell_coord(p, 1)) * dims[2] + cell_coord(p, 2);
+        cell_of[i] = (int)c;
+        start[c + 1]++;
+    }
+    for (size_t c = 0; c < ncell; c++) start[c + 1] += start[c];
+    {
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (int i = 0; i < N; i++) order[fill[cell_of[i]]++] = i;
+    }
+    double minh = std::min(hc[0], std::min(hc[1], hc[2]));
+    std::atomic<int> tie_count(0);
+    std::atomic<int> failed(0);
+    parallel_for(N, nthreads, [&](int i) {
+        const double* q = xyz + 3 * (size_t)i;
+        int cc[3] = {cell_coord(q, 0), cell_coord(q, 1), cell_coord(q, 2)};
+        std::vector<std::pair<double, int>> cand;
+        cand.reserve(4 * n);
+        int maxr = std::max(dims[0], std::max(dims[1], dims[2]));
+        for (int R = 0; R <= maxr; R++) {
+            // add the shell of cells at Chebyshev distance R
+            for (int a = cc[0] - R; a <= cc[0] + R; a++) {
+                if (a < 0 || a >= dims[0]) continue;
+                for (int b = cc[1] - R; b <= cc[1] + R; b++) {
+                    if (b < 0 || b >= dims[1]) continue;
+                    for (int c = cc[2] - R; c <= cc[2] + R; c++) {
+                        if (c < 0 || c >= dims[2]) continue;
+                        int ring = std::max(std::abs(a - cc[0]), std::max(std::abs(b - cc[1]), std::abs(c - cc[2])));
+                        if (ring != R) continue;
+                        size_t cell = ((size_t)a * dims[1] + b) * dims[2] + c;
+                        for (int t = start[cell]; t < start[cell + 1]; t++) {
+                            int j = order[t];
+                            cand.emplace_back(dist2(q, xyz + 3 * (size_t)j), j);
+                        }
+                    }
+                }
+            }
+            if ((int)cand.size() >= n) {
+                std::nth_element(cand.begin(), cand.begin() + (n - 1), cand.end());
+                double kth = cand[n - 1].first;
+                double reach = R * minh;  // every unsearched node is farther than this
+                if (kth < reach * reach || R == maxr) break;
+            }
+        }
+        if ((int)cand.size() < n) {
+            failed.store(1);
+            return;
+        }
+        std::sort(cand.begin(), cand.end());  // (distance, index): closest first
+        int* out = st + (size_t)i * n;
+        for (int k = 0; k < n; k++) out[k] = cand[k].second;
+        if (out[0] != i) {
+            // duplicate point at distance 0 sorted ahead of the centre: put the centre first
+            for (int k = 1; k < n; k++)
+                if (out[k] == i) { std::swap(out[0], out[k]); break; }
+        }
+        for (int k = 0; k + 1 < (int)cand.size() && k < n; k++)
+            if (cand[k].first == cand[k + 1].first) { tie_count.fetch_add(1); break; }
+    });
+    if (ties) *ties = tie_count.load();
+    return failed.load() ? RBFFD_ERR_INVALID : RBFFD_OK;
+}
+
+extern "C" int rbffd_exact_cosine_bell(int N, const double* xyz, double a, double* h)
+{
+    if (N < 0 || !xyz || !h) return RBFFD_ERR_INVALID;
+    const double PI = 3.14159265358979323846264338327950288;
+    const double h0 = 1.0, R = a / 3.0, lambda_c = (3. * PI) / 2., theta_c = 0.;
+    for (int i = 0; i < N; i++) {
+        double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
+        double LI = std::atan2(y, x), TI = std::atan2(z, std::sqrt(x * x + y * y));
+        double r = a * std::acos(std::sin(theta_c) * std::sin(TI) + std::cos(theta_c) * std::cos(TI) * std::cos(LI - lambda_c));
+        double v = (h0 / 2.) * (1. + std::cos(PI * (r / R)));
+        h[i] = (r >= R) ? 0.0 : v;
+    }
+    return RBFFD_OK;
+}
+
+// Real, orthonormal spherical harmonics Y_lm on the unit sphere, l <= lmax,
+// coefficient order (l, m = -l..l).  u(x, t) = sum c_lm exp(-kappa l(l+1) t) Y_lm(x):
+// the exact solution of u_t = kappa * Laplace-Beltrami(u).
+extern "C" int rbffd_exact_sph_heat(int N, const double* xyz, int lmax, const double* coeffs, double kappa, double t,
+                                    double* u)
+{
+    if (N < 0 || !xyz || !coeffs || !u || lmax < 0 || lmax > 200) return RBFFD_ERR_INVALID;
+    const double PI = 3.14159265358979323846264338327950288;
+    std::vector<double> decay(lmax + 1);
+    for (int l = 0; l <= lmax; l++) decay[l] = std::exp(-kappa * l * (l + 1.0) * t);
+    parallel_for(N, 0, [&](int i) {
+        double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
+        double rho = std::sqrt(x * x + y * y);
+        double ct = z, st = rho;  // cos/sin of colatitude
+        double lam = std::atan2(y, x);
+        std::vector<double> P((size_t)(lmax + 1) * (lmax + 1));
+        auto idx = [&](int l, int m) { return (size_t)l * (lmax + 1) + m; };
+        // fully normalised associated Legendre functions (4pi-normalised / 4pi)
+        P[idx(0, 0)] = std::sqrt(1.0 / (4.0 * PI));
+        for (int m = 1; m <= lmax; m++) P[idx(m, m)] = -std::sqrt((2.0 * m + 1.0) / (2.0 * m)) * st * P[idx(m - 1, m - 1)];
+        for (int m = 0; m < lmax; m++) P[idx(m + 1, m)] = std::sqrt(2.0 * m + 3.0) * ct * P[idx(m, m)];
+        for (int m = 0; m <= lmax; m++)
+            for (int l = m + 2; l <= lmax; l++) {
+                double a = std::sqrt((4.0 * l * l - 1.0) / ((double)l * l - (double)m * m));
+                double b = std::sqrt(((l - 1.0) * (l - 1.0) - (double)m * m) / (4.0 * (l - 1.0) * (l - 1.0) - 1.0));
+                P[idx(l, m)] = a * (ct * P[idx(l - 1, m)] - b * P[idx(l - 2, m)]);
+            }
+        double s = 0.0;
+        size_t k = 0;
+        for (int l = 0; l <= lmax; l++) {
+            double acc = 0.0;
+            for (int m = -l; m <= l; m++, k++) {
+                int am = m < 0 ? -m : m;
+                double Y = P[idx(l, am)];
+                if (m > 0) Y *= std::sqrt(2.0) * std::cos(am * lam);
+                if (m < 0) Y *= std::sqrt(2.0) * std::sin(am * lam);
+                acc += coeffs[k] * Y;
+            }
+            s += decay[l] * acc;
+        }
+        u[i] = s;
+    });
+    return RBFFD_OK;
+}

@@ -1,0 +1,79 @@
+// Internal declarations shared by the translation units of librbffd_sm100.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/rbffd_sm100.h"
+
+#define RBFFD_VERSION_STRING "rbffd_sm100 0.1.0 (sm_100a)"
+
+// Index of a DerType bit (0..15) or -1.
+inline int der_index(unsigned t)
+{
+    if (t == 0 || (t & (t - 1))) return -1;
+    int i = 0;
+    while (!(t & 1u)) { t >>= 1; i++; }
+    return i < 16 ? i : -1;
+}
+
+struct TuneKey {
+    int kernel, dtype, ntracers, N, n_pad;
+    bool operator<(const TuneKey& o) const
+    {
+        return std::tie(kernel, dtype, ntracers, N, n_pad) < std::tie(o.kernel, o.dtype, o.ntracers, o.N, o.n_pad);
+    }
+};
+struct Shape {
+    int lanes = 0, block = 0;
+};
+
+struct rbffd_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    size_t held = 0;
+    std::mutex mu;
+    std::map<TuneKey, Shape> tuned;  // autotuner results per problem shape
+};
+
+struct rbffd_grid {
+    rbffd_ctx* ctx = nullptr;
+    int N = 0, n_pad = 0, Np = 0;  // Np: column stride of the slot-major ELL arrays (N rounded up to 32)
+    int* d_idx = nullptr;          // [n_pad][Np] node indices, padding = centre
+    int* d_len = nullptr;          // [N] stencil lengths
+    double4* d_xyz = nullptr;      // [N] node coordinates (w unused)
+    double* d_w64[16] = {};        // per operator: [n_pad][Np] FP64 weights, padding 0
+    float* d_w32[16] = {};         // FP32 copies (rounded to nearest)
+    std::vector<int> h_len;        // host copy of stencil lengths
+    size_t bytes = 0;
+};
+
+struct rbffd_pde;  // defined in rk4.cu
+
+// ---- error helpers --------------------------------------------------------
+int set_error(rbffd_ctx* ctx, int status, const char* fmt, ...);
+int cuda_error(rbffd_ctx* ctx, cudaError_t e, const char* what);
+
+#define RBFFD_CUDA_TRY(ctx, call)                                     \
+    do {                                                              \
+        cudaError_t _e = (call);                                      \
+        if (_e != cudaSuccess) return cuda_error((ctx), _e, #call);   \
+    } while (0)
+
+// Device allocation that is accounted against the context.
+int dev_alloc(rbffd_ctx* ctx, void** p, size_t bytes);
+void dev_free(rbffd_ctx* ctx, void* p, size_t bytes);
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// FP32 copy of an FP64 slot-major weight array (kernel in grid.cu).
+int grid_make_f32(rbffd_grid* g, int op);

@@ -1,0 +1,704 @@
+// K3: classical RK4 with the derivative application and the PDE right-hand
+// side fused into each stage (TimeDependentPDE::advanceRungeKutta4,
+// src/pdes/time_dependent_pde.cpp:172-304; the reference GPU form is
+// evaluateRK4_classic / advanceRK4_classic, src/cl_kernels/rk4_thread_per_stencil.cl).
+//
+// One launch per stage.  Stage kernel, per stencil row i (and tracer t):
+//   d_k   = sum_s W_k[s][i] * x[idx[s][i]]            (K = 1..3 operators)
+//   f     = RHS(d_0, d_1, d_2)                         (cosine bell / heat / advection)
+//   stage 0:  acc = f;           xnext = u + (dt/2) f
+//   stage 1:  acc = acc + 2 f;   xnext = u + (dt/2) f
+//   stage 2:  acc = acc + 2 f;   xnext = u + dt f
+//   stage 3:  u   = u + (dt/6)(acc + f)
+// which is the reference's update u + dt/6 (k1 + 2k2 + 2k3 + k4) with the sum
+// evaluated in the same left-to-right order.  Four state buffers (u, two
+// ping-pong stage inputs, acc) replace the reference's eight
+// (time_dependent_pde_cl.cpp:677-708).  The stage input x is gathered while
+// xnext is written, so the two never alias; stage 3 writes u[i] only from row
+// i, which no other row of that launch gathers (it gathers x).
+//
+// FP64 arithmetic uses explicit round-to-nearest intrinsics so the order of
+// operations is fixed: with one lane per row the result equals a CPU loop
+// that fuses the same multiply-adds.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <type_traits>
+
+#include "internal.h"
+
+int grid_apply_dev(rbffd_grid* g, int op, int dtype, int T_tr, const void* u, void* out, int start, int count, int G,
+                   cudaStream_t s);
+
+enum { KIND_ADVECT = 0, KIND_HEAT = 1 };
+
+struct rbffd_pde {
+    rbffd_grid* g = nullptr;
+    rbffd_ctx* ctx = nullptr;
+    int kind = 0, T = 1, dtype = RBFFD_F64, use_hv = 0;
+    int op[3] = {-1, -1, -1};
+    void *u = nullptr, *xa = nullptr, *xb = nullptr, *acc = nullptr;
+    void *cu = nullptr, *cv = nullptr;
+    void *d[3] = {nullptr, nullptr, nullptr};  // unfused path: one output per operator
+    double* stage64 = nullptr;                  // FP64 staging for host state copies of an FP32 PDE
+    double kappa = 1.0;
+    double t = 0.0;
+    Shape shape;
+    bool forced = false;
+    cudaGraphExec_t gexec = nullptr;
+    double g_dt = 0.0;
+    int g_steps = 0;
+    Shape g_shape;
+    size_t bytes = 0;
+};
+
+// ---------------------------------------------------------------------------
+// arithmetic with a fixed rounding sequence
+
+template <typename T>
+struct Ar;
+template <>
+struct Ar<double> {
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+};
+template <>
+struct Ar<float> {
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+};
+
+template <typename T>
+struct StageParams {
+    const int* __restrict__ idx;
+    const T* __restrict__ w0;
+    const T* __restrict__ w1;
+    const T* __restrict__ w2;
+    const T* __restrict__ cu;
+    const T* __restrict__ cv;
+    const T* x;   // gathered stage input
+    T* u;         // u_n (written in stage 3)
+    T* xnext;     // next stage input
+    T* acc;       // RK accumulator
+    T c;          // dt/2, dt/2, dt, dt/6 for stages 0..3
+    T kappa;
+    int N, Np, n_pad, T_tr, stage;
+};
+
+// Right-hand side and the stage update for one (row, tracer) value.
+template <typename T, int KIND, bool HV>
+__device__ __forceinline__ void stage_update(const StageParams<T>& p, int i, size_t e, T d0, T d1, T d2, T cu, T cv)
+{
+    T f;
+    if (KIND == KIND_ADVECT) {
+        // CosineBell::solve: f = -((vel_u/a) * dlambda + (vel_v/a) * dtheta) (+ hv), cosine_bell.cpp:47-57
+        f = -Ar<T>::fma(cu, d0, Ar<T>::mul(cv, d1));
+        if (HV) f = Ar<T>::add(f, d2);
+    } else {
+        f = Ar<T>::mul(p.kappa, d0);
+    }
+    T ui = p.u[e];
+    switch (p.stage) {
+    case 0:
+        p.acc[e] = f;
+        p.xnext[e] = Ar<T>::fma(p.c, f, ui);
+        break;
+    case 1:
+    case 2:
+        p.acc[e] = Ar<T>::add(p.acc[e], Ar<T>::mul(T(2), f));
+        p.xnext[e] = Ar<T>::fma(p.c, f, ui);
+        break;
+    default:
+        p.u[e] = Ar<T>::fma(p.c, Ar<T>::add(p.acc[e], f), ui);
+        break;
+    }
+}
+
+// Single tracer, G lanes per row, slots split across the lanes.
+template <typename T, int KIND, bool HV, int G>
+__global__ void __launch_bounds__(512) k_stage_scalar(StageParams<T> p)
+{
+    int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = gt / G, lane = gt % G;
+    bool active = i < p.N;
+    int ii = active ? i : 0;
+    T d0 = T(0), d1 = T(0), d2 = T(0);
+    const int* __restrict__ ip = p.idx + ii;
+#pragma unroll 4
+    for (int s = lane; s < p.n_pad; s += G) {
+        size_t o = (size_t)s * p.Np;
+        int j = __ldg(ip + o);
+        T xj = p.x[j];
+        d0 = Ar<T>::fma(__ldg(p.w0 + o + ii), xj, d0);
+        if (KIND == KIND_ADVECT) {
+            d1 = Ar<T>::fma(__ldg(p.w1 + o + ii), xj, d1);
+            if (HV) d2 = Ar<T>::fma(__ldg(p.w2 + o + ii), xj, d2);
+        }
+    }
+    if (G > 1) {
+#pragma unroll
+        for (int m = G / 2; m > 0; m >>= 1) {
+            d0 += __shfl_xor_sync(0xffffffffu, d0, m, G);
+            if (KIND == KIND_ADVECT) {
+                d1 += __shfl_xor_sync(0xffffffffu, d1, m, G);
+                if (HV) d2 += __shfl_xor_sync(0xffffffffu, d2, m, G);
+            }
+        }
+    }
+    if (!active || lane != 0) return;
+    T cu = T(0), cv = T(0);
+    if (KIND == KIND_ADVECT) {
+        cu = p.cu[i];
+        cv = p.cv[i];
+    }
+    stage_update<T, KIND, HV>(p, i, (size_t)i, d0, d1, d2, cu, cv);
+}
+
+// Multiple tracers: state [N][T_tr]; VEC consecutive tracers per lane, loaded
+// as one 16-byte vector; T_tr / VEC lanes per row share the row's weights.
+template <typename T, int VEC>
+struct VecT;
+template <>
+struct VecT<float, 4> { typedef float4 type; };
+template <>
+struct VecT<double, 2> { typedef double2 type; };
+template <>
+struct VecT<float, 1> { typedef float type; };
+template <>
+struct VecT<double, 1> { typedef double type; };
+
+template <typename T, int VEC>
+__device__ __forceinline__ void vload(const T* p, T (&v)[VEC])
+{
+    typedef typename VecT<T, VEC>::type V;
+    V t = *reinterpret_cast<const V*>(p);
+    static_assert(sizeof(V) == VEC * sizeof(T), "vector width");
+    memcpy(v, &t, sizeof(V));
+}
+
+template <typename T, int VEC, int KIND, bool HV>
+__global__ void __launch_bounds__(512) k_stage_vec(StageParams<T> p)
+{
+    int lpr = p.T_tr / VEC;
+    int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = gt / lpr, lane = gt % lpr;
+    if (i >= p.N) return;
+    T d0[VEC], d1[VEC], d2[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; v++) d0[v] = d1[v] = d2[v] = T(0);
+    const size_t toff = (size_t)lane * VEC;
+#pragma unroll 2
+    for (int s = 0; s < p.n_pad; s++) {
+        size_t o = (size_t)s * p.Np + i;
+        int j = __ldg(p.idx + o);
+        T xj[VEC];
+        vload<T, VEC>(p.x + (size_t)j * p.T_tr + toff, xj);
+        T a = __ldg(p.w0 + o);
+        T b = KIND == KIND_ADVECT ? __ldg(p.w1 + o) : T(0);
+        T c = (KIND == KIND_ADVECT && HV) ? __ldg(p.w2 + o) : T(0);
+#pragma unroll
+        for (int v = 0; v < VEC; v++) {
+            d0[v] = Ar<T>::fma(a, xj[v], d0[v]);
+            if (KIND == KIND_ADVECT) {
+                d1[v] = Ar<T>::fma(b, xj[v], d1[v]);
+                if (HV) d2[v] = Ar<T>::fma(c, xj[v], d2[v]);
+            }
+        }
+    }
+    T cu = T(0), cv = T(0);
+    if (KIND == KIND_ADVECT) {
+        cu = p.cu[i];
+        cv = p.cv[i];
+    }
+#pragma unroll
+    for (int v = 0; v < VEC; v++)
+        stage_update<T, KIND, HV>(p, i, (size_t)i * p.T_tr + toff + v, d0[v], d1[v], d2[v], cu, cv);
+}
+
+// Unfused right-hand side + stage update from per-operator outputs (the plain path).
+template <typename T, int KIND, bool HV>
+__global__ void k_rhs_axpy(StageParams<T> p, const T* __restrict__ d0, const T* __restrict__ d1, const T* __restrict__ d2)
+{
+    size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)p.N * p.T_tr) return;
+    int i = (int)(e / p.T_tr);
+    T cu = T(0), cv = T(0);
+    if (KIND == KIND_ADVECT) {
+        cu = p.cu[i];
+        cv = p.cv[i];
+    }
+    stage_update<T, KIND, HV>(p, i, e, d0[e], KIND == KIND_ADVECT ? d1[e] : T(0), HV ? d2[e] : T(0), cu, cv);
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+
+template <typename T>
+static StageParams<T> make_params(rbffd_pde* P, int stage, double dt)
+{
+    rbffd_grid* g = P->g;
+    StageParams<T> p;
+    auto W = [&](int k) -> const T* {
+        if (k < 0 || P->op[k] < 0) return nullptr;
+        return std::is_same<T, double>::value ? (const T*)g->d_w64[P->op[k]] : (const T*)g->d_w32[P->op[k]];
+    };
+    p.idx = g->d_idx;
+    p.w0 = W(0);
+    p.w1 = W(1);
+    p.w2 = W(2);
+    p.cu = (const T*)P->cu;
+    p.cv = (const T*)P->cv;
+    T* u = (T*)P->u;
+    T* xa = (T*)P->xa;
+    T* xb = (T*)P->xb;
+    static const double cfac[4] = {0.5, 0.5, 1.0, 0.0};
+    double c = stage == 3 ? dt / 6. : cfac[stage] * dt;
+    p.c = (T)c;
+    p.kappa = (T)P->kappa;
+    p.x = stage == 0 ? u : (stage == 1 ? xa : (stage == 2 ? xb : xa));
+    p.xnext = stage == 0 ? xa : (stage == 1 ? xb : (stage == 2 ? xa : nullptr));
+    p.u = u;
+    p.acc = (T*)P->acc;
+    p.N = g->N;
+    p.Np = g->Np;
+    p.n_pad = g->n_pad;
+    p.T_tr = P->T;
+    p.stage = stage;
+    return p;
+}
+
+template <typename T, int KIND, bool HV>
+static void launch_stage_t(rbffd_pde* P, const StageParams<T>& p, Shape sh, cudaStream_t s)
+{
+    int B = sh.block > 0 ? sh.block : 256;
+    if (P->T == 1) {
+        int G = sh.lanes > 0 ? sh.lanes : 1;
+        long long threads = (long long)P->g->N * G;
+        int nb = (int)((threads + B - 1) / B);
+        switch (G) {
+        case 1: k_stage_scalar<T, KIND, HV, 1><<<nb, B, 0, s>>>(p); break;
+        case 2: k_stage_scalar<T, KIND, HV, 2><<<nb, B, 0, s>>>(p); break;
+        case 4: k_stage_scalar<T, KIND, HV, 4><<<nb, B, 0, s>>>(p); break;
+        default: k_stage_scalar<T, KIND, HV, 8><<<nb, B, 0, s>>>(p); break;
+        }
+        return;
+    }
+    const int V = std::is_same<T, float>::value ? 4 : 2;
+    if (P->T % V == 0) {
+        long long threads = (long long)P->g->N * (P->T / V);
+        k_stage_vec<T, std::is_same<T, float>::value ? 4 : 2, KIND, HV><<<(int)((threads + B - 1) / B), B, 0, s>>>(p);
+    } else {
+        long long threads = (long long)P->g->N * P->T;
+        k_stage_vec<T, 1, KIND, HV><<<(int)((threads + B - 1) / B), B, 0, s>>>(p);
+    }
+}
+
+template <typename T>
+static void launch_stage(rbffd_pde* P, int stage, double dt, Shape sh, cudaStream_t s)
+{
+    StageParams<T> p = make_params<T>(P, stage, dt);
+    if (P->kind == KIND_HEAT)
+        launch_stage_t<T, KIND_HEAT, false>(P, p, sh, s);
+    else if (P->use_hv)
+        launch_stage_t<T, KIND_ADVECT, true>(P, p, sh, s);
+    else
+        launch_stage_t<T, KIND_ADVECT, false>(P, p, sh, s);
+}
+
+static void launch_stage_any(rbffd_pde* P, int stage, double dt, Shape sh, cudaStream_t s)
+{
+    if (P->dtype == RBFFD_F64)
+        launch_stage<double>(P, stage, dt, sh, s);
+    else
+        launch_stage<float>(P, stage, dt, sh, s);
+}
+
+template <typename T>
+static int unfused_stage(rbffd_pde* P, int stage, double dt, cudaStream_t s)
+{
+    int nops = P->kind == KIND_HEAT ? 1 : (P->use_hv ? 3 : 2);
+    for (int k = 0; k < nops; k++) {
+        StageParams<T> p = make_params<T>(P, stage, dt);
+        int rc = grid_apply_dev(P->g, P->op[k], P->dtype, P->T, p.x, P->d[k], 0, P->g->N, 1, s);
+        if (rc) return rc;
+    }
+    StageParams<T> p = make_params<T>(P, stage, dt);
+    size_t n = (size_t)P->g->N * P->T;
+    int nb = (int)((n + 255) / 256);
+    const T *d0 = (const T*)P->d[0], *d1 = (const T*)P->d[1], *d2 = (const T*)P->d[2];
+    if (P->kind == KIND_HEAT)
+        k_rhs_axpy<T, KIND_HEAT, false><<<nb, 256, 0, s>>>(p, d0, d1, d2);
+    else if (P->use_hv)
+        k_rhs_axpy<T, KIND_ADVECT, true><<<nb, 256, 0, s>>>(p, d0, d1, d2);
+    else
+        k_rhs_axpy<T, KIND_ADVECT, false><<<nb, 256, 0, s>>>(p, d0, d1, d2);
+    return RBFFD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner: time stage 0 (which reads u and writes only the scratch buffers
+// xa and acc) for each candidate shape; keep the fastest per problem shape.
+
+static Shape autotune(rbffd_pde* P)
+{
+    rbffd_ctx* ctx = P->ctx;
+    TuneKey key{P->kind * 4 + (P->use_hv ? 2 : 0), P->dtype, P->T, P->g->N, P->g->n_pad};
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto it = ctx->tuned.find(key);
+        if (it != ctx->tuned.end()) return it->second;
+    }
+    std::vector<Shape> cands;
+    const int blocks[3] = {128, 256, 512};
+    if (P->T == 1) {
+        const int lanes[4] = {1, 2, 4, 8};
+        for (int G : lanes)
+            for (int B : blocks) cands.push_back(Shape{G, B});
+    } else {
+        for (int B : blocks) cands.push_back(Shape{0, B});
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    Shape best = cands[0];
+    float best_ms = 1e30f;
+    for (const Shape& c : cands) {
+        for (int w = 0; w < 2; w++) launch_stage_any(P, 0, 0.0, c, ctx->stream);
+        cudaEventRecord(e0, ctx->stream);
+        const int reps = 5;
+        for (int r = 0; r < reps; r++) launch_stage_any(P, 0, 0.0, c, ctx->stream);
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->tuned[key] = best;
+    return best;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+static void pde_free(rbffd_pde* P)
+{
+    if (!P) return;
+    rbffd_ctx* ctx = P->ctx;
+    size_t es = (P->dtype == RBFFD_F64 ? 8 : 4);
+    size_t n = (size_t)P->g->N * P->T * es;
+    if (P->gexec) cudaGraphExecDestroy(P->gexec);
+    dev_free(ctx, P->u, n);
+    dev_free(ctx, P->xa, n);
+    dev_free(ctx, P->xb, n);
+    dev_free(ctx, P->acc, n);
+    for (int k = 0; k < 3; k++) dev_free(ctx, P->d[k], n);
+    dev_free(ctx, P->stage64, (size_t)P->g->N * P->T * 8);
+    dev_free(ctx, P->cu, (size_t)P->g->N * es);
+    dev_free(ctx, P->cv, (size_t)P->g->N * es);
+    delete P;
+}
+
+extern "C" int rbffd_pde_create(rbffd_grid* g, const rbffd_pde_params* prm, rbffd_pde** out)
+{
+    if (!g || !prm || !out) return RBFFD_ERR_INVALID;
+    *out = nullptr;
+    rbffd_ctx* ctx = g->ctx;
+    if (prm->dtype != RBFFD_F32 && prm->dtype != RBFFD_F64)
+        return set_error(ctx, RBFFD_ERR_INVALID, "bad dtype %d", prm->dtype);
+    if (prm->ntracers < 1 || prm->ntracers > 1024)
+        return set_error(ctx, RBFFD_ERR_INVALID, "ntracers %d outside [1, 1024]", prm->ntracers);
+    int kind;
+    int ops[3] = {-1, -1, -1};
+    if (prm->rhs_kind == RBFFD_RHS_HEAT) {
+        kind = KIND_HEAT;
+        ops[0] = der_index(RBFFD_LSFC);
+    } else if (prm->rhs_kind == RBFFD_RHS_COSINE_BELL || prm->rhs_kind == RBFFD_RHS_ADVECTION) {
+        kind = KIND_ADVECT;
+        ops[0] = der_index(RBFFD_LAMBDA);
+        ops[1] = der_index(RBFFD_THETA);
+        if (prm->use_hv) ops[2] = der_index(RBFFD_HV);
+        if (prm->rhs_kind == RBFFD_RHS_ADVECTION && (!prm->cu || !prm->cv))
+            return set_error(ctx, RBFFD_ERR_INVALID, "advection needs per-node coefficients cu and cv");
+        if (prm->rhs_kind == RBFFD_RHS_COSINE_BELL && prm->sphere_radius == 0.0)
+            return set_error(ctx, RBFFD_ERR_INVALID, "cosine bell needs a nonzero sphere radius");
+    } else {
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "rhs_kind %d", prm->rhs_kind);
+    }
+    for (int k = 0; k < 3; k++)
+        if (ops[k] >= 0 && !g->d_w64[ops[k]])
+            return set_error(ctx, RBFFD_ERR_STATE, "weights of operator 0x%x are not on the device", 1u << ops[k]);
+    cudaSetDevice(ctx->device);
+    rbffd_pde* P = new (std::nothrow) rbffd_pde();
+    if (!P) return RBFFD_ERR_OOM;
+    P->g = g;
+    P->ctx = ctx;
+    P->kind = kind;
+    P->T = prm->ntracers;
+    P->dtype = prm->dtype;
+    P->use_hv = kind == KIND_ADVECT && prm->use_hv;
+    P->kappa = prm->kappa;
+    memcpy(P->op, ops, sizeof ops);
+    int N = g->N;
+    size_t es = (P->dtype == RBFFD_F64 ? 8 : 4);
+    size_t n = (size_t)N * P->T * es;
+    int rc;
+    if ((rc = dev_alloc(ctx, &P->u, n)) || (rc = dev_alloc(ctx, &P->xa, n)) || (rc = dev_alloc(ctx, &P->xb, n)) ||
+        (rc = dev_alloc(ctx, &P->acc, n))) {
+        pde_free(P);
+        return rc;
+    }
+    P->bytes = 4 * n;
+    if (P->dtype == RBFFD_F32) {
+        if ((rc = dev_alloc(ctx, (void**)&P->stage64, (size_t)N * P->T * 8))) {
+            pde_free(P);
+            return rc;
+        }
+        P->bytes += (size_t)N * P->T * 8;
+    }
+    cudaStream_t s = ctx->stream;
+    if (kind == KIND_ADVECT) {
+        // Per-node coefficients cu = vel_u / a and cv = vel_v / a, computed on the
+        // host in FP64 exactly as CosineBell::solve does every stage
+        // (cosine_bell.cpp:35-49); the velocity field is steady.
+        std::vector<double> cu(N), cv(N);
+        if (prm->rhs_kind == RBFFD_RHS_COSINE_BELL) {
+            std::vector<double> xyz((size_t)N * 4);
+            cudaError_t e = cudaMemcpyAsync(xyz.data(), g->d_xyz, (size_t)N * sizeof(double4), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) {
+                pde_free(P);
+                return cuda_error(ctx, e, "rbffd_pde_create");
+            }
+            double a = prm->sphere_radius, alpha = prm->alpha, u0 = prm->u0;
+            for (int i = 0; i < N; i++) {
+                double x = xyz[4 * (size_t)i], y = xyz[4 * (size_t)i + 1], z = xyz[4 * (size_t)i + 2];
+                double lambda = atan2(y, x);
+                double theta = atan2(z, sqrt(x * x + y * y));
+                double vel_u = u0 * (cos(theta) * cos(alpha) + sin(theta) * cos(lambda) * sin(alpha));
+                double vel_v = -u0 * (sin(lambda) * sin(alpha));
+                cu[i] = vel_u / a;
+                cv[i] = vel_v / a;
+            }
+        } else {
+            memcpy(cu.data(), prm->cu, N * sizeof(double));
+            memcpy(cv.data(), prm->cv, N * sizeof(double));
+        }
+        if ((rc = dev_alloc(ctx, &P->cu, N * es)) || (rc = dev_alloc(ctx, &P->cv, N * es))) {
+            pde_free(P);
+            return rc;
+        }
+        P->bytes += 2 * N * es;
+        std::vector<float> f32;
+        const void* src_u = cu.data();
+        const void* src_v = cv.data();
+        std::vector<float> fu, fv;
+        if (P->dtype == RBFFD_F32) {
+            fu.resize(N);
+            fv.resize(N);
+            for (int i = 0; i < N; i++) {
+                fu[i] = (float)cu[i];
+                fv[i] = (float)cv[i];
+            }
+            src_u = fu.data();
+            src_v = fv.data();
+        }
+        cudaError_t e = cudaMemcpyAsync(P->cu, src_u, N * es, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(P->cv, src_v, N * es, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            pde_free(P);
+            return cuda_error(ctx, e, "rbffd_pde_create");
+        }
+    }
+    // FP32 weight copies exist whenever FP64 weights do (grid_make_f32).
+    for (int k = 0; k < 3; k++)
+        if (ops[k] >= 0 && !g->d_w32[ops[k]] && (rc = grid_make_f32(g, ops[k]))) {
+            pde_free(P);
+            return rc;
+        }
+    RBFFD_CUDA_TRY(ctx, cudaMemsetAsync(P->u, 0, n, s));
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    *out = P;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_destroy(rbffd_pde* P)
+{
+    if (!P) return RBFFD_ERR_INVALID;
+    cudaSetDevice(P->ctx->device);
+    cudaStreamSynchronize(P->ctx->stream);
+    pde_free(P);
+    return RBFFD_OK;
+}
+
+__global__ void k_to_dtype_f(const double* __restrict__ a, float* __restrict__ b, size_t n)
+{
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = __double2float_rn(a[i]);
+}
+__global__ void k_from_f(const float* __restrict__ a, double* __restrict__ b, size_t n)
+{
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (double)a[i];
+}
+
+extern "C" int rbffd_pde_set_state(rbffd_pde* P, const double* u)
+{
+    if (!P || !u) return RBFFD_ERR_INVALID;
+    rbffd_ctx* ctx = P->ctx;
+    cudaSetDevice(ctx->device);
+    size_t n = (size_t)P->g->N * P->T;
+    cudaStream_t s = ctx->stream;
+    if (P->dtype == RBFFD_F64) {
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(P->u, u, n * 8, cudaMemcpyHostToDevice, s));
+    } else {
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(P->stage64, u, n * 8, cudaMemcpyHostToDevice, s));
+        k_to_dtype_f<<<(int)((n + 255) / 256), 256, 0, s>>>(P->stage64, (float*)P->u, n);
+        RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_get_state(rbffd_pde* P, double* u)
+{
+    if (!P || !u) return RBFFD_ERR_INVALID;
+    rbffd_ctx* ctx = P->ctx;
+    cudaSetDevice(ctx->device);
+    size_t n = (size_t)P->g->N * P->T;
+    cudaStream_t s = ctx->stream;
+    if (P->dtype == RBFFD_F64) {
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(u, P->u, n * 8, cudaMemcpyDeviceToHost, s));
+    } else {
+        k_from_f<<<(int)((n + 255) / 256), 256, 0, s>>>((const float*)P->u, P->stage64, n);
+        RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(u, P->stage64, n * 8, cudaMemcpyDeviceToHost, s));
+    }
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_set_time(rbffd_pde* P, double t)
+{
+    if (!P) return RBFFD_ERR_INVALID;
+    P->t = t;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_get_time(rbffd_pde* P, double* t)
+{
+    if (!P || !t) return RBFFD_ERR_INVALID;
+    *t = P->t;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_set_shape(rbffd_pde* P, int lanes, int block)
+{
+    if (!P) return RBFFD_ERR_INVALID;
+    if (lanes == 0 && block == 0) {
+        P->forced = false;
+        P->shape = Shape{};
+        return RBFFD_OK;
+    }
+    if (!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8)) return RBFFD_ERR_INVALID;
+    if (!(block == 0 || block == 64 || block == 128 || block == 256 || block == 512)) return RBFFD_ERR_INVALID;
+    if (P->T > 1 && lanes > 1) return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "lanes per row apply to one tracer only");
+    P->shape = Shape{lanes ? lanes : 1, block ? block : 256};
+    P->forced = true;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_get_shape(rbffd_pde* P, int* lanes, int* block)
+{
+    if (!P || !lanes || !block) return RBFFD_ERR_INVALID;
+    *lanes = P->shape.lanes;
+    *block = P->shape.block;
+    return RBFFD_OK;
+}
+
+static void run_steps(rbffd_pde* P, double dt, int nsteps, Shape sh)
+{
+    for (int k = 0; k < nsteps; k++)
+        for (int st = 0; st < 4; st++) launch_stage_any(P, st, dt, sh, P->ctx->stream);
+}
+
+extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps, int flags)
+{
+    if (!P) return RBFFD_ERR_INVALID;
+    rbffd_ctx* ctx = P->ctx;
+    if (scheme != 2) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "time scheme %d (only RK4 = 2)", scheme);
+    if (nsteps < 0) return set_error(ctx, RBFFD_ERR_INVALID, "nsteps < 0");
+    if (nsteps == 0) return RBFFD_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    if (flags & RBFFD_ADVANCE_UNFUSED) {
+        // plain path: per-operator SpMV launches, separate RHS/axpy, host sync per step
+        size_t n = (size_t)P->g->N * P->T * (P->dtype == RBFFD_F64 ? 8 : 4);
+        int nops = P->kind == KIND_HEAT ? 1 : (P->use_hv ? 3 : 2);
+        for (int k = 0; k < nops; k++)
+            if (!P->d[k]) {
+                int rc = dev_alloc(ctx, &P->d[k], n);
+                if (rc) return rc;
+                P->bytes += n;
+            }
+        for (int k = 0; k < nsteps; k++) {
+            for (int st = 0; st < 4; st++) {
+                int rc = P->dtype == RBFFD_F64 ? unfused_stage<double>(P, st, dt, s) : unfused_stage<float>(P, st, dt, s);
+                if (rc) return rc;
+            }
+            RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+            P->t += dt;
+        }
+        return RBFFD_OK;
+    }
+    if (!P->forced && P->shape.block == 0) P->shape = autotune(P);
+    Shape sh = P->shape;
+    if (flags & RBFFD_ADVANCE_GRAPH) {
+        const int chunk = 25;
+        int full = nsteps / chunk, rest = nsteps % chunk;
+        if (full > 0) {
+            if (!P->gexec || P->g_dt != dt || P->g_steps != chunk || P->g_shape.lanes != sh.lanes ||
+                P->g_shape.block != sh.block) {
+                if (P->gexec) {
+                    cudaGraphExecDestroy(P->gexec);
+                    P->gexec = nullptr;
+                }
+                cudaGraph_t graph;
+                RBFFD_CUDA_TRY(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                run_steps(P, dt, chunk, sh);
+                cudaError_t e = cudaStreamEndCapture(s, &graph);
+                if (e != cudaSuccess) return cuda_error(ctx, e, "graph capture");
+                e = cudaGraphInstantiate(&P->gexec, graph, 0);
+                cudaGraphDestroy(graph);
+                if (e != cudaSuccess) {
+                    P->gexec = nullptr;
+                    return cuda_error(ctx, e, "graph instantiate");
+                }
+                P->g_dt = dt;
+                P->g_steps = chunk;
+                P->g_shape = sh;
+            }
+            for (int r = 0; r < full; r++) RBFFD_CUDA_TRY(ctx, cudaGraphLaunch(P->gexec, s));
+        }
+        run_steps(P, dt, rest, sh);
+    } else {
+        run_steps(P, dt, nsteps, sh);
+    }
+    RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    P->t += dt * nsteps;
+    if (!(flags & RBFFD_ADVANCE_ASYNC)) RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    return RBFFD_OK;
+}

@@ -1,0 +1,863 @@
+// K1: batched FP64 RBF-FD weight computation.
+//
+// Per stencil (RBFFD::computeAllWeightsForStencil_Direct, src/rbffd/rbffd.cpp:225-352):
+//   assemble  A = [Phi P; P^T 0] (distanceMatrix rbffd.cpp:888-969, getStencilLHS :129-191)
+//   assemble  B = one column per selected operator (getStencilRHS :356-537)
+//   solve     A W = B  (arma::solve -> LAPACK dgesv, :259)
+//   store     weights[type][stencil][j] = W(j, col) * scale (HV: getHVScalar, :285-306)
+// all fused in one kernel: a "team" of TW threads owns one system at a time,
+// holds the augmented matrix [A | B] (m x (m+K), FP64) in shared memory and
+// runs Gaussian elimination with partial pivoting (first maximal |pivot|,
+// multipliers by division, fused updates) and a column-oriented back
+// substitution -- the arithmetic of dgetf2 + dgetrs, so given the same
+// assembled matrix the solution equals the CPU restatement bit for bit.
+// Teams loop over the systems of one size bucket (persistent, grid-stride);
+// buckets group stencils by system size m = n + np so shared memory is sized
+// per bucket, and a small autotuner picks the team width per bucket.
+//
+// Polynomial augmentation: poly_deg 0 is the reference build (constant
+// column, RHS row 0 for every operator, rbffd.cpp:1,150-155,506-508);
+// poly_deg 1 is {1,x,y,z} (rbffd.cpp:150-172) with the operator applied
+// exactly to each function (the reference does this for X/Y/Z/LAPL only and
+// zeroes the other rows with a warning, rbffd.cpp:510-531).  Beyond the
+// reference, poly_deg 2..4 use polynomials of total degree <= d in scaled
+// tangent-plane coordinates of the centre c,
+//   xi = (x - c).e_lambda / s,  eta = (x - c).e_theta / s,  s = max_j |x_j - c|,
+// (d+1)(d+2)/2 terms; 3-D monomials restricted to a small cap are nearly
+// dependent and would make the border block singular to working precision.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "internal.h"
+
+int grid_alloc_w64(rbffd_grid* g, int op);
+
+namespace {
+
+constexpr int MAX_K = 8;       // operators per solve
+constexpr int MAX_WARPS = 8;   // per team
+
+struct WParams {
+    const double4* xyz;
+    const int* idx;
+    const int* len;
+    const double* eps;
+    const int* deg;
+    const int* rows;
+    double* w[MAX_K];
+    int* status;  // min(row) + 1 over rows with a zero pivot, INT_MAX if none
+    double eps_uniform, hv_scale;
+    int Np, n_pad, deg_uniform, nrows, K, m, dim, hv_k, team_stride;  // team_stride: doubles per team
+    int opbit[MAX_K];
+};
+
+struct Team {
+    int tid, size, id;  // thread index in team, team width, team index in CTA
+    __device__ __forceinline__ void sync() const
+    {
+        if (size == 32)
+            __syncwarp();
+        else
+            asm volatile("bar.sync %0, %1;" ::"r"(id + 1), "r"(size) : "memory");
+    }
+    __device__ __forceinline__ int warp() const { return tid >> 5; }
+    __device__ __forceinline__ int lane() const { return tid & 31; }
+    __device__ __forceinline__ int nwarps() const { return size >> 5; }
+};
+
+__device__ __forceinline__ double ipow(double x, int a)
+{
+    double r = 1.0;
+    for (int i = 0; i < a; i++) r *= x;
+    return r;
+}
+
+// exponent of basis function q (ordering documented above)
+__device__ void basis_exp(int q, int& a, int& b, int& c)
+{
+    int t = 0;
+    while ((t + 1) * (t + 1) <= q) t++;  // first index of degree t is t^2
+    int r = q - t * t;
+    if (r <= t) {
+        a = t - r; b = r; c = 0;
+    } else {
+        r -= t + 1;
+        a = t - 1 - r; b = r; c = 1;
+    }
+}
+
+// d^(da,db,dc) of x^a y^b z^c at (x,y,z)
+__device__ double mono_d(int a, int b, int c, int da, int db, int dc, double x, double y, double z)
+{
+    if (da > a || db > b || dc > c) return 0.0;
+    double k = 1.0;
+    for (int i = 0; i < da; i++) k *= (a - i);
+    for (int i = 0; i < db; i++) k *= (b - i);
+    for (int i = 0; i < dc; i++) k *= (c - i);
+    return k * ipow(x, a - da) * ipow(y, b - db) * ipow(z, c - dc);
+}
+
+__device__ double lapl_dim(int a, int b, int c, int dim, double x, double y, double z)
+{
+    double s = mono_d(a, b, c, 2, 0, 0, x, y, z);
+    if (dim > 1) s += mono_d(a, b, c, 0, 2, 0, x, y, z);
+    if (dim > 2) s += mono_d(a, b, c, 0, 0, 2, x, y, z);
+    return s;
+}
+
+// Operator `bit` applied to basis function q at the centre c.
+__device__ double poly_row(unsigned bit, int q, const double* c, int dim, int hv_k, double lam, double th)
+{
+    int a, b, cc;
+    basis_exp(q, a, b, cc);
+    double x = c[0], y = c[1], z = c[2];
+    double gx = mono_d(a, b, cc, 1, 0, 0, x, y, z), gy = mono_d(a, b, cc, 0, 1, 0, x, y, z),
+           gz = mono_d(a, b, cc, 0, 0, 1, x, y, z);
+    double cg = x * gx + y * gy + z * gz;
+    switch (bit) {
+    case RBFFD_X: return gx;
+    case RBFFD_Y: return gy;
+    case RBFFD_Z: return gz;
+    case RBFFD_LAPL: return lapl_dim(a, b, cc, dim, x, y, z);
+    case RBFFD_INTERP: return mono_d(a, b, cc, 0, 0, 0, x, y, z);
+    case RBFFD_LAMBDA: return -sin(lam) * gx + cos(lam) * gy;
+    case RBFFD_THETA: return -sin(th) * cos(lam) * gx - sin(th) * sin(lam) * gy + cos(th) * gz;
+    case RBFFD_LSFC: {
+        double H[3][3];
+        const int e[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                H[i][j] = mono_d(a, b, cc, e[i][0] + e[j][0], e[i][1] + e[j][1], e[i][2] + e[j][2], x, y, z);
+        double tr = H[0][0] + H[1][1] + H[2][2], qf = 0.0;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) qf += c[i] * H[i][j] * c[j];
+        return tr - qf - 2.0 * cg;
+    }
+    case RBFFD_XSFC: return gx - x * cg;
+    case RBFFD_YSFC: return gy - y * cg;
+    case RBFFD_ZSFC: return gz - z * cg;
+    case RBFFD_HV: {
+        if (hv_k == 0) return mono_d(a, b, cc, 0, 0, 0, x, y, z);
+        if (hv_k == 1) return lapl_dim(a, b, cc, dim, x, y, z);
+        if (hv_k == 2) {
+            double s = 0.0;
+            for (int i = 0; i < dim && i < 3; i++)
+                for (int j = 0; j < dim && j < 3; j++) {
+                    int d[3] = {0, 0, 0};
+                    d[i] += 2;
+                    d[j] += 2;
+                    s += mono_d(a, b, cc, d[0], d[1], d[2], x, y, z);
+                }
+            return s;
+        }
+        return 0.0;  // degree <= 4 < 2k
+    }
+    default: return 0.0;  // R, ALT_*: no polynomial counterpart (rbffd.cpp:527-531)
+    }
+}
+
+__host__ __device__ inline int poly_size(int deg)
+{
+    return deg < 0 ? 0 : (deg == 0 ? 1 : (deg == 1 ? 4 : (deg + 1) * (deg + 2) / 2));
+}
+
+// exponents (a, b) of tangent basis function q: total degree t, a = t..0
+__device__ void tangent_exp(int q, int& a, int& b)
+{
+    int t = 0;
+    while ((t + 1) * (t + 2) / 2 <= q) t++;
+    int r = q - t * (t + 1) / 2;
+    a = t - r;
+    b = r;
+}
+
+__device__ double dfact(int a)
+{
+    double f = 1.0;
+    for (int i = 2; i <= a; i++) f *= i;
+    return f;
+}
+
+// Operator `bit` applied to xi^a eta^b at the centre (xi = eta = 0).
+__device__ double tangent_row(unsigned bit, int a, int b, const double* e1, const double* e2, double s, int dim, int hv_k)
+{
+    const int t = a + b;
+    switch (bit) {
+    case RBFFD_INTERP: return t == 0 ? 1.0 : 0.0;
+    case RBFFD_LAMBDA: return (a == 1 && b == 0) ? 1.0 / s : 0.0;
+    case RBFFD_THETA: return (a == 0 && b == 1) ? 1.0 / s : 0.0;
+    case RBFFD_X: case RBFFD_Y: case RBFFD_Z: case RBFFD_XSFC: case RBFFD_YSFC: case RBFFD_ZSFC: {
+        int ax = (bit == RBFFD_X || bit == RBFFD_XSFC) ? 0 : ((bit == RBFFD_Y || bit == RBFFD_YSFC) ? 1 : 2);
+        if (a == 1 && b == 0) return e1[ax] / s;
+        if (a == 0 && b == 1) return e2[ax] / s;
+        return 0.0;
+    }
+    case RBFFD_LSFC: return ((a == 2 && b == 0) || (a == 0 && b == 2)) ? 2.0 / (s * s) : 0.0;
+    case RBFFD_LAPL: {
+        double q = 0.0;
+        for (int ax = 0; ax < dim && ax < 3; ax++) {
+            if (a == 2 && b == 0) q += 2.0 * e1[ax] * e1[ax];
+            if (a == 1 && b == 1) q += 2.0 * e1[ax] * e2[ax];
+            if (a == 0 && b == 2) q += 2.0 * e2[ax] * e2[ax];
+        }
+        return q / (s * s);
+    }
+    case RBFFD_HV: {
+        if (t != 2 * hv_k || (a & 1) || (b & 1)) return 0.0;
+        double binom = dfact(hv_k) / (dfact(a / 2) * dfact(hv_k - a / 2));
+        return binom * dfact(a) * dfact(b) / pow(s, 2 * hv_k);
+    }
+    default: return 0.0;
+    }
+}
+
+// Gaussian RBF pieces (src/rbffd/rbfs/rbf_gaussian.h)
+__device__ __forceinline__ double g_eval(double eps2, double r2) { return exp(-(r2 * eps2)); }
+
+__device__ double hv_p_k(double eps2r2, int dim, int k)
+{
+    // iterative form of RBF_Gaussian::hv_p_k (rbf_gaussian.h:229-249), same arithmetic per level
+    if (k == 0) return 1.0;
+    double pm2 = 1.0, pm1 = 4. * eps2r2 - 2. * dim;
+    for (int j = 2; j <= k; j++) {
+        double p = 4. * (eps2r2 - 2. * (j - 1) - dim / 2.) * pm1 - 8. * (j - 1) * (2. * (j - 1) - 2. + dim) * pm2;
+        pm2 = pm1;
+        pm1 = p;
+    }
+    return pm1;
+}
+
+// RHS entry for node j (rbffd.cpp:375-503); diff = x0 - xj.
+__device__ double rhs_rbf(unsigned bit, const double* x0, const double* xj, double eps, double eps2, int dim, int hv_k,
+                          double lam_i, double th_i, double lam_j, double th_j)
+{
+    double dx = x0[0] - xj[0], dy = x0[1] - xj[1], dz = x0[2] - xj[2];
+    double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    double phi = g_eval(eps2, r2);
+    double rdr = -2. * eps2 * phi;  // rderiv_over_r
+    switch (bit) {
+    case RBFFD_X: return -2. * (dx * eps2) * phi;
+    case RBFFD_Y: return -2. * (dy * eps2) * phi;
+    case RBFFD_Z: return -2. * (dz * eps2) * phi;
+    case RBFFD_LAPL:
+        if (dim == 1) return 2. * eps2 * (-1. + 2. * (dx * dx * eps2)) * phi;
+        if (dim == 2) return 4. * eps2 * (-1. + dx * dx * eps2 + dy * dy * eps2) * phi;
+        return (-6. * eps2 + 4. * (r2 * (eps2 * eps2))) * phi;
+    case RBFFD_INTERP: return phi;
+    case RBFFD_R: return -2. * (sqrt(r2) * eps2) * phi;
+    case RBFFD_LAMBDA: {
+        double d = cos(th_j) * sin(lam_i - lam_j);
+        return fabs(d) > 0. ? d * rdr : 0.;
+    }
+    case RBFFD_THETA: {
+        double d = cos(th_j) * sin(th_i) * cos(lam_i - lam_j) - sin(th_j) * cos(th_i);
+        return fabs(d) > 0. ? d * rdr : 0.;
+    }
+    case RBFFD_LSFC: {
+        double rd2 = rdr + 4. * (eps2 * eps2) * r2 * phi;  // rderiv2
+        return (1. / 4.) * ((4. - r2) * rd2 + (4. - 3. * r2) * rdr);
+    }
+    case RBFFD_XSFC:
+    case RBFFD_YSFC:
+    case RBFFD_ZSFC: {
+        double xTx = x0[0] * xj[0] + x0[1] * xj[1] + x0[2] * xj[2];
+        int ax = bit == RBFFD_XSFC ? 0 : (bit == RBFFD_YSFC ? 1 : 2);
+        return (x0[ax] * xTx - xj[ax]) * rdr;
+    }
+    case RBFFD_HV: return pow(eps, 2 * hv_k) * hv_p_k(eps2 * r2, dim, hv_k) * phi;
+    default: return 0.;  // ALT_*: rbffd.cpp:490-494
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Team elimination on the augmented row-major matrix a (m x ld, ld = m + K).
+// cand_v / cand_r: one pivot candidate per warp.  Returns false on a zero pivot.
+
+__device__ void team_pivot_column0(const Team& T, const double* a, int m, int ld, double* cand_v, int* cand_r)
+{
+    // candidates for step 0: rows handled warp-strided, first maximum kept
+    double bv = -1.0;
+    int br = INT_MAX;
+    for (int i = T.tid; i < m; i += T.size) {
+        double v = fabs(a[i * ld]);
+        if (v > bv) { bv = v; br = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        int orr = __shfl_xor_sync(0xffffffffu, br, o);
+        if (ov > bv || (ov == bv && orr < br)) { bv = ov; br = orr; }
+    }
+    if (T.lane() == 0) {
+        cand_v[T.warp()] = bv;
+        cand_r[T.warp()] = br;
+    }
+}
+
+// Returns 0, or k + 1 when the pivot column at step k is exactly zero (dgetrf's INFO).
+__device__ int team_eliminate(const Team& T, double* a, int m, int K, double* cand_v, int* cand_r)
+{
+    const int ld = m + K;
+    const int nw = T.nwarps(), w = T.warp(), lane = T.lane();
+    team_pivot_column0(T, a, m, ld, cand_v, cand_r);
+    T.sync();
+    for (int k = 0; k < m; k++) {
+        // reduce the per-warp candidates (every thread, identical result)
+        double bv = cand_v[0];
+        int p = cand_r[0];
+        for (int q = 1; q < nw; q++) {
+            double v = cand_v[q];
+            int r = cand_r[q];
+            if (v > bv || (v == bv && r < p)) { bv = v; p = r; }
+        }
+        if (!(bv > 0.0)) return k + 1;  // exactly zero (or NaN) pivot column
+        if (p != k)
+            for (int j = k + T.tid; j < ld; j += T.size) {
+                double t = a[k * ld + j];
+                a[k * ld + j] = a[p * ld + j];
+                a[p * ld + j] = t;
+            }
+        T.sync();
+        const double piv = a[k * ld + k];
+        // rows split across warps, columns across lanes; lane 0 of the j-loop
+        // holds column k+1 and tracks the next pivot candidate
+        double nbv = -1.0;
+        int nbr = INT_MAX;
+        for (int i = k + 1 + w; i < m; i += nw) {
+            double l = 0.0;
+            if (lane == 0) l = a[i * ld + k] / piv;
+            l = __shfl_sync(0xffffffffu, l, 0);
+            for (int j = k + 1 + lane; j < ld; j += 32) {
+                double v = __fma_rn(-l, a[k * ld + j], a[i * ld + j]);
+                a[i * ld + j] = v;
+                if (j == k + 1) {
+                    double av = fabs(v);
+                    if (av > nbv) { nbv = av; nbr = i; }
+                }
+            }
+        }
+        if (lane == 0) {
+            cand_v[w] = nbv;
+            cand_r[w] = nbr;
+        }
+        T.sync();
+    }
+    return 0;
+}
+
+// Column-oriented back substitution (dtrsm upper, non-unit), one warp per RHS column.
+__device__ void team_back_substitute(const Team& T, double* a, int m, int K)
+{
+    const int ld = m + K;
+    for (int c = T.warp(); c < K; c += T.nwarps()) {
+        const int col = m + c;
+        for (int k = m - 1; k >= 0; k--) {
+            double xk = 0.0;
+            if (T.lane() == 0) {
+                xk = a[k * ld + col] / a[k * ld + k];
+                a[k * ld + col] = xk;
+            }
+            xk = __shfl_sync(0xffffffffu, xk, 0);
+            for (int i = T.lane(); i < k; i += 32) a[i * ld + col] = __fma_rn(-xk, a[i * ld + k], a[i * ld + col]);
+            __syncwarp();
+        }
+    }
+    T.sync();
+}
+
+// ---------------------------------------------------------------------------
+
+// Team assembly of the augmented system [A | B] of stencil r into a (m x (m+K)).
+// xs: scratch for the stencil's coordinates; fr: 7 doubles of scratch (tangent frame).
+// Returns m.  Ends with a team barrier.
+__device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, double* xs, double* fr, int& n_out)
+{
+    const int n = P.len[r];
+    const int deg = P.deg ? P.deg[r] : P.deg_uniform;
+    const int np = poly_size(deg);
+    const int m = n + np, K = P.K, ld = m + K;
+    const double eps = P.eps ? P.eps[r] : P.eps_uniform;  // var_epsilon[stencil[0]]
+    const double eps2 = eps * eps;
+    for (int q = T.tid; q < n; q += T.size) {
+        double4 v = P.xyz[P.idx[(size_t)q * P.Np + r]];
+        xs[3 * q] = v.x;
+        xs[3 * q + 1] = v.y;
+        xs[3 * q + 2] = v.z;
+    }
+    T.sync();
+    const double x0[3] = {xs[0], xs[1], xs[2]};
+    const double lam_i = atan2(x0[1], x0[0]), th_i = atan2(x0[2], sqrt(x0[0] * x0[0] + x0[1] * x0[1]));
+    if (deg >= 2 && T.tid == 0) {
+        fr[0] = -sin(lam_i); fr[1] = cos(lam_i); fr[2] = 0.0;
+        fr[3] = -sin(th_i) * cos(lam_i); fr[4] = -sin(th_i) * sin(lam_i); fr[5] = cos(th_i);
+        double s2 = 0.0;
+        for (int j = 0; j < n; j++) {
+            double dx = xs[3 * j] - x0[0], dy = xs[3 * j + 1] - x0[1], dz = xs[3 * j + 2] - x0[2];
+            double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            s2 = fmax(s2, r2);
+        }
+        fr[6] = s2 > 0.0 ? sqrt(s2) : 1.0;
+    }
+    // Phi block: ar(j, i) = phi(x_i - x_j)   (rbffd.cpp:943-966)
+    for (int e = T.tid; e < n * n; e += T.size) {
+        int j = e / n, i = e - j * n;
+        double dx = xs[3 * i] - xs[3 * j], dy = xs[3 * i + 1] - xs[3 * j + 1], dz = xs[3 * i + 2] - xs[3 * j + 2];
+        double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        a[j * ld + i] = g_eval(eps2, r2);
+    }
+    T.sync();  // frame visible
+    const double* e1 = fr;
+    const double* e2 = fr + 3;
+    const double s = fr[6];
+    // polynomial border and zero block
+    for (int e = T.tid; e < np * n; e += T.size) {
+        int q = e / n, i = e - q * n;
+        double v;
+        if (deg >= 2) {
+            int pa, pb;
+            tangent_exp(q, pa, pb);
+            double dx = xs[3 * i] - x0[0], dy = xs[3 * i + 1] - x0[1], dz = xs[3 * i + 2] - x0[2];
+            double u = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, e1[0]), __dmul_rn(dy, e1[1])), __dmul_rn(dz, e1[2])), s);
+            double w = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, e2[0]), __dmul_rn(dy, e2[1])), __dmul_rn(dz, e2[2])), s);
+            v = ipow(u, pa) * ipow(w, pb);
+        } else {
+            int pa, pb, pc;
+            basis_exp(q, pa, pb, pc);
+            v = ipow(xs[3 * i], pa) * ipow(xs[3 * i + 1], pb) * ipow(xs[3 * i + 2], pc);
+        }
+        a[(n + q) * ld + i] = v;
+        a[i * ld + (n + q)] = v;
+    }
+    for (int e = T.tid; e < np * np; e += T.size) a[(n + e / np) * ld + n + e % np] = 0.0;
+    // right-hand sides, one column per operator in bit order (rbffd.cpp:106-125)
+    for (int j = T.tid; j < m; j += T.size) {
+        if (j < n) {
+            const double* xj = xs + 3 * j;
+            double lam_j = atan2(xj[1], xj[0]), th_j = atan2(xj[2], sqrt(xj[0] * xj[0] + xj[1] * xj[1]));
+            for (int c = 0; c < K; c++)
+                a[j * ld + m + c] = rhs_rbf(P.opbit[c], x0, xj, eps, eps2, P.dim, P.hv_k, lam_i, th_i, lam_j, th_j);
+        } else {
+            for (int c = 0; c < K; c++) {
+                double v = 0.0;
+                if (deg == 1) v = poly_row(P.opbit[c], j - n, x0, P.dim, P.hv_k, lam_i, th_i);
+                if (deg >= 2) {
+                    int pa, pb;
+                    tangent_exp(j - n, pa, pb);
+                    v = tangent_row(P.opbit[c], pa, pb, e1, e2, s, P.dim, P.hv_k);
+                }
+                a[j * ld + m + c] = v;
+            }
+        }
+    }
+    T.sync();
+    n_out = n;
+    return m;
+}
+
+// Per-team shared memory: [a: m x (m+K)] [xs: 3 n_pad] [frame: 8] [cand_v: MAX_WARPS] [cand_r: MAX_WARPS ints]
+__global__ void __launch_bounds__(512) k_weights(WParams P, int team_size)
+{
+    extern __shared__ double smem[];
+    Team T;
+    T.size = team_size;
+    T.id = threadIdx.x / team_size;
+    T.tid = threadIdx.x % team_size;
+    const int teams_per_cta = blockDim.x / team_size;
+    double* a = smem + (size_t)T.id * P.team_stride;
+    double* xs = a + (size_t)P.m * (P.m + P.K);
+    double* fr = xs + 3 * P.n_pad;
+    double* cand_v = fr + 8;
+    int* cand_r = (int*)(cand_v + MAX_WARPS);
+    const int K = P.K;
+    for (int t = blockIdx.x * teams_per_cta + T.id; t < P.nrows; t += gridDim.x * teams_per_cta) {
+        const int r = P.rows[t];
+        int n;
+        const int m = team_assemble(T, P, r, a, xs, fr, n);
+        const int ld = m + K;
+        const bool ok = team_eliminate(T, a, m, K, cand_v, cand_r) == 0;
+        if (ok) team_back_substitute(T, a, m, K);
+        if (!ok && T.tid == 0) atomicMin(P.status, r + 1);
+        // store: weights[type][r][j] = W(j, col) * scale, slot-major (rbffd.cpp:300-306)
+        for (int e = T.tid; e < K * P.n_pad; e += T.size) {
+            int c = e / P.n_pad, j = e - c * P.n_pad;
+            double scale = P.opbit[c] == RBFFD_HV ? P.hv_scale : 1.0;
+            double v = (j < n) ? (ok ? a[j * ld + m + c] * scale : __longlong_as_double(0x7ff8000000000000ll)) : 0.0;
+            P.w[c][(size_t)j * P.Np + r] = v;
+        }
+        T.sync();
+    }
+}
+
+// Assembled systems only (inspection): out[t] = [A | B] of row rows[t], m x (m+K) row-major.
+__global__ void __launch_bounds__(512) k_assemble(WParams P, int team_size, double* out)
+{
+    extern __shared__ double smem[];
+    Team T;
+    T.size = team_size;
+    T.id = threadIdx.x / team_size;
+    T.tid = threadIdx.x % team_size;
+    const int teams_per_cta = blockDim.x / team_size;
+    double* a = smem + (size_t)T.id * P.team_stride;
+    double* xs = a + (size_t)P.m * (P.m + P.K);
+    double* fr = xs + 3 * P.n_pad;
+    const size_t sz = (size_t)P.m * (P.m + P.K);
+    for (int t = blockIdx.x * teams_per_cta + T.id; t < P.nrows; t += gridDim.x * teams_per_cta) {
+        int n;
+        team_assemble(T, P, P.rows[t], a, xs, fr, n);
+        for (size_t e = T.tid; e < sz; e += T.size) out[(size_t)t * sz + e] = a[e];
+        T.sync();
+    }
+}
+
+// Plain batched solve: A [batch][m][m], B [batch][m][nrhs] row-major, X -> B.
+__global__ void __launch_bounds__(512) k_gesv(double* A, double* B, int* info, int m, int K, int batch, int team_size,
+                                              int team_stride)
+{
+    extern __shared__ double smem[];
+    Team T;
+    T.size = team_size;
+    T.id = threadIdx.x / team_size;
+    T.tid = threadIdx.x % team_size;
+    const int teams_per_cta = blockDim.x / team_size;
+    const int ld = m + K;
+    double* a = smem + (size_t)T.id * team_stride;
+    double* cand_v = a + (size_t)m * ld;
+    int* cand_r = (int*)(cand_v + MAX_WARPS);
+    for (int b = blockIdx.x * teams_per_cta + T.id; b < batch; b += gridDim.x * teams_per_cta) {
+        const double* Ab = A + (size_t)b * m * m;
+        double* Bb = B + (size_t)b * m * K;
+        for (int e = T.tid; e < m * m; e += T.size) a[(e / m) * ld + e % m] = Ab[e];
+        for (int e = T.tid; e < m * K; e += T.size) a[(e / K) * ld + m + e % K] = Bb[e];
+        T.sync();
+        const int st = team_eliminate(T, a, m, K, cand_v, cand_r);
+        if (st == 0) team_back_substitute(T, a, m, K);
+        if (T.tid == 0) info[b] = st;
+        for (int e = T.tid; e < m * K; e += T.size) Bb[e] = a[(e / K) * ld + m + e % K];
+        T.sync();
+    }
+}
+
+size_t team_bytes_w(int m, int K, int n_pad)
+{
+    return ((size_t)m * (m + K) + 3 * (size_t)n_pad + 8 + 2 * MAX_WARPS) * sizeof(double);
+}
+
+int max_smem_optin(rbffd_ctx* ctx)
+{
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+    return v;
+}
+
+struct WShape {
+    int team, block;
+};
+
+}  // namespace
+
+// Candidate team shapes for a bucket: (team width, CTA threads) such that the
+// teams fit the shared memory of one CTA.
+static std::vector<WShape> w_candidates(int m, size_t team_bytes, int smem_max)
+{
+    std::vector<WShape> out;
+    const int teams[4] = {32, 64, 128, 256};
+    const int blocks[3] = {128, 256, 512};
+    for (int tw : teams)
+        for (int b : blocks) {
+            if (b < tw || b / tw > 15) continue;
+            if (tw > 32 * MAX_WARPS) continue;
+            if ((size_t)(b / tw) * team_bytes > (size_t)smem_max) continue;
+            if (m <= 40 && tw > 64) continue;  // small systems: narrow teams only
+            out.push_back(WShape{tw, b});
+        }
+    return out;
+}
+
+static int launch_weights(rbffd_ctx* ctx, const WParams& P, WShape sh, size_t team_bytes, int nrows_cap)
+{
+    WParams Q = P;
+    if (nrows_cap > 0) Q.nrows = std::min(Q.nrows, nrows_cap);
+    int teams_per_cta = sh.block / sh.team;
+    size_t smem = (size_t)teams_per_cta * team_bytes;
+    RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(k_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_weights, sh.block, smem));
+    if (per_sm < 1) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "weight kernel shape does not fit an SM");
+    int need = (Q.nrows + teams_per_cta - 1) / teams_per_cta;
+    int grid = std::max(1, std::min(need, per_sm * ctx->sm_count));
+    k_weights<<<grid, sh.block, smem, ctx->stream>>>(Q, sh.team);
+    RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* prm, const double* eps, double eps_uniform,
+                                     const int* deg_per_row)
+{
+    if (!g || !prm) return RBFFD_ERR_INVALID;
+    rbffd_ctx* ctx = g->ctx;
+    unsigned types = prm->der_types & 0xFFFFu;
+    if (!types) return set_error(ctx, RBFFD_ERR_INVALID, "no operator selected");
+    if (types & 0x7000u) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "ALT_*SFC operators are not implemented");
+    if (prm->poly_deg < -1 || prm->poly_deg > 4) return set_error(ctx, RBFFD_ERR_INVALID, "poly_deg %d outside [-1, 4]", prm->poly_deg);
+    if (prm->dim < 1 || prm->dim > 3) return set_error(ctx, RBFFD_ERR_INVALID, "dim %d outside [1, 3]", prm->dim);
+    if (prm->hv_k < 0 || prm->hv_k > 16) return set_error(ctx, RBFFD_ERR_INVALID, "hv_k %d outside [0, 16]", prm->hv_k);
+    if (!eps && !(eps_uniform > 0.0) && eps_uniform != 0.0) return set_error(ctx, RBFFD_ERR_INVALID, "bad epsilon");
+    WParams P;
+    memset(&P, 0, sizeof P);
+    int K = 0;
+    for (int b = 0; b < 16; b++)
+        if (types & (1u << b)) {
+            if (K == MAX_K) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "more than %d operators in one solve", MAX_K);
+            P.opbit[K++] = 1u << b;
+        }
+    P.K = K;
+    int N = g->N;
+    std::vector<int> deg(N, prm->poly_deg);
+    if (deg_per_row)
+        for (int i = 0; i < N; i++) {
+            if (deg_per_row[i] < -1 || deg_per_row[i] > 4)
+                return set_error(ctx, RBFFD_ERR_INVALID, "deg_per_row[%d] = %d outside [-1, 4]", i, deg_per_row[i]);
+            deg[i] = deg_per_row[i];
+        }
+    // buckets by system size m
+    std::map<int, std::vector<int>> buckets;
+    for (int i = 0; i < N; i++) {
+        int np = poly_size(deg[i]);
+        buckets[g->h_len[i] + np].push_back(i);
+    }
+    int smem_max = max_smem_optin(ctx);
+    for (auto& kv : buckets)
+        if (team_bytes_w(kv.first, K, g->n_pad) > (size_t)smem_max)
+            return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "system size %d with %d operators exceeds shared memory", kv.first, K);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    int rc;
+    for (int c = 0; c < K; c++) {
+        int op = der_index(P.opbit[c]);
+        if ((rc = grid_alloc_w64(g, op))) return rc;
+        P.w[c] = g->d_w64[op];
+    }
+    // device inputs
+    int *d_rows = nullptr, *d_deg = nullptr, *d_status = nullptr;
+    double* d_eps = nullptr;
+    size_t b_rows = (size_t)N * sizeof(int);
+    auto cleanup = [&]() {
+        dev_free(ctx, d_rows, b_rows);
+        dev_free(ctx, d_deg, b_rows);
+        dev_free(ctx, d_status, sizeof(int));
+        dev_free(ctx, d_eps, (size_t)N * sizeof(double));
+    };
+    if ((rc = dev_alloc(ctx, (void**)&d_rows, b_rows)) || (rc = dev_alloc(ctx, (void**)&d_deg, b_rows)) ||
+        (rc = dev_alloc(ctx, (void**)&d_status, sizeof(int))) ||
+        (eps && (rc = dev_alloc(ctx, (void**)&d_eps, (size_t)N * sizeof(double))))) {
+        cleanup();
+        return rc;
+    }
+    std::vector<int> rows;
+    rows.reserve(N);
+    for (auto& kv : buckets) rows.insert(rows.end(), kv.second.begin(), kv.second.end());
+    int status0 = INT_MAX;
+    cudaError_t e = cudaMemcpyAsync(d_rows, rows.data(), b_rows, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_deg, deg.data(), b_rows, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_status, &status0, sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && eps) e = cudaMemcpyAsync(d_eps, eps, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        cleanup();
+        return cuda_error(ctx, e, "rbffd_weights_compute upload");
+    }
+    P.xyz = g->d_xyz;
+    P.idx = g->d_idx;
+    P.len = g->d_len;
+    P.eps = d_eps;
+    P.eps_uniform = eps_uniform;
+    P.deg = d_deg;
+    P.deg_uniform = prm->poly_deg;
+    P.status = d_status;
+    P.Np = g->Np;
+    P.n_pad = g->n_pad;
+    P.dim = prm->dim;
+    P.hv_k = prm->hv_k;
+    double hvN = prm->hv_nodes > 0 ? prm->hv_nodes : (double)N;
+    P.hv_scale = -prm->hv_gamma * pow(hvN, -(double)prm->hv_k);
+    size_t off = 0;
+    for (auto& kv : buckets) {
+        int m = kv.first;
+        int cnt = (int)kv.second.size();
+        WParams Q = P;
+        Q.rows = d_rows + off;
+        Q.nrows = cnt;
+        Q.m = m;
+        size_t tb = team_bytes_w(m, K, g->n_pad);
+        tb = (tb + 127) / 128 * 128;  // keep teams 128-byte aligned
+        Q.team_stride = (int)(tb / sizeof(double));
+        TuneKey key{100 + K, m, g->n_pad, 0, 0};
+        WShape best{0, 0};
+        {
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            auto it = ctx->tuned.find(key);
+            if (it != ctx->tuned.end()) best = WShape{it->second.lanes, it->second.block};
+        }
+        if (best.team == 0) {
+            std::vector<WShape> cands = w_candidates(m, tb, smem_max);
+            if (cands.empty()) {
+                cleanup();
+                return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "no kernel shape fits system size %d", m);
+            }
+            best = cands[0];
+            if (cands.size() > 1 && cnt >= 2048) {
+                // time each shape on a prefix of the bucket (outputs are rewritten by the full launch)
+                cudaEvent_t e0, e1;
+                cudaEventCreate(&e0);
+                cudaEventCreate(&e1);
+                float best_ms = 1e30f;
+                int cap = std::min(cnt, 8 * ctx->sm_count * 8);
+                for (const WShape& c : cands) {
+                    cudaEventRecord(e0, s);
+                    if (launch_weights(ctx, Q, c, tb, cap) != RBFFD_OK) continue;
+                    cudaEventRecord(e1, s);
+                    if (cudaEventSynchronize(e1) != cudaSuccess) {
+                        cudaGetLastError();
+                        continue;
+                    }
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = c;
+                    }
+                }
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+            }
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            ctx->tuned[key] = Shape{best.team, best.block};
+        }
+        if ((rc = launch_weights(ctx, Q, best, tb, 0))) {
+            cleanup();
+            return rc;
+        }
+        off += cnt;
+    }
+    int status = INT_MAX;
+    e = cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cleanup();
+    if (e != cudaSuccess) return cuda_error(ctx, e, "rbffd_weights_compute");
+    if (status != INT_MAX)
+        return set_error(ctx, RBFFD_ERR_SINGULAR, "stencil %d: zero pivot in the weight system", status - 1);
+    for (int c = 0; c < K; c++)
+        if ((rc = grid_make_f32(g, der_index(P.opbit[c])))) return rc;
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_batched_gesv_dev(rbffd_ctx* ctx, int m, int nrhs, int batch, void* A, void* B, void* info)
+{
+    if (!ctx || !A || !B || !info || m < 1 || m > 160 || nrhs < 1 || nrhs > 16 || batch < 0) return RBFFD_ERR_INVALID;
+    if (batch == 0) return RBFFD_OK;
+    cudaSetDevice(ctx->device);
+    size_t tb = ((size_t)m * (m + nrhs) + 2 * MAX_WARPS) * sizeof(double);
+    tb = (tb + 127) / 128 * 128;
+    int smem_max = max_smem_optin(ctx);
+    if (tb > (size_t)smem_max) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "system %d x %d exceeds shared memory", m, m);
+    int team = m <= 48 ? 32 : (m <= 96 ? 64 : 128);
+    int teams = std::max(1, std::min(8, (int)(smem_max / tb)));
+    while (teams > 1 && team * teams > 512) teams--;
+    int block = team * teams;
+    size_t smem = tb * teams;
+    RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(k_gesv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gesv, block, smem));
+    int grid = std::max(1, std::min((batch + teams - 1) / teams, std::max(1, per_sm) * ctx->sm_count));
+    k_gesv<<<grid, block, smem, ctx->stream>>>((double*)A, (double*)B, (int*)info, m, nrhs, batch, team,
+                                                (int)(tb / sizeof(double)));
+    RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_weights_assemble(rbffd_grid* g, const rbffd_weight_params* prm, const double* eps,
+                                      double eps_uniform, const int* deg_per_row, const int* rows, int count,
+                                      double* out)
+{
+    if (!g || !prm || !rows || !out || count < 0) return RBFFD_ERR_INVALID;
+    rbffd_ctx* ctx = g->ctx;
+    if (count == 0) return RBFFD_OK;
+    unsigned types = prm->der_types & 0xFFFFu;
+    if (!types || (types & 0x7000u)) return set_error(ctx, RBFFD_ERR_INVALID, "bad operator set 0x%x", types);
+    if (prm->poly_deg < -1 || prm->poly_deg > 4 || prm->dim < 1 || prm->dim > 3)
+        return set_error(ctx, RBFFD_ERR_INVALID, "bad poly_deg or dim");
+    WParams P;
+    memset(&P, 0, sizeof P);
+    int K = 0;
+    for (int b = 0; b < 16; b++)
+        if (types & (1u << b)) {
+            if (K == MAX_K) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "more than %d operators", MAX_K);
+            P.opbit[K++] = 1u << b;
+        }
+    int N = g->N, m = -1;
+    std::vector<int> deg(N, prm->poly_deg);
+    if (deg_per_row)
+        for (int i = 0; i < N; i++) deg[i] = deg_per_row[i];
+    for (int t = 0; t < count; t++) {
+        if (rows[t] < 0 || rows[t] >= N) return set_error(ctx, RBFFD_ERR_INVALID, "row %d out of range", rows[t]);
+        int mt = g->h_len[rows[t]] + poly_size(deg[rows[t]]);
+        if (m >= 0 && mt != m) return set_error(ctx, RBFFD_ERR_INVALID, "rows of one call must share the system size");
+        m = mt;
+    }
+    size_t tb = (team_bytes_w(m, K, g->n_pad) + 127) / 128 * 128;
+    if (tb > (size_t)max_smem_optin(ctx)) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "system too large");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    int *d_rows = nullptr, *d_deg = nullptr;
+    double *d_eps = nullptr, *d_out = nullptr;
+    size_t osz = (size_t)count * m * (m + K) * sizeof(double);
+    int rc;
+    auto cleanup = [&]() {
+        dev_free(ctx, d_rows, count * sizeof(int));
+        dev_free(ctx, d_deg, (size_t)N * sizeof(int));
+        dev_free(ctx, d_eps, (size_t)N * sizeof(double));
+        dev_free(ctx, d_out, osz);
+    };
+    if ((rc = dev_alloc(ctx, (void**)&d_rows, count * sizeof(int))) ||
+        (rc = dev_alloc(ctx, (void**)&d_deg, (size_t)N * sizeof(int))) ||
+        (eps && (rc = dev_alloc(ctx, (void**)&d_eps, (size_t)N * sizeof(double)))) ||
+        (rc = dev_alloc(ctx, (void**)&d_out, osz))) {
+        cleanup();
+        return rc;
+    }
+    cudaError_t e = cudaMemcpyAsync(d_rows, rows, count * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_deg, deg.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && eps) e = cudaMemcpyAsync(d_eps, eps, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
+    P.xyz = g->d_xyz;
+    P.idx = g->d_idx;
+    P.len = g->d_len;
+    P.eps = d_eps;
+    P.eps_uniform = eps_uniform;
+    P.deg = d_deg;
+    P.deg_uniform = prm->poly_deg;
+    P.rows = d_rows;
+    P.nrows = count;
+    P.K = K;
+    P.m = m;
+    P.Np = g->Np;
+    P.n_pad = g->n_pad;
+    P.dim = prm->dim;
+    P.hv_k = prm->hv_k;
+    P.team_stride = (int)(tb / sizeof(double));
+    if (e == cudaSuccess) {
+        const int team = 64;
+        RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb));
+        k_assemble<<<std::min(count, 4 * ctx->sm_count), team, tb, s>>>(P, team, d_out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, osz, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cleanup();
+    if (e != cudaSuccess) return cuda_error(ctx, e, "rbffd_weights_assemble");
+    return RBFFD_OK;
+}

@@ -1,0 +1,149 @@
+"""K3 parity: the fused RK4 stages against the oracle's restatement of
+TimeDependentPDE::advanceRungeKutta4 (time_dependent_pde.cpp:172-304) with
+CosineBell::solve (cosine_bell.cpp:23-70) and the heat right-hand side.
+
+Weights are shared (the oracle's, installed with rbffd_weights_set) so the
+comparison isolates the time stepping:
+* FP64, one lane per stencil row: bit-exact after every tested step count
+  (same accumulation order, same fused multiply-adds);
+* FP64 with the autotuned shape (slots split across lanes): rel. L2 <= 1e-12;
+* CUDA-graph replay and the unfused plain path: bit-exact with the fused path;
+* FP32 (FP32 weights, state and accumulation): rel. L2 against the FP64 oracle
+  <= 1e-5 on the tested horizons.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import rbffd_gpu_b200 as R
+from tests.helpers import sphere_problem, cosine_bell_setup, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def bell(ctx):
+    N, n = 4096, 31
+    xyz, st = sphere_problem(N, n, 1)
+    types = O.LAMBDA | O.THETA | O.HV
+    W = O.weights(xyz, st, None, 0.035 * np.sqrt(N), types, dim=2, poly_deg=2, hv_k=4, hv_scale=-1e-3 * N ** -4.0)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(types, grid, 2)
+    for t, w in W.items():
+        der.setWeights(t, w)
+    p = cosine_bell_setup()
+    cu, cv = O.cosine_bell_coeffs(xyz, a=p["a"], alpha=p["alpha"], u0=p["u0"])
+    h0 = R.exact_cosine_bell(xyz)
+    yield dict(xyz=xyz, st=st, W=W, grid=grid, der=der, p=p, cu=cu, cv=cv, h0=h0)
+    grid.close()
+
+
+def _oracle_bell(b, steps, u0=None):
+    return O.rk4_advect(b["st"], None, b["W"][O.LAMBDA], b["W"][O.THETA], b["W"][O.HV], b["cu"], b["cv"],
+                        b["h0"] if u0 is None else u0, b["p"]["dt"], steps)
+
+
+def _gpu_bell(b, steps, dtype=R.F64, shape=(1, 256), graph=False, unfused=False):
+    p = b["p"]
+    pde = R.CosineBell(b["grid"], b["der"], p["a"], p["alpha"], p["T"], True, dtype=dtype)
+    if shape is not None:
+        pde.setShape(*shape)
+    pde.fillInitialConditions(b["h0"])
+    pde.advance(R.RK4, p["dt"], steps, graph=graph, unfused=unfused)
+    out = pde.getLocalSolution()
+    t = pde.getTime()
+    pde.close()
+    return out, t
+
+
+@pytest.mark.parametrize("steps", [1, 4, 10])
+def test_cosine_bell_fp64_bit_exact(bell, steps):
+    out, t = _gpu_bell(bell, steps)
+    assert np.array_equal(out, _oracle_bell(bell, steps))
+    assert t == pytest.approx(steps * bell["p"]["dt"])
+
+
+def test_cosine_bell_fp64_autotuned_shape(bell):
+    out, _ = _gpu_bell(bell, 10, shape=None)
+    assert rel_l2(out, _oracle_bell(bell, 10)) < 1e-12
+
+
+@pytest.mark.parametrize("lanes", [2, 4, 8])
+def test_cosine_bell_fp64_split_rows(bell, lanes):
+    out, _ = _gpu_bell(bell, 10, shape=(lanes, 128))
+    assert rel_l2(out, _oracle_bell(bell, 10)) < 1e-12
+
+
+def test_graph_and_unfused_paths_bit_exact(bell):
+    ref, _ = _gpu_bell(bell, 60)
+    g, _ = _gpu_bell(bell, 60, graph=True)
+    u, _ = _gpu_bell(bell, 60, unfused=True)
+    assert np.array_equal(g, ref)
+    assert np.array_equal(u, ref)
+
+
+def test_cosine_bell_fp32_tolerance(bell):
+    out, _ = _gpu_bell(bell, 10, dtype=R.F32, shape=None)
+    assert rel_l2(out, _oracle_bell(bell, 10)) < 1e-5
+
+
+@pytest.fixture(scope="module")
+def heat(ctx):
+    N, n = 10242, 50
+    xyz, st = sphere_problem(N, n, 2)
+    W = O.weights(xyz, st, None, 0.044 * np.sqrt(N) - 0.14, O.LSFC, dim=2, poly_deg=3)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(O.LSFC, grid, 2)
+    der.setWeights(O.LSFC, W[O.LSFC])
+    lmax = 20
+    c = np.random.default_rng(2).standard_normal((lmax + 1) ** 2)
+    u0 = R.exact_sph_heat(xyz, lmax, c, 0.0)
+    yield dict(xyz=xyz, st=st, W=W, grid=grid, der=der, u0=u0, c=c, lmax=lmax)
+    grid.close()
+
+
+def _gpu_heat(h, steps, dt, dtype=R.F64, shape=(1, 256), graph=False):
+    pde = R.HeatSphere(h["grid"], h["der"], 1.0, dtype=dtype)
+    if shape is not None:
+        pde.setShape(*shape)
+    pde.fillInitialConditions(h["u0"])
+    pde.advance(R.RK4, dt, steps, graph=graph)
+    out = pde.getLocalSolution()
+    pde.close()
+    return out
+
+
+def test_heat_fp64_bit_exact(heat):
+    out = _gpu_heat(heat, 25, 1e-6)
+    assert np.array_equal(out, O.rk4_heat(heat["st"], None, heat["W"][O.LSFC], heat["u0"], 1e-6, 25))
+
+
+def test_heat_fp32_tolerance_and_exact_decay(heat):
+    steps, dt = 100, 1e-6
+    ref = O.rk4_heat(heat["st"], None, heat["W"][O.LSFC], heat["u0"], dt, steps)
+    out = _gpu_heat(heat, steps, dt, dtype=R.F32, shape=None, graph=True)
+    assert rel_l2(out, ref) < 1e-5
+    ex = R.exact_sph_heat(heat["xyz"], heat["lmax"], heat["c"], steps * dt)
+    assert rel_l2(ref, ex) < 1e-3
+
+
+@pytest.mark.parametrize("dtype,tol", [(R.F64, 0.0), (R.F32, 1e-5)])
+def test_multi_tracer_advection(bell, dtype, tol):
+    T = 16
+    rng = np.random.default_rng(4)
+    xyz = bell["xyz"]
+    cen = rng.normal(size=(T, 3))
+    cen /= np.linalg.norm(cen, axis=1)[:, None]
+    u0 = np.exp(-8.0 * ((xyz[:, None, :] - cen[None, :, :]) ** 2).sum(2))  # Gaussian hills, [N][T]
+    steps, dt = 10, bell["p"]["dt"]
+    ref = O.rk4_advect(bell["st"], None, bell["W"][O.LAMBDA], bell["W"][O.THETA], bell["W"][O.HV], bell["cu"],
+                       bell["cv"], u0, dt, steps)
+    pde = R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=dtype, ntracers=T)
+    pde.fillInitialConditions(u0)
+    pde.advance(R.RK4, dt, steps, graph=True)
+    out = pde.getLocalSolution()
+    pde.close()
+    if tol == 0.0:
+        assert np.array_equal(out, ref)
+    else:
+        assert rel_l2(out, ref) < tol

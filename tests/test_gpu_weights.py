@@ -1,0 +1,162 @@
+"""K1 parity: batched FP64 weights on the device against the oracle's
+restatement of RBFFD::computeAllWeightsForStencil_Direct (rbffd.cpp:225-352).
+
+The chain, step by step:
+1. assembly -- every entry of the device-built [A | B] within a few ulp of the
+   oracle's (the difference is CUDA's vs glibc's exp/sin/cos/atan2);
+2. elimination -- on identical systems the device solver's result equals the
+   oracle's dgesv restatement bit for bit;
+3. weights -- within a bound set by the conditioning of the systems (RBF-FD
+   saddle-point systems reach kappa ~ 1e13-1e15 here, so one-ulp input
+   differences move weights by up to ~kappa * 1e-16), and the derivatives
+   they produce agree with the oracle's and with the exact derivative.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle as O
+import rbffd_gpu_b200 as R
+from rbffd_gpu_b200 import _lib
+from tests.helpers import sphere_problem, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _params(types, dim=2, deg=0, hv_k=4, hv_gamma=0.0, hv_nodes=0.0):
+    return _lib.WeightParams(types, dim, deg, hv_k, hv_gamma, hv_nodes)
+
+
+def _device_assemble(grid, types, deg, eps, rows, dim=2, hv_k=4):
+    K = bin(types).count("1")
+    n = grid.n_pad
+    m = n + O.lib().orc_poly_size(deg)
+    out = np.zeros((len(rows), m, m + K))
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    epsv = np.full(grid.N, eps)
+    p = _params(types, dim, deg, hv_k)
+    grid.ctx.check(grid.ctx.L.rbffd_weights_assemble(grid.h, ctypes.byref(p), epsv.ctypes.data_as(_lib.dp), 0.0, None,
+                                                     rows.ctypes.data_as(_lib.ip), len(rows),
+                                                     out.ctypes.data_as(_lib.dp)), "assemble")
+    return out
+
+
+@pytest.mark.parametrize("N,n,deg,eps,types", [
+    (4096, 31, 0, 2.24, O.LAMBDA | O.THETA | O.HV),
+    (4096, 31, 2, 2.24, O.LAMBDA | O.THETA | O.HV),
+    (10242, 50, 3, 0.044 * np.sqrt(10242) - 0.14, O.LSFC),
+    (10242, 17, 1, 4.0, O.XSFC | O.YSFC | O.ZSFC),
+    (2562, 101, 4, 9.0, O.XSFC | O.YSFC | O.ZSFC | O.LAPL | O.INTERP),
+])
+def test_assembly_matches_oracle(ctx, N, n, deg, eps, types):
+    xyz, st = sphere_problem(N, n, 1)
+    grid = R.Grid(ctx, xyz, st)
+    rows = list(range(0, N, max(1, N // 37)))
+    dev = _device_assemble(grid, types, deg, eps, rows)
+    for k, r in enumerate(rows):
+        ref = O.assemble(xyz, st[r], deg, eps, types, dim=2, hv_k=4)
+        col_scale = np.abs(ref).max(axis=0)
+        err = np.abs(dev[k] - ref)
+        assert (err <= 8e-16 * np.abs(ref) + 4e-16 * col_scale[None, :]).all(), (r, err.max())
+    grid.close()
+
+
+def _gesv_dev(ctx, A, B):
+    batch, m, _ = A.shape
+    nrhs = B.shape[2]
+    dA = torch.tensor(A, dtype=torch.float64, device="cuda")
+    dB = torch.tensor(B, dtype=torch.float64, device="cuda")
+    info = torch.zeros(batch, dtype=torch.int32, device="cuda")
+    ctx.check(ctx.L.rbffd_batched_gesv_dev(ctx.h, m, nrhs, batch, dA.data_ptr(), dB.data_ptr(), info.data_ptr()),
+              "gesv")
+    return dB.cpu().numpy(), info.cpu().numpy()
+
+
+@pytest.mark.parametrize("deg", [0, 2, 3])
+def test_elimination_bit_exact_on_identical_systems(ctx, deg):
+    xyz, st = sphere_problem(4096, 31, 1)
+    systems = [O.assemble(xyz, st[r], deg, 2.24, O.LAMBDA | O.THETA | O.HV) for r in range(0, 4096, 64)]
+    m = systems[0].shape[0]
+    A = np.stack([s[:, :m] for s in systems])
+    B = np.stack([s[:, m:] for s in systems])
+    X, info = _gesv_dev(ctx, A, B)
+    assert (info == 0).all()
+    for k in range(len(systems)):
+        assert np.array_equal(X[k], O.lu_solve(A[k], B[k]))
+
+
+@pytest.mark.parametrize("m,nrhs", [(1, 1), (7, 2), (32, 3), (33, 1), (100, 4), (126, 3), (160, 2)])
+def test_elimination_bit_exact_random(ctx, m, nrhs):
+    rng = np.random.default_rng(m)
+    A = rng.normal(size=(9, m, m))
+    B = rng.normal(size=(9, m, nrhs))
+    X, info = _gesv_dev(ctx, A, B)
+    assert (info == 0).all()
+    for k in range(9):
+        assert np.array_equal(X[k], O.lu_solve(A[k], B[k]))
+
+
+def test_elimination_reports_zero_pivot(ctx):
+    A = np.eye(6)[None].repeat(2, axis=0)
+    A[1, :, 3] = 0.0  # column 3 exactly zero: zero pivot at step 3
+    B = np.ones((2, 6, 1))
+    _, info = _gesv_dev(ctx, A, B)
+    assert info[0] == 0 and info[1] == 4
+
+
+def test_weights_match_oracle_cosine_bell_setup(ctx):
+    N, n = 4096, 31
+    xyz, st = sphere_problem(N, n, 1)
+    types = O.LAMBDA | O.THETA | O.HV
+    eps = 0.035 * np.sqrt(N)
+    grid = R.Grid(ctx, xyz, st)
+    for deg in (0, 2):
+        der = R.RBFFD(types, grid, 2)
+        der.setEpsilon(eps)
+        der.setHVScalars(4, 1e-3)
+        der.setPolynomialDegree(deg)
+        der.computeAllWeightsForAllStencils()
+        W = O.weights(xyz, st, None, eps, types, dim=2, poly_deg=deg, hv_k=4, hv_scale=der.getHVScalar())
+        x, y, z = xyz.T
+        f = np.exp(np.sin(2 * x) + np.cos(3 * y) * z)
+        for t in (O.LAMBDA, O.THETA, O.HV):
+            wg = der.getWeights(t)
+            # kappa ~ 1e14 here (see module docstring): weights agree to ~1e-3, derivatives much closer
+            assert rel_l2(wg, W[t]) < 5e-3, (deg, t)
+            dg = O.apply(st, None, wg, f)
+            do = O.apply(st, None, W[t], f)
+            assert rel_l2(dg, do) < 1e-6, (deg, t)
+    grid.close()
+
+
+def test_weights_mixed_sizes_bucketed(ctx):
+    """Mixed stencil sizes and polynomial degrees in one call (the batched
+    configuration): n in {17,31,50,101}, degree matched {1,2,3,4}."""
+    N = 6000
+    xyz = R.fibonacci_nodes(N, 3)
+    full = R.knn_stencils(xyz, 101)
+    rng = np.random.default_rng(3)
+    sizes = np.array([17, 31, 50, 101])
+    pick = rng.integers(0, 4, N)
+    lens = sizes[pick].astype(np.int32)
+    degs = (pick + 1).astype(np.int32)
+    eps = rng.uniform(10.0, 16.0, N)  # kappa moderate on this node count
+    types = O.XSFC | O.YSFC | O.ZSFC
+    grid = R.Grid(ctx, xyz, full, st_len=lens)
+    der = R.RBFFD(types, grid, 2)
+    der.setEpsilon(eps)
+    der.setPolynomialDegree(1, deg_per_row=degs)
+    der.computeAllWeightsForAllStencils()
+    W = O.weights(xyz, full, lens, eps, types, dim=2, deg_per_row=degs)
+    x, y, z = xyz.T
+    f = np.sin(2 * x + y) * np.cos(z)
+    for t in (O.XSFC, O.YSFC, O.ZSFC):
+        wg = der.getWeights(t)
+        for k in range(4):
+            rows = pick == k
+            assert np.all(wg[rows][:, sizes[k]:] == 0.0)
+        assert rel_l2(O.apply(full, lens, wg, f), O.apply(full, lens, W[t], f)) < 1e-6
+    grid.close()

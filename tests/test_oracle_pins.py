@@ -1,0 +1,182 @@
+"""Pins of the oracle (CPU restatement in oracle/oracle.c) against the
+reference itself and against the reference's own known-answer tests.
+
+* RBF_Gaussian and cart2sph: bit-exact against the reference header
+  src/rbffd/rbfs/rbf_gaussian.h and src/utils/geom/cart2sph.cpp, compiled from
+  the reference sources into oracle/_ref.
+* The dgesv restatement: against numpy.linalg.solve (LAPACK dgesv), the
+  routine arma::solve calls (rbffd.cpp:259).
+* Stencils: the product's kNN against the reference k-d tree
+  (external/kdtree/KDTree.h), ordered lists bit-exact.
+* Weights: the reference's polynomial-reproduction test
+  (src/rbffd/derivative_tests.cpp:23-63, threshold :426-431) and the LSFC
+  test on Y_3^2 (tests/util/viennacl_spmv_benchmark/main_ublas.cpp:192-210).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import rbffd_gpu_b200 as R
+from tests.helpers import sphere_problem, rel_l2, rel_linf
+
+
+def test_rbf_functions_bit_exact_vs_reference_header():
+    L = O.ref_lib("ref_rbf")
+    if L is None:
+        pytest.skip("reference RBF header not built (no reference tree)")
+    rng = np.random.default_rng(0)
+    for which in range(9):
+        for _ in range(300):
+            d = rng.normal(size=3) * rng.choice([1e-3, 1e-1, 0.5])
+            eps = rng.uniform(0.5, 9.0)
+            dim = int(rng.integers(1, 4))
+            k = int(rng.integers(0, 9))
+            a = O.lib().orc_rbf(which, eps, dim, *d, k)
+            b = L.ref_rbf(which, eps, dim, *d, k)
+            assert a == b or (np.isnan(a) and np.isnan(b)), (which, eps, dim, k, a, b)
+
+
+def test_cart2sph_matches_reference():
+    import ctypes
+    L = O.ref_lib("ref_rbf")
+    if L is None:
+        pytest.skip("reference not built")
+    xyz = R.fibonacci_nodes(500, 7)
+    for p in xyz:
+        t, ph, r = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        L.ref_cart2sph(*p, ctypes.byref(t), ctypes.byref(ph), ctypes.byref(r))
+        assert (t.value, ph.value) == O.cart2sph(*p)
+
+
+@pytest.mark.parametrize("m,nrhs", [(5, 1), (21, 3), (40, 3), (66, 1), (126, 3)])
+def test_lu_restatement_vs_lapack(m, nrhs):
+    rng = np.random.default_rng(m)
+    A = rng.normal(size=(m, m)) + np.eye(m) * 0.1
+    B = rng.normal(size=(m, nrhs))
+    X = O.lu_solve(A, B)
+    Xr = np.linalg.solve(A, B)
+    cond = np.linalg.cond(A)
+    assert np.abs(X - Xr).max() / np.abs(Xr).max() < 1e-15 * cond * m
+
+
+def test_lu_restatement_on_stencil_systems_vs_lapack():
+    # saddle-point systems of the real problem (zero block needs pivoting)
+    xyz, st = sphere_problem(4096, 31, 1)
+    for deg in (0, 1, 2):
+        for row in (0, 1000, 3699):
+            a = O.assemble(xyz, st[row], deg, 2.24, O.LAMBDA | O.THETA | O.HV, dim=2, hv_k=4)
+            m = a.shape[0]
+            X = O.lu_solve(a[:, :m], a[:, m:])
+            Xr = np.linalg.solve(a[:, :m], a[:, m:])
+            # weights (first n rows) agree to the conditioning of the system
+            err = np.abs(X[:31] - Xr[:31]).max() / np.abs(Xr[:31]).max()
+            assert err < 1e-16 * np.linalg.cond(a[:, :m]), (deg, row, err)
+
+
+@pytest.mark.parametrize("N,n,seed", [(4096, 31, 1), (10242, 50, 2), (2562, 101, 5)])
+def test_knn_bit_exact_vs_reference_kdtree(N, n, seed):
+    xyz = R.fibonacci_nodes(N, seed)
+    st, ties = R.knn_stencils(xyz, n, return_ties=True)
+    ref = O.ref_knn(xyz, n)
+    if ref is None:
+        pytest.skip("reference k-d tree not built")
+    assert ties == 0
+    assert np.array_equal(st, ref[0])
+    assert (st[:, 0] == np.arange(N)).all()
+
+
+def _poly_funcs():
+    # DerivativeTests functions (derivative_tests.h:13): 0, x, y, x^2, xy, y^2, x^3, x^2y, xy^2, y^3
+    return [
+        (lambda x, y, z: 0 * x, lambda x, y, z: (0 * x, 0 * x, 0 * x)),
+        (lambda x, y, z: x, lambda x, y, z: (1 + 0 * x, 0 * x, 0 * x)),
+        (lambda x, y, z: y, lambda x, y, z: (0 * x, 1 + 0 * x, 0 * x)),
+        (lambda x, y, z: x * x, lambda x, y, z: (2 * x, 0 * x, 0 * x)),
+        (lambda x, y, z: x * y, lambda x, y, z: (y, x, 0 * x)),
+        (lambda x, y, z: y * y, lambda x, y, z: (0 * x, 2 * y, 0 * x)),
+        (lambda x, y, z: x ** 3, lambda x, y, z: (3 * x * x, 0 * x, 0 * x)),
+        (lambda x, y, z: x * x * y, lambda x, y, z: (2 * x * y, x * x, 0 * x)),
+        (lambda x, y, z: x * y * y, lambda x, y, z: (y * y, 2 * x * y, 0 * x)),
+        (lambda x, y, z: y ** 3, lambda x, y, z: (0 * x, 3 * y * y, 0 * x)),
+    ]
+
+
+@pytest.mark.parametrize("deg", [0, 2])
+def test_polynomial_reproduction_tangential_operators(deg):
+    """DerivativeTests::testAllFunctions on the sphere: the tangential
+    gradient operators (XSFC/YSFC/ZSFC) applied to the ten test functions;
+    fails when the average L2 error exceeds 1e-2 (derivative_tests.cpp:426)."""
+    N, n = 2562, 31
+    xyz, st = sphere_problem(N, n, 3)
+    W = O.weights(xyz, st, None, 6.0, O.XSFC | O.YSFC | O.ZSFC, dim=3, poly_deg=deg)
+    x, y, z = xyz.T
+    for f, g in _poly_funcs():
+        u = f(x, y, z)
+        gx, gy, gz = g(x, y, z)
+        gd = gx * x + gy * y + gz * z
+        exact = [gx - x * gd, gy - y * gd, gz - z * gd]
+        for k, t in enumerate((O.XSFC, O.YSFC, O.ZSFC)):
+            d = O.apply(st, None, W[t], u)
+            l2_avg = np.linalg.norm(d - exact[k]) / N
+            assert l2_avg < 1e-2 and np.isfinite(l2_avg)
+
+
+@pytest.mark.parametrize("deg", [1, 2, 3, 4])
+def test_polynomial_constraints_hold(deg):
+    """Beyond-reference polynomial augmentation: the solved weights satisfy
+    the border equations P^T w = (operator applied to the basis) -- the
+    weights differentiate every basis polynomial exactly."""
+    N, n = 2562, 31
+    xyz, st = sphere_problem(N, n, 3)
+    types = O.LAMBDA | O.THETA | O.LSFC | O.XSFC
+    for row in (0, 17, 1234, 2561):
+        a = O.assemble(xyz, st[row], deg, 4.0, types, dim=2)
+        m = a.shape[0]
+        X = O.lu_solve(a[:, :m], a[:, m:])
+        P = a[n:m, :n]
+        resid = P @ X[:n] - a[n:m, m:]
+        scale = np.abs(P).max(axis=1)[:, None] * np.abs(X[:n]).max(axis=0)[None, :]
+        assert (np.abs(resid) <= 1e-9 * scale + 1e-12).all(), (deg, row)
+
+
+def test_tangent_basis_improves_accuracy():
+    """Degree-2 tangent-plane augmentation gives more accurate LAMBDA/LSFC than the
+    reference's constant augmentation on a smooth field."""
+    N, n = 4096, 31
+    xyz, st = sphere_problem(N, n, 1)
+    x, y, z = xyz.T
+    lam = np.arctan2(y, x)
+    Y = np.sqrt(105 / np.pi) * (x - y) * (x + y) * z / 4.0
+    errs = {}
+    for deg in (0, 2):
+        W = O.weights(xyz, st, None, 0.035 * np.sqrt(N), O.LSFC, dim=2, poly_deg=deg)
+        errs[deg] = rel_l2(O.apply(st, None, W[O.LSFC], Y), -12 * Y)
+    assert errs[2] < errs[0]
+
+
+def test_lsfc_on_spherical_harmonic_Y32():
+    """-LSFC applied to Y_3^2 against its analytic surface Laplacian
+    (main_ublas.cpp:192-210 with SphericalHarmonic::Sph32, spherical_harmonics.h:39-58):
+    Laplace-Beltrami Y_3^2 = -12 Y_3^2."""
+    N, n = 4096, 31
+    xyz, st = sphere_problem(N, n, 1)
+    x, y, z = xyz.T
+    Y = np.sqrt(105 / np.pi) * (x - y) * (x + y) * z / 4.0
+    W = O.weights(xyz, st, None, 0.035 * np.sqrt(N), O.LSFC, dim=2, poly_deg=0)
+    d = O.apply(st, None, W[O.LSFC], Y)
+    assert rel_l2(d, -12 * Y) < 1e-3
+    assert rel_linf(d, -12 * Y) < 1e-2
+
+
+def test_heat_oracle_tracks_exact_spectral_decay():
+    """Heat on the sphere: RK4 of u_t = LSFC u against sum c_lm e^{-l(l+1)t} Y_lm."""
+    N, n = 4096, 31
+    xyz, st = sphere_problem(N, n, 1)
+    lmax = 6
+    c = np.random.default_rng(2).standard_normal((lmax + 1) ** 2)
+    u0 = R.exact_sph_heat(xyz, lmax, c, 0.0)
+    W = O.weights(xyz, st, None, 4.0, O.LSFC, dim=2, poly_deg=2)
+    dt, steps = 1e-4, 50
+    u = O.rk4_heat(st, None, W[O.LSFC], u0, dt, steps)
+    ex = R.exact_sph_heat(xyz, lmax, c, dt * steps)
+    assert rel_l2(u, ex) < 1e-4
