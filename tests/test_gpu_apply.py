@@ -5,9 +5,11 @@ The weights are the oracle's FP64 weights installed through
 rbffd_weights_set, so the comparison isolates the SpMV:
 * FP64 with one lane per row sums in the reference's order with fused
   multiply-adds: bit-exact.
-* FP32 (FP32 weights, FP32 accumulation, rbffd_cl.cpp:669-682): relative error
-  of the output within 2e-6 of the FP64 result (rel. L2 over the grid; the
-  bound is ~ n * 2^-24 * sum|w u| / |sum w u|, measured here for smooth u).
+* FP32 (FP32 weights, FP32 accumulation, rbffd_cl.cpp:669-682): relative L2
+  error of the output against the FP64 result within ~ sqrt(n) * 2^-24 *
+  sum|w u| / |sum w u|: 2e-6 for the first-derivative operators; 5e-5 for the
+  Laplace-Beltrami operator, whose weights (~1/h^2, summing to zero) cancel by
+  a factor of ~100 on a smooth field.
 """
 import numpy as np
 import pytest
@@ -42,11 +44,11 @@ def test_apply_fp64_bit_exact(setup, t):
     assert np.array_equal(d, ref)
 
 
-@pytest.mark.parametrize("t", [O.LAMBDA, O.THETA, O.LSFC])
-def test_apply_fp32_tolerance(setup, t):
+@pytest.mark.parametrize("t,tol", [(O.LAMBDA, 2e-6), (O.THETA, 2e-6), (O.LSFC, 5e-5)])
+def test_apply_fp32_tolerance(setup, t, tol):
     d = setup["der"].applyWeightsForDeriv(t, setup["u"], dtype=R.F32)
     ref = O.apply(setup["st"], None, setup["W"][t], setup["u"])
-    assert rel_l2(d, ref) < 2e-6
+    assert rel_l2(d, ref) < tol
 
 
 def test_apply_subrange_writes_only_range(setup):

@@ -91,7 +91,8 @@ def test_cosine_bell_fp32_tolerance(bell):
 def heat(ctx):
     N, n = 10242, 50
     xyz, st = sphere_problem(N, n, 2)
-    W = O.weights(xyz, st, None, 0.044 * np.sqrt(N) - 0.14, O.LSFC, dim=2, poly_deg=3)
+    # eps h = 0.25 (the benchmark's rule; flatter choices make kappa ~ 1e15 at large N)
+    W = O.weights(xyz, st, None, 0.25 / np.sqrt(4 * np.pi / N), O.LSFC, dim=2, poly_deg=3)
     grid = R.Grid(ctx, xyz, st)
     der = R.RBFFD(O.LSFC, grid, 2)
     der.setWeights(O.LSFC, W[O.LSFC])
