@@ -1,12 +1,12 @@
 // Context, grid and derivative application (K2: ELL SpMV) of librbffd_sm100.
 //
-// Device layout of a grid (slot-major ELL): for stencil slot s and row i,
-//   idx[s * Np + i], w[s * Np + i]
-// so that consecutive rows are consecutive in memory for every slot: a warp
-// handling 32 rows (or 32/G rows with G lanes per row) reads whole 32-byte
-// sectors of the weight and index streams.  Padding slots (s >= len[i]) hold
-// the centre index and weight 0, as RBFFD_CL's ELL packing does
-// (src/rbffd/rbffd_cl.cpp:238-242, 349-353), so every row runs n_pad slots
+// Device layout of a grid (row-major ELL): for row i and stencil slot s,
+//   idx[i * n4 + s], w[i * n4 + s],   n4 = n_pad rounded up to 4,
+// so a lane reads four consecutive slots of its row with one 16-byte index
+// load and one 16-byte (FP32) or two 16-byte (FP64) weight loads, and the G
+// lanes that share a row read its contiguous run together.  Padding slots
+// (s >= len[i]) hold the centre index and weight 0, as RBFFD_CL's ELL packing
+// does (src/rbffd/rbffd_cl.cpp:238-242, 349-353), so every row runs n4 slots
 // without a length check and the extra terms add exactly zero.
 #include <cuda_runtime.h>
 
@@ -14,6 +14,7 @@
 #include <cstring>
 #include <new>
 
+#include "ell.cuh"
 #include "internal.h"
 
 // ---------------------------------------------------------------------------
@@ -164,15 +165,14 @@ extern "C" int rbffd_ctx_stream(rbffd_ctx* ctx, void** stream)
 // ---------------------------------------------------------------------------
 // grid
 
-// Row-major host stencils [N][n_pad] (valid prefix len[i]) -> slot-major device
-// array with centre padding.
-__global__ void k_pack_stencils(const int* __restrict__ st_rm, const int* __restrict__ len, int N, int n_pad, int Np,
-                                int* __restrict__ idx)
+// Host stencils [N][n_pad] (valid prefix len[i]) -> sliced ELL with centre padding.
+__global__ void k_pack_stencils(const int* __restrict__ st_rm, const int* __restrict__ len, int N, int n_pad, int n4,
+                                int nc, int* __restrict__ idx)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     int L = len[i];
-    for (int s = 0; s < n_pad; s++) idx[(size_t)s * Np + i] = (s < L) ? st_rm[(size_t)i * n_pad + s] : i;
+    for (int s = 0; s < n4; s++) idx[sell_elem(i, s, nc)] = (s < L) ? st_rm[(size_t)i * n_pad + s] : i;
 }
 
 __global__ void k_xyz4(const double* __restrict__ xyz, int N, double4* __restrict__ out)
@@ -209,9 +209,12 @@ extern "C" int rbffd_grid_create(rbffd_ctx* ctx, int N, const double* xyz, int n
     g->ctx = ctx;
     g->N = N;
     g->n_pad = n_pad;
-    g->Np = round_up(N, 32);
+    g->n4 = round_up(n_pad, 4);
+    g->nc = g->n4 / 4;
+    g->N32 = round_up(N, 32);
     g->h_len = len;
-    size_t b_idx = (size_t)n_pad * g->Np * sizeof(int), b_len = (size_t)N * sizeof(int), b_xyz = (size_t)N * sizeof(double4);
+    size_t b_idx = (size_t)g->N32 * g->n4 * sizeof(int), b_len = (size_t)N * sizeof(int),
+           b_xyz = (size_t)N * sizeof(double4);
     int rc;
     int* d_st = nullptr;
     double* d_x3 = nullptr;
@@ -233,7 +236,7 @@ extern "C" int rbffd_grid_create(rbffd_ctx* ctx, int N, const double* xyz, int n
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_x3, xyz, (size_t)N * 3 * sizeof(double), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
         int B = 256, G = (N + B - 1) / B;
-        k_pack_stencils<<<G, B, 0, s>>>(d_st, g->d_len, N, n_pad, g->Np, g->d_idx);
+        k_pack_stencils<<<G, B, 0, s>>>(d_st, g->d_len, N, n_pad, g->n4, g->nc, g->d_idx);
         k_xyz4<<<G, B, 0, s>>>(d_x3, N, g->d_xyz);
         e = cudaGetLastError();
     }
@@ -254,7 +257,7 @@ extern "C" int rbffd_grid_destroy(rbffd_grid* g)
     rbffd_ctx* ctx = g->ctx;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    size_t wsz = (size_t)g->n_pad * g->Np;
+    size_t wsz = (size_t)g->N32 * g->n4;
     for (int t = 0; t < 16; t++) {
         dev_free(ctx, g->d_w64[t], wsz * sizeof(double));
         dev_free(ctx, g->d_w32[t], wsz * sizeof(float));
@@ -276,20 +279,21 @@ extern "C" int rbffd_grid_nbytes(const rbffd_grid* g, size_t* bytes)
 // ---------------------------------------------------------------------------
 // weights in and out
 
-__global__ void k_rowmajor_to_slot(const double* __restrict__ w_rm, const int* __restrict__ len, int N, int n_pad, int Np,
-                                   double* __restrict__ w)
+// host layout [N][n_pad] -> sliced ELL, zero beyond the stencil length
+__global__ void k_pad_rows(const double* __restrict__ w_rm, const int* __restrict__ len, int N, int n_pad, int n4, int nc,
+                           double* __restrict__ w)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     int L = len[i];
-    for (int s = 0; s < n_pad; s++) w[(size_t)s * Np + i] = (s < L) ? w_rm[(size_t)i * n_pad + s] : 0.0;
+    for (int s = 0; s < n4; s++) w[sell_elem(i, s, nc)] = (s < L) ? w_rm[(size_t)i * n_pad + s] : 0.0;
 }
 
-__global__ void k_slot_to_rowmajor(const double* __restrict__ w, int N, int n_pad, int Np, double* __restrict__ w_rm)
+__global__ void k_unpad_rows(const double* __restrict__ w, int N, int n_pad, int nc, double* __restrict__ w_rm)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    for (int s = 0; s < n_pad; s++) w_rm[(size_t)i * n_pad + s] = w[(size_t)s * Np + i];
+    for (int s = 0; s < n_pad; s++) w_rm[(size_t)i * n_pad + s] = w[sell_elem(i, s, nc)];
 }
 
 __global__ void k_cast_f32(const double* __restrict__ a, float* __restrict__ b, size_t n)
@@ -302,7 +306,7 @@ __global__ void k_cast_f32(const double* __restrict__ a, float* __restrict__ b, 
 int grid_make_f32(rbffd_grid* g, int op)
 {
     rbffd_ctx* ctx = g->ctx;
-    size_t n = (size_t)g->n_pad * g->Np;
+    size_t n = (size_t)g->N32 * g->n4;
     if (!g->d_w32[op]) {
         int rc = dev_alloc(ctx, (void**)&g->d_w32[op], n * sizeof(float));
         if (rc) return rc;
@@ -318,7 +322,7 @@ int grid_make_f32(rbffd_grid* g, int op)
 int grid_alloc_w64(rbffd_grid* g, int op)
 {
     if (g->d_w64[op]) return RBFFD_OK;
-    size_t n = (size_t)g->n_pad * g->Np;
+    size_t n = (size_t)g->N32 * g->n4;
     int rc = dev_alloc(g->ctx, (void**)&g->d_w64[op], n * sizeof(double));
     if (rc) return rc;
     g->bytes += n * sizeof(double);
@@ -340,7 +344,8 @@ extern "C" int rbffd_weights_set(rbffd_grid* g, unsigned der_type, const double*
     if ((rc = dev_alloc(ctx, (void**)&tmp, bytes))) return rc;
     cudaError_t e = cudaMemcpyAsync(tmp, w, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
-        k_rowmajor_to_slot<<<(g->N + 255) / 256, 256, 0, ctx->stream>>>(tmp, g->d_len, g->N, g->n_pad, g->Np, g->d_w64[op]);
+        k_pad_rows<<<(g->N + 255) / 256, 256, 0, ctx->stream>>>(tmp, g->d_len, g->N, g->n_pad, g->n4, g->nc,
+                                                                 g->d_w64[op]);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -363,7 +368,7 @@ extern "C" int rbffd_weights_get(rbffd_grid* g, unsigned der_type, double* w)
     double* tmp = nullptr;
     int rc = dev_alloc(ctx, (void**)&tmp, bytes);
     if (rc) return rc;
-    k_slot_to_rowmajor<<<(g->N + 255) / 256, 256, 0, ctx->stream>>>(g->d_w64[op], g->N, g->n_pad, g->Np, tmp);
+    k_unpad_rows<<<(g->N + 255) / 256, 256, 0, ctx->stream>>>(g->d_w64[op], g->N, g->n_pad, g->nc, tmp);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(w, tmp, bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -373,20 +378,13 @@ extern "C" int rbffd_weights_get(rbffd_grid* g, unsigned der_type, double* w)
 }
 
 // ---------------------------------------------------------------------------
-// K2: ELL apply.  G lanes per row; lane g handles slots g, g+G, ...; partial
-// sums combined by xor-shuffle.  With G == 1 the accumulation order is the
-// reference's (s = 0 .. n-1, rbffd.cpp:680-684) and FP64 results are exactly
-// those of a fused-multiply-add CPU loop.
-
-template <typename T>
-__device__ __forceinline__ T fmaT(T a, T b, T c);
-template <>
-__device__ __forceinline__ double fmaT<double>(double a, double b, double c) { return __fma_rn(a, b, c); }
-template <>
-__device__ __forceinline__ float fmaT<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// K2: ELL apply.  G lanes per (row, tracer); lane g handles the 4-slot chunks
+// g, g+G, ...; partial sums combined by xor-shuffle.  With G == 1 the
+// accumulation order is the reference's (s = 0 .. n-1, rbffd.cpp:680-684) and
+// FP64 results equal those of a fused-multiply-add CPU loop.
 
 template <typename T, int G>
-__global__ void __launch_bounds__(256) k_ell_apply(const int* __restrict__ idx, const T* __restrict__ w, int Np, int n_pad,
+__global__ void __launch_bounds__(256) k_ell_apply(const int* __restrict__ idx, const T* __restrict__ w, int nc,
                                                    const T* __restrict__ u, T* __restrict__ out, int start, int count,
                                                    int T_tr)
 {
@@ -396,13 +394,19 @@ __global__ void __launch_bounds__(256) k_ell_apply(const int* __restrict__ idx, 
     bool active = r < rows;
     int i = start + (active ? r / T_tr : 0), t = active ? r % T_tr : 0;
     T acc = T(0);
-    if (active)
-        for (int s = lane; s < n_pad; s += G) {
-            size_t o = (size_t)s * Np + i;
-            acc = fmaT<T>(__ldg(w + o), __ldg(u + (size_t)__ldg(idx + o) * T_tr + t), acc);
+    if (active) {
+        for (int c = lane; c < nc; c += G) {
+            const size_t o = sell_off(i, c, nc);
+            int4 j = ld_idx4(idx + o);
+            T wv[4];
+            ld_w4(w + o, wv);
+            acc = fma_rn<T>(wv[0], __ldg(u + (size_t)j.x * T_tr + t), acc);
+            acc = fma_rn<T>(wv[1], __ldg(u + (size_t)j.y * T_tr + t), acc);
+            acc = fma_rn<T>(wv[2], __ldg(u + (size_t)j.z * T_tr + t), acc);
+            acc = fma_rn<T>(wv[3], __ldg(u + (size_t)j.w * T_tr + t), acc);
         }
-#pragma unroll
-    for (int m = G / 2; m > 0; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m, G);
+    }
+    acc = group_sum<G>(acc);
     if (active && lane == 0) out[(size_t)i * T_tr + t] = acc;
 }
 
@@ -413,10 +417,10 @@ static void launch_apply(rbffd_grid* g, const T* w, const T* u, T* out, int star
     long long threads = (long long)count * T_tr * G;
     int B = 256, nb = (int)((threads + B - 1) / B);
     switch (G) {
-    case 1: k_ell_apply<T, 1><<<nb, B, 0, s>>>(g->d_idx, w, g->Np, g->n_pad, u, out, start, count, T_tr); break;
-    case 2: k_ell_apply<T, 2><<<nb, B, 0, s>>>(g->d_idx, w, g->Np, g->n_pad, u, out, start, count, T_tr); break;
-    case 4: k_ell_apply<T, 4><<<nb, B, 0, s>>>(g->d_idx, w, g->Np, g->n_pad, u, out, start, count, T_tr); break;
-    default: k_ell_apply<T, 8><<<nb, B, 0, s>>>(g->d_idx, w, g->Np, g->n_pad, u, out, start, count, T_tr); break;
+    case 1: k_ell_apply<T, 1><<<nb, B, 0, s>>>(g->d_idx, w, g->nc, u, out, start, count, T_tr); break;
+    case 2: k_ell_apply<T, 2><<<nb, B, 0, s>>>(g->d_idx, w, g->nc, u, out, start, count, T_tr); break;
+    case 4: k_ell_apply<T, 4><<<nb, B, 0, s>>>(g->d_idx, w, g->nc, u, out, start, count, T_tr); break;
+    default: k_ell_apply<T, 8><<<nb, B, 0, s>>>(g->d_idx, w, g->nc, u, out, start, count, T_tr); break;
     }
 }
 

@@ -47,11 +47,12 @@ struct rbffd_ctx {
 
 struct rbffd_grid {
     rbffd_ctx* ctx = nullptr;
-    int N = 0, n_pad = 0, Np = 0;  // Np: column stride of the slot-major ELL arrays (N rounded up to 32)
-    int* d_idx = nullptr;          // [n_pad][Np] node indices, padding = centre
+    int N = 0, n_pad = 0, n4 = 0;  // n4: slots per row (n_pad rounded up to 4)
+    int N32 = 0, nc = 0;           // rows rounded up to 32; chunks of 4 slots per row
+    int* d_idx = nullptr;          // sliced ELL (ell.cuh), N32 x n4: node indices, padding = centre
     int* d_len = nullptr;          // [N] stencil lengths
     double4* d_xyz = nullptr;      // [N] node coordinates (w unused)
-    double* d_w64[16] = {};        // per operator: [n_pad][Np] FP64 weights, padding 0
+    double* d_w64[16] = {};        // per operator, sliced ELL N32 x n4: FP64 weights, padding 0
     float* d_w32[16] = {};         // FP32 copies (rounded to nearest)
     std::vector<int> h_len;        // host copy of stencil lengths
     size_t bytes = 0;

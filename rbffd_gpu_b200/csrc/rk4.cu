@@ -27,6 +27,7 @@
 #include <new>
 #include <type_traits>
 
+#include "ell.cuh"
 #include "internal.h"
 
 int grid_apply_dev(rbffd_grid* g, int op, int dtype, int T_tr, const void* u, void* out, int start, int count, int G,
@@ -80,13 +81,13 @@ struct StageParams {
     const T* __restrict__ w2;
     const T* __restrict__ cu;
     const T* __restrict__ cv;
-    const T* x;   // gathered stage input
+    const T* x;   // gathered stage input (never written during a launch)
     T* u;         // u_n (written in stage 3)
     T* xnext;     // next stage input
     T* acc;       // RK accumulator
     T c;          // dt/2, dt/2, dt, dt/6 for stages 0..3
     T kappa;
-    int N, Np, n_pad, T_tr, stage;
+    int N, nc, T_tr, stage;  // nc: 4-slot chunks per row (sliced ELL, ell.cuh)
 };
 
 // Right-hand side and the stage update for one (row, tracer) value.
@@ -118,7 +119,8 @@ __device__ __forceinline__ void stage_update(const StageParams<T>& p, int i, siz
     }
 }
 
-// Single tracer, G lanes per row, slots split across the lanes.
+// Single tracer, G lanes per row; lane g handles the 4-slot chunks g, g+G, ...
+// With G == 1 the slots are accumulated in stencil order.
 template <typename T, int KIND, bool HV, int G>
 __global__ void __launch_bounds__(512) k_stage_scalar(StageParams<T> p)
 {
@@ -127,26 +129,31 @@ __global__ void __launch_bounds__(512) k_stage_scalar(StageParams<T> p)
     bool active = i < p.N;
     int ii = active ? i : 0;
     T d0 = T(0), d1 = T(0), d2 = T(0);
-    const int* __restrict__ ip = p.idx + ii;
-#pragma unroll 4
-    for (int s = lane; s < p.n_pad; s += G) {
-        size_t o = (size_t)s * p.Np;
-        int j = __ldg(ip + o);
-        T xj = p.x[j];
-        d0 = Ar<T>::fma(__ldg(p.w0 + o + ii), xj, d0);
+#pragma unroll 2
+    for (int c = lane; c < p.nc; c += G) {
+        const size_t o = sell_off(ii, c, p.nc);
+        int4 j = ld_idx4(p.idx + o);
+        T x[4] = {__ldg(p.x + j.x), __ldg(p.x + j.y), __ldg(p.x + j.z), __ldg(p.x + j.w)};
+        T w[4];
+        ld_w4(p.w0 + o, w);
+#pragma unroll
+        for (int k = 0; k < 4; k++) d0 = Ar<T>::fma(w[k], x[k], d0);
         if (KIND == KIND_ADVECT) {
-            d1 = Ar<T>::fma(__ldg(p.w1 + o + ii), xj, d1);
-            if (HV) d2 = Ar<T>::fma(__ldg(p.w2 + o + ii), xj, d2);
+            ld_w4(p.w1 + o, w);
+#pragma unroll
+            for (int k = 0; k < 4; k++) d1 = Ar<T>::fma(w[k], x[k], d1);
+            if (HV) {
+                ld_w4(p.w2 + o, w);
+#pragma unroll
+                for (int k = 0; k < 4; k++) d2 = Ar<T>::fma(w[k], x[k], d2);
+            }
         }
     }
     if (G > 1) {
-#pragma unroll
-        for (int m = G / 2; m > 0; m >>= 1) {
-            d0 += __shfl_xor_sync(0xffffffffu, d0, m, G);
-            if (KIND == KIND_ADVECT) {
-                d1 += __shfl_xor_sync(0xffffffffu, d1, m, G);
-                if (HV) d2 += __shfl_xor_sync(0xffffffffu, d2, m, G);
-            }
+        d0 = group_sum<G>(d0);
+        if (KIND == KIND_ADVECT) {
+            d1 = group_sum<G>(d1);
+            if (HV) d2 = group_sum<G>(d2);
         }
     }
     if (!active || lane != 0) return;
@@ -159,7 +166,8 @@ __global__ void __launch_bounds__(512) k_stage_scalar(StageParams<T> p)
 }
 
 // Multiple tracers: state [N][T_tr]; VEC consecutive tracers per lane, loaded
-// as one 16-byte vector; T_tr / VEC lanes per row share the row's weights.
+// as one 16-byte vector; T_tr / VEC lanes per row share the row's weights and
+// indices (same addresses: one transaction per chunk for the group).
 template <typename T, int VEC>
 struct VecT;
 template <>
@@ -175,8 +183,8 @@ template <typename T, int VEC>
 __device__ __forceinline__ void vload(const T* p, T (&v)[VEC])
 {
     typedef typename VecT<T, VEC>::type V;
-    V t = *reinterpret_cast<const V*>(p);
     static_assert(sizeof(V) == VEC * sizeof(T), "vector width");
+    V t = __ldg(reinterpret_cast<const V*>(p));
     memcpy(v, &t, sizeof(V));
 }
 
@@ -191,21 +199,27 @@ __global__ void __launch_bounds__(512) k_stage_vec(StageParams<T> p)
 #pragma unroll
     for (int v = 0; v < VEC; v++) d0[v] = d1[v] = d2[v] = T(0);
     const size_t toff = (size_t)lane * VEC;
-#pragma unroll 2
-    for (int s = 0; s < p.n_pad; s++) {
-        size_t o = (size_t)s * p.Np + i;
-        int j = __ldg(p.idx + o);
-        T xj[VEC];
-        vload<T, VEC>(p.x + (size_t)j * p.T_tr + toff, xj);
-        T a = __ldg(p.w0 + o);
-        T b = KIND == KIND_ADVECT ? __ldg(p.w1 + o) : T(0);
-        T c = (KIND == KIND_ADVECT && HV) ? __ldg(p.w2 + o) : T(0);
+    for (int c = 0; c < p.nc; c++) {
+        const size_t o = sell_off(i, c, p.nc);
+        int4 j4 = ld_idx4(p.idx + o);
+        const int jj[4] = {j4.x, j4.y, j4.z, j4.w};
+        T wa[4], wb[4], wc[4];
+        ld_w4(p.w0 + o, wa);
+        if (KIND == KIND_ADVECT) {
+            ld_w4(p.w1 + o, wb);
+            if (HV) ld_w4(p.w2 + o, wc);
+        }
 #pragma unroll
-        for (int v = 0; v < VEC; v++) {
-            d0[v] = Ar<T>::fma(a, xj[v], d0[v]);
-            if (KIND == KIND_ADVECT) {
-                d1[v] = Ar<T>::fma(b, xj[v], d1[v]);
-                if (HV) d2[v] = Ar<T>::fma(c, xj[v], d2[v]);
+        for (int k = 0; k < 4; k++) {
+            T xj[VEC];
+            vload<T, VEC>(p.x + (size_t)jj[k] * p.T_tr + toff, xj);
+#pragma unroll
+            for (int v = 0; v < VEC; v++) {
+                d0[v] = Ar<T>::fma(wa[k], xj[v], d0[v]);
+                if (KIND == KIND_ADVECT) {
+                    d1[v] = Ar<T>::fma(wb[k], xj[v], d1[v]);
+                    if (HV) d2[v] = Ar<T>::fma(wc[k], xj[v], d2[v]);
+                }
             }
         }
     }
@@ -264,8 +278,7 @@ static StageParams<T> make_params(rbffd_pde* P, int stage, double dt)
     p.u = u;
     p.acc = (T*)P->acc;
     p.N = g->N;
-    p.Np = g->Np;
-    p.n_pad = g->n_pad;
+    p.nc = g->nc;
     p.T_tr = P->T;
     p.stage = stage;
     return p;
@@ -283,7 +296,8 @@ static void launch_stage_t(rbffd_pde* P, const StageParams<T>& p, Shape sh, cuda
         case 1: k_stage_scalar<T, KIND, HV, 1><<<nb, B, 0, s>>>(p); break;
         case 2: k_stage_scalar<T, KIND, HV, 2><<<nb, B, 0, s>>>(p); break;
         case 4: k_stage_scalar<T, KIND, HV, 4><<<nb, B, 0, s>>>(p); break;
-        default: k_stage_scalar<T, KIND, HV, 8><<<nb, B, 0, s>>>(p); break;
+        case 8: k_stage_scalar<T, KIND, HV, 8><<<nb, B, 0, s>>>(p); break;
+        default: k_stage_scalar<T, KIND, HV, 16><<<nb, B, 0, s>>>(p); break;
         }
         return;
     }
@@ -355,7 +369,7 @@ static Shape autotune(rbffd_pde* P)
     std::vector<Shape> cands;
     const int blocks[3] = {128, 256, 512};
     if (P->T == 1) {
-        const int lanes[4] = {1, 2, 4, 8};
+        const int lanes[5] = {1, 2, 4, 8, 16};
         for (int G : lanes)
             for (int B : blocks) cands.push_back(Shape{G, B});
     } else {
@@ -613,7 +627,7 @@ extern "C" int rbffd_pde_set_shape(rbffd_pde* P, int lanes, int block)
         P->shape = Shape{};
         return RBFFD_OK;
     }
-    if (!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8)) return RBFFD_ERR_INVALID;
+    if (!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16)) return RBFFD_ERR_INVALID;
     if (!(block == 0 || block == 64 || block == 128 || block == 256 || block == 512)) return RBFFD_ERR_INVALID;
     if (P->T > 1 && lanes > 1) return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "lanes per row apply to one tracer only");
     P->shape = Shape{lanes ? lanes : 1, block ? block : 256};

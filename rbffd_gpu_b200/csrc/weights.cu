@@ -33,6 +33,7 @@
 #include <map>
 #include <vector>
 
+#include "ell.cuh"
 #include "internal.h"
 
 int grid_alloc_w64(rbffd_grid* g, int op);
@@ -52,7 +53,7 @@ struct WParams {
     double* w[MAX_K];
     int* status;  // min(row) + 1 over rows with a zero pivot, INT_MAX if none
     double eps_uniform, hv_scale;
-    int Np, n_pad, deg_uniform, nrows, K, m, dim, hv_k, team_stride;  // team_stride: doubles per team
+    int n4, n_pad, deg_uniform, nrows, K, m, dim, hv_k, team_stride;  // n4: row stride; team_stride: doubles per team
     int opbit[MAX_K];
 };
 
@@ -383,7 +384,7 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
     const double eps = P.eps ? P.eps[r] : P.eps_uniform;  // var_epsilon[stencil[0]]
     const double eps2 = eps * eps;
     for (int q = T.tid; q < n; q += T.size) {
-        double4 v = P.xyz[P.idx[(size_t)q * P.Np + r]];
+        double4 v = P.xyz[P.idx[sell_elem(r, q, P.n4 >> 2)]];
         xs[3 * q] = v.x;
         xs[3 * q + 1] = v.y;
         xs[3 * q + 2] = v.z;
@@ -481,12 +482,12 @@ __global__ void __launch_bounds__(512) k_weights(WParams P, int team_size)
         const bool ok = team_eliminate(T, a, m, K, cand_v, cand_r) == 0;
         if (ok) team_back_substitute(T, a, m, K);
         if (!ok && T.tid == 0) atomicMin(P.status, r + 1);
-        // store: weights[type][r][j] = W(j, col) * scale, slot-major (rbffd.cpp:300-306)
-        for (int e = T.tid; e < K * P.n_pad; e += T.size) {
-            int c = e / P.n_pad, j = e - c * P.n_pad;
+        // store: weights[type][r][j] = W(j, col) * scale (rbffd.cpp:300-306), row r of the sliced ELL
+        for (int e = T.tid; e < K * P.n4; e += T.size) {
+            int c = e / P.n4, j = e - c * P.n4;
             double scale = P.opbit[c] == RBFFD_HV ? P.hv_scale : 1.0;
             double v = (j < n) ? (ok ? a[j * ld + m + c] * scale : __longlong_as_double(0x7ff8000000000000ll)) : 0.0;
-            P.w[c][(size_t)j * P.Np + r] = v;
+            P.w[c][sell_elem(r, j, P.n4 >> 2)] = v;
         }
         T.sync();
     }
@@ -677,7 +678,7 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
     P.deg = d_deg;
     P.deg_uniform = prm->poly_deg;
     P.status = d_status;
-    P.Np = g->Np;
+    P.n4 = g->n4;
     P.n_pad = g->n_pad;
     P.dim = prm->dim;
     P.hv_k = prm->hv_k;
@@ -844,7 +845,7 @@ extern "C" int rbffd_weights_assemble(rbffd_grid* g, const rbffd_weight_params* 
     P.nrows = count;
     P.K = K;
     P.m = m;
-    P.Np = g->Np;
+    P.n4 = g->n4;
     P.n_pad = g->n_pad;
     P.dim = prm->dim;
     P.hv_k = prm->hv_k;
