@@ -206,6 +206,23 @@ enum rbffd_advance_flags {
  * (src/pdes/time_dependent_pde.cpp:53-73,172-304), nsteps times.
  * scheme must be 2 (TimeDependentPDE::RK4). */
 int rbffd_pde_advance(rbffd_pde* pde, int scheme, double dt, int nsteps, int flags);
+/* Heat-equation RK4 that allocates no device memory.  No counterpart in the
+ * reference: it exists for callers that cannot let a library allocate on the
+ * GPU -- applications that reserve the device's memory for their own pool, or
+ * latency-critical loops where cudaMalloc/cudaFree would synchronise the
+ * device.  The caller passes the state u_dev, N values of dtype in its own
+ * device memory, advanced in place by nsteps RK4 steps of
+ * u_t = kappa * LSFC u on the grid's Laplace-Beltrami weights (computed or
+ * set beforehand).  The three RK4 stage buffers live in one fixed array
+ * inside the library, reserved on each GPU when the library's device code is
+ * loaded there and held until the process exits: grids above 262144 nodes
+ * (FP64) or 524288 nodes (FP32) are rejected with RBFFD_ERR_INVALID.  The
+ * first call on a device looks up that array's device address, so make it
+ * before any stream capture.  All calls on a device share the array and
+ * leave their stage values in it: calls that overlap on the GPU race and
+ * must be serialised by the caller.  Runs on the context stream and returns
+ * after the steps complete. */
+int rbffd_heat_rk4_noalloc(rbffd_grid* grid, int dtype, double kappa, double dt, int nsteps, void* u_dev);
 /* Kernel-shape choice for this PDE's stage kernel (lanes per stencil row and
  * threads per block); 0 = autotuned. */
 int rbffd_pde_set_shape(rbffd_pde* pde, int lanes_per_row, int block_threads);

@@ -716,3 +716,102 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
     if (!(flags & RBFFD_ADVANCE_ASYNC)) RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     return RBFFD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free RK4 for the heat equation.
+//
+// Some callers cannot let a library allocate device memory: applications that
+// reserve (almost) all of the GPU's memory up front for their own pool, so a
+// cudaMalloc inside the library would fail or fragment that pool, and callers
+// on latency-critical paths, where cudaMalloc/cudaFree may synchronise the
+// device.  rbffd_heat_rk4_noalloc serves them: the caller passes the state
+// vector in its own device memory and the three stage buffers RK4 needs live
+// in the file-scope array below, reserved when this library's device code is
+// loaded on a GPU and held until the process exits.
+//
+// Limits and sharing: NOALLOC_MAX_NODES nodes in FP64 (twice that in FP32);
+// larger grids are rejected.  Every call on a device uses the same array, so
+// calls that overlap on that GPU (other streams, other threads, other
+// contexts of this process) overwrite each other's stage buffers: serialise
+// them.  Stage 0 writes every scratch element a later stage reads, so the
+// array needs no clearing between calls.
+constexpr int NOALLOC_MAX_NODES = 262144;
+static __device__ __align__(256) double g_noalloc_scratch[3 * NOALLOC_MAX_NODES];  // 6 MiB per GPU
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[128];  // device address of g_noalloc_scratch, per device ordinal
+
+// The host-side name g_noalloc_scratch is not a device address: the address a
+// kernel may use is looked up once per device, with that device current.
+static int noalloc_scratch(rbffd_ctx* ctx, void** out)
+{
+    if (ctx->device < 0 || ctx->device >= 128) return set_error(ctx, RBFFD_ERR_INVALID, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[ctx->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return cuda_error(ctx, e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
+        g_noalloc_ptr[ctx->device] = p;
+    }
+    *out = g_noalloc_ptr[ctx->device];
+    return RBFFD_OK;
+}
+
+template <typename T>
+static void noalloc_steps(rbffd_grid* g, const T* w, T* u, T* scratch, T kappa, double dt, int nsteps, cudaStream_t s)
+{
+    const int N = g->N;
+    T* xa = scratch;
+    T* xb = scratch + N;
+    T* acc = scratch + 2 * (size_t)N;
+    StageParams<T> p;
+    p.idx = g->d_idx;
+    p.w0 = w;
+    p.w1 = nullptr;
+    p.w2 = nullptr;
+    p.cu = nullptr;
+    p.cv = nullptr;
+    p.u = u;
+    p.acc = acc;
+    p.kappa = kappa;
+    p.N = N;
+    p.nc = g->nc;
+    p.T_tr = 1;
+    const int B = 256, nb = (N + B - 1) / B;
+    for (int k = 0; k < nsteps; k++)
+        for (int st = 0; st < 4; st++) {
+            static const double cfac[3] = {0.5, 0.5, 1.0};
+            p.c = (T)(st == 3 ? dt / 6. : cfac[st] * dt);
+            p.x = st == 0 ? u : (st == 1 ? xa : (st == 2 ? xb : xa));
+            p.xnext = st == 0 ? xa : (st == 1 ? xb : (st == 2 ? xa : nullptr));
+            p.stage = st;
+            k_stage_scalar<T, KIND_HEAT, false, 1><<<nb, B, 0, s>>>(p);
+        }
+}
+
+extern "C" int rbffd_heat_rk4_noalloc(rbffd_grid* g, int dtype, double kappa, double dt, int nsteps, void* u_dev)
+{
+    if (!g || !u_dev || nsteps < 0) return RBFFD_ERR_INVALID;
+    rbffd_ctx* ctx = g->ctx;
+    if (dtype != RBFFD_F32 && dtype != RBFFD_F64) return set_error(ctx, RBFFD_ERR_INVALID, "bad dtype %d", dtype);
+    const int max_nodes = dtype == RBFFD_F64 ? NOALLOC_MAX_NODES : 2 * NOALLOC_MAX_NODES;
+    if (g->N > max_nodes)
+        return set_error(ctx, RBFFD_ERR_INVALID,
+                         "rbffd_heat_rk4_noalloc: grid has %d nodes, the fixed scratch holds at most %d (%s)", g->N,
+                         max_nodes, dtype == RBFFD_F64 ? "FP64" : "FP32");
+    const int op = der_index(RBFFD_LSFC);
+    const void* w = dtype == RBFFD_F64 ? (const void*)g->d_w64[op] : (const void*)g->d_w32[op];
+    if (!w) return set_error(ctx, RBFFD_ERR_STATE, "Laplace-Beltrami (LSFC) weights are not on the device");
+    if (nsteps == 0) return RBFFD_OK;
+    RBFFD_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(ctx, &scratch);
+    if (rc) return rc;
+    if (dtype == RBFFD_F64)
+        noalloc_steps<double>(g, (const double*)w, (double*)u_dev, (double*)scratch, kappa, dt, nsteps, ctx->stream);
+    else
+        noalloc_steps<float>(g, (const float*)w, (float*)u_dev, (float*)scratch, (float)kappa, dt, nsteps, ctx->stream);
+    RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return RBFFD_OK;
+}
