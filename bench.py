@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="setup plus 25 un-graphed RK4 steps with a fixed kernel shape, for ncu captures")
+    ap.add_argument("--profile-multitracer", default=None, metavar="ROWS,LANES",
+                    help="16-tracer vortex case on N=163842, n=101 (weights > L2), 3 un-graphed RK4 steps with the "
+                         "tiled shape ROWS,LANES (0,0 = global-memory gathers), for ncu captures")
     return ap.parse_args()
 
 
@@ -360,6 +363,69 @@ def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
     out["shape_fp32"] = pde32.getShape()
     p64.close()
     pplain.close()
+    out["multitracer"] = bench_multitracer(R, torch, ctx)
+    return out
+
+
+MULTITRACER = dict(name="vortex_16tracers_N655362_n101_deg2_2000steps", N=655362, n=101, T=16, deg=2, eps_h=0.5,
+                   hv_k=4, hv_gamma=1e-3, dt=1.5e-3, steps=2000, seed=4)
+
+
+def bench_multitracer(R, torch, ctx):
+    """16 tracers (cosine bells and Gaussian hills) in a deformational vortex flow:
+    the vortex roll-up turning about a seeded tilted axis; LAMBDA + THETA + Delta^4
+    hyperviscosity; 2000 RK4 steps captured in CUDA graphs; FP32 and FP64.  The
+    working set (>1 GB per stage) exceeds L2: this is the HBM-bound case."""
+    from rbffd_gpu_b200 import workloads as WL
+    C = MULTITRACER
+    N, n, T, steps, dt = C["N"], C["n"], C["T"], C["steps"], C["dt"]
+    xyz = R.fibonacci_nodes(N, C["seed"])
+    st = R.knn_stencils(xyz, n)
+    axis = WL.seeded_axis(C["seed"])
+    cu, cv = WL.vortex_coefficients(xyz, axis)
+    tracers = WL.tracer_set(T, C["seed"])
+    u0 = WL.tracer_field(xyz, *tracers)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(R.LAMBDA | R.THETA | R.HV, grid, 2)
+    der.setEpsilon(C["eps_h"] / np.sqrt(4 * np.pi / N))
+    der.setHVScalars(C["hv_k"], C["hv_gamma"])
+    der.setPolynomialDegree(C["deg"])
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    der.computeAllWeightsForAllStencils()
+    t_weights = time.perf_counter() - t
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    res = {}
+    for dtype in (R.F32, R.F64):
+        pde = R.Advection(grid, der, cu, cv, True, dtype=dtype, ntracers=T)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, dt, 25, graph=True)
+        pde.fillInitialConditions(u0)
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
+        e1.record(stream)
+        ctx.synchronize()
+        res[dtype] = (pde.getLocalSolution(), e0.elapsed_time(e1) * 1e-3, pde.getShape())
+        pde.close()
+    exact = WL.vortex_exact(xyz, axis, tracers, steps * dt)
+    u32, u64 = res[R.F32][0], res[R.F64][0]
+    peak, peak_kind = load_peaks()
+    out = {"workload": C["name"], "weights_setup_s": t_weights}
+    for dtype, tag, wb, sb in ((R.F32, "fp32", 4, 4), (R.F64, "fp64", 8, 8)):
+        secs = res[dtype][1]
+        per_launch = secs / (4 * steps)
+        bytes_launch = N * (3 * n * wb + 4 * n + 4 * T * sb)
+        out[tag] = {"node_updates_per_s": N * steps / secs, "tracer_node_updates_per_s": N * T * steps / secs,
+                    "ms_per_rk4_step": 1e3 * secs / steps, "shape": res[dtype][2],
+                    "roofline": {"bound": "hbm", "achieved": bytes_launch / per_launch / 1e9, "peak": peak,
+                                 "unit": "GB/s", "frac": bytes_launch / per_launch / 1e9 / peak,
+                                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_launch}}
+    out["rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64))
+    out["rel_linf_fp32_vs_fp64"] = float(np.abs(u32 - u64).max() / np.abs(u64).max())
+    out["rel_l2_fp64_vs_exact"] = float(np.linalg.norm(u64 - exact) / np.linalg.norm(exact))
+    grid.close()
     return out
 
 
@@ -382,9 +448,41 @@ def run_profile():
     print("profile run done")
 
 
+def run_profile_multitracer(spec):
+    import rbffd_gpu_b200 as R
+    from rbffd_gpu_b200 import workloads as WL
+    rows, lanes = (int(x) for x in spec.split(","))
+    N, n, T = 163842, 101, 16
+    xyz = R.fibonacci_nodes(N, 4)
+    st = R.knn_stencils(xyz, n)
+    axis = WL.seeded_axis(4)
+    cu, cv = WL.vortex_coefficients(xyz, axis)
+    u0 = WL.tracer_field(xyz, *WL.tracer_set(T, 4))
+    ctx = R.Context(0)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(R.LAMBDA | R.THETA | R.HV, grid, 2)
+    der.setEpsilon(0.5 / np.sqrt(4 * np.pi / N))
+    der.setHVScalars(4, 1e-3)
+    der.setPolynomialDegree(2)
+    der.computeAllWeightsForAllStencils()
+    pde = R.Advection(grid, der, cu, cv, True, dtype=R.F32, ntracers=T)
+    if rows > 0:
+        pde.setTiledShape(rows, lanes)
+    else:
+        pde.setShape(1, 256)
+    pde.fillInitialConditions(u0)
+    pde.advance(R.RK4, 3e-3, 3)
+    pde.close()
+    grid.close()
+    ctx.close()
+    print("profile run done")
+
+
 def main():
     args = parse()
-    if args.profile:
+    if args.profile_multitracer:
+        run_profile_multitracer(args.profile_multitracer)
+    elif args.profile:
         run_profile()
     elif args.impl == "reference":
         run_reference(args)

@@ -213,9 +213,10 @@ int rbffd_pde_advance(rbffd_pde* pde, int scheme, double dt, int nsteps, int fla
  * device.  The caller passes the state u_dev, N values of dtype in its own
  * device memory, advanced in place by nsteps RK4 steps of
  * u_t = kappa * LSFC u on the grid's Laplace-Beltrami weights (computed or
- * set beforehand).  The three RK4 stage buffers live in one fixed array
- * inside the library, reserved on each GPU when the library's device code is
- * loaded there and held until the process exits: grids above 262144 nodes
+ * set beforehand).  A copy of the state in the grid's internal node order and
+ * the three RK4 stage buffers live in one fixed 8 MiB array inside the
+ * library, reserved on each GPU when the library's device code is loaded
+ * there and held until the process exits: grids above 262144 nodes
  * (FP64) or 524288 nodes (FP32) are rejected with RBFFD_ERR_INVALID.  The
  * first call on a device looks up that array's device address, so make it
  * before any stream capture.  All calls on a device share the array and
@@ -227,6 +228,17 @@ int rbffd_heat_rk4_noalloc(rbffd_grid* grid, int dtype, double kappa, double dt,
  * threads per block); 0 = autotuned. */
 int rbffd_pde_set_shape(rbffd_pde* pde, int lanes_per_row, int block_threads);
 int rbffd_pde_get_shape(rbffd_pde* pde, int* lanes_per_row, int* block_threads);
+/* Tiled stage kernel: each thread block takes rows_per_block consecutive rows
+ * (a multiple of 32) and stages the node values their stencils gather in
+ * shared memory; lanes (1, 2 or 4) split each row's slots.  With
+ * stream_weights (one lane per row) the block's weights and indices are also
+ * streamed into shared memory by asynchronous bulk copies (TMA), several
+ * stages ahead; its waits are bounded and a timeout is reported by
+ * rbffd_pde_advance as RBFFD_ERR_TIMEOUT.  Returns RBFFD_ERR_UNSUPPORTED if
+ * the staged data do not fit shared memory.
+ * get_tiling reports 0 when the stage kernel gathers from global memory. */
+int rbffd_pde_set_tiled_shape(rbffd_pde* pde, int rows_per_block, int lanes, int stream_weights);
+int rbffd_pde_get_tiling(rbffd_pde* pde, int* rows_per_block);
 
 #ifdef __cplusplus
 }

@@ -311,9 +311,15 @@ class TimeDependentPDE:
         self.ctx.check(self.ctx.L.rbffd_pde_set_shape(self.h, lanes_per_row, block_threads), "set_shape")
 
     def getShape(self):
-        a, b = ctypes.c_int(), ctypes.c_int()
+        """(lanes per row, threads per block, rows per tiled block or 0)."""
+        a, b, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         self.ctx.check(self.ctx.L.rbffd_pde_get_shape(self.h, ctypes.byref(a), ctypes.byref(b)))
-        return a.value, b.value
+        self.ctx.check(self.ctx.L.rbffd_pde_get_tiling(self.h, ctypes.byref(r)))
+        return a.value, b.value, r.value
+
+    def setTiledShape(self, rows_per_block, lanes=1, stream_weights=False):
+        self.ctx.check(self.ctx.L.rbffd_pde_set_tiled_shape(self.h, rows_per_block, lanes, int(stream_weights)),
+                       "set_tiled_shape")
 
     def close(self):
         if getattr(self, "h", None):

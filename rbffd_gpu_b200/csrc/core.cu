@@ -1,18 +1,22 @@
 // Context, grid and derivative application (K2: ELL SpMV) of librbffd_sm100.
 //
-// Device layout of a grid (row-major ELL): for row i and stencil slot s,
-//   idx[i * n4 + s], w[i * n4 + s],   n4 = n_pad rounded up to 4,
-// so a lane reads four consecutive slots of its row with one 16-byte index
-// load and one 16-byte (FP32) or two 16-byte (FP64) weight loads, and the G
-// lanes that share a row read its contiguous run together.  Padding slots
-// (s >= len[i]) hold the centre index and weight 0, as RBFFD_CL's ELL packing
-// does (src/rbffd/rbffd_cl.cpp:238-242, 349-353), so every row runs n4 slots
-// without a length check and the extra terms add exactly zero.
+// Device layout of a grid: the sliced ELL arrays of ell.cuh (32-row slices,
+// 4-slot chunks), n4 = n_pad rounded up to 4 slots per row, rows in the
+// grid's internal (Morton) order.  A lane reads four consecutive slots of its
+// row with one 16-byte index load and one 16-byte (FP32) or two 16-byte
+// (FP64) weight loads.  Padding slots (s >= len[i]) hold the centre index and
+// weight 0, as RBFFD_CL's ELL packing does (src/rbffd/rbffd_cl.cpp:238-242,
+// 349-353), so every row runs n4 slots without a length check and the extra
+// terms add exactly zero.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <functional>
+#include <iterator>
 #include <new>
+#include <thread>
 
 #include "ell.cuh"
 #include "internal.h"
@@ -117,8 +121,27 @@ extern "C" int rbffd_ctx_create(int device, rbffd_ctx** out)
         return RBFFD_ERR_CUDA;
     }
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (cudaMalloc((void**)&c->d_status, sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        if (c->d_status) cudaFree(c->d_status);
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return RBFFD_ERR_CUDA;
+    }
     *out = c;
     return RBFFD_OK;
+}
+
+int ctx_check_device_status(rbffd_ctx* ctx)
+{
+    int st = 0;
+    RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (st == DEV_STATUS_OK) return RBFFD_OK;
+    RBFFD_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return set_error(ctx, RBFFD_ERR_TIMEOUT, "a stage kernel gave up waiting for its bulk copies (device status %d)", st);
 }
 
 extern "C" int rbffd_ctx_destroy(rbffd_ctx* ctx)
@@ -127,6 +150,7 @@ extern "C" int rbffd_ctx_destroy(rbffd_ctx* ctx)
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
+    if (ctx->d_status) cudaFree(ctx->d_status);
     delete ctx;
     return RBFFD_OK;
 }
@@ -212,14 +236,53 @@ extern "C" int rbffd_grid_create(rbffd_ctx* ctx, int N, const double* xyz, int n
     g->n4 = round_up(n_pad, 4);
     g->nc = g->n4 / 4;
     g->N32 = round_up(N, 32);
-    g->h_len = len;
+    // Internal order: nodes sorted along a 3-D Morton curve (21 bits per axis),
+    // ties by index, so consecutive rows are spatial neighbours and share most
+    // of the nodes their stencils gather.
+    {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int i = 0; i < N; i++)
+            for (int a = 0; a < 3; a++) {
+                lo[a] = std::min(lo[a], xyz[3 * (size_t)i + a]);
+                hi[a] = std::max(hi[a], xyz[3 * (size_t)i + a]);
+            }
+        std::vector<std::pair<uint64_t, int>> key(N);
+        for (int i = 0; i < N; i++) {
+            uint64_t code = 0;
+            uint32_t q[3];
+            for (int a = 0; a < 3; a++) {
+                double ext = hi[a] - lo[a];
+                double f = ext > 0 ? (xyz[3 * (size_t)i + a] - lo[a]) / ext : 0.0;
+                q[a] = (uint32_t)std::min(2097151.0, std::max(0.0, f * 2097151.0));
+            }
+            for (int b = 20; b >= 0; b--)
+                for (int a = 0; a < 3; a++) code = (code << 1) | ((q[a] >> b) & 1u);
+            key[i] = {code, i};
+        }
+        std::sort(key.begin(), key.end());
+        g->h_perm.resize(N);
+        g->h_iperm.resize(N);
+        for (int i = 0; i < N; i++) {
+            g->h_perm[i] = key[i].second;
+            g->h_iperm[key[i].second] = i;
+        }
+    }
+    std::vector<int> st_int((size_t)N * n_pad, 0);
+    std::vector<double> xyz_int((size_t)N * 3);
+    g->h_len.resize(N);
+    for (int i = 0; i < N; i++) {
+        const int o = g->h_perm[i];
+        g->h_len[i] = len[o];
+        for (int s = 0; s < len[o]; s++) st_int[(size_t)i * n_pad + s] = g->h_iperm[st[(size_t)o * n_pad + s]];
+        for (int a = 0; a < 3; a++) xyz_int[3 * (size_t)i + a] = xyz[3 * (size_t)o + a];
+    }
     size_t b_idx = (size_t)g->N32 * g->n4 * sizeof(int), b_len = (size_t)N * sizeof(int),
            b_xyz = (size_t)N * sizeof(double4);
     int rc;
     int* d_st = nullptr;
     double* d_x3 = nullptr;
     if ((rc = dev_alloc(ctx, (void**)&g->d_idx, b_idx)) || (rc = dev_alloc(ctx, (void**)&g->d_len, b_len)) ||
-        (rc = dev_alloc(ctx, (void**)&g->d_xyz, b_xyz)) ||
+        (rc = dev_alloc(ctx, (void**)&g->d_xyz, b_xyz)) || (rc = dev_alloc(ctx, (void**)&g->d_perm, b_len)) ||
         (rc = dev_alloc(ctx, (void**)&d_st, (size_t)N * n_pad * sizeof(int))) ||
         (rc = dev_alloc(ctx, (void**)&d_x3, (size_t)N * 3 * sizeof(double)))) {
         dev_free(ctx, d_st, (size_t)N * n_pad * sizeof(int));
@@ -227,13 +290,14 @@ extern "C" int rbffd_grid_create(rbffd_ctx* ctx, int N, const double* xyz, int n
         rbffd_grid_destroy(g);
         return rc;
     }
-    g->bytes = b_idx + b_len + b_xyz;
+    g->bytes = b_idx + 2 * b_len + b_xyz;
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMemsetAsync(g->d_idx, 0, b_idx, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_st, st, (size_t)N * n_pad * sizeof(int), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(g->d_len, len.data(), b_len, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_x3, xyz, (size_t)N * 3 * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_st, st_int.data(), (size_t)N * n_pad * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(g->d_len, g->h_len.data(), b_len, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(g->d_perm, g->h_perm.data(), b_len, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_x3, xyz_int.data(), (size_t)N * 3 * sizeof(double), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
         int B = 256, G = (N + B - 1) / B;
         k_pack_stencils<<<G, B, 0, s>>>(d_st, g->d_len, N, n_pad, g->n4, g->nc, g->d_idx);
@@ -264,9 +328,188 @@ extern "C" int rbffd_grid_destroy(rbffd_grid* g)
     }
     dev_free(ctx, g->d_idx, wsz * sizeof(int));
     dev_free(ctx, g->d_len, (size_t)g->N * sizeof(int));
+    dev_free(ctx, g->d_perm, (size_t)g->N * sizeof(int));
     dev_free(ctx, g->d_xyz, (size_t)g->N * sizeof(double4));
+    for (auto& kv : g->halos) {
+        Halo* h = kv.second;
+        dev_free(ctx, h->d_ptr, (size_t)(h->nblocks + 1) * sizeof(int));
+        dev_free(ctx, h->d_rows, (size_t)(h->nblocks + 1) * sizeof(int));
+        dev_free(ctx, h->d_nodes, h->b_nodes);
+        dev_free(ctx, h->d_lidx, h->b_lidx);
+        delete h;
+    }
     delete g;
     return RBFFD_OK;
+}
+
+// Row blocks and their halos (see struct Halo).  Built on the host from the
+// device's stencil array the first time a block size is used.
+int grid_halo(rbffd_grid* g, int R, const Halo** out)
+{
+    auto it = g->halos.find(R);
+    if (it != g->halos.end()) {
+        *out = it->second;
+        return RBFFD_OK;
+    }
+    rbffd_ctx* ctx = g->ctx;
+    if (R < 32 || R % 32) return set_error(ctx, RBFFD_ERR_INVALID, "rows per block %d must be a multiple of 32", R);
+    const int N = g->N, nc = g->nc, n4 = g->n4;
+    const size_t nidx = (size_t)g->N32 * n4;
+    std::vector<int> idx(nidx);
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    RBFFD_CUDA_TRY(ctx, cudaMemcpy(idx.data(), g->d_idx, nidx * sizeof(int), cudaMemcpyDeviceToHost));
+    // Per-slice (32 rows) sorted unique node lists.
+    const int nsl = (N + 31) / 32;
+    std::vector<std::vector<int>> snodes(nsl);
+    auto run = [&](int count, const std::function<void(int)>& f) {
+        std::atomic<int> next(0);
+        unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < hw; t++)
+            pool.emplace_back([&]() {
+                for (int k; (k = next.fetch_add(1)) < count;) f(k);
+            });
+        for (auto& t : pool) t.join();
+    };
+    run(nsl, [&](int q) {
+        std::vector<int>& v = snodes[q];
+        for (int r = 32 * q; r < std::min(N, 32 * q + 32); r++)
+            for (int s = 0; s < n4; s++) v.push_back(idx[sell_elem(r, s, nc)]);
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+    });
+    auto merge = [](const std::vector<int>& x, const std::vector<int>& y) {
+        std::vector<int> m;
+        m.reserve(x.size() + y.size());
+        std::set_union(x.begin(), x.end(), y.begin(), y.end(), std::back_inserter(m));
+        return m;
+    };
+    // Cap on a block's halo: the 90th percentile of fixed R-row blocks' halos
+    // (shared memory is sized by the largest halo, so outliers are split).
+    const int spb = R / 32, nfixed = (nsl + spb - 1) / spb;
+    std::vector<int> fsize(nfixed);
+    run(nfixed, [&](int b) {
+        std::vector<int> u;
+        for (int q = b * spb; q < std::min(nsl, (b + 1) * spb); q++) u = merge(u, snodes[q]);
+        fsize[b] = (int)u.size();
+    });
+    std::vector<int> sorted_f(fsize);
+    std::sort(sorted_f.begin(), sorted_f.end());
+    size_t cap = (size_t)sorted_f[(size_t)(0.9 * (sorted_f.size() - 1))];
+    for (int q = 0; q < nsl; q++) cap = std::max(cap, snodes[q].size());
+    if (cap > 65535) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a block halo exceeds 65535 nodes");
+    // Greedy partition: grow each block slice by slice while the halo stays under the cap.
+    std::vector<int> bstart;
+    std::vector<std::vector<int>> nodes;
+    for (int q = 0; q < nsl;) {
+        bstart.push_back(q);
+        std::vector<int> cur = snodes[q++];
+        while (q < nsl && q - bstart.back() < spb) {
+            std::vector<int> m = merge(cur, snodes[q]);
+            if (m.size() > cap) break;
+            cur.swap(m);
+            q++;
+        }
+        nodes.push_back(std::move(cur));
+    }
+    const int nblocks = (int)bstart.size();
+    bstart.push_back(nsl);
+    std::vector<int> rows(nblocks + 1);
+    for (int b = 0; b <= nblocks; b++) rows[b] = std::min(N, 32 * bstart[b]);
+    std::vector<unsigned short> lidx(nidx, 0);
+    run(nblocks, [&](int b) {
+        const std::vector<int>& v = nodes[b];
+        for (int r = rows[b]; r < rows[b + 1]; r++)
+            for (int s = 0; s < n4; s++) {
+                const size_t e = sell_elem(r, s, nc);
+                lidx[e] = (unsigned short)(std::lower_bound(v.begin(), v.end(), idx[e]) - v.begin());
+            }
+    });
+    std::vector<int> ptr(nblocks + 1, 0), flat;
+    int max_halo = 0;
+    for (int b = 0; b < nblocks; b++) {
+        ptr[b + 1] = ptr[b] + (int)nodes[b].size();
+        max_halo = std::max(max_halo, (int)nodes[b].size());
+    }
+    flat.reserve(ptr[nblocks]);
+    for (int b = 0; b < nblocks; b++) flat.insert(flat.end(), nodes[b].begin(), nodes[b].end());
+    Halo* h = new (std::nothrow) Halo();
+    if (!h) return RBFFD_ERR_OOM;
+    h->R = R;
+    h->nblocks = nblocks;
+    h->max_halo = max_halo;
+    const size_t b_ptr = ptr.size() * sizeof(int), b_nodes = flat.size() * sizeof(int),
+                 b_lidx = nidx * sizeof(unsigned short);
+    int rc;
+    if ((rc = dev_alloc(ctx, (void**)&h->d_ptr, b_ptr)) || (rc = dev_alloc(ctx, (void**)&h->d_nodes, b_nodes)) ||
+        (rc = dev_alloc(ctx, (void**)&h->d_lidx, b_lidx)) || (rc = dev_alloc(ctx, (void**)&h->d_rows, b_ptr))) {
+        dev_free(ctx, h->d_ptr, b_ptr);
+        dev_free(ctx, h->d_nodes, b_nodes);
+        dev_free(ctx, h->d_lidx, b_lidx);
+        delete h;
+        return rc;
+    }
+    cudaError_t e = cudaMemcpy(h->d_ptr, ptr.data(), b_ptr, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_rows, rows.data(), b_ptr, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_nodes, flat.data(), b_nodes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_lidx, lidx.data(), b_lidx, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        dev_free(ctx, h->d_ptr, b_ptr);
+        dev_free(ctx, h->d_nodes, b_nodes);
+        dev_free(ctx, h->d_lidx, b_lidx);
+        dev_free(ctx, h->d_rows, b_ptr);
+        delete h;
+        return cuda_error(ctx, e, "grid_halo upload");
+    }
+    h->b_nodes = b_nodes;
+    h->b_lidx = b_lidx;
+    g->bytes += 2 * b_ptr + b_nodes + b_lidx;
+    g->halos[R] = h;
+    *out = h;
+    return RBFFD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// caller order <-> internal order
+
+template <typename E>
+__global__ void k_permute(const E* __restrict__ src, E* __restrict__ dst, const int* __restrict__ perm, int N, int T,
+                          int to_internal)
+{
+    size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)N * T) return;
+    int i = (int)(e / T), t = (int)(e % T);
+    size_t o = (size_t)perm[i] * T + t;
+    if (to_internal)
+        dst[e] = src[o];
+    else
+        dst[o] = src[e];
+}
+
+static int grid_permute(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s, int to_int)
+{
+    size_t n = (size_t)g->N * T;
+    int nb = (int)((n + 255) / 256);
+    if (elem_bytes == 8)
+        k_permute<unsigned long long><<<nb, 256, 0, s>>>((const unsigned long long*)src, (unsigned long long*)dst,
+                                                         g->d_perm, g->N, T, to_int);
+    else if (elem_bytes == 4)
+        k_permute<unsigned int><<<nb, 256, 0, s>>>((const unsigned int*)src, (unsigned int*)dst, g->d_perm, g->N, T,
+                                                   to_int);
+    else
+        return set_error(g->ctx, RBFFD_ERR_INVALID, "element size %d", elem_bytes);
+    RBFFD_CUDA_TRY(g->ctx, cudaGetLastError());
+    return RBFFD_OK;
+}
+
+int grid_to_internal(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s)
+{
+    return grid_permute(g, src, dst, T, elem_bytes, s, 1);
+}
+
+int grid_to_caller(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s)
+{
+    return grid_permute(g, src, dst, T, elem_bytes, s, 0);
 }
 
 extern "C" int rbffd_grid_nbytes(const rbffd_grid* g, size_t* bytes)
@@ -279,21 +522,25 @@ extern "C" int rbffd_grid_nbytes(const rbffd_grid* g, size_t* bytes)
 // ---------------------------------------------------------------------------
 // weights in and out
 
-// host layout [N][n_pad] -> sliced ELL, zero beyond the stencil length
-__global__ void k_pad_rows(const double* __restrict__ w_rm, const int* __restrict__ len, int N, int n_pad, int n4, int nc,
-                           double* __restrict__ w)
+// host layout [N][n_pad] in the caller's order -> sliced ELL in internal
+// order (internal row i is the caller's row perm[i]), zero beyond the stencil length
+__global__ void k_pad_rows(const double* __restrict__ w_rm, const int* __restrict__ len, const int* __restrict__ perm,
+                           int N, int n_pad, int n4, int nc, double* __restrict__ w)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     int L = len[i];
-    for (int s = 0; s < n4; s++) w[sell_elem(i, s, nc)] = (s < L) ? w_rm[(size_t)i * n_pad + s] : 0.0;
+    const double* src = w_rm + (size_t)perm[i] * n_pad;
+    for (int s = 0; s < n4; s++) w[sell_elem(i, s, nc)] = (s < L) ? src[s] : 0.0;
 }
 
-__global__ void k_unpad_rows(const double* __restrict__ w, int N, int n_pad, int nc, double* __restrict__ w_rm)
+__global__ void k_unpad_rows(const double* __restrict__ w, const int* __restrict__ perm, int N, int n_pad, int nc,
+                             double* __restrict__ w_rm)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    for (int s = 0; s < n_pad; s++) w_rm[(size_t)i * n_pad + s] = w[sell_elem(i, s, nc)];
+    double* dst = w_rm + (size_t)perm[i] * n_pad;
+    for (int s = 0; s < n_pad; s++) dst[s] = w[sell_elem(i, s, nc)];
 }
 
 __global__ void k_cast_f32(const double* __restrict__ a, float* __restrict__ b, size_t n)
@@ -344,8 +591,8 @@ extern "C" int rbffd_weights_set(rbffd_grid* g, unsigned der_type, const double*
     if ((rc = dev_alloc(ctx, (void**)&tmp, bytes))) return rc;
     cudaError_t e = cudaMemcpyAsync(tmp, w, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
-        k_pad_rows<<<(g->N + 255) / 256, 256, 0, ctx->stream>>>(tmp, g->d_len, g->N, g->n_pad, g->n4, g->nc,
-                                                                 g->d_w64[op]);
+        k_pad_rows<<<(g->N + 255) / 256, 256, 0, ctx->stream>>>(tmp, g->d_len, g->d_perm, g->N, g->n_pad, g->n4,
+                                                                 g->nc, g->d_w64[op]);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -368,7 +615,7 @@ extern "C" int rbffd_weights_get(rbffd_grid* g, unsigned der_type, double* w)
     double* tmp = nullptr;
     int rc = dev_alloc(ctx, (void**)&tmp, bytes);
     if (rc) return rc;
-    k_unpad_rows<<<(g->N + 255) / 256, 256, 0, ctx->stream>>>(g->d_w64[op], g->N, g->n_pad, g->nc, tmp);
+    k_unpad_rows<<<(g->N + 255) / 256, 256, 0, ctx->stream>>>(g->d_w64[op], g->d_perm, g->N, g->n_pad, g->nc, tmp);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(w, tmp, bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -475,15 +722,18 @@ extern "C" int rbffd_apply(rbffd_grid* g, unsigned der_type, int dtype, unsigned
         return rc;
     }
     cudaStream_t s = ctx->stream;
+    // du: caller order -> dd: internal order -> apply (all rows) -> du -> dd: caller order
     cudaError_t e = cudaMemcpyAsync(du, u, b64, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess) rc = grid_to_internal(g, du, dd, 1, 8, s);
+    if (e == cudaSuccess && rc == RBFFD_OK) {
         if (dtype == RBFFD_F64) {
-            rc = grid_apply_dev(g, op, dtype, 1, du, dd, (int)start, (int)count, 1, s);
+            rc = grid_apply_dev(g, op, dtype, 1, dd, du, 0, N, 1, s);
         } else {
-            k_d2f<<<(N + 255) / 256, 256, 0, s>>>(du, fu, N);
-            rc = grid_apply_dev(g, op, dtype, 1, fu, fd, (int)start, (int)count, 1, s);
-            if (rc == RBFFD_OK) k_f2d<<<(N + 255) / 256, 256, 0, s>>>(fd, dd, N);
+            k_d2f<<<(N + 255) / 256, 256, 0, s>>>(dd, fu, N);
+            rc = grid_apply_dev(g, op, dtype, 1, fu, fd, 0, N, 1, s);
+            if (rc == RBFFD_OK) k_f2d<<<(N + 255) / 256, 256, 0, s>>>(fd, du, N);
         }
+        if (rc == RBFFD_OK) rc = grid_to_caller(g, du, dd, 1, 8, s);
         e = cudaGetLastError();
     }
     if (rc == RBFFD_OK && e == cudaSuccess)
@@ -505,6 +755,24 @@ extern "C" int rbffd_apply_dev(rbffd_grid* g, unsigned der_type, int dtype, int 
     if (dtype != RBFFD_F32 && dtype != RBFFD_F64) return set_error(g->ctx, RBFFD_ERR_INVALID, "bad dtype %d", dtype);
     int op = der_index(der_type);
     if (op < 0) return set_error(g->ctx, RBFFD_ERR_INVALID, "der_type 0x%x is not a single operator", der_type);
-    cudaSetDevice(g->ctx->device);
-    return grid_apply_dev(g, op, dtype, ntracers, u_dev, deriv_dev, 0, g->N, 1, g->ctx->stream);
+    rbffd_ctx* ctx = g->ctx;
+    cudaSetDevice(ctx->device);
+    const int es = dtype == RBFFD_F64 ? 8 : 4;
+    const size_t bytes = (size_t)g->N * ntracers * es;
+    void *tin = nullptr, *tout = nullptr;
+    int rc;
+    if ((rc = dev_alloc(ctx, &tin, bytes)) || (rc = dev_alloc(ctx, &tout, bytes))) {
+        dev_free(ctx, tin, bytes);
+        return rc;
+    }
+    cudaStream_t s = ctx->stream;
+    rc = grid_to_internal(g, u_dev, tin, ntracers, es, s);
+    if (rc == RBFFD_OK) rc = grid_apply_dev(g, op, dtype, ntracers, tin, tout, 0, g->N, 1, s);
+    if (rc == RBFFD_OK) rc = grid_to_caller(g, tout, deriv_dev, ntracers, es, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    dev_free(ctx, tin, bytes);
+    dev_free(ctx, tout, bytes);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "rbffd_apply_dev");
+    return RBFFD_OK;
 }

@@ -41,6 +41,26 @@ __device__ __forceinline__ void ld_w4(const double* p, double (&w)[4])
     w[3] = b.y;
 }
 
+// four consecutive weights from shared memory (16-byte aligned)
+__device__ __forceinline__ void ld_w4_shared(const float* p, float (&w)[4])
+{
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    w[0] = t.x;
+    w[1] = t.y;
+    w[2] = t.z;
+    w[3] = t.w;
+}
+
+__device__ __forceinline__ void ld_w4_shared(const double* p, double (&w)[4])
+{
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    w[0] = a.x;
+    w[1] = a.y;
+    w[2] = b.x;
+    w[3] = b.y;
+}
+
 template <typename T>
 __device__ __forceinline__ T fma_rn(T a, T b, T c);
 template <>

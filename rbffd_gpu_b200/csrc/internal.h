@@ -33,7 +33,13 @@ struct TuneKey {
 };
 struct Shape {
     int lanes = 0, block = 0;
+    int tile = 0;  // rows per block with the halo staged in shared memory; 0 = gather from global memory
+    int tma = 0;   // tiled kernel that streams weights and indices into shared memory with bulk copies
 };
+
+// Device status word of a context: kernels whose waits are bounded write a
+// nonzero code here instead of hanging or trapping; the host reads and clears it.
+enum { DEV_STATUS_OK = 0, DEV_STATUS_WAIT_TIMEOUT = 1 };
 
 struct rbffd_ctx {
     int device = 0;
@@ -43,7 +49,11 @@ struct rbffd_ctx {
     size_t held = 0;
     std::mutex mu;
     std::map<TuneKey, Shape> tuned;  // autotuner results per problem shape
+    int* d_status = nullptr;         // DEV_STATUS_* written by kernels with bounded waits
 };
+
+// Read and clear the context's device status; RBFFD_ERR_TIMEOUT if a kernel gave up waiting.
+int ctx_check_device_status(rbffd_ctx* ctx);
 
 struct rbffd_grid {
     rbffd_ctx* ctx = nullptr;
@@ -54,9 +64,36 @@ struct rbffd_grid {
     double4* d_xyz = nullptr;      // [N] node coordinates (w unused)
     double* d_w64[16] = {};        // per operator, sliced ELL N32 x n4: FP64 weights, padding 0
     float* d_w32[16] = {};         // FP32 copies (rounded to nearest)
-    std::vector<int> h_len;        // host copy of stencil lengths
+    // Rows and nodes are stored in an internal order (a 3-D Morton curve through
+    // the nodes) so that rows handled together gather from nearby nodes; the
+    // stencil slot order is kept, so each row's arithmetic is unchanged.
+    int* d_perm = nullptr;         // [N] internal row -> caller's node index
+    std::vector<int> h_perm;       // same, on the host
+    std::vector<int> h_iperm;      // caller's node index -> internal row
+    std::vector<int> h_len;        // stencil lengths, internal order
+    std::map<int, struct Halo*> halos;  // per rows-per-block R, built on first use
     size_t bytes = 0;
 };
+
+// Move [N][T] values (elem_bytes each) between the caller's node order and the
+// grid's internal order (device arrays, on stream s).
+int grid_to_internal(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s);
+int grid_to_caller(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s);
+
+// Row blocks of R consecutive internal rows with their halo: the sorted unique
+// nodes their stencils reference.  A block's kernel stages the halo's values in
+// shared memory and reads them through 16-bit local indices (lidx, the sliced
+// ELL layout of the stencils with each node index replaced by its position in
+// the block's halo).
+struct Halo {
+    int R = 0, nblocks = 0, max_halo = 0;  // R: most rows in a block (blocks hold whole 32-row slices)
+    int* d_rows = nullptr;       // [nblocks + 1] first row of each block
+    int* d_ptr = nullptr;        // [nblocks + 1] offsets into d_nodes
+    int* d_nodes = nullptr;      // halo node indices (internal order)
+    unsigned short* d_lidx = nullptr;  // sliced ELL, N32 x n4
+    size_t b_nodes = 0, b_lidx = 0;
+};
+int grid_halo(rbffd_grid* g, int R, const Halo** out);
 
 struct rbffd_pde;  // defined in rk4.cu
 

@@ -29,6 +29,7 @@
 
 #include "ell.cuh"
 #include "internal.h"
+#include "tma.cuh"
 
 int grid_apply_dev(rbffd_grid* g, int op, int dtype, int T_tr, const void* u, void* out, int start, int count, int G,
                    cudaStream_t s);
@@ -233,6 +234,222 @@ __global__ void __launch_bounds__(512) k_stage_vec(StageParams<T> p)
         stage_update<T, KIND, HV>(p, i, (size_t)i * p.T_tr + toff + v, d0[v], d1[v], d2[v], cu, cv);
 }
 
+// Tiled stage kernel: one CTA per block of R consecutive internal rows.  The
+// CTA first copies the values of its halo (the unique nodes its rows' stencils
+// reference, struct Halo) from global memory into shared memory -- each node's
+// T values once, as 16-byte vectors -- then every row gathers from shared
+// memory through 16-bit local indices.  The per-row arithmetic is that of
+// k_stage_vec / k_stage_scalar: lane group (T/VEC lanes) x G chunk lanes per
+// row, chunks in stencil order per lane.
+struct TileParams {
+    const int* __restrict__ ptr;
+    const int* __restrict__ nodes;
+    const unsigned short* __restrict__ lidx;
+    const int* __restrict__ rows;  // [nblocks + 1]: block b owns rows [rows[b], rows[b+1])
+    int R;                         // most rows in a block
+    int N32;                       // rows of the sliced ELL arrays (N rounded up to 32)
+};
+
+template <typename T, int VEC, int G, int KIND, bool HV>
+__global__ void __launch_bounds__(1024) k_stage_tile(StageParams<T> p, TileParams tp)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sx = reinterpret_cast<T*>(smem_raw);
+    typedef typename VecT<T, VEC>::type V;
+    const int vpn = p.T_tr / VEC;  // vectors per node (= lanes per tracer group of a row)
+    const int L = vpn * G;         // threads per row
+    const int b = blockIdx.x;
+    const int h0 = __ldg(tp.ptr + b), hn = __ldg(tp.ptr + b + 1) - h0;
+    for (int e = threadIdx.x; e < hn * vpn; e += blockDim.x) {
+        const int h = e / vpn, v = e - h * vpn;
+        const int node = __ldg(tp.nodes + h0 + h);
+        reinterpret_cast<V*>(sx)[(size_t)h * vpn + v] =
+            __ldg(reinterpret_cast<const V*>(p.x + (size_t)node * p.T_tr) + v);
+    }
+    __syncthreads();
+    const int lr = threadIdx.x % L, rl = threadIdx.x / L;
+    const int i = __ldg(tp.rows + b) + rl;
+    const bool active = i < __ldg(tp.rows + b + 1);
+    const int tv = lr % vpn, g = lr / vpn;
+    T d0[VEC], d1[VEC], d2[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; v++) d0[v] = d1[v] = d2[v] = T(0);
+    if (active) {
+#pragma unroll 2
+        for (int c = g; c < p.nc; c += G) {
+            const size_t o = sell_off(i, c, p.nc);
+            const ushort4 l4 = __ldg(reinterpret_cast<const ushort4*>(tp.lidx + o));
+            const int ll[4] = {l4.x, l4.y, l4.z, l4.w};
+            T wa[4], wb[4], wc[4];
+            ld_w4(p.w0 + o, wa);
+            if (KIND == KIND_ADVECT) {
+                ld_w4(p.w1 + o, wb);
+                if (HV) ld_w4(p.w2 + o, wc);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                T xj[VEC];
+                const V t = reinterpret_cast<const V*>(sx)[(size_t)ll[k] * vpn + tv];
+                memcpy(xj, &t, sizeof(V));
+#pragma unroll
+                for (int v = 0; v < VEC; v++) {
+                    d0[v] = Ar<T>::fma(wa[k], xj[v], d0[v]);
+                    if (KIND == KIND_ADVECT) {
+                        d1[v] = Ar<T>::fma(wb[k], xj[v], d1[v]);
+                        if (HV) d2[v] = Ar<T>::fma(wc[k], xj[v], d2[v]);
+                    }
+                }
+            }
+        }
+    }
+    if (G > 1) {
+#pragma unroll
+        for (int m = G / 2; m > 0; m >>= 1)
+#pragma unroll
+            for (int v = 0; v < VEC; v++) {
+                d0[v] += __shfl_xor_sync(0xffffffffu, d0[v], m * vpn, L);
+                if (KIND == KIND_ADVECT) {
+                    d1[v] += __shfl_xor_sync(0xffffffffu, d1[v], m * vpn, L);
+                    if (HV) d2[v] += __shfl_xor_sync(0xffffffffu, d2[v], m * vpn, L);
+                }
+            }
+    }
+    if (!active || g != 0) return;
+    T cu = T(0), cv = T(0);
+    if (KIND == KIND_ADVECT) {
+        cu = p.cu[i];
+        cv = p.cv[i];
+    }
+#pragma unroll
+    for (int v = 0; v < VEC; v++)
+        stage_update<T, KIND, HV>(p, i, (size_t)i * p.T_tr + (size_t)tv * VEC + v, d0[v], d1[v], d2[v], cu, cv);
+}
+
+// Tiled stage kernel with bulk-copy streaming.  Same per-row arithmetic as
+// k_stage_tile with one chunk lane per row, but the block's weights and local
+// indices -- in the sliced layout one contiguous run per operator per 32-row
+// slice -- are streamed into a ring of TMA_NB shared-memory stage buffers by
+// asynchronous bulk copies (cp.async.bulk, completion counted on an mbarrier),
+// TMA_CS chunks per stage, so the copy engine keeps TMA_NB stages of the weight
+// stream in flight per block without holding them in registers.  Thread 0
+// issues the copies; a stage buffer is refilled after the block's barrier
+// that ends its use.  Every wait is bounded: on timeout the block records
+// DEV_STATUS_WAIT_TIMEOUT in *status, waits (bounded) for its copies still in
+// flight and returns.
+constexpr int TMA_CS = 4;
+constexpr int TMA_NB = 3;
+constexpr long long TMA_WAIT_LIMIT = 1ll << 22;
+
+template <typename T, int VEC, int KIND, bool HV>
+__global__ void __launch_bounds__(1024) k_stage_tma(StageParams<T> p, TileParams tp, int* status, int halo_bytes,
+                                                   int stage_bytes)
+{
+    extern __shared__ __align__(128) unsigned char smem_tma[];
+    constexpr int K = KIND == KIND_ADVECT ? (HV ? 3 : 2) : 1;
+    typedef typename VecT<T, VEC>::type V;
+    T* sx = reinterpret_cast<T*>(smem_tma);
+    unsigned char* ring = smem_tma + halo_bytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ring + (size_t)TMA_NB * stage_bytes);
+    const int R = tp.R, nc = p.nc, vpn = p.T_tr / VEC;
+    const int b = blockIdx.x, tid = threadIdx.x;
+    const int r0 = __ldg(tp.rows + b), r1 = __ldg(tp.rows + b + 1);  // r0 is a multiple of 32
+    const int nslices = (min(tp.N32, (r1 + 31) & ~31) - r0) >> 5;
+    const int nstages = (nc + TMA_CS - 1) / TMA_CS;
+    const size_t op_bytes = (size_t)R * TMA_CS * 4 * sizeof(T);       // one operator's region of a stage
+    const size_t slice_w = (size_t)TMA_CS * 32 * 4 * sizeof(T);        // one slice in an operator region
+    const size_t slice_l = (size_t)TMA_CS * 32 * 4 * sizeof(unsigned short);
+    const T* wsrc[3] = {p.w0, p.w1, p.w2};
+
+    auto issue = [&](int j) {  // thread 0: copies of stage j into buffer j % TMA_NB
+        unsigned char* buf = ring + (size_t)(j % TMA_NB) * stage_bytes;
+        if (j >= TMA_NB) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the block's reads
+        const int c0 = j * TMA_CS, cs = min(TMA_CS, nc - c0);
+        const uint32_t bw = (uint32_t)(cs * 32 * 4 * sizeof(T)), bl = (uint32_t)(cs * 32 * 4 * sizeof(unsigned short));
+        mbar_arrive_expect_tx(&bars[j % TMA_NB], (uint32_t)nslices * (K * bw + bl));
+        for (int q = 0; q < nslices; q++) {
+            const size_t off = sell_off(r0 + 32 * q, c0, nc);
+            for (int k = 0; k < K; k++) bulk_load(buf + k * op_bytes + q * slice_w, wsrc[k] + off, bw, &bars[j % TMA_NB]);
+            bulk_load(buf + K * op_bytes + q * slice_l, tp.lidx + off, bl, &bars[j % TMA_NB]);
+        }
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < TMA_NB; s++) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int j = 0; j < min(TMA_NB, nstages); j++) issue(j);
+    // stage the halo's node values while the first copies are in flight
+    const int h0 = __ldg(tp.ptr + b), hn = __ldg(tp.ptr + b + 1) - h0;
+    for (int e = tid; e < hn * vpn; e += blockDim.x) {
+        const int h = e / vpn, v = e - h * vpn;
+        const int node = __ldg(tp.nodes + h0 + h);
+        reinterpret_cast<V*>(sx)[(size_t)h * vpn + v] = __ldg(reinterpret_cast<const V*>(p.x + (size_t)node * p.T_tr) + v);
+    }
+    __syncthreads();
+
+    const int rl = tid / vpn, tv = tid - rl * vpn;
+    const int i = r0 + rl;
+    const bool active = i < r1;
+    const int q = rl >> 5, l = rl & 31;
+    T d0[VEC], d1[VEC], d2[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; v++) d0[v] = d1[v] = d2[v] = T(0);
+    for (int j = 0; j < nstages; j++) {
+        const int s = j % TMA_NB;
+        const bool ok = mbar_wait_bounded(&bars[s], (uint32_t)((j / TMA_NB) & 1), TMA_WAIT_LIMIT);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicExch(status, DEV_STATUS_WAIT_TIMEOUT);
+                for (int jj = j; jj < min(j + TMA_NB, nstages); jj++)
+                    mbar_wait_bounded(&bars[jj % TMA_NB], (uint32_t)((jj / TMA_NB) & 1), TMA_WAIT_LIMIT);
+            }
+            return;
+        }
+        const unsigned char* buf = ring + (size_t)s * stage_bytes;
+        const int cs = min(TMA_CS, nc - j * TMA_CS);
+        if (active) {
+            for (int cc = 0; cc < cs; cc++) {
+                const size_t cell = ((size_t)q * TMA_CS + cc) * 32 + l;  // this row's chunk in a region
+                const ushort4 l4 = reinterpret_cast<const ushort4*>(buf + K * op_bytes)[cell];
+                const int ll[4] = {l4.x, l4.y, l4.z, l4.w};
+                T wa[4], wb[4], wc[4];
+                ld_w4_shared(reinterpret_cast<const T*>(buf) + cell * 4, wa);
+                if (KIND == KIND_ADVECT) {
+                    ld_w4_shared(reinterpret_cast<const T*>(buf + op_bytes) + cell * 4, wb);
+                    if (HV) ld_w4_shared(reinterpret_cast<const T*>(buf + 2 * op_bytes) + cell * 4, wc);
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    T xj[VEC];
+                    const V t = reinterpret_cast<const V*>(sx)[(size_t)ll[k] * vpn + tv];
+                    memcpy(xj, &t, sizeof(V));
+#pragma unroll
+                    for (int v = 0; v < VEC; v++) {
+                        d0[v] = Ar<T>::fma(wa[k], xj[v], d0[v]);
+                        if (KIND == KIND_ADVECT) {
+                            d1[v] = Ar<T>::fma(wb[k], xj[v], d1[v]);
+                            if (HV) d2[v] = Ar<T>::fma(wc[k], xj[v], d2[v]);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();  // buffer s is free again
+        if (tid == 0 && j + TMA_NB < nstages) issue(j + TMA_NB);
+    }
+    if (!active) return;
+    T cu = T(0), cv = T(0);
+    if (KIND == KIND_ADVECT) {
+        cu = p.cu[i];
+        cv = p.cv[i];
+    }
+#pragma unroll
+    for (int v = 0; v < VEC; v++)
+        stage_update<T, KIND, HV>(p, i, (size_t)i * p.T_tr + (size_t)tv * VEC + v, d0[v], d1[v], d2[v], cu, cv);
+}
+
 // Unfused right-hand side + stage update from per-operator outputs (the plain path).
 template <typename T, int KIND, bool HV>
 __global__ void k_rhs_axpy(StageParams<T> p, const T* __restrict__ d0, const T* __restrict__ d1, const T* __restrict__ d2)
@@ -284,9 +501,98 @@ static StageParams<T> make_params(rbffd_pde* P, int stage, double dt)
     return p;
 }
 
+// Tiled launch geometry for a shape, or false if the tiled kernel cannot run it.
+struct TileGeom {
+    const Halo* h = nullptr;
+    int vec = 1, vpn = 1, G = 1, threads = 0;
+    int tma = 0, halo_bytes = 0, stage_bytes = 0;
+    size_t smem = 0;
+};
+
+static bool tile_geom(rbffd_pde* P, Shape sh, TileGeom* tg)
+{
+    if (sh.tile <= 0) return false;
+    auto it = P->g->halos.find(sh.tile);
+    if (it == P->g->halos.end()) return false;
+    const int es = P->dtype == RBFFD_F64 ? 8 : 4;
+    const int V = P->dtype == RBFFD_F64 ? 2 : 4;
+    TileGeom t;
+    t.h = it->second;
+    if (P->T == 1)
+        t.vec = 1;
+    else if (P->T % V == 0)
+        t.vec = V;
+    else
+        return false;
+    t.vpn = P->T / t.vec;
+    t.G = sh.lanes > 0 ? sh.lanes : 1;
+    if (t.G != 1 && t.G != 2 && t.G != 4) return false;
+    const int L = t.vpn * t.G;
+    if (L > 32 || (L & (L - 1))) return false;
+    t.threads = sh.tile * L;
+    if (t.threads > 1024) return false;
+    t.smem = (size_t)t.h->max_halo * P->T * es;
+    if (sh.tma) {
+        if (t.G != 1) return false;
+        const int K = P->kind == KIND_HEAT ? 1 : (P->use_hv ? 3 : 2);
+        t.tma = 1;
+        t.halo_bytes = round_up((int)t.smem, 128);
+        t.stage_bytes = round_up(K * sh.tile * TMA_CS * 4 * es + sh.tile * TMA_CS * 4 * 2, 128);
+        t.smem = (size_t)t.halo_bytes + (size_t)TMA_NB * t.stage_bytes + TMA_NB * sizeof(uint64_t);
+    }
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->ctx->device);
+    if (t.smem > (size_t)optin) return false;
+    *tg = t;
+    return true;
+}
+
+template <typename T, int VEC, int KIND, bool HV>
+static void launch_tile_v(const StageParams<T>& p, const TileParams& tp, const TileGeom& t, cudaStream_t s)
+{
+    const int nb = t.h->nblocks;
+    switch (t.G) {
+    case 1:
+        cudaFuncSetAttribute(k_stage_tile<T, VEC, 1, KIND, HV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem);
+        k_stage_tile<T, VEC, 1, KIND, HV><<<nb, t.threads, t.smem, s>>>(p, tp);
+        break;
+    case 2:
+        cudaFuncSetAttribute(k_stage_tile<T, VEC, 2, KIND, HV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem);
+        k_stage_tile<T, VEC, 2, KIND, HV><<<nb, t.threads, t.smem, s>>>(p, tp);
+        break;
+    default:
+        cudaFuncSetAttribute(k_stage_tile<T, VEC, 4, KIND, HV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem);
+        k_stage_tile<T, VEC, 4, KIND, HV><<<nb, t.threads, t.smem, s>>>(p, tp);
+        break;
+    }
+}
+
+template <typename T, int VEC, int KIND, bool HV>
+static void launch_tma_v(const StageParams<T>& p, const TileParams& tp, const TileGeom& t, int* status, cudaStream_t s)
+{
+    cudaFuncSetAttribute(k_stage_tma<T, VEC, KIND, HV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem);
+    k_stage_tma<T, VEC, KIND, HV><<<t.h->nblocks, t.threads, t.smem, s>>>(p, tp, status, t.halo_bytes, t.stage_bytes);
+}
+
 template <typename T, int KIND, bool HV>
 static void launch_stage_t(rbffd_pde* P, const StageParams<T>& p, Shape sh, cudaStream_t s)
 {
+    TileGeom tg;
+    if (tile_geom(P, sh, &tg)) {
+        TileParams tp{tg.h->d_ptr, tg.h->d_nodes, tg.h->d_lidx, tg.h->d_rows, tg.h->R, P->g->N32};
+        constexpr int VV = std::is_same<T, float>::value ? 4 : 2;
+        if (tg.tma) {
+            if (tg.vec == 1)
+                launch_tma_v<T, 1, KIND, HV>(p, tp, tg, P->ctx->d_status, s);
+            else
+                launch_tma_v<T, VV, KIND, HV>(p, tp, tg, P->ctx->d_status, s);
+        } else if (tg.vec == 1) {
+            launch_tile_v<T, 1, KIND, HV>(p, tp, tg, s);
+        } else {
+            launch_tile_v<T, VV, KIND, HV>(p, tp, tg, s);
+        }
+        return;
+    }
     int B = sh.block > 0 ? sh.block : 256;
     if (P->T == 1) {
         int G = sh.lanes > 0 ? sh.lanes : 1;
@@ -375,23 +681,59 @@ static Shape autotune(rbffd_pde* P)
     } else {
         for (int B : blocks) cands.push_back(Shape{0, B});
     }
+    // tiled candidates: halo staged in shared memory, R rows per block
+    const int rows_per_block[3] = {64, 128, 256};
+    for (int R : rows_per_block) {
+        const Halo* h = nullptr;
+        if (grid_halo(P->g, R, &h) != RBFFD_OK) continue;
+        for (int G : {1, 2, 4}) {
+            Shape c{G, 0, R, 0};
+            TileGeom tg;
+            if (tile_geom(P, c, &tg)) cands.push_back(c);
+        }
+        Shape c{1, 0, R, 1};  // weights and indices streamed by bulk copies
+        TileGeom tg;
+        if (tile_geom(P, c, &tg)) cands.push_back(c);
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     Shape best = cands[0];
     float best_ms = 1e30f;
+    // Each candidate: 20 back-to-back stage launches captured in a CUDA graph (as
+    // the solver replays them), one warm replay, then the faster of two timed replays.
+    const bool log = getenv("RBFFD_TUNE_LOG") != nullptr;
+    const int reps = 20;
     for (const Shape& c : cands) {
-        for (int w = 0; w < 2; w++) launch_stage_any(P, 0, 0.0, c, ctx->stream);
-        cudaEventRecord(e0, ctx->stream);
-        const int reps = 5;
-        for (int r = 0; r < reps; r++) launch_stage_any(P, 0, 0.0, c, ctx->stream);
-        cudaEventRecord(e1, ctx->stream);
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             cudaGetLastError();
             continue;
         }
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
+        for (int r = 0; r < reps; r++) launch_stage_any(P, 0, 0.0, c, ctx->stream);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        float ms = 1e30f;
+        for (int trial = 0; e == cudaSuccess && trial < 3; trial++) {
+            cudaEventRecord(e0, ctx->stream);
+            e = cudaGraphLaunch(exec, ctx->stream);
+            cudaEventRecord(e1, ctx->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float t = 0;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (trial > 0) ms = std::min(ms, t);  // trial 0 warms caches and clocks
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (log)
+            fprintf(stderr, "[rbffd tune] kind=%d hv=%d dtype=%d T=%d N=%d n_pad=%d lanes=%d block=%d tile=%d tma=%d: %.2f us\n",
+                    P->kind, P->use_hv, P->dtype, P->T, P->g->N, P->g->n_pad, c.lanes, c.block, c.tile, c.tma,
+                    1e3f * ms / reps);
         if (ms < best_ms) {
             best_ms = ms;
             best = c;
@@ -507,8 +849,10 @@ extern "C" int rbffd_pde_create(rbffd_grid* g, const rbffd_pde_params* prm, rbff
                 cv[i] = vel_v / a;
             }
         } else {
-            memcpy(cu.data(), prm->cu, N * sizeof(double));
-            memcpy(cv.data(), prm->cv, N * sizeof(double));
+            for (int i = 0; i < N; i++) {  // caller's node order -> internal row order
+                cu[i] = prm->cu[g->h_perm[i]];
+                cv[i] = prm->cv[g->h_perm[i]];
+            }
         }
         if ((rc = dev_alloc(ctx, &P->cu, N * es)) || (rc = dev_alloc(ctx, &P->cv, N * es))) {
             pde_free(P);
@@ -576,12 +920,16 @@ extern "C" int rbffd_pde_set_state(rbffd_pde* P, const double* u)
     cudaSetDevice(ctx->device);
     size_t n = (size_t)P->g->N * P->T;
     cudaStream_t s = ctx->stream;
+    // the stage buffers xa/xb are free between steps and serve as staging
+    int rc;
     if (P->dtype == RBFFD_F64) {
-        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(P->u, u, n * 8, cudaMemcpyHostToDevice, s));
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(P->xa, u, n * 8, cudaMemcpyHostToDevice, s));
+        if ((rc = grid_to_internal(P->g, P->xa, P->u, P->T, 8, s))) return rc;
     } else {
         RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(P->stage64, u, n * 8, cudaMemcpyHostToDevice, s));
-        k_to_dtype_f<<<(int)((n + 255) / 256), 256, 0, s>>>(P->stage64, (float*)P->u, n);
+        k_to_dtype_f<<<(int)((n + 255) / 256), 256, 0, s>>>(P->stage64, (float*)P->xb, n);
         RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+        if ((rc = grid_to_internal(P->g, P->xb, P->u, P->T, 4, s))) return rc;
     }
     RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     return RBFFD_OK;
@@ -594,10 +942,13 @@ extern "C" int rbffd_pde_get_state(rbffd_pde* P, double* u)
     cudaSetDevice(ctx->device);
     size_t n = (size_t)P->g->N * P->T;
     cudaStream_t s = ctx->stream;
+    int rc;
     if (P->dtype == RBFFD_F64) {
-        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(u, P->u, n * 8, cudaMemcpyDeviceToHost, s));
+        if ((rc = grid_to_caller(P->g, P->u, P->xa, P->T, 8, s))) return rc;
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(u, P->xa, n * 8, cudaMemcpyDeviceToHost, s));
     } else {
-        k_from_f<<<(int)((n + 255) / 256), 256, 0, s>>>((const float*)P->u, P->stage64, n);
+        if ((rc = grid_to_caller(P->g, P->u, P->xb, P->T, 4, s))) return rc;
+        k_from_f<<<(int)((n + 255) / 256), 256, 0, s>>>((const float*)P->xb, P->stage64, n);
         RBFFD_CUDA_TRY(ctx, cudaGetLastError());
         RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(u, P->stage64, n * 8, cudaMemcpyDeviceToHost, s));
     }
@@ -630,7 +981,7 @@ extern "C" int rbffd_pde_set_shape(rbffd_pde* P, int lanes, int block)
     if (!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16)) return RBFFD_ERR_INVALID;
     if (!(block == 0 || block == 64 || block == 128 || block == 256 || block == 512)) return RBFFD_ERR_INVALID;
     if (P->T > 1 && lanes > 1) return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "lanes per row apply to one tracer only");
-    P->shape = Shape{lanes ? lanes : 1, block ? block : 256};
+    P->shape = Shape{lanes ? lanes : 1, block ? block : 256, 0};
     P->forced = true;
     return RBFFD_OK;
 }
@@ -640,6 +991,34 @@ extern "C" int rbffd_pde_get_shape(rbffd_pde* P, int* lanes, int* block)
     if (!P || !lanes || !block) return RBFFD_ERR_INVALID;
     *lanes = P->shape.lanes;
     *block = P->shape.block;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_set_tiled_shape(rbffd_pde* P, int rows_per_block, int lanes, int stream_weights)
+{
+    if (!P) return RBFFD_ERR_INVALID;
+    if (rows_per_block < 32 || rows_per_block > 1024 || rows_per_block % 32 || !(lanes == 1 || lanes == 2 || lanes == 4))
+        return set_error(P->ctx, RBFFD_ERR_INVALID, "rows_per_block must be a multiple of 32, lanes 1, 2 or 4");
+    if (stream_weights && lanes != 1)
+        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights use one lane per row");
+    cudaSetDevice(P->ctx->device);
+    const Halo* h = nullptr;
+    int rc = grid_halo(P->g, rows_per_block, &h);
+    if (rc) return rc;
+    Shape c{lanes, 0, rows_per_block, stream_weights ? 1 : 0};
+    TileGeom tg;
+    if (!tile_geom(P, c, &tg))
+        return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "tiled shape (%d rows, %d lanes) does not fit this PDE",
+                         rows_per_block, lanes);
+    P->shape = c;
+    P->forced = true;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_get_tiling(rbffd_pde* P, int* rows_per_block)
+{
+    if (!P || !rows_per_block) return RBFFD_ERR_INVALID;
+    *rows_per_block = P->shape.tile;
     return RBFFD_OK;
 }
 
@@ -678,14 +1057,19 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
         }
         return RBFFD_OK;
     }
-    if (!P->forced && P->shape.block == 0) P->shape = autotune(P);
+    if (!P->forced && P->shape.block == 0 && P->shape.tile == 0) P->shape = autotune(P);
     Shape sh = P->shape;
+    if (sh.tile > 0) {  // the halo must exist before any capture (building it copies to the device)
+        const Halo* h = nullptr;
+        int rc = grid_halo(P->g, sh.tile, &h);
+        if (rc) return rc;
+    }
     if (flags & RBFFD_ADVANCE_GRAPH) {
         const int chunk = 25;
         int full = nsteps / chunk, rest = nsteps % chunk;
         if (full > 0) {
             if (!P->gexec || P->g_dt != dt || P->g_steps != chunk || P->g_shape.lanes != sh.lanes ||
-                P->g_shape.block != sh.block) {
+                P->g_shape.block != sh.block || P->g_shape.tile != sh.tile || P->g_shape.tma != sh.tma) {
                 if (P->gexec) {
                     cudaGraphExecDestroy(P->gexec);
                     P->gexec = nullptr;
@@ -713,7 +1097,10 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
     }
     RBFFD_CUDA_TRY(ctx, cudaGetLastError());
     P->t += dt * nsteps;
-    if (!(flags & RBFFD_ADVANCE_ASYNC)) RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    if (!(flags & RBFFD_ADVANCE_ASYNC)) {
+        RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+        if (sh.tma) return ctx_check_device_status(ctx);
+    }
     return RBFFD_OK;
 }
 
@@ -725,18 +1112,19 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
 // cudaMalloc inside the library would fail or fragment that pool, and callers
 // on latency-critical paths, where cudaMalloc/cudaFree may synchronise the
 // device.  rbffd_heat_rk4_noalloc serves them: the caller passes the state
-// vector in its own device memory and the three stage buffers RK4 needs live
-// in the file-scope array below, reserved when this library's device code is
-// loaded on a GPU and held until the process exits.
+// vector in its own device memory; the copy of the state in the grid's
+// internal node order and the three stage buffers RK4 needs live in the
+// file-scope array below, reserved when this library's device code is loaded
+// on a GPU and held until the process exits.
 //
 // Limits and sharing: NOALLOC_MAX_NODES nodes in FP64 (twice that in FP32);
 // larger grids are rejected.  Every call on a device uses the same array, so
 // calls that overlap on that GPU (other streams, other threads, other
-// contexts of this process) overwrite each other's stage buffers: serialise
-// them.  Stage 0 writes every scratch element a later stage reads, so the
-// array needs no clearing between calls.
+// contexts of this process) overwrite each other's buffers: serialise them.
+// Each call first writes the whole state copy, and stage 0 writes every stage
+// element a later stage reads, so the array needs no clearing between calls.
 constexpr int NOALLOC_MAX_NODES = 262144;
-static __device__ __align__(256) double g_noalloc_scratch[3 * NOALLOC_MAX_NODES];  // 6 MiB per GPU
+static __device__ __align__(256) double g_noalloc_scratch[4 * NOALLOC_MAX_NODES];  // 8 MiB per GPU
 
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_ptr[128];  // device address of g_noalloc_scratch, per device ordinal
@@ -757,6 +1145,7 @@ static int noalloc_scratch(rbffd_ctx* ctx, void** out)
     return RBFFD_OK;
 }
 
+// u: the state in the grid's internal order (a region of the scratch array)
 template <typename T>
 static void noalloc_steps(rbffd_grid* g, const T* w, T* u, T* scratch, T kappa, double dt, int nsteps, cudaStream_t s)
 {
@@ -807,11 +1196,16 @@ extern "C" int rbffd_heat_rk4_noalloc(rbffd_grid* g, int dtype, double kappa, do
     void* scratch = nullptr;
     int rc = noalloc_scratch(ctx, &scratch);
     if (rc) return rc;
+    // scratch layout (elements of dtype): [xa | xb | acc | state in internal order], N each
+    const int es = dtype == RBFFD_F64 ? 8 : 4;
+    void* u_int = (char*)scratch + 3 * (size_t)g->N * es;
+    if ((rc = grid_to_internal(g, u_dev, u_int, 1, es, ctx->stream))) return rc;
     if (dtype == RBFFD_F64)
-        noalloc_steps<double>(g, (const double*)w, (double*)u_dev, (double*)scratch, kappa, dt, nsteps, ctx->stream);
+        noalloc_steps<double>(g, (const double*)w, (double*)u_int, (double*)scratch, kappa, dt, nsteps, ctx->stream);
     else
-        noalloc_steps<float>(g, (const float*)w, (float*)u_dev, (float*)scratch, (float)kappa, dt, nsteps, ctx->stream);
+        noalloc_steps<float>(g, (const float*)w, (float*)u_int, (float*)scratch, (float)kappa, dt, nsteps, ctx->stream);
     RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    if ((rc = grid_to_caller(g, u_int, u_dev, 1, es, ctx->stream))) return rc;
     RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return RBFFD_OK;
 }

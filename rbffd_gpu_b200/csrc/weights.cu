@@ -622,7 +622,7 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
         for (int i = 0; i < N; i++) {
             if (deg_per_row[i] < -1 || deg_per_row[i] > 4)
                 return set_error(ctx, RBFFD_ERR_INVALID, "deg_per_row[%d] = %d outside [-1, 4]", i, deg_per_row[i]);
-            deg[i] = deg_per_row[i];
+            deg[g->h_iperm[i]] = deg_per_row[i];  // internal row order
         }
     // buckets by system size m
     std::map<int, std::vector<int>> buckets;
@@ -665,7 +665,14 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
     cudaError_t e = cudaMemcpyAsync(d_rows, rows.data(), b_rows, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_deg, deg.data(), b_rows, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_status, &status0, sizeof(int), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && eps) e = cudaMemcpyAsync(d_eps, eps, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
+    std::vector<double> eps_int;
+    if (eps) {
+        eps_int.resize(N);
+        for (int i = 0; i < N; i++) eps_int[i] = eps[g->h_perm[i]];  // internal row order
+    }
+    if (e == cudaSuccess && eps)
+        e = cudaMemcpyAsync(d_eps, eps_int.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // host vectors above go out of scope after this block
     if (e != cudaSuccess) {
         cleanup();
         return cuda_error(ctx, e, "rbffd_weights_compute upload");
@@ -749,7 +756,8 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
     cleanup();
     if (e != cudaSuccess) return cuda_error(ctx, e, "rbffd_weights_compute");
     if (status != INT_MAX)
-        return set_error(ctx, RBFFD_ERR_SINGULAR, "stencil %d: zero pivot in the weight system", status - 1);
+        return set_error(ctx, RBFFD_ERR_SINGULAR, "stencil %d: zero pivot in the weight system",
+                         g->h_perm[status - 1]);
     for (int c = 0; c < K; c++)
         if ((rc = grid_make_f32(g, der_index(P.opbit[c])))) return rc;
     RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
@@ -801,12 +809,19 @@ extern "C" int rbffd_weights_assemble(rbffd_grid* g, const rbffd_weight_params* 
             P.opbit[K++] = 1u << b;
         }
     int N = g->N, m = -1;
-    std::vector<int> deg(N, prm->poly_deg);
+    // internal row order for degrees, epsilons and the requested rows
+    std::vector<int> deg(N, prm->poly_deg), rows_int(count);
+    std::vector<double> eps_int;
     if (deg_per_row)
-        for (int i = 0; i < N; i++) deg[i] = deg_per_row[i];
+        for (int i = 0; i < N; i++) deg[g->h_iperm[i]] = deg_per_row[i];
+    if (eps) {
+        eps_int.resize(N);
+        for (int i = 0; i < N; i++) eps_int[i] = eps[g->h_perm[i]];
+    }
     for (int t = 0; t < count; t++) {
         if (rows[t] < 0 || rows[t] >= N) return set_error(ctx, RBFFD_ERR_INVALID, "row %d out of range", rows[t]);
-        int mt = g->h_len[rows[t]] + poly_size(deg[rows[t]]);
+        rows_int[t] = g->h_iperm[rows[t]];
+        int mt = g->h_len[rows_int[t]] + poly_size(deg[rows_int[t]]);
         if (m >= 0 && mt != m) return set_error(ctx, RBFFD_ERR_INVALID, "rows of one call must share the system size");
         m = mt;
     }
@@ -831,9 +846,10 @@ extern "C" int rbffd_weights_assemble(rbffd_grid* g, const rbffd_weight_params* 
         cleanup();
         return rc;
     }
-    cudaError_t e = cudaMemcpyAsync(d_rows, rows, count * sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaMemcpyAsync(d_rows, rows_int.data(), count * sizeof(int), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_deg, deg.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && eps) e = cudaMemcpyAsync(d_eps, eps, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && eps)
+        e = cudaMemcpyAsync(d_eps, eps_int.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
     P.xyz = g->d_xyz;
     P.idx = g->d_idx;
     P.len = g->d_len;

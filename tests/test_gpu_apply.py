@@ -81,6 +81,24 @@ def test_apply_ragged_stencils(ctx):
     grid.close()
 
 
+@pytest.mark.parametrize("dtype", [R.F64, R.F32])
+def test_apply_dev_multi_tracer_caller_order(setup, dtype):
+    """Device-pointer apply on [N][T] data in the caller's node order."""
+    torch = pytest.importorskip("torch")
+    T = 3
+    u = np.stack([setup["u"], np.cos(setup["u"]), setup["u"] ** 2], axis=1)
+    tdt = torch.float64 if dtype == R.F64 else torch.float32
+    du = torch.tensor(u, dtype=tdt, device="cuda")
+    out = torch.zeros_like(du)
+    setup["der"].applyWeightsForDerivDev(O.LSFC, du.data_ptr(), out.data_ptr(), dtype=dtype, ntracers=T)
+    ref = O.apply(setup["st"], None, setup["W"][O.LSFC], u)
+    got = out.double().cpu().numpy()
+    if dtype == R.F64:
+        assert np.array_equal(got, ref)
+    else:
+        assert rel_l2(got, ref) < 5e-5
+
+
 def test_grid_rejects_bad_stencils(ctx):
     xyz, st = sphere_problem(2562, 17, 5)
     bad = st.copy()

@@ -74,6 +74,39 @@ def test_cosine_bell_fp64_split_rows(bell, lanes):
     assert rel_l2(out, _oracle_bell(bell, 10)) < 1e-12
 
 
+def _gpu_bell_tiled(b, steps, rows, lanes, dtype=R.F64, stream=False):
+    p = b["p"]
+    pde = R.CosineBell(b["grid"], b["der"], p["a"], p["alpha"], p["T"], True, dtype=dtype)
+    pde.setTiledShape(rows, lanes, stream)
+    assert pde.getShape()[2] == rows
+    pde.fillInitialConditions(b["h0"])
+    pde.advance(R.RK4, p["dt"], steps, graph=True)
+    out = pde.getLocalSolution()
+    pde.close()
+    return out
+
+
+@pytest.mark.parametrize("rows", [32, 64, 128, 256])
+def test_cosine_bell_tiled_fp64_bit_exact(bell, rows):
+    """Halo staged in shared memory, one lane per row: same arithmetic as the oracle."""
+    assert np.array_equal(_gpu_bell_tiled(bell, 10, rows, 1), _oracle_bell(bell, 10))
+
+
+@pytest.mark.parametrize("rows", [32, 64, 128])
+def test_cosine_bell_streamed_weights_fp64_bit_exact(bell, rows):
+    """Weights and indices streamed into shared memory by bulk copies (TMA)."""
+    assert np.array_equal(_gpu_bell_tiled(bell, 10, rows, 1, stream=True), _oracle_bell(bell, 10))
+
+
+def test_cosine_bell_streamed_weights_fp32(bell):
+    assert rel_l2(_gpu_bell_tiled(bell, 10, 128, 1, dtype=R.F32, stream=True), _oracle_bell(bell, 10)) < 1e-5
+
+
+@pytest.mark.parametrize("rows,lanes", [(64, 2), (128, 4)])
+def test_cosine_bell_tiled_split_rows(bell, rows, lanes):
+    assert rel_l2(_gpu_bell_tiled(bell, 10, rows, lanes), _oracle_bell(bell, 10)) < 1e-12
+
+
 def test_graph_and_unfused_paths_bit_exact(bell):
     ref, _ = _gpu_bell(bell, 60)
     g, _ = _gpu_bell(bell, 60, graph=True)
@@ -128,8 +161,10 @@ def test_heat_fp32_tolerance_and_exact_decay(heat):
     assert rel_l2(ref, ex) < 1e-3
 
 
-@pytest.mark.parametrize("dtype,tol", [(R.F64, 0.0), (R.F32, 1e-5)])
-def test_multi_tracer_advection(bell, dtype, tol):
+@pytest.mark.parametrize("dtype,tol,tiled", [(R.F64, 0.0, None), (R.F32, 1e-5, None), (R.F64, 0.0, (64, 1)),
+                                             (R.F64, 1e-12, (32, 4)), (R.F32, 1e-5, (128, 2)),
+                                             (R.F64, 0.0, (64, 1, True)), (R.F32, 1e-5, (128, 1, True))])
+def test_multi_tracer_advection(bell, dtype, tol, tiled):
     T = 16
     rng = np.random.default_rng(4)
     xyz = bell["xyz"]
@@ -140,6 +175,10 @@ def test_multi_tracer_advection(bell, dtype, tol):
     ref = O.rk4_advect(bell["st"], None, bell["W"][O.LAMBDA], bell["W"][O.THETA], bell["W"][O.HV], bell["cu"],
                        bell["cv"], u0, dt, steps)
     pde = R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=dtype, ntracers=T)
+    if tiled:
+        pde.setTiledShape(*tiled)
+    elif tol == 0.0:
+        pde.setShape(1, 256)  # one lane per (row, tracer group): the oracle's summation order
     pde.fillInitialConditions(u0)
     pde.advance(R.RK4, dt, steps, graph=True)
     out = pde.getLocalSolution()
