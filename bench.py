@@ -364,6 +364,7 @@ def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
     p64.close()
     pplain.close()
     out["multitracer"] = bench_multitracer(R, torch, ctx)
+    out["serving"] = bench_serving(R, torch, ctx)
     return out
 
 
@@ -427,6 +428,165 @@ def bench_multitracer(R, torch, ctx):
     out["rel_l2_fp64_vs_exact"] = float(np.linalg.norm(u64 - exact) / np.linalg.norm(exact))
     grid.close()
     return out
+
+
+SERVING = dict(name="serving_poisson200_first128_of_4096", requests=128, stream=4096, rate=200.0, seed=5,
+               sizes=(2562, 10242, 40962, 163842, 655362), stencils=(31, 50, 101), steps=(100, 2000),
+               heat_deg={31: 2, 50: 3, 101: 4}, hbm_fraction=0.8)
+
+
+def serving_stream(C):
+    """The seeded request stream: Poisson arrivals at C['rate']/s; heat or
+    advection 50/50; N uniform over the icosahedral sizes (log-uniform in N);
+    n uniform over the stencil sizes; steps uniform in [100, 2000].  The whole
+    4096-request stream is drawn so the sample is its prefix."""
+    rng = np.random.default_rng(C["seed"])
+    m = C["stream"]
+    t = np.cumsum(rng.exponential(1.0 / C["rate"], m))
+    kind = rng.integers(0, 2, m)
+    N = rng.choice(C["sizes"], m)
+    n = rng.choice(C["stencils"], m)
+    steps = rng.integers(C["steps"][0], C["steps"][1] + 1, m)
+    return [dict(t=float(t[i]), heat=bool(kind[i]), N=int(N[i]), n=int(n[i]), steps=int(steps[i]))
+            for i in range(C["requests"])]
+
+
+def serving_grid(R, ctx, N, n, C):
+    """A cached (N, n) grid with the heat operator (LSFC) and the advection
+    operators (LAMBDA, THETA, Delta^4 HV) computed on the device in FP64."""
+    xyz = R.fibonacci_nodes(N, C["seed"])
+    st = R.knn_stencils(xyz, n)
+    grid = R.Grid(ctx, xyz, st)
+    h = np.sqrt(4 * np.pi / N)
+    dh = R.RBFFD(R.LSFC, grid, 2)
+    dh.setEpsilon(0.25 / h)
+    dh.setPolynomialDegree(C["heat_deg"][n])
+    dh.computeAllWeightsForAllStencils()
+    da = R.RBFFD(R.LAMBDA | R.THETA | R.HV, grid, 2)
+    da.setEpsilon(0.5 / h)
+    da.setHVScalars(4, 1e-3)
+    da.setPolynomialDegree(2)
+    da.computeAllWeightsForAllStencils()
+    return dict(grid=grid, xyz=xyz, heat=dh, adv=da)
+
+
+def bench_serving(R, torch, ctx):
+    """Continuous batching of a Poisson request stream through rbffd_server
+    (FP32), against plain one-request-at-a-time FP64 solves (the unfused path:
+    one SpMV launch per operator, separate RHS/RK4 launches, a host
+    synchronisation every step).  Weights are cached on the device per (N, n)
+    grid before the stream starts."""
+    C = SERVING
+    reqs = serving_stream(C)
+    bell = dict(a=1.0, alpha=np.pi / 2, T=1036800.0)
+    t0 = time.perf_counter()
+    grids = {}
+    for r in reqs:
+        key = (r["N"], r["n"])
+        if key not in grids:
+            grids[key] = serving_grid(R, ctx, r["N"], r["n"], C)
+    setup_s = time.perf_counter() - t0
+    rng = np.random.default_rng(C["seed"] + 1)
+    for k, r in enumerate(reqs):
+        g = grids[(r["N"], r["n"])]
+        if r["heat"]:
+            r["u0"] = R.exact_sph_heat(g["xyz"], 10, rng.standard_normal(121), 0.0)
+            r["dt"] = 1e-6 * 163842.0 / r["N"]  # fixed dt * spectral radius across sizes
+        else:
+            cen = rng.normal(size=3)
+            cen /= np.linalg.norm(cen)
+            r["u0"] = np.exp(-6.0 * ((g["xyz"] - cen) ** 2).sum(1))
+            r["dt"] = bell["T"] / 1000.0 * np.sqrt(4096.0 / r["N"])  # fixed CFL number across sizes
+    heat32 = R.heat_params(1.0, R.F32)
+    adv32 = R.cosine_bell_params(bell["a"], bell["alpha"], bell["T"], True, dtype=R.F32)
+    # warm-up: one short request per grid and kind (module load, slot buffers)
+    srv = R.Server(ctx, hbm_fraction=C["hbm_fraction"])
+    for key, g in grids.items():
+        for p in (heat32, adv32):
+            srv.submit(g["grid"], p, np.zeros(key[0]), 1e-9, 2)
+    srv.wait_idle(120)
+    s0 = srv.stats()
+    # ---- the stream: submit at the arrival times, wait for all results ----
+    ids = []
+    t_start = time.perf_counter()
+    for r in reqs:
+        delay = r["t"] - (time.perf_counter() - t_start)
+        if delay > 0:
+            time.sleep(delay)
+        g = grids[(r["N"], r["n"])]
+        ids.append(srv.submit(g["grid"], heat32 if r["heat"] else adv32, r["u0"], r["dt"], r["steps"]))
+    srv.wait_idle(900)
+    makespan = time.perf_counter() - t_start
+    s1 = srv.stats()
+    lat, queue, outs = [], [], []
+    for rid in ids:
+        done, status, l_s, q_s = srv.poll(rid)
+        assert done and status == 0, status
+        lat.append(l_s)
+        queue.append(q_s)
+    work = float(sum(r["N"] * r["steps"] for r in reqs))
+    # accuracy: served FP32 against plain FP64 of the same request, one request per (kind, grid) class
+    checked, errs = set(), []
+    # ---- plain FP64, one request at a time: measured per class, summed over the stream ----
+    plain_step_s = {}
+    for k, r in enumerate(reqs):
+        cls = (r["heat"], r["N"], r["n"])
+        g = grids[(r["N"], r["n"])]
+        if cls not in plain_step_s:
+            pde = (R.HeatSphere(g["grid"], g["heat"], 1.0, dtype=R.F64) if r["heat"] else
+                   R.CosineBell(g["grid"], g["adv"], bell["a"], bell["alpha"], bell["T"], True, dtype=R.F64))
+            pde.fillInitialConditions(r["u0"])
+            pde.advance(R.RK4, r["dt"], 2, unfused=True)
+            ctx.synchronize()
+            reps = 20
+            t = time.perf_counter()
+            pde.advance(R.RK4, r["dt"], reps, unfused=True)
+            ctx.synchronize()
+            plain_step_s[cls] = (time.perf_counter() - t) / reps
+            if len(checked) < 6 and r["steps"] <= 1200:
+                pde.fillInitialConditions(r["u0"])
+                pde.advance(R.RK4, r["dt"], r["steps"], graph=True)
+                ref = pde.getLocalSolution()
+                out = srv.result(ids[k])
+                errs.append(float(np.linalg.norm(out - ref) / np.linalg.norm(ref)))
+                checked.add(cls)
+            pde.close()
+    srv.stop()
+    # plain sequential service of the same arrivals (first come, first served)
+    t_free, plain_lat = 0.0, []
+    for r in reqs:
+        svc = r["steps"] * plain_step_s[(r["heat"], r["N"], r["n"])]
+        t_free = max(t_free, r["t"]) + svc
+        plain_lat.append(t_free - r["t"])
+    plain_busy = sum(r["steps"] * plain_step_s[(r["heat"], r["N"], r["n"])] for r in reqs)
+    for g in grids.values():
+        g["grid"].close()
+    served_rate = work / makespan
+    plain_rate = work / plain_busy
+    return {
+        "workload": C["name"],
+        "sample": "first %d requests of the seeded %d-request stream (%.2f s of arrivals)" % (
+            C["requests"], C["stream"], reqs[-1]["t"]),
+        "grids_cached": len(grids), "grid_setup_s": setup_s,
+        "served_fp32": {
+            "node_updates_per_s": served_rate, "makespan_s": makespan,
+            "gpu_busy_node_updates_per_s": (s1["node_updates"] - s0["node_updates"]) / (
+                s1["gpu_busy_s"] - s0["gpu_busy_s"]),
+            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+            "queue_p50_s": float(np.percentile(queue, 50)), "queue_p99_s": float(np.percentile(queue, 99)),
+            "max_active": s1["max_active_seen"], "batches": s1["ticks"] - s0["ticks"],
+            "launches": s1["launches"] - s0["launches"], "slots_reused": s1["slots_reused"] - s0["slots_reused"]},
+        "plain_fp64_sequential": {
+            "node_updates_per_s": plain_rate, "busy_s": plain_busy,
+            "latency_p50_s": float(np.percentile(plain_lat, 50)),
+            "latency_p99_s": float(np.percentile(plain_lat, 99)),
+            "method": "per-step time of the unfused FP64 path measured over 20 steps for each (kind, N, n) "
+                      "class of the sample; service times summed and queued first come, first served on "
+                      "the same arrival times"},
+        "served_over_plain": served_rate / plain_rate,
+        "rel_l2_served_fp32_vs_fp64_max": max(errs) if errs else None,
+        "accuracy_checked_requests": len(errs),
+    }
 
 
 def run_profile():

@@ -40,7 +40,8 @@ enum rbffd_status {
     RBFFD_ERR_STATE = -6,       /* call out of order (e.g. weights missing) */
     RBFFD_ERR_SINGULAR = -7,    /* a stencil system had an exactly zero pivot */
     RBFFD_ERR_BUDGET = -8,      /* admission refused: over the HBM budget */
-    RBFFD_ERR_NO_DEVICE = -9    /* no CUDA device / driver */
+    RBFFD_ERR_NO_DEVICE = -9,   /* no CUDA device / driver */
+    RBFFD_ERR_CANCELLED = -10   /* serving: the request was cancelled */
 };
 
 /* Arithmetic type of a kernel path. */
@@ -239,6 +240,70 @@ int rbffd_pde_get_shape(rbffd_pde* pde, int* lanes_per_row, int* block_threads);
  * get_tiling reports 0 when the stage kernel gathers from global memory. */
 int rbffd_pde_set_tiled_shape(rbffd_pde* pde, int rows_per_block, int lanes, int stream_weights);
 int rbffd_pde_get_tiling(rbffd_pde* pde, int* rows_per_block);
+
+/* ---- serving: persistent request loop with continuous batching --------- *
+ * No counterpart in the reference, whose drivers run one PDE per process
+ * (tests/experiments/cosine_bell_on_sphere/main.cpp:280-515).  A server owns
+ * one host thread that advances every admitted request by RK4 steps; each
+ * stage of a step is one launch over the rows of all active requests, so
+ * requests of different grids, stencil sizes and right-hand sides share the
+ * device.  Requests arriving while others run are admitted at the next step
+ * boundary, in arrival order, while the context's device memory plus the
+ * request's stays within hbm_fraction of the device's memory and fewer than
+ * max_active requests run.  Every row is computed by one thread in stencil
+ * order with the arithmetic of rbffd_pde_advance with one lane per row, so a
+ * request's result does not depend on what else is in the batch (FP64
+ * results equal the one-lane rbffd_pde_advance result bit for bit; FP32
+ * results equal the FP32 one-lane result). */
+typedef struct rbffd_server rbffd_server;
+
+typedef struct rbffd_request {
+    rbffd_grid* grid;     /* grid with the operators' weights on the device (kept by the caller) */
+    rbffd_pde_params pde; /* right-hand side and dtype; ntracers must be 1 */
+    const double* u0;     /* [N] initial state in the caller's node order, copied at submission */
+    double dt;            /* RK4 step */
+    int nsteps;           /* RK4 steps, >= 0 */
+    double* out;          /* [N] result, written before the request reports done; the caller
+                             keeps it valid until then (or until rbffd_server_cancel returns) */
+} rbffd_request;
+
+typedef struct rbffd_server_stats {
+    long long submitted, completed, failed, cancelled; /* completed: results written */
+    long long pending, active, max_active_seen;
+    long long ticks;        /* batches of steps issued */
+    long long launches;     /* stage-kernel launches */
+    long long slots_reused; /* admissions that reused a finished request's device buffers */
+    double node_updates;    /* sum over executed request steps of the request's N */
+    double gpu_busy_s;      /* device time of the issued batches (CUDA events) */
+    double budget_bytes, held_bytes;
+} rbffd_server_stats;
+
+/* Start the loop on ctx's device.  hbm_fraction in (0, 1]; max_active <= 0
+ * means no slot limit. */
+int rbffd_server_start(rbffd_ctx* ctx, double hbm_fraction, int max_active, rbffd_server** out);
+/* Queue a request; *id identifies it.  Returns RBFFD_ERR_BUDGET when the
+ * request alone could never fit the budget, RBFFD_ERR_INVALID /
+ * RBFFD_ERR_STATE / RBFFD_ERR_UNSUPPORTED for a malformed request. */
+int rbffd_server_submit(rbffd_server* srv, const rbffd_request* req, uint64_t* id);
+/* done = 1 once the request has finished, failed or been cancelled; status is
+ * then its outcome (RBFFD_OK: out holds the result).  latency_s: submission to
+ * completion; queue_s: submission to admission (-1 while unknown). */
+int rbffd_server_poll(rbffd_server* srv, uint64_t id, int* done, int* status, double* latency_s, double* queue_s);
+/* Block until the request is done (returns its status) or timeout_s passes
+ * (RBFFD_ERR_TIMEOUT). */
+int rbffd_server_wait(rbffd_server* srv, uint64_t id, double timeout_s);
+/* Block until nothing is pending or active, or timeout_s passes. */
+int rbffd_server_wait_idle(rbffd_server* srv, double timeout_s);
+/* Cancel a pending or active request (an active one leaves at the next step
+ * boundary; out is not written afterwards).  Returns after it has left. */
+int rbffd_server_cancel(rbffd_server* srv, uint64_t id);
+int rbffd_server_get_stats(rbffd_server* srv, rbffd_server_stats* stats);
+/* Fault injection on the host: the next count admissions fail as if the
+ * device allocation had failed (status RBFFD_ERR_OOM). */
+int rbffd_server_inject_admission_failures(rbffd_server* srv, int count);
+/* Stop the loop: pending requests end with RBFFD_ERR_CANCELLED, active ones
+ * run to completion first; all device memory of the server is released. */
+int rbffd_server_stop(rbffd_server* srv);
 
 #ifdef __cplusplus
 }

@@ -28,6 +28,17 @@ class PdeParams(ctypes.Structure):
                 ("cu", dp), ("cv", dp)]
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("grid", c_void_p), ("pde", PdeParams), ("u0", dp), ("dt", c_double), ("nsteps", c_int),
+                ("out", dp)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_longlong) for k in ("submitted", "completed", "failed", "cancelled", "pending", "active",
+                                                 "max_active_seen", "ticks", "launches", "slots_reused")] + \
+               [(k, c_double) for k in ("node_updates", "gpu_busy_s", "budget_bytes", "held_bytes")]
+
+
 # name -> (restype, argtypes)
 PROTOTYPES = {
     "rbffd_version": (c_char_p, []),
@@ -65,6 +76,15 @@ PROTOTYPES = {
     "rbffd_pde_get_tiling": (c_int, [c_void_p, ip]),
     "rbffd_heat_rk4_noalloc": (c_int, [c_void_p, c_int, c_double, c_double, c_int, c_void_p]),
     "rbffd_pde_get_shape": (c_int, [c_void_p, ip, ip]),
+    "rbffd_server_start": (c_int, [c_void_p, c_double, c_int, P(c_void_p)]),
+    "rbffd_server_submit": (c_int, [c_void_p, P(Request), P(c_uint64)]),
+    "rbffd_server_poll": (c_int, [c_void_p, c_uint64, ip, ip, dp, dp]),
+    "rbffd_server_wait": (c_int, [c_void_p, c_uint64, c_double]),
+    "rbffd_server_wait_idle": (c_int, [c_void_p, c_double]),
+    "rbffd_server_cancel": (c_int, [c_void_p, c_uint64]),
+    "rbffd_server_get_stats": (c_int, [c_void_p, P(ServerStats)]),
+    "rbffd_server_inject_admission_failures": (c_int, [c_void_p, c_int]),
+    "rbffd_server_stop": (c_int, [c_void_p]),
 }
 
 _LIB = None

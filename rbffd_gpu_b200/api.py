@@ -355,3 +355,93 @@ class Advection(TimeDependentPDE):
         p = _lib.PdeParams(RHS_ADVECTION, ntracers, dtype, int(useHyperviscosity), 1.0, 0.0, 0.0, 1.0,
                            _dp(self._cu), _dp(self._cv))
         super().__init__(grid, der, p)
+
+
+# ---------------------------------------------------------------------------
+# serving
+
+ERR_OOM, ERR_TIMEOUT, ERR_BUDGET, ERR_CANCELLED = -2, -4, -8, -10
+
+
+def heat_params(kappa=1.0, dtype=F32):
+    """Right-hand side of a served heat request (u_t = kappa * LSFC u)."""
+    return _lib.PdeParams(RHS_HEAT, 1, dtype, 0, 1.0, 0.0, 0.0, kappa, None, None)
+
+
+def cosine_bell_params(earth_radius, velocity_angle, one_revolution_in_seconds, useHyperviscosity, dtype=F32):
+    """Right-hand side of a served solid-body advection request (CosineBell::solve)."""
+    u0 = (2.0 * np.pi * earth_radius) / one_revolution_in_seconds
+    return _lib.PdeParams(RHS_COSINE_BELL, 1, dtype, int(useHyperviscosity), earth_radius, velocity_angle, u0, 1.0,
+                          None, None)
+
+
+class Server:
+    """Persistent request loop with continuous batching (rbffd_server_*).
+
+    Requests (a grid with its weights, right-hand side parameters, an initial
+    state, dt and a step count) are admitted against an HBM budget and advanced
+    together, one launch per RK4 stage over all active requests."""
+
+    def __init__(self, ctx, hbm_fraction=0.8, max_active=0):
+        self.ctx, self.L = ctx, ctx.L
+        h = ctypes.c_void_p()
+        ctx.check(self.L.rbffd_server_start(ctx.h, hbm_fraction, max_active, ctypes.byref(h)), "rbffd_server_start")
+        self.h = h
+        self._out = {}
+
+    def submit(self, grid, params, u0, dt, nsteps, cu=None, cv=None):
+        """Queue a request; returns its id.  Raises RbffdError on a refused request."""
+        u = _f64(u0)
+        assert u.shape == (grid.N,)
+        out = np.zeros(grid.N)
+        keep = [u, out]
+        if cu is not None:
+            a, b = _f64(cu), _f64(cv)
+            keep += [a, b]
+            params = _lib.PdeParams(params.rhs_kind, params.ntracers, params.dtype, params.use_hv,
+                                    params.sphere_radius, params.alpha, params.u0, params.kappa, _dp(a), _dp(b))
+        req = _lib.Request(grid.h, params, _dp(u), dt, nsteps, _dp(out))
+        rid = ctypes.c_uint64()
+        self.ctx.check(self.L.rbffd_server_submit(self.h, ctypes.byref(req), ctypes.byref(rid)), "rbffd_server_submit")
+        self._out[rid.value] = out
+        return rid.value
+
+    def poll(self, rid):
+        """(done, status, latency_s, queue_s)."""
+        d, s = ctypes.c_int(), ctypes.c_int()
+        lat, q = ctypes.c_double(), ctypes.c_double()
+        self.ctx.check(self.L.rbffd_server_poll(self.h, rid, ctypes.byref(d), ctypes.byref(s), ctypes.byref(lat),
+                                                ctypes.byref(q)), "rbffd_server_poll")
+        return bool(d.value), s.value, lat.value, q.value
+
+    def wait(self, rid, timeout=600.0):
+        """Status of the request once it is done (ERR_TIMEOUT if timeout passes first)."""
+        return self.L.rbffd_server_wait(self.h, rid, timeout)
+
+    def result(self, rid):
+        """The request's result; raises unless it completed."""
+        done, st, _, _ = self.poll(rid)
+        if not done or st != 0:
+            raise RbffdError(st if done else -6, "request %d has no result" % rid)
+        return self._out[rid]
+
+    def wait_idle(self, timeout=600.0):
+        self.ctx.check(self.L.rbffd_server_wait_idle(self.h, timeout), "rbffd_server_wait_idle")
+
+    def cancel(self, rid):
+        self.ctx.check(self.L.rbffd_server_cancel(self.h, rid), "rbffd_server_cancel")
+
+    def inject_admission_failures(self, count):
+        self.ctx.check(self.L.rbffd_server_inject_admission_failures(self.h, count))
+
+    def stats(self):
+        s = _lib.ServerStats()
+        self.ctx.check(self.L.rbffd_server_get_stats(self.h, ctypes.byref(s)), "rbffd_server_get_stats")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def stop(self):
+        if getattr(self, "h", None):
+            self.ctx.check(self.L.rbffd_server_stop(self.h), "rbffd_server_stop")
+            self.h = None
+
+    close = stop

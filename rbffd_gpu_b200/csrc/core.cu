@@ -32,6 +32,7 @@ int set_error(rbffd_ctx* ctx, int status, const char* fmt, ...)
         va_start(ap, fmt);
         vsnprintf(buf, sizeof buf, fmt, ap);
         va_end(ap);
+        std::lock_guard<std::mutex> lk(ctx->err_mu);
         ctx->last_error = buf;
     }
     return status;
@@ -81,6 +82,7 @@ extern "C" const char* rbffd_status_string(int s)
     case RBFFD_ERR_SINGULAR: return "singular stencil system";
     case RBFFD_ERR_BUDGET: return "over device memory budget";
     case RBFFD_ERR_NO_DEVICE: return "no CUDA device";
+    case RBFFD_ERR_CANCELLED: return "request cancelled";
     }
     return "unknown status";
 }

@@ -68,6 +68,24 @@ __device__ __forceinline__ double fma_rn<double>(double a, double b, double c) {
 template <>
 __device__ __forceinline__ float fma_rn<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
+// Arithmetic with a fixed rounding sequence (no contraction or reassociation
+// by the compiler): every kernel that must reproduce another's result bit for
+// bit spells its operations through these.
+template <typename T>
+struct Ar;
+template <>
+struct Ar<double> {
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+};
+template <>
+struct Ar<float> {
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+};
+
 // Sum of G lanes' partial values (lanes of a group are consecutive in the warp).
 template <int G, typename T>
 __device__ __forceinline__ T group_sum(T v)

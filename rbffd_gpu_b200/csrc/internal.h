@@ -46,6 +46,7 @@ struct rbffd_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     std::string last_error;
+    std::mutex err_mu;  // last_error is also written by the serving loop's thread
     size_t held = 0;
     std::mutex mu;
     std::map<TuneKey, Shape> tuned;  // autotuner results per problem shape
@@ -95,7 +96,31 @@ struct Halo {
 };
 int grid_halo(rbffd_grid* g, int R, const Halo** out);
 
-struct rbffd_pde;  // defined in rk4.cu
+enum { KIND_ADVECT = 0, KIND_HEAT = 1 };
+
+// Device-resident state of one time-dependent PDE (rk4.cu); the serving loop
+// (server.cu) advances several of them in shared launches.
+struct rbffd_pde {
+    rbffd_grid* g = nullptr;
+    rbffd_ctx* ctx = nullptr;
+    int kind = 0, T = 1, dtype = RBFFD_F64, use_hv = 0;
+    int op[3] = {-1, -1, -1};
+    void *u = nullptr, *xa = nullptr, *xb = nullptr, *acc = nullptr;
+    void *cu = nullptr, *cv = nullptr;
+    void *d[3] = {nullptr, nullptr, nullptr};  // unfused path: one output per operator
+    double* stage64 = nullptr;                  // FP64 staging for host state copies of an FP32 PDE
+    double kappa = 1.0;
+    double t = 0.0;
+    Shape shape;
+    bool forced = false;
+    cudaGraphExec_t gexec = nullptr;
+    double g_dt = 0.0;
+    int g_steps = 0;
+    Shape g_shape;
+    size_t bytes = 0;
+};
+// Device bytes rbffd_pde_create allocates for these parameters on grid g.
+size_t pde_bytes(const rbffd_grid* g, const rbffd_pde_params* prm);
 
 // ---- error helpers --------------------------------------------------------
 int set_error(rbffd_ctx* ctx, int status, const char* fmt, ...);

@@ -34,46 +34,6 @@
 int grid_apply_dev(rbffd_grid* g, int op, int dtype, int T_tr, const void* u, void* out, int start, int count, int G,
                    cudaStream_t s);
 
-enum { KIND_ADVECT = 0, KIND_HEAT = 1 };
-
-struct rbffd_pde {
-    rbffd_grid* g = nullptr;
-    rbffd_ctx* ctx = nullptr;
-    int kind = 0, T = 1, dtype = RBFFD_F64, use_hv = 0;
-    int op[3] = {-1, -1, -1};
-    void *u = nullptr, *xa = nullptr, *xb = nullptr, *acc = nullptr;
-    void *cu = nullptr, *cv = nullptr;
-    void *d[3] = {nullptr, nullptr, nullptr};  // unfused path: one output per operator
-    double* stage64 = nullptr;                  // FP64 staging for host state copies of an FP32 PDE
-    double kappa = 1.0;
-    double t = 0.0;
-    Shape shape;
-    bool forced = false;
-    cudaGraphExec_t gexec = nullptr;
-    double g_dt = 0.0;
-    int g_steps = 0;
-    Shape g_shape;
-    size_t bytes = 0;
-};
-
-// ---------------------------------------------------------------------------
-// arithmetic with a fixed rounding sequence
-
-template <typename T>
-struct Ar;
-template <>
-struct Ar<double> {
-    static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
-    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
-    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
-};
-template <>
-struct Ar<float> {
-    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
-};
-
 template <typename T>
 struct StageParams {
     const int* __restrict__ idx;
@@ -748,6 +708,15 @@ static Shape autotune(rbffd_pde* P)
 
 // ---------------------------------------------------------------------------
 // C ABI
+
+size_t pde_bytes(const rbffd_grid* g, const rbffd_pde_params* prm)
+{
+    const size_t es = prm->dtype == RBFFD_F64 ? 8 : 4, nt = (size_t)g->N * (prm->ntracers > 0 ? prm->ntracers : 1);
+    size_t b = 4 * nt * es;                     // u, xa, xb, acc
+    if (prm->dtype == RBFFD_F32) b += nt * 8;  // FP64 staging
+    if (prm->rhs_kind != RBFFD_RHS_HEAT) b += 2 * (size_t)g->N * es;
+    return b;
+}
 
 static void pde_free(rbffd_pde* P)
 {

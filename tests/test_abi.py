@@ -109,3 +109,36 @@ def test_cosine_bell_exact_solution_shape():
     h = R.exact_cosine_bell(xyz)
     assert h.max() <= 1.0 and h.min() == 0.0
     assert 0.02 < (h > 0).mean() < 0.04  # cap of radius 1/3 covers (1-cos(1/3))/2 of the sphere
+
+
+def test_server_rejects_null_handles():
+    L = _lib.load()
+    assert L.rbffd_server_start(None, 0.8, 0, None) == -1
+    assert L.rbffd_server_submit(None, None, None) == -1
+    assert L.rbffd_server_stop(None) == -1
+    assert L.rbffd_server_cancel(None, 1) == -1
+    assert L.rbffd_server_wait_idle(None, 1.0) == -1
+
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """The Python binding's structs have the C compiler's sizes and offsets."""
+    structs = {"rbffd_pde_params": _lib.PdeParams, "rbffd_request": _lib.Request,
+               "rbffd_server_stats": _lib.ServerStats, "rbffd_weight_params": _lib.WeightParams}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rbffd_sm100.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f, _ in py._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    assert os.system("gcc -std=c99 -I%s %s -o %s" % (os.path.join(ROOT, "include"), src, exe)) == 0
+    got = {}
+    for line in os.popen(str(exe)).read().splitlines():
+        a, b, c = line.split()
+        got[(a, b)] = int(c)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)

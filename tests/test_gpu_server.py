@@ -1,0 +1,252 @@
+"""Serving: the persistent request loop with continuous batching (rbffd_server_*).
+
+* FP64 served requests equal the oracle's RK4 (TimeDependentPDE::advanceRungeKutta4,
+  time_dependent_pde.cpp:172-304) bit for bit, heat and cosine bell;
+* every request's result is identical alone and in a mix of grids, stencil
+  sizes, right-hand sides, dtypes and step counts with staggered arrivals, and
+  FP32 results equal the one-lane rbffd_pde_advance result;
+* admission: a request that can never fit the HBM budget is refused at
+  submission; a budget with room for one request runs them one at a time;
+* cancellation (pending and active), injected admission failures, malformed
+  requests and zero-step requests.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import oracle as O
+import rbffd_gpu_b200 as R
+from tests.helpers import sphere_problem, cosine_bell_setup
+
+pytestmark = pytest.mark.gpu
+
+
+def _grid(ctx, N, n, seed):
+    xyz, st = sphere_problem(N, n, seed)
+    h = np.sqrt(4 * np.pi / N)
+    W = O.weights(xyz, st, None, 0.25 / h, O.LSFC, dim=2, poly_deg=3)
+    W.update(O.weights(xyz, st, None, 0.035 * np.sqrt(N), O.LAMBDA | O.THETA | O.HV, dim=2, poly_deg=2, hv_k=4,
+                       hv_scale=-1e-3 * N ** -4.0))
+    g = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(O.LSFC | O.LAMBDA | O.THETA | O.HV, g, 2)
+    for t, w in W.items():
+        der.setWeights(t, w)
+    return dict(xyz=xyz, st=st, W=W, grid=g, der=der, N=N)
+
+
+@pytest.fixture(scope="module")
+def grids(ctx):
+    gs = [_grid(ctx, 2562, 31, 5), _grid(ctx, 4096, 50, 6)]
+    yield gs
+    for g in gs:
+        g["grid"].close()
+
+
+def _heat_u0(g, seed):
+    c = np.random.default_rng(seed).standard_normal(11 ** 2)
+    return R.exact_sph_heat(g["xyz"], 10, c, 0.0)
+
+
+def _bell_u0(g, seed):
+    rng = np.random.default_rng(seed)
+    cen = rng.normal(size=3)
+    cen /= np.linalg.norm(cen)
+    return np.exp(-6.0 * ((g["xyz"] - cen) ** 2).sum(1))
+
+
+BELL = cosine_bell_setup()
+
+
+def _bell_params(dtype):
+    return R.cosine_bell_params(BELL["a"], BELL["alpha"], BELL["T"], True, dtype=dtype)
+
+
+def _specs(grids):
+    """A mix: both grids, heat and advection, FP32 and FP64, 7 to 90 steps."""
+    out = []
+    for k in range(10):
+        g = grids[k % 2]
+        dtype = R.F32 if k % 3 else R.F64
+        steps = [7, 90, 23, 41, 12, 66, 30, 9, 55, 18][k]
+        if k % 4 < 2:
+            out.append((g, R.heat_params(1.0 + 0.1 * k, dtype), _heat_u0(g, k), 1e-5, steps))
+        else:
+            out.append((g, _bell_params(dtype), _bell_u0(g, k), BELL["dt"], steps))
+    return out
+
+
+def _submit(srv, spec):
+    g, p, u0, dt, steps = spec
+    return srv.submit(g["grid"], p, u0, dt, steps)
+
+
+def test_served_fp64_matches_oracle_bit_exact(ctx, grids):
+    g0, g1 = grids
+    srv = R.Server(ctx)
+    try:
+        u_h = _heat_u0(g0, 1)
+        u_b = _bell_u0(g1, 2)
+        rh = srv.submit(g0["grid"], R.heat_params(1.0, R.F64), u_h, 1e-5, 12)
+        rb = srv.submit(g1["grid"], _bell_params(R.F64), u_b, BELL["dt"], 9)
+        assert srv.wait(rh) == 0 and srv.wait(rb) == 0
+        ref_h = O.rk4_heat(g0["st"], None, g0["W"][O.LSFC], u_h, 1e-5, 12)
+        assert np.array_equal(srv.result(rh), ref_h)
+        cu, cv = O.cosine_bell_coeffs(g1["xyz"], a=BELL["a"], alpha=BELL["alpha"], u0=BELL["u0"])
+        ref_b = O.rk4_advect(g1["st"], None, g1["W"][O.LAMBDA], g1["W"][O.THETA], g1["W"][O.HV], cu, cv, u_b,
+                             BELL["dt"], 9)
+        assert np.array_equal(srv.result(rb), ref_b)
+    finally:
+        srv.stop()
+
+
+def test_alone_and_in_mix_identical(ctx, grids):
+    specs = _specs(grids)
+    srv = R.Server(ctx)
+    try:
+        alone = []
+        for s in specs:
+            rid = _submit(srv, s)
+            assert srv.wait(rid) == 0
+            alone.append(srv.result(rid).copy())
+        st0 = srv.stats()
+        # the mix: half now, the rest once the first batch runs (they join at a step boundary)
+        ids = [_submit(srv, s) for s in specs[:5]]
+        t0 = time.time()
+        while srv.poll(ids[1])[3] < 0 and time.time() - t0 < 10:
+            time.sleep(0.001)
+        ids += [_submit(srv, s) for s in specs[5:]]
+        srv.wait_idle(120)
+        for k, (a, rid) in enumerate(zip(alone, ids)):
+            done, status, lat, q = srv.poll(rid)
+            assert done and status == 0, (k, status)
+            assert lat >= q >= 0
+            assert np.array_equal(srv.result(rid), a), k
+        st = srv.stats()
+        assert st["max_active_seen"] >= 2
+        assert st["completed"] == 20 and st["failed"] == 0
+        assert st["slots_reused"] > st0["slots_reused"]  # finished requests' buffers serve later ones
+        assert st["node_updates"] == pytest.approx(2 * sum(s[0]["N"] * s[4] for s in specs))
+    finally:
+        srv.stop()
+
+
+def test_served_fp32_equals_one_lane_pde_path(ctx, grids):
+    g = grids[1]
+    u0 = _heat_u0(g, 3)
+    srv = R.Server(ctx)
+    try:
+        rid = srv.submit(g["grid"], R.heat_params(1.0, R.F32), u0, 1e-5, 40)
+        assert srv.wait(rid) == 0
+        served = srv.result(rid)
+    finally:
+        srv.stop()
+    pde = R.HeatSphere(g["grid"], g["der"], 1.0, dtype=R.F32)
+    pde.setShape(1, 128)
+    pde.fillInitialConditions(u0)
+    pde.advance(R.RK4, 1e-5, 40)
+    ref = pde.getLocalSolution()
+    pde.close()
+    assert np.array_equal(served, ref)
+
+
+def _need_fp32_heat(N):
+    return N * (4 * 4 + 8)  # u, xa, xb, acc + FP64 staging
+
+
+def test_request_that_can_never_fit_is_refused(ctx, grids):
+    g = grids[1]
+    held, _, total = ctx.mem_info()
+    srv = R.Server(ctx, hbm_fraction=(held + _need_fp32_heat(g["N"]) // 2) / total)
+    try:
+        with pytest.raises(R.RbffdError) as e:
+            srv.submit(g["grid"], R.heat_params(1.0, R.F32), _heat_u0(g, 0), 1e-5, 5)
+        assert e.value.status == R.ERR_BUDGET
+    finally:
+        srv.stop()
+
+
+def test_budget_for_one_request_serialises_admission(ctx, grids):
+    g = grids[1]
+    held, _, total = ctx.mem_info()
+    # room for the server's segment table (64 KiB) and one request's buffers, not two
+    srv = R.Server(ctx, hbm_fraction=(held + 65536 + 1.5 * _need_fp32_heat(g["N"])) / total)
+    try:
+        u0 = [_heat_u0(g, k) for k in range(3)]
+        ids = [srv.submit(g["grid"], R.heat_params(1.0, R.F32), u, 1e-5, 20) for u in u0]
+        srv.wait_idle(60)
+        outs = [srv.result(i) for i in ids]
+        st = srv.stats()
+        assert st["max_active_seen"] == 1 and st["completed"] == 3
+        assert st["held_bytes"] <= st["budget_bytes"]
+    finally:
+        srv.stop()
+    pde = R.HeatSphere(g["grid"], g["der"], 1.0, dtype=R.F32)
+    pde.setShape(1, 128)
+    for u, out in zip(u0, outs):
+        pde.fillInitialConditions(u)
+        pde.advance(R.RK4, 1e-5, 20)
+        assert np.array_equal(pde.getLocalSolution(), out)
+    pde.close()
+
+
+def test_cancel_pending_and_active(ctx, grids):
+    g = grids[0]
+    srv = R.Server(ctx, max_active=1)
+    try:
+        p = R.heat_params(1.0, R.F32)
+        a = srv.submit(g["grid"], p, _heat_u0(g, 0), 1e-7, 2_000_000)  # runs until cancelled
+        b = srv.submit(g["grid"], p, _heat_u0(g, 1), 1e-7, 10)         # waits for the slot
+        t0 = time.time()
+        while srv.poll(a)[3] < 0 and time.time() - t0 < 10:
+            time.sleep(0.001)
+        srv.cancel(b)
+        assert srv.poll(b)[:2] == (True, R.ERR_CANCELLED)
+        srv.cancel(a)
+        assert srv.poll(a)[:2] == (True, R.ERR_CANCELLED)
+        c = srv.submit(g["grid"], p, _heat_u0(g, 2), 1e-7, 10)
+        assert srv.wait(c) == 0
+        st = srv.stats()
+        assert st["cancelled"] == 2 and st["completed"] == 1 and st["slots_reused"] >= 1
+    finally:
+        srv.stop()
+
+
+def test_injected_admission_failure(ctx, grids):
+    g = grids[0]
+    srv = R.Server(ctx)
+    try:
+        srv.inject_admission_failures(1)
+        p = R.heat_params(1.0, R.F32)
+        a = srv.submit(g["grid"], p, _heat_u0(g, 0), 1e-5, 5)
+        assert srv.wait(a) == R.ERR_OOM
+        b = srv.submit(g["grid"], p, _heat_u0(g, 0), 1e-5, 5)
+        assert srv.wait(b) == 0
+        st = srv.stats()
+        assert st["failed"] == 1 and st["completed"] == 1
+    finally:
+        srv.stop()
+
+
+def test_malformed_and_trivial_requests(ctx, grids):
+    g = grids[0]
+    srv = R.Server(ctx)
+    bare = R.Grid(ctx, g["xyz"], g["st"])  # no weights
+    try:
+        p = R.heat_params(1.0, R.F32)
+        p.ntracers = 2
+        with pytest.raises(R.RbffdError) as e:
+            srv.submit(g["grid"], p, _heat_u0(g, 0), 1e-5, 5)
+        assert e.value.status == -5
+        with pytest.raises(R.RbffdError) as e:
+            srv.submit(bare, R.heat_params(1.0, R.F32), _heat_u0(g, 0), 1e-5, 5)
+        assert e.value.status == -6
+        with pytest.raises(R.RbffdError) as e:
+            srv.submit(g["grid"], R.heat_params(1.0, R.F32), _heat_u0(g, 0), 1e-5, -1)
+        assert e.value.status == -1
+        u0 = _heat_u0(g, 4)
+        z = srv.submit(g["grid"], R.heat_params(1.0, R.F64), u0, 1e-5, 0)
+        assert srv.wait(z) == 0 and np.array_equal(srv.result(z), u0)
+    finally:
+        srv.stop()
+        bare.close()
