@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--profile-multitracer", default=None, metavar="ROWS,LANES",
                     help="16-tracer vortex case on N=163842, n=101 (weights > L2), 3 un-graphed RK4 steps with the "
                          "tiled shape ROWS,LANES (0,0 = global-memory gathers), for ncu captures")
+    ap.add_argument("--profile-serving", action="store_true",
+                    help="grouped serving kernel: 8 + 8 requests on two N=163842 grids, 3 RK4 steps, for ncu")
     return ap.parse_args()
 
 
@@ -563,6 +565,9 @@ def bench_serving(R, torch, ctx):
         g["grid"].close()
     served_rate = work / makespan
     plain_rate = work / plain_busy
+    busy = s1["gpu_busy_s"] - s0["gpu_busy_s"]
+    gbs = (s1["stage_bytes"] - s0["stage_bytes"]) / busy / 1e9
+    peak, peak_kind = load_peaks()
     return {
         "workload": C["name"],
         "sample": "first %d requests of the seeded %d-request stream (%.2f s of arrivals)" % (
@@ -570,8 +575,15 @@ def bench_serving(R, torch, ctx):
         "grids_cached": len(grids), "grid_setup_s": setup_s,
         "served_fp32": {
             "node_updates_per_s": served_rate, "makespan_s": makespan,
-            "gpu_busy_node_updates_per_s": (s1["node_updates"] - s0["node_updates"]) / (
-                s1["gpu_busy_s"] - s0["gpu_busy_s"]),
+            "gpu_busy_node_updates_per_s": (s1["node_updates"] - s0["node_updates"]) / busy,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "peak_kind": peak_kind,
+                         "kernel": "k_stage_bank_tile (banks of requests sharing a grid and right-hand side, "
+                                   "one launch per stage, dtype, bank width and operator count)",
+                         "algorithmic_bytes": s1["stage_bytes"] - s0["stage_bytes"],
+                         "note": "algorithmic bytes: per bank and row the stencil's 16-bit local indices and "
+                                 "each operator's weights once (FP32 advection: one fused operator), per row "
+                                 "four state values per bank column; time: device time of the batches"},
             "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
             "queue_p50_s": float(np.percentile(queue, 50)), "queue_p99_s": float(np.percentile(queue, 99)),
             "max_active": s1["max_active_seen"], "batches": s1["ticks"] - s0["ticks"],
@@ -638,9 +650,39 @@ def run_profile_multitracer(spec):
     print("profile run done")
 
 
+def run_profile_serving():
+    """Two N=163842 grids (n=101 advection with HV, n=50 heat), eight FP32
+    requests on each, admitted while the server is paused and then stepped
+    together (groups of 8), 3 RK4 steps: the grouped stage kernel for ncu."""
+    import rbffd_gpu_b200 as R
+    C = dict(SERVING, seed=7)
+    ctx = R.Context(0)
+    ga = serving_grid(R, ctx, 163842, 101, C)
+    gh = serving_grid(R, ctx, 163842, 50, C)
+    srv = R.Server(ctx)
+    srv.pause()
+    rng = np.random.default_rng(0)
+    ids = []
+    for k in range(8):
+        ids.append(srv.submit(ga["grid"], R.cosine_bell_params(1.0, np.pi / 2, 1036800.0, True, dtype=R.F32),
+                              rng.random(163842), 100.0, 3))
+        ids.append(srv.submit(gh["grid"], R.heat_params(1.0, R.F32), rng.random(163842), 1e-6, 3))
+    while any(srv.poll(i)[3] < 0 for i in ids):
+        time.sleep(0.001)
+    srv.pause(False)
+    srv.wait_idle(120)
+    print("profile run done", srv.stats()["launches"])
+    srv.stop()
+    ga["grid"].close()
+    gh["grid"].close()
+    ctx.close()
+
+
 def main():
     args = parse()
-    if args.profile_multitracer:
+    if args.profile_serving:
+        run_profile_serving()
+    elif args.profile_multitracer:
         run_profile_multitracer(args.profile_multitracer)
     elif args.profile:
         run_profile()

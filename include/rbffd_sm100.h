@@ -244,17 +244,20 @@ int rbffd_pde_get_tiling(rbffd_pde* pde, int* rows_per_block);
 /* ---- serving: persistent request loop with continuous batching --------- *
  * No counterpart in the reference, whose drivers run one PDE per process
  * (tests/experiments/cosine_bell_on_sphere/main.cpp:280-515).  A server owns
- * one host thread that advances every admitted request by RK4 steps; each
- * stage of a step is one launch over the rows of all active requests, so
- * requests of different grids, stencil sizes and right-hand sides share the
- * device.  Requests arriving while others run are admitted at the next step
- * boundary, in arrival order, while the context's device memory plus the
- * request's stays within hbm_fraction of the device's memory and fewer than
- * max_active requests run.  Every row is computed by one thread in stencil
- * order with the arithmetic of rbffd_pde_advance with one lane per row, so a
- * request's result does not depend on what else is in the batch (FP64
- * results equal the one-lane rbffd_pde_advance result bit for bit; FP32
- * results equal the FP32 one-lane result). */
+ * two host threads: one admits requests in arrival order while the
+ * context's device memory plus the request's stays within hbm_fraction of
+ * the device's memory and fewer than max_active requests run (allocation and
+ * upload overlap the running steps); the other advances every admitted
+ * request by batches of RK4 steps.  Each stage of a step is one launch per
+ * dtype and group size over the rows of all active requests, so requests of
+ * different grids, stencil sizes and right-hand sides share the device, and
+ * requests on the same grid share one read of its weights and indices.
+ * Requests admitted while others run join at the next step boundary.  Each
+ * request's sums run over its stencil in order with the arithmetic of
+ * rbffd_pde_advance with one lane per row, so its result does not depend on
+ * what else is in the batch (FP64 results equal the one-lane
+ * rbffd_pde_advance result bit for bit; FP32 results equal the FP32
+ * one-lane result). */
 typedef struct rbffd_server rbffd_server;
 
 typedef struct rbffd_request {
@@ -275,6 +278,9 @@ typedef struct rbffd_server_stats {
     long long slots_reused; /* admissions that reused a finished request's device buffers */
     double node_updates;    /* sum over executed request steps of the request's N */
     double gpu_busy_s;      /* device time of the issued batches (CUDA events) */
+    double stage_bytes;     /* algorithmic bytes of the issued stage launches: per group and
+                               row the stencil's indices and each operator's weights once, per
+                               request and row four state values (+ two coefficients) */
     double budget_bytes, held_bytes;
 } rbffd_server_stats;
 
@@ -298,6 +304,10 @@ int rbffd_server_wait_idle(rbffd_server* srv, double timeout_s);
  * boundary; out is not written afterwards).  Returns after it has left. */
 int rbffd_server_cancel(rbffd_server* srv, uint64_t id);
 int rbffd_server_get_stats(rbffd_server* srv, rbffd_server_stats* stats);
+/* paused != 0: issue no further batches of steps (requests are still
+ * admitted, and a batch already issued completes); 0 resumes.  Stopping a
+ * paused server resumes it to finish the admitted requests. */
+int rbffd_server_pause(rbffd_server* srv, int paused);
 /* Fault injection on the host: the next count admissions fail as if the
  * device allocation had failed (status RBFFD_ERR_OOM). */
 int rbffd_server_inject_admission_failures(rbffd_server* srv, int count);

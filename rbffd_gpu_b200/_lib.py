@@ -36,7 +36,7 @@ class Request(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_longlong) for k in ("submitted", "completed", "failed", "cancelled", "pending", "active",
                                                  "max_active_seen", "ticks", "launches", "slots_reused")] + \
-               [(k, c_double) for k in ("node_updates", "gpu_busy_s", "budget_bytes", "held_bytes")]
+               [(k, c_double) for k in ("node_updates", "gpu_busy_s", "stage_bytes", "budget_bytes", "held_bytes")]
 
 
 # name -> (restype, argtypes)
@@ -83,6 +83,7 @@ PROTOTYPES = {
     "rbffd_server_wait_idle": (c_int, [c_void_p, c_double]),
     "rbffd_server_cancel": (c_int, [c_void_p, c_uint64]),
     "rbffd_server_get_stats": (c_int, [c_void_p, P(ServerStats)]),
+    "rbffd_server_pause": (c_int, [c_void_p, c_int]),
     "rbffd_server_inject_admission_failures": (c_int, [c_void_p, c_int]),
     "rbffd_server_stop": (c_int, [c_void_p]),
 }

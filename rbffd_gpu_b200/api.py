@@ -431,6 +431,10 @@ class Server:
     def cancel(self, rid):
         self.ctx.check(self.L.rbffd_server_cancel(self.h, rid), "rbffd_server_cancel")
 
+    def pause(self, paused=True):
+        """Hold (or release) the stepping of admitted requests; admission continues."""
+        self.ctx.check(self.L.rbffd_server_pause(self.h, int(paused)), "rbffd_server_pause")
+
     def inject_admission_failures(self, count):
         self.ctx.check(self.L.rbffd_server_inject_admission_failures(self.h, count))
 

@@ -121,6 +121,9 @@ struct rbffd_pde {
 };
 // Device bytes rbffd_pde_create allocates for these parameters on grid g.
 size_t pde_bytes(const rbffd_grid* g, const rbffd_pde_params* prm);
+// Advection coefficients of an advection right-hand side, internal node order,
+// in prm->dtype, into device arrays of N values (rk4.cu).
+int advect_coefficients(rbffd_grid* g, const rbffd_pde_params* prm, void* cu_dev, void* cv_dev, cudaStream_t s);
 
 // ---- error helpers --------------------------------------------------------
 int set_error(rbffd_ctx* ctx, int status, const char* fmt, ...);

@@ -709,6 +709,53 @@ static Shape autotune(rbffd_pde* P)
 // ---------------------------------------------------------------------------
 // C ABI
 
+// Per-node advection coefficients cu = vel_u / a and cv = vel_v / a in the
+// grid's internal order, stored in prm->dtype at cu_dev / cv_dev.  The cosine
+// bell's are computed on the host in FP64 exactly as CosineBell::solve does
+// every stage (cosine_bell.cpp:35-49; the velocity field is steady);
+// RBFFD_RHS_ADVECTION's are the caller's, reordered.
+int advect_coefficients(rbffd_grid* g, const rbffd_pde_params* prm, void* cu_dev, void* cv_dev, cudaStream_t s)
+{
+    rbffd_ctx* ctx = g->ctx;
+    const int N = g->N;
+    std::vector<double> cu(N), cv(N);
+    if (prm->rhs_kind == RBFFD_RHS_COSINE_BELL) {
+        std::vector<double> xyz((size_t)N * 4);
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(xyz.data(), g->d_xyz, (size_t)N * sizeof(double4), cudaMemcpyDeviceToHost, s));
+        RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+        const double a = prm->sphere_radius, alpha = prm->alpha, u0 = prm->u0;
+        for (int i = 0; i < N; i++) {
+            const double x = xyz[4 * (size_t)i], y = xyz[4 * (size_t)i + 1], z = xyz[4 * (size_t)i + 2];
+            const double lambda = atan2(y, x);
+            const double theta = atan2(z, sqrt(x * x + y * y));
+            const double vel_u = u0 * (cos(theta) * cos(alpha) + sin(theta) * cos(lambda) * sin(alpha));
+            const double vel_v = -u0 * (sin(lambda) * sin(alpha));
+            cu[i] = vel_u / a;
+            cv[i] = vel_v / a;
+        }
+    } else {
+        for (int i = 0; i < N; i++) {  // caller's node order -> internal row order
+            cu[i] = prm->cu[g->h_perm[i]];
+            cv[i] = prm->cv[g->h_perm[i]];
+        }
+    }
+    if (prm->dtype == RBFFD_F64) {
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(cu_dev, cu.data(), (size_t)N * 8, cudaMemcpyHostToDevice, s));
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(cv_dev, cv.data(), (size_t)N * 8, cudaMemcpyHostToDevice, s));
+        RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    } else {
+        std::vector<float> fu(N), fv(N);
+        for (int i = 0; i < N; i++) {
+            fu[i] = (float)cu[i];
+            fv[i] = (float)cv[i];
+        }
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(cu_dev, fu.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s));
+        RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(cv_dev, fv.data(), (size_t)N * 4, cudaMemcpyHostToDevice, s));
+        RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    }
+    return RBFFD_OK;
+}
+
 size_t pde_bytes(const rbffd_grid* g, const rbffd_pde_params* prm)
 {
     const size_t es = prm->dtype == RBFFD_F64 ? 8 : 4, nt = (size_t)g->N * (prm->ntracers > 0 ? prm->ntracers : 1);
@@ -795,60 +842,12 @@ extern "C" int rbffd_pde_create(rbffd_grid* g, const rbffd_pde_params* prm, rbff
     }
     cudaStream_t s = ctx->stream;
     if (kind == KIND_ADVECT) {
-        // Per-node coefficients cu = vel_u / a and cv = vel_v / a, computed on the
-        // host in FP64 exactly as CosineBell::solve does every stage
-        // (cosine_bell.cpp:35-49); the velocity field is steady.
-        std::vector<double> cu(N), cv(N);
-        if (prm->rhs_kind == RBFFD_RHS_COSINE_BELL) {
-            std::vector<double> xyz((size_t)N * 4);
-            cudaError_t e = cudaMemcpyAsync(xyz.data(), g->d_xyz, (size_t)N * sizeof(double4), cudaMemcpyDeviceToHost, s);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-            if (e != cudaSuccess) {
-                pde_free(P);
-                return cuda_error(ctx, e, "rbffd_pde_create");
-            }
-            double a = prm->sphere_radius, alpha = prm->alpha, u0 = prm->u0;
-            for (int i = 0; i < N; i++) {
-                double x = xyz[4 * (size_t)i], y = xyz[4 * (size_t)i + 1], z = xyz[4 * (size_t)i + 2];
-                double lambda = atan2(y, x);
-                double theta = atan2(z, sqrt(x * x + y * y));
-                double vel_u = u0 * (cos(theta) * cos(alpha) + sin(theta) * cos(lambda) * sin(alpha));
-                double vel_v = -u0 * (sin(lambda) * sin(alpha));
-                cu[i] = vel_u / a;
-                cv[i] = vel_v / a;
-            }
-        } else {
-            for (int i = 0; i < N; i++) {  // caller's node order -> internal row order
-                cu[i] = prm->cu[g->h_perm[i]];
-                cv[i] = prm->cv[g->h_perm[i]];
-            }
-        }
-        if ((rc = dev_alloc(ctx, &P->cu, N * es)) || (rc = dev_alloc(ctx, &P->cv, N * es))) {
+        if ((rc = dev_alloc(ctx, &P->cu, N * es)) || (rc = dev_alloc(ctx, &P->cv, N * es)) ||
+            (rc = advect_coefficients(g, prm, P->cu, P->cv, s))) {
             pde_free(P);
             return rc;
         }
         P->bytes += 2 * N * es;
-        std::vector<float> f32;
-        const void* src_u = cu.data();
-        const void* src_v = cv.data();
-        std::vector<float> fu, fv;
-        if (P->dtype == RBFFD_F32) {
-            fu.resize(N);
-            fv.resize(N);
-            for (int i = 0; i < N; i++) {
-                fu[i] = (float)cu[i];
-                fv[i] = (float)cv[i];
-            }
-            src_u = fu.data();
-            src_v = fv.data();
-        }
-        cudaError_t e = cudaMemcpyAsync(P->cu, src_u, N * es, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(P->cv, src_v, N * es, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) {
-            pde_free(P);
-            return cuda_error(ctx, e, "rbffd_pde_create");
-        }
     }
     // FP32 weight copies exist whenever FP64 weights do (grid_make_f32).
     for (int k = 0; k < 3; k++)

@@ -1,25 +1,55 @@
 // Serving: a persistent request loop with continuous batching.
 //
 // A request is one time-dependent PDE solve (heat or advection on a grid whose
-// weights are on the device, any step count).  One host thread per server runs
-// the loop:
-//   1. admission, in arrival order: a request is admitted while fewer than
-//      max_active requests run and the context's device memory plus the
-//      request's buffers stays within the HBM budget.  Its buffers are an
-//      rbffd_pde; a finished request's rbffd_pde with the same grid and
-//      right-hand side is reused (a "slot") instead of allocating, and idle
-//      slots are released first when the budget is short;
-//   2. a batch of RK4 steps for every active request: each of the four stages
-//      of a step is ONE launch of k_stage_batched over the concatenated rows
-//      of all active requests (per dtype), a segment table mapping blocks to
-//      requests.  The batch length is the smallest remaining step count,
-//      capped so a batch takes about TICK_TARGET_S of device time: requests
-//      that arrive meanwhile join at the next batch;
-//   3. requests that reached their step count copy their state to the
-//      caller's buffer and leave; their rbffd_pde becomes an idle slot.
-// Each row is computed by one thread in stencil order with the rounding
-// sequence of k_stage_scalar with one lane per row (rk4.cu), so a request's
-// result does not depend on the rest of the batch.
+// weights are on the device, any step count, its own dt and kappa).
+//
+// Banks.  Requests on the same grid with the same right-hand side (kind,
+// hyperviscosity, advection field) and dtype share a bank: state arrays u,
+// xa, xb, acc with room for BANK_W_F32 (FP32) or BANK_W_F64 (FP64) values per
+// node (one for requests with their own per-node coefficients), in the grid's
+// internal node order, plus the bank's advection coefficients.  The K
+// requests of a bank occupy columns 0..K-1 of an interleaved [N][W] layout
+// whose row stride W is K rounded up to a power of two; a stage kernel row
+// reads the stencil's indices and each operator's weights once for all W
+// columns and gathers a neighbour's W values with one vector load, so
+// requests on a grid share both the operator stream and the gathers, and a
+// lone request runs on the plain [N] layout.  When requests join or leave,
+// the bank is repacked at the next step boundary (u into the free xa buffer
+// at the new stride, then the two are swapped).
+//
+// FP32 advection banks fuse their right-hand side into one operator: the
+// velocity field is steady and the same for every column, so
+//   f_i = -(cu_i D_lambda + cv_i D_theta) u + D_hv u = sum_s Wf[i][s] u[idx[i][s]]
+// with Wf[i][s] = -(cu_i W_lambda[i][s] + cv_i W_theta[i][s]) + W_hv[i][s]
+// formed once per bank in FP64 from the FP64 weights and rounded to FP32: one
+// weight stream per stage instead of three.  FP64 banks keep the three
+// operators and the reference's arithmetic (results equal the oracle's).
+//
+// Stage launches take the grid's row blocks with their halos (struct Halo,
+// blocks of up to SEG_ROWS rows): a block first copies the bank values of its
+// halo nodes into shared memory (one vector per node), then its rows gather
+// from there through the 16-bit local indices -- half the index stream of the
+// int32 indices, and gathers that never leave the SM.
+//
+// Two host threads per server:
+//   * admission (admission_loop), in arrival order: a request gets a free
+//     column of a matching bank, or a new bank, while the context's device
+//     memory plus what the request adds stays within the HBM budget and fewer
+//     than max_active requests are admitted (idle banks are freed first,
+//     oldest first, when the budget is short).  Its initial state is uploaded
+//     into an I/O buffer of its own; all this overlaps the running batches;
+//   * stepping (worker_loop): at a step boundary, banks whose membership
+//     changed are repacked, joining requests' initial states written into
+//     their columns; then a batch of RK4 steps for
+//     every bank with active columns, each of the four stages of a step one
+//     launch of k_stage_bank per (dtype, width, operator count) over the rows
+//     of all those banks (a table maps blocks to banks).  A batch is the
+//     smallest remaining step count, capped at about TICK_TARGET_S of device
+//     time.  Requests that reached their step count read their column out
+//     and leave.
+// A column's sums run over its stencil's slots in order with the rounding
+// sequence of k_stage_scalar with one lane per row (rk4.cu), and free columns
+// hold zeros, so a request's result does not depend on the rest of the batch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,6 +61,7 @@
 #include <memory>
 #include <new>
 #include <thread>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -39,149 +70,362 @@
 
 namespace {
 
-constexpr int SEG_ROWS = 128;            // rows (threads) per block of the batched launch
-constexpr double TICK_TARGET_S = 2e-3;   // device time aimed at per batch of steps
+constexpr int SEG_ROWS = 128;               // rows (threads) per block of a stage launch
+constexpr int BANK_W_F32 = 8;               // columns of an FP32 bank (32-byte rows)
+constexpr int BANK_W_F64 = 4;               // columns of an FP64 bank (32-byte rows)
+constexpr int BANK_W_MAX = 8;
+constexpr double TICK_TARGET_S = 2e-3;      // device time aimed at per batch of steps
 constexpr int TICK_MAX_STEPS = 64;
-constexpr size_t TABLE_BYTES0 = 64 * 1024;  // initial segment-table capacity
+constexpr size_t TABLE_BYTES0 = 64 * 1024;  // initial capacity of the bank tables
+constexpr int TILE_SMEM_MAX = 96 * 1024;    // shared memory for a block's halo values (two blocks per SM)
 
+// One bank as a stage launch sees it.
 template <typename T>
-struct Segment {
+struct BankDesc {
     const int* idx;
     const T* w0;
     const T* w1;
     const T* w2;
-    const T* cu;
+    const T* cu;  // [N] advection coefficients (advection banks)
     const T* cv;
-    T* u;
+    T* u;  // [N][W] state and stage buffers
     T* xa;
     T* xb;
     T* acc;
-    T c[4];  // dt/2, dt/2, dt, dt/6
-    T kappa;
-    int N, nc, kind, use_hv;
-    int block0;  // first block of this request in the launch
+    T c[4][BANK_W_MAX];  // per column: dt/2, dt/2, dt, dt/6 (0 for free columns)
+    T kappa[BANK_W_MAX];
+    // row blocks and halos of the grid (tiled launches)
+    const int* hrows;             // [nblocks + 1] first row of each block
+    const int* hptr;              // [nblocks + 1] offsets into hnodes
+    const int* hnodes;            // halo node indices
+    const unsigned short* lidx;   // sliced ELL local indices into the block's halo
+    int N, nc, kind;
+    int block0;  // first block of this bank in the launch
 };
 
-// One RK4 stage for the rows of all requests of one dtype.  Stage inputs:
-// 0: u -> xa, 1: xa -> xb, 2: xb -> xa, 3: xa -> u (the buffers of k_stage_*).
-template <typename T>
-__global__ void __launch_bounds__(SEG_ROWS) k_stage_batched(const Segment<T>* __restrict__ segs, int nseg, int stage)
+// W consecutive values (W * sizeof(T) = 4, 8 or a multiple of 16 bytes)
+template <typename T, int W>
+__device__ __forceinline__ void ldw(const T* p, T (&v)[W], bool readonly)
 {
-    int lo = 0, hi = nseg - 1;  // last segment with block0 <= blockIdx.x
+    if (W * sizeof(T) == 8) {
+        float2 t = readonly ? __ldg(reinterpret_cast<const float2*>(p)) : *reinterpret_cast<const float2*>(p);
+        memcpy(&v[0], &t, 8);
+    } else if (W * sizeof(T) % 16 == 0) {
+#pragma unroll
+        for (int q = 0; q < W * (int)sizeof(T) / 16; q++) {
+            float4 t = readonly ? __ldg(reinterpret_cast<const float4*>(p) + q) : reinterpret_cast<const float4*>(p)[q];
+            memcpy(&v[q * 16 / sizeof(T)], &t, 16);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < W; k++) v[k] = readonly ? __ldg(p + k) : p[k];
+    }
+}
+
+template <typename T, int W>
+__device__ __forceinline__ void stw(T* p, const T (&v)[W])
+{
+    if (W * sizeof(T) == 8) {
+        float2 t;
+        memcpy(&t, &v[0], 8);
+        *reinterpret_cast<float2*>(p) = t;
+    } else if (W * sizeof(T) % 16 == 0) {
+#pragma unroll
+        for (int q = 0; q < W * (int)sizeof(T) / 16; q++) {
+            float4 t;
+            memcpy(&t, &v[q * 16 / sizeof(T)], 16);
+            reinterpret_cast<float4*>(p)[q] = t;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < W; k++) p[k] = v[k];
+    }
+}
+
+// Right-hand side and RK4 stage update of row i, all W columns (the
+// arithmetic of stage_update in rk4.cu, per column).
+template <typename T, int W, int NOPS>
+__device__ __forceinline__ void bank_stage_update(const BankDesc<T>& B, int i, int stage, const T (&d0)[W],
+                                                  const T (&d1)[W], const T (&d2)[W])
+{
+    const bool adv = B.kind == KIND_ADVECT;
+    const T cu = adv ? B.cu[i] : T(0), cv = adv ? B.cv[i] : T(0);
+    const size_t row = (size_t)i * W;
+    T ui[W], ac[W], out[W];
+    ldw<T, W>(B.u + row, ui, false);
+    if (stage > 0) ldw<T, W>(B.acc + row, ac, false);
+#pragma unroll
+    for (int v = 0; v < W; v++) {
+        T f;
+        if (adv) {
+            f = -Ar<T>::fma(cu, d0[v], Ar<T>::mul(cv, d1[v]));
+            if (NOPS > 2) f = Ar<T>::add(f, d2[v]);
+        } else {
+            f = Ar<T>::mul(B.kappa[v], d0[v]);
+        }
+        const T c = B.c[stage][v];
+        if (stage == 0) {
+            ac[v] = f;
+            out[v] = Ar<T>::fma(c, f, ui[v]);
+        } else if (stage < 3) {
+            ac[v] = Ar<T>::add(ac[v], Ar<T>::mul(T(2), f));
+            out[v] = Ar<T>::fma(c, f, ui[v]);
+        } else {
+            out[v] = Ar<T>::fma(c, Ar<T>::add(ac[v], f), ui[v]);
+        }
+    }
+    if (stage < 3) {
+        stw<T, W>(B.acc + row, ac);
+        stw<T, W>((stage == 1 ? B.xb : B.xa) + row, out);
+    } else {
+        stw<T, W>(B.u + row, out);
+    }
+}
+
+// One RK4 stage for the rows of every bank of one launch.  Stage buffers as in
+// k_stage_scalar: 0: u -> xa, 1: xa -> xb, 2: xb -> xa, 3: xa -> u.  Column v
+// of row i accumulates w[s] * x[idx[s]][v] over the slots s in stencil order
+// with fused multiply-adds, exactly the single-request sequence.
+template <typename T, int W, int NOPS>
+__global__ void __launch_bounds__(SEG_ROWS) k_stage_bank(const BankDesc<T>* __restrict__ banks, int nbanks, int stage)
+{
+    int lo = 0, hi = nbanks - 1;  // last bank with block0 <= blockIdx.x
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (segs[mid].block0 <= (int)blockIdx.x) lo = mid;
+        if (banks[mid].block0 <= (int)blockIdx.x) lo = mid;
         else hi = mid - 1;
     }
-    const Segment<T>& S = segs[lo];
-    const int i = ((int)blockIdx.x - S.block0) * SEG_ROWS + (int)threadIdx.x;
-    if (i >= S.N) return;
-    const T* x = stage == 0 ? S.u : (stage == 2 ? S.xb : S.xa);
-    const bool adv = S.kind == KIND_ADVECT, hv = adv && S.use_hv;
-    T d0 = T(0), d1 = T(0), d2 = T(0);
-    for (int c = 0; c < S.nc; c++) {
-        const size_t o = sell_off(i, c, S.nc);
-        const int4 j = ld_idx4(S.idx + o);
-        const T xv[4] = {__ldg(x + j.x), __ldg(x + j.y), __ldg(x + j.z), __ldg(x + j.w)};
-        T w[4];
-        ld_w4(S.w0 + o, w);
+    const BankDesc<T>& B = banks[lo];
+    const int i = ((int)blockIdx.x - B.block0) * SEG_ROWS + (int)threadIdx.x;
+    if (i >= B.N) return;
+    const T* x = stage == 0 ? B.u : (stage == 2 ? B.xb : B.xa);
+    T d0[W], d1[W], d2[W];
 #pragma unroll
-        for (int k = 0; k < 4; k++) d0 = Ar<T>::fma(w[k], xv[k], d0);
-        if (adv) {
-            ld_w4(S.w1 + o, w);
+    for (int v = 0; v < W; v++) d0[v] = d1[v] = d2[v] = T(0);
+    for (int c = 0; c < B.nc; c++) {
+        const size_t o = sell_off(i, c, B.nc);
+        const int4 j4 = ld_idx4(B.idx + o);
+        const int jj[4] = {j4.x, j4.y, j4.z, j4.w};
+        T wa[4], wb[4], wc[4];
+        ld_w4(B.w0 + o, wa);
+        if (NOPS > 1) ld_w4(B.w1 + o, wb);
+        if (NOPS > 2) ld_w4(B.w2 + o, wc);
 #pragma unroll
-            for (int k = 0; k < 4; k++) d1 = Ar<T>::fma(w[k], xv[k], d1);
-            if (hv) {
-                ld_w4(S.w2 + o, w);
+        for (int e = 0; e < 4; e++) {
+            T xv[W];
+            ldw<T, W>(x + (size_t)jj[e] * W, xv, true);
 #pragma unroll
-                for (int k = 0; k < 4; k++) d2 = Ar<T>::fma(w[k], xv[k], d2);
+            for (int v = 0; v < W; v++) {
+                d0[v] = Ar<T>::fma(wa[e], xv[v], d0[v]);
+                if (NOPS > 1) d1[v] = Ar<T>::fma(wb[e], xv[v], d1[v]);
+                if (NOPS > 2) d2[v] = Ar<T>::fma(wc[e], xv[v], d2[v]);
             }
         }
     }
-    T f;
-    if (adv) {
-        f = -Ar<T>::fma(S.cu[i], d0, Ar<T>::mul(S.cv[i], d1));
-        if (hv) f = Ar<T>::add(f, d2);
-    } else {
-        f = Ar<T>::mul(S.kappa, d0);
+    bank_stage_update<T, W, NOPS>(B, i, stage, d0, d1, d2);
+}
+
+// The same stage over a grid's halo row blocks: the block's halo values of x
+// are staged in shared memory ([halo node][W]), gathers read them through the
+// 16-bit local indices.  Same per-column arithmetic as k_stage_bank.
+template <typename T, int W, int NOPS>
+__global__ void __launch_bounds__(SEG_ROWS) k_stage_bank_tile(const BankDesc<T>* __restrict__ banks, int nbanks,
+                                                              int stage)
+{
+    extern __shared__ __align__(16) unsigned char smem_bank[];
+    T* sx = reinterpret_cast<T*>(smem_bank);
+    int lo = 0, hi = nbanks - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (banks[mid].block0 <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
     }
-    const T ui = S.u[i];
-    const T c = S.c[stage];
-    switch (stage) {
-    case 0:
-        S.acc[i] = f;
-        S.xa[i] = Ar<T>::fma(c, f, ui);
-        break;
-    case 1:
-        S.acc[i] = Ar<T>::add(S.acc[i], Ar<T>::mul(T(2), f));
-        S.xb[i] = Ar<T>::fma(c, f, ui);
-        break;
-    case 2:
-        S.acc[i] = Ar<T>::add(S.acc[i], Ar<T>::mul(T(2), f));
-        S.xa[i] = Ar<T>::fma(c, f, ui);
-        break;
-    default:
-        S.u[i] = Ar<T>::fma(c, Ar<T>::add(S.acc[i], f), ui);
-        break;
+    const BankDesc<T>& B = banks[lo];
+    const int b = (int)blockIdx.x - B.block0;
+    const int r0 = __ldg(B.hrows + b), r1 = __ldg(B.hrows + b + 1);
+    const int h0 = __ldg(B.hptr + b), hn = __ldg(B.hptr + b + 1) - h0;
+    const T* x = stage == 0 ? B.u : (stage == 2 ? B.xb : B.xa);
+    for (int h = threadIdx.x; h < hn; h += blockDim.x) {
+        T v[W];
+        ldw<T, W>(x + (size_t)__ldg(B.hnodes + h0 + h) * W, v, true);
+        stw<T, W>(sx + (size_t)h * W, v);
+    }
+    __syncthreads();
+    const int i = r0 + (int)threadIdx.x;
+    if (i >= r1) return;
+    T d0[W], d1[W], d2[W];
+#pragma unroll
+    for (int v = 0; v < W; v++) d0[v] = d1[v] = d2[v] = T(0);
+    for (int c = 0; c < B.nc; c++) {
+        const size_t o = sell_off(i, c, B.nc);
+        const ushort4 l4 = __ldg(reinterpret_cast<const ushort4*>(B.lidx + o));
+        const int ll[4] = {l4.x, l4.y, l4.z, l4.w};
+        T wa[4], wb[4], wc[4];
+        ld_w4(B.w0 + o, wa);
+        if (NOPS > 1) ld_w4(B.w1 + o, wb);
+        if (NOPS > 2) ld_w4(B.w2 + o, wc);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            T xv[W];
+            ldw<T, W>(sx + (size_t)ll[e] * W, xv, false);
+#pragma unroll
+            for (int v = 0; v < W; v++) {
+                d0[v] = Ar<T>::fma(wa[e], xv[v], d0[v]);
+                if (NOPS > 1) d1[v] = Ar<T>::fma(wb[e], xv[v], d1[v]);
+                if (NOPS > 2) d2[v] = Ar<T>::fma(wc[e], xv[v], d2[v]);
+            }
+        }
+    }
+    bank_stage_update<T, W, NOPS>(B, i, stage, d0, d1, d2);
+}
+
+// A bank's new layout at a step boundary: column c of dst (row stride wdst)
+// takes column from[c] of src (stride wsrc), or the initial state of a
+// joining request (FP64, caller's node order, rounded to T), or zero.
+constexpr int FROM_ZERO = -1, FROM_IO = -2;
+
+template <typename T>
+struct Repack {
+    T* dst;
+    const T* src;
+    int wsrc, wdst, N;
+    int from[BANK_W_MAX];
+    const double* io[BANK_W_MAX];
+    const int* perm;  // internal row -> caller's node index
+};
+
+template <typename T>
+__global__ void k_repack(Repack<T> a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.N) return;
+    for (int c = 0; c < a.wdst; c++) {
+        T v = T(0);
+        if (a.from[c] >= 0) v = a.src[(size_t)i * a.wsrc + a.from[c]];
+        else if (a.from[c] == FROM_IO) v = (T)a.io[c][a.perm[i]];
+        a.dst[(size_t)i * a.wdst + c] = v;
+    }
+}
+
+// A request's column, back to FP64 in the caller's node order.
+template <typename T>
+__global__ void k_column_out(const T* u, int W, int col, double* __restrict__ io, const int* __restrict__ perm, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) io[perm[i]] = (double)u[(size_t)i * W + col];
+}
+
+// Fused advection operator of a bank, row by row over the padded rows (sliced
+// ELL; padding rows and slots stay 0): Wf = -(cu W_lambda + cv W_theta) + W_hv.
+__global__ void k_fuse_advection(float* __restrict__ wf, const double* __restrict__ wl,
+                                 const double* __restrict__ wt, const double* __restrict__ wh,
+                                 const double* __restrict__ cu, const double* __restrict__ cv, int N, int rows, int nc)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const double a = i < N ? cu[i] : 0.0, c = i < N ? cv[i] : 0.0;
+    for (int s = 0; s < 4 * nc; s++) {
+        const size_t o = sell_elem(i, s, nc);
+        double w = -(a * wl[o] + c * wt[o]);
+        if (wh) w += wh[o];
+        wf[o] = i < N ? __double2float_rn(w) : 0.0f;
     }
 }
 
 using Clock = std::chrono::steady_clock;
+
+struct Bank;
 
 struct Request {
     uint64_t id = 0;
     rbffd_request p{};
     std::vector<double> u0, cu, cv;  // copies taken at submission
     Clock::time_point t_submit, t_admit, t_done;
-    bool admitted = false, cancel = false;
+    bool admitted = false, cancel = false, inserted = false;
     int done = 0, status = RBFFD_OK;
-    rbffd_pde* pde = nullptr;
-    size_t bytes = 0;
+    Bank* bank = nullptr;
+    int col = -1;
+    double* d_io = nullptr;  // [N] FP64, caller's order: initial state in, result out
     int steps_done = 0;
 };
 
-// An idle rbffd_pde kept for reuse by a later request with the same grid and
-// right-hand side (per-node coefficients included).
-struct Slot {
-    rbffd_pde* pde;
-    rbffd_pde_params prm;
-    rbffd_grid* grid;
-    size_t bytes;
+struct Bank {
+    rbffd_grid* grid = nullptr;
+    rbffd_pde_params prm{};  // right-hand side (coefficient pointers unused)
+    uint64_t owner = 0;      // request id for a bank with caller-given coefficients
+    int dtype = RBFFD_F32, kind = KIND_HEAT, nops = 1;
+    int Wcap = 1;  // values per node the arrays hold
+    int op[3] = {-1, -1, -1};
+    void *u = nullptr, *xa = nullptr, *xb = nullptr, *acc = nullptr, *cu = nullptr, *cv = nullptr;
+    void* wf = nullptr;  // fused advection operator (FP32 advection banks), sliced ELL
+    const Halo* halo = nullptr;  // the grid's row blocks of SEG_ROWS rows (nullptr: untiled)
+    size_t bytes = 0;
+    int members = 0;       // admitted requests assigned to the bank (S->mu)
+    bool in_plan = false;  // referenced by the stepping thread's current tables (S->mu)
+    Clock::time_point idle_since;
+    // layout, owned by the stepping thread
+    int W = 1;                   // row stride
+    std::vector<Request*> cols;  // occupant of each column 0..W-1 (nullptr: free)
+    std::vector<Request*> join;  // admitted, placed at the next step boundary
+    bool dirty = false;          // membership changed since the last repack
 };
 
-bool slot_fits(const Slot& s, const rbffd_grid* g, const rbffd_pde_params& p)
+size_t state_bytes(const rbffd_pde_params& p) { return p.dtype == RBFFD_F64 ? 8 : 4; }
+
+int bank_capacity(const rbffd_pde_params& p)
 {
-    if (s.grid != g || s.prm.rhs_kind != p.rhs_kind || s.prm.dtype != p.dtype) return false;
-    if (p.rhs_kind == RBFFD_RHS_HEAT) return true;        // kappa is a per-request scalar
-    if (p.rhs_kind == RBFFD_RHS_ADVECTION) return false;  // caller-given coefficients: never shared
-    return s.prm.use_hv == p.use_hv && s.prm.sphere_radius == p.sphere_radius && s.prm.alpha == p.alpha &&
-           s.prm.u0 == p.u0;
+    if (p.rhs_kind == RBFFD_RHS_ADVECTION) return 1;
+    return p.dtype == RBFFD_F64 ? BANK_W_F64 : BANK_W_F32;
 }
 
-enum { ADMIT_WAIT = 1 };
+bool bank_fused(const rbffd_pde_params& p) { return p.rhs_kind != RBFFD_RHS_HEAT && p.dtype == RBFFD_F32; }
+
+size_t fused_bytes(const rbffd_grid* g) { return (size_t)g->N32 * g->n4 * sizeof(float); }
+
+size_t bank_bytes(const rbffd_grid* g, const rbffd_pde_params& p)
+{
+    const size_t es = state_bytes(p), N = (size_t)g->N;
+    const size_t rhs = p.rhs_kind == RBFFD_RHS_HEAT ? 0 : (bank_fused(p) ? fused_bytes(g) : 2 * N * es);
+    return 4 * N * bank_capacity(p) * es + rhs;
+}
+
+bool bank_fits(const Bank& b, const Request& r)
+{
+    const rbffd_pde_params& p = r.p.pde;
+    if (b.grid != r.p.grid || b.prm.rhs_kind != p.rhs_kind || b.dtype != p.dtype) return false;
+    if (p.rhs_kind == RBFFD_RHS_ADVECTION) return b.owner == r.id;  // caller-given coefficients
+    if (p.rhs_kind == RBFFD_RHS_HEAT) return true;                  // kappa is per column
+    return b.prm.use_hv == p.use_hv && b.prm.sphere_radius == p.sphere_radius && b.prm.alpha == p.alpha &&
+           b.prm.u0 == p.u0;
+}
 
 }  // namespace
 
 struct rbffd_server {
     rbffd_ctx* ctx = nullptr;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;   // stepping thread: stage launches, column in/out, results
+    cudaStream_t astream = nullptr;  // admission thread: bank set-up, initial-state uploads
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     size_t budget = 0;
     int max_active = 0;
-    std::mutex mu;  // guards everything below that the worker and callers share
-    std::condition_variable cv_work, cv_done;
-    std::deque<std::shared_ptr<Request>> pending;
-    std::vector<std::shared_ptr<Request>> active;
+    std::mutex mu;  // guards everything below up to the stepping-thread state
+    std::condition_variable cv_work;   // the stepping thread waits for admitted requests
+    std::condition_variable cv_admit;  // the admission thread waits for requests, columns or memory
+    std::condition_variable cv_done;   // callers wait for results
+    std::deque<std::shared_ptr<Request>> pending;  // submitted, not yet admitted
+    std::vector<std::shared_ptr<Request>> ready;   // admitted, join at the next step boundary
+    std::vector<std::shared_ptr<Request>> active;  // stepping
     std::map<uint64_t, std::shared_ptr<Request>> all;
+    std::vector<std::unique_ptr<Bank>> banks;
     uint64_t next_id = 1;
-    bool stop = false;
+    bool stop = false, admitter_done = false;
+    bool paused = false;  // no batches are issued while set (admission continues)
     int inject_fail = 0;
-    size_t owned = 0;  // device bytes of the server's rbffd_pde objects (active + idle slots)
+    size_t owned = 0;  // device bytes of banks and I/O buffers (reserved or allocated)
     rbffd_server_stats st{};
-    std::thread worker;
-    // worker-only state
-    std::vector<Slot> slots;
-    void* h_tab = nullptr;  // pinned host segment tables
+    std::thread worker, admitter;
+    // stepping-thread state
+    void* h_tab = nullptr;  // pinned host bank tables
     void* d_tab = nullptr;
     size_t tab_cap = 0;
     double step_s = 0.0;  // device seconds per step of the last batch
@@ -202,185 +446,116 @@ size_t ctx_held(rbffd_ctx* ctx)
     return ctx->held;
 }
 
-// Give a request's rbffd_pde back as an idle slot, or free it.
-void retire_pde(rbffd_server* S, Request& r, bool keep)
+void ctx_account(rbffd_ctx* ctx, size_t add, size_t sub)
 {
-    if (!r.pde) return;
-    if (keep) {
-        S->slots.push_back(Slot{r.pde, r.p.pde, r.p.grid, r.bytes});
-    } else {
-        rbffd_pde_destroy(r.pde);
-        std::lock_guard<std::mutex> lk(S->mu);
-        S->owned -= std::min(S->owned, r.bytes);
-    }
-    r.pde = nullptr;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->held += add;
+    ctx->held -= std::min(ctx->held, sub);
 }
 
-void drop_slot(rbffd_server* S, size_t k)
+void bank_free_memory(rbffd_ctx* ctx, Bank& b)
 {
-    rbffd_pde_destroy(S->slots[k].pde);
-    {
-        std::lock_guard<std::mutex> lk(S->mu);
-        S->owned -= std::min(S->owned, S->slots[k].bytes);
-    }
-    S->slots.erase(S->slots.begin() + (long)k);
+    const size_t es = b.dtype == RBFFD_F64 ? 8 : 4, n = (size_t)b.grid->N * b.Wcap * es, nc = (size_t)b.grid->N * es;
+    dev_free(ctx, b.u, n);
+    dev_free(ctx, b.xa, n);
+    dev_free(ctx, b.xb, n);
+    dev_free(ctx, b.acc, n);
+    dev_free(ctx, b.cu, nc);
+    dev_free(ctx, b.cv, nc);
+    dev_free(ctx, b.wf, fused_bytes(b.grid));
+    b.u = b.xa = b.xb = b.acc = b.cu = b.cv = b.wf = nullptr;
 }
 
-// Give the request device buffers holding its initial state.  RBFFD_OK,
-// ADMIT_WAIT (the budget frees up when active requests finish) or an error.
-int admit(rbffd_server* S, Request& r, bool nothing_active, bool* reused)
+// Device arrays of a new bank for request r (zeroed state, advection
+// coefficients); called without S->mu held.
+int bank_create(rbffd_server* S, const Request& r, Bank& b)
 {
-    *reused = false;
+    rbffd_ctx* ctx = S->ctx;
     rbffd_grid* g = r.p.grid;
-    rbffd_pde* P = nullptr;
-    for (size_t k = 0; k < S->slots.size(); k++)
-        if (slot_fits(S->slots[k], g, r.p.pde)) {
-            P = S->slots[k].pde;
-            r.bytes = S->slots[k].bytes;
-            S->slots.erase(S->slots.begin() + (long)k);
-            *reused = true;
-            break;
-        }
-    if (!P) {
-        const size_t need = pde_bytes(g, &r.p.pde);
-        while (ctx_held(S->ctx) + need > S->budget && !S->slots.empty()) drop_slot(S, 0);  // oldest idle first
-        if (ctx_held(S->ctx) + need > S->budget) {
-            if (!nothing_active) return ADMIT_WAIT;
-            return set_error(S->ctx, RBFFD_ERR_BUDGET, "request of %zu bytes does not fit the budget of %zu bytes",
-                             need, S->budget);
-        }
-        {
-            // reserve before allocating: submissions meanwhile see these bytes as the server's
-            std::lock_guard<std::mutex> lk(S->mu);
-            S->owned += need;
-        }
-        const int rc = rbffd_pde_create(g, &r.p.pde, &P);
-        std::lock_guard<std::mutex> lk(S->mu);
-        S->owned -= std::min(S->owned, need);
-        if (rc) return rc;
-        r.bytes = P->bytes;
-        S->owned += r.bytes;
+    const rbffd_pde_params& p = r.p.pde;
+    b.grid = g;
+    b.prm = p;
+    b.prm.cu = b.prm.cv = nullptr;
+    b.owner = p.rhs_kind == RBFFD_RHS_ADVECTION ? r.id : 0;
+    b.dtype = p.dtype;
+    b.Wcap = bank_capacity(p);
+    if (p.rhs_kind == RBFFD_RHS_HEAT) {
+        b.kind = KIND_HEAT;
+        b.nops = 1;
+        b.op[0] = der_index(RBFFD_LSFC);
+    } else {
+        b.kind = KIND_ADVECT;
+        b.nops = p.use_hv ? 3 : 2;
+        b.op[0] = der_index(RBFFD_LAMBDA);
+        b.op[1] = der_index(RBFFD_THETA);
+        if (p.use_hv) b.op[2] = der_index(RBFFD_HV);
     }
-    P->kappa = r.p.pde.kappa;
-    P->t = 0.0;
-    const int rc = rbffd_pde_set_state(P, r.u0.data());
-    r.pde = P;
-    if (rc) {
-        retire_pde(S, r, false);
+    b.bytes = bank_bytes(g, p);
+    int rc;
+    for (int k = 0; k < b.nops; k++)  // FP32 weight copies are made on first use
+        if (b.dtype == RBFFD_F32 && !g->d_w32[b.op[k]] && (rc = grid_make_f32(g, b.op[k]))) return rc;
+    const size_t es = state_bytes(p), n = (size_t)g->N * b.Wcap * es;
+    if ((rc = dev_alloc(ctx, &b.u, n)) || (rc = dev_alloc(ctx, &b.xa, n)) || (rc = dev_alloc(ctx, &b.xb, n)) ||
+        (rc = dev_alloc(ctx, &b.acc, n))) {
+        bank_free_memory(ctx, b);
         return rc;
     }
-    return RBFFD_OK;
-}
-
-template <typename T>
-void fill_segment(Segment<T>& s, const Request& r, int block0)
-{
-    const rbffd_pde* P = r.pde;
-    const rbffd_grid* g = P->g;
-    auto W = [&](int k) -> const T* {
-        if (P->op[k] < 0) return nullptr;
-        return std::is_same<T, double>::value ? (const T*)g->d_w64[P->op[k]] : (const T*)g->d_w32[P->op[k]];
-    };
-    s.idx = g->d_idx;
-    s.w0 = W(0);
-    s.w1 = W(1);
-    s.w2 = W(2);
-    s.cu = (const T*)P->cu;
-    s.cv = (const T*)P->cv;
-    s.u = (T*)P->u;
-    s.xa = (T*)P->xa;
-    s.xb = (T*)P->xb;
-    s.acc = (T*)P->acc;
-    // the stage coefficients of rbffd_pde_advance
-    const double dt = r.p.dt;
-    s.c[0] = (T)(0.5 * dt);
-    s.c[1] = (T)(0.5 * dt);
-    s.c[2] = (T)(1.0 * dt);
-    s.c[3] = (T)(dt / 6.);
-    s.kappa = (T)P->kappa;
-    s.N = g->N;
-    s.nc = g->nc;
-    s.kind = P->kind;
-    s.use_hv = P->use_hv;
-    s.block0 = block0;
-}
-
-struct Tables {
-    int n32 = 0, n64 = 0, blocks32 = 0, blocks64 = 0;
-    size_t off64 = 0;  // byte offset of the FP64 table
-};
-
-// Build the segment tables of the active set and upload them (stream-ordered
-// before the launches that read them; the previous batch has completed, so
-// the pinned host copy is free to rewrite).
-int upload_tables(rbffd_server* S, const std::vector<std::shared_ptr<Request>>& act, Tables& t)
-{
-    t = Tables{};
-    for (auto& r : act) (r->pde->dtype == RBFFD_F64 ? t.n64 : t.n32)++;
-    const size_t b32 = (size_t)t.n32 * sizeof(Segment<float>), b64 = (size_t)t.n64 * sizeof(Segment<double>);
-    t.off64 = (b32 + 255) / 256 * 256;
-    const size_t need = t.off64 + b64;
-    if (need > S->tab_cap) {
-        const size_t cap = std::max<size_t>(need * 2, TABLE_BYTES0);
-        if (S->h_tab) cudaFreeHost(S->h_tab);
-        dev_free(S->ctx, S->d_tab, S->tab_cap);
-        S->h_tab = nullptr;
-        S->d_tab = nullptr;
-        S->tab_cap = 0;
-        RBFFD_CUDA_TRY(S->ctx, cudaMallocHost(&S->h_tab, cap));
-        const int rc = dev_alloc(S->ctx, &S->d_tab, cap);
-        if (rc) return rc;
-        S->tab_cap = cap;
+    // the grid's row blocks and halos; banks whose halos would not fit shared memory stay untiled
+    const Halo* h = nullptr;
+    if (grid_halo(g, SEG_ROWS, &h) == RBFFD_OK && (size_t)h->max_halo * b.Wcap * es <= (size_t)TILE_SMEM_MAX)
+        b.halo = h;
+    cudaError_t e = cudaMemsetAsync(b.u, 0, n, S->astream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.xa, 0, n, S->astream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.xb, 0, n, S->astream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.acc, 0, n, S->astream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->astream);
+    if (e != cudaSuccess) {
+        bank_free_memory(ctx, b);
+        return cuda_error(ctx, e, "bank set-up");
     }
-    Segment<float>* s32 = (Segment<float>*)S->h_tab;
-    Segment<double>* s64 = (Segment<double>*)((char*)S->h_tab + t.off64);
-    int k32 = 0, k64 = 0;
-    for (auto& r : act) {
-        const int nb = (r->pde->g->N + SEG_ROWS - 1) / SEG_ROWS;
-        if (r->pde->dtype == RBFFD_F64) {
-            fill_segment(s64[k64++], *r, t.blocks64);
-            t.blocks64 += nb;
+    if (b.kind == KIND_ADVECT) {
+        rbffd_pde_params q = p;
+        q.cu = r.cu.empty() ? nullptr : r.cu.data();
+        q.cv = r.cv.empty() ? nullptr : r.cv.data();
+        if (bank_fused(p)) {  // FP64 coefficients and weights -> one FP32 operator
+            q.dtype = RBFFD_F64;
+            void *cu64 = nullptr, *cv64 = nullptr;
+            const size_t nc = (size_t)g->N * sizeof(double);
+            if (!(rc = dev_alloc(ctx, &cu64, nc)) && !(rc = dev_alloc(ctx, &cv64, nc)) &&
+                !(rc = advect_coefficients(g, &q, cu64, cv64, S->astream)) &&
+                !(rc = dev_alloc(ctx, &b.wf, fused_bytes(g)))) {
+                const int rows = g->N32;
+                k_fuse_advection<<<(rows + 127) / 128, 128, 0, S->astream>>>(
+                    (float*)b.wf, g->d_w64[b.op[0]], g->d_w64[b.op[1]], b.op[2] >= 0 ? g->d_w64[b.op[2]] : nullptr,
+                    (const double*)cu64, (const double*)cv64, g->N, rows, g->nc);
+                cudaError_t e = cudaGetLastError();
+                if (e == cudaSuccess) e = cudaStreamSynchronize(S->astream);
+                if (e != cudaSuccess) rc = cuda_error(ctx, e, "fused advection operator");
+            }
+            dev_free(ctx, cu64, nc);
+            dev_free(ctx, cv64, nc);
         } else {
-            fill_segment(s32[k32++], *r, t.blocks32);
-            t.blocks32 += nb;
+            const size_t nc = (size_t)g->N * es;
+            if (!(rc = dev_alloc(ctx, &b.cu, nc)) && !(rc = dev_alloc(ctx, &b.cv, nc)))
+                rc = advect_coefficients(g, &q, b.cu, b.cv, S->astream);
+        }
+        if (rc) {
+            bank_free_memory(ctx, b);
+            return rc;
         }
     }
-    RBFFD_CUDA_TRY(S->ctx, cudaMemcpyAsync(S->d_tab, S->h_tab, need, cudaMemcpyHostToDevice, S->stream));
     return RBFFD_OK;
 }
 
-// Issue nsteps RK4 steps for the active set; returns after they complete.
-int run_steps(rbffd_server* S, const Tables& t, int nsteps, double* seconds, long long* launches)
-{
-    const Segment<float>* d32 = (const Segment<float>*)S->d_tab;
-    const Segment<double>* d64 = (const Segment<double>*)((char*)S->d_tab + t.off64);
-    RBFFD_CUDA_TRY(S->ctx, cudaEventRecord(S->ev0, S->stream));
-    for (int step = 0; step < nsteps; step++)
-        for (int stage = 0; stage < 4; stage++) {
-            if (t.n32) {
-                k_stage_batched<float><<<t.blocks32, SEG_ROWS, 0, S->stream>>>(d32, t.n32, stage);
-                ++*launches;
-            }
-            if (t.n64) {
-                k_stage_batched<double><<<t.blocks64, SEG_ROWS, 0, S->stream>>>(d64, t.n64, stage);
-                ++*launches;
-            }
-        }
-    RBFFD_CUDA_TRY(S->ctx, cudaGetLastError());
-    RBFFD_CUDA_TRY(S->ctx, cudaEventRecord(S->ev1, S->stream));
-    RBFFD_CUDA_TRY(S->ctx, cudaEventSynchronize(S->ev1));
-    float ms = 0.f;
-    RBFFD_CUDA_TRY(S->ctx, cudaEventElapsedTime(&ms, S->ev0, S->ev1));
-    *seconds = ms * 1e-3;
-    return RBFFD_OK;
-}
-
-void worker_loop(rbffd_server* S)
+// Admission thread.  In arrival order, each pending request gets a column of a
+// matching bank (a new bank when none has room and the budget allows; idle
+// banks are freed first, oldest first) and an I/O buffer holding its initial
+// state, then moves to the ready list.  Runs beside the stepping thread, so
+// allocation and the upload overlap the running batches.
+void admission_loop(rbffd_server* S)
 {
     cudaSetDevice(S->ctx->device);
     std::unique_lock<std::mutex> lk(S->mu);
-    bool changed = true;
-    Tables tab;
     for (;;) {
         // cancelled requests still waiting leave now (all of them once the server stops);
         // only this thread removes requests from the queue
@@ -393,79 +568,472 @@ void worker_loop(rbffd_server* S)
             } else {
                 ++it;
             }
-        // admission in arrival order
-        while (!S->stop && !S->pending.empty() && (S->max_active <= 0 || (int)S->active.size() < S->max_active)) {
-            std::shared_ptr<Request> r = S->pending.front();
-            int rc;
-            bool reused = false;
-            if (S->inject_fail > 0) {
-                S->inject_fail--;
-                rc = set_error(S->ctx, RBFFD_ERR_OOM, "injected admission failure");
-            } else {
-                const bool nothing_active = S->active.empty();
-                lk.unlock();
-                rc = admit(S, *r, nothing_active, &reused);
-                lk.lock();
-            }
-            if (rc == ADMIT_WAIT) break;
+        if (S->stop) break;
+        const int running = (int)(S->active.size() + S->ready.size());
+        if (S->pending.empty() || (S->max_active > 0 && running >= S->max_active)) {
+            S->cv_admit.wait(lk);
+            continue;
+        }
+        std::shared_ptr<Request> r = S->pending.front();
+        if (S->inject_fail > 0) {
+            S->inject_fail--;
             S->pending.pop_front();
-            if (rc != RBFFD_OK) {
-                finish_request(*r, rc);
-                S->st.failed++;
-                S->cv_done.notify_all();
+            finish_request(*r, set_error(S->ctx, RBFFD_ERR_OOM, "injected admission failure"));
+            S->st.failed++;
+            S->cv_done.notify_all();
+            continue;
+        }
+        rbffd_grid* g = r->p.grid;
+        const size_t io_bytes = (size_t)g->N * sizeof(double);
+        Bank* bank = nullptr;
+        for (auto& b : S->banks)
+            if (bank_fits(*b, *r) && b->members < b->Wcap) {
+                bank = b.get();
+                break;
+            }
+        const size_t need = io_bytes + (bank ? 0 : bank_bytes(g, r->p.pde));
+        if (ctx_held(S->ctx) + need > S->budget) {
+            size_t k = S->banks.size();  // the idle bank that has been idle longest
+            for (size_t q = 0; q < S->banks.size(); q++)
+                if (S->banks[q].get() != bank && S->banks[q]->members == 0 && !S->banks[q]->in_plan &&
+                    (k == S->banks.size() || S->banks[q]->idle_since < S->banks[k]->idle_since))
+                    k = q;
+            if (k < S->banks.size()) {
+                std::unique_ptr<Bank> b = std::move(S->banks[k]);
+                S->banks.erase(S->banks.begin() + (long)k);
+                S->owned -= std::min(S->owned, b->bytes);
+                lk.unlock();
+                bank_free_memory(S->ctx, *b);
+                lk.lock();
                 continue;
             }
-            r->admitted = true;
-            r->t_admit = Clock::now();
-            if (reused) S->st.slots_reused++;
-            S->active.push_back(r);
-            S->st.max_active_seen = std::max<long long>(S->st.max_active_seen, (long long)S->active.size());
-            changed = true;
+            if (running > 0) {  // memory frees up when a running request finishes
+                S->cv_admit.wait(lk);
+                continue;
+            }
+            S->pending.pop_front();
+            finish_request(*r, set_error(S->ctx, RBFFD_ERR_BUDGET,
+                                         "request needing %zu bytes does not fit the budget of %zu bytes", need,
+                                         S->budget));
+            S->st.failed++;
+            S->cv_done.notify_all();
+            continue;
         }
-        if (S->active.empty()) {
-            if (S->stop && S->pending.empty()) break;
+        S->owned += need;  // reserved before allocating: submissions meanwhile count it as the server's
+        if (bank) bank->members++;
+        lk.unlock();
+        int rc = RBFFD_OK;
+        std::unique_ptr<Bank> fresh;
+        if (!bank) {
+            fresh.reset(new (std::nothrow) Bank());
+            rc = fresh ? bank_create(S, *r, *fresh) : RBFFD_ERR_OOM;
+        }
+        double* io = nullptr;
+        if (rc == RBFFD_OK) {
+            cudaError_t e = cudaMallocAsync((void**)&io, io_bytes, S->astream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(io, r->u0.data(), io_bytes, cudaMemcpyHostToDevice, S->astream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(S->astream);
+            if (e != cudaSuccess) {
+                rc = cuda_error(S->ctx, e, "request upload");
+                if (io) cudaFreeAsync(io, S->astream);
+                io = nullptr;
+            } else {
+                ctx_account(S->ctx, io_bytes, 0);
+            }
+        }
+        if (rc != RBFFD_OK && fresh) bank_free_memory(S->ctx, *fresh);  // no-op after a failed bank_create
+        lk.lock();
+        S->pending.pop_front();  // still r: only this thread removes from the queue
+        if (rc != RBFFD_OK) {
+            S->owned -= std::min(S->owned, need);
+            if (bank && --bank->members == 0) bank->idle_since = Clock::now();
+            finish_request(*r, rc);
+            S->st.failed++;
+            S->cv_done.notify_all();
+            continue;
+        }
+        if (!bank) {
+            bank = fresh.get();
+            bank->members = 1;
+            S->banks.push_back(std::move(fresh));
+        } else {
+            S->st.slots_reused++;
+        }
+        r->bank = bank;
+        r->d_io = io;
+        r->admitted = true;
+        r->t_admit = Clock::now();
+        S->ready.push_back(r);
+        S->cv_work.notify_one();
+    }
+    S->admitter_done = true;
+    S->cv_work.notify_all();
+}
+
+template <typename T>
+void fill_desc(BankDesc<T>& d, const Bank& b, int block0)
+{
+    const rbffd_grid* g = b.grid;
+    auto W = [&](int k) -> const T* {
+        if (b.op[k] < 0) return nullptr;
+        return std::is_same<T, double>::value ? (const T*)g->d_w64[b.op[k]] : (const T*)g->d_w32[b.op[k]];
+    };
+    d.idx = g->d_idx;
+    d.w0 = b.wf ? (const T*)b.wf : W(0);
+    d.w1 = b.wf ? nullptr : W(1);
+    d.w2 = b.wf ? nullptr : W(2);
+    d.cu = (const T*)b.cu;
+    d.cv = (const T*)b.cv;
+    d.u = (T*)b.u;
+    d.xa = (T*)b.xa;
+    d.xb = (T*)b.xb;
+    d.acc = (T*)b.acc;
+    for (int v = 0; v < BANK_W_MAX; v++) {
+        const Request* r = v < b.W ? b.cols[v] : nullptr;
+        const bool on = r != nullptr;
+        // the stage coefficients of rbffd_pde_advance; free columns hold zeros and stay zero
+        const double dt = on ? r->p.dt : 0.0;
+        d.c[0][v] = (T)(0.5 * dt);
+        d.c[1][v] = (T)(0.5 * dt);
+        d.c[2][v] = (T)(1.0 * dt);
+        d.c[3][v] = (T)(dt / 6.);
+        // a fused operator is applied as f = 1 * (Wf u)
+        d.kappa[v] = on ? (b.wf ? T(1) : (T)r->p.pde.kappa) : T(0);
+    }
+    d.hrows = b.halo ? b.halo->d_rows : nullptr;
+    d.hptr = b.halo ? b.halo->d_ptr : nullptr;
+    d.hnodes = b.halo ? b.halo->d_nodes : nullptr;
+    d.lidx = b.halo ? b.halo->d_lidx : nullptr;
+    d.N = g->N;
+    d.nc = g->nc;
+    d.kind = b.wf ? KIND_HEAT : b.kind;
+    d.block0 = block0;
+}
+
+// One kernel launch per stage: the banks of one dtype, width and operator count.
+struct Launch {
+    int dtype = 0, W = 1, nops = 1, tiled = 0, nbanks = 0, blocks = 0;
+    size_t off = 0;      // byte offset of its bank table
+    size_t smem = 0;     // dynamic shared memory (tiled launches)
+    double bytes = 0.0;  // algorithmic bytes per stage
+};
+
+inline size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+// Lay out the bank tables of every launch for the banks with active columns
+// and upload them, stream-ordered before the launches that read them (the
+// previous batch has completed, so the pinned host copy is free to rewrite).
+// Called with S->mu held (reads bank membership); the copy is asynchronous.
+int upload_tables(rbffd_server* S, std::vector<Launch>& plan)
+{
+    plan.clear();
+    for (auto& b : S->banks) b->in_plan = false;
+    std::vector<Bank*> bs;
+    for (auto& b : S->banks) {
+        bool any = false;
+        for (const Request* r : b->cols) any |= r != nullptr;
+        if (any) bs.push_back(b.get());
+    }
+    std::vector<std::vector<Bank*>> per_launch;
+    size_t off = 0;
+    for (int dt = 0; dt < 2; dt++)
+        for (int W : {1, 2, 4, 8})
+            for (int no = 1; no <= 3; no++)
+            for (int ti = 0; ti < 2; ti++) {
+                std::vector<Bank*> sel;
+                for (Bank* b : bs)
+                    if (b->dtype == (dt ? RBFFD_F64 : RBFFD_F32) && b->W == W && (b->wf ? 1 : b->nops) == no &&
+                        (b->halo != nullptr) == (ti == 1))
+                        sel.push_back(b);
+                if (sel.empty()) continue;
+                Launch L;
+                L.dtype = dt ? RBFFD_F64 : RBFFD_F32;
+                L.W = W;
+                L.nops = no;
+                L.tiled = ti;
+                for (Bank* b : sel)
+                    if (ti) L.smem = std::max(L.smem, (size_t)b->halo->max_halo * W * (dt ? 8 : 4));
+                L.nbanks = (int)sel.size();
+                L.off = off;
+                off = align256(off + sel.size() * (dt ? sizeof(BankDesc<double>) : sizeof(BankDesc<float>)));
+                plan.push_back(L);
+                per_launch.push_back(sel);
+            }
+    if (off > S->tab_cap) {
+        const size_t cap = std::max<size_t>(off * 2, TABLE_BYTES0);
+        if (S->h_tab) cudaFreeHost(S->h_tab);
+        dev_free(S->ctx, S->d_tab, S->tab_cap);
+        S->h_tab = nullptr;
+        S->d_tab = nullptr;
+        S->tab_cap = 0;
+        RBFFD_CUDA_TRY(S->ctx, cudaMallocHost(&S->h_tab, cap));
+        const int rc = dev_alloc(S->ctx, &S->d_tab, cap);
+        if (rc) return rc;
+        S->tab_cap = cap;
+    }
+    char* h = (char*)S->h_tab;
+    for (size_t l = 0; l < plan.size(); l++) {
+        Launch& L = plan[l];
+        for (size_t q = 0; q < per_launch[l].size(); q++) {
+            Bank* b = per_launch[l][q];
+            b->in_plan = true;
+            if (L.dtype == RBFFD_F64) fill_desc(((BankDesc<double>*)(h + L.off))[q], *b, L.blocks);
+            else fill_desc(((BankDesc<float>*)(h + L.off))[q], *b, L.blocks);
+            L.blocks += L.tiled ? b->halo->nblocks : (b->grid->N + SEG_ROWS - 1) / SEG_ROWS;
+            const double wb = L.dtype == RBFFD_F64 ? 8.0 : 4.0, ib = L.tiled ? 2.0 : 4.0;
+            const bool coef = b->kind == KIND_ADVECT && !b->wf;
+            L.bytes += (double)b->grid->N * (b->grid->n_pad * (L.nops * wb + ib) + wb * (4.0 * b->W + (coef ? 2.0 : 0.0)));
+        }
+    }
+    if (off) RBFFD_CUDA_TRY(S->ctx, cudaMemcpyAsync(S->d_tab, S->h_tab, off, cudaMemcpyHostToDevice, S->stream));
+    return RBFFD_OK;
+}
+
+template <typename T, int W, int NOPS>
+void launch_bank(const Launch& L, const BankDesc<T>* d, int stage, cudaStream_t s)
+{
+    if (L.tiled) k_stage_bank_tile<T, W, NOPS><<<L.blocks, SEG_ROWS, L.smem, s>>>(d, L.nbanks, stage);
+    else k_stage_bank<T, W, NOPS><<<L.blocks, SEG_ROWS, 0, s>>>(d, L.nbanks, stage);
+}
+
+template <typename T, int W>
+void launch_bank_w(const Launch& L, const BankDesc<T>* d, int stage, cudaStream_t s)
+{
+    switch (L.nops) {
+    case 1: launch_bank<T, W, 1>(L, d, stage, s); break;
+    case 2: launch_bank<T, W, 2>(L, d, stage, s); break;
+    default: launch_bank<T, W, 3>(L, d, stage, s); break;
+    }
+}
+
+// Allow the tiled instantiations TILE_SMEM_MAX of dynamic shared memory on the current device.
+template <typename T, int W>
+cudaError_t tile_attrs_w()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_stage_bank_tile<T, W, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TILE_SMEM_MAX);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_stage_bank_tile<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TILE_SMEM_MAX);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_stage_bank_tile<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TILE_SMEM_MAX);
+    return e;
+}
+
+cudaError_t tile_attrs()
+{
+    cudaError_t e = tile_attrs_w<float, 1>();
+    if (e == cudaSuccess) e = tile_attrs_w<float, 2>();
+    if (e == cudaSuccess) e = tile_attrs_w<float, 4>();
+    if (e == cudaSuccess) e = tile_attrs_w<float, 8>();
+    if (e == cudaSuccess) e = tile_attrs_w<double, 1>();
+    if (e == cudaSuccess) e = tile_attrs_w<double, 2>();
+    if (e == cudaSuccess) e = tile_attrs_w<double, 4>();
+    return e;
+}
+
+void launch_stage(const Launch& L, char* d, int stage, cudaStream_t s)
+{
+    if (L.dtype == RBFFD_F64) {
+        const BankDesc<double>* t = (const BankDesc<double>*)(d + L.off);
+        switch (L.W) {
+        case 1: launch_bank_w<double, 1>(L, t, stage, s); break;
+        case 2: launch_bank_w<double, 2>(L, t, stage, s); break;
+        default: launch_bank_w<double, 4>(L, t, stage, s); break;
+        }
+    } else {
+        const BankDesc<float>* t = (const BankDesc<float>*)(d + L.off);
+        switch (L.W) {
+        case 1: launch_bank_w<float, 1>(L, t, stage, s); break;
+        case 2: launch_bank_w<float, 2>(L, t, stage, s); break;
+        case 4: launch_bank_w<float, 4>(L, t, stage, s); break;
+        default: launch_bank_w<float, 8>(L, t, stage, s); break;
+        }
+    }
+}
+
+// Issue nsteps RK4 steps for the planned banks; returns after they complete.
+int run_steps(rbffd_server* S, const std::vector<Launch>& plan, int nsteps, double* seconds, long long* launches,
+              double* bytes)
+{
+    char* d = (char*)S->d_tab;
+    for (const Launch& L : plan) *bytes += 4.0 * nsteps * L.bytes;
+    RBFFD_CUDA_TRY(S->ctx, cudaEventRecord(S->ev0, S->stream));
+    for (int step = 0; step < nsteps; step++)
+        for (int stage = 0; stage < 4; stage++)
+            for (const Launch& L : plan) {
+                launch_stage(L, d, stage, S->stream);
+                ++*launches;
+            }
+    RBFFD_CUDA_TRY(S->ctx, cudaGetLastError());
+    RBFFD_CUDA_TRY(S->ctx, cudaEventRecord(S->ev1, S->stream));
+    RBFFD_CUDA_TRY(S->ctx, cudaEventSynchronize(S->ev1));
+    float ms = 0.f;
+    RBFFD_CUDA_TRY(S->ctx, cudaEventElapsedTime(&ms, S->ev0, S->ev1));
+    *seconds = ms * 1e-3;
+    return RBFFD_OK;
+}
+
+// New layout of a bank whose membership changed: its remaining requests in
+// order, then the joining ones, in columns 0..K-1 at stride K rounded up to a
+// power of two (written into xa, which is free between steps, then swapped
+// with u).  Stepping thread, between batches.
+template <typename T>
+void bank_repack(Bank& b, cudaStream_t s)
+{
+    std::vector<Request*> keep;
+    std::vector<int> from;
+    for (int c = 0; c < (int)b.cols.size(); c++)
+        if (b.cols[c]) {
+            keep.push_back(b.cols[c]);
+            from.push_back(c);
+        }
+    for (Request* r : b.join) {
+        keep.push_back(r);
+        from.push_back(FROM_IO);
+    }
+    b.join.clear();
+    b.dirty = false;
+    const int K = (int)keep.size();
+    if (K == 0) {
+        b.cols.clear();
+        return;
+    }
+    int W = 1;
+    while (W < K) W *= 2;
+    Repack<T> a;
+    a.dst = (T*)b.xa;
+    a.src = (const T*)b.u;
+    a.wsrc = b.W;
+    a.wdst = W;
+    a.N = b.grid->N;
+    a.perm = b.grid->d_perm;
+    for (int c = 0; c < BANK_W_MAX; c++) {
+        a.from[c] = c < K ? from[c] : FROM_ZERO;
+        a.io[c] = c < K ? keep[c]->d_io : nullptr;
+    }
+    k_repack<T><<<(a.N + 255) / 256, 256, 0, s>>>(a);
+    std::swap(b.u, b.xa);
+    b.W = W;
+    b.cols.assign(W, nullptr);
+    for (int c = 0; c < K; c++) {
+        b.cols[c] = keep[c];
+        keep[c]->col = c;
+        keep[c]->inserted = true;
+    }
+}
+
+template <typename T>
+void column_out(const Request& r, cudaStream_t s)
+{
+    const Bank& b = *r.bank;
+    const int N = b.grid->N;
+    k_column_out<T><<<(N + 255) / 256, 256, 0, s>>>((const T*)b.u, b.W, r.col, r.d_io, b.grid->d_perm, N);
+}
+
+// A leaving request: read its column out into its I/O buffer and,
+// unless it was cancelled, copy the result to the caller; free the buffer.
+int column_leave(rbffd_server* S, Request& r, bool copy_out)
+{
+    if (r.inserted) {
+        if (r.bank->dtype == RBFFD_F64) column_out<double>(r, S->stream);
+        else column_out<float>(r, S->stream);
+    }
+    const size_t io_bytes = (size_t)r.p.grid->N * sizeof(double);
+    int rc = RBFFD_OK;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && copy_out) e = cudaMemcpyAsync(r.p.out, r.d_io, io_bytes, cudaMemcpyDeviceToHost, S->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+    if (e != cudaSuccess) rc = cuda_error(S->ctx, e, "request result");
+    cudaFreeAsync(r.d_io, S->stream);
+    r.d_io = nullptr;
+    ctx_account(S->ctx, 0, io_bytes);
+    return rc;
+}
+
+// Stepping thread: admitted requests join at step boundaries; batches of RK4
+// steps for every bank with active columns.
+void worker_loop(rbffd_server* S)
+{
+    cudaSetDevice(S->ctx->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    bool changed = true;
+    std::vector<Launch> plan;
+    for (;;) {
+        const bool hold = S->paused && !S->stop;
+        std::vector<std::shared_ptr<Request>> joining;
+        if (!hold) {
+            joining.swap(S->ready);
+            for (auto& r : joining) S->active.push_back(r);
+            S->st.max_active_seen = std::max<long long>(S->st.max_active_seen, (long long)S->active.size());
+        }
+        if (S->active.empty() || hold) {
+            if (S->active.empty()) {
+                for (auto& b : S->banks) b->in_plan = false;  // no batch in flight
+                if (S->stop && S->admitter_done && S->ready.empty()) break;
+            }
             S->cv_work.wait(lk);
             continue;
         }
-        // one batch of steps for every active request
+        for (auto& r : joining) {
+            r->bank->join.push_back(r.get());
+            r->bank->dirty = true;
+        }
+        std::vector<Bank*> dirty;  // banks with requests (not freeable meanwhile) whose membership changed
+        for (auto& b : S->banks)
+            if (b->dirty) {
+                if (b->members > 0) dirty.push_back(b.get());
+                else bank_repack<float>(*b, S->stream);  // no request left: just forget the layout
+            }
+        lk.unlock();
+        int rc = RBFFD_OK;
+        for (Bank* b : dirty) {  // new layouts and initial states, before the batch
+            if (b->dtype == RBFFD_F64) bank_repack<double>(*b, S->stream);
+            else bank_repack<float>(*b, S->stream);
+        }
+        if (!dirty.empty()) {
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) rc = cuda_error(S->ctx, e, "bank repack");
+        }
+        lk.lock();
+        changed |= !dirty.empty();
         std::vector<std::shared_ptr<Request>> act = S->active;
         int nsteps = TICK_MAX_STEPS;
         if (S->step_s > 0.0) nsteps = std::max(1, std::min(TICK_MAX_STEPS, (int)(TICK_TARGET_S / S->step_s)));
         for (auto& r : act) nsteps = std::min(nsteps, r->p.nsteps - r->steps_done);
-        lk.unlock();
-        int rc = RBFFD_OK;
-        if (changed) {
-            rc = upload_tables(S, act, tab);
+        if (changed && rc == RBFFD_OK) {
+            rc = upload_tables(S, plan);
             changed = false;
         }
-        double secs = 0.0;
+        lk.unlock();
+        double secs = 0.0, bytes = 0.0;
         long long launches = 0;
-        if (rc == RBFFD_OK) rc = run_steps(S, tab, nsteps, &secs, &launches);
+        if (rc == RBFFD_OK) rc = run_steps(S, plan, nsteps, &secs, &launches, &bytes);
         if (rc == RBFFD_OK) S->step_s = secs / nsteps;
         double nu = 0.0;
         std::vector<std::shared_ptr<Request>> left;
         for (auto& r : act) {
             r->steps_done += nsteps;
-            nu += (double)r->pde->g->N * nsteps;
+            nu += (double)r->p.grid->N * nsteps;
             bool cancel;
             {
                 std::lock_guard<std::mutex> g(S->mu);
                 cancel = r->cancel;
             }
+            int st;
             if (rc != RBFFD_OK) {
-                retire_pde(S, *r, false);
-                r->status = rc;
+                st = rc;
+                column_leave(S, *r, false);
             } else if (cancel) {
-                retire_pde(S, *r, true);
-                r->status = RBFFD_ERR_CANCELLED;
+                st = RBFFD_ERR_CANCELLED;
+                column_leave(S, *r, false);
             } else if (r->steps_done >= r->p.nsteps) {
-                r->pde->t = r->p.dt * r->p.nsteps;
-                const int grc = rbffd_pde_get_state(r->pde, r->p.out);
-                retire_pde(S, *r, grc == RBFFD_OK);
-                r->status = grc;
+                st = column_leave(S, *r, true);
             } else {
                 continue;
             }
+            r->status = st;
             left.push_back(r);
         }
         lk.lock();
@@ -473,15 +1041,29 @@ void worker_loop(rbffd_server* S)
         S->st.launches += launches;
         S->st.node_updates += nu;
         S->st.gpu_busy_s += secs;
-        for (auto& r : left) {
-            finish_request(*r, r->status);
-            if (r->status == RBFFD_OK) S->st.completed++;
-            else if (r->status == RBFFD_ERR_CANCELLED) S->st.cancelled++;
+        S->st.stage_bytes += bytes;
+        for (auto& rp : left) {
+            Request& r = *rp;
+            Bank* b = r.bank;
+            b->cols[r.col] = nullptr;
+            b->dirty = true;
+            S->owned -= std::min(S->owned, (size_t)r.p.grid->N * sizeof(double));
+            if (--b->members == 0) {
+                b->idle_since = Clock::now();
+                b->in_plan = false;  // the next batch uses tables rebuilt without it
+            }
+            r.bank = nullptr;
+            finish_request(r, r.status);
+            if (r.status == RBFFD_OK) S->st.completed++;
+            else if (r.status == RBFFD_ERR_CANCELLED) S->st.cancelled++;
             else S->st.failed++;
-            S->active.erase(std::find(S->active.begin(), S->active.end(), r));
+            S->active.erase(std::find(S->active.begin(), S->active.end(), rp));
             changed = true;
         }
-        if (!left.empty()) S->cv_done.notify_all();
+        if (!left.empty()) {
+            S->cv_done.notify_all();
+            S->cv_admit.notify_one();  // columns and memory to admit the next requests
+        }
     }
 }
 
@@ -499,25 +1081,30 @@ extern "C" int rbffd_server_start(rbffd_ctx* ctx, double hbm_fraction, int max_a
     S->ctx = ctx;
     S->budget = (size_t)(hbm_fraction * (double)total_b);
     S->max_active = max_active > 0 ? max_active : 0;
-    // segment tables for a few hundred active requests, held from the start so
-    // that they count against the budget before the first admission
+    // bank tables for a few hundred banks, held from the start so that they
+    // count against the budget before the first admission
     const size_t tab = TABLE_BYTES0;
     cudaError_t e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->astream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev1);
     if (e == cudaSuccess) e = cudaMallocHost(&S->h_tab, tab);
+    if (e == cudaSuccess) e = tile_attrs();
     int rc = e == cudaSuccess ? RBFFD_OK : cuda_error(ctx, e, "rbffd_server_start");
     if (rc == RBFFD_OK && (rc = dev_alloc(ctx, &S->d_tab, tab)) == RBFFD_OK) S->tab_cap = tab;
     if (rc != RBFFD_OK) {
+        dev_free(ctx, S->d_tab, S->tab_cap);
         if (S->h_tab) cudaFreeHost(S->h_tab);
         if (S->ev0) cudaEventDestroy(S->ev0);
         if (S->ev1) cudaEventDestroy(S->ev1);
+        if (S->astream) cudaStreamDestroy(S->astream);
         if (S->stream) cudaStreamDestroy(S->stream);
         delete S;
         return rc;
     }
     S->st.budget_bytes = (double)S->budget;
     S->worker = std::thread(worker_loop, S);
+    S->admitter = std::thread(admission_loop, S);
     *out = S;
     return RBFFD_OK;
 }
@@ -548,7 +1135,8 @@ extern "C" int rbffd_server_submit(rbffd_server* S, const rbffd_request* req, ui
     for (int b = 0; b < 16; b++)
         if ((ops >> b & 1u) && !g->d_w64[b])
             return set_error(ctx, RBFFD_ERR_STATE, "weights of operator 0x%x are not on the device", 1u << b);
-    const size_t need = pde_bytes(g, &p);
+    // the most a request can add: a new bank and its I/O buffer
+    const size_t need = bank_bytes(g, p) + (size_t)g->N * sizeof(double);
     auto r = std::make_shared<Request>();
     r->p = *req;
     const int N = g->N;
@@ -556,18 +1144,15 @@ extern "C" int rbffd_server_submit(rbffd_server* S, const rbffd_request* req, ui
     if (p.rhs_kind == RBFFD_RHS_ADVECTION) {
         r->cu.assign(p.cu, p.cu + N);
         r->cv.assign(p.cv, p.cv + N);
-        r->p.pde.cu = r->cu.data();
-        r->p.pde.cv = r->cv.data();
-    } else {
-        r->p.pde.cu = r->p.pde.cv = nullptr;
     }
+    r->p.pde.cu = r->p.pde.cv = nullptr;
     r->p.u0 = r->u0.data();
     std::lock_guard<std::mutex> lk(S->mu);
     if (S->stop) return set_error(ctx, RBFFD_ERR_STATE, "server is stopping");
     // memory the server cannot free (grids, the caller's own PDEs) plus this request
     const size_t held = ctx_held(ctx);
     if (held - std::min(held, S->owned) + need > S->budget)
-        return set_error(ctx, RBFFD_ERR_BUDGET, "request of %zu bytes can never fit the budget of %zu bytes", need,
+        return set_error(ctx, RBFFD_ERR_BUDGET, "request needing %zu bytes can never fit the budget of %zu bytes", need,
                          S->budget);
     r->id = S->next_id++;
     r->t_submit = Clock::now();
@@ -580,7 +1165,7 @@ extern "C" int rbffd_server_submit(rbffd_server* S, const rbffd_request* req, ui
         S->st.completed++;
     } else {
         S->pending.push_back(r);
-        S->cv_work.notify_one();
+        S->cv_admit.notify_one();
     }
     S->all[r->id] = r;
     *id = r->id;
@@ -619,7 +1204,7 @@ extern "C" int rbffd_server_wait_idle(rbffd_server* S, double timeout_s)
     if (!S || !(timeout_s >= 0.0)) return RBFFD_ERR_INVALID;
     std::unique_lock<std::mutex> lk(S->mu);
     if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
-                             [&] { return S->pending.empty() && S->active.empty(); }))
+                             [&] { return S->pending.empty() && S->ready.empty() && S->active.empty(); }))
         return RBFFD_ERR_TIMEOUT;
     return RBFFD_OK;
 }
@@ -633,6 +1218,7 @@ extern "C" int rbffd_server_cancel(rbffd_server* S, uint64_t id)
     std::shared_ptr<Request> r = it->second;
     if (r->done) return RBFFD_OK;
     r->cancel = true;
+    S->cv_admit.notify_one();
     S->cv_work.notify_one();
     S->cv_done.wait(lk, [&] { return r->done != 0; });
     return RBFFD_OK;
@@ -644,8 +1230,17 @@ extern "C" int rbffd_server_get_stats(rbffd_server* S, rbffd_server_stats* out)
     std::lock_guard<std::mutex> lk(S->mu);
     *out = S->st;
     out->pending = (long long)S->pending.size();
-    out->active = (long long)S->active.size();
+    out->active = (long long)(S->active.size() + S->ready.size());
     out->held_bytes = (double)ctx_held(S->ctx);
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_server_pause(rbffd_server* S, int paused)
+{
+    if (!S) return RBFFD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->paused = paused != 0;
+    S->cv_work.notify_all();
     return RBFFD_OK;
 }
 
@@ -661,19 +1256,25 @@ extern "C" int rbffd_server_stop(rbffd_server* S)
 {
     if (!S) return RBFFD_ERR_INVALID;
     {
-        // the worker cancels the pending requests and finishes the active ones
+        // the admission thread cancels the pending requests; the stepping thread
+        // finishes the admitted ones
         std::lock_guard<std::mutex> lk(S->mu);
         S->stop = true;
     }
+    S->cv_admit.notify_all();
     S->cv_work.notify_all();
+    if (S->admitter.joinable()) S->admitter.join();
     if (S->worker.joinable()) S->worker.join();
     cudaSetDevice(S->ctx->device);
-    while (!S->slots.empty()) drop_slot(S, S->slots.size() - 1);
     cudaStreamSynchronize(S->stream);
+    cudaStreamSynchronize(S->astream);
+    for (auto& b : S->banks) bank_free_memory(S->ctx, *b);
+    S->banks.clear();
     if (S->h_tab) cudaFreeHost(S->h_tab);
     dev_free(S->ctx, S->d_tab, S->tab_cap);
     cudaEventDestroy(S->ev0);
     cudaEventDestroy(S->ev1);
+    cudaStreamDestroy(S->astream);
     cudaStreamDestroy(S->stream);
     delete S;
     return RBFFD_OK;

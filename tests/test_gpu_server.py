@@ -3,8 +3,9 @@
 * FP64 served requests equal the oracle's RK4 (TimeDependentPDE::advanceRungeKutta4,
   time_dependent_pde.cpp:172-304) bit for bit, heat and cosine bell;
 * every request's result is identical alone and in a mix of grids, stencil
-  sizes, right-hand sides, dtypes and step counts with staggered arrivals, and
-  FP32 results equal the one-lane rbffd_pde_advance result;
+  sizes, right-hand sides, dtypes and step counts with staggered arrivals;
+  FP32 heat results equal the one-lane rbffd_pde_advance result, FP32
+  advection (one fused operator per bank) is within 1e-5 of the FP64 oracle;
 * admission: a request that can never fit the HBM budget is refused at
   submission; a budget with room for one request runs them one at a time;
 * cancellation (pending and active), injected admission failures, malformed
@@ -17,7 +18,7 @@ import pytest
 
 import oracle as O
 import rbffd_gpu_b200 as R
-from tests.helpers import sphere_problem, cosine_bell_setup
+from tests.helpers import sphere_problem, cosine_bell_setup, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -131,6 +132,29 @@ def test_alone_and_in_mix_identical(ctx, grids):
         srv.stop()
 
 
+def test_many_requests_on_one_grid_share_launches_bit_exact(ctx, grids):
+    """11 FP64 requests on one grid: groups of up to 8 read the operators once
+    per row for all members; each member still equals the oracle bit for bit."""
+    g = grids[0]
+    srv = R.Server(ctx)
+    try:
+        specs = [(_heat_u0(g, 20 + k), 1.0 + 0.05 * k, 5 + 3 * k) for k in range(11)]
+        srv.pause()  # all 11 are admitted before the first batch: one group of 8 and one of 3
+        ids = [srv.submit(g["grid"], R.heat_params(kap, R.F64), u, 1e-5, steps) for u, kap, steps in specs]
+        t0 = time.time()
+        while any(srv.poll(i)[3] < 0 for i in ids) and time.time() - t0 < 30:
+            time.sleep(0.001)
+        assert srv.stats()["ticks"] == 0
+        srv.pause(False)
+        srv.wait_idle(60)
+        for (u, kap, steps), rid in zip(specs, ids):
+            ref = O.rk4_heat(g["st"], None, g["W"][O.LSFC], u, 1e-5, steps, kappa=kap)
+            assert np.array_equal(srv.result(rid), ref), (kap, steps)
+        assert srv.stats()["max_active_seen"] == 11
+    finally:
+        srv.stop()
+
+
 def test_served_fp32_equals_one_lane_pde_path(ctx, grids):
     g = grids[1]
     u0 = _heat_u0(g, 3)
@@ -150,8 +174,38 @@ def test_served_fp32_equals_one_lane_pde_path(ctx, grids):
     assert np.array_equal(served, ref)
 
 
+def test_served_fp32_advection_fused_operator(ctx, grids):
+    """FP32 advection banks apply one fused operator per bank,
+    Wf = -(cu W_lambda + cv W_theta) + W_hv formed in FP64 and rounded once to
+    FP32: within 1e-5 relative L2 of the FP64 oracle after 30 steps, and
+    identical whether the request runs alone or beside others in its bank.
+    (dt/20: these weights, eps = 0.035 sqrt(N), carry growing modes that
+    amplify any rounding difference over full cosine-bell steps.)"""
+    g = grids[1]
+    dt = BELL["dt"] / 20
+    u_b = [_bell_u0(g, 30 + k) for k in range(3)]
+    srv = R.Server(ctx)
+    try:
+        alone = srv.submit(g["grid"], _bell_params(R.F32), u_b[0], dt, 30)
+        assert srv.wait(alone) == 0
+        srv.pause()
+        ids = [srv.submit(g["grid"], _bell_params(R.F32), u, dt, 30) for u in u_b]
+        while any(srv.poll(i)[3] < 0 for i in ids):
+            time.sleep(0.001)
+        srv.pause(False)
+        srv.wait_idle(60)
+        assert np.array_equal(srv.result(ids[0]), srv.result(alone))
+        cu, cv = O.cosine_bell_coeffs(g["xyz"], a=BELL["a"], alpha=BELL["alpha"], u0=BELL["u0"])
+        for u, rid in zip(u_b, ids):
+            ref = O.rk4_advect(g["st"], None, g["W"][O.LAMBDA], g["W"][O.THETA], g["W"][O.HV], cu, cv, u, dt, 30)
+            assert rel_l2(srv.result(rid), ref) < 1e-5
+    finally:
+        srv.stop()
+
+
 def _need_fp32_heat(N):
-    return N * (4 * 4 + 8)  # u, xa, xb, acc + FP64 staging
+    """Device bytes of a new FP32 heat bank (u, xa, xb, acc of 8 columns) and one I/O buffer."""
+    return N * (4 * 8 * 4 + 8)
 
 
 def test_request_that_can_never_fit_is_refused(ctx, grids):
@@ -169,8 +223,9 @@ def test_request_that_can_never_fit_is_refused(ctx, grids):
 def test_budget_for_one_request_serialises_admission(ctx, grids):
     g = grids[1]
     held, _, total = ctx.mem_info()
-    # room for the server's segment table (64 KiB) and one request's buffers, not two
-    srv = R.Server(ctx, hbm_fraction=(held + 65536 + 1.5 * _need_fp32_heat(g["N"])) / total)
+    # room for the server's bank table (64 KiB), one bank and one request's I/O
+    # buffer (8 N bytes), not two: the next request waits for the first to leave
+    srv = R.Server(ctx, hbm_fraction=(held + 65536 + _need_fp32_heat(g["N"]) + 4 * g["N"]) / total)
     try:
         u0 = [_heat_u0(g, k) for k in range(3)]
         ids = [srv.submit(g["grid"], R.heat_params(1.0, R.F32), u, 1e-5, 20) for u in u0]
