@@ -367,6 +367,7 @@ def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
     pplain.close()
     out["multitracer"] = bench_multitracer(R, torch, ctx)
     out["serving"] = bench_serving(R, torch, ctx)
+    out["weights"] = bench_weights(R, torch, ctx)
     return out
 
 
@@ -430,6 +431,84 @@ def bench_multitracer(R, torch, ctx):
     out["rel_l2_fp64_vs_exact"] = float(np.linalg.norm(u64 - exact) / np.linalg.norm(exact))
     grid.close()
     return out
+
+
+WEIGHTS = dict(name="batched_weights_1e6_mixed_n17_31_50_101", N=1_000_000, sizes=(17, 31, 50, 101),
+               degs=(1, 2, 3, 4), eps=(2.0, 8.0), seed=3, cpu_sample=20000)
+
+
+def weights_flops(m):
+    """FP64 flops of one m x m system with three right-hand sides: m^2/2
+    kernel evaluations, 2/3 m^3 for the LU factorisation, 2 m^2 per solve."""
+    return m * m / 2.0 + 2.0 * m ** 3 / 3.0 + 6.0 * m * m
+
+
+def bench_weights(R, torch, ctx):
+    """Batched FP64 stencil weights: 1e6 stencils, n uniform over {17, 31, 50,
+    101} with polynomial degree {1, 2, 3, 4} matched to n, eps ~ U[2, 8] per
+    stencil, the three tangential gradient operators XSFC, YSFC, ZSFC, in one
+    call (K1).  Checked over all stencils by polynomial reproduction: the
+    weights differentiate the degree-1 functions x, y, z exactly (to rounding)."""
+    import oracle as O
+    C = WEIGHTS
+    N = C["N"]
+    xyz = R.fibonacci_nodes(N, C["seed"])
+    t0 = time.perf_counter()
+    full = R.knn_stencils(xyz, max(C["sizes"]))
+    t_knn = time.perf_counter() - t0
+    rng = np.random.default_rng(C["seed"])
+    pick = rng.integers(0, len(C["sizes"]), N)
+    lens = np.array(C["sizes"], dtype=np.int32)[pick]
+    degs = np.array(C["degs"], dtype=np.int32)[pick]
+    eps = rng.uniform(C["eps"][0], C["eps"][1], N)
+    psize = {1: 4, 2: 6, 3: 10, 4: 15}  # polynomial terms of each degree (tangent-plane basis above 1)
+    ms = lens + np.array([psize[int(d)] for d in C["degs"]])[pick]
+    flops = float(sum(weights_flops(float(m)) for m in ms))
+    types = R.XSFC | R.YSFC | R.ZSFC
+    grid = R.Grid(ctx, xyz, full, st_len=lens)
+    der = R.RBFFD(types, grid, 2)
+    der.setEpsilon(eps)
+    der.setPolynomialDegree(1, deg_per_row=degs)
+    der.computeAllWeightsForAllStencils()  # first call: autotuning of the team shapes
+    ctx.synchronize()
+    times = []
+    for _ in range(3):
+        t = time.perf_counter()
+        der.computeAllWeightsForAllStencils()
+        ctx.synchronize()
+        times.append(time.perf_counter() - t)
+    best = min(times)
+    # polynomial reproduction: every stencil differentiates constants exactly;
+    # degree-1 stencils ({1, x, y, z}) also x, y, z: Dx_sfc x = 1 - x^2, Dx_sfc y = -x y, ...
+    x, y, z = xyz.T
+    lin = degs == 1
+    worst_const, worst_lin = 0.0, 0.0
+    for t, comp in ((R.XSFC, x), (R.YSFC, y), (R.ZSFC, z)):
+        worst_const = max(worst_const, float(np.abs(der.applyWeightsForDeriv(t, np.ones(N))).max()))
+        for f in (x, y, z):
+            exact = (1.0 if f is comp else 0.0) - comp * f
+            got = der.applyWeightsForDeriv(t, f)
+            worst_lin = max(worst_lin, float(np.abs(got - exact)[lin].max()))
+    grid.close()
+    # CPU: the oracle on a bounded sample of the same mix, all host threads
+    S = C["cpu_sample"]
+    nth = O.max_threads()
+    t = time.perf_counter()
+    O.weights(xyz[:], full[:S], lens[:S], eps[:S], types, dim=2, deg_per_row=degs[:S], nthreads=nth)
+    cpu_s = time.perf_counter() - t
+    cpu_flops = float(sum(weights_flops(float(m)) for m in ms[:S]))
+    return {
+        "workload": C["name"], "stencils": N, "system_sizes_m": sorted(set(int(m) for m in ms)),
+        "seconds": best, "all_runs_s": times, "stencils_per_s": N / best, "fp64_gflops": flops / best / 1e9,
+        "flops_per_call": flops, "knn_s": t_knn,
+        "max_abs_derivative_of_constant": worst_const,
+        "max_abs_reproduction_error_xyz_degree1_rows": worst_lin,
+        "cpu_baseline": {"stencils_per_s": S / cpu_s, "fp64_gflops": cpu_flops / cpu_s / 1e9, "cores": nth,
+                         "kind": "port", "sample": "first %d stencils of the mix, %.1f s, oracle with %d threads" % (
+                             S, cpu_s, nth)},
+        "note": "flops: m^2/2 kernel evaluations + 2/3 m^3 (LU) + 6 m^2 (three solves) per system; m = n + "
+                "polynomial terms (4, 6, 10, 15 for degrees 1-4)",
+    }
 
 
 SERVING = dict(name="serving_poisson200_first128_of_4096", requests=128, stream=4096, rate=200.0, seed=5,

@@ -66,7 +66,23 @@ def build(force=False, verbose=False, ptxas_v=False):
                 sys.stdout.write(out)
     if force or _mtime(LIB) < max(_mtime(o) for o in objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread"])
+    build_drivers(force)
     return LIB
+
+
+CPP = os.path.join(HERE, "cpp")
+# C++ drivers on the C++ API (cpp/rbffd_cuda.hpp), linked against the library
+DRIVERS = {"cosine_bell_cuda": "cosine_bell_main.cpp"}
+
+
+def build_drivers(force=False):
+    hdr = max(_mtime(os.path.join(CPP, "rbffd_cuda.hpp")), _mtime(os.path.join(ROOT, "include", "rbffd_sm100.h")))
+    for exe, src in DRIVERS.items():
+        out = os.path.join(LIBDIR, exe)
+        srcp = os.path.join(CPP, src)
+        if force or _mtime(out) < max(_mtime(srcp), hdr, _mtime(LIB)):
+            _run(["g++", "-O2", "-std=c++17", "-Wall", "-I" + os.path.join(ROOT, "include"), "-I" + CPP, srcp,
+                  "-L" + LIBDIR, "-lrbffd_sm100", "-Wl,-rpath,$ORIGIN", "-o", out])
 
 
 if __name__ == "__main__":

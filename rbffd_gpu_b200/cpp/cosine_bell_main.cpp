@@ -1,0 +1,102 @@
+// Cosine bell on the sphere through the C++ classes of rbffd_cuda.hpp: the
+// flow of the reference's experiment driver
+// (tests/experiments/cosine_bell_on_sphere/main.cpp:280-515) -- nodes, kNN
+// stencils, RBFFD weights for d/dlambda, d/dtheta and hyperviscosity,
+// CosineBell, fillInitialConditions, advance(RK4, dt) per step, error
+// against the exact solution after whole revolutions.
+//
+// Settings are KEY=VALUE arguments with the reference's test.conf names where
+// it has them: GRID_SIZE, STENCIL_SIZE, NUM_TIMESTEPS (per revolution),
+// NUM_REVOLUTIONS, TIME_FOR_ONE_REVOLUTION, SPHERE_RADIUS, EPSILON_C1,
+// EPSILON_C2, HV_K, HV_GAMMA, USE_HYPERVISCOSITY, plus STEPS (steps to run;
+// default all of the revolutions), POLY_DEG, DTYPE (64 or 32), SEED, GRAPH
+// (1: all steps in one CUDA-graph call) and OUTPUT (file for the final
+// solution, N doubles in node order).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "rbffd_cuda.hpp"
+
+using namespace rbffd_sm100;
+
+int main(int argc, char** argv)
+{
+    std::map<std::string, std::string> cfg;
+    for (int a = 1; a < argc; a++) {
+        const char* eq = std::strchr(argv[a], '=');
+        if (!eq) {
+            std::fprintf(stderr, "usage: %s KEY=VALUE ...\n", argv[0]);
+            return 2;
+        }
+        cfg[std::string(argv[a], eq - argv[a])] = eq + 1;
+    }
+    auto num = [&](const char* k, double dflt) { return cfg.count(k) ? std::atof(cfg[k].c_str()) : dflt; };
+    const int N = (int)num("GRID_SIZE", 4096);
+    const int n = (int)num("STENCIL_SIZE", 31);
+    const double steps_per_rev = num("NUM_TIMESTEPS", 1000);
+    const double revs = num("NUM_REVOLUTIONS", 1);
+    const double T = num("TIME_FOR_ONE_REVOLUTION", 1036800);
+    const double a = num("SPHERE_RADIUS", 1.0);
+    const int steps = (int)num("STEPS", steps_per_rev * revs);
+    const double dt = T / steps_per_rev;
+    const int dtype = num("DTYPE", 64) == 32 ? RBFFD_F32 : RBFFD_F64;
+
+    // nodes: Fibonacci spiral under a seeded rotation; stencils: n nearest neighbours
+    std::vector<double> xyz(3 * (size_t)N);
+    check(nullptr, rbffd_nodes_fibonacci(N, (uint64_t)num("SEED", 1), xyz.data()), "nodes");
+    std::vector<int> st((size_t)N * n);
+    check(nullptr, rbffd_stencils_knn(xyz.data(), N, n, st.data(), nullptr, 0), "stencils");
+    std::vector<Vec3> nodes(N);
+    std::vector<StencilType> stencils(N);
+    for (int i = 0; i < N; i++) {
+        nodes[i] = Vec3{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+        stencils[i].assign(st.begin() + (size_t)i * n, st.begin() + (size_t)(i + 1) * n);
+    }
+
+    Context ctx(0);
+    Grid_CUDA grid(ctx, nodes, stencils);
+    RBFFD_CUDA der(RBFFD_CUDA::LAMBDA | RBFFD_CUDA::THETA, &grid, 2);
+    if (cfg.count("EPSILON_C1")) der.setEpsilonByParameters(num("EPSILON_C1", 0), num("EPSILON_C2", 0));
+    else der.setEpsilonByStencilSize();
+    if (cfg.count("HV_K")) der.setHVScalars((int)num("HV_K", 4), num("HV_GAMMA", 0));
+    const int useHV = (int)num("USE_HYPERVISCOSITY", 1);
+    der.setUseHyperviscosity(useHV);
+    der.setPolynomialDegree((int)num("POLY_DEG", 2));
+    der.computeAllWeightsForAllStencils();
+
+    CosineBell_CUDA pde(&grid, &der, a, M_PI / 2., T, useHV, dtype);
+    std::vector<double> h0(N);
+    check(nullptr, rbffd_exact_cosine_bell(N, xyz.data(), a, h0.data()), "exact solution");
+    pde.fillInitialConditions(h0);
+    if (num("GRAPH", 0) != 0.0) {
+        pde.advance(TimeDependentPDE_CUDA::RK4, dt, steps, true);
+    } else {
+        for (int it = 0; it < steps; it++) pde.advance(TimeDependentPDE_CUDA::RK4, dt);
+    }
+    std::vector<double> h = pde.getLocalSolution();
+
+    // after whole revolutions the exact solution is the initial bell
+    double e2 = 0, r2 = 0, einf = 0, rinf = 0;
+    for (int i = 0; i < N; i++) {
+        e2 += (h[i] - h0[i]) * (h[i] - h0[i]);
+        r2 += h0[i] * h0[i];
+        einf = std::max(einf, std::fabs(h[i] - h0[i]));
+        rinf = std::max(rinf, std::fabs(h0[i]));
+    }
+    std::printf("t = %.6g (%d steps of dt = %.6g), revolutions = %.6g\n", pde.getTime(), steps, dt, steps / steps_per_rev);
+    std::printf("rel L2 = %.6e, rel Linf = %.6e against the initial bell\n", std::sqrt(e2 / r2), einf / rinf);
+    if (cfg.count("OUTPUT")) {
+        FILE* f = std::fopen(cfg["OUTPUT"].c_str(), "wb");
+        if (!f || std::fwrite(h.data(), sizeof(double), N, f) != (size_t)N) {
+            std::fprintf(stderr, "cannot write %s\n", cfg["OUTPUT"].c_str());
+            return 1;
+        }
+        std::fclose(f);
+    }
+    return 0;
+}

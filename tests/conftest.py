@@ -1,3 +1,4 @@
+import glob
 import os
 import sys
 
@@ -13,14 +14,14 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "slow: longer CPU test")
 
 
-def _has_gpu():
-    # Decided from the device nodes, not from the library: on a GPU machine a
-    # missing or broken librbffd_sm100.so must fail the gpu tests, not skip them.
-    return os.path.exists("/dev/nvidia0") or os.path.exists("/dev/nvidiactl")
+def has_gpu():
+    """Decided from the device nodes, not from the library: on a GPU machine a
+    missing or broken librbffd_sm100.so must fail the gpu tests, not skip them."""
+    return os.path.exists("/dev/nvidiactl") or bool(glob.glob("/dev/nvidia[0-9]*"))
 
 
 def pytest_collection_modifyitems(config, items):
-    if _has_gpu():
+    if has_gpu():
         return
     skip = pytest.mark.skip(reason="no CUDA device in this environment")
     for it in items:

@@ -1,4 +1,7 @@
 """Shared problem set-ups for the tests (seeded, deterministic)."""
+import glob
+import os
+
 import numpy as np
 
 import rbffd_gpu_b200 as R
@@ -34,3 +37,8 @@ def rel_l2(a, b):
 
 def rel_linf(a, b):
     return float(np.abs(np.ravel(a) - np.ravel(b)).max() / np.abs(np.ravel(b)).max())
+
+
+def has_gpu():
+    """A CUDA device node is present (the same test as conftest's)."""
+    return os.path.exists("/dev/nvidiactl") or bool(glob.glob("/dev/nvidia[0-9]*"))

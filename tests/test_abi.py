@@ -9,6 +9,7 @@ import pytest
 
 import rbffd_gpu_b200 as R
 from rbffd_gpu_b200 import _lib
+from tests.helpers import has_gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -49,7 +50,7 @@ def test_version_and_status_strings():
 
 
 def test_context_without_device_reports_no_device():
-    if os.path.exists("/dev/nvidia0"):
+    if has_gpu():
         pytest.skip("a GPU is present")
     L = _lib.load()
     h = ctypes.c_void_p()

@@ -1,0 +1,79 @@
+"""The C++ API (rbffd_gpu_b200/cpp/rbffd_cuda.hpp): classes shaped like the
+reference's RBFFD / TimeDependentPDE / CosineBell (src/rbffd/rbffd.h:29-547,
+src/pdes/time_dependent_pde.h:9-126, src/pdes/hyperbolic/cosine_bell.h:31-46)
+over the C ABI, and the cosine-bell driver built on them
+(rbffd_gpu_b200/lib/cosine_bell_cuda)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import rbffd_gpu_b200 as R
+from rbffd_gpu_b200 import _lib
+from tests.helpers import has_gpu, rel_l2
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "rbffd_gpu_b200", "lib", "cosine_bell_cuda")
+HEADER_DIR = os.path.join(ROOT, "rbffd_gpu_b200", "cpp")
+
+
+def test_header_compiles_in_throw_mode(tmp_path):
+    src = tmp_path / "use.cpp"
+    src.write_text(
+        '#define RBFFD_CUDA_THROW\n#include "rbffd_cuda.hpp"\n'
+        "int main() {\n"
+        "  try { rbffd_sm100::Context ctx(0); (void)ctx; }\n"
+        "  catch (const rbffd_sm100::Error& e) { return e.status == RBFFD_ERR_NO_DEVICE ? 3 : 4; }\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "use"
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I" + os.path.join(ROOT, "include"),
+                        "-I" + HEADER_DIR, str(src), "-L" + os.path.dirname(_lib.LIB_PATH), "-lrbffd_sm100",
+                        "-Wl,-rpath," + os.path.dirname(_lib.LIB_PATH), "-o", str(exe)], capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
+    rc = subprocess.run([str(exe)]).returncode
+    if has_gpu():
+        assert rc == 0
+    else:
+        assert rc == 3  # no device: the error surfaces as rbffd_sm100::Error with the C status
+
+
+def test_driver_is_built_and_exits_like_the_reference_on_error():
+    assert os.access(DRIVER, os.X_OK)
+    if has_gpu():
+        pytest.skip("a GPU is present")
+    r = subprocess.run([DRIVER, "GRID_SIZE=64"], capture_output=True, text=True)
+    assert r.returncode == 1 and "no CUDA device" in r.stderr  # print + exit(EXIT_FAILURE)
+
+
+@pytest.mark.gpu
+def test_cosine_bell_driver_matches_python_path(tmp_path):
+    """The C++ driver (RBFFD_CUDA + CosineBell_CUDA, advance one step per
+    call) and the Python view of the same C ABI give the same solution."""
+    N, n, steps = 4096, 31, 12
+    out = tmp_path / "h.bin"
+    r = subprocess.run([DRIVER, "GRID_SIZE=%d" % N, "STENCIL_SIZE=%d" % n, "STEPS=%d" % steps, "OUTPUT=%s" % out],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "rel L2" in r.stdout
+    h_cpp = np.fromfile(out, dtype=np.float64)
+    ctx = R.Context(0)
+    xyz = R.fibonacci_nodes(N, 1)
+    st = R.knn_stencils(xyz, n)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(R.LAMBDA | R.THETA, grid, 2)
+    der.setEpsilonByParameters(0.035, 0.1)  # the reference's table entry for n = 31 (rbffd.h:300-345)
+    der.setHVScalars(4, 5e-2)
+    der.setUseHyperviscosity(1)
+    der.setPolynomialDegree(2)
+    der.computeAllWeightsForAllStencils()
+    T = 1036800.0
+    pde = R.CosineBell(grid, der, 1.0, np.pi / 2, T, True)
+    pde.fillInitialConditions(R.exact_cosine_bell(xyz))
+    pde.advance(R.RK4, T / 1000.0, steps)
+    h_py = pde.getLocalSolution()
+    pde.close()
+    grid.close()
+    ctx.close()
+    assert rel_l2(h_cpp, h_py) < 1e-12  # same kernels; the autotuned lane split may differ per process
