@@ -50,8 +50,8 @@ def parse():
     ap.add_argument("--profile-multitracer", default=None, metavar="ROWS,LANES",
                     help="16-tracer vortex case on N=163842, n=101 (weights > L2), 3 un-graphed RK4 steps with the "
                          "tiled shape ROWS,LANES (0,0 = global-memory gathers), for ncu captures")
-    ap.add_argument("--profile-serving", action="store_true",
-                    help="grouped serving kernel: 8 + 8 requests on two N=163842 grids, 3 RK4 steps, for ncu")
+    ap.add_argument("--profile-serving", type=int, default=0, metavar="K",
+                    help="serving stage kernels: K + K requests on two N=163842 grids, 3 RK4 steps, for ncu")
     return ap.parse_args()
 
 
@@ -729,10 +729,10 @@ def run_profile_multitracer(spec):
     print("profile run done")
 
 
-def run_profile_serving():
-    """Two N=163842 grids (n=101 advection with HV, n=50 heat), eight FP32
+def run_profile_serving(K):
+    """Two N=163842 grids (n=101 advection with HV, n=50 heat), K FP32
     requests on each, admitted while the server is paused and then stepped
-    together (groups of 8), 3 RK4 steps: the grouped stage kernel for ncu."""
+    together (banks of K columns), 3 RK4 steps: the serving stage kernels for ncu."""
     import rbffd_gpu_b200 as R
     C = dict(SERVING, seed=7)
     ctx = R.Context(0)
@@ -742,7 +742,7 @@ def run_profile_serving():
     srv.pause()
     rng = np.random.default_rng(0)
     ids = []
-    for k in range(8):
+    for k in range(K):
         ids.append(srv.submit(ga["grid"], R.cosine_bell_params(1.0, np.pi / 2, 1036800.0, True, dtype=R.F32),
                               rng.random(163842), 100.0, 3))
         ids.append(srv.submit(gh["grid"], R.heat_params(1.0, R.F32), rng.random(163842), 1e-6, 3))
@@ -760,7 +760,7 @@ def run_profile_serving():
 def main():
     args = parse()
     if args.profile_serving:
-        run_profile_serving()
+        run_profile_serving(args.profile_serving)
     elif args.profile_multitracer:
         run_profile_multitracer(args.profile_multitracer)
     elif args.profile:

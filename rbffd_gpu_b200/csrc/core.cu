@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cstring>
 #include <functional>
@@ -418,23 +419,80 @@ int grid_halo(rbffd_grid* g, int R, const Halo** out)
     bstart.push_back(nsl);
     std::vector<int> rows(nblocks + 1);
     for (int b = 0; b <= nblocks; b++) rows[b] = std::min(N, 32 * bstart[b]);
+    // Placement of each block's halo nodes in shared memory.  A block's kernel
+    // reads, per stencil slot, one value (or 16-byte vector) per row; the 8
+    // rows of a quarter-warp are served in one shared-memory wavefront only if
+    // their nodes sit in different 16-byte bank groups (position mod 8).  A
+    // greedy colouring gives the nodes read together different positions mod 8
+    // where it can: position = 8 * rank + colour, padding slots repeat a node
+    // of the block (staging stays branch-free).  Only positions change: the
+    // arithmetic of every row is the same.
     std::vector<unsigned short> lidx(nidx, 0);
+    std::vector<std::vector<int>> layout(nblocks);
     run(nblocks, [&](int b) {
         const std::vector<int>& v = nodes[b];
-        for (int r = rows[b]; r < rows[b + 1]; r++)
+        const int K = (int)v.size(), r0 = rows[b], r1 = rows[b + 1];
+        std::vector<int> kidx((size_t)(r1 - r0) * n4);  // sorted-halo index of each (row, slot)
+        for (int r = r0; r < r1; r++)
+            for (int s = 0; s < n4; s++)
+                kidx[(size_t)(r - r0) * n4 + s] =
+                    (int)(std::lower_bound(v.begin(), v.end(), idx[sell_elem(r, s, nc)]) - v.begin());
+        // groups: the distinct nodes that 8 consecutive rows read at one slot
+        std::vector<std::vector<int>> groups;
+        std::vector<std::vector<int>> of_node(K);
+        for (int q0 = r0; q0 < r1; q0 += 8)
             for (int s = 0; s < n4; s++) {
-                const size_t e = sell_elem(r, s, nc);
-                lidx[e] = (unsigned short)(std::lower_bound(v.begin(), v.end(), idx[e]) - v.begin());
+                std::vector<int> gset;
+                for (int r = q0; r < std::min(r1, q0 + 8); r++) gset.push_back(kidx[(size_t)(r - r0) * n4 + s]);
+                std::sort(gset.begin(), gset.end());
+                gset.erase(std::unique(gset.begin(), gset.end()), gset.end());
+                if (gset.size() < 2) continue;
+                for (int k : gset) of_node[k].push_back((int)groups.size());
+                groups.push_back(std::move(gset));
             }
+        std::vector<int> order(K), colour(K, -1), used(8, 0);
+        std::vector<std::array<int, 8>> cnt(groups.size());
+        for (auto& c : cnt) c.fill(0);
+        for (int k = 0; k < K; k++) order[k] = k;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int c) { return of_node[a].size() > of_node[c].size(); });
+        const int cap = (K + 7) / 8 + 1;
+        for (int k : order) {
+            int best = -1;
+            long best_cost = 0;
+            for (int c = 0; c < 8; c++) {
+                if (used[c] >= cap) continue;
+                long cost = 0;
+                for (int g : of_node[k]) cost += cnt[g][c];
+                if (best < 0 || cost < best_cost || (cost == best_cost && used[c] < used[best])) {
+                    best = c;
+                    best_cost = cost;
+                }
+            }
+            colour[k] = best;
+            used[best]++;
+            for (int g : of_node[k]) cnt[g][best]++;
+        }
+        std::vector<int> pos(K), rank(8, 0);
+        for (int k = 0; k < K; k++) pos[k] = 8 * rank[colour[k]]++ + colour[k];
+        int hn = 0;
+        for (int k = 0; k < K; k++) hn = std::max(hn, pos[k] + 1);
+        std::vector<int>& lay = layout[b];
+        lay.assign(hn, v[0]);
+        for (int k = 0; k < K; k++) lay[pos[k]] = v[k];
+        for (int r = r0; r < r1; r++)
+            for (int s = 0; s < n4; s++)
+                lidx[sell_elem(r, s, nc)] = (unsigned short)pos[kidx[(size_t)(r - r0) * n4 + s]];
     });
     std::vector<int> ptr(nblocks + 1, 0), flat;
     int max_halo = 0;
     for (int b = 0; b < nblocks; b++) {
-        ptr[b + 1] = ptr[b] + (int)nodes[b].size();
-        max_halo = std::max(max_halo, (int)nodes[b].size());
+        if (layout[b].size() > 65535) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a block halo exceeds 65535 slots");
+        ptr[b + 1] = ptr[b] + (int)layout[b].size();
+        max_halo = std::max(max_halo, (int)layout[b].size());
     }
     flat.reserve(ptr[nblocks]);
-    for (int b = 0; b < nblocks; b++) flat.insert(flat.end(), nodes[b].begin(), nodes[b].end());
+    for (int b = 0; b < nblocks; b++) flat.insert(flat.end(), layout[b].begin(), layout[b].end());
     Halo* h = new (std::nothrow) Halo();
     if (!h) return RBFFD_ERR_OOM;
     h->R = R;

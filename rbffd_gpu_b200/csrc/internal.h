@@ -81,16 +81,18 @@ struct rbffd_grid {
 int grid_to_internal(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s);
 int grid_to_caller(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s);
 
-// Row blocks of R consecutive internal rows with their halo: the sorted unique
-// nodes their stencils reference.  A block's kernel stages the halo's values in
+// Row blocks of R consecutive internal rows with their halo: the unique nodes
+// their stencils reference.  A block's kernel stages the halo's values in
 // shared memory and reads them through 16-bit local indices (lidx, the sliced
 // ELL layout of the stencils with each node index replaced by its position in
-// the block's halo).
+// the block's halo).  Positions are chosen so that the nodes 8 consecutive
+// rows read at one slot fall in different 16-byte bank groups where possible;
+// padding positions repeat a node of the block.
 struct Halo {
     int R = 0, nblocks = 0, max_halo = 0;  // R: most rows in a block (blocks hold whole 32-row slices)
     int* d_rows = nullptr;       // [nblocks + 1] first row of each block
     int* d_ptr = nullptr;        // [nblocks + 1] offsets into d_nodes
-    int* d_nodes = nullptr;      // halo node indices (internal order)
+    int* d_nodes = nullptr;      // node staged at each halo position (internal order)
     unsigned short* d_lidx = nullptr;  // sliced ELL, N32 x n4
     size_t b_nodes = 0, b_lidx = 0;
 };

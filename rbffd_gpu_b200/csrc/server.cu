@@ -245,10 +245,20 @@ __global__ void __launch_bounds__(SEG_ROWS) k_stage_bank_tile(const BankDesc<T>*
     const int r0 = __ldg(B.hrows + b), r1 = __ldg(B.hrows + b + 1);
     const int h0 = __ldg(B.hptr + b), hn = __ldg(B.hptr + b + 1) - h0;
     const T* x = stage == 0 ? B.u : (stage == 2 ? B.xb : B.xa);
+    // 32-byte rows are staged as two 16-byte planes ([plane][halo position]):
+    // each gather instruction then reads 16-byte vectors at a 16-byte stride,
+    // the access the halo placement spreads over the bank groups
+    constexpr int P = W * sizeof(T) == 32 ? 2 : 1, VP = W / P;
     for (int h = threadIdx.x; h < hn; h += blockDim.x) {
         T v[W];
         ldw<T, W>(x + (size_t)__ldg(B.hnodes + h0 + h) * W, v, true);
-        stw<T, W>(sx + (size_t)h * W, v);
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            T vp[VP];
+#pragma unroll
+            for (int q = 0; q < VP; q++) vp[q] = v[p * VP + q];
+            stw<T, VP>(sx + ((size_t)p * hn + h) * VP, vp);
+        }
     }
     __syncthreads();
     const int i = r0 + (int)threadIdx.x;
@@ -267,7 +277,13 @@ __global__ void __launch_bounds__(SEG_ROWS) k_stage_bank_tile(const BankDesc<T>*
 #pragma unroll
         for (int e = 0; e < 4; e++) {
             T xv[W];
-            ldw<T, W>(sx + (size_t)ll[e] * W, xv, false);
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                T vp[VP];
+                ldw<T, VP>(sx + ((size_t)p * hn + ll[e]) * VP, vp, false);
+#pragma unroll
+                for (int q = 0; q < VP; q++) xv[p * VP + q] = vp[q];
+            }
 #pragma unroll
             for (int v = 0; v < W; v++) {
                 d0[v] = Ar<T>::fma(wa[e], xv[v], d0[v]);
