@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--profile", action="store_true",
-                    help="setup plus 25 un-graphed RK4 steps with a fixed kernel shape, for ncu captures")
+                    help="setup plus 25 un-graphed RK4 steps with the autotuned kernel shape, for ncu captures")
     ap.add_argument("--profile-multitracer", default=None, metavar="ROWS,LANES",
                     help="16-tracer vortex case on N=163842, n=101 (weights > L2), 3 un-graphed RK4 steps with the "
                          "tiled shape ROWS,LANES (0,0 = global-memory gathers), for ncu captures")
@@ -135,11 +135,12 @@ def heat_eps(N):
     return 0.25 / np.sqrt(4.0 * np.pi / N)
 
 
-def stage_bytes(n, wbytes, sbytes):
-    """Algorithmic bytes per node per RK4 stage: n weights + n int32 indices
-    + the state terms (one gathered read of the stage input, read u_n, read and
-    write of the accumulator, write of the next stage input)."""
-    return n * wbytes + 4 * n + 4 * sbytes
+def stage_bytes(n, wbytes, sbytes, ibytes=4):
+    """Algorithmic bytes per node per RK4 stage: n weights + n indices (int32,
+    or 16-bit local indices for the halo-tiled kernels) + the state terms (one
+    gathered read of the stage input, read u_n, read and write of the
+    accumulator, write of the next stage input)."""
+    return n * wbytes + ibytes * n + 4 * sbytes
 
 
 def cpu_baseline_heat(st, w_lsfc, u0, steps):
@@ -253,14 +254,19 @@ def run_ours(args):
     value = node_updates / (tot_ms * 1e-3)
     launches = 4 * steps * args.steps  # one fused stage kernel per RK4 stage
     per_launch_s = tot_ms * 1e-3 / launches
-    bytes_launch = N * stage_bytes(n, 4, 4)
+    shape = pde.getShape()  # (lanes per row, threads per block, rows per halo tile or 0), chosen by the autotuner
+    tiled = shape[2] > 0
+    kernel_name = ("k_stage_tile<float,HEAT> (halo tile of %d rows, 16-bit local indices)" % shape[2] if tiled else
+                   "k_stage_scalar<float,HEAT> (%d lane(s) per row)" % shape[0])
+    bytes_launch = N * stage_bytes(n, 4, 4, 2 if tiled else 4)
     achieved = bytes_launch / per_launch_s / 1e9
     peak, peak_kind = load_peaks()
     traffic = None
     tp = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
     if os.path.exists(tp):
         try:
-            traffic = json.load(open(tp)).get("heat_f32_dram_bytes_per_launch")
+            traffic = json.load(open(tp)).get("heat_f32_tile_dram_bytes_per_launch" if tiled else
+                                              "heat_f32_dram_bytes_per_launch")
         except (OSError, ValueError):
             traffic = None
     # ---- end to end through the C ABI with host buffers ----
@@ -307,7 +313,7 @@ def run_ours(args):
                        "l2_flush": "256 MiB buffer written between timed steps"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_stage_scalar<float,HEAT> (fused SpMV + RHS + RK4 stage)",
+                         "kernel": kernel_name + ", fused SpMV + RHS + RK4 stage", "shape": shape,
                          "algorithmic_bytes_per_launch": bytes_launch,
                          "note": "per-launch time = timed region / launches (includes graph launch gaps); "
                                  "FP32 weights+indices (65.5 MB) fit the 126 MB L2"},
@@ -420,7 +426,8 @@ def bench_multitracer(R, torch, ctx):
     for dtype, tag, wb, sb in ((R.F32, "fp32", 4, 4), (R.F64, "fp64", 8, 8)):
         secs = res[dtype][1]
         per_launch = secs / (4 * steps)
-        bytes_launch = N * (3 * n * wb + 4 * n + 4 * T * sb)
+        ib = 2 if res[dtype][2][2] > 0 else 4  # 16-bit local indices in the halo-tiled kernels
+        bytes_launch = N * (3 * n * wb + ib * n + 4 * T * sb)
         out[tag] = {"node_updates_per_s": N * steps / secs, "tracer_node_updates_per_s": N * T * steps / secs,
                     "ms_per_rk4_step": 1e3 * secs / steps, "shape": res[dtype][2],
                     "roofline": {"bound": "hbm", "achieved": bytes_launch / per_launch / 1e9, "peak": peak,
@@ -690,13 +697,12 @@ def run_profile():
     der.setPolynomialDegree(WORKLOAD["deg"])
     der.computeAllWeightsForAllStencils()
     pde = R.HeatSphere(grid, der, 1.0, dtype=R.F32)
-    pde.setShape(1, 256)
     pde.fillInitialConditions(u0)
-    pde.advance(R.RK4, WORKLOAD["dt"], 25)
+    pde.advance(R.RK4, WORKLOAD["dt"], 25)  # the autotuner picks the shape, as in the benchmark
+    print("profile run done, shape", pde.getShape())
     pde.close()
     grid.close()
     ctx.close()
-    print("profile run done")
 
 
 def run_profile_multitracer(spec):
