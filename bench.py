@@ -463,6 +463,12 @@ def bench_weights(R, torch, ctx):
     t0 = time.perf_counter()
     full = R.knn_stencils(xyz, max(C["sizes"]))
     t_knn = time.perf_counter() - t0
+    R.knn_stencils_gpu(ctx, xyz[:4096], 17)  # warm-up (module load)
+    t0 = time.perf_counter()
+    full_gpu = R.knn_stencils_gpu(ctx, xyz, max(C["sizes"]))
+    t_knn_gpu = time.perf_counter() - t0
+    knn_equal = bool(np.array_equal(full_gpu, full))
+    del full_gpu
     rng = np.random.default_rng(C["seed"])
     pick = rng.integers(0, len(C["sizes"]), N)
     lens = np.array(C["sizes"], dtype=np.int32)[pick]
@@ -507,7 +513,10 @@ def bench_weights(R, torch, ctx):
     return {
         "workload": C["name"], "stencils": N, "system_sizes_m": sorted(set(int(m) for m in ms)),
         "seconds": best, "all_runs_s": times, "stencils_per_s": N / best, "fp64_gflops": flops / best / 1e9,
-        "flops_per_call": flops, "knn_s": t_knn,
+        "flops_per_call": flops,
+        "knn": {"host_s": t_knn, "gpu_s": t_knn_gpu, "gpu_equals_host": knn_equal,
+                "note": "n=101 nearest neighbours of 1e6 nodes; host: exact cell search on all host threads; "
+                        "gpu: rbffd_stencils_knn_gpu including host binning and transfers"},
         "max_abs_derivative_of_constant": worst_const,
         "max_abs_reproduction_error_xyz_degree1_rows": worst_lin,
         "cpu_baseline": {"stencils_per_s": S / cpu_s, "fp64_gflops": cpu_flops / cpu_s / 1e9, "cores": nth,

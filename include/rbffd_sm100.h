@@ -85,6 +85,11 @@ int rbffd_nodes_fibonacci(int N, uint64_t seed, double* xyz);
  * k-d tree of external/kdtree/KDTree.h:407-433.  st[N][n].  *ties (optional)
  * receives the number of stencils whose distance list had an exact tie. */
 int rbffd_stencils_knn(const double* xyz, int N, int n, int* st, int* ties, int nthreads);
+/* The same stencils (identical lists and tie count) computed on ctx's device:
+ * the host bins the points into a uniform cell grid, one warp per node
+ * searches the surrounding cells.  Replaces the same reference call
+ * (grid_interface.cpp:688-725, KDTree.h:407-433); n <= 255. */
+int rbffd_stencils_knn_gpu(rbffd_ctx* ctx, const double* xyz, int N, int n, int* st, int* ties);
 /* Cosine bell ExactAdvection::operator() (tests/experiments/cosine_bell_on_sphere/exact_advection.h:37-53). */
 int rbffd_exact_cosine_bell(int N, const double* xyz, double sphere_radius, double* h);
 /* Heat on the unit sphere: u = sum_{l<=lmax,m} c_lm exp(-kappa l(l+1) t) Y_lm (real orthonormal Y_lm). */

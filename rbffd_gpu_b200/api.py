@@ -76,6 +76,16 @@ def knn_stencils(xyz, n, nthreads=0, return_ties=False):
     return (st, ties.value) if return_ties else st
 
 
+def knn_stencils_gpu(ctx, xyz, n, return_ties=False):
+    """The stencils of knn_stencils (identical lists), searched on ctx's device."""
+    xyz = _f64(xyz)
+    N = xyz.shape[0]
+    st = np.zeros((N, n), dtype=np.int32)
+    ties = ctypes.c_int(0)
+    ctx.check(ctx.L.rbffd_stencils_knn_gpu(ctx.h, _dp(xyz), N, n, _ip(st), ctypes.byref(ties)), "rbffd_stencils_knn_gpu")
+    return (st, ties.value) if return_ties else st
+
+
 def exact_cosine_bell(xyz, a=1.0):
     xyz = _f64(xyz)
     h = np.zeros(xyz.shape[0])
