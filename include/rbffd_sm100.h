@@ -141,6 +141,19 @@ int rbffd_weights_set(rbffd_grid* grid, unsigned der_type, const double* w);
 /* Read one operator's FP64 weights back, [N][n_pad]; padding slots are 0.
  * RBFFD::getStencilWeights (rbffd.h:395). */
 int rbffd_weights_get(rbffd_grid* grid, unsigned der_type, double* w);
+/* Weight files in the reference's Matrix Market forms, host only (no GPU):
+ * RBFFD::writeToAsciiFile / writeToBinaryFile (src/rbffd/rbffd.cpp:1265-1375)
+ * and loadFromAsciiFile / loadFromBinaryFile (rbffd.cpp:983-1210).  binary = 0
+ * writes "row col %24.16le" text entries, 1 raw int/int/double records after
+ * the same text header; rows are the stencils' centres, columns their nodes,
+ * 1-based, in stencil order.  stencils [N][n_pad] with lengths st_len (NULL:
+ * all n_pad); w [N][n_pad] (read: padding set to 0).  Reading refuses
+ * (RBFFD_ERR_INVALID) a file whose sizes, order or stencil nodes differ from
+ * the given stencils; unreadable / unwritable files also give RBFFD_ERR_INVALID. */
+int rbffd_weights_file_write(const char* filename, int binary, int N, int n_pad, const int* stencils,
+                             const int* st_len, const double* w);
+int rbffd_weights_file_read(const char* filename, int binary, int N, int n_pad, const int* stencils,
+                            const int* st_len, double* w);
 
 /* ---- apply (derivative evaluation) ------------------------------------- */
 /* deriv[i] = sum_s w[i][s] * u[st_i[s]] for i in [start, start+count):

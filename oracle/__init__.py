@@ -72,6 +72,9 @@ def ref_lib(name):
             L.ref_cart2sph.restype = None
         if L is not None and name == "ref_kdtree":
             L.ref_knn.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _ip, _dp]
+        if L is not None and name == "ref_mmio":
+            L.ref_mm_write_header.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+            L.ref_mm_read_header.argtypes = [ctypes.c_char_p, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_long)]
     return _REF[name]
 
 

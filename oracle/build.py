@@ -8,6 +8,8 @@
 * ``oracle/_ref/libref_rbf.so`` -- the reference's own ``src/rbffd/rbfs/rbf_gaussian.h``
   and ``src/utils/geom/cart2sph.cpp``, with ``oracle/shim/armadillo`` standing in
   for the Armadillo header that ``rbf.h`` includes.
+* ``oracle/_ref/libref_mmio.so`` -- the reference's own ``external/nist/mmio.cpp``
+  (the Matrix Market header of its weight files).
 
 The reference's full RBFFD class (``src/rbffd/rbffd.cpp``) needs Armadillo,
 LAPACK, MPI and Boost, none of which exist here, so it is treated as
@@ -76,6 +78,11 @@ def build_ref(force=False):
                        "-I" + os.path.join(REF, "src"), "-I" + util, rb_src[0], rb_src[2],
                        os.path.join(util, "Vec3d.cpp"), os.path.join(util, "CVec3.cpp"), "-o", rb])
     built.append(rb)
+    mm = os.path.join(outdir, "libref_mmio.so")
+    mm_src = [os.path.join(HERE, "ref_mmio.cpp"), os.path.join(REF, "external/nist/mmio.cpp")]
+    if force or _newer(mm, mm_src):
+        _run(["g++", "-O2", "-fPIC", "-shared", "-w", "-I" + os.path.join(REF, "external/nist")] + mm_src + ["-o", mm])
+    built.append(mm)
     return built
 
 

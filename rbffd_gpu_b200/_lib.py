@@ -62,6 +62,8 @@ PROTOTYPES = {
     "rbffd_weights_assemble": (c_int, [c_void_p, P(WeightParams), dp, c_double, ip, ip, c_int, dp]),
     "rbffd_weights_set": (c_int, [c_void_p, c_uint, dp]),
     "rbffd_weights_get": (c_int, [c_void_p, c_uint, dp]),
+    "rbffd_weights_file_write": (c_int, [c_char_p, c_int, c_int, c_int, ip, ip, dp]),
+    "rbffd_weights_file_read": (c_int, [c_char_p, c_int, c_int, c_int, ip, ip, dp]),
     "rbffd_apply": (c_int, [c_void_p, c_uint, c_int, c_uint, c_uint, dp, dp]),
     "rbffd_apply_dev": (c_int, [c_void_p, c_uint, c_int, c_int, c_void_p, c_void_p]),
     "rbffd_batched_gesv_dev": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),

@@ -76,6 +76,32 @@ def knn_stencils(xyz, n, nthreads=0, return_ties=False):
     return (st, ties.value) if return_ties else st
 
 
+def write_weights_file(filename, stencils, w, st_len=None, binary=True):
+    """The reference's weight file (Matrix Market, text or binary form) for
+    weights w [N][n_pad] of stencils [N][n_pad]; host only."""
+    st = _i32(stencils)
+    w = _f64(w)
+    N, n_pad = st.shape
+    sl = None if st_len is None else _i32(st_len)
+    rc = _lib.load().rbffd_weights_file_write(filename.encode(), int(binary), N, n_pad, _ip(st),
+                                              None if sl is None else _ip(sl), _dp(w))
+    if rc:
+        raise RbffdError(rc, "rbffd_weights_file_write(%s)" % filename)
+
+
+def read_weights_file(filename, stencils, st_len=None, binary=True):
+    """Weights [N][n_pad] from the reference's weight file for these stencils; host only."""
+    st = _i32(stencils)
+    N, n_pad = st.shape
+    sl = None if st_len is None else _i32(st_len)
+    w = np.zeros((N, n_pad))
+    rc = _lib.load().rbffd_weights_file_read(filename.encode(), int(binary), N, n_pad, _ip(st),
+                                             None if sl is None else _ip(sl), _dp(w))
+    if rc:
+        raise RbffdError(rc, "rbffd_weights_file_read(%s)" % filename)
+    return w
+
+
 def knn_stencils_gpu(ctx, xyz, n, return_ties=False):
     """The stencils of knn_stencils (identical lists), searched on ctx's device."""
     xyz = _f64(xyz)
@@ -209,6 +235,7 @@ class RBFFD:
         self.useHyperviscosity = 0
         self.var_epsilon = np.ones(grid.N)
         self.poly_deg = 0  # ONE_MONOMIAL (rbffd.cpp:1)
+        self.asciiWeights = 0  # binary weight files unless setAsciiWeights(1)
         self.deg_per_row = None
 
     # -- parameters (rbffd.h:213-381) --
@@ -262,6 +289,30 @@ class RBFFD:
         ctx = self.grid.ctx
         ctx.check(ctx.L.rbffd_weights_get(self.grid.h, which, _dp(w)), "rbffd_weights_get")
         return w
+
+    # -- weight files (rbffd.h:400-410; rbffd.cpp:973-1375) --
+    def setAsciiWeights(self, binary_or_ascii):
+        """1: text Matrix Market files; 0: the binary form (the reference's default)."""
+        self.asciiWeights = int(binary_or_ascii)
+
+    def writeToFile(self, which, filename):
+        g = self.grid
+        w = self.getWeights(which)
+        rc = g.ctx.L.rbffd_weights_file_write(filename.encode(), 0 if self.asciiWeights else 1,
+                                              g.N, g.n_pad, _ip(g.stencils),
+                                              None if g.st_len is None else _ip(g.st_len), _dp(w))
+        if rc:
+            raise RbffdError(rc, "writeToFile(%s)" % filename)
+
+    def loadFromFile(self, which, filename):
+        g = self.grid
+        w = np.zeros((g.N, g.n_pad))
+        rc = g.ctx.L.rbffd_weights_file_read(filename.encode(), 0 if self.asciiWeights else 1,
+                                             g.N, g.n_pad, _ip(g.stencils),
+                                             None if g.st_len is None else _ip(g.st_len), _dp(w))
+        if rc:
+            raise RbffdError(rc, "loadFromFile(%s)" % filename)
+        self.setWeights(which, w)
 
     def getStencilWeights(self, which, st_indx):
         return self.getWeights(which)[st_indx]

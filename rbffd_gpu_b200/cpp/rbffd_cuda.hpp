@@ -88,13 +88,14 @@ public:
             xyz[3 * i + 1] = nodes[i].y;
             xyz[3 * i + 2] = nodes[i].z;
         }
-        std::vector<int> st((size_t)N * n_pad_, 0), len(N);
+        st_.assign((size_t)N * n_pad_, 0);
+        len_.assign(N, 0);
         for (int i = 0; i < N; i++) {
-            len[i] = (int)stencils[i].size();
-            for (int s = 0; s < len[i]; s++) st[(size_t)i * n_pad_ + s] = stencils[i][s];
-            for (int s = len[i]; s < n_pad_; s++) st[(size_t)i * n_pad_ + s] = i;
+            len_[i] = (int)stencils[i].size();
+            for (int s = 0; s < len_[i]; s++) st_[(size_t)i * n_pad_ + s] = stencils[i][s];
+            for (int s = len_[i]; s < n_pad_; s++) st_[(size_t)i * n_pad_ + s] = i;
         }
-        check(ctx.handle(), rbffd_grid_create(ctx.handle(), N, xyz.data(), n_pad_, st.data(), len.data(), &h_),
+        check(ctx.handle(), rbffd_grid_create(ctx.handle(), N, xyz.data(), n_pad_, st_.data(), len_.data(), &h_),
               "rbffd_grid_create");
     }
     ~Grid_CUDA() { rbffd_grid_destroy(h_); }
@@ -109,11 +110,15 @@ public:
     unsigned getMaxStencilSize() const { return (unsigned)n_pad_; }
     rbffd_grid* handle() const { return h_; }
     Context& context() const { return ctx_; }
+    // stencils as [N][getMaxStencilSize()] (padding = centre) and their lengths
+    const std::vector<int>& paddedStencils() const { return st_; }
+    const std::vector<int>& stencilLengths() const { return len_; }
 
 private:
     Context& ctx_;
     std::vector<Vec3> nodes_;
     std::vector<StencilType> stencils_;
+    std::vector<int> st_, len_;
     unsigned global_;
     int n_pad_ = 1;
     rbffd_grid* h_ = nullptr;
@@ -223,6 +228,30 @@ public:
         return std::vector<double>(all.begin() + st_indx * n, all.begin() + (st_indx + 1) * n);
     }
 
+    // -- weight files (rbffd.h:400-410): the reference's Matrix Market forms --
+    void setAsciiWeights(int binary_or_ascii) { asciiWeights = binary_or_ascii; }
+    void writeToFile(DerType which, const std::string& filename)
+    {
+        std::vector<double> w = getWeights(which);
+        check(grid_ref.context().handle(),
+              rbffd_weights_file_write(filename.c_str(), asciiWeights ? 0 : 1, (int)grid_ref.getStencilsSize(),
+                                       (int)grid_ref.getMaxStencilSize(), grid_ref.paddedStencils().data(),
+                                       grid_ref.stencilLengths().data(), w.data()),
+              "writeToFile");
+    }
+    // returns 0 (the reference's loadFromFile returns nonzero codes on failure)
+    int loadFromFile(DerType which, const std::string& filename)
+    {
+        std::vector<double> w((size_t)grid_ref.getStencilsSize() * grid_ref.getMaxStencilSize());
+        check(grid_ref.context().handle(),
+              rbffd_weights_file_read(filename.c_str(), asciiWeights ? 0 : 1, (int)grid_ref.getStencilsSize(),
+                                      (int)grid_ref.getMaxStencilSize(), grid_ref.paddedStencils().data(),
+                                      grid_ref.stencilLengths().data(), w.data()),
+              "loadFromFile");
+        setWeights(which, w);
+        return 0;
+    }
+
     // -- apply (rbffd.h:257-274) --
     virtual void applyWeightsForDeriv(DerType which, std::vector<double>& u, std::vector<double>& deriv,
                                       bool isChangedU = true)
@@ -256,6 +285,7 @@ protected:
     int poly_deg = 0;
     std::vector<int> deg_rows;
     int dtype = RBFFD_F64;
+    int asciiWeights = 0;  // binary weight files unless setAsciiWeights(1)
 };
 
 class TimeDependentPDE_CUDA {
