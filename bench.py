@@ -374,6 +374,7 @@ def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
     out["multitracer"] = bench_multitracer(R, torch, ctx)
     out["serving"] = bench_serving(R, torch, ctx)
     out["weights"] = bench_weights(R, torch, ctx)
+    out["cosine_bell"] = bench_cosine_bell(R, torch, ctx)
     return out
 
 
@@ -437,6 +438,79 @@ def bench_multitracer(R, torch, ctx):
     out["rel_linf_fp32_vs_fp64"] = float(np.abs(u32 - u64).max() / np.abs(u64).max())
     out["rel_l2_fp64_vs_exact"] = float(np.linalg.norm(u64 - exact) / np.linalg.norm(exact))
     grid.close()
+    return out
+
+
+COSINE_BELL = dict(name="cosine_bell_N4096_n31_deg2_1000steps", N=4096, n=31, seed=1, deg=2, hv_k=4, gamma=1e-3,
+                   T=1036800.0, steps=1000, eps_configuration=0.035 * 64.0, eps_stable=6.0, short_steps=100)
+
+
+def bench_cosine_bell(R, torch, ctx):
+    """The plain method, small: solid-body rotation of the cosine bell, N=4096,
+    n=31, d/dlambda + d/dtheta + Delta^4 hyperviscosity (gamma = 1e-3 N^-4),
+    degree-2 polynomials, one revolution in 1000 RK4 steps, FP64.  GPU and
+    oracle step with the same (oracle) weights, so the comparison isolates the
+    time stepping; the GPU runs one lane per row (the oracle's summation
+    order).  At the configuration's eps = 0.035 sqrt(N) the operator has
+    growing modes on these nodes (reported over a short horizon); a full
+    revolution uses eps = 6."""
+    import oracle as O
+    C = COSINE_BELL
+    N, n = C["N"], C["n"]
+    xyz = R.fibonacci_nodes(N, C["seed"])
+    st = R.knn_stencils(xyz, n)
+    h0 = R.exact_cosine_bell(xyz)
+    a, alpha, T = 1.0, np.pi / 2, C["T"]
+    dt = T / 1000.0
+    cu, cv = O.cosine_bell_coeffs(xyz, a=a, alpha=alpha, u0=2 * np.pi * a / T)
+    types = R.LAMBDA | R.THETA | R.HV
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    out = {"workload": C["name"]}
+
+    def rel(x, y):
+        dn = float(np.linalg.norm(y))
+        return float(np.linalg.norm(x - y) / dn) if np.isfinite(dn) and dn > 0 else None
+
+    for tag, eps, steps in (("eps_configuration", C["eps_configuration"], C["short_steps"]),
+                            ("eps_stable", C["eps_stable"], C["steps"])):
+        W = O.weights(xyz, st, None, eps, types, dim=2, poly_deg=C["deg"], hv_k=C["hv_k"],
+                      hv_scale=-C["gamma"] * N ** -float(C["hv_k"]))
+        grid = R.Grid(ctx, xyz, st)
+        der = R.RBFFD(types, grid, 2)
+        for t, w in W.items():
+            der.setWeights(t, w)
+        res = {"eps": eps, "steps": steps}
+        for dname, dtype in (("fp64", R.F64), ("fp32", R.F32)):
+            pde = R.CosineBell(grid, der, a, alpha, T, True, dtype=dtype)
+            pde.setShape(1, 256)
+            pde.fillInitialConditions(h0)
+            pde.advance(R.RK4, dt, 10, graph=True)  # warm-up (graph instantiation)
+            pde.fillInitialConditions(h0)
+            ctx.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
+            e1.record(stream)
+            ctx.synchronize()
+            res[dname] = {"h": pde.getLocalSolution(), "node_updates_per_s": N * steps / (e0.elapsed_time(e1) * 1e-3)}
+            pde.close()
+        t = time.perf_counter()
+        h_or = O.rk4_advect(st, None, W[R.LAMBDA], W[R.THETA], W[R.HV], cu, cv, h0, dt, steps, nthreads=1)
+        cpu_s = time.perf_counter() - t
+        h64, h32 = res["fp64"].pop("h"), res["fp32"].pop("h")
+        res["fp64_equals_oracle_bitwise"] = bool(np.array_equal(h64, h_or))
+        res["rel_l2_fp64_vs_oracle"] = rel(h64, h_or)
+        res["rel_l2_fp32_vs_oracle"] = rel(h32, h_or)
+        res["rel_linf_fp32_vs_oracle"] = (float(np.abs(h32 - h_or).max() / np.abs(h_or).max())
+                                          if np.all(np.isfinite(h_or)) else None)
+        if steps == C["steps"]:  # one revolution: the exact solution is the initial bell
+            res["rel_l2_fp64_vs_exact"] = rel(h64, h0)
+            res["rel_linf_fp64_vs_exact"] = float(np.abs(h64 - h0).max() / np.abs(h0).max())
+        else:
+            res["growth_max_abs"] = float(np.abs(h_or).max() / np.abs(h0).max())
+        res["cpu_oracle_1_thread_node_updates_per_s"] = N * steps / cpu_s
+        out[tag] = res
+        grid.close()
     return out
 
 

@@ -324,14 +324,16 @@ __device__ int team_eliminate(const Team& T, double* a, int m, int K, double* ca
             }
         T.sync();
         const double piv = a[k * ld + k];
+        // the multipliers of all rows at once, one division per thread, kept in
+        // column k (where LAPACK keeps L; nothing reads it afterwards)
+        for (int i = k + 1 + T.tid; i < m; i += T.size) a[i * ld + k] = a[i * ld + k] / piv;
+        T.sync();
         // rows split across warps, columns across lanes; lane 0 of the j-loop
         // holds column k+1 and tracks the next pivot candidate
         double nbv = -1.0;
         int nbr = INT_MAX;
         for (int i = k + 1 + w; i < m; i += nw) {
-            double l = 0.0;
-            if (lane == 0) l = a[i * ld + k] / piv;
-            l = __shfl_sync(0xffffffffu, l, 0);
+            const double l = a[i * ld + k];
             for (int j = k + 1 + lane; j < ld; j += 32) {
                 double v = __fma_rn(-l, a[k * ld + j], a[i * ld + j]);
                 a[i * ld + j] = v;
