@@ -42,6 +42,8 @@ namespace {
 
 constexpr int MAX_K = 8;       // operators per solve
 constexpr int MAX_WARPS = 8;   // per team
+constexpr int MAX_M = 160;     // largest system (stencil + polynomial terms)
+constexpr int ELIM_CHUNKS = (MAX_M + MAX_K + 31) / 32;  // 32-column chunks of a row
 
 struct WParams {
     const double4* xyz;
@@ -328,18 +330,31 @@ __device__ int team_eliminate(const Team& T, double* a, int m, int K, double* ca
         // column k (where LAPACK keeps L; nothing reads it afterwards)
         for (int i = k + 1 + T.tid; i < m; i += T.size) a[i * ld + k] = a[i * ld + k] / piv;
         T.sync();
-        // rows split across warps, columns across lanes; lane 0 of the j-loop
-        // holds column k+1 and tracks the next pivot candidate
+        // rows split across warps, columns across lanes (column k+1+lane+32c);
+        // each lane keeps its columns of the pivot row in registers for the
+        // step; lane 0's first column is k+1, where it tracks the next pivot
+        double pr[ELIM_CHUNKS];
+#pragma unroll
+        for (int c = 0; c < ELIM_CHUNKS; c++) {
+            const int j = k + 1 + lane + 32 * c;
+            pr[c] = j < ld ? a[k * ld + j] : 0.0;
+        }
         double nbv = -1.0;
         int nbr = INT_MAX;
+#pragma unroll 2
         for (int i = k + 1 + w; i < m; i += nw) {
             const double l = a[i * ld + k];
-            for (int j = k + 1 + lane; j < ld; j += 32) {
-                double v = __fma_rn(-l, a[k * ld + j], a[i * ld + j]);
-                a[i * ld + j] = v;
-                if (j == k + 1) {
-                    double av = fabs(v);
-                    if (av > nbv) { nbv = av; nbr = i; }
+            double* ai = a + (size_t)i * ld;
+#pragma unroll
+            for (int c = 0; c < ELIM_CHUNKS; c++) {
+                const int j = k + 1 + lane + 32 * c;
+                if (j < ld) {
+                    const double v = __fma_rn(-l, pr[c], ai[j]);
+                    ai[j] = v;
+                    if (c == 0 && lane == 0) {
+                        const double av = fabs(v);
+                        if (av > nbv) { nbv = av; nbr = i; }
+                    }
                 }
             }
         }
