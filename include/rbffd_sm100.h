@@ -155,6 +155,33 @@ int rbffd_weights_file_write(const char* filename, int binary, int N, int n_pad,
 int rbffd_weights_file_read(const char* filename, int binary, int N, int n_pad, const int* stencils,
                             const int* st_len, double* w);
 
+/* ---- eigenvalue stability check ---------------------------------------- */
+/* RBFFD::EigenvalueOutput (src/rbffd/rbffd.h:91-100). */
+typedef struct rbffd_eig_output {
+    double max_pos_eig, min_pos_eig, max_neg_eig, min_neg_eig;
+    int nb_positive, nb_negative, nb_zero;
+} rbffd_eig_output;
+/* The classification of RBFFD::computeEigenvalues (src/rbffd/rbffd.cpp:781-858)
+ * over real parts re[0..n): counts of real parts > zero_tol, < -zero_tol and
+ * in between (the reference's tolerance is 1e-8), with the largest and
+ * smallest magnitude among the positive and among the negative ones, all four
+ * starting from |re[0]| as in the reference.  *max_neg_eig (optional) gets the
+ * reference's return value.  Host only, no GPU. */
+int rbffd_eig_classify(const double* re, int n, double zero_tol, rbffd_eig_output* out, double* max_neg_eig);
+/* RBFFD::computeEigenvalues (rbffd.cpp:703-873): every eigenvalue of the
+ * grid's N x N operator der_type, plus the HV operator when use_hv (the
+ * reference adds its hyperviscosity weights, rbffd.cpp:737-749), from the
+ * dense nonsymmetric eigenproblem the reference solves with eig_gen: the
+ * matrix is assembled on the device from the FP64 weights and solved with
+ * cuSOLVER's geev (loaded at first use; RBFFD_ERR_UNSUPPORTED if absent).
+ * Sphere grids have no boundary nodes, so the reference's identity rows for
+ * them do not occur.  eig_re / eig_im (optional, host, N each) receive the
+ * eigenvalues in the solver's order; out and max_neg_eig as
+ * rbffd_eig_classify with tolerance 1e-8.  N <= RBFFD_EIG_MAX_N. */
+#define RBFFD_EIG_MAX_N 16384
+int rbffd_eigenvalues(rbffd_grid* grid, unsigned der_type, int use_hv, double* eig_re, double* eig_im,
+                      rbffd_eig_output* out, double* max_neg_eig);
+
 /* ---- apply (derivative evaluation) ------------------------------------- */
 /* deriv[i] = sum_s w[i][s] * u[st_i[s]] for i in [start, start+count):
  * RBFFD::applyWeightsForDeriv(which, start_indx, nb_stencils, u, deriv)

@@ -200,3 +200,47 @@ def cart2sph(x, y, z):
 
 def max_threads():
     return lib().orc_max_threads()
+
+
+def dense_operator(st, st_len, w, w_hv=None):
+    """The dense N x N matrix RBFFD::computeEigenvalues builds
+    (src/rbffd/rbffd.cpp:724-764): row i holds stencil i's weights at its
+    nodes' columns, plus the hyperviscosity weights when given (rbffd.cpp:737-749).
+    The sphere has no boundary nodes, so no identity rows."""
+    N, n_pad = st.shape
+    A = np.zeros((N, N))
+    lens = np.full(N, n_pad) if st_len is None else np.asarray(st_len)
+    for i in range(N):
+        L = lens[i]
+        A[i, st[i, :L]] = w[i, :L] + (w_hv[i, :L] if w_hv is not None else 0.0)
+    return A
+
+
+def eigenvalues(A):
+    """Every eigenvalue of a dense real matrix: LAPACK dgeev through numpy, the
+    routine Armadillo's eig_gen calls (rbffd.cpp:768)."""
+    return np.linalg.eigvals(A)
+
+
+def eig_classify(re, zero_tol=1e-8):
+    """Restatement of the classification loop of RBFFD::computeEigenvalues
+    (rbffd.cpp:771-858): all four extremes start at |Re(eig(0))|; real parts
+    above zero_tol count as positive, below -zero_tol as negative, the rest as
+    zero.  Returns (EigenvalueOutput fields as a dict, max_neg_eig -- the
+    reference's return value)."""
+    re = [float(x) for x in re]
+    e0 = abs(re[0])
+    o = dict(max_pos_eig=e0, min_pos_eig=e0, max_neg_eig=e0, min_neg_eig=e0, nb_positive=0, nb_negative=0,
+             nb_zero=0)
+    for e in re:
+        if e > zero_tol:
+            o["nb_positive"] += 1
+            o["max_pos_eig"] = abs(e) if abs(e) > o["max_pos_eig"] else o["max_pos_eig"]
+            o["min_pos_eig"] = abs(e) if abs(e) < o["min_pos_eig"] else o["min_pos_eig"]
+        elif e < -zero_tol:
+            o["nb_negative"] += 1
+            o["max_neg_eig"] = abs(e) if abs(e) > o["max_neg_eig"] else o["max_neg_eig"]
+            o["min_neg_eig"] = abs(e) if abs(e) < o["min_neg_eig"] else o["min_neg_eig"]
+        else:
+            o["nb_zero"] += 1
+    return o, o["max_neg_eig"]

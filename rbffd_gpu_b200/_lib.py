@@ -33,6 +33,11 @@ class Request(ctypes.Structure):
                 ("out", dp)]
 
 
+class EigOutput(ctypes.Structure):
+    _fields_ = [(k, c_double) for k in ("max_pos_eig", "min_pos_eig", "max_neg_eig", "min_neg_eig")] + \
+               [(k, c_int) for k in ("nb_positive", "nb_negative", "nb_zero")]
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_longlong) for k in ("submitted", "completed", "failed", "cancelled", "pending", "active",
                                                  "max_active_seen", "ticks", "launches", "slots_reused")] + \
@@ -64,6 +69,8 @@ PROTOTYPES = {
     "rbffd_weights_get": (c_int, [c_void_p, c_uint, dp]),
     "rbffd_weights_file_write": (c_int, [c_char_p, c_int, c_int, c_int, ip, ip, dp]),
     "rbffd_weights_file_read": (c_int, [c_char_p, c_int, c_int, c_int, ip, ip, dp]),
+    "rbffd_eig_classify": (c_int, [dp, c_int, c_double, c_void_p, dp]),
+    "rbffd_eigenvalues": (c_int, [c_void_p, c_uint, c_int, dp, dp, c_void_p, dp]),
     "rbffd_apply": (c_int, [c_void_p, c_uint, c_int, c_uint, c_uint, dp, dp]),
     "rbffd_apply_dev": (c_int, [c_void_p, c_uint, c_int, c_int, c_void_p, c_void_p]),
     "rbffd_batched_gesv_dev": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),

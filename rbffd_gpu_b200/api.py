@@ -102,6 +102,23 @@ def read_weights_file(filename, stencils, st_len=None, binary=True):
     return w
 
 
+def eig_output_dict(o):
+    return {k: getattr(o, k) for k, _ in _lib.EigOutput._fields_}
+
+
+def eig_classify(re, zero_tol=1e-8):
+    """The reference's classification of eigenvalue real parts
+    (rbffd.cpp:781-858): (EigenvalueOutput as a dict, max |Re| of the negative
+    ones).  Host only."""
+    re = _f64(re)
+    o = _lib.EigOutput()
+    ret = ctypes.c_double()
+    rc = _lib.load().rbffd_eig_classify(_dp(re), re.size, float(zero_tol), ctypes.byref(o), ctypes.byref(ret))
+    if rc:
+        raise RbffdError(rc, "rbffd_eig_classify")
+    return eig_output_dict(o), ret.value
+
+
 def knn_stencils_gpu(ctx, xyz, n, return_ties=False):
     """The stencils of knn_stencils (identical lists), searched on ctx's device."""
     xyz = _f64(xyz)
@@ -316,6 +333,34 @@ class RBFFD:
 
     def getStencilWeights(self, which, st_indx):
         return self.getWeights(which)[st_indx]
+
+    # -- eigenvalue stability check (rbffd.h:281,412-417; rbffd.cpp:703-873) --
+    def computeEigenvalues(self, which, exit_on_fail=False, output=None, return_eigenvalues=False):
+        """Every eigenvalue of the dense operator `which` (+ HV when
+        hyperviscosity is on), classified as the reference does; returns the
+        reference's value, max |Re| among the negative eigenvalues (and the
+        complex eigenvalues when asked).  `output`, if a dict, receives the
+        EigenvalueOutput fields.  Where the reference exits (both signs
+        present, or more than one eigenvalue within 1e-8 of zero) this raises
+        RbffdError when exit_on_fail."""
+        g = self.grid
+        re, im = np.zeros(g.N), np.zeros(g.N)
+        o = _lib.EigOutput()
+        ret = ctypes.c_double()
+        g.ctx.check(g.ctx.L.rbffd_eigenvalues(g.h, which, int(bool(self.useHyperviscosity)), _dp(re), _dp(im),
+                                              ctypes.byref(o), ctypes.byref(ret)), "rbffd_eigenvalues")
+        res = eig_output_dict(o)
+        self.cachedEigenvalues = res
+        if output is not None:
+            output.update(res)
+        if exit_on_fail and ((res["nb_negative"] > 0 and res["nb_positive"] > 0) or res["nb_zero"] > 1):
+            raise RbffdError(-1, "computeEigenvalues: eigenvalues of both signs or more than one zero: %r" % res)
+        return (ret.value, re + 1j * im) if return_eigenvalues else ret.value
+
+    def getEigenvalues(self):
+        if getattr(self, "cachedEigenvalues", None) is None:
+            self.computeEigenvalues(LAPL, False)
+        return self.cachedEigenvalues
 
     # -- apply (rbffd.h:257-274) --
     def applyWeightsForDeriv(self, which, u, deriv=None, isChangedU=True, start_indx=0, nb_stencils=None, dtype=F64):

@@ -252,6 +252,57 @@ public:
         return 0;
     }
 
+    // -- eigenvalue stability check (rbffd.h:91-100,281,412-417; rbffd.cpp:703-873) --
+    typedef rbffd_eig_output EigenvalueOutput;
+    // Every eigenvalue of the operator (+ HV when hyperviscosity is on) on the
+    // device; counts and extremes as the reference prints them, the eigenvalues
+    // written "%+lf%+lfi" one per line to eigenvalue_file when one is named.
+    // Returns max |Re| among the negative eigenvalues.  Like the reference, a
+    // mix of signs or more than one zero eigenvalue is an error that exits when
+    // exit_on_fail.
+    double computeEigenvalues(DerType which, bool exit_on_fail, EigenvalueOutput* output = nullptr,
+                              const char* eigenvalue_file = nullptr)
+    {
+        const int N = (int)grid_ref.getStencilsSize();
+        std::vector<double> re(N), im(N);
+        EigenvalueOutput o;
+        double ret = 0.0;
+        check(grid_ref.context().handle(),
+              rbffd_eigenvalues(grid_ref.handle(), which, useHyperviscosity, re.data(), im.data(), &o, &ret),
+              "computeEigenvalues");
+        if (eigenvalue_file) {
+            FILE* f = std::fopen(eigenvalue_file, "w");
+            if (f) {
+                for (int i = 0; i < N; i++) std::fprintf(f, "%+lf%+lfi\n", re[i], im[i]);
+                std::fclose(f);
+            }
+        }
+        std::printf("\n[RBFFD] ****** Number positive eigenvalues: %d (nb_bnd: 0) *******\n\n", o.nb_positive);
+        std::printf("\n[RBFFD] ****** Number negative eigenvalues: %d *******\n\n", o.nb_negative);
+        std::printf("\n[RBFFD] ****** Number zero (-1e-8 <= eval <= 1e-8) eigenvalues: %d *******\n\n", o.nb_zero);
+        if (output) *output = o;
+        cachedEigenvalues = o;
+        eigenvalues_computed = true;
+        const bool mixed = o.nb_negative > 0 && o.nb_positive > 0, zeros = o.nb_zero > 1;
+        if (mixed || zeros) {
+            std::printf("[RBFFD] Error: %s\n", mixed ? "we expect either all positive or all negative eigenvalues."
+                                                     : "more than one eigenvalue is zero.");
+            if (exit_on_fail) {
+#ifdef RBFFD_CUDA_THROW
+                throw Error(RBFFD_ERR_INVALID, "computeEigenvalues: unstable operator");
+#else
+                std::exit(EXIT_FAILURE);
+#endif
+            }
+        }
+        return ret;
+    }
+    EigenvalueOutput getEigenvalues()
+    {
+        if (!eigenvalues_computed) computeEigenvalues(LAPL, false);
+        return cachedEigenvalues;
+    }
+
     // -- apply (rbffd.h:257-274) --
     virtual void applyWeightsForDeriv(DerType which, std::vector<double>& u, std::vector<double>& deriv,
                                       bool isChangedU = true)
@@ -286,6 +337,8 @@ protected:
     std::vector<int> deg_rows;
     int dtype = RBFFD_F64;
     int asciiWeights = 0;  // binary weight files unless setAsciiWeights(1)
+    EigenvalueOutput cachedEigenvalues = {};
+    bool eigenvalues_computed = false;
 };
 
 class TimeDependentPDE_CUDA {

@@ -124,7 +124,8 @@ def test_server_rejects_null_handles():
 def test_ctypes_structs_match_the_header_layout(tmp_path):
     """The Python binding's structs have the C compiler's sizes and offsets."""
     structs = {"rbffd_pde_params": _lib.PdeParams, "rbffd_request": _lib.Request,
-               "rbffd_server_stats": _lib.ServerStats, "rbffd_weight_params": _lib.WeightParams}
+               "rbffd_server_stats": _lib.ServerStats, "rbffd_weight_params": _lib.WeightParams,
+               "rbffd_eig_output": _lib.EigOutput}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rbffd_sm100.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
