@@ -375,6 +375,52 @@ def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
     out["serving"] = bench_serving(R, torch, ctx)
     out["weights"] = bench_weights(R, torch, ctx)
     out["cosine_bell"] = bench_cosine_bell(R, torch, ctx)
+    out["eigenvalues"] = bench_eigenvalues(R, ctx)
+    return out
+
+
+EIGEN = dict(name="eigenvalues_dense_N4096_n31_lambda_plus_hv", N=4096, n=31, seed=1, deg=2, hv_k=4, gamma=1e-3,
+             eps=(0.035 * 64.0, 6.0))
+
+
+def bench_eigenvalues(R, ctx):
+    """Stability check of the cosine bell's operator Dlambda + hyperviscosity
+    (N=4096, n=31, degree 2, hv_k=4, gamma=1e-3): every eigenvalue of the
+    dense operator on the device (assembly + cuSOLVER geev), at the
+    configuration's eps and at eps = 6; the host's LAPACK dgeev (numpy, all
+    host threads) on the oracle's dense matrix of the same weights at the
+    configuration's eps, as the CPU baseline and the check of the counts."""
+    import oracle as O
+    C = EIGEN
+    N = C["N"]
+    xyz = R.fibonacci_nodes(N, C["seed"])
+    st = R.knn_stencils(xyz, C["n"])
+    grid = R.Grid(ctx, xyz, st)
+    out = {"workload": C["name"]}
+    for k, eps in enumerate(C["eps"]):
+        der = R.RBFFD(R.LAMBDA, grid, 2)
+        der.setUseHyperviscosity(1)
+        der.setHVScalars(C["hv_k"], C["gamma"])
+        der.setEpsilon(eps)
+        der.setPolynomialDegree(C["deg"])
+        der.computeAllWeightsForAllStencils()
+        der.computeEigenvalues(R.LAMBDA)  # loads the solver
+        t = time.perf_counter()
+        _, ev = der.computeEigenvalues(R.LAMBDA, return_eigenvalues=True)
+        gpu_s = time.perf_counter() - t
+        res = {"eps": eps, "gpu_s": gpu_s, "max_real_part": float(ev.real.max()), **der.cachedEigenvalues}
+        if k == 0:
+            A = O.dense_operator(st, None, der.getWeights(R.LAMBDA), der.getWeights(R.HV))
+            t = time.perf_counter()
+            ref = O.eigenvalues(A)
+            res["cpu_lapack_s"] = time.perf_counter() - t
+            res["cpu_threads"] = os.cpu_count()
+            want = O.eig_classify(ref.real)[0]
+            res["counts_equal_lapack"] = all(want[c] == res[c] for c in ("nb_positive", "nb_negative", "nb_zero"))
+            d = np.abs(ev[:, None] - ref[None, :])
+            res["set_distance_rel_spectral_radius"] = float(max(d.min(0).max(), d.min(1).max()) / np.abs(ref).max())
+        out["eps_%g" % eps] = res
+    grid.close()
     return out
 
 
