@@ -285,6 +285,15 @@ int rbffd_pde_get_shape(rbffd_pde* pde, int* lanes_per_row, int* block_threads);
  * get_tiling reports 0 when the stage kernel gathers from global memory. */
 int rbffd_pde_set_tiled_shape(rbffd_pde* pde, int rows_per_block, int lanes, int stream_weights);
 int rbffd_pde_get_tiling(rbffd_pde* pde, int* rows_per_block);
+/* FP32 advection with time-independent coefficients: replace the three
+ * operators of each stage (CosineBell::solve's Dlambda, Dtheta and HV,
+ * cosine_bell.cpp:47-57) by one fused operator
+ * Wf = -(cu W_lambda + cv W_theta) + W_hv, formed once in FP64 from the FP64
+ * weights and rounded to FP32, so a stage streams one weight array instead of
+ * three (beyond the reference; results within FP32 rounding of the
+ * three-operator path, not bit-identical).  on = 0 returns to three
+ * operators.  RBFFD_ERR_UNSUPPORTED for heat or FP64 PDEs. */
+int rbffd_pde_set_fused_operator(rbffd_pde* pde, int on);
 
 /* ---- serving: persistent request loop with continuous batching --------- *
  * No counterpart in the reference, whose drivers run one PDE per process

@@ -82,6 +82,7 @@ PROTOTYPES = {
     "rbffd_pde_get_time": (c_int, [c_void_p, dp]),
     "rbffd_pde_advance": (c_int, [c_void_p, c_int, c_double, c_int, c_int]),
     "rbffd_pde_set_shape": (c_int, [c_void_p, c_int, c_int]),
+    "rbffd_pde_set_fused_operator": (c_int, [c_void_p, c_int]),
     "rbffd_pde_set_tiled_shape": (c_int, [c_void_p, c_int, c_int, c_int]),
     "rbffd_pde_get_tiling": (c_int, [c_void_p, ip]),
     "rbffd_heat_rk4_noalloc": (c_int, [c_void_p, c_int, c_double, c_double, c_int, c_void_p]),

@@ -423,6 +423,10 @@ class TimeDependentPDE:
         self.ctx.check(self.ctx.L.rbffd_pde_get_tiling(self.h, ctypes.byref(r)))
         return a.value, b.value, r.value
 
+    def setFusedOperator(self, on=True):
+        """FP32 advection: one fused operator -(cu Wl + cv Wt) + Whv per stage."""
+        self.ctx.check(self.ctx.L.rbffd_pde_set_fused_operator(self.h, int(bool(on))), "set_fused_operator")
+
     def setTiledShape(self, rows_per_block, lanes=1, stream_weights=False):
         self.ctx.check(self.ctx.L.rbffd_pde_set_tiled_shape(self.h, rows_per_block, lanes, int(stream_weights)),
                        "set_tiled_shape")

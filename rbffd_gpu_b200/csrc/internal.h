@@ -109,6 +109,11 @@ struct rbffd_pde {
     int op[3] = {-1, -1, -1};
     void *u = nullptr, *xa = nullptr, *xb = nullptr, *acc = nullptr;
     void *cu = nullptr, *cv = nullptr;
+    // FP32 advection with one fused operator -(cu W_lambda + cv W_theta) + W_hv
+    // (sliced ELL, formed in FP64 and rounded once): the stages stream one
+    // weight array instead of three
+    float* wf = nullptr;
+    bool fused = false;
     void *d[3] = {nullptr, nullptr, nullptr};  // unfused path: one output per operator
     double* stage64 = nullptr;                  // FP64 staging for host state copies of an FP32 PDE
     double kappa = 1.0;

@@ -441,6 +441,10 @@ static StageParams<T> make_params(rbffd_pde* P, int stage, double dt)
     p.w0 = W(0);
     p.w1 = W(1);
     p.w2 = W(2);
+    if (P->fused) {  // the heat stage with kappa = 1 over the fused operator
+        p.w0 = (const T*)P->wf;
+        p.w1 = p.w2 = nullptr;
+    }
     p.cu = (const T*)P->cu;
     p.cv = (const T*)P->cv;
     T* u = (T*)P->u;
@@ -449,7 +453,7 @@ static StageParams<T> make_params(rbffd_pde* P, int stage, double dt)
     static const double cfac[4] = {0.5, 0.5, 1.0, 0.0};
     double c = stage == 3 ? dt / 6. : cfac[stage] * dt;
     p.c = (T)c;
-    p.kappa = (T)P->kappa;
+    p.kappa = P->fused ? T(1) : (T)P->kappa;
     p.x = stage == 0 ? u : (stage == 1 ? xa : (stage == 2 ? xb : xa));
     p.xnext = stage == 0 ? xa : (stage == 1 ? xb : (stage == 2 ? xa : nullptr));
     p.u = u;
@@ -581,7 +585,7 @@ template <typename T>
 static void launch_stage(rbffd_pde* P, int stage, double dt, Shape sh, cudaStream_t s)
 {
     StageParams<T> p = make_params<T>(P, stage, dt);
-    if (P->kind == KIND_HEAT)
+    if (P->kind == KIND_HEAT || P->fused)
         launch_stage_t<T, KIND_HEAT, false>(P, p, sh, s);
     else if (P->use_hv)
         launch_stage_t<T, KIND_ADVECT, true>(P, p, sh, s);
@@ -626,7 +630,7 @@ static int unfused_stage(rbffd_pde* P, int stage, double dt, cudaStream_t s)
 static Shape autotune(rbffd_pde* P)
 {
     rbffd_ctx* ctx = P->ctx;
-    TuneKey key{P->kind * 4 + (P->use_hv ? 2 : 0), P->dtype, P->T, P->g->N, P->g->n_pad};
+    TuneKey key{P->fused ? KIND_HEAT * 4 : P->kind * 4 + (P->use_hv ? 2 : 0), P->dtype, P->T, P->g->N, P->g->n_pad};
     {
         std::lock_guard<std::mutex> lk(ctx->mu);
         auto it = ctx->tuned.find(key);
@@ -780,7 +784,61 @@ static void pde_free(rbffd_pde* P)
     dev_free(ctx, P->stage64, (size_t)P->g->N * P->T * 8);
     dev_free(ctx, P->cu, (size_t)P->g->N * es);
     dev_free(ctx, P->cv, (size_t)P->g->N * es);
+    dev_free(ctx, P->wf, (size_t)P->g->N32 * P->g->n4 * sizeof(float));
     delete P;
+}
+
+// Fused advection operator of an FP32 PDE, row by row over the padded rows
+// (padding rows and slots 0): Wf = -(cu W_lambda + cv W_theta) (+ W_hv) in
+// FP64 from the FP64 weights and the PDE's FP32 coefficients, rounded once.
+__global__ void k_fuse_operator(float* __restrict__ wf, const double* __restrict__ wl, const double* __restrict__ wt,
+                                const double* __restrict__ wh, const float* __restrict__ cu,
+                                const float* __restrict__ cv, int N, int rows, int nc)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const double a = i < N ? (double)cu[i] : 0.0, c = i < N ? (double)cv[i] : 0.0;
+    for (int s = 0; s < 4 * nc; s++) {
+        const size_t o = sell_elem(i, s, nc);
+        double w = -__fma_rn(a, wl[o], __dmul_rn(c, wt[o]));
+        if (wh) w = __dadd_rn(w, wh[o]);
+        wf[o] = i < N ? __double2float_rn(w) : 0.0f;
+    }
+}
+
+extern "C" int rbffd_pde_set_fused_operator(rbffd_pde* P, int on)
+{
+    if (!P) return RBFFD_ERR_INVALID;
+    rbffd_ctx* ctx = P->ctx;
+    if (!on) {
+        if (P->fused && P->gexec) {
+            cudaGraphExecDestroy(P->gexec);
+            P->gexec = nullptr;
+        }
+        P->fused = false;
+        return RBFFD_OK;
+    }
+    if (P->kind != KIND_ADVECT || P->dtype != RBFFD_F32)
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a fused operator is built for FP32 advection only");
+    if (P->fused) return RBFFD_OK;
+    rbffd_grid* g = P->g;
+    cudaSetDevice(ctx->device);
+    const size_t bytes = (size_t)g->N32 * g->n4 * sizeof(float);
+    if (!P->wf) {
+        int rc = dev_alloc(ctx, (void**)&P->wf, bytes);
+        if (rc) return rc;
+        P->bytes += bytes;
+    }
+    k_fuse_operator<<<(g->N32 + 127) / 128, 128, 0, ctx->stream>>>(
+        P->wf, g->d_w64[P->op[0]], g->d_w64[P->op[1]], P->op[2] >= 0 ? g->d_w64[P->op[2]] : nullptr,
+        (const float*)P->cu, (const float*)P->cv, g->N, g->N32, g->nc);
+    RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    if (P->gexec) {
+        cudaGraphExecDestroy(P->gexec);
+        P->gexec = nullptr;
+    }
+    P->fused = true;
+    return RBFFD_OK;
 }
 
 extern "C" int rbffd_pde_create(rbffd_grid* g, const rbffd_pde_params* prm, rbffd_pde** out)

@@ -187,3 +187,55 @@ def test_multi_tracer_advection(bell, dtype, tol, tiled):
         assert np.array_equal(out, ref)
     else:
         assert rel_l2(out, ref) < tol
+
+
+@pytest.mark.parametrize("ntr,shape", [(1, None), (1, (128, 1)), (16, None), (16, (128, 1)), (16, (64, 1, True))])
+def test_fused_advection_operator_fp32(bell, ntr, shape):
+    """FP32 advection with the three operators fused into one
+    (-(cu Wl + cv Wt) + Whv, formed in FP64, rounded once): within 1e-5
+    (rel. L2) of the FP64 oracle's three-operator RK4; switching back gives the
+    three-operator FP32 bits again."""
+    p = bell["p"]
+    rng = np.random.default_rng(12)
+    u0 = bell["h0"] if ntr == 1 else rng.random((bell["xyz"].shape[0], ntr))
+    steps, dt = 10, p["dt"]
+    ref = O.rk4_advect(bell["st"], None, bell["W"][O.LAMBDA], bell["W"][O.THETA], bell["W"][O.HV], bell["cu"],
+                       bell["cv"], u0, dt, steps)
+
+    def run(fused_then_off=False, fused=True):
+        pde = R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=R.F32, ntracers=ntr)
+        if shape is not None:
+            pde.setTiledShape(*shape)
+        else:
+            pde.setShape(1, 256)
+        if fused or fused_then_off:
+            pde.setFusedOperator(True)
+        pde.fillInitialConditions(u0)
+        if fused_then_off:
+            pde.advance(R.RK4, dt, 30, graph=True)  # a graph of the fused stages exists now
+            pde.setFusedOperator(False)
+            pde.fillInitialConditions(u0)
+            pde.setTime(0.0)
+        pde.advance(R.RK4, dt, steps, graph=True)
+        out = pde.getLocalSolution()
+        pde.close()
+        return out
+
+    fused = run()
+    assert rel_l2(fused, ref) < 1e-5
+    assert np.array_equal(run(fused_then_off=True, fused=False), run(fused=False))
+
+
+def test_fused_operator_errors(bell, heat):
+    pde = R.CosineBell(bell["grid"], bell["der"], bell["p"]["a"], bell["p"]["alpha"], bell["p"]["T"], True,
+                       dtype=R.F64)
+    with pytest.raises(R.RbffdError) as e:
+        pde.setFusedOperator(True)
+    assert e.value.status == -5
+    pde.setFusedOperator(False)  # off is always accepted
+    pde.close()
+    hp = R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=R.F32)
+    with pytest.raises(R.RbffdError) as e:
+        hp.setFusedOperator(True)
+    assert e.value.status == -5
+    hp.close()
