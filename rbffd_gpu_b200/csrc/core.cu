@@ -328,6 +328,7 @@ extern "C" int rbffd_grid_destroy(rbffd_grid* g)
     for (int t = 0; t < 16; t++) {
         dev_free(ctx, g->d_w64[t], wsz * sizeof(double));
         dev_free(ctx, g->d_w32[t], wsz * sizeof(float));
+        dev_free(ctx, g->d_w32s[t], wsz * sizeof(float));
     }
     dev_free(ctx, g->d_idx, wsz * sizeof(int));
     dev_free(ctx, g->d_len, (size_t)g->N * sizeof(int));
@@ -339,6 +340,8 @@ extern "C" int rbffd_grid_destroy(rbffd_grid* g)
         dev_free(ctx, h->d_rows, (size_t)(h->nblocks + 1) * sizeof(int));
         dev_free(ctx, h->d_nodes, h->b_nodes);
         dev_free(ctx, h->d_lidx, h->b_lidx);
+        dev_free(ctx, h->d_lidx_s, h->b_lidx);
+        dev_free(ctx, h->d_slot_s, h->b_lidx);
         delete h;
     }
     delete g;
@@ -347,6 +350,163 @@ extern "C" int rbffd_grid_destroy(rbffd_grid* g)
 
 // Row blocks and their halos (see struct Halo).  Built on the host from the
 // device's stencil array the first time a block size is used.
+// Weights in a slot schedule: element e of the sliced ELL array (row i,
+// scheduled slot t) takes row i's weight at its original slot slot[e], or 0
+// for a padding entry.
+__global__ void k_schedule_f32(const float* __restrict__ w, const unsigned short* __restrict__ slot, size_t n, int nc,
+                               float* __restrict__ ws)
+{
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const size_t q = e >> 2;                      // (slice, chunk, lane) of the element
+    const int i = (int)((q / 32) / nc) * 32 + (int)(q % 32);
+    const unsigned short s = slot[e];
+    ws[e] = s == SLOT_FREE ? 0.0f : w[sell_elem(i, s, nc)];
+}
+
+static void parallel_for(int count, const std::function<void(int)>& f)
+{
+    std::atomic<int> next(0);
+    unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < hw; t++)
+        pool.emplace_back([&]() {
+            for (int k; (k = next.fetch_add(1)) < count;) f(k);
+        });
+    for (auto& t : pool) t.join();
+}
+
+// Slot schedule of one quarter-warp group (rows q0 .. q1-1, at most 8) of a
+// block whose halo has hn positions.  A thread serves one row and, at each of
+// the n4 steps, reads one halo position per row; the 16-byte reads of the
+// group's rows take one shared-memory wavefront when their positions are
+// different mod 8 (the bank group).  Each step is a maximum matching of rows
+// to bank groups (Kuhn's augmenting paths): a row may take a remaining slot
+// of that group (preferring the group it has most slots left in) or, while it
+// has padding entries to spend, a padding entry placed in any free group.
+// Rows that stay unmatched take a remaining slot anyway (a conflict).
+static void schedule_group(const rbffd_grid* g, const std::vector<unsigned short>& lidx, int q0, int q1, int hn,
+                           std::vector<unsigned short>& lidx_s, std::vector<unsigned short>& slot_s)
+{
+    const int nc = g->nc, n4 = g->n4, G = q1 - q0;
+    std::vector<int> by[8][8];  // by[row][group]: remaining slots, the lowest last
+    int realrem[8] = {}, freerem[8] = {};
+    for (int r = 0; r < G; r++) {
+        const int len = g->h_len[q0 + r];
+        for (int s = len - 1; s >= 0; s--) by[r][lidx[sell_elem(q0 + r, s, nc)] & 7].push_back(s);
+        realrem[r] = len;
+        freerem[r] = n4 - len;
+    }
+    for (int t = 0; t < n4; t++) {
+        int pref[8][8], npref[8] = {};
+        for (int r = 0; r < G; r++) {
+            int cs[8], k = 0;
+            for (int c = 0; c < 8; c++)
+                if (!by[r][c].empty()) cs[k++] = c;
+            std::sort(cs, cs + k, [&](int a, int b) { return by[r][a].size() > by[r][b].size(); });
+            for (int j = 0; j < k; j++) pref[r][npref[r]++] = cs[j];
+            if (freerem[r] > 0)
+                for (int c = 0; c < 8; c++)
+                    if (by[r][c].empty()) pref[r][npref[r]++] = c;
+        }
+        int order[8];
+        for (int r = 0; r < G; r++) order[r] = r;
+        std::sort(order, order + G, [&](int a, int b) {
+            if ((freerem[a] == 0) != (freerem[b] == 0)) return freerem[a] == 0;
+            return npref[a] < npref[b];
+        });
+        int owner[8];
+        for (int c = 0; c < 8; c++) owner[c] = -1;
+        std::function<bool(int, unsigned&)> augment = [&](int r, unsigned& seen) {
+            for (int j = 0; j < npref[r]; j++) {
+                const int c = pref[r][j];
+                if (seen & (1u << c)) continue;
+                seen |= 1u << c;
+                if (owner[c] < 0 || augment(owner[c], seen)) {
+                    owner[c] = r;
+                    return true;
+                }
+            }
+            return false;
+        };
+        for (int j = 0; j < G; j++) {
+            unsigned seen = 0;
+            augment(order[j], seen);
+        }
+        int colour[8];
+        for (int r = 0; r < G; r++) colour[r] = -1;
+        for (int c = 0; c < 8; c++)
+            if (owner[c] >= 0) colour[owner[c]] = c;
+        for (int r = 0; r < G; r++) {
+            const size_t e = sell_elem(q0 + r, t, nc);
+            int c = colour[r];
+            if (c < 0 || (by[r][c].empty() && freerem[r] == 0)) {  // unmatched: a conflicting slot
+                c = -1;
+                for (int k = 0; k < 8; k++)
+                    if (!by[r][k].empty() && (c < 0 || by[r][k].size() > by[r][c].size())) c = k;
+            }
+            if (c >= 0 && !by[r][c].empty()) {
+                const int s = by[r][c].back();
+                by[r][c].pop_back();
+                realrem[r]--;
+                slot_s[e] = (unsigned short)s;
+                lidx_s[e] = lidx[sell_elem(q0 + r, s, nc)];
+            } else {  // a padding entry, placed in group c (or 0)
+                freerem[r]--;
+                const int p = c < 0 ? 0 : c;
+                slot_s[e] = SLOT_FREE;
+                lidx_s[e] = (unsigned short)(p < hn ? p : p % std::max(hn, 1));
+            }
+        }
+    }
+}
+
+int grid_halo_schedule(rbffd_grid* g, int R, const Halo** out)
+{
+    const Halo* hc = nullptr;
+    int rc = grid_halo(g, R, &hc);
+    if (rc) return rc;
+    Halo* h = const_cast<Halo*>(hc);
+    if (h->d_lidx_s) {
+        *out = h;
+        return RBFFD_OK;
+    }
+    rbffd_ctx* ctx = g->ctx;
+    if (g->sched_R != 0 && g->sched_R != R)
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a grid keeps one slot schedule");
+    const size_t nidx = (size_t)g->N32 * g->n4;
+    std::vector<unsigned short> lidx(nidx), lidx_s(nidx, 0), slot_s(nidx, SLOT_FREE);
+    std::vector<int> rows(h->nblocks + 1), ptr(h->nblocks + 1);
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    RBFFD_CUDA_TRY(ctx, cudaMemcpy(lidx.data(), h->d_lidx, nidx * sizeof(unsigned short), cudaMemcpyDeviceToHost));
+    RBFFD_CUDA_TRY(ctx, cudaMemcpy(rows.data(), h->d_rows, rows.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    RBFFD_CUDA_TRY(ctx, cudaMemcpy(ptr.data(), h->d_ptr, ptr.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    parallel_for(h->nblocks, [&](int b) {
+        const int hn = ptr[b + 1] - ptr[b];
+        for (int q0 = rows[b]; q0 < rows[b + 1]; q0 += 8)
+            schedule_group(g, lidx, q0, std::min(rows[b + 1], q0 + 8), hn, lidx_s, slot_s);
+    });
+    const size_t bytes = nidx * sizeof(unsigned short);
+    if ((rc = dev_alloc(ctx, (void**)&h->d_lidx_s, bytes))) return rc;
+    if ((rc = dev_alloc(ctx, (void**)&h->d_slot_s, bytes))) {
+        dev_free(ctx, h->d_lidx_s, bytes);
+        h->d_lidx_s = nullptr;
+        return rc;
+    }
+    cudaError_t e = cudaMemcpy(h->d_lidx_s, lidx_s.data(), bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_slot_s, slot_s.data(), bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        dev_free(ctx, h->d_lidx_s, bytes);
+        dev_free(ctx, h->d_slot_s, bytes);
+        h->d_lidx_s = h->d_slot_s = nullptr;
+        return cuda_error(ctx, e, "slot schedule upload");
+    }
+    g->bytes += 2 * bytes;
+    g->sched_R = R;
+    *out = h;
+    return RBFFD_OK;
+}
+
 int grid_halo(rbffd_grid* g, int R, const Halo** out)
 {
     auto it = g->halos.find(R);
@@ -622,6 +782,31 @@ int grid_make_f32(rbffd_grid* g, int op)
     k_cast_f32<<<std::max(1, std::min<int>((int)((n + 255) / 256), ctx->sm_count * 16)), 256, 0, ctx->stream>>>(
         g->d_w64[op], g->d_w32[op], n);
     RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    if (g->d_w32s[op]) {  // keep the scheduled copy in step
+        const Halo* h = g->halos.at(g->sched_R);
+        k_schedule_f32<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(g->d_w32[op], h->d_slot_s, n, g->nc,
+                                                                          g->d_w32s[op]);
+        RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    return RBFFD_OK;
+}
+
+int grid_f32_scheduled(rbffd_grid* g, int op, const float** out)
+{
+    rbffd_ctx* ctx = g->ctx;
+    if (g->sched_R == 0) return set_error(ctx, RBFFD_ERR_STATE, "no slot schedule on this grid");
+    int rc;
+    if (!g->d_w32[op] && (rc = grid_make_f32(g, op))) return rc;
+    if (!g->d_w32s[op]) {
+        const size_t n = (size_t)g->N32 * g->n4;
+        if ((rc = dev_alloc(ctx, (void**)&g->d_w32s[op], n * sizeof(float)))) return rc;
+        g->bytes += n * sizeof(float);
+        const Halo* h = g->halos.at(g->sched_R);
+        k_schedule_f32<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(g->d_w32[op], h->d_slot_s, n, g->nc,
+                                                                          g->d_w32s[op]);
+        RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    *out = g->d_w32s[op];
     return RBFFD_OK;
 }
 

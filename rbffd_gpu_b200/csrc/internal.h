@@ -65,6 +65,8 @@ struct rbffd_grid {
     double4* d_xyz = nullptr;      // [N] node coordinates (w unused)
     double* d_w64[16] = {};        // per operator, sliced ELL N32 x n4: FP64 weights, padding 0
     float* d_w32[16] = {};         // FP32 copies (rounded to nearest)
+    float* d_w32s[16] = {};        // FP32 copies in the slot schedule of halo sched_R
+    int sched_R = 0;               // rows per block of the halo that has a slot schedule (0: none)
     // Rows and nodes are stored in an internal order (a 3-D Morton curve through
     // the nodes) so that rows handled together gather from nearby nodes; the
     // stencil slot order is kept, so each row's arithmetic is unchanged.
@@ -95,8 +97,21 @@ struct Halo {
     int* d_nodes = nullptr;      // node staged at each halo position (internal order)
     unsigned short* d_lidx = nullptr;  // sliced ELL, N32 x n4
     size_t b_nodes = 0, b_lidx = 0;
+    // Conflict-avoiding slot schedule (built on demand, grid_halo_schedule):
+    // each row's slots reordered so that at each step the 8 rows of a
+    // quarter-warp read halo positions in different 16-byte bank groups where
+    // their stencils allow; padding entries (weight 0) take any free group.
+    // Changes the summation order of a row, so only FP32 serving uses it.
+    unsigned short* d_lidx_s = nullptr;  // sliced ELL: position read at scheduled slot t
+    unsigned short* d_slot_s = nullptr;  // original slot of scheduled slot t, SLOT_FREE for padding
 };
+constexpr unsigned short SLOT_FREE = 0xFFFF;
 int grid_halo(rbffd_grid* g, int R, const Halo** out);
+// The halo of R rows per block with its slot schedule.
+int grid_halo_schedule(rbffd_grid* g, int R, const Halo** out);
+// FP32 weights of operator op in the schedule of the grid's scheduled halo
+// (made on first use, refreshed with the FP32 copy).
+int grid_f32_scheduled(rbffd_grid* g, int op, const float** out);
 
 enum { KIND_ADVECT = 0, KIND_HEAT = 1 };
 

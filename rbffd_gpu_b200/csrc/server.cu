@@ -74,8 +74,8 @@ constexpr int SEG_ROWS = 128;               // rows (threads) per block of a sta
 constexpr int BANK_W_F32 = 8;               // columns of an FP32 bank (32-byte rows)
 constexpr int BANK_W_F64 = 4;               // columns of an FP64 bank (32-byte rows)
 constexpr int BANK_W_MAX = 8;
-constexpr double TICK_TARGET_S = 2e-3;      // device time aimed at per batch of steps
-constexpr int TICK_MAX_STEPS = 64;
+constexpr double TICK_TARGET_S = 5e-3;      // device time aimed at per batch of steps
+constexpr int TICK_MAX_STEPS = 160;
 constexpr size_t TABLE_BYTES0 = 64 * 1024;  // initial capacity of the bank tables
 constexpr int TILE_SMEM_MAX = 96 * 1024;    // shared memory for a block's halo values (two blocks per SM)
 
@@ -332,19 +332,28 @@ __global__ void k_column_out(const T* u, int W, int col, double* __restrict__ io
 }
 
 // Fused advection operator of a bank, row by row over the padded rows (sliced
-// ELL; padding rows and slots stay 0): Wf = -(cu W_lambda + cv W_theta) + W_hv.
+// ELL; padding rows and slots stay 0): Wf = -(cu W_lambda + cv W_theta) + W_hv,
+// in the halo's slot schedule when slot is given (entry t of row i takes the
+// row's original slot slot[t], 0 for a padding entry).
 __global__ void k_fuse_advection(float* __restrict__ wf, const double* __restrict__ wl,
                                  const double* __restrict__ wt, const double* __restrict__ wh,
-                                 const double* __restrict__ cu, const double* __restrict__ cv, int N, int rows, int nc)
+                                 const double* __restrict__ cu, const double* __restrict__ cv,
+                                 const unsigned short* __restrict__ slot, int N, int rows, int nc)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
     const double a = i < N ? cu[i] : 0.0, c = i < N ? cv[i] : 0.0;
-    for (int s = 0; s < 4 * nc; s++) {
+    for (int t = 0; t < 4 * nc; t++) {
+        const size_t ot = sell_elem(i, t, nc);
+        const int s = slot ? slot[ot] : t;
+        if (i >= N || s == SLOT_FREE) {
+            wf[ot] = 0.0f;
+            continue;
+        }
         const size_t o = sell_elem(i, s, nc);
         double w = -(a * wl[o] + c * wt[o]);
         if (wh) w += wh[o];
-        wf[o] = i < N ? __double2float_rn(w) : 0.0f;
+        wf[ot] = __double2float_rn(w);
     }
 }
 
@@ -375,6 +384,11 @@ struct Bank {
     void *u = nullptr, *xa = nullptr, *xb = nullptr, *acc = nullptr, *cu = nullptr, *cv = nullptr;
     void* wf = nullptr;  // fused advection operator (FP32 advection banks), sliced ELL
     const Halo* halo = nullptr;  // the grid's row blocks of SEG_ROWS rows (nullptr: untiled)
+    // FP32 tiled banks read the halo's conflict-avoiding slot schedule: local
+    // indices d_lidx_s and weights in the same order (wf, or the grid's
+    // scheduled FP32 copy wsched for heat)
+    bool sched = false;
+    const float* wsched = nullptr;
     size_t bytes = 0;
     int members = 0;       // admitted requests assigned to the bank (S->mu)
     bool in_plan = false;  // referenced by the stepping thread's current tables (S->mu)
@@ -520,6 +534,15 @@ int bank_create(rbffd_server* S, const Request& r, Bank& b)
     const Halo* h = nullptr;
     if (grid_halo(g, SEG_ROWS, &h) == RBFFD_OK && (size_t)h->max_halo * b.Wcap * es <= (size_t)TILE_SMEM_MAX)
         b.halo = h;
+    if (b.halo && b.dtype == RBFFD_F32) {  // FP32: the conflict-avoiding slot schedule
+        const Halo* hs = nullptr;
+        if ((rc = grid_halo_schedule(g, SEG_ROWS, &hs)) ||
+            (b.kind == KIND_HEAT && (rc = grid_f32_scheduled(g, b.op[0], &b.wsched)))) {
+            bank_free_memory(ctx, b);
+            return rc;
+        }
+        b.sched = true;
+    }
     cudaError_t e = cudaMemsetAsync(b.u, 0, n, S->astream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b.xa, 0, n, S->astream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b.xb, 0, n, S->astream);
@@ -543,7 +566,8 @@ int bank_create(rbffd_server* S, const Request& r, Bank& b)
                 const int rows = g->N32;
                 k_fuse_advection<<<(rows + 127) / 128, 128, 0, S->astream>>>(
                     (float*)b.wf, g->d_w64[b.op[0]], g->d_w64[b.op[1]], b.op[2] >= 0 ? g->d_w64[b.op[2]] : nullptr,
-                    (const double*)cu64, (const double*)cv64, g->N, rows, g->nc);
+                    (const double*)cu64, (const double*)cv64, b.sched ? b.halo->d_slot_s : nullptr, g->N, rows,
+                    g->nc);
                 cudaError_t e = cudaGetLastError();
                 if (e == cudaSuccess) e = cudaStreamSynchronize(S->astream);
                 if (e != cudaSuccess) rc = cuda_error(ctx, e, "fused advection operator");
@@ -695,7 +719,7 @@ void fill_desc(BankDesc<T>& d, const Bank& b, int block0)
         return std::is_same<T, double>::value ? (const T*)g->d_w64[b.op[k]] : (const T*)g->d_w32[b.op[k]];
     };
     d.idx = g->d_idx;
-    d.w0 = b.wf ? (const T*)b.wf : W(0);
+    d.w0 = b.wf ? (const T*)b.wf : (b.sched ? (const T*)b.wsched : W(0));
     d.w1 = b.wf ? nullptr : W(1);
     d.w2 = b.wf ? nullptr : W(2);
     d.cu = (const T*)b.cu;
@@ -719,7 +743,7 @@ void fill_desc(BankDesc<T>& d, const Bank& b, int block0)
     d.hrows = b.halo ? b.halo->d_rows : nullptr;
     d.hptr = b.halo ? b.halo->d_ptr : nullptr;
     d.hnodes = b.halo ? b.halo->d_nodes : nullptr;
-    d.lidx = b.halo ? b.halo->d_lidx : nullptr;
+    d.lidx = b.halo ? (b.sched ? b.halo->d_lidx_s : b.halo->d_lidx) : nullptr;
     d.N = g->N;
     d.nc = g->nc;
     d.kind = b.wf ? KIND_HEAT : b.kind;

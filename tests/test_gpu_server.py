@@ -155,7 +155,10 @@ def test_many_requests_on_one_grid_share_launches_bit_exact(ctx, grids):
         srv.stop()
 
 
-def test_served_fp32_equals_one_lane_pde_path(ctx, grids):
+def test_served_fp32_heat_against_oracle_and_pde_path(ctx, grids):
+    """FP32 banks sum each row in the halo's conflict-avoiding slot order:
+    within FP32 rounding of the one-lane FP32 PDE path (stencil order) and
+    within 1e-5 of the FP64 oracle."""
     g = grids[1]
     u0 = _heat_u0(g, 3)
     srv = R.Server(ctx)
@@ -169,9 +172,12 @@ def test_served_fp32_equals_one_lane_pde_path(ctx, grids):
     pde.setShape(1, 128)
     pde.fillInitialConditions(u0)
     pde.advance(R.RK4, 1e-5, 40)
-    ref = pde.getLocalSolution()
+    ref32 = pde.getLocalSolution()
     pde.close()
-    assert np.array_equal(served, ref)
+    ref = O.rk4_heat(g["st"], None, g["W"][O.LSFC], u0, 1e-5, 40)
+    assert rel_l2(served, ref32) < 2e-6
+    assert rel_l2(served, ref) < 1e-5
+    assert not np.array_equal(served, ref32)  # the scheduled order is in use
 
 
 def test_served_fp32_advection_fused_operator(ctx, grids):
@@ -241,7 +247,7 @@ def test_budget_for_one_request_serialises_admission(ctx, grids):
     for u, out in zip(u0, outs):
         pde.fillInitialConditions(u)
         pde.advance(R.RK4, 1e-5, 20)
-        assert np.array_equal(pde.getLocalSolution(), out)
+        assert rel_l2(out, pde.getLocalSolution()) < 2e-6
     pde.close()
 
 
