@@ -49,9 +49,12 @@ def parse():
                     help="setup plus 25 un-graphed RK4 steps with the autotuned kernel shape, for ncu captures")
     ap.add_argument("--profile-multitracer", default=None, metavar="ROWS,LANES",
                     help="16-tracer vortex case on N=163842, n=101 (weights > L2), 3 un-graphed RK4 steps with the "
-                         "tiled shape ROWS,LANES (0,0 = global-memory gathers), for ncu captures")
+                         "tiled shape ROWS,LANES (0,0 = global-memory gathers; a third field f = FP32 fused "
+                         "operator), for ncu captures")
     ap.add_argument("--profile-serving", type=int, default=0, metavar="K",
                     help="serving stage kernels: K + K requests on two N=163842 grids, 3 RK4 steps, for ncu")
+    ap.add_argument("--profile-weights", type=int, default=0, metavar="N",
+                    help="batched weights (the 1e6-stencil mix at N stencils): a tuned call, then one more, for ncu")
     return ap.parse_args()
 
 
@@ -846,7 +849,9 @@ def run_profile():
 def run_profile_multitracer(spec):
     import rbffd_gpu_b200 as R
     from rbffd_gpu_b200 import workloads as WL
-    rows, lanes = (int(x) for x in spec.split(","))
+    fields = spec.split(",")
+    rows, lanes = int(fields[0]), int(fields[1])
+    fused = len(fields) > 2 and fields[2] == "f"
     N, n, T = 163842, 101, 16
     xyz = R.fibonacci_nodes(N, 4)
     st = R.knn_stencils(xyz, n)
@@ -861,6 +866,8 @@ def run_profile_multitracer(spec):
     der.setPolynomialDegree(2)
     der.computeAllWeightsForAllStencils()
     pde = R.Advection(grid, der, cu, cv, True, dtype=R.F32, ntracers=T)
+    if fused:
+        pde.setFusedOperator(True)
     if rows > 0:
         pde.setTiledShape(rows, lanes)
     else:
@@ -868,6 +875,32 @@ def run_profile_multitracer(spec):
     pde.fillInitialConditions(u0)
     pde.advance(R.RK4, 3e-3, 3)
     pde.close()
+    grid.close()
+    ctx.close()
+    print("profile run done")
+
+
+def run_profile_weights(N):
+    """The batched-weights mix (n over {17, 31, 50, 101} with degrees 1-4,
+    eps ~ U[2, 8], XSFC/YSFC/ZSFC) on N stencils: the tuned call, then one
+    more (the launches to capture)."""
+    import rbffd_gpu_b200 as R
+    C = WEIGHTS
+    ctx = R.Context(0)
+    xyz = R.fibonacci_nodes(N, C["seed"])
+    full = R.knn_stencils(xyz, max(C["sizes"]))
+    rng = np.random.default_rng(C["seed"])
+    pick = rng.integers(0, len(C["sizes"]), N)
+    lens = np.array(C["sizes"], dtype=np.int32)[pick]
+    degs = np.array(C["degs"], dtype=np.int32)[pick]
+    eps = rng.uniform(C["eps"][0], C["eps"][1], N)
+    grid = R.Grid(ctx, xyz, full, st_len=lens)
+    der = R.RBFFD(R.XSFC | R.YSFC | R.ZSFC, grid, 2)
+    der.setEpsilon(eps)
+    der.setPolynomialDegree(1, deg_per_row=degs)
+    der.computeAllWeightsForAllStencils()
+    der.computeAllWeightsForAllStencils()
+    ctx.synchronize()
     grid.close()
     ctx.close()
     print("profile run done")
@@ -905,6 +938,8 @@ def main():
     args = parse()
     if args.profile_serving:
         run_profile_serving(args.profile_serving)
+    elif args.profile_weights:
+        run_profile_weights(args.profile_weights)
     elif args.profile_multitracer:
         run_profile_multitracer(args.profile_multitracer)
     elif args.profile:

@@ -433,9 +433,11 @@ bool bank_fits(const Bank& b, const Request& r)
 
 struct rbffd_server {
     rbffd_ctx* ctx = nullptr;
-    cudaStream_t stream = nullptr;   // stepping thread: stage launches, column in/out, results
+    cudaStream_t stream = nullptr;   // stepping thread: stage launches, repacks, column read-outs
     cudaStream_t astream = nullptr;  // admission thread: bank set-up, initial-state uploads
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t cstream = nullptr;  // stepping thread: results copied to the callers
+    cudaEvent_t ev[2][3] = {};       // per batch slot: start, end, finished columns read out
+    cudaEvent_t ev_tab = nullptr;    // the last bank tables copied to the device
     size_t budget = 0;
     int max_active = 0;
     std::mutex mu;  // guards everything below up to the stepping-thread state
@@ -445,6 +447,7 @@ struct rbffd_server {
     std::deque<std::shared_ptr<Request>> pending;  // submitted, not yet admitted
     std::vector<std::shared_ptr<Request>> ready;   // admitted, join at the next step boundary
     std::vector<std::shared_ptr<Request>> active;  // stepping
+    int finishing = 0;  // left `active` with the batch in flight, not yet completed
     std::map<uint64_t, std::shared_ptr<Request>> all;
     std::vector<std::unique_ptr<Bank>> banks;
     uint64_t next_id = 1;
@@ -609,7 +612,7 @@ void admission_loop(rbffd_server* S)
                 ++it;
             }
         if (S->stop) break;
-        const int running = (int)(S->active.size() + S->ready.size());
+        const int running = (int)(S->active.size() + S->ready.size()) + S->finishing;
         if (S->pending.empty() || (S->max_active > 0 && running >= S->max_active)) {
             S->cv_admit.wait(lk);
             continue;
@@ -801,6 +804,7 @@ int upload_tables(rbffd_server* S, std::vector<Launch>& plan)
             }
     if (off > S->tab_cap) {
         const size_t cap = std::max<size_t>(off * 2, TABLE_BYTES0);
+        RBFFD_CUDA_TRY(S->ctx, cudaStreamSynchronize(S->stream));  // no batch reads the old tables
         if (S->h_tab) cudaFreeHost(S->h_tab);
         dev_free(S->ctx, S->d_tab, S->tab_cap);
         S->h_tab = nullptr;
@@ -811,6 +815,7 @@ int upload_tables(rbffd_server* S, std::vector<Launch>& plan)
         if (rc) return rc;
         S->tab_cap = cap;
     }
+    RBFFD_CUDA_TRY(S->ctx, cudaEventSynchronize(S->ev_tab));  // the previous copy has left h_tab
     char* h = (char*)S->h_tab;
     for (size_t l = 0; l < plan.size(); l++) {
         Launch& L = plan[l];
@@ -826,6 +831,7 @@ int upload_tables(rbffd_server* S, std::vector<Launch>& plan)
         }
     }
     if (off) RBFFD_CUDA_TRY(S->ctx, cudaMemcpyAsync(S->d_tab, S->h_tab, off, cudaMemcpyHostToDevice, S->stream));
+    RBFFD_CUDA_TRY(S->ctx, cudaEventRecord(S->ev_tab, S->stream));
     return RBFFD_OK;
 }
 
@@ -893,13 +899,14 @@ void launch_stage(const Launch& L, char* d, int stage, cudaStream_t s)
     }
 }
 
-// Issue nsteps RK4 steps for the planned banks; returns after they complete.
-int run_steps(rbffd_server* S, const std::vector<Launch>& plan, int nsteps, double* seconds, long long* launches,
-              double* bytes)
+// Issue nsteps RK4 steps for the planned banks between the events e0 and e1
+// (returns at once; the batch runs on the stepping stream).
+int launch_steps(rbffd_server* S, const std::vector<Launch>& plan, int nsteps, cudaEvent_t e0, cudaEvent_t e1,
+                 long long* launches, double* bytes)
 {
     char* d = (char*)S->d_tab;
     for (const Launch& L : plan) *bytes += 4.0 * nsteps * L.bytes;
-    RBFFD_CUDA_TRY(S->ctx, cudaEventRecord(S->ev0, S->stream));
+    RBFFD_CUDA_TRY(S->ctx, cudaEventRecord(e0, S->stream));
     for (int step = 0; step < nsteps; step++)
         for (int stage = 0; stage < 4; stage++)
             for (const Launch& L : plan) {
@@ -907,11 +914,7 @@ int run_steps(rbffd_server* S, const std::vector<Launch>& plan, int nsteps, doub
                 ++*launches;
             }
     RBFFD_CUDA_TRY(S->ctx, cudaGetLastError());
-    RBFFD_CUDA_TRY(S->ctx, cudaEventRecord(S->ev1, S->stream));
-    RBFFD_CUDA_TRY(S->ctx, cudaEventSynchronize(S->ev1));
-    float ms = 0.f;
-    RBFFD_CUDA_TRY(S->ctx, cudaEventElapsedTime(&ms, S->ev0, S->ev1));
-    *seconds = ms * 1e-3;
+    RBFFD_CUDA_TRY(S->ctx, cudaEventRecord(e1, S->stream));
     return RBFFD_OK;
 }
 
@@ -972,43 +975,109 @@ void column_out(const Request& r, cudaStream_t s)
     k_column_out<T><<<(N + 255) / 256, 256, 0, s>>>((const T*)b.u, b.W, r.col, r.d_io, b.grid->d_perm, N);
 }
 
-// A leaving request: read its column out into its I/O buffer and,
-// unless it was cancelled, copy the result to the caller; free the buffer.
-int column_leave(rbffd_server* S, Request& r, bool copy_out)
+// A batch of steps in flight.  Requests that finish with it leave the banks
+// when it is issued (their columns are read out into their I/O buffers on the
+// stepping stream right behind it); it completes once the next batch is
+// already queued, so the device does not wait for the host between batches.
+struct Flight {
+    bool on = false, launched = false;
+    int slot = 0, nsteps = 0, rc = RBFFD_OK;
+    long long launches = 0;
+    double bytes = 0.0, nu = 0.0;
+    std::vector<std::shared_ptr<Request>> leave;  // finish with this batch (status set when issued)
+    std::vector<Bank*> banks;                     // banks its tables reference
+};
+
+// Completes a batch (stepping thread, without S->mu): waits for it, copies
+// its finished requests' results to their callers on the copy stream (behind
+// the read-out), frees their I/O buffers, then publishes results, statistics
+// and the banks that no queued batch references any more.
+void complete(rbffd_server* S, Flight& f, const std::vector<Bank*>& still_used)
 {
-    if (r.inserted) {
-        if (r.bank->dtype == RBFFD_F64) column_out<double>(r, S->stream);
-        else column_out<float>(r, S->stream);
+    double secs = 0.0;
+    int rc = f.rc;
+    if (f.launched) {
+        cudaError_t e = cudaEventSynchronize(S->ev[f.slot][1]);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, S->ev[f.slot][0], S->ev[f.slot][1]);
+        if (e != cudaSuccess && rc == RBFFD_OK) rc = cuda_error(S->ctx, e, "batch");
+        secs = ms * 1e-3;
     }
-    const size_t io_bytes = (size_t)r.p.grid->N * sizeof(double);
-    int rc = RBFFD_OK;
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess && copy_out) e = cudaMemcpyAsync(r.p.out, r.d_io, io_bytes, cudaMemcpyDeviceToHost, S->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
-    if (e != cudaSuccess) rc = cuda_error(S->ctx, e, "request result");
-    cudaFreeAsync(r.d_io, S->stream);
-    r.d_io = nullptr;
-    ctx_account(S->ctx, 0, io_bytes);
-    return rc;
+    if (!f.leave.empty()) {
+        cudaError_t e = cudaStreamWaitEvent(S->cstream, S->ev[f.slot][2], 0);
+        for (auto& rp : f.leave) {
+            Request& r = *rp;
+            if (rc != RBFFD_OK && r.status == RBFFD_OK) r.status = rc;
+            if (r.status == RBFFD_OK && e == cudaSuccess)
+                e = cudaMemcpyAsync(r.p.out, r.d_io, (size_t)r.p.grid->N * sizeof(double), cudaMemcpyDeviceToHost,
+                                    S->cstream);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(S->cstream);
+        const int copy_rc = e == cudaSuccess ? RBFFD_OK : cuda_error(S->ctx, e, "request result");
+        for (auto& rp : f.leave) {
+            Request& r = *rp;
+            if (copy_rc != RBFFD_OK && r.status == RBFFD_OK) r.status = copy_rc;
+            if (r.d_io) cudaFreeAsync(r.d_io, S->cstream);
+            r.d_io = nullptr;
+            ctx_account(S->ctx, 0, (size_t)r.p.grid->N * sizeof(double));
+        }
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (f.launched && rc == RBFFD_OK && f.nsteps > 0) S->step_s = secs / f.nsteps;
+    S->st.ticks++;
+    S->st.launches += f.launches;
+    S->st.node_updates += f.nu;
+    S->st.gpu_busy_s += secs;
+    S->st.stage_bytes += f.bytes;
+    for (auto& rp : f.leave) {
+        Request& r = *rp;
+        Bank* b = r.bank;
+        S->owned -= std::min(S->owned, (size_t)r.p.grid->N * sizeof(double));
+        if (--b->members == 0) b->idle_since = Clock::now();
+        r.bank = nullptr;
+        S->finishing--;
+        finish_request(r, r.status);
+        if (r.status == RBFFD_OK) S->st.completed++;
+        else if (r.status == RBFFD_ERR_CANCELLED) S->st.cancelled++;
+        else S->st.failed++;
+    }
+    for (Bank* b : f.banks)
+        if (std::find(still_used.begin(), still_used.end(), b) == still_used.end()) b->in_plan = false;
+    if (!f.leave.empty()) {
+        S->cv_done.notify_all();
+        S->cv_admit.notify_one();  // columns and memory to admit the next requests
+    }
+    f = Flight();
 }
 
 // Stepping thread: admitted requests join at step boundaries; batches of RK4
-// steps for every bank with active columns.
+// steps for every bank with active columns, the next batch queued before the
+// previous one is completed.
 void worker_loop(rbffd_server* S)
 {
     cudaSetDevice(S->ctx->device);
     std::unique_lock<std::mutex> lk(S->mu);
     bool changed = true;
     std::vector<Launch> plan;
+    std::vector<Bank*> plan_banks;  // banks the current tables reference
+    Flight flight;                  // the batch in flight
+    int slot = 0;
     for (;;) {
         const bool hold = S->paused && !S->stop;
         std::vector<std::shared_ptr<Request>> joining;
         if (!hold) {
             joining.swap(S->ready);
             for (auto& r : joining) S->active.push_back(r);
-            S->st.max_active_seen = std::max<long long>(S->st.max_active_seen, (long long)S->active.size());
+            S->st.max_active_seen = std::max<long long>(
+                S->st.max_active_seen, (long long)(S->active.size() + (flight.on ? flight.leave.size() : 0)));
         }
         if (S->active.empty() || hold) {
+            if (flight.on) {  // finish the batch in flight first
+                lk.unlock();
+                complete(S, flight, plan_banks);
+                lk.lock();
+                continue;
+            }
             if (S->active.empty()) {
                 for (auto& b : S->banks) b->in_plan = false;  // no batch in flight
                 if (S->stop && S->admitter_done && S->ready.empty()) break;
@@ -1028,7 +1097,7 @@ void worker_loop(rbffd_server* S)
             }
         lk.unlock();
         int rc = RBFFD_OK;
-        for (Bank* b : dirty) {  // new layouts and initial states, before the batch
+        for (Bank* b : dirty) {  // new layouts and initial states, behind the batch in flight
             if (b->dtype == RBFFD_F64) bank_repack<double>(*b, S->stream);
             else bank_repack<float>(*b, S->stream);
         }
@@ -1045,65 +1114,60 @@ void worker_loop(rbffd_server* S)
         if (changed && rc == RBFFD_OK) {
             rc = upload_tables(S, plan);
             changed = false;
+            plan_banks.clear();
+            for (auto& b : S->banks)
+                if (b->in_plan) plan_banks.push_back(b.get());
         }
+        for (Bank* b : flight.banks) b->in_plan = true;  // still running
         lk.unlock();
-        double secs = 0.0, bytes = 0.0;
-        long long launches = 0;
-        if (rc == RBFFD_OK) rc = run_steps(S, plan, nsteps, &secs, &launches, &bytes);
-        if (rc == RBFFD_OK) S->step_s = secs / nsteps;
-        double nu = 0.0;
-        std::vector<std::shared_ptr<Request>> left;
+        Flight nf;
+        nf.on = true;
+        nf.slot = slot;
+        slot ^= 1;
+        nf.nsteps = nsteps;
+        nf.banks = plan_banks;
+        if (rc == RBFFD_OK) {
+            rc = launch_steps(S, plan, nsteps, S->ev[nf.slot][0], S->ev[nf.slot][1], &nf.launches, &nf.bytes);
+            nf.launched = rc == RBFFD_OK;
+        }
+        nf.rc = rc;
         for (auto& r : act) {
             r->steps_done += nsteps;
-            nu += (double)r->p.grid->N * nsteps;
+            nf.nu += (double)r->p.grid->N * nsteps;
             bool cancel;
             {
                 std::lock_guard<std::mutex> g(S->mu);
                 cancel = r->cancel;
             }
             int st;
-            if (rc != RBFFD_OK) {
-                st = rc;
-                column_leave(S, *r, false);
-            } else if (cancel) {
-                st = RBFFD_ERR_CANCELLED;
-                column_leave(S, *r, false);
-            } else if (r->steps_done >= r->p.nsteps) {
-                st = column_leave(S, *r, true);
-            } else {
-                continue;
+            if (rc != RBFFD_OK) st = rc;
+            else if (cancel) st = RBFFD_ERR_CANCELLED;
+            else if (r->steps_done >= r->p.nsteps) st = RBFFD_OK;
+            else continue;
+            if (st == RBFFD_OK && r->inserted) {  // read the column out right behind the batch
+                if (r->bank->dtype == RBFFD_F64) column_out<double>(*r, S->stream);
+                else column_out<float>(*r, S->stream);
             }
             r->status = st;
-            left.push_back(r);
+            nf.leave.push_back(r);
         }
+        cudaEventRecord(S->ev[nf.slot][2], S->stream);
+        if (cudaGetLastError() != cudaSuccess)
+            for (auto& r : nf.leave)
+                if (r->status == RBFFD_OK) r->status = set_error(S->ctx, RBFFD_ERR_CUDA, "result read-out");
         lk.lock();
-        S->st.ticks++;
-        S->st.launches += launches;
-        S->st.node_updates += nu;
-        S->st.gpu_busy_s += secs;
-        S->st.stage_bytes += bytes;
-        for (auto& rp : left) {
-            Request& r = *rp;
-            Bank* b = r.bank;
-            b->cols[r.col] = nullptr;
+        for (auto& rp : nf.leave) {  // leave the banks now: the next layouts are built without them
+            Bank* b = rp->bank;
+            if (rp->col >= 0 && rp->col < (int)b->cols.size() && b->cols[rp->col] == rp.get()) b->cols[rp->col] = nullptr;
             b->dirty = true;
-            S->owned -= std::min(S->owned, (size_t)r.p.grid->N * sizeof(double));
-            if (--b->members == 0) {
-                b->idle_since = Clock::now();
-                b->in_plan = false;  // the next batch uses tables rebuilt without it
-            }
-            r.bank = nullptr;
-            finish_request(r, r.status);
-            if (r.status == RBFFD_OK) S->st.completed++;
-            else if (r.status == RBFFD_ERR_CANCELLED) S->st.cancelled++;
-            else S->st.failed++;
             S->active.erase(std::find(S->active.begin(), S->active.end(), rp));
+            S->finishing++;
             changed = true;
         }
-        if (!left.empty()) {
-            S->cv_done.notify_all();
-            S->cv_admit.notify_one();  // columns and memory to admit the next requests
-        }
+        lk.unlock();
+        if (flight.on) complete(S, flight, plan_banks);
+        flight = std::move(nf);
+        lk.lock();
     }
 }
 
@@ -1126,8 +1190,11 @@ extern "C" int rbffd_server_start(rbffd_ctx* ctx, double hbm_fraction, int max_a
     const size_t tab = TABLE_BYTES0;
     cudaError_t e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->astream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreate(&S->ev0);
-    if (e == cudaSuccess) e = cudaEventCreate(&S->ev1);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->cstream, cudaStreamNonBlocking);
+    for (int k = 0; k < 2; k++)
+        for (int j = 0; j < 3 && e == cudaSuccess; j++)
+            e = j < 2 ? cudaEventCreate(&S->ev[k][j]) : cudaEventCreateWithFlags(&S->ev[k][j], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->ev_tab, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMallocHost(&S->h_tab, tab);
     if (e == cudaSuccess) e = tile_attrs();
     int rc = e == cudaSuccess ? RBFFD_OK : cuda_error(ctx, e, "rbffd_server_start");
@@ -1135,8 +1202,11 @@ extern "C" int rbffd_server_start(rbffd_ctx* ctx, double hbm_fraction, int max_a
     if (rc != RBFFD_OK) {
         dev_free(ctx, S->d_tab, S->tab_cap);
         if (S->h_tab) cudaFreeHost(S->h_tab);
-        if (S->ev0) cudaEventDestroy(S->ev0);
-        if (S->ev1) cudaEventDestroy(S->ev1);
+        for (int k = 0; k < 2; k++)
+            for (int j = 0; j < 3; j++)
+                if (S->ev[k][j]) cudaEventDestroy(S->ev[k][j]);
+        if (S->ev_tab) cudaEventDestroy(S->ev_tab);
+        if (S->cstream) cudaStreamDestroy(S->cstream);
         if (S->astream) cudaStreamDestroy(S->astream);
         if (S->stream) cudaStreamDestroy(S->stream);
         delete S;
@@ -1244,7 +1314,10 @@ extern "C" int rbffd_server_wait_idle(rbffd_server* S, double timeout_s)
     if (!S || !(timeout_s >= 0.0)) return RBFFD_ERR_INVALID;
     std::unique_lock<std::mutex> lk(S->mu);
     if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
-                             [&] { return S->pending.empty() && S->ready.empty() && S->active.empty(); }))
+                             [&] {
+                                 return S->pending.empty() && S->ready.empty() && S->active.empty() &&
+                                        S->finishing == 0;
+                             }))
         return RBFFD_ERR_TIMEOUT;
     return RBFFD_OK;
 }
@@ -1270,7 +1343,7 @@ extern "C" int rbffd_server_get_stats(rbffd_server* S, rbffd_server_stats* out)
     std::lock_guard<std::mutex> lk(S->mu);
     *out = S->st;
     out->pending = (long long)S->pending.size();
-    out->active = (long long)(S->active.size() + S->ready.size());
+    out->active = (long long)(S->active.size() + S->ready.size()) + S->finishing;
     out->held_bytes = (double)ctx_held(S->ctx);
     return RBFFD_OK;
 }
@@ -1308,12 +1381,15 @@ extern "C" int rbffd_server_stop(rbffd_server* S)
     cudaSetDevice(S->ctx->device);
     cudaStreamSynchronize(S->stream);
     cudaStreamSynchronize(S->astream);
+    cudaStreamSynchronize(S->cstream);
     for (auto& b : S->banks) bank_free_memory(S->ctx, *b);
     S->banks.clear();
     if (S->h_tab) cudaFreeHost(S->h_tab);
     dev_free(S->ctx, S->d_tab, S->tab_cap);
-    cudaEventDestroy(S->ev0);
-    cudaEventDestroy(S->ev1);
+    for (int k = 0; k < 2; k++)
+        for (int j = 0; j < 3; j++) cudaEventDestroy(S->ev[k][j]);
+    cudaEventDestroy(S->ev_tab);
+    cudaStreamDestroy(S->cstream);
     cudaStreamDestroy(S->astream);
     cudaStreamDestroy(S->stream);
     delete S;

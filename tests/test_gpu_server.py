@@ -209,6 +209,29 @@ def test_served_fp32_advection_fused_operator(ctx, grids):
         srv.stop()
 
 
+def test_wait_idle_means_every_request_is_done(ctx, grids):
+    """The next batch is queued before the previous one completes; requests
+    finishing with a batch still count until their results are delivered, so
+    wait_idle returns only once every request is done and its result copied."""
+    srv = R.Server(ctx)
+    try:
+        ids = []
+        for k in range(14):
+            g = grids[k % 2]
+            p = R.heat_params(1.0, R.F32 if k % 3 else R.F64) if k % 2 else _bell_params(R.F32)
+            u0 = _heat_u0(g, k) if k % 2 else _bell_u0(g, k)
+            ids.append(srv.submit(g["grid"], p, u0, 1e-5 if k % 2 else BELL["dt"] / 20, 3 + 7 * k))
+        srv.wait_idle(120)
+        for rid in ids:
+            done, status, _, _ = srv.poll(rid)
+            assert done and status == 0, rid
+            assert np.all(np.isfinite(srv.result(rid)))
+        st = srv.stats()
+        assert st["active"] == 0 and st["pending"] == 0 and st["completed"] == len(ids)
+    finally:
+        srv.stop()
+
+
 def _need_fp32_heat(N):
     """Device bytes of a new FP32 heat bank (u, xa, xb, acc of 8 columns) and one I/O buffer."""
     return N * (4 * 8 * 4 + 8)
