@@ -624,8 +624,13 @@ static int unfused_stage(rbffd_pde* P, int stage, double dt, cudaStream_t s)
 }
 
 // ---------------------------------------------------------------------------
-// autotuner: time stage 0 (which reads u and writes only the scratch buffers
-// xa and acc) for each candidate shape; keep the fastest per problem shape.
+// autotuner.  Round 1 times every candidate shape on the stage sequence
+// 0, 1, 2 (the stages that write only the scratch buffers xa, xb and acc).
+// Round 2 times the three fastest as the solver runs them: 25 full RK4 steps
+// in one CUDA graph, with dt = 0 (every stage then writes u back unchanged,
+// u + 0 * f) and u saved and restored around the timing besides, so the
+// caller's state is untouched.  The fastest of round 2 is kept per problem
+// shape.
 
 static Shape autotune(rbffd_pde* P)
 {
@@ -662,25 +667,22 @@ static Shape autotune(rbffd_pde* P)
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    Shape best = cands[0];
-    float best_ms = 1e30f;
-    // Each candidate: 20 back-to-back stage launches captured in a CUDA graph (as
-    // the solver replays them), one warm replay, then the faster of two timed replays.
     const bool log = getenv("RBFFD_TUNE_LOG") != nullptr;
-    const int reps = 20;
-    for (const Shape& c : cands) {
+    // Launches captured in a CUDA graph, one warm replay, then the fastest of
+    // `trials` timed replays, per launch in ms (negative if the shape failed).
+    auto time_graph = [&](const Shape& c, int launches, bool full_steps, int trials) -> float {
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             cudaGetLastError();
-            continue;
+            return -1.f;
         }
-        for (int r = 0; r < reps; r++) launch_stage_any(P, 0, 0.0, c, ctx->stream);
+        for (int r = 0; r < launches; r++) launch_stage_any(P, full_steps ? r % 4 : r % 3, 0.0, c, ctx->stream);
         cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
         if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
         float ms = 1e30f;
-        for (int trial = 0; e == cudaSuccess && trial < 3; trial++) {
+        for (int trial = 0; e == cudaSuccess && trial <= trials; trial++) {
             cudaEventRecord(e0, ctx->stream);
             e = cudaGraphLaunch(exec, ctx->stream);
             cudaEventRecord(e1, ctx->stream);
@@ -692,17 +694,39 @@ static Shape autotune(rbffd_pde* P)
         if (exec) cudaGraphExecDestroy(exec);
         if (e != cudaSuccess) {
             cudaGetLastError();
-            continue;
+            return -1.f;
         }
         if (log)
-            fprintf(stderr, "[rbffd tune] kind=%d hv=%d dtype=%d T=%d N=%d n_pad=%d lanes=%d block=%d tile=%d tma=%d: %.2f us\n",
+            fprintf(stderr, "[rbffd tune] kind=%d hv=%d dtype=%d T=%d N=%d n_pad=%d lanes=%d block=%d tile=%d tma=%d%s: %.2f us\n",
                     P->kind, P->use_hv, P->dtype, P->T, P->g->N, P->g->n_pad, c.lanes, c.block, c.tile, c.tma,
-                    1e3f * ms / reps);
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = c;
-        }
+                    full_steps ? " (full steps)" : "", 1e3f * ms / launches);
+        return ms / launches;
+    };
+    std::vector<std::pair<float, int>> round1;
+    for (int k = 0; k < (int)cands.size(); k++) {
+        const float t = time_graph(cands[k], 21, false, 2);
+        if (t >= 0.f) round1.push_back({t, k});
     }
+    std::sort(round1.begin(), round1.end());
+    Shape best = round1.empty() ? cands[0] : cands[round1[0].second];
+    const size_t ubytes = (size_t)P->g->N * P->T * (P->dtype == RBFFD_F64 ? 8 : 4);
+    void* saved = nullptr;
+    if (round1.size() > 1 && dev_alloc(ctx, &saved, ubytes) == RBFFD_OK) {
+        if (cudaMemcpyAsync(saved, P->u, ubytes, cudaMemcpyDeviceToDevice, ctx->stream) == cudaSuccess) {
+            float best_ms = 1e30f;
+            for (int r = 0; r < (int)round1.size() && r < 3; r++) {
+                const float t = time_graph(cands[round1[r].second], 100, true, 3);
+                if (t >= 0.f && t < best_ms) {
+                    best_ms = t;
+                    best = cands[round1[r].second];
+                }
+            }
+            cudaMemcpyAsync(P->u, saved, ubytes, cudaMemcpyDeviceToDevice, ctx->stream);
+        }
+        cudaStreamSynchronize(ctx->stream);
+        dev_free(ctx, saved, ubytes);
+    }
+    cudaGetLastError();
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> lk(ctx->mu);
