@@ -699,6 +699,68 @@ def serving_grid(R, ctx, N, n, C):
     return dict(grid=grid, xyz=xyz, heat=dh, adv=da)
 
 
+def _cpu_heat_process(args):
+    """One CPU process of the P-process baseline: the single-threaded oracle's
+    heat RK4 on its own copy of an (N, n) grid with synthetic weights, started
+    at a common wall-clock time; returns (start, end, node-updates)."""
+    N, n, steps, start_at = args
+    import rbffd_gpu_b200 as R
+    import oracle as O
+    xyz = R.fibonacci_nodes(N, 5)
+    st = R.knn_stencils(xyz, n, nthreads=1)
+    w = np.random.default_rng(5).standard_normal((N, n)) * 1e-3
+    u = np.random.default_rng(6).standard_normal(N)
+    while time.time() < start_at:
+        time.sleep(0.001)
+    t0 = time.time()
+    O.rk4_heat(st, None, w, u, 1e-6, steps, nthreads=1)
+    return t0, time.time(), N * steps
+
+
+def serving_cpu_baseline(R, reqs, grids, bell, P):
+    """The served stream on the host's cores: the oracle (single-threaded, one
+    request per process) timed for every (kind, N, n) class of the stream on
+    the cached grids' weights, and P processes of it run at once on one class
+    to measure how the cores share memory bandwidth; the stream's CPU
+    throughput with P independent processes follows from both."""
+    import multiprocessing as mp
+    import oracle as O
+    step_s = {}
+    for r in reqs:
+        cls = (r["heat"], r["N"], r["n"])
+        if cls in step_s:
+            continue
+        g = grids[(r["N"], r["n"])]
+        st = g["grid"].stencils
+        steps = max(1, int(4e6 / (r["N"] * r["n"])))
+        if r["heat"]:
+            w = g["heat"].getWeights(R.LSFC)
+            t = time.perf_counter()
+            O.rk4_heat(st, None, w, r["u0"], r["dt"], steps, nthreads=1)
+        else:
+            wl, wt, wh = (g["adv"].getWeights(k) for k in (R.LAMBDA, R.THETA, R.HV))
+            cu, cv = O.cosine_bell_coeffs(g["xyz"], a=bell["a"], alpha=bell["alpha"], u0=2 * np.pi * bell["a"] / bell["T"])
+            t = time.perf_counter()
+            O.rk4_advect(st, None, wl, wt, wh, cu, cv, r["u0"], r["dt"], steps, nthreads=1)
+        step_s[cls] = (time.perf_counter() - t) / steps
+    one_thread_s = sum(r["steps"] * step_s[(r["heat"], r["N"], r["n"])] for r in reqs)
+    # P processes at once on one mid-size class: the cores' shared-bandwidth efficiency
+    Nc, nc, steps = 40962, 50, 40
+    ctxm = mp.get_context("spawn")
+    with ctxm.Pool(P) as pool:
+        single = pool.map(_cpu_heat_process, [(Nc, nc, steps, time.time() + 2.0)])[0]
+        many = pool.map(_cpu_heat_process, [(Nc, nc, steps, time.time() + 4.0)] * P)
+    rate1 = single[2] / (single[1] - single[0])
+    rateP = sum(m[2] for m in many) / (max(m[1] for m in many) - min(m[0] for m in many))
+    eff = rateP / (P * rate1)
+    work = float(sum(r["N"] * r["steps"] for r in reqs))
+    return {"node_updates_per_s": work / (one_thread_s / (P * eff)), "cores": P, "kind": "port",
+            "single_process_node_updates_per_s": work / one_thread_s, "parallel_efficiency": eff,
+            "sample": "oracle RK4 (FP64, one thread) timed for each of the stream's %d (kind, N, n) classes "
+                      "(1-%d steps each, ~4e6 stencil slots per class); %d concurrent processes on N=%d, n=%d "
+                      "heat for the efficiency" % (len(step_s), max(1, int(4e6 / (2562 * 31))), P, Nc, nc)}
+
+
 def bench_serving(R, torch, ctx):
     """Continuous batching of a Poisson request stream through rbffd_server
     (FP32), against plain one-request-at-a-time FP64 solves (the unfused path:
@@ -781,6 +843,7 @@ def bench_serving(R, torch, ctx):
                 checked.add(cls)
             pde.close()
     srv.stop()
+    cpu = serving_cpu_baseline(R, reqs, grids, bell, os.cpu_count() or 1)
     # plain sequential service of the same arrivals (first come, first served)
     t_free, plain_lat = 0.0, []
     for r in reqs:
@@ -823,6 +886,7 @@ def bench_serving(R, torch, ctx):
                       "class of the sample; service times summed and queued first come, first served on "
                       "the same arrival times"},
         "served_over_plain": served_rate / plain_rate,
+        "cpu_baseline_processes": cpu,
         "rel_l2_served_fp32_vs_fp64_max": max(errs) if errs else None,
         "accuracy_checked_requests": len(errs),
     }
