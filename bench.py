@@ -379,6 +379,52 @@ def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
     out["weights"] = bench_weights(R, torch, ctx)
     out["cosine_bell"] = bench_cosine_bell(R, torch, ctx)
     out["eigenvalues"] = bench_eigenvalues(R, ctx)
+    out["node_order"] = bench_node_order(R, torch, ctx, xyz, st, u0)
+    return out
+
+
+def bench_node_order(R, torch, ctx, xyz, st, u0):
+    """The heat workload (FP32, autotuned stage kernel, 500 graphed steps) with
+    the grid stored in each node order: the Morton curve (the default), reverse
+    Cuthill-McKee, the caller's order (Fibonacci nodes come along a spiral in
+    z), and the caller's order after a random relabelling of the nodes."""
+    W = WORKLOAD
+    N, steps, dt = W["N"], W["steps"], W["dt"]
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    p = np.random.default_rng(11).permutation(N)
+    inv = np.empty(N, dtype=np.int64)
+    inv[p] = np.arange(N)
+    cases = {"morton": (xyz, st, u0, R.ORDER_MORTON), "rcm": (xyz, st, u0, R.ORDER_RCM),
+             "given_fibonacci_spiral": (xyz, st, u0, R.ORDER_GIVEN),
+             "given_random_relabelling": (xyz[p], inv[st[p]].astype(np.int32), u0[p], R.ORDER_GIVEN)}
+    out = {"workload": W["name"]}
+    for name, (x, s_, u, order) in cases.items():
+        t = time.perf_counter()
+        ordr = R.node_order(order, xyz=x, stencils=s_)
+        order_s = time.perf_counter() - t
+        grid = R.Grid(ctx, x, s_, order=order)
+        der = R.RBFFD(R.LSFC, grid, 2)
+        der.setEpsilon(heat_eps(N))
+        der.setPolynomialDegree(W["deg"])
+        der.computeAllWeightsForAllStencils()
+        pde = R.HeatSphere(grid, der, 1.0, dtype=R.F32)
+        pde.fillInitialConditions(u)
+        pde.advance(R.RK4, dt, steps, graph=True)
+        ctx.synchronize()
+        best = 1e30
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
+            e1.record(stream)
+            ctx.synchronize()
+            best = min(best, e0.elapsed_time(e1) * 1e-3)
+        pos = np.empty(N, dtype=np.int64)
+        pos[ordr] = np.arange(N)
+        out[name] = {"node_updates_per_s": N * steps / best, "shape": pde.getShape(), "order_host_s": order_s,
+                     "bandwidth": int(np.abs(pos[s_] - pos[:, None]).max())}
+        pde.close()
+        grid.close()
     return out
 
 

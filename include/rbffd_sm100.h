@@ -95,6 +95,21 @@ int rbffd_exact_cosine_bell(int N, const double* xyz, double sphere_radius, doub
 /* Heat on the unit sphere: u = sum_{l<=lmax,m} c_lm exp(-kappa l(l+1) t) Y_lm (real orthonormal Y_lm). */
 int rbffd_exact_sph_heat(int N, const double* xyz, int lmax, const double* coeffs, double kappa, double t, double* u);
 
+/* ---- node orders -------------------------------------------------------- */
+/* The order in which a grid stores its rows and nodes (the reordering step
+ * before the SpMV: tests/util/cuthill_mckee/{main.cpp,reorder.h}).  order[k]
+ * is the node placed at position k, as the reference's `order` vector
+ * (reorder.h: inv_order[order[i]] = i).  MORTON: along a 3-D Morton curve of
+ * the coordinates (xyz needed), the order grids use by default.  RCM: reverse
+ * Cuthill-McKee on the stencil graph (stencils needed), the order the
+ * reference's utility computes with Boost's cuthill_mckee_ordering
+ * (reorder.h:50-60); ties may break differently from Boost's, whose
+ * neighbour lists keep insertion order.  GIVEN: the caller's order.  Host
+ * only, no GPU. */
+enum rbffd_order_method { RBFFD_ORDER_MORTON = 0, RBFFD_ORDER_RCM = 1, RBFFD_ORDER_GIVEN = 2 };
+int rbffd_node_order(int N, const double* xyz, int n_pad, const int* stencils, const int* st_len, int method,
+                     int* order);
+
 /* ---- grid (nodes + stencils resident on the device) -------------------- */
 /* Uploads nodes and stencils; replaces RBFFD_CL::updateStencilsOnGPU /
  * updateNodesOnGPU (src/rbffd/rbffd_cl.cpp:186-257).  st_len may be NULL
@@ -102,6 +117,12 @@ int rbffd_exact_sph_heat(int N, const double* xyz, int lmax, const double* coeff
  * weight 0, as the reference's ELL packing does (rbffd_cl.cpp:238-242). */
 int rbffd_grid_create(rbffd_ctx* ctx, int N, const double* xyz, int n_pad, const int* stencils, const int* st_len,
                       rbffd_grid** out);
+/* The same with the grid's internal order chosen (rbffd_order_method);
+ * rbffd_grid_create uses RBFFD_ORDER_MORTON.  The order changes where rows
+ * and nodes sit in device memory, never a row's arithmetic: results are the
+ * same bits in every order. */
+int rbffd_grid_create_ordered(rbffd_ctx* ctx, int N, const double* xyz, int n_pad, const int* stencils,
+                              const int* st_len, int order_method, rbffd_grid** out);
 int rbffd_grid_destroy(rbffd_grid* grid);
 /* Device bytes held by the grid (nodes, stencils, all weights). */
 int rbffd_grid_nbytes(const rbffd_grid* grid, size_t* bytes);

@@ -244,3 +244,84 @@ def eig_classify(re, zero_tol=1e-8):
         else:
             o["nb_zero"] += 1
     return o, o["max_neg_eig"]
+
+
+def morton_order(xyz):
+    """The grids' default node order: a 3-D Morton curve of the coordinates
+    scaled to 21-bit integers over the bounding box (bits interleaved x, y, z
+    from the top), ties by index."""
+    xyz = np.asarray(xyz, dtype=np.float64)
+    lo, hi = xyz.min(0), xyz.max(0)
+    ext = hi - lo
+    f = np.where(ext > 0, (xyz - lo) / np.where(ext > 0, ext, 1.0), 0.0)
+    q = np.minimum(2097151.0, np.maximum(0.0, f * 2097151.0)).astype(np.uint64)
+    code = np.zeros(len(xyz), dtype=np.uint64)
+    for b in range(20, -1, -1):
+        for a in range(3):
+            code = (code << np.uint64(1)) | ((q[:, a] >> np.uint64(b)) & np.uint64(1))
+    return np.lexsort((np.arange(len(xyz)), code)).astype(np.int32)
+
+
+def rcm_order(st, st_len=None):
+    """Reverse Cuthill-McKee on the stencil graph, restating the algorithm of
+    the reference's reordering utility (tests/util/cuthill_mckee/reorder.h:50-60,
+    Boost's cuthill_mckee_ordering: starting node per component by
+    find_starting_node's pseudo-peripheral search, neighbours by increasing
+    degree; Boost is not in the reference tree, so ties follow (degree, index)
+    and neighbour lists are sorted by index).  Pure Python: small graphs."""
+    st = np.asarray(st)
+    N, n_pad = st.shape
+    lens = [n_pad] * N if st_len is None else [int(x) for x in st_len]
+    nb = [set() for _ in range(N)]
+    for i in range(N):
+        for j in st[i, :lens[i]]:
+            j = int(j)
+            if j != i:
+                nb[i].add(j)
+                nb[j].add(i)
+    adj = [sorted(s) for s in nb]
+    deg = [len(a) for a in adj]
+    numbered = [False] * N
+
+    def last_level(r):
+        seen = {r}
+        level = [r]
+        ecc = 0
+        while True:
+            nxt = []
+            for v in level:
+                for w in adj[v]:
+                    if not numbered[w] and w not in seen:
+                        seen.add(w)
+                        nxt.append(w)
+            if not nxt:
+                break
+            level = nxt
+            ecc += 1
+        best = level[0]
+        for v in level:
+            if deg[v] < deg[best]:
+                best = v
+        return best, ecc
+
+    cm = []
+    for v0 in range(N):
+        if numbered[v0]:
+            continue
+        r = v0
+        x, ecc_r = last_level(r)
+        y, ecc_x = last_level(x)
+        while ecc_x > ecc_r:
+            r, ecc_r, x = x, ecc_x, y
+            y, ecc_x = last_level(x)
+        head = len(cm)
+        numbered[x] = True
+        cm.append(x)
+        while head < len(cm):
+            v = cm[head]
+            head += 1
+            fresh = [w for w in adj[v] if not numbered[w]]
+            for w in fresh:
+                numbered[w] = True
+            cm.extend(sorted(fresh, key=lambda w: (deg[w], w)))
+    return np.array(cm[::-1], dtype=np.int32)

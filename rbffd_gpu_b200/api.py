@@ -102,6 +102,25 @@ def read_weights_file(filename, stencils, st_len=None, binary=True):
     return w
 
 
+ORDER_MORTON, ORDER_RCM, ORDER_GIVEN = 0, 1, 2
+
+
+def node_order(method, xyz=None, stencils=None, st_len=None):
+    """The node order a grid can use (reorder.h's `order`: order[k] is the
+    node placed at position k): ORDER_MORTON (needs xyz), ORDER_RCM (reverse
+    Cuthill-McKee on the stencil graph; needs stencils) or ORDER_GIVEN.  Host only."""
+    st = None if stencils is None else _i32(stencils)
+    N = len(xyz) if xyz is not None else st.shape[0]
+    n_pad = 0 if st is None else st.shape[1]
+    order = np.zeros(N, dtype=np.int32)
+    rc = _lib.load().rbffd_node_order(N, None if xyz is None else _dp(_f64(xyz)), n_pad,
+                                      None if st is None else _ip(st), None if st_len is None else _ip(_i32(st_len)),
+                                      int(method), _ip(order))
+    if rc:
+        raise RbffdError(rc, "rbffd_node_order")
+    return order
+
+
 def eig_output_dict(o):
     return {k: getattr(o, k) for k, _ in _lib.EigOutput._fields_}
 
@@ -196,7 +215,8 @@ class Context:
 class Grid:
     """Nodes and stencils (the reference Grid: getNodeList, getStencils, getMaxStencilSize)."""
 
-    def __init__(self, ctx, nodes, stencils, st_len=None, global_nodes=None):
+    def __init__(self, ctx, nodes, stencils, st_len=None, global_nodes=None, order=None):
+        """order: the internal node order (ORDER_MORTON by default, ORDER_RCM or ORDER_GIVEN)."""
         self.ctx = ctx
         self.nodes = _f64(nodes)
         self.stencils = _i32(stencils)
@@ -204,8 +224,9 @@ class Grid:
         self.st_len = None if st_len is None else _i32(st_len)
         self.global_nodes = global_nodes or self.N
         h = ctypes.c_void_p()
-        ctx.check(ctx.L.rbffd_grid_create(ctx.h, self.N, _dp(self.nodes), self.n_pad, _ip(self.stencils),
-                                          None if self.st_len is None else _ip(self.st_len), ctypes.byref(h)),
+        ctx.check(ctx.L.rbffd_grid_create_ordered(ctx.h, self.N, _dp(self.nodes), self.n_pad, _ip(self.stencils),
+                                                  None if self.st_len is None else _ip(self.st_len),
+                                                  ORDER_MORTON if order is None else int(order), ctypes.byref(h)),
                   "rbffd_grid_create")
         self.h = h
 

@@ -212,6 +212,12 @@ __global__ void k_xyz4(const double* __restrict__ xyz, int N, double4* __restric
 extern "C" int rbffd_grid_create(rbffd_ctx* ctx, int N, const double* xyz, int n_pad, const int* st, const int* st_len,
                                  rbffd_grid** out)
 {
+    return rbffd_grid_create_ordered(ctx, N, xyz, n_pad, st, st_len, RBFFD_ORDER_MORTON, out);
+}
+
+extern "C" int rbffd_grid_create_ordered(rbffd_ctx* ctx, int N, const double* xyz, int n_pad, const int* st,
+                                         const int* st_len, int order_method, rbffd_grid** out)
+{
     if (!ctx || !out || !xyz || !st || N <= 0 || n_pad <= 0 || n_pad > 1024) return RBFFD_ERR_INVALID;
     *out = nullptr;
     // Host-side validation: every index in range, centre first, lengths in [1, n_pad].
@@ -239,36 +245,18 @@ extern "C" int rbffd_grid_create(rbffd_ctx* ctx, int N, const double* xyz, int n
     g->n4 = round_up(n_pad, 4);
     g->nc = g->n4 / 4;
     g->N32 = round_up(N, 32);
-    // Internal order: nodes sorted along a 3-D Morton curve (21 bits per axis),
-    // ties by index, so consecutive rows are spatial neighbours and share most
-    // of the nodes their stencils gather.
+    // Internal order (rbffd_node_order): by default nodes along a 3-D Morton
+    // curve, so consecutive rows are spatial neighbours and share most of the
+    // nodes their stencils gather.
+    g->h_perm.resize(N);
+    g->h_iperm.resize(N);
     {
-        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        for (int i = 0; i < N; i++)
-            for (int a = 0; a < 3; a++) {
-                lo[a] = std::min(lo[a], xyz[3 * (size_t)i + a]);
-                hi[a] = std::max(hi[a], xyz[3 * (size_t)i + a]);
-            }
-        std::vector<std::pair<uint64_t, int>> key(N);
-        for (int i = 0; i < N; i++) {
-            uint64_t code = 0;
-            uint32_t q[3];
-            for (int a = 0; a < 3; a++) {
-                double ext = hi[a] - lo[a];
-                double f = ext > 0 ? (xyz[3 * (size_t)i + a] - lo[a]) / ext : 0.0;
-                q[a] = (uint32_t)std::min(2097151.0, std::max(0.0, f * 2097151.0));
-            }
-            for (int b = 20; b >= 0; b--)
-                for (int a = 0; a < 3; a++) code = (code << 1) | ((q[a] >> b) & 1u);
-            key[i] = {code, i};
+        const int rc = rbffd_node_order(N, xyz, n_pad, st, st_len, order_method, g->h_perm.data());
+        if (rc) {
+            delete g;
+            return set_error(ctx, rc, "node order %d", order_method);
         }
-        std::sort(key.begin(), key.end());
-        g->h_perm.resize(N);
-        g->h_iperm.resize(N);
-        for (int i = 0; i < N; i++) {
-            g->h_perm[i] = key[i].second;
-            g->h_iperm[key[i].second] = i;
-        }
+        for (int i = 0; i < N; i++) g->h_iperm[g->h_perm[i]] = i;
     }
     std::vector<int> st_int((size_t)N * n_pad, 0);
     std::vector<double> xyz_int((size_t)N * 3);

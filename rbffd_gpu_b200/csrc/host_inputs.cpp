@@ -251,3 +251,180 @@ extern "C" int rbffd_exact_sph_heat(int N, const double* xyz, int lmax, const do
     });
     return RBFFD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Node orders.  A grid stores its rows and nodes in an internal order so that
+// rows handled together gather from nearby nodes (the reordering step before
+// the SpMV, tests/util/cuthill_mckee/{main.cpp,reorder.h} in the reference).
+// order[k] is the node placed at position k, as the reference's `order`
+// vector (reorder.h: inv_order[order[i]] = i).
+//
+//   RBFFD_ORDER_MORTON -- nodes along a 3-D Morton curve: coordinates scaled
+//     to 21-bit integers over the bounding box, bits interleaved x, y, z from
+//     the top, ties by index.  The order every grid uses by default.
+//   RBFFD_ORDER_RCM -- reverse Cuthill-McKee on the stencil graph, the order
+//     the reference's utility computes with Boost's cuthill_mckee_ordering
+//     (reorder.h:50-60; Boost is not part of the reference tree and its version
+//     is not pinned).  Restated from the published algorithm (George & Liu):
+//     the undirected graph joins every stencil's centre to its other nodes;
+//     components are taken in order of their smallest node; each starts from a
+//     pseudo-peripheral node found as Boost's find_starting_node does (from a
+//     node r, x = the first node of least degree, in breadth-first order, on
+//     the last level of r's level structure; repeat from x while its
+//     eccentricity grows); a breadth-first search numbers each node's
+//     unnumbered neighbours by increasing degree (ties by index); the whole
+//     sequence is reversed.  Neighbour lists are sorted by index here, while
+//     Boost keeps insertion order, so ties may break differently.
+namespace {
+
+void morton_order(int N, const double* xyz, int* order)
+{
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < N; i++)
+        for (int a = 0; a < 3; a++) {
+            lo[a] = std::min(lo[a], xyz[3 * (size_t)i + a]);
+            hi[a] = std::max(hi[a], xyz[3 * (size_t)i + a]);
+        }
+    std::vector<std::pair<uint64_t, int>> key(N);
+    for (int i = 0; i < N; i++) {
+        uint64_t code = 0;
+        uint32_t q[3];
+        for (int a = 0; a < 3; a++) {
+            const double ext = hi[a] - lo[a];
+            const double f = ext > 0 ? (xyz[3 * (size_t)i + a] - lo[a]) / ext : 0.0;
+            q[a] = (uint32_t)std::min(2097151.0, std::max(0.0, f * 2097151.0));
+        }
+        for (int b = 20; b >= 0; b--)
+            for (int a = 0; a < 3; a++) code = (code << 1) | ((q[a] >> b) & 1u);
+        key[i] = {code, i};
+    }
+    std::sort(key.begin(), key.end());
+    for (int i = 0; i < N; i++) order[i] = key[i].second;
+}
+
+struct StencilGraph {
+    std::vector<int> ptr, adj;  // CSR, neighbours sorted by index, no self loops
+    int deg(int v) const { return ptr[v + 1] - ptr[v]; }
+};
+
+StencilGraph stencil_graph(int N, int n_pad, const int* st, const int* st_len)
+{
+    std::vector<std::vector<int>> nb(N);
+    for (int i = 0; i < N; i++) {
+        const int L = st_len ? st_len[i] : n_pad;
+        for (int s = 0; s < L; s++) {
+            const int j = st[(size_t)i * n_pad + s];
+            if (j == i) continue;
+            nb[i].push_back(j);
+            nb[j].push_back(i);
+        }
+    }
+    StencilGraph G;
+    G.ptr.assign(N + 1, 0);
+    for (int v = 0; v < N; v++) {
+        std::sort(nb[v].begin(), nb[v].end());
+        nb[v].erase(std::unique(nb[v].begin(), nb[v].end()), nb[v].end());
+        G.ptr[v + 1] = G.ptr[v] + (int)nb[v].size();
+    }
+    G.adj.reserve(G.ptr[N]);
+    for (int v = 0; v < N; v++) G.adj.insert(G.adj.end(), nb[v].begin(), nb[v].end());
+    return G;
+}
+
+// Breadth-first level structure from r over the nodes not yet numbered:
+// returns the first node of least degree on the last level and sets ecc to
+// r's eccentricity.
+int last_level_min_degree(const StencilGraph& G, int r, const std::vector<char>& numbered, std::vector<int>& mark,
+                          int stamp, int* ecc)
+{
+    std::vector<int> level{r}, next;
+    mark[r] = stamp;
+    int e = 0;
+    for (;;) {
+        next.clear();
+        for (int v : level)
+            for (int k = G.ptr[v]; k < G.ptr[v + 1]; k++) {
+                const int w = G.adj[k];
+                if (!numbered[w] && mark[w] != stamp) {
+                    mark[w] = stamp;
+                    next.push_back(w);
+                }
+            }
+        if (next.empty()) break;
+        level.swap(next);
+        e++;
+    }
+    *ecc = e;
+    int best = level[0];
+    for (int v : level)
+        if (G.deg(v) < G.deg(best)) best = v;
+    return best;
+}
+
+void rcm_order(int N, int n_pad, const int* st, const int* st_len, int* order)
+{
+    const StencilGraph G = stencil_graph(N, n_pad, st, st_len);
+    std::vector<char> numbered(N, 0);
+    std::vector<int> mark(N, -1), cm;
+    cm.reserve(N);
+    int stamp = 0;
+    for (int v0 = 0; v0 < N; v0++) {
+        if (numbered[v0]) continue;
+        // starting node of v0's component (Boost's find_starting_node)
+        int r = v0, ecc_r = 0, ecc_x = 0;
+        int x = last_level_min_degree(G, r, numbered, mark, stamp++, &ecc_r);
+        int y = last_level_min_degree(G, x, numbered, mark, stamp++, &ecc_x);
+        while (ecc_x > ecc_r) {
+            r = x;
+            ecc_r = ecc_x;
+            x = y;
+            y = last_level_min_degree(G, x, numbered, mark, stamp++, &ecc_x);
+        }
+        // Cuthill-McKee from x: unnumbered neighbours by increasing degree, ties by index
+        const size_t head0 = cm.size();
+        numbered[x] = 1;
+        cm.push_back(x);
+        std::vector<int> fresh;
+        for (size_t h = head0; h < cm.size(); h++) {
+            const int v = cm[h];
+            fresh.clear();
+            for (int k = G.ptr[v]; k < G.ptr[v + 1]; k++)
+                if (!numbered[G.adj[k]]) {
+                    numbered[G.adj[k]] = 1;
+                    fresh.push_back(G.adj[k]);
+                }
+            std::sort(fresh.begin(), fresh.end(), [&](int a, int b) {
+                return G.deg(a) != G.deg(b) ? G.deg(a) < G.deg(b) : a < b;
+            });
+            cm.insert(cm.end(), fresh.begin(), fresh.end());
+        }
+    }
+    for (int k = 0; k < N; k++) order[k] = cm[N - 1 - k];  // reversed
+}
+
+}  // namespace
+
+extern "C" int rbffd_node_order(int N, const double* xyz, int n_pad, const int* st, const int* st_len, int method,
+                                int* order)
+{
+    if (N <= 0 || !order) return RBFFD_ERR_INVALID;
+    if (method == RBFFD_ORDER_MORTON) {
+        if (!xyz) return RBFFD_ERR_INVALID;
+        morton_order(N, xyz, order);
+        return RBFFD_OK;
+    }
+    if (method == RBFFD_ORDER_GIVEN) {
+        for (int i = 0; i < N; i++) order[i] = i;
+        return RBFFD_OK;
+    }
+    if (method != RBFFD_ORDER_RCM) return RBFFD_ERR_INVALID;
+    if (!st || n_pad <= 0) return RBFFD_ERR_INVALID;
+    for (int i = 0; i < N; i++) {
+        const int L = st_len ? st_len[i] : n_pad;
+        if (L < 1 || L > n_pad) return RBFFD_ERR_INVALID;
+        for (int s = 0; s < L; s++)
+            if (st[(size_t)i * n_pad + s] < 0 || st[(size_t)i * n_pad + s] >= N) return RBFFD_ERR_INVALID;
+    }
+    rcm_order(N, n_pad, st, st_len, order);
+    return RBFFD_OK;
+}

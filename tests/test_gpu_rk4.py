@@ -239,3 +239,31 @@ def test_fused_operator_errors(bell, heat):
         hp.setFusedOperator(True)
     assert e.value.status == -5
     hp.close()
+
+
+@pytest.mark.parametrize("dtype", [R.F64, R.F32])
+def test_autotuner_leaves_the_state_untouched(heat, dtype):
+    """The autotuner times full RK4 steps on the PDE's own buffers (dt = 0,
+    the state saved and restored): a PDE tuned on its first advance gives the
+    same bits as one forced to the chosen shape from the start."""
+    ctx2 = R.Context(0)  # a fresh context: no tuned shape cached yet
+    grid = R.Grid(ctx2, heat["xyz"], heat["st"])
+    der = R.RBFFD(R.LSFC, grid, 2)
+    der.setWeights(R.LSFC, heat["W"][O.LSFC])
+    tuned = R.HeatSphere(grid, der, 1.0, dtype=dtype)
+    tuned.fillInitialConditions(heat["u0"])
+    tuned.advance(R.RK4, 1e-6, 7)
+    lanes, block, rows = tuned.getShape()
+    out_tuned = tuned.getLocalSolution()
+    tuned.close()
+    forced = R.HeatSphere(grid, der, 1.0, dtype=dtype)
+    if rows > 0:
+        forced.setTiledShape(rows, lanes)
+    else:
+        forced.setShape(lanes, block)
+    forced.fillInitialConditions(heat["u0"])
+    forced.advance(R.RK4, 1e-6, 7)
+    assert np.array_equal(forced.getLocalSolution(), out_tuned)
+    forced.close()
+    grid.close()
+    ctx2.close()
