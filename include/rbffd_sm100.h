@@ -90,6 +90,24 @@ int rbffd_stencils_knn(const double* xyz, int N, int n, int* st, int* ties, int 
  * searches the surrounding cells.  Replaces the same reference call
  * (grid_interface.cpp:688-725, KDTree.h:407-433); n <= 255. */
 int rbffd_stencils_knn_gpu(rbffd_ctx* ctx, const double* xyz, int N, int n, int* st, int* ties);
+/* Hash-grid stencils as the reference's cosine-bell experiment generates
+ * them: Grid::generateStencilsHash (src/grids/grid_interface.cpp:733-966,
+ * called at tests/experiments/cosine_bell_on_sphere/main.cpp:197-200).  Not
+ * an exact kNN: candidates come from the nbx x nby x nbz overlay cells around
+ * a node's cell (levels until they hold n nodes, at least one ring).  The
+ * reference renumbers the grid by cell; order[k] is the node placed at k and
+ * st[N][n] (centre first, closest first, ties in decreasing number) and
+ * st_len[N] use the new numbering; stencils are trimmed to the nodes closer
+ * than max_radius (DBL_MAX: no trimming), padding is the centre.  extents
+ * [xmin, xmax, ymin, ymax, zmin, zmax], or NULL for the reference grid's
+ * defaults widened by the nodes (Grid::refreshExtents).  RBFFD_ERR_INVALID
+ * where the reference would not terminate or index out of range (fewer
+ * reachable nodes than n, nodes outside the extents, a flat extent).  As in
+ * the reference, the z cell index is bounded by nby: with nbz > nby some
+ * cells are never searched and some stencils miss their own centre (such
+ * stencils are refused by rbffd_grid_create). */
+int rbffd_stencils_hash(const double* xyz, int N, int n, int nbx, int nby, int nbz, const double* extents,
+                        double max_radius, int* order, int* st, int* st_len);
 /* Cosine bell ExactAdvection::operator() (tests/experiments/cosine_bell_on_sphere/exact_advection.h:37-53). */
 int rbffd_exact_cosine_bell(int N, const double* xyz, double sphere_radius, double* h);
 /* Heat on the unit sphere: u = sum_{l<=lmax,m} c_lm exp(-kappa l(l+1) t) Y_lm (real orthonormal Y_lm). */

@@ -72,6 +72,9 @@ def ref_lib(name):
             L.ref_cart2sph.restype = None
         if L is not None and name == "ref_kdtree":
             L.ref_knn.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _ip, _dp]
+        if L is not None and name == "ref_grid":
+            L.ref_stencils_hash.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            _dp, ctypes.c_double, _dp, _ip, _ip]
         if L is not None and name == "ref_mmio":
             L.ref_mm_write_header.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
             L.ref_mm_read_header.argtypes = [ctypes.c_char_p, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_long)]
@@ -325,3 +328,26 @@ def rcm_order(st, st_len=None):
                 numbered[w] = True
             cm.extend(sorted(fresh, key=lambda w: (deg[w], w)))
     return np.array(cm[::-1], dtype=np.int32)
+
+
+def ref_stencils_hash(xyz, n, dims=(10, 10, 10), extents=None, max_radius=1.7976931348623157e308):
+    """The reference's own Grid::generateStencilsHash (compiled into
+    oracle/_ref/libref_grid.so): (node order, stencils [N][n] in the new
+    numbering padded with -1, stencil lengths).  The order is recovered by
+    matching the re-sorted coordinates to the input (coordinates are unique)."""
+    L = ref_lib("ref_grid")
+    if L is None:
+        return None
+    xyz = _c(xyz, np.float64)
+    N = len(xyz)
+    xs = np.zeros_like(xyz)
+    st = np.zeros((N, n), dtype=np.int32)
+    ln = np.zeros(N, dtype=np.int32)
+    ext = None if extents is None else _c(extents, np.float64)
+    rc = L.ref_stencils_hash(_p(xyz), N, n, dims[0], dims[1], dims[2], _p(ext), max_radius, _p(xs), _p(st, _ip),
+                             _p(ln, _ip))
+    if rc:
+        raise RuntimeError("ref_stencils_hash")
+    key = {tuple(p): i for i, p in enumerate(xyz.tolist())}
+    order = np.array([key[tuple(p)] for p in xs.tolist()], dtype=np.int32)
+    return order, st, ln

@@ -5,6 +5,8 @@
 * ``oracle/_ref/libref_kdtree.so`` -- the reference's own ``external/kdtree/KDTree.h``
   compiled from its sources where they lie (plus ``external/timers/timer_eb.cpp`` and
   ``external/graphics_lib/utilities/Vec3d.cpp``).
+* ``oracle/_ref/libref_grid.so`` -- the reference's own ``Grid::generateStencilsHash``
+  (``src/grids/grid_interface.cpp``), through ``oracle/ref_grid.cpp``;
 * ``oracle/_ref/libref_rbf.so`` -- the reference's own ``src/rbffd/rbfs/rbf_gaussian.h``
   and ``src/utils/geom/cart2sph.cpp``, with ``oracle/shim/armadillo`` standing in
   for the Armadillo header that ``rbf.h`` includes.
@@ -78,6 +80,17 @@ def build_ref(force=False):
                        "-I" + os.path.join(REF, "src"), "-I" + util, rb_src[0], rb_src[2],
                        os.path.join(util, "Vec3d.cpp"), os.path.join(util, "CVec3.cpp"), "-o", rb])
     built.append(rb)
+    gr = os.path.join(outdir, "libref_grid.so")
+    gr_src = [os.path.join(HERE, "ref_grid.cpp"), os.path.join(REF, "src/grids/grid_interface.cpp"),
+              os.path.join(REF, "src/grids/grid_interface.h")]
+    if force or _newer(gr, gr_src):
+        _run(common + ["-std=c++98"] + ["-I" + os.path.join(REF, d) for d in
+                                        ("src", "src/grids", "src/utils", "external/kdtree", "external/timers",
+                                         "external/nist")] +
+             ["-I" + util, gr_src[0], gr_src[1], os.path.join(REF, "src/utils/random.cpp"),
+              os.path.join(util, "Vec3d.cpp"), os.path.join(REF, "external/nist/mmio.cpp"),
+              os.path.join(REF, "external/timers/timer_eb.cpp"), "-o", gr])
+    built.append(gr)
     mm = os.path.join(outdir, "libref_mmio.so")
     mm_src = [os.path.join(HERE, "ref_mmio.cpp"), os.path.join(REF, "external/nist/mmio.cpp")]
     if force or _newer(mm, mm_src):

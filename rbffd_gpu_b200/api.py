@@ -102,6 +102,24 @@ def read_weights_file(filename, stencils, st_len=None, binary=True):
     return w
 
 
+def stencils_hash(xyz, n, dims=(10, 10, 10), extents=None, max_radius=1.7976931348623157e308):
+    """Grid::generateStencilsHash (the cosine-bell experiment's generator):
+    (order, stencils, lengths), the stencils in the new numbering where node
+    order[k] is placed at k.  Host only."""
+    xyz = _f64(xyz)
+    N = len(xyz)
+    order = np.zeros(N, dtype=np.int32)
+    st = np.zeros((N, n), dtype=np.int32)
+    ln = np.zeros(N, dtype=np.int32)
+    ext = None if extents is None else _f64(extents)
+    rc = _lib.load().rbffd_stencils_hash(_dp(xyz), N, n, int(dims[0]), int(dims[1]), int(dims[2]),
+                                         None if ext is None else _dp(ext), float(max_radius), _ip(order), _ip(st),
+                                         _ip(ln))
+    if rc:
+        raise RbffdError(rc, "rbffd_stencils_hash")
+    return order, st, ln
+
+
 ORDER_MORTON, ORDER_RCM, ORDER_GIVEN = 0, 1, 2
 
 

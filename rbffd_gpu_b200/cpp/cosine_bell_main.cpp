@@ -12,6 +12,7 @@
 // default all of the revolutions), POLY_DEG, DTYPE (64 or 32), SEED, GRAPH
 // (1: all steps in one CUDA-graph call) and OUTPUT (file for the final
 // solution, N doubles in node order).
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -46,16 +47,35 @@ int main(int argc, char** argv)
     const double dt = T / steps_per_rev;
     const int dtype = num("DTYPE", 64) == 32 ? RBFFD_F32 : RBFFD_F64;
 
-    // nodes: Fibonacci spiral under a seeded rotation; stencils: n nearest neighbours
+    // nodes: Fibonacci spiral under a seeded rotation.  Stencils as the
+    // reference experiment makes them (main.cpp:197-200): the hash-grid
+    // generator on an NS_NB_X x NS_NB_Y x NS_NB_Z overlay, which renumbers the
+    // nodes by cell; STENCIL_GENERATOR=kdtree takes the n nearest neighbours.
     std::vector<double> xyz(3 * (size_t)N);
     check(nullptr, rbffd_nodes_fibonacci(N, (uint64_t)num("SEED", 1), xyz.data()), "nodes");
-    std::vector<int> st((size_t)N * n);
-    check(nullptr, rbffd_stencils_knn(xyz.data(), N, n, st.data(), nullptr, 0), "stencils");
+    std::vector<int> st((size_t)N * n), len(N, n);
+    const std::string generator = cfg.count("STENCIL_GENERATOR") ? cfg["STENCIL_GENERATOR"] : "hash";
+    if (generator == "kdtree") {
+        check(nullptr, rbffd_stencils_knn(xyz.data(), N, n, st.data(), nullptr, 0), "stencils");
+    } else if (generator == "hash") {
+        std::vector<int> order(N);
+        check(nullptr,
+              rbffd_stencils_hash(xyz.data(), N, n, (int)num("NS_NB_X", 10), (int)num("NS_NB_Y", 10),
+                                  (int)num("NS_NB_Z", 10), nullptr, DBL_MAX, order.data(), st.data(), len.data()),
+              "stencils");
+        std::vector<double> renumbered(3 * (size_t)N);
+        for (int k = 0; k < N; k++)
+            for (int c = 0; c < 3; c++) renumbered[3 * (size_t)k + c] = xyz[3 * (size_t)order[k] + c];
+        xyz.swap(renumbered);
+    } else {
+        std::fprintf(stderr, "STENCIL_GENERATOR must be hash or kdtree\n");
+        return 2;
+    }
     std::vector<Vec3> nodes(N);
     std::vector<StencilType> stencils(N);
     for (int i = 0; i < N; i++) {
         nodes[i] = Vec3{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
-        stencils[i].assign(st.begin() + (size_t)i * n, st.begin() + (size_t)(i + 1) * n);
+        stencils[i].assign(st.begin() + (size_t)i * n, st.begin() + (size_t)i * n + len[i]);
     }
 
     Context ctx(0);

@@ -428,3 +428,135 @@ extern "C" int rbffd_node_order(int N, const double* xyz, int n_pad, const int* 
     rcm_order(N, n_pad, st, st_len, order);
     return RBFFD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Hash-grid stencils: Grid::generateStencilsHash
+// (src/grids/grid_interface.cpp:733-966), the generator the reference's
+// cosine-bell experiment uses (tests/experiments/cosine_bell_on_sphere/main.cpp:197-200).
+// Not an exact nearest-neighbour search: candidates come from the cells around
+// a node's cell, so a closer node just outside them can be missed.  Restated
+// step by step so that the stencils and the node order are the reference's:
+//  * extents: given, or the Grid defaults [0,1] x [0,1] x [0,0] widened by the
+//    nodes (refreshExtents, grid_interface.h:376-398, as GridReader sets them);
+//  * each node's cell (floor of (p - min) / cell size, the top cell closed);
+//  * the node list re-sorted by cell id (nodes of a cell in index order): the
+//    reference renumbers the grid, and order[k] is the node placed at k;
+//  * per node, the cells within Chebyshev level 0, 1, 2, ... joined until they
+//    hold at least n nodes and the level has passed 1; the z index is bounded
+//    by the y cell count, as in the reference (grid_interface.cpp:894);
+//  * candidates by distance sqrt(dx*dx + dy*dy + dz*dz) (Vec3d::magnitude), ties
+//    in decreasing node number (the order the reference's std::set with a
+//    `<=` comparator leaves them in, grid_interface.h:465-471), the first n
+//    below max_radius kept (shorter stencils are trimmed).
+// Where the reference would loop forever (fewer reachable nodes than n) or
+// index out of range (a node outside given extents, a cell id past the last
+// cell), this returns RBFFD_ERR_INVALID instead.
+extern "C" int rbffd_stencils_hash(const double* xyz, int N, int n, int nbx, int nby, int nbz, const double* extents,
+                                   double max_radius, int* order, int* st, int* st_len)
+{
+    if (!xyz || N <= 0 || n < 1 || n > N || nbx < 1 || nby < 1 || nbz < 1 || !order || !st || !st_len)
+        return RBFFD_ERR_INVALID;
+    const unsigned hnx = nbx, hny = nby, hnz = nbz;
+    const size_t ncell = (size_t)hnx * hny * hnz;
+    double lo[3], hi[3];
+    if (extents) {
+        lo[0] = extents[0], hi[0] = extents[1], lo[1] = extents[2], hi[1] = extents[3], lo[2] = extents[4],
+        hi[2] = extents[5];
+    } else {
+        lo[0] = 0., hi[0] = 1., lo[1] = 0., hi[1] = 1., lo[2] = 0., hi[2] = 0.;
+        for (int i = 0; i < N; i++)
+            for (int a = 0; a < 3; a++) {
+                const double v = xyz[3 * (size_t)i + a];
+                if (v < lo[a]) lo[a] = v;
+                if (v > hi[a]) hi[a] = v;
+            }
+    }
+    const double cd[3] = {(hi[0] - lo[0]) / hnx, (hi[1] - lo[1]) / hny, (hi[2] - lo[2]) / hnz};
+    if (!(cd[0] > 0 && cd[1] > 0 && cd[2] > 0)) return RBFFD_ERR_INVALID;  // a flat extent
+    const unsigned hn[3] = {hnx, hny, hnz};
+    std::vector<unsigned> cc(3 * (size_t)N);  // cell coordinates of each node
+    for (int i = 0; i < N; i++)
+        for (int a = 0; a < 3; a++) {
+            const double f = std::floor((xyz[3 * (size_t)i + a] - lo[a]) / cd[a]);
+            if (!(f >= 0.0 && f <= (double)hn[a])) return RBFFD_ERR_INVALID;  // outside the extents
+            unsigned c = (unsigned)f;
+            if (c == hn[a]) c--;
+            cc[3 * (size_t)i + a] = c;
+        }
+    auto cell_of = [&](int i) {
+        return ((size_t)cc[3 * (size_t)i] * hny + cc[3 * (size_t)i + 1]) * hnz + cc[3 * (size_t)i + 2];
+    };
+    // re-sort the nodes by cell: new number k holds old node order[k]
+    std::vector<size_t> start(ncell + 1, 0);
+    for (int i = 0; i < N; i++) start[cell_of(i) + 1]++;
+    for (size_t c = 0; c < ncell; c++) start[c + 1] += start[c];
+    {
+        std::vector<size_t> fill(start.begin(), start.end() - 1);
+        for (int i = 0; i < N; i++) order[fill[cell_of(i)]++] = i;
+    }
+    // node k (new numbering) lies in cell cell_of(order[k]); cell c holds new numbers start[c] .. start[c+1]-1
+    std::atomic<int> failed(0);
+    parallel_for(N, 0, [&](int p) {
+        const int op = order[p];
+        const int xc = (int)cc[3 * (size_t)op], yc = (int)cc[3 * (size_t)op + 1], zc = (int)cc[3 * (size_t)op + 2];
+        static thread_local std::vector<char> in;  // the reference's std::set of non-empty neighbour cells
+        if (in.size() < ncell) in.assign(ncell, 0);
+        std::vector<size_t> cells;
+        struct Clear {  // leave the flags cleared for this thread's next node
+            std::vector<char>& f;
+            std::vector<size_t>& c;
+            ~Clear()
+            {
+                for (size_t k : c) f[k] = 0;
+            }
+        } clear{in, cells};
+        size_t count = 0;
+        const int maxlevel = (int)std::max(hnx, std::max(hny, hnz)) + 1;
+        for (int level = 0; count < (size_t)n || level < 2; level++) {
+            if (level > maxlevel) {  // every reachable cell is in: the reference would not stop
+                failed = 1;
+                return;
+            }
+            const int xl = level, yl = hny > 1 ? level : 0, zl = hnz > 1 ? level : 0;
+            for (int dx = -xl; dx <= xl; dx++)
+                for (int dy = -yl; dy <= yl; dy++)
+                    for (int dz = -zl; dz <= zl; dz++) {
+                        const int xo = xc + dx, yo = yc + dy, zo = zc + dz;
+                        if (xo < 0 || xo >= (int)hnx || yo < 0 || yo >= (int)hny || zo < 0 || zo >= (int)hny)
+                            continue;
+                        const size_t cid = ((size_t)xo * hny + yo) * hnz + zo;
+                        if (cid >= ncell) continue;  // past the last cell: undefined in the reference
+                        if (!in[cid] && start[cid + 1] > start[cid]) {
+                            in[cid] = 1;
+                            cells.push_back(cid);
+                            count += start[cid + 1] - start[cid];
+                        }
+                    }
+        }
+        const double* P = xyz + 3 * (size_t)op;
+        std::vector<std::pair<double, int>> cand;
+        cand.reserve(count);
+        for (size_t cid : cells)
+            for (size_t k = start[cid]; k < start[cid + 1]; k++) {
+                const double* Q = xyz + 3 * (size_t)order[k];
+                const double a = P[0] - Q[0], b = P[1] - Q[1], c = P[2] - Q[2];
+                double s = a * a;
+                s = s + b * b;
+                s = s + c * c;
+                cand.push_back({std::sqrt(s), (int)k});
+            }
+        auto less = [](const std::pair<double, int>& u, const std::pair<double, int>& v) {
+            return u.first < v.first || (u.first == v.first && u.second > v.second);
+        };
+        std::nth_element(cand.begin(), cand.begin() + (n - 1), cand.end(), less);
+        std::sort(cand.begin(), cand.begin() + n, less);
+        int L = 0;
+        while (L < n && cand[L].first < max_radius) {
+            st[(size_t)p * n + L] = cand[L].second;
+            L++;
+        }
+        for (int j = L; j < n; j++) st[(size_t)p * n + j] = p;  // padding: the centre
+        st_len[p] = L;
+    });
+    return failed ? RBFFD_ERR_INVALID : RBFFD_OK;
+}
