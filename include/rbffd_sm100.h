@@ -52,7 +52,8 @@ enum rbffd_dtype { RBFFD_F32 = 0, RBFFD_F64 = 1 };
 enum rbffd_der_type {
     RBFFD_X = 0x1, RBFFD_Y = 0x2, RBFFD_Z = 0x4, RBFFD_LAPL = 0x8, RBFFD_R = 0x10, RBFFD_HV = 0x20,
     RBFFD_LAMBDA = 0x40, RBFFD_THETA = 0x80, RBFFD_LSFC = 0x100, RBFFD_XSFC = 0x200, RBFFD_YSFC = 0x400,
-    RBFFD_ZSFC = 0x800, RBFFD_INTERP = 0x8000
+    RBFFD_ZSFC = 0x800, RBFFD_ALT_XSFC = 0x1000, RBFFD_ALT_YSFC = 0x2000, RBFFD_ALT_ZSFC = 0x4000,
+    RBFFD_INTERP = 0x8000
 };
 
 typedef struct rbffd_ctx rbffd_ctx;
@@ -110,6 +111,20 @@ int rbffd_stencils_hash(const double* xyz, int N, int n, int nbx, int nby, int n
                         double max_radius, int* order, int* st, int* st_len);
 /* Cosine bell ExactAdvection::operator() (tests/experiments/cosine_bell_on_sphere/exact_advection.h:37-53). */
 int rbffd_exact_cosine_bell(int N, const double* xyz, double sphere_radius, double* h);
+/* Vortex roll-up (VortexRollup::solve, src/pdes/hyperbolic/vortex_rollup.cpp:27-57):
+ * w(theta) = Vt / rho per node, rho = 3 cos(theta), Vt = (3 sqrt(3) / 2)
+ * sech(rho)^2 tanh(rho), 0 where |rho| < 4 eps; theta the latitude of
+ * cart2sph.  f = -w D_lambda h is RBFFD_RHS_ADVECTION with cu = w, cv = NULL. */
+int rbffd_vortex_rollup_coefficients(int N, const double* xyz, double* w);
+/* ExactRollup::operator() (tests/experiments/vortex_rollup_on_sphere/exact_rollup.h:25-35):
+ * h = 1 - tanh((rho / 5) sin(lambda - w t)). */
+int rbffd_exact_vortex_rollup(int N, const double* xyz, double t, double* h);
+/* PDE::calcSolNorms (src/pdes/pde.cpp:467-510; src/utils/norms.cpp): out[0..5]
+ * = l1 absolute, l1 relative, l2 absolute, l2 relative, linf absolute, linf
+ * relative of sol against exact over n values, sums in index order; a
+ * relative norm whose exact norm is at most 1e-10 is (abs + 1) / (exact + 1),
+ * as in the reference.  Host only. */
+int rbffd_sol_norms(const double* sol, const double* exact, int n, double* out);
 /* Heat on the unit sphere: u = sum_{l<=lmax,m} c_lm exp(-kappa l(l+1) t) Y_lm (real orthonormal Y_lm). */
 int rbffd_exact_sph_heat(int N, const double* xyz, int lmax, const double* coeffs, double kappa, double t, double* u);
 
@@ -251,7 +266,10 @@ enum rbffd_rhs_kind {
     /* heat on the sphere: f = kappa * D_lsfc u (one Laplace-Beltrami operator, rbffd.cpp:458-464) */
     RBFFD_RHS_HEAT = 2,
     /* advection with caller-given per-node coefficients cu, cv:
-     * f = -(cu * D_lambda h + cv * D_theta h) [+ D_hv h] */
+     * f = -(cu * D_lambda h + cv * D_theta h) [+ D_hv h]; with cv = NULL,
+     * f = -cu * D_lambda h [+ D_hv h] (no D_theta weights needed), the form of
+     * VortexRollup::solve (src/pdes/hyperbolic/vortex_rollup.cpp:27-57) with
+     * cu = rbffd_vortex_rollup_coefficients */
     RBFFD_RHS_ADVECTION = 3
 };
 
@@ -265,7 +283,7 @@ typedef struct rbffd_pde_params {
     double u0;            /* cosine bell speed 2*pi*a / (one revolution) */
     double kappa;         /* heat diffusivity */
     const double* cu;     /* RBFFD_RHS_ADVECTION: host [N] coefficients */
-    const double* cv;
+    const double* cv;     /* (NULL: no D_theta term) */
 } rbffd_pde_params;
 
 /* Creates the device-resident state of a TimeDependentPDE

@@ -75,6 +75,9 @@ def ref_lib(name):
         if L is not None and name == "ref_grid":
             L.ref_stencils_hash.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             _dp, ctypes.c_double, _dp, _ip, _ip]
+        if L is not None and name == "ref_norms":
+            L.ref_sol_norms.argtypes = [_dp, _dp, ctypes.c_int, _dp]
+            L.ref_sol_norms.restype = None
         if L is not None and name == "ref_mmio":
             L.ref_mm_write_header.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
             L.ref_mm_read_header.argtypes = [ctypes.c_char_p, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_long)]
@@ -351,3 +354,54 @@ def ref_stencils_hash(xyz, n, dims=(10, 10, 10), extents=None, max_radius=1.7976
     key = {tuple(p): i for i, p in enumerate(xyz.tolist())}
     order = np.array([key[tuple(p)] for p in xs.tolist()], dtype=np.int32)
     return order, st, ln
+
+
+def alt_sfc(xyz, wx, wy, wz):
+    """ALT_XSFC, ALT_YSFC, ALT_ZSFC from the X, Y, Z weights: the projection
+    (I - x x^T) at each stencil centre, left to right without fused
+    multiply-adds, as RBFFD::computeAllWeightsForStencil_Direct forms them
+    (src/rbffd/rbffd.cpp:337-347).  xyz are the centres, w* [N][n]."""
+    x, y, z = (np.asarray(xyz)[:, k:k + 1] for k in range(3))
+    ax = (1 - x * x) * wx + (-x * y) * wy + (-x * z) * wz
+    ay = (-x * y) * wx + (1 - y * y) * wy + (-y * z) * wz
+    az = (-x * z) * wx + (-y * z) * wy + (1 - z * z) * wz
+    return ax, ay, az
+
+
+def ref_sol_norms(sol, exact):
+    """The reference's own l1/l2/linf norms and calcSolNorms' relative rule
+    (oracle/_ref/libref_norms.so): [l1, l1 rel, l2, l2 rel, linf, linf rel]."""
+    L = ref_lib("ref_norms")
+    out = np.zeros(6)
+    sol, exact = _c(sol, np.float64), _c(exact, np.float64)
+    L.ref_sol_norms(_p(sol), _p(exact), len(sol), _p(out))
+    return out
+
+
+def vortex_rollup_w(xyz):
+    """Angular velocity of VortexRollup::solve (src/pdes/hyperbolic/vortex_rollup.cpp:34-47):
+    theta the cart2sph latitude, rho = 3 cos(theta), Vt = (3 sqrt(3)/2)
+    sech(rho)^2 tanh(rho), w = Vt / rho (0 where |rho| < 4 eps), with the
+    C library's functions through Python's math module."""
+    import math
+    out = np.zeros(len(xyz))
+    c = 3.0 * math.sqrt(3.0) / 2.0
+    for i, (x, y, z) in enumerate(np.asarray(xyz).tolist()):
+        th = math.atan2(z, math.sqrt(x * x + y * y))
+        rho = 3.0 * math.cos(th)
+        s = 1.0 / math.cosh(rho)
+        vt = c * (s * s) * math.tanh(rho)
+        out[i] = 0.0 if abs(rho) < 4.0 * 2.220446049250313e-16 else vt / rho
+    return out
+
+
+def exact_vortex_rollup(xyz, t):
+    """ExactRollup::operator() (tests/experiments/vortex_rollup_on_sphere/exact_rollup.h:25-35),
+    gamma = 5: h = 1 - tanh((rho / gamma) sin(lambda - w t))."""
+    import math
+    w = vortex_rollup_w(xyz)
+    out = np.zeros(len(xyz))
+    for i, (x, y, z) in enumerate(np.asarray(xyz).tolist()):
+        rho = 3.0 * math.cos(math.atan2(z, math.sqrt(x * x + y * y)))
+        out[i] = 1.0 - math.tanh((rho / 5.0) * math.sin(math.atan2(y, x) - w[i] * t))
+    return out

@@ -10,6 +10,8 @@
 * ``oracle/_ref/libref_rbf.so`` -- the reference's own ``src/rbffd/rbfs/rbf_gaussian.h``
   and ``src/utils/geom/cart2sph.cpp``, with ``oracle/shim/armadillo`` standing in
   for the Armadillo header that ``rbf.h`` includes.
+* ``oracle/_ref/libref_norms.so`` -- the reference's own ``src/utils/norms.cpp`` with
+  ``PDE::calcSolNorms``' relative rule, through ``oracle/ref_norms.cpp``.
 * ``oracle/_ref/libref_mmio.so`` -- the reference's own ``external/nist/mmio.cpp``
   (the Matrix Market header of its weight files).
 
@@ -91,6 +93,13 @@ def build_ref(force=False):
               os.path.join(util, "Vec3d.cpp"), os.path.join(REF, "external/nist/mmio.cpp"),
               os.path.join(REF, "external/timers/timer_eb.cpp"), "-o", gr])
     built.append(gr)
+    nm = os.path.join(outdir, "libref_norms.so")
+    nm_src = [os.path.join(HERE, "ref_norms.cpp"), os.path.join(REF, "src/utils/norms.cpp")]
+    if force or _newer(nm, nm_src):
+        _run(common + ["-I" + os.path.join(REF, "src"), "-I" + os.path.join(REF, "src/utils"), "-I" + util,
+                       nm_src[0], nm_src[1], os.path.join(REF, "src/utils/random.cpp"), os.path.join(util, "Vec3d.cpp"),
+                       "-o", nm])
+    built.append(nm)
     mm = os.path.join(outdir, "libref_mmio.so")
     mm_src = [os.path.join(HERE, "ref_mmio.cpp"), os.path.join(REF, "external/nist/mmio.cpp")]
     if force or _newer(mm, mm_src):

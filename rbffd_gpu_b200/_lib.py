@@ -64,6 +64,9 @@ PROTOTYPES = {
     "rbffd_grid_create_ordered": (c_int, [c_void_p, c_int, dp, c_int, ip, ip, c_int, P(c_void_p)]),
     "rbffd_node_order": (c_int, [c_int, dp, c_int, ip, ip, c_int, ip]),
     "rbffd_stencils_hash": (c_int, [dp, c_int, c_int, c_int, c_int, c_int, dp, c_double, ip, ip, ip]),
+    "rbffd_vortex_rollup_coefficients": (c_int, [c_int, dp, dp]),
+    "rbffd_exact_vortex_rollup": (c_int, [c_int, dp, c_double, dp]),
+    "rbffd_sol_norms": (c_int, [dp, dp, c_int, dp]),
     "rbffd_grid_destroy": (c_int, [c_void_p]),
     "rbffd_grid_nbytes": (c_int, [c_void_p, P(c_size_t)]),
     "rbffd_weights_compute": (c_int, [c_void_p, P(WeightParams), dp, c_double, ip]),

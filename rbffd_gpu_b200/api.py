@@ -16,6 +16,7 @@ from . import _lib
 F32, F64 = 0, 1
 X, Y, Z, LAPL, R, HV, LAMBDA, THETA = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20, 0x40, 0x80
 LSFC, XSFC, YSFC, ZSFC, INTERP = 0x100, 0x200, 0x400, 0x800, 0x8000
+ALT_XSFC, ALT_YSFC, ALT_ZSFC = 0x1000, 0x2000, 0x4000
 EULER, MIDPOINT, RK4 = 0, 1, 2  # TimeDependentPDE::TimeScheme (time_dependent_pde.h:20)
 
 ADVANCE_GRAPH, ADVANCE_UNFUSED, ADVANCE_ASYNC = 0x1, 0x2, 0x4
@@ -29,7 +30,7 @@ class RbffdError(RuntimeError):
 
 
 def _dp(a):
-    return a.ctypes.data_as(_lib.dp)
+    return None if a is None else a.ctypes.data_as(_lib.dp)
 
 
 def _ip(a):
@@ -100,6 +101,39 @@ def read_weights_file(filename, stencils, st_len=None, binary=True):
     if rc:
         raise RbffdError(rc, "rbffd_weights_file_read(%s)" % filename)
     return w
+
+
+def vortex_rollup_coefficients(xyz):
+    """w(theta) of VortexRollup::solve per node (vortex_rollup.cpp:34-47)."""
+    xyz = _f64(xyz)
+    w = np.zeros(len(xyz))
+    rc = _lib.load().rbffd_vortex_rollup_coefficients(len(xyz), _dp(xyz), _dp(w))
+    if rc:
+        raise RbffdError(rc, "rbffd_vortex_rollup_coefficients")
+    return w
+
+
+def exact_vortex_rollup(xyz, t):
+    """ExactRollup (exact_rollup.h:25-35)."""
+    xyz = _f64(xyz)
+    h = np.zeros(len(xyz))
+    rc = _lib.load().rbffd_exact_vortex_rollup(len(xyz), _dp(xyz), float(t), _dp(h))
+    if rc:
+        raise RbffdError(rc, "rbffd_exact_vortex_rollup")
+    return h
+
+
+NORM_NAMES = ("l1", "l1_rel", "l2", "l2_rel", "linf", "linf_rel")
+
+
+def sol_norms(sol, exact):
+    """PDE::calcSolNorms (pde.cpp:467-510): absolute and relative l1, l2, linf errors."""
+    sol, exact = _f64(sol).ravel(), _f64(exact).ravel()
+    out = np.zeros(6)
+    rc = _lib.load().rbffd_sol_norms(_dp(sol), _dp(exact), len(sol), _dp(out))
+    if rc:
+        raise RbffdError(rc, "rbffd_sol_norms")
+    return dict(zip(NORM_NAMES, out.tolist()))
 
 
 def stencils_hash(xyz, n, dims=(10, 10, 10), extents=None, max_radius=1.7976931348623157e308):
@@ -281,6 +315,7 @@ class RBFFD:
     """Mirror of class RBFFD (src/rbffd/rbffd.h:29-547) on the device."""
     X, Y, Z, LAPL, R, HV, LAMBDA, THETA = X, Y, Z, LAPL, R, HV, LAMBDA, THETA
     LSFC, XSFC, YSFC, ZSFC, INTERP = LSFC, XSFC, YSFC, ZSFC, INTERP
+    ALT_XSFC, ALT_YSFC, ALT_ZSFC = ALT_XSFC, ALT_YSFC, ALT_ZSFC
 
     def __init__(self, typesToCompute, grid, dim_num, rank=0):
         self.computedTypes = typesToCompute
@@ -327,7 +362,15 @@ class RBFFD:
         self.deg_per_row = None if deg_per_row is None else _i32(deg_per_row)
 
     # -- weights --
+    def adjustForSFCTypes(self):
+        """rbffd.h:507-522: any ALT_*SFC type brings X, Y, Z and all three ALT types."""
+        if self.computedTypes & (ALT_XSFC | ALT_YSFC | ALT_ZSFC):
+            self.computedTypes |= X | Y | Z | ALT_XSFC | ALT_YSFC | ALT_ZSFC
+            return True
+        return False
+
     def computeAllWeightsForAllStencils(self):
+        self.adjustForSFCTypes()
         ctx = self.grid.ctx
         p = _lib.WeightParams(self.computedTypes, self.dim_num, self.poly_deg, self.hv_k, self.hv_gamma,
                               float(self.grid.getGlobalNodeListSize()))
@@ -444,6 +487,26 @@ class TimeDependentPDE:
             ADVANCE_ASYNC if asynchronous else 0)
         self.ctx.check(self.ctx.L.rbffd_pde_advance(self.h, which, delta_t, nsteps, flags), "rbffd_pde_advance")
 
+    def checkLocalError(self, exact, rel_err_max=-1.0):
+        """PDE::checkLocalError / checkError (pde.h:120-127, pde.cpp:385-465):
+        the error norms of the solution against the exact values, printed per
+        node group as the reference prints them (the sphere has no boundary
+        nodes: the boundary group is empty, the other three are the whole
+        grid); returns the whole grid's norms.  Like checkLocalError, a high
+        error is reported, never fatal."""
+        u = self.getLocalSolution()
+        full = sol_norms(u, exact)
+        empty = sol_norms(np.zeros(0), np.zeros(0))
+        for label, nrm, cnt in (("Boundary", empty, 0), ("Interior Stencils w/o Boundary", full, u.size),
+                                ("All Interior", full, u.size), ("Interior & Boundary", full, u.size)):
+            for p in ("l1", "l2", "linf"):
+                print("%s %s error (%d nodes):   Absolute = %le,    Relative = %le " % (
+                    label, p, cnt, nrm[p], nrm[p + "_rel"]))
+        if rel_err_max > 0 and full["l2_rel"] > rel_err_max:
+            print("[PDE] Error! l2 relative error (=%f%%) is too high to continue. We require %f%% or less." % (
+                100.0 * full["l2_rel"], 100.0 * rel_err_max))
+        return full
+
     def setTime(self, t):
         self.ctx.check(self.ctx.L.rbffd_pde_set_time(self.h, t))
 
@@ -500,10 +563,20 @@ class Advection(TimeDependentPDE):
     """f = -(cu * D_lambda h + cv * D_theta h) [+ D_hv h] with caller-given per-node coefficients."""
 
     def __init__(self, grid, der, cu, cv, useHyperviscosity, dtype=F64, ntracers=1):
-        self._cu, self._cv = _f64(cu), _f64(cv)
+        """cv None: no D_theta term (f = -cu D_lambda h [+ D_hv h])."""
+        self._cu, self._cv = _f64(cu), None if cv is None else _f64(cv)
         p = _lib.PdeParams(RHS_ADVECTION, ntracers, dtype, int(useHyperviscosity), 1.0, 0.0, 0.0, 1.0,
                            _dp(self._cu), _dp(self._cv))
         super().__init__(grid, der, p)
+
+
+class VortexRollup(Advection):
+    """VortexRollup (src/pdes/hyperbolic/vortex_rollup.h:7-30):
+    f = -w(theta) * D_lambda h [+ D_hv h]; needs the LAMBDA (and HV) weights only."""
+
+    def __init__(self, grid, der, useHyperviscosity, dtype=F64, ntracers=1):
+        super().__init__(grid, der, vortex_rollup_coefficients(grid.nodes), None, useHyperviscosity, dtype=dtype,
+                         ntracers=ntracers)
 
 
 # ---------------------------------------------------------------------------

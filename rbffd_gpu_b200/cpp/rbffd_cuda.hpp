@@ -82,7 +82,8 @@ public:
     {
         const int N = (int)nodes.size();
         for (const StencilType& s : stencils) n_pad_ = std::max(n_pad_, (int)s.size());
-        std::vector<double> xyz(3 * (size_t)N);
+        std::vector<double>& xyz = xyz_;
+        xyz.resize(3 * (size_t)N);
         for (int i = 0; i < N; i++) {
             xyz[3 * i] = nodes[i].x;
             xyz[3 * i + 1] = nodes[i].y;
@@ -113,12 +114,15 @@ public:
     // stencils as [N][getMaxStencilSize()] (padding = centre) and their lengths
     const std::vector<int>& paddedStencils() const { return st_; }
     const std::vector<int>& stencilLengths() const { return len_; }
+    // node coordinates as [N][3]
+    const std::vector<double>& coordinates() const { return xyz_; }
 
 private:
     Context& ctx_;
     std::vector<Vec3> nodes_;
     std::vector<StencilType> stencils_;
     std::vector<int> st_, len_;
+    std::vector<double> xyz_;
     unsigned global_;
     int n_pad_ = 1;
     rbffd_grid* h_ = nullptr;
@@ -130,7 +134,8 @@ public:
     enum DerType {
         X = RBFFD_X, Y = RBFFD_Y, Z = RBFFD_Z, LAPL = RBFFD_LAPL, R = RBFFD_R, HV = RBFFD_HV,
         LAMBDA = RBFFD_LAMBDA, THETA = RBFFD_THETA, LSFC = RBFFD_LSFC, XSFC = RBFFD_XSFC, YSFC = RBFFD_YSFC,
-        ZSFC = RBFFD_ZSFC, INTERP = RBFFD_INTERP
+        ZSFC = RBFFD_ZSFC, ALT_XSFC = RBFFD_ALT_XSFC, ALT_YSFC = RBFFD_ALT_YSFC, ALT_ZSFC = RBFFD_ALT_ZSFC,
+        INTERP = RBFFD_INTERP
     };
     typedef unsigned int DerTypes;
     enum DataType { FP32 = RBFFD_F32, FP64 = RBFFD_F64 };
@@ -195,8 +200,17 @@ public:
     }
 
     // -- weights --
+    // rbffd.h:507-522: any ALT_*SFC type brings X, Y, Z and all three ALT types
+    bool adjustForSFCTypes()
+    {
+        const DerTypes alt = ALT_XSFC | ALT_YSFC | ALT_ZSFC;
+        if (!(computedTypes & alt)) return false;
+        computedTypes |= X | Y | Z | alt;
+        return true;
+    }
     void computeAllWeightsForAllStencils()
     {
+        adjustForSFCTypes();
         rbffd_weight_params p;
         p.der_types = computedTypes;
         p.dim = dim_num;
@@ -369,6 +383,28 @@ public:
         return u;
     }
     void setTime(double t) { check(ctx(), rbffd_pde_set_time(h_, t), "setTime"); }
+    // PDE::checkLocalError (pde.h:120-127): the solution's error norms against
+    // exact values, printed as the reference prints them (no boundary nodes on
+    // the sphere); a high error is reported, never fatal.  Returns the norms
+    // rbffd_sol_norms gives: l1, l1 rel, l2, l2 rel, linf, linf rel.
+    std::vector<double> checkLocalError(const std::vector<double>& exact, double rel_err_max = -1.)
+    {
+        std::vector<double> u = getLocalSolution(), nrm(6), none(6);
+        check(nullptr, rbffd_sol_norms(u.data(), exact.data(), (int)u.size(), nrm.data()), "checkLocalError");
+        check(nullptr, rbffd_sol_norms(nullptr, nullptr, 0, none.data()), "checkLocalError");
+        const char* labels[4] = {"Boundary", "Interior Stencils w/o Boundary", "All Interior", "Interior & Boundary"};
+        const char* p[3] = {"l1", "l2", "linf"};
+        for (int g = 0; g < 4; g++)
+            for (int k = 0; k < 3; k++) {
+                const std::vector<double>& v = g == 0 ? none : nrm;
+                std::printf("%s %s error (%d nodes):   Absolute = %le,    Relative = %le \n", labels[g], p[k],
+                            g == 0 ? 0 : (int)u.size(), v[2 * k], v[2 * k + 1]);
+            }
+        if (rel_err_max > 0 && nrm[3] > rel_err_max)
+            std::printf("[PDE] Error! l2 relative error (=%f%%) is too high to continue. We require %f%% or less.\n",
+                        100. * nrm[3], 100. * rel_err_max);
+        return nrm;
+    }
     double getTime()
     {
         double t = 0.0;
@@ -459,6 +495,35 @@ private:
         p.use_hv = hv;
         p.cu = cu.data();
         p.cv = cv.data();
+        return p;
+    }
+};
+
+// VortexRollup(Domain*, RBFFD*, Communicator*, int useHyperviscosity) (vortex_rollup.h:16):
+// f = -w(theta) D_lambda h [+ D_hv h], w from rbffd_vortex_rollup_coefficients.
+class VortexRollup_CUDA : public TimeDependentPDE_CUDA {
+public:
+    VortexRollup_CUDA(Grid_CUDA* grid, RBFFD_CUDA* der, int useHyperviscosity, int dtype = RBFFD_F64,
+                      int ntracers = 1)
+        : TimeDependentPDE_CUDA(grid, der, params(coefficients(*grid), useHyperviscosity, dtype, ntracers))
+    {
+    }
+
+private:
+    static const std::vector<double>& coefficients(Grid_CUDA& g)
+    {
+        static thread_local std::vector<double> w;  // read by rbffd_pde_create inside the base constructor
+        const std::vector<double>& xyz = g.coordinates();
+        w.assign(xyz.size() / 3, 0.0);
+        check(nullptr, rbffd_vortex_rollup_coefficients((int)w.size(), xyz.data(), w.data()), "VortexRollup");
+        return w;
+    }
+    static rbffd_pde_params params(const std::vector<double>& w, int hv, int dtype, int ntracers)
+    {
+        rbffd_pde_params p = pde_params(RBFFD_RHS_ADVECTION, dtype, ntracers);
+        p.use_hv = hv;
+        p.cu = w.data();
+        p.cv = nullptr;
         return p;
     }
 };

@@ -560,3 +560,68 @@ extern "C" int rbffd_stencils_hash(const double* xyz, int N, int n, int nbx, int
     });
     return failed ? RBFFD_ERR_INVALID : RBFFD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Vortex roll-up and solution norms.
+
+namespace {
+
+// The angular velocity of VortexRollup::solve / ExactRollup at one node, with
+// the reference's operations: latitude from cart2sph, sech = 1 / cosh.
+double rollup_w(double x, double y, double z, double* rho_out)
+{
+    const double theta_p = std::atan2(z, std::sqrt(x * x + y * y));
+    const double rho_p = 3. * std::cos(theta_p);
+    const double sech = 1. / std::cosh(rho_p);
+    const double Vt = (3. * std::sqrt(3.) / 2.) * (sech * sech) * std::tanh(rho_p);
+    if (rho_out) *rho_out = rho_p;
+    return (std::fabs(rho_p) < 4. * 2.220446049250313080847e-16) ? 0. : Vt / rho_p;
+}
+
+}  // namespace
+
+extern "C" int rbffd_vortex_rollup_coefficients(int N, const double* xyz, double* w)
+{
+    if (N < 0 || !xyz || !w) return RBFFD_ERR_INVALID;
+    for (int i = 0; i < N; i++) w[i] = rollup_w(xyz[3 * (size_t)i], xyz[3 * (size_t)i + 1], xyz[3 * (size_t)i + 2], nullptr);
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_exact_vortex_rollup(int N, const double* xyz, double t, double* h)
+{
+    if (N < 0 || !xyz || !h) return RBFFD_ERR_INVALID;
+    const double gamma = 5.;
+    for (int i = 0; i < N; i++) {
+        const double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
+        double rho_p;
+        const double w = rollup_w(x, y, z, &rho_p);
+        const double phi_p = std::atan2(y, x);
+        h[i] = 1. - std::tanh((rho_p / gamma) * std::sin(phi_p - w * t));
+    }
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_sol_norms(const double* sol, const double* exact, int n, double* out)
+{
+    if (n < 0 || !out || (n > 0 && (!sol || !exact))) return RBFFD_ERR_INVALID;
+    double l1 = 0., l1d = 0., l2 = 0., l2d = 0., li = 0., lid = 0.;
+    for (int i = 0; i < n; i++) {  // norms.cpp: l1norm, l2norm, linfnorm, in index order
+        const double err = std::fabs(sol[i] - exact[i]);
+        l1 += err;
+        l2 += err * err;
+        li = (li < err) ? err : li;
+        l1d += std::fabs(exact[i]);
+        l2d += exact[i] * exact[i];
+        lid = (lid < std::fabs(exact[i])) ? std::fabs(exact[i]) : lid;
+    }
+    l2 = std::sqrt(l2);
+    l2d = std::sqrt(l2d);
+    auto rel = [](double a, double d) { return d > 1e-10 ? a / d : (a + 1.) / (d + 1.); };  // pde.cpp:470-480
+    out[0] = l1;
+    out[1] = rel(l1, l1d);
+    out[2] = l2;
+    out[3] = rel(l2, l2d);
+    out[4] = li;
+    out[5] = rel(li, lid);
+    return RBFFD_OK;
+}

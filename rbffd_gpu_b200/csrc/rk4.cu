@@ -764,7 +764,7 @@ int advect_coefficients(rbffd_grid* g, const rbffd_pde_params* prm, void* cu_dev
     } else {
         for (int i = 0; i < N; i++) {  // caller's node order -> internal row order
             cu[i] = prm->cu[g->h_perm[i]];
-            cv[i] = prm->cv[g->h_perm[i]];
+            cv[i] = prm->cv ? prm->cv[g->h_perm[i]] : 0.0;
         }
     }
     if (prm->dtype == RBFFD_F64) {
@@ -884,8 +884,11 @@ extern "C" int rbffd_pde_create(rbffd_grid* g, const rbffd_pde_params* prm, rbff
         ops[0] = der_index(RBFFD_LAMBDA);
         ops[1] = der_index(RBFFD_THETA);
         if (prm->use_hv) ops[2] = der_index(RBFFD_HV);
-        if (prm->rhs_kind == RBFFD_RHS_ADVECTION && (!prm->cu || !prm->cv))
-            return set_error(ctx, RBFFD_ERR_INVALID, "advection needs per-node coefficients cu and cv");
+        if (prm->rhs_kind == RBFFD_RHS_ADVECTION && !prm->cu)
+            return set_error(ctx, RBFFD_ERR_INVALID, "advection needs per-node coefficients cu");
+        // no cv: f = -cu D_lambda h (+ HV), as VortexRollup::solve (vortex_rollup.cpp:27-57); the
+        // D_theta slot reads the D_lambda weights again with cv = 0 (the same bits: 0 * d = 0)
+        if (prm->rhs_kind == RBFFD_RHS_ADVECTION && !prm->cv) ops[1] = ops[0];
         if (prm->rhs_kind == RBFFD_RHS_COSINE_BELL && prm->sphere_radius == 0.0)
             return set_error(ctx, RBFFD_ERR_INVALID, "cosine bell needs a nonzero sphere radius");
     } else {

@@ -612,6 +612,35 @@ static int launch_weights(rbffd_ctx* ctx, const WParams& P, WShape sh, size_t te
     return RBFFD_OK;
 }
 
+constexpr unsigned ALT_BITS = RBFFD_ALT_XSFC | RBFFD_ALT_YSFC | RBFFD_ALT_ZSFC;
+
+// ALT_XSFC, ALT_YSFC, ALT_ZSFC: the X, Y, Z weights projected on the tangent
+// plane at the stencil centre (x, y, z), (I - x x^T) [wX; wY; wZ], the
+// reference's loop (rbffd.cpp:337-347) with its left-to-right sums and no
+// fused multiply-adds.  Padding rows and slots stay 0.
+__global__ void k_alt_sfc(const double* __restrict__ wx, const double* __restrict__ wy,
+                          const double* __restrict__ wz, const double4* __restrict__ xyz, int N, int rows, int nc,
+                          double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    double x = 0, y = 0, z = 0;
+    if (i < N) {
+        const double4 c = xyz[i];
+        x = c.x, y = c.y, z = c.z;
+    }
+    const double axx = __dsub_rn(1.0, __dmul_rn(x, x)), ayy = __dsub_rn(1.0, __dmul_rn(y, y)),
+                 azz = __dsub_rn(1.0, __dmul_rn(z, z));
+    const double axy = __dmul_rn(-x, y), axz = __dmul_rn(-x, z), ayz = __dmul_rn(-y, z);
+    for (int s = 0; s < 4 * nc; s++) {
+        const size_t o = sell_elem(i, s, nc);
+        const double a = wx[o], b = wy[o], c = wz[o];
+        ax[o] = __dadd_rn(__dadd_rn(__dmul_rn(axx, a), __dmul_rn(axy, b)), __dmul_rn(axz, c));
+        ay[o] = __dadd_rn(__dadd_rn(__dmul_rn(axy, a), __dmul_rn(ayy, b)), __dmul_rn(ayz, c));
+        az[o] = __dadd_rn(__dadd_rn(__dmul_rn(axz, a), __dmul_rn(ayz, b)), __dmul_rn(azz, c));
+    }
+}
+
 extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* prm, const double* eps, double eps_uniform,
                                      const int* deg_per_row)
 {
@@ -619,7 +648,10 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
     rbffd_ctx* ctx = g->ctx;
     unsigned types = prm->der_types & 0xFFFFu;
     if (!types) return set_error(ctx, RBFFD_ERR_INVALID, "no operator selected");
-    if (types & 0x7000u) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "ALT_*SFC operators are not implemented");
+    // ALT_*SFC are formed from the X, Y and Z weights; asking for one computes
+    // all three and X, Y, Z (RBFFD::adjustForSFCTypes, rbffd.h:507-522)
+    const bool alt = (types & ALT_BITS) != 0;
+    if (alt) types = (types & ~ALT_BITS) | RBFFD_X | RBFFD_Y | RBFFD_Z;
     if (prm->poly_deg < -1 || prm->poly_deg > 4) return set_error(ctx, RBFFD_ERR_INVALID, "poly_deg %d outside [-1, 4]", prm->poly_deg);
     if (prm->dim < 1 || prm->dim > 3) return set_error(ctx, RBFFD_ERR_INVALID, "dim %d outside [1, 3]", prm->dim);
     if (prm->hv_k < 0 || prm->hv_k > 16) return set_error(ctx, RBFFD_ERR_INVALID, "hv_k %d outside [0, 16]", prm->hv_k);
@@ -777,6 +809,18 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
                          g->h_perm[status - 1]);
     for (int c = 0; c < K; c++)
         if ((rc = grid_make_f32(g, der_index(P.opbit[c])))) return rc;
+    if (alt) {
+        const int ox = der_index(RBFFD_X), oy = der_index(RBFFD_Y), oz = der_index(RBFFD_Z);
+        const int oa[3] = {der_index(RBFFD_ALT_XSFC), der_index(RBFFD_ALT_YSFC), der_index(RBFFD_ALT_ZSFC)};
+        for (int k = 0; k < 3; k++)
+            if ((rc = grid_alloc_w64(g, oa[k]))) return rc;
+        k_alt_sfc<<<(g->N32 + 127) / 128, 128, 0, s>>>(g->d_w64[ox], g->d_w64[oy], g->d_w64[oz], g->d_xyz, g->N,
+                                                       g->N32, g->nc, g->d_w64[oa[0]], g->d_w64[oa[1]],
+                                                       g->d_w64[oa[2]]);
+        RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+        for (int k = 0; k < 3; k++)
+            if ((rc = grid_make_f32(g, oa[k]))) return rc;
+    }
     RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     return RBFFD_OK;
 }

@@ -167,3 +167,27 @@ def test_weights_mixed_sizes_bucketed(ctx):
             assert np.all(wg[rows][:, sizes[k]:] == 0.0)
         assert rel_l2(O.apply(full, lens, wg, f), O.apply(full, lens, W[t], f)) < 1e-6
     grid.close()
+
+
+def test_alt_sfc_operators(ctx):
+    """ALT_XSFC/YSFC/ZSFC: asking for one computes X, Y, Z and all three
+    (RBFFD::adjustForSFCTypes), and their weights are the oracle's projection
+    of the device's X, Y, Z weights bit for bit (rbffd.cpp:337-347); on a
+    smooth function they approximate the tangential gradient XSFC does."""
+    N, n = 4096, 31
+    xyz, st = sphere_problem(N, n, 3)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(R.ALT_YSFC | R.XSFC, grid, 2)
+    der.setEpsilon(0.3 * np.sqrt(N))
+    der.setPolynomialDegree(2)
+    der.computeAllWeightsForAllStencils()
+    assert der.computedTypes & (R.X | R.Y | R.Z | R.ALT_XSFC | R.ALT_ZSFC) == (R.X | R.Y | R.Z | R.ALT_XSFC | R.ALT_ZSFC)
+    wx, wy, wz = (der.getWeights(t) for t in (R.X, R.Y, R.Z))
+    want = O.alt_sfc(xyz, wx, wy, wz)
+    for t, w in zip((R.ALT_XSFC, R.ALT_YSFC, R.ALT_ZSFC), want):
+        assert np.array_equal(der.getWeights(t), w)
+    f = np.exp(xyz[:, 0]) * np.sin(2 * xyz[:, 1])
+    a = der.applyWeightsForDeriv(R.ALT_XSFC, f)
+    b = der.applyWeightsForDeriv(R.XSFC, f)
+    assert rel_l2(a, b) < 1e-2
+    grid.close()
