@@ -477,10 +477,24 @@ class TimeDependentPDE:
         u = _f64(values).reshape(self.grid.N, self.T) if self.T > 1 else _f64(values)
         self.ctx.check(self.ctx.L.rbffd_pde_set_state(self.h, _dp(np.ascontiguousarray(u))), "set_state")
 
-    def getLocalSolution(self):
+    def getLocalSolution(self, indx=None):
+        """The solution (pde.h:161); one node's value with indx."""
         u = np.zeros((self.grid.N, self.T)) if self.T > 1 else np.zeros(self.grid.N)
         self.ctx.check(self.ctx.L.rbffd_pde_get_state(self.h, _dp(u)), "get_state")
-        return u
+        return u if indx is None else u[indx]
+
+    def syncCPUtoGPU(self):
+        """PDE::syncCPUtoGPU (pde.h:166): the device holds the state and every
+        read copies it, so there is nothing to synchronise."""
+
+    def setStartEndTime(self, start, end):
+        """TimeDependentPDE::setStartEndTime (time_dependent_pde.h:52-56)."""
+        self.start_time, self.end_time = float(start), float(end)
+        self.setTime(start)
+
+    def checkGlobalError(self, exact, global_grid=None, rel_err_max=-1.0, ignore_sol_error=True):
+        """PDE::checkGlobalError (pde.h:130-147): on one rank, checkLocalError."""
+        return self.checkLocalError(exact, rel_err_max)
 
     def advance(self, which=RK4, delta_t=1.0, nsteps=1, graph=False, unfused=False, asynchronous=False):
         flags = (ADVANCE_GRAPH if graph else 0) | (ADVANCE_UNFUSED if unfused else 0) | (

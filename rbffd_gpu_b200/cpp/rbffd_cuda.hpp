@@ -405,6 +405,25 @@ public:
                         100. * nrm[3], 100. * rel_err_max);
         return nrm;
     }
+    // PDE::checkGlobalError (pde.h:130-147): on one rank, checkLocalError
+    std::vector<double> checkGlobalError(const std::vector<double>& exact, Grid_CUDA* global_grid = nullptr,
+                                         double rel_err_max = -1., bool ignore_sol_error = true)
+    {
+        (void)global_grid;
+        (void)ignore_sol_error;
+        return checkLocalError(exact, rel_err_max);
+    }
+    // pde.h:161: one node's value
+    double getLocalSolution(unsigned indx) { return getLocalSolution()[indx]; }
+    // PDE::syncCPUtoGPU (pde.h:166): the device holds the state and every read copies it
+    void syncCPUtoGPU() {}
+    // TimeDependentPDE::setStartEndTime (time_dependent_pde.h:52-56)
+    void setStartEndTime(double start, double end)
+    {
+        start_time_ = start;
+        end_time_ = end;
+        setTime(start);
+    }
     double getTime()
     {
         double t = 0.0;
@@ -423,6 +442,7 @@ protected:
     Grid_CUDA& grid_;
     int T_;
     rbffd_pde* h_ = nullptr;
+    double start_time_ = 0., end_time_ = 0.;
 };
 
 inline rbffd_pde_params pde_params(int kind, int dtype, int ntracers)

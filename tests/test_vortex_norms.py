@@ -66,6 +66,10 @@ def test_vortex_rollup_pde():
     exact = R.exact_vortex_rollup(xyz, dt * steps)
     norms = pde.checkLocalError(exact)
     assert norms == R.sol_norms(pde.getLocalSolution(), exact)
+    assert pde.checkGlobalError(exact) == norms
+    assert pde.getLocalSolution(7) == pde.getLocalSolution()[7]
+    pde.setStartEndTime(2.0, 3.0)
+    assert pde.getTime() == 2.0
     assert norms["l2_rel"] < 0.1  # 3.7e-2 at t = 0.5: the roll-up steepens, n = 31 on 4096 nodes
     pde.close()
     p32 = R.VortexRollup(grid, der, True, dtype=R.F32)
