@@ -380,6 +380,58 @@ def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
     out["cosine_bell"] = bench_cosine_bell(R, torch, ctx)
     out["eigenvalues"] = bench_eigenvalues(R, ctx)
     out["node_order"] = bench_node_order(R, torch, ctx, xyz, st, u0)
+    out["heat_hbm_bound"] = bench_heat_hbm_bound(R, torch, ctx)
+    return out
+
+
+HEAT_LARGE = dict(name="heat_sphere_N655362_n50_n101_100steps", N=655362, sizes=((50, 3), (101, 4)), steps=100,
+                  dt=1e-7, seed=2)
+
+
+def bench_heat_hbm_bound(R, torch, ctx):
+    """The heat stage where it cannot stay in L2: N = 655362 nodes with n = 50
+    (degree 3) and n = 101 (degree 4), FP32 and FP64, 100 graphed RK4 steps
+    with the autotuned stage kernel; roofline against the measured HBM peak by
+    algorithmic bytes per stage launch (n weights, n indices -- 16-bit in the
+    halo-tiled kernels -- and four state accesses)."""
+    C = HEAT_LARGE
+    N, steps, dt = C["N"], C["steps"], C["dt"]
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    peak, peak_kind = load_peaks()
+    xyz = R.fibonacci_nodes(N, C["seed"])
+    u0 = R.exact_sph_heat(xyz, 10, np.random.default_rng(1).standard_normal(121), 0.0)
+    out = {"workload": C["name"]}
+    for n, deg in C["sizes"]:
+        st = R.knn_stencils_gpu(ctx, xyz, n)
+        grid = R.Grid(ctx, xyz, st)
+        der = R.RBFFD(R.LSFC, grid, 2)
+        der.setEpsilon(heat_eps(N))
+        der.setPolynomialDegree(deg)
+        der.computeAllWeightsForAllStencils()
+        for tag, dtype, wb in (("fp32", R.F32, 4), ("fp64", R.F64, 8)):
+            pde = R.HeatSphere(grid, der, 1.0, dtype=dtype)
+            pde.fillInitialConditions(u0)
+            pde.advance(R.RK4, dt, steps, graph=True)
+            ctx.synchronize()
+            best = 1e30
+            for _ in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
+                e1.record(stream)
+                ctx.synchronize()
+                best = min(best, e0.elapsed_time(e1) * 1e-3)
+            shape = pde.getShape()
+            ib = 2 if shape[2] > 0 else 4
+            per_launch = best / (4 * steps)
+            byt = N * stage_bytes(n, wb, wb, ib)
+            out["n%d_%s" % (n, tag)] = {
+                "node_updates_per_s": N * steps / best, "us_per_launch": per_launch * 1e6, "shape": shape,
+                "roofline": {"bound": "hbm", "achieved": byt / per_launch / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": byt / per_launch / 1e9 / peak, "peak_kind": peak_kind,
+                             "algorithmic_bytes_per_launch": byt}}
+            pde.close()
+        grid.close()
     return out
 
 
