@@ -612,7 +612,7 @@ int orc_rk4_heat(int N, int n_pad, const int* st, const int* st_len, const doubl
 int orc_max_threads(void)
 {
 #ifdef _OPENMP
-    return omp_get_max_threads();
+    return omp_get_num_procs();  /* not omp_get_max_threads: a call with nthreads = 1 lowers that for the process */
 #else
     return 1;
 #endif
