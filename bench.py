@@ -53,6 +53,9 @@ def parse():
                          "operator), for ncu captures")
     ap.add_argument("--profile-serving", type=int, default=0, metavar="K",
                     help="serving stage kernels: K + K requests on two N=163842 grids, 3 RK4 steps, for ncu")
+    ap.add_argument("--profile-heat-hbm", action="store_true",
+                    help="the heat stage where it is HBM-bound: N=655362, FP32 n=50 then FP64 n=101, halo tiles of "
+                         "128 rows, 3 un-graphed RK4 steps each (12 launches each), for ncu")
     ap.add_argument("--profile-weights", type=int, default=0, metavar="N",
                     help="batched weights (the 1e6-stencil mix at N stencils): a tuned call, then one more, for ncu")
     return ap.parse_args()
@@ -1047,6 +1050,29 @@ def run_profile_multitracer(spec):
     print("profile run done")
 
 
+def run_profile_heat_hbm():
+    import rbffd_gpu_b200 as R
+    ctx = R.Context(0)
+    N = HEAT_LARGE["N"]
+    xyz = R.fibonacci_nodes(N, HEAT_LARGE["seed"])
+    u0 = R.exact_sph_heat(xyz, 10, np.random.default_rng(1).standard_normal(121), 0.0)
+    for n, deg, dtype in ((50, 3, R.F32), (101, 4, R.F64)):
+        st = R.knn_stencils_gpu(ctx, xyz, n)
+        grid = R.Grid(ctx, xyz, st)
+        der = R.RBFFD(R.LSFC, grid, 2)
+        der.setEpsilon(heat_eps(N))
+        der.setPolynomialDegree(deg)
+        der.computeAllWeightsForAllStencils()
+        pde = R.HeatSphere(grid, der, 1.0, dtype=dtype)
+        pde.setTiledShape(128, 1)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, 1e-7, 3)
+        ctx.synchronize()
+        pde.close()
+        grid.close()
+    print("profile run done")
+
+
 def run_profile_weights(N):
     """The batched-weights mix (n over {17, 31, 50, 101} with degrees 1-4,
     eps ~ U[2, 8], XSFC/YSFC/ZSFC) on N stencils: the tuned call, then one
@@ -1107,6 +1133,8 @@ def main():
         run_profile_serving(args.profile_serving)
     elif args.profile_weights:
         run_profile_weights(args.profile_weights)
+    elif args.profile_heat_hbm:
+        run_profile_heat_hbm()
     elif args.profile_multitracer:
         run_profile_multitracer(args.profile_multitracer)
     elif args.profile:
