@@ -612,7 +612,8 @@ def bench_cosine_bell(R, torch, ctx):
     time stepping; the GPU runs one lane per row (the oracle's summation
     order).  At the configuration's eps = 0.035 sqrt(N) the operator has
     growing modes on these nodes (reported over a short horizon); a full
-    revolution uses eps = 6."""
+    revolution uses eps = 6, with the degree-2 basis and with the reference's
+    own basis {1} (np = 1, m = 32)."""
     import oracle as O
     C = COSINE_BELL
     N, n = C["N"], C["n"]
@@ -630,15 +631,16 @@ def bench_cosine_bell(R, torch, ctx):
         dn = float(np.linalg.norm(y))
         return float(np.linalg.norm(x - y) / dn) if np.isfinite(dn) and dn > 0 else None
 
-    for tag, eps, steps in (("eps_configuration", C["eps_configuration"], C["short_steps"]),
-                            ("eps_stable", C["eps_stable"], C["steps"])):
-        W = O.weights(xyz, st, None, eps, types, dim=2, poly_deg=C["deg"], hv_k=C["hv_k"],
+    for tag, eps, steps, deg in (("eps_configuration", C["eps_configuration"], C["short_steps"], C["deg"]),
+                                 ("eps_stable", C["eps_stable"], C["steps"], C["deg"]),
+                                 ("eps_stable_reference_basis_np1", C["eps_stable"], C["steps"], 0)):
+        W = O.weights(xyz, st, None, eps, types, dim=2, poly_deg=deg, hv_k=C["hv_k"],
                       hv_scale=-C["gamma"] * N ** -float(C["hv_k"]))
         grid = R.Grid(ctx, xyz, st)
         der = R.RBFFD(types, grid, 2)
         for t, w in W.items():
             der.setWeights(t, w)
-        res = {"eps": eps, "steps": steps}
+        res = {"eps": eps, "steps": steps, "poly_deg": deg, "system_size_m": n + O.lib().orc_poly_size(deg)}
         for dname, dtype in (("fp64", R.F64), ("fp32", R.F32)):
             pde = R.CosineBell(grid, der, a, alpha, T, True, dtype=dtype)
             pde.setShape(1, 256)
