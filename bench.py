@@ -49,8 +49,8 @@ def parse():
                     help="setup plus 25 un-graphed RK4 steps with the autotuned kernel shape, for ncu captures")
     ap.add_argument("--profile-multitracer", default=None, metavar="ROWS,LANES",
                     help="16-tracer vortex case on N=163842, n=101 (weights > L2), 3 un-graphed RK4 steps with the "
-                         "tiled shape ROWS,LANES (0,0 = global-memory gathers; a third field f = FP32 fused "
-                         "operator), for ncu captures")
+                         "tiled shape ROWS,LANES (0,0 = global-memory gathers; further fields: f = FP32 fused "
+                         "operator, s = conflict-avoiding slot schedule), for ncu captures")
     ap.add_argument("--profile-serving", type=int, default=0, metavar="K",
                     help="serving stage kernels: K + K requests on two N=163842 grids, 3 RK4 steps, for ncu")
     ap.add_argument("--profile-heat-hbm", action="store_true",
@@ -571,7 +571,7 @@ def bench_multitracer(R, torch, ctx):
         pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
         e1.record(stream)
         ctx.synchronize()
-        res[dtype] = (pde.getLocalSolution(), e0.elapsed_time(e1) * 1e-3, pde.getShape())
+        res[dtype] = (pde.getLocalSolution(), e0.elapsed_time(e1) * 1e-3, pde.getShape() + (pde.getTileFlags(),))
         pde.close()
     exact = WL.vortex_exact(xyz, axis, tracers, steps * dt)
     u32, u64 = res[R.F32][0], res[R.F64][0]
@@ -1023,7 +1023,8 @@ def run_profile_multitracer(spec):
     from rbffd_gpu_b200 import workloads as WL
     fields = spec.split(",")
     rows, lanes = int(fields[0]), int(fields[1])
-    fused = len(fields) > 2 and fields[2] == "f"
+    fused = "f" in fields[2:]
+    sched = "s" in fields[2:]
     N, n, T = 163842, 101, 16
     xyz = R.fibonacci_nodes(N, 4)
     st = R.knn_stencils(xyz, n)
@@ -1041,7 +1042,7 @@ def run_profile_multitracer(spec):
     if fused:
         pde.setFusedOperator(True)
     if rows > 0:
-        pde.setTiledShape(rows, lanes)
+        pde.setTiledShape(rows, lanes, slot_schedule=sched)
     else:
         pde.setShape(1, 256)
     pde.fillInitialConditions(u0)

@@ -333,15 +333,26 @@ int rbffd_pde_set_shape(rbffd_pde* pde, int lanes_per_row, int block_threads);
 int rbffd_pde_get_shape(rbffd_pde* pde, int* lanes_per_row, int* block_threads);
 /* Tiled stage kernel: each thread block takes rows_per_block consecutive rows
  * (a multiple of 32) and stages the node values their stencils gather in
- * shared memory; lanes (1, 2 or 4) split each row's slots.  With
- * stream_weights (one lane per row) the block's weights and indices are also
- * streamed into shared memory by asynchronous bulk copies (TMA), several
- * stages ahead; its waits are bounded and a timeout is reported by
- * rbffd_pde_advance as RBFFD_ERR_TIMEOUT.  Returns RBFFD_ERR_UNSUPPORTED if
- * the staged data do not fit shared memory.
- * get_tiling reports 0 when the stage kernel gathers from global memory. */
-int rbffd_pde_set_tiled_shape(rbffd_pde* pde, int rows_per_block, int lanes, int stream_weights);
+ * shared memory; lanes (1, 2 or 4) split each row's slots.  flags (one lane
+ * per row):
+ *   RBFFD_TILE_STREAM_WEIGHTS: the block's weights and indices are also
+ *     streamed into shared memory by asynchronous bulk copies (TMA), several
+ *     stages ahead; its waits are bounded and a timeout is reported by
+ *     rbffd_pde_advance as RBFFD_ERR_TIMEOUT;
+ *   RBFFD_TILE_SLOT_SCHEDULE: FP32 PDEs that stream one operator (heat, or a
+ *     fused advection operator) with 4, 8 or 16 tracers: each row reads its
+ *     slots in an order chosen so that the rows sharing a shared-memory
+ *     wavefront read different bank groups (fewer bank conflicts).  Changes
+ *     each row's FP32 summation order.
+ * (flags = 1, the former stream_weights argument, keeps its meaning.)
+ * Returns RBFFD_ERR_UNSUPPORTED if the staged data do not fit shared memory
+ * or the flags do not apply to the PDE.
+ * get_tiling reports 0 when the stage kernel gathers from global memory;
+ * get_tile_flags the flags of the shape in use (set or autotuned). */
+enum { RBFFD_TILE_STREAM_WEIGHTS = 1, RBFFD_TILE_SLOT_SCHEDULE = 2 };
+int rbffd_pde_set_tiled_shape(rbffd_pde* pde, int rows_per_block, int lanes, int flags);
 int rbffd_pde_get_tiling(rbffd_pde* pde, int* rows_per_block);
+int rbffd_pde_get_tile_flags(rbffd_pde* pde, int* flags);
 /* FP32 advection with time-independent coefficients: replace the three
  * operators of each stage (CosineBell::solve's Dlambda, Dtheta and HV,
  * cosine_bell.cpp:47-57) by one fused operator

@@ -91,6 +91,7 @@ PROTOTYPES = {
     "rbffd_pde_set_fused_operator": (c_int, [c_void_p, c_int]),
     "rbffd_pde_set_tiled_shape": (c_int, [c_void_p, c_int, c_int, c_int]),
     "rbffd_pde_get_tiling": (c_int, [c_void_p, ip]),
+    "rbffd_pde_get_tile_flags": (c_int, [c_void_p, ip]),
     "rbffd_heat_rk4_noalloc": (c_int, [c_void_p, c_int, c_double, c_double, c_int, c_void_p]),
     "rbffd_pde_get_shape": (c_int, [c_void_p, ip, ip]),
     "rbffd_server_start": (c_int, [c_void_p, c_double, c_int, P(c_void_p)]),

@@ -543,9 +543,20 @@ class TimeDependentPDE:
         """FP32 advection: one fused operator -(cu Wl + cv Wt) + Whv per stage."""
         self.ctx.check(self.ctx.L.rbffd_pde_set_fused_operator(self.h, int(bool(on))), "set_fused_operator")
 
-    def setTiledShape(self, rows_per_block, lanes=1, stream_weights=False):
-        self.ctx.check(self.ctx.L.rbffd_pde_set_tiled_shape(self.h, rows_per_block, lanes, int(stream_weights)),
-                       "set_tiled_shape")
+    TILE_STREAM_WEIGHTS, TILE_SLOT_SCHEDULE = 1, 2
+
+    def setTiledShape(self, rows_per_block, lanes=1, stream_weights=False, slot_schedule=False):
+        """Tiled stage kernel of rows_per_block rows; stream_weights: bulk-copy
+        weight streaming; slot_schedule: FP32 rows read their slots in the
+        halo's conflict-avoiding order (one operator, 4/8/16 tracers)."""
+        flags = (self.TILE_STREAM_WEIGHTS if stream_weights else 0) | (self.TILE_SLOT_SCHEDULE if slot_schedule else 0)
+        self.ctx.check(self.ctx.L.rbffd_pde_set_tiled_shape(self.h, rows_per_block, lanes, flags), "set_tiled_shape")
+
+    def getTileFlags(self):
+        """Flags of the tiled shape in use: TILE_STREAM_WEIGHTS | TILE_SLOT_SCHEDULE."""
+        f = ctypes.c_int()
+        self.ctx.check(self.ctx.L.rbffd_pde_get_tile_flags(self.h, ctypes.byref(f)))
+        return f.value
 
     def close(self):
         if getattr(self, "h", None):

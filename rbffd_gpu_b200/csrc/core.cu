@@ -328,8 +328,10 @@ extern "C" int rbffd_grid_destroy(rbffd_grid* g)
         dev_free(ctx, h->d_rows, (size_t)(h->nblocks + 1) * sizeof(int));
         dev_free(ctx, h->d_nodes, h->b_nodes);
         dev_free(ctx, h->d_lidx, h->b_lidx);
-        dev_free(ctx, h->d_lidx_s, h->b_lidx);
-        dev_free(ctx, h->d_slot_s, h->b_lidx);
+        for (int k = 0; k < 4; k++) {
+            dev_free(ctx, h->d_lidx_s[k], h->b_lidx);
+            dev_free(ctx, h->d_slot_s[k], h->b_lidx);
+        }
         delete h;
     }
     delete g;
@@ -364,24 +366,24 @@ static void parallel_for(int count, const std::function<void(int)>& f)
     for (auto& t : pool) t.join();
 }
 
-// Slot schedule of one quarter-warp group (rows q0 .. q1-1, at most 8) of a
-// block whose halo has hn positions.  A thread serves one row and, at each of
-// the n4 steps, reads one halo position per row; the 16-byte reads of the
-// group's rows take one shared-memory wavefront when their positions are
-// different mod 8 (the bank group).  Each step is a maximum matching of rows
-// to bank groups (Kuhn's augmenting paths): a row may take a remaining slot
-// of that group (preferring the group it has most slots left in) or, while it
-// has padding entries to spend, a padding entry placed in any free group.
-// Rows that stay unmatched take a remaining slot anyway (a conflict).
+// Slot schedule of one wavefront group (rows q0 .. q1-1, at most P) of a
+// block whose halo has hn positions.  A row's reads of one step are 16-byte
+// vectors of a 128/P-byte node record; the group's rows read in one
+// shared-memory wavefront when their positions are different mod P (the bank
+// group).  Each step is a maximum matching of rows to bank groups (Kuhn's
+// augmenting paths): a row may take a remaining slot of that group
+// (preferring the group it has most slots left in) or, while it has padding
+// entries to spend, a padding entry placed in any free group.  Rows that stay
+// unmatched take a remaining slot anyway (a conflict).
 static void schedule_group(const rbffd_grid* g, const std::vector<unsigned short>& lidx, int q0, int q1, int hn,
-                           std::vector<unsigned short>& lidx_s, std::vector<unsigned short>& slot_s)
+                           int P, std::vector<unsigned short>& lidx_s, std::vector<unsigned short>& slot_s)
 {
     const int nc = g->nc, n4 = g->n4, G = q1 - q0;
     std::vector<int> by[8][8];  // by[row][group]: remaining slots, the lowest last
     int realrem[8] = {}, freerem[8] = {};
     for (int r = 0; r < G; r++) {
         const int len = g->h_len[q0 + r];
-        for (int s = len - 1; s >= 0; s--) by[r][lidx[sell_elem(q0 + r, s, nc)] & 7].push_back(s);
+        for (int s = len - 1; s >= 0; s--) by[r][lidx[sell_elem(q0 + r, s, nc)] & (P - 1)].push_back(s);
         realrem[r] = len;
         freerem[r] = n4 - len;
     }
@@ -389,12 +391,12 @@ static void schedule_group(const rbffd_grid* g, const std::vector<unsigned short
         int pref[8][8], npref[8] = {};
         for (int r = 0; r < G; r++) {
             int cs[8], k = 0;
-            for (int c = 0; c < 8; c++)
+            for (int c = 0; c < P; c++)
                 if (!by[r][c].empty()) cs[k++] = c;
             std::sort(cs, cs + k, [&](int a, int b) { return by[r][a].size() > by[r][b].size(); });
             for (int j = 0; j < k; j++) pref[r][npref[r]++] = cs[j];
             if (freerem[r] > 0)
-                for (int c = 0; c < 8; c++)
+                for (int c = 0; c < P; c++)
                     if (by[r][c].empty()) pref[r][npref[r]++] = c;
         }
         int order[8];
@@ -404,7 +406,7 @@ static void schedule_group(const rbffd_grid* g, const std::vector<unsigned short
             return npref[a] < npref[b];
         });
         int owner[8];
-        for (int c = 0; c < 8; c++) owner[c] = -1;
+        for (int c = 0; c < P; c++) owner[c] = -1;
         std::function<bool(int, unsigned&)> augment = [&](int r, unsigned& seen) {
             for (int j = 0; j < npref[r]; j++) {
                 const int c = pref[r][j];
@@ -423,14 +425,14 @@ static void schedule_group(const rbffd_grid* g, const std::vector<unsigned short
         }
         int colour[8];
         for (int r = 0; r < G; r++) colour[r] = -1;
-        for (int c = 0; c < 8; c++)
+        for (int c = 0; c < P; c++)
             if (owner[c] >= 0) colour[owner[c]] = c;
         for (int r = 0; r < G; r++) {
             const size_t e = sell_elem(q0 + r, t, nc);
             int c = colour[r];
             if (c < 0 || (by[r][c].empty() && freerem[r] == 0)) {  // unmatched: a conflicting slot
                 c = -1;
-                for (int k = 0; k < 8; k++)
+                for (int k = 0; k < P; k++)
                     if (!by[r][k].empty() && (c < 0 || by[r][k].size() > by[r][c].size())) c = k;
             }
             if (c >= 0 && !by[r][c].empty()) {
@@ -449,19 +451,19 @@ static void schedule_group(const rbffd_grid* g, const std::vector<unsigned short
     }
 }
 
-int grid_halo_schedule(rbffd_grid* g, int R, const Halo** out)
+int grid_halo_schedule(rbffd_grid* g, int R, int P, const Halo** out)
 {
+    rbffd_ctx* ctx = g->ctx;
+    const int k = P == 2 ? 1 : (P == 4 ? 2 : (P == 8 ? 3 : -1));
+    if (k < 0) return set_error(ctx, RBFFD_ERR_INVALID, "slot schedule for %d rows per wavefront", P);
     const Halo* hc = nullptr;
     int rc = grid_halo(g, R, &hc);
     if (rc) return rc;
     Halo* h = const_cast<Halo*>(hc);
-    if (h->d_lidx_s) {
+    if (h->d_lidx_s[k]) {
         *out = h;
         return RBFFD_OK;
     }
-    rbffd_ctx* ctx = g->ctx;
-    if (g->sched_R != 0 && g->sched_R != R)
-        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a grid keeps one slot schedule");
     const size_t nidx = (size_t)g->N32 * g->n4;
     std::vector<unsigned short> lidx(nidx), lidx_s(nidx, 0), slot_s(nidx, SLOT_FREE);
     std::vector<int> rows(h->nblocks + 1), ptr(h->nblocks + 1);
@@ -471,26 +473,25 @@ int grid_halo_schedule(rbffd_grid* g, int R, const Halo** out)
     RBFFD_CUDA_TRY(ctx, cudaMemcpy(ptr.data(), h->d_ptr, ptr.size() * sizeof(int), cudaMemcpyDeviceToHost));
     parallel_for(h->nblocks, [&](int b) {
         const int hn = ptr[b + 1] - ptr[b];
-        for (int q0 = rows[b]; q0 < rows[b + 1]; q0 += 8)
-            schedule_group(g, lidx, q0, std::min(rows[b + 1], q0 + 8), hn, lidx_s, slot_s);
+        for (int q0 = rows[b]; q0 < rows[b + 1]; q0 += P)
+            schedule_group(g, lidx, q0, std::min(rows[b + 1], q0 + P), hn, P, lidx_s, slot_s);
     });
     const size_t bytes = nidx * sizeof(unsigned short);
-    if ((rc = dev_alloc(ctx, (void**)&h->d_lidx_s, bytes))) return rc;
-    if ((rc = dev_alloc(ctx, (void**)&h->d_slot_s, bytes))) {
-        dev_free(ctx, h->d_lidx_s, bytes);
-        h->d_lidx_s = nullptr;
+    if ((rc = dev_alloc(ctx, (void**)&h->d_lidx_s[k], bytes))) return rc;
+    if ((rc = dev_alloc(ctx, (void**)&h->d_slot_s[k], bytes))) {
+        dev_free(ctx, h->d_lidx_s[k], bytes);
+        h->d_lidx_s[k] = nullptr;
         return rc;
     }
-    cudaError_t e = cudaMemcpy(h->d_lidx_s, lidx_s.data(), bytes, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(h->d_slot_s, slot_s.data(), bytes, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(h->d_lidx_s[k], lidx_s.data(), bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_slot_s[k], slot_s.data(), bytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
-        dev_free(ctx, h->d_lidx_s, bytes);
-        dev_free(ctx, h->d_slot_s, bytes);
-        h->d_lidx_s = h->d_slot_s = nullptr;
+        dev_free(ctx, h->d_lidx_s[k], bytes);
+        dev_free(ctx, h->d_slot_s[k], bytes);
+        h->d_lidx_s[k] = h->d_slot_s[k] = nullptr;
         return cuda_error(ctx, e, "slot schedule upload");
     }
     g->bytes += 2 * bytes;
-    g->sched_R = R;
     *out = h;
     return RBFFD_OK;
 }
@@ -770,27 +771,41 @@ int grid_make_f32(rbffd_grid* g, int op)
     k_cast_f32<<<std::max(1, std::min<int>((int)((n + 255) / 256), ctx->sm_count * 16)), 256, 0, ctx->stream>>>(
         g->d_w64[op], g->d_w32[op], n);
     RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    g->w32_ver[op]++;
     if (g->d_w32s[op]) {  // keep the scheduled copy in step
         const Halo* h = g->halos.at(g->sched_R);
-        k_schedule_f32<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(g->d_w32[op], h->d_slot_s, n, g->nc,
+        k_schedule_f32<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(g->d_w32[op], h->d_slot_s[3], n, g->nc,
                                                                           g->d_w32s[op]);
         RBFFD_CUDA_TRY(ctx, cudaGetLastError());
     }
     return RBFFD_OK;
 }
 
-int grid_f32_scheduled(rbffd_grid* g, int op, const float** out)
+int grid_schedule_weights(rbffd_grid* g, const float* src, const unsigned short* slot, float* dst, cudaStream_t s)
+{
+    const size_t n = (size_t)g->N32 * g->n4;
+    k_schedule_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, slot, n, g->nc, dst);
+    RBFFD_CUDA_TRY(g->ctx, cudaGetLastError());
+    return RBFFD_OK;
+}
+
+int grid_f32_scheduled(rbffd_grid* g, int R, int op, const float** out)
 {
     rbffd_ctx* ctx = g->ctx;
-    if (g->sched_R == 0) return set_error(ctx, RBFFD_ERR_STATE, "no slot schedule on this grid");
-    int rc;
+    // the grid's scheduled copies (d_w32s) all follow the 8-row schedule of one halo
+    if (g->sched_R != 0 && g->sched_R != R)
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a grid keeps its scheduled FP32 weights for one block size");
+    const Halo* hs = nullptr;
+    int rc = grid_halo_schedule(g, R, 8, &hs);
+    if (rc) return rc;
+    g->sched_R = R;
     if (!g->d_w32[op] && (rc = grid_make_f32(g, op))) return rc;
     if (!g->d_w32s[op]) {
         const size_t n = (size_t)g->N32 * g->n4;
         if ((rc = dev_alloc(ctx, (void**)&g->d_w32s[op], n * sizeof(float)))) return rc;
         g->bytes += n * sizeof(float);
         const Halo* h = g->halos.at(g->sched_R);
-        k_schedule_f32<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(g->d_w32[op], h->d_slot_s, n, g->nc,
+        k_schedule_f32<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(g->d_w32[op], h->d_slot_s[3], n, g->nc,
                                                                           g->d_w32s[op]);
         RBFFD_CUDA_TRY(ctx, cudaGetLastError());
     }

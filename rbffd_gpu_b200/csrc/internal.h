@@ -35,6 +35,7 @@ struct Shape {
     int lanes = 0, block = 0;
     int tile = 0;  // rows per block with the halo staged in shared memory; 0 = gather from global memory
     int tma = 0;   // tiled kernel that streams weights and indices into shared memory with bulk copies
+    int sched = 0; // tiled, FP32, one operator: each row reads its slots in the halo's conflict-avoiding schedule
 };
 
 // Device status word of a context: kernels whose waits are bounded write a
@@ -65,8 +66,9 @@ struct rbffd_grid {
     double4* d_xyz = nullptr;      // [N] node coordinates (w unused)
     double* d_w64[16] = {};        // per operator, sliced ELL N32 x n4: FP64 weights, padding 0
     float* d_w32[16] = {};         // FP32 copies (rounded to nearest)
-    float* d_w32s[16] = {};        // FP32 copies in the slot schedule of halo sched_R
-    int sched_R = 0;               // rows per block of the halo that has a slot schedule (0: none)
+    float* d_w32s[16] = {};        // FP32 copies in the 8-row slot schedule of halo sched_R
+    int sched_R = 0;               // rows per block of the halo that has an 8-row slot schedule (0: none)
+    unsigned w32_ver[16] = {};     // counts refreshes of d_w32[op] (copies made from it follow it)
     // Rows and nodes are stored in an internal order (a 3-D Morton curve through
     // the nodes) so that rows handled together gather from nearby nodes; the
     // stencil slot order is kept, so each row's arithmetic is unchanged.
@@ -97,21 +99,29 @@ struct Halo {
     int* d_nodes = nullptr;      // node staged at each halo position (internal order)
     unsigned short* d_lidx = nullptr;  // sliced ELL, N32 x n4
     size_t b_nodes = 0, b_lidx = 0;
-    // Conflict-avoiding slot schedule (built on demand, grid_halo_schedule):
-    // each row's slots reordered so that at each step the 8 rows of a
-    // quarter-warp read halo positions in different 16-byte bank groups where
-    // their stencils allow; padding entries (weight 0) take any free group.
-    // Changes the summation order of a row, so only FP32 serving uses it.
-    unsigned short* d_lidx_s = nullptr;  // sliced ELL: position read at scheduled slot t
-    unsigned short* d_slot_s = nullptr;  // original slot of scheduled slot t, SLOT_FREE for padding
+    // Conflict-avoiding slot schedules (built on demand, grid_halo_schedule):
+    // each row's slots reordered so that at each step the P rows whose 16-byte
+    // reads share one shared-memory wavefront read halo records in different
+    // bank groups (position mod P) where their stencils allow; padding entries
+    // (weight 0) take any free group.  P = 128 bytes / record bytes: 8 for
+    // 16-byte records (four FP32 values per node), 4 for 32-byte, 2 for
+    // 64-byte.  Index k = log2(P).  Changes the summation order of a row, so
+    // only FP32 paths use it.
+    unsigned short* d_lidx_s[4] = {};  // sliced ELL: position read at scheduled slot t
+    unsigned short* d_slot_s[4] = {};  // original slot of scheduled slot t, SLOT_FREE for padding
 };
 constexpr unsigned short SLOT_FREE = 0xFFFF;
 int grid_halo(rbffd_grid* g, int R, const Halo** out);
-// The halo of R rows per block with its slot schedule.
-int grid_halo_schedule(rbffd_grid* g, int R, const Halo** out);
-// FP32 weights of operator op in the schedule of the grid's scheduled halo
-// (made on first use, refreshed with the FP32 copy).
-int grid_f32_scheduled(rbffd_grid* g, int op, const float** out);
+// The halo of R rows per block with its slot schedule for P rows per
+// wavefront (P = 2, 4 or 8).
+int grid_halo_schedule(rbffd_grid* g, int R, int P, const Halo** out);
+// FP32 weights of operator op in the 8-row slot schedule of the halo of R
+// rows per block (made on first use, refreshed with the FP32 copy; one R per
+// grid).
+int grid_f32_scheduled(rbffd_grid* g, int R, int op, const float** out);
+// dst (sliced ELL, N32 x n4 floats) = the FP32 weights src in the slot order
+// `slot` of a schedule (padding entries 0), on stream s.
+int grid_schedule_weights(rbffd_grid* g, const float* src, const unsigned short* slot, float* dst, cudaStream_t s);
 
 enum { KIND_ADVECT = 0, KIND_HEAT = 1 };
 
@@ -129,6 +139,13 @@ struct rbffd_pde {
     // weight array instead of three
     float* wf = nullptr;
     bool fused = false;
+    // The one FP32 operator the stages stream (wf, or the grid's FP32 copy)
+    // in the slot schedule of halo ws_R for ws_P rows per wavefront; remade
+    // when its source changes (ws_src, ws_ver)
+    float* ws = nullptr;
+    int ws_R = 0, ws_P = 0;
+    const void* ws_src = nullptr;
+    unsigned ws_ver = 0;
     void *d[3] = {nullptr, nullptr, nullptr};  // unfused path: one output per operator
     double* stage64 = nullptr;                  // FP64 staging for host state copies of an FP32 PDE
     double kappa = 1.0;

@@ -470,8 +470,51 @@ struct TileGeom {
     const Halo* h = nullptr;
     int vec = 1, vpn = 1, G = 1, threads = 0;
     int tma = 0, halo_bytes = 0, stage_bytes = 0;
+    int sched = -1;  // index of the halo's slot schedule the rows read (-1: stencil order)
     size_t smem = 0;
 };
+
+// Rows per 16-byte-load wavefront of the FP32 tiled kernel with one lane group
+// per row: 128 bytes / (T * 4)-byte node records (8, 4 or 2 for T = 4, 8, 16),
+// or 0 where a slot schedule does not apply (one operator streamed, FP32,
+// four values per vector).
+static int sched_rows(const rbffd_pde* P)
+{
+    if (P->dtype != RBFFD_F32 || !(P->kind == KIND_HEAT || P->fused)) return 0;
+    return P->T == 4 ? 8 : (P->T == 8 ? 4 : (P->T == 16 ? 2 : 0));
+}
+
+static int log2_rows(int Pw) { return Pw == 2 ? 1 : (Pw == 4 ? 2 : 3); }
+
+// The halo schedule of R rows per block and the PDE's operator in its slot
+// order (P->ws), made or refreshed before launches that read them.
+static int pde_sched_prepare(rbffd_pde* P, int R)
+{
+    rbffd_grid* g = P->g;
+    rbffd_ctx* ctx = P->ctx;
+    const int Pw = sched_rows(P);
+    if (!Pw) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a slot schedule needs FP32, one operator and 4, 8 or 16 tracers");
+    const Halo* h = nullptr;
+    int rc = grid_halo_schedule(g, R, Pw, &h);
+    if (rc) return rc;
+    const float* src = P->fused ? P->wf : g->d_w32[P->op[0]];
+    const unsigned ver = P->fused ? 0u : g->w32_ver[P->op[0]];
+    if (!src) return set_error(ctx, RBFFD_ERR_STATE, "no FP32 weights for the slot schedule");
+    if (!P->ws) {
+        const size_t bytes = (size_t)g->N32 * g->n4 * sizeof(float);
+        if ((rc = dev_alloc(ctx, (void**)&P->ws, bytes))) return rc;
+        P->bytes += bytes;
+        P->ws_src = nullptr;
+    }
+    if (P->ws_R != R || P->ws_P != Pw || P->ws_src != src || P->ws_ver != ver) {
+        if ((rc = grid_schedule_weights(g, src, h->d_slot_s[log2_rows(Pw)], P->ws, ctx->stream))) return rc;
+        P->ws_R = R;
+        P->ws_P = Pw;
+        P->ws_src = src;
+        P->ws_ver = ver;
+    }
+    return RBFFD_OK;
+}
 
 static bool tile_geom(rbffd_pde* P, Shape sh, TileGeom* tg)
 {
@@ -496,6 +539,13 @@ static bool tile_geom(rbffd_pde* P, Shape sh, TileGeom* tg)
     t.threads = sh.tile * L;
     if (t.threads > 1024) return false;
     t.smem = (size_t)t.h->max_halo * P->T * es;
+    if (sh.sched) {  // prepared by pde_sched_prepare for this block size
+        const int Pw = sched_rows(P);
+        if (!Pw || t.G != 1 || t.vec != 4 || sh.tma || !P->ws || P->ws_R != sh.tile || P->ws_P != Pw ||
+            !t.h->d_lidx_s[log2_rows(Pw)])
+            return false;
+        t.sched = log2_rows(Pw);
+    }
     if (sh.tma) {
         if (t.G != 1) return false;
         const int K = P->kind == KIND_HEAT ? 1 : (P->use_hv ? 3 : 2);
@@ -545,6 +595,13 @@ static void launch_stage_t(rbffd_pde* P, const StageParams<T>& p, Shape sh, cuda
     if (tile_geom(P, sh, &tg)) {
         TileParams tp{tg.h->d_ptr, tg.h->d_nodes, tg.h->d_lidx, tg.h->d_rows, tg.h->R, P->g->N32};
         constexpr int VV = std::is_same<T, float>::value ? 4 : 2;
+        if (tg.sched >= 0) {  // slot-scheduled rows: local indices and the one operator in that order
+            StageParams<T> ps = p;
+            ps.w0 = (const T*)P->ws;
+            tp.lidx = tg.h->d_lidx_s[tg.sched];
+            launch_tile_v<T, VV, KIND, HV>(ps, tp, tg, s);
+            return;
+        }
         if (tg.tma) {
             if (tg.vec == 1)
                 launch_tma_v<T, 1, KIND, HV>(p, tp, tg, P->ctx->d_status, s);
@@ -663,6 +720,10 @@ static Shape autotune(rbffd_pde* P)
         Shape c{1, 0, R, 1};  // weights and indices streamed by bulk copies
         TileGeom tg;
         if (tile_geom(P, c, &tg)) cands.push_back(c);
+        if (sched_rows(P) && pde_sched_prepare(P, R) == RBFFD_OK) {  // rows in the conflict-avoiding slot order
+            Shape cs{1, 0, R, 0, 1};
+            if (tile_geom(P, cs, &tg)) cands.push_back(cs);
+        }
     }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -673,6 +734,7 @@ static Shape autotune(rbffd_pde* P)
     auto time_graph = [&](const Shape& c, int launches, bool full_steps, int trials) -> float {
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
+        if (c.sched && pde_sched_prepare(P, c.tile) != RBFFD_OK) return -1.f;
         if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             cudaGetLastError();
             return -1.f;
@@ -697,8 +759,10 @@ static Shape autotune(rbffd_pde* P)
             return -1.f;
         }
         if (log)
-            fprintf(stderr, "[rbffd tune] kind=%d hv=%d dtype=%d T=%d N=%d n_pad=%d lanes=%d block=%d tile=%d tma=%d%s: %.2f us\n",
-                    P->kind, P->use_hv, P->dtype, P->T, P->g->N, P->g->n_pad, c.lanes, c.block, c.tile, c.tma,
+            fprintf(stderr,
+                    "[rbffd tune] kind=%d hv=%d dtype=%d T=%d N=%d n_pad=%d lanes=%d block=%d tile=%d tma=%d sched=%d%s: "
+                    "%.2f us\n",
+                    P->kind, P->use_hv, P->dtype, P->T, P->g->N, P->g->n_pad, c.lanes, c.block, c.tile, c.tma, c.sched,
                     full_steps ? " (full steps)" : "", 1e3f * ms / launches);
         return ms / launches;
     };
@@ -809,6 +873,7 @@ static void pde_free(rbffd_pde* P)
     dev_free(ctx, P->cu, (size_t)P->g->N * es);
     dev_free(ctx, P->cv, (size_t)P->g->N * es);
     dev_free(ctx, P->wf, (size_t)P->g->N32 * P->g->n4 * sizeof(float));
+    dev_free(ctx, P->ws, (size_t)P->g->N32 * P->g->n4 * sizeof(float));
     delete P;
 }
 
@@ -857,6 +922,7 @@ extern "C" int rbffd_pde_set_fused_operator(rbffd_pde* P, int on)
         P->wf, g->d_w64[P->op[0]], g->d_w64[P->op[1]], P->op[2] >= 0 ? g->d_w64[P->op[2]] : nullptr,
         (const float*)P->cu, (const float*)P->cv, g->N, g->N32, g->nc);
     RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    P->ws_src = nullptr;  // a scheduled copy of the previous operator is stale
     if (P->gexec) {
         cudaGraphExecDestroy(P->gexec);
         P->gexec = nullptr;
@@ -1047,18 +1113,24 @@ extern "C" int rbffd_pde_get_shape(rbffd_pde* P, int* lanes, int* block)
     return RBFFD_OK;
 }
 
-extern "C" int rbffd_pde_set_tiled_shape(rbffd_pde* P, int rows_per_block, int lanes, int stream_weights)
+extern "C" int rbffd_pde_set_tiled_shape(rbffd_pde* P, int rows_per_block, int lanes, int flags)
 {
     if (!P) return RBFFD_ERR_INVALID;
     if (rows_per_block < 32 || rows_per_block > 1024 || rows_per_block % 32 || !(lanes == 1 || lanes == 2 || lanes == 4))
         return set_error(P->ctx, RBFFD_ERR_INVALID, "rows_per_block must be a multiple of 32, lanes 1, 2 or 4");
-    if (stream_weights && lanes != 1)
-        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights use one lane per row");
+    if (flags & ~(RBFFD_TILE_STREAM_WEIGHTS | RBFFD_TILE_SLOT_SCHEDULE))
+        return set_error(P->ctx, RBFFD_ERR_INVALID, "unknown tiled-shape flags 0x%x", flags);
+    const bool stream_weights = flags & RBFFD_TILE_STREAM_WEIGHTS, sched = flags & RBFFD_TILE_SLOT_SCHEDULE;
+    if ((stream_weights || sched) && lanes != 1)
+        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights and slot schedules use one lane per row");
+    if (stream_weights && sched)
+        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights and a slot schedule do not combine");
     cudaSetDevice(P->ctx->device);
     const Halo* h = nullptr;
     int rc = grid_halo(P->g, rows_per_block, &h);
     if (rc) return rc;
-    Shape c{lanes, 0, rows_per_block, stream_weights ? 1 : 0};
+    if (sched && (rc = pde_sched_prepare(P, rows_per_block))) return rc;
+    Shape c{lanes, 0, rows_per_block, stream_weights ? 1 : 0, sched ? 1 : 0};
     TileGeom tg;
     if (!tile_geom(P, c, &tg))
         return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "tiled shape (%d rows, %d lanes) does not fit this PDE",
@@ -1072,6 +1144,13 @@ extern "C" int rbffd_pde_get_tiling(rbffd_pde* P, int* rows_per_block)
 {
     if (!P || !rows_per_block) return RBFFD_ERR_INVALID;
     *rows_per_block = P->shape.tile;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_get_tile_flags(rbffd_pde* P, int* flags)
+{
+    if (!P || !flags) return RBFFD_ERR_INVALID;
+    *flags = (P->shape.tma ? RBFFD_TILE_STREAM_WEIGHTS : 0) | (P->shape.sched ? RBFFD_TILE_SLOT_SCHEDULE : 0);
     return RBFFD_OK;
 }
 
@@ -1116,13 +1195,15 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
         const Halo* h = nullptr;
         int rc = grid_halo(P->g, sh.tile, &h);
         if (rc) return rc;
+        if (sh.sched && (rc = pde_sched_prepare(P, sh.tile))) return rc;
     }
     if (flags & RBFFD_ADVANCE_GRAPH) {
         const int chunk = 25;
         int full = nsteps / chunk, rest = nsteps % chunk;
         if (full > 0) {
             if (!P->gexec || P->g_dt != dt || P->g_steps != chunk || P->g_shape.lanes != sh.lanes ||
-                P->g_shape.block != sh.block || P->g_shape.tile != sh.tile || P->g_shape.tma != sh.tma) {
+                P->g_shape.block != sh.block || P->g_shape.tile != sh.tile || P->g_shape.tma != sh.tma ||
+                P->g_shape.sched != sh.sched) {
                 if (P->gexec) {
                     cudaGraphExecDestroy(P->gexec);
                     P->gexec = nullptr;

@@ -539,8 +539,8 @@ int bank_create(rbffd_server* S, const Request& r, Bank& b)
         b.halo = h;
     if (b.halo && b.dtype == RBFFD_F32) {  // FP32: the conflict-avoiding slot schedule
         const Halo* hs = nullptr;
-        if ((rc = grid_halo_schedule(g, SEG_ROWS, &hs)) ||
-            (b.kind == KIND_HEAT && (rc = grid_f32_scheduled(g, b.op[0], &b.wsched)))) {
+        if ((rc = grid_halo_schedule(g, SEG_ROWS, 8, &hs)) ||
+            (b.kind == KIND_HEAT && (rc = grid_f32_scheduled(g, SEG_ROWS, b.op[0], &b.wsched)))) {
             bank_free_memory(ctx, b);
             return rc;
         }
@@ -569,7 +569,7 @@ int bank_create(rbffd_server* S, const Request& r, Bank& b)
                 const int rows = g->N32;
                 k_fuse_advection<<<(rows + 127) / 128, 128, 0, S->astream>>>(
                     (float*)b.wf, g->d_w64[b.op[0]], g->d_w64[b.op[1]], b.op[2] >= 0 ? g->d_w64[b.op[2]] : nullptr,
-                    (const double*)cu64, (const double*)cv64, b.sched ? b.halo->d_slot_s : nullptr, g->N, rows,
+                    (const double*)cu64, (const double*)cv64, b.sched ? b.halo->d_slot_s[3] : nullptr, g->N, rows,
                     g->nc);
                 cudaError_t e = cudaGetLastError();
                 if (e == cudaSuccess) e = cudaStreamSynchronize(S->astream);
@@ -746,7 +746,7 @@ void fill_desc(BankDesc<T>& d, const Bank& b, int block0)
     d.hrows = b.halo ? b.halo->d_rows : nullptr;
     d.hptr = b.halo ? b.halo->d_ptr : nullptr;
     d.hnodes = b.halo ? b.halo->d_nodes : nullptr;
-    d.lidx = b.halo ? (b.sched ? b.halo->d_lidx_s : b.halo->d_lidx) : nullptr;
+    d.lidx = b.halo ? (b.sched ? b.halo->d_lidx_s[3] : b.halo->d_lidx) : nullptr;
     d.N = g->N;
     d.nc = g->nc;
     d.kind = b.wf ? KIND_HEAT : b.kind;

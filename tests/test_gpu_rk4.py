@@ -254,11 +254,12 @@ def test_autotuner_leaves_the_state_untouched(heat, dtype):
     tuned.fillInitialConditions(heat["u0"])
     tuned.advance(R.RK4, 1e-6, 7)
     lanes, block, rows = tuned.getShape()
+    flags = tuned.getTileFlags()
     out_tuned = tuned.getLocalSolution()
     tuned.close()
     forced = R.HeatSphere(grid, der, 1.0, dtype=dtype)
     if rows > 0:
-        forced.setTiledShape(rows, lanes)
+        forced.setTiledShape(rows, lanes, stream_weights=bool(flags & 1), slot_schedule=bool(flags & 2))
     else:
         forced.setShape(lanes, block)
     forced.fillInitialConditions(heat["u0"])
@@ -267,3 +268,80 @@ def test_autotuner_leaves_the_state_untouched(heat, dtype):
     forced.close()
     grid.close()
     ctx2.close()
+
+
+@pytest.mark.parametrize("ntr", [4, 8, 16])
+def test_slot_schedule_heat_multi_tracer(heat, ntr):
+    """FP32 heat with 4, 8 or 16 tracers, rows reading their slots in the
+    halo's conflict-avoiding order: within FP32 rounding of the same tile in
+    stencil order, and within 1e-5 of the FP64 oracle."""
+    rng = np.random.default_rng(30 + ntr)
+    u0 = heat["u0"][:, None] * (1.0 + 0.1 * rng.random((1, ntr)))
+    steps, dt = 40, 1e-6
+    ref = O.rk4_heat(heat["st"], None, heat["W"][O.LSFC], u0, dt, steps)
+
+    def run(sched):
+        pde = R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=R.F32, ntracers=ntr)
+        pde.setTiledShape(128, 1, slot_schedule=sched)
+        assert pde.getTileFlags() == (R.TimeDependentPDE.TILE_SLOT_SCHEDULE if sched else 0)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, dt, steps, graph=True)
+        out = pde.getLocalSolution()
+        pde.close()
+        return out
+
+    s, plain = run(True), run(False)
+    assert rel_l2(s, ref) < 1e-5
+    assert rel_l2(s, plain) < 2e-6
+    assert not np.array_equal(s, plain)  # a different summation order
+
+
+def test_slot_schedule_fused_advection_and_refresh(bell):
+    """16 tracers with the fused advection operator in slot order: within 1e-5
+    of the FP64 oracle; after the operator is fused again (off, on) the
+    scheduled copy follows it (same bits as a fresh PDE)."""
+    T = 16
+    rng = np.random.default_rng(31)
+    u0 = rng.random((bell["xyz"].shape[0], T))
+    steps, dt = 10, bell["p"]["dt"]
+    ref = O.rk4_advect(bell["st"], None, bell["W"][O.LAMBDA], bell["W"][O.THETA], bell["W"][O.HV], bell["cu"],
+                       bell["cv"], u0, dt, steps)
+
+    def make():
+        pde = R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=R.F32, ntracers=T)
+        pde.setFusedOperator(True)
+        pde.setTiledShape(128, 1, slot_schedule=True)
+        pde.fillInitialConditions(u0)
+        return pde
+
+    pde = make()
+    pde.advance(R.RK4, dt, steps, graph=True)
+    first = pde.getLocalSolution()
+    assert rel_l2(first, ref) < 1e-5
+    pde.setFusedOperator(False)
+    pde.setFusedOperator(True)
+    pde.fillInitialConditions(u0)
+    pde.setTime(0.0)
+    pde.advance(R.RK4, dt, steps, graph=True)
+    assert np.array_equal(pde.getLocalSolution(), first)
+    pde.close()
+
+
+def test_slot_schedule_refused_where_it_does_not_apply(bell, heat):
+    cases = [R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=R.F64, ntracers=4),   # FP64
+             R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=R.F32, ntracers=1),   # scalar records
+             R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=R.F32, ntracers=32),  # 128-byte records
+             R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=R.F32, ntracers=16)]  # 3 ops
+    for pde in cases:
+        with pytest.raises(R.RbffdError) as e:
+            pde.setTiledShape(128, 1, slot_schedule=True)
+        assert e.value.status == -5
+        pde.close()
+    pde = R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=R.F32, ntracers=4)
+    with pytest.raises(R.RbffdError) as e:
+        pde.setTiledShape(128, 2, slot_schedule=True)  # one lane per row only
+    assert e.value.status == -1
+    with pytest.raises(R.RbffdError) as e:
+        pde.setTiledShape(128, 1, stream_weights=True, slot_schedule=True)
+    assert e.value.status == -1
+    pde.close()
