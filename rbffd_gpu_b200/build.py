@@ -72,7 +72,7 @@ def build(force=False, verbose=False, ptxas_v=False):
 
 CPP = os.path.join(HERE, "cpp")
 # C++ drivers on the C++ API (cpp/rbffd_cuda.hpp), linked against the library
-DRIVERS = {"cosine_bell_cuda": "cosine_bell_main.cpp"}
+DRIVERS = {"cosine_bell_cuda": "cosine_bell_main.cpp", "vortex_rollup_cuda": "vortex_rollup_main.cpp"}
 
 
 def build_drivers(force=False):

@@ -79,3 +79,54 @@ def test_cosine_bell_driver_matches_python_path(tmp_path):
     grid.close()
     ctx.close()
     assert rel_l2(h_cpp, h_py) < 1e-12  # same kernels; the autotuned lane split may differ per process
+
+
+VORTEX = os.path.join(ROOT, "rbffd_gpu_b200", "lib", "vortex_rollup_cuda")
+
+
+def test_vortex_driver_is_built_and_exits_like_the_reference_on_error():
+    assert os.access(VORTEX, os.X_OK)
+    if has_gpu():
+        pytest.skip("a GPU is present")
+    r = subprocess.run([VORTEX, "GRID_SIZE=64", "STENCIL_SIZE=9"], capture_output=True, text=True)
+    assert r.returncode == 1 and "no CUDA device" in r.stderr
+
+
+@pytest.mark.gpu
+def test_vortex_rollup_driver_matches_python_path(tmp_path):
+    """The C++ vortex roll-up driver (RBFFD_CUDA + VortexRollup_CUDA, one
+    advance per iteration, hash-grid stencils, the eigenvalue check of the
+    d/dlambda operator) and the Python view of the same C ABI give the same
+    solution, and it tracks the exact roll-up."""
+    N, n, dt, t_end = 4096, 31, 0.01, 0.3
+    out = tmp_path / "h.bin"
+    args = ["GRID_SIZE=%d" % N, "STENCIL_SIZE=%d" % n, "EPSILON_C1=0.09375", "EPSILON_C2=0", "HV_K=4",
+            "HV_GAMMA=1e-3", "POLY_DEG=2", "DT=%g" % dt, "END_TIME=%g" % t_end, "LOCAL_SOL_DUMP_FREQUENCY=10",
+            "DERIVATIVE_EIGENVALUE_TEST=1", "OUTPUT=%s" % out]
+    r = subprocess.run([VORTEX] + args, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "Suggested max_dt based on eigenvalues" in r.stdout
+    assert r.stdout.count("Local Solution [ Iteration:") == 3  # iterations 0, 10, 20
+    h_cpp = np.fromfile(out, dtype=np.float64)
+    ctx = R.Context(0)
+    xyz = R.fibonacci_nodes(N, 1)
+    order, st, _ = R.stencils_hash(xyz, n)
+    xyz = xyz[order]
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(R.LAMBDA, grid, 2)
+    der.setUseHyperviscosity(1)
+    der.setEpsilonByParameters(0.09375, 0.0)
+    der.setHVScalars(4, 1e-3)
+    der.setPolynomialDegree(2)
+    der.computeAllWeightsForAllStencils()
+    pde = R.VortexRollup(grid, der, True)
+    pde.fillInitialConditions(R.exact_vortex_rollup(xyz, 0.0))
+    steps = int(t_end / dt)
+    for _ in range(steps):
+        pde.advance(R.RK4, dt, 1)
+    h_py = pde.getLocalSolution()
+    pde.close()
+    grid.close()
+    ctx.close()
+    assert rel_l2(h_cpp, h_py) < 1e-12  # same kernels; the autotuned lane split may differ per process
+    assert rel_l2(h_cpp, R.exact_vortex_rollup(xyz, steps * dt)) < 0.1
