@@ -681,13 +681,13 @@ static int unfused_stage(rbffd_pde* P, int stage, double dt, cudaStream_t s)
 }
 
 // ---------------------------------------------------------------------------
-// autotuner.  Round 1 times every candidate shape on the stage sequence
-// 0, 1, 2 (the stages that write only the scratch buffers xa, xb and acc).
-// Round 2 times the three fastest as the solver runs them: 25 full RK4 steps
-// in one CUDA graph, with dt = 0 (every stage then writes u back unchanged,
-// u + 0 * f) and u saved and restored around the timing besides, so the
-// caller's state is untouched.  The fastest of round 2 is kept per problem
-// shape.
+// autotuner.  A first pass times every candidate shape on the stage
+// sequence 0, 1, 2 (the stages that write only the scratch buffers xa, xb and
+// acc).  A second pass times the three fastest as the solver runs them: 25
+// full RK4 steps in one CUDA graph, with dt = 0 (every stage then writes u
+// back unchanged, u + 0 * f) and u saved and restored around the timing
+// besides, so the caller's state is untouched.  The fastest of the second
+// pass is kept per problem shape.
 
 static Shape autotune(rbffd_pde* P)
 {
@@ -766,23 +766,23 @@ static Shape autotune(rbffd_pde* P)
                     full_steps ? " (full steps)" : "", 1e3f * ms / launches);
         return ms / launches;
     };
-    std::vector<std::pair<float, int>> round1;
+    std::vector<std::pair<float, int>> first_pass;
     for (int k = 0; k < (int)cands.size(); k++) {
         const float t = time_graph(cands[k], 21, false, 2);
-        if (t >= 0.f) round1.push_back({t, k});
+        if (t >= 0.f) first_pass.push_back({t, k});
     }
-    std::sort(round1.begin(), round1.end());
-    Shape best = round1.empty() ? cands[0] : cands[round1[0].second];
+    std::sort(first_pass.begin(), first_pass.end());
+    Shape best = first_pass.empty() ? cands[0] : cands[first_pass[0].second];
     const size_t ubytes = (size_t)P->g->N * P->T * (P->dtype == RBFFD_F64 ? 8 : 4);
     void* saved = nullptr;
-    if (round1.size() > 1 && dev_alloc(ctx, &saved, ubytes) == RBFFD_OK) {
+    if (first_pass.size() > 1 && dev_alloc(ctx, &saved, ubytes) == RBFFD_OK) {
         if (cudaMemcpyAsync(saved, P->u, ubytes, cudaMemcpyDeviceToDevice, ctx->stream) == cudaSuccess) {
             float best_ms = 1e30f;
-            for (int r = 0; r < (int)round1.size() && r < 3; r++) {
-                const float t = time_graph(cands[round1[r].second], 100, true, 3);
+            for (int r = 0; r < (int)first_pass.size() && r < 3; r++) {
+                const float t = time_graph(cands[first_pass[r].second], 100, true, 3);
                 if (t >= 0.f && t < best_ms) {
                     best_ms = t;
-                    best = cands[round1[r].second];
+                    best = cands[first_pass[r].second];
                 }
             }
             cudaMemcpyAsync(P->u, saved, ubytes, cudaMemcpyDeviceToDevice, ctx->stream);
