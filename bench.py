@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="setup plus 25 un-graphed RK4 steps with the autotuned kernel shape, for ncu captures")
+    ap.add_argument("--profile-tile", type=int, default=0, metavar="ROWS",
+                    help="as --profile, with the halo-tiled stage kernel of ROWS rows and one lane per row forced "
+                         "(no autotuning)")
     ap.add_argument("--profile-multitracer", default=None, metavar="ROWS,LANES",
                     help="16-tracer vortex case on N=163842, n=101 (weights > L2), 3 un-graphed RK4 steps with the "
                          "tiled shape ROWS,LANES (0,0 = global-memory gathers; further fields: f = FP32 fused "
@@ -1000,7 +1003,7 @@ def bench_serving(R, torch, ctx):
     }
 
 
-def run_profile():
+def run_profile(tile_rows=0):
     import rbffd_gpu_b200 as R
     xyz, st, u0, eps, _ = setup_problem()
     ctx = R.Context(0)
@@ -1010,8 +1013,10 @@ def run_profile():
     der.setPolynomialDegree(WORKLOAD["deg"])
     der.computeAllWeightsForAllStencils()
     pde = R.HeatSphere(grid, der, 1.0, dtype=R.F32)
+    if tile_rows:
+        pde.setTiledShape(tile_rows, 1)
     pde.fillInitialConditions(u0)
-    pde.advance(R.RK4, WORKLOAD["dt"], 25)  # the autotuner picks the shape, as in the benchmark
+    pde.advance(R.RK4, WORKLOAD["dt"], 25)  # unless forced, the autotuner picks the shape, as in the benchmark
     print("profile run done, shape", pde.getShape())
     pde.close()
     grid.close()
@@ -1140,8 +1145,8 @@ def main():
         run_profile_heat_hbm()
     elif args.profile_multitracer:
         run_profile_multitracer(args.profile_multitracer)
-    elif args.profile:
-        run_profile()
+    elif args.profile or args.profile_tile:
+        run_profile(args.profile_tile)
     elif args.impl == "reference":
         run_reference(args)
     else:
