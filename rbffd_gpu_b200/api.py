@@ -543,13 +543,15 @@ class TimeDependentPDE:
         """FP32 advection: one fused operator -(cu Wl + cv Wt) + Whv per stage."""
         self.ctx.check(self.ctx.L.rbffd_pde_set_fused_operator(self.h, int(bool(on))), "set_fused_operator")
 
-    TILE_STREAM_WEIGHTS, TILE_SLOT_SCHEDULE = 1, 2
+    TILE_STREAM_WEIGHTS, TILE_SLOT_SCHEDULE, TILE_PREFETCH = 1, 2, 4
 
-    def setTiledShape(self, rows_per_block, lanes=1, stream_weights=False, slot_schedule=False):
+    def setTiledShape(self, rows_per_block, lanes=1, stream_weights=False, slot_schedule=False, prefetch=False):
         """Tiled stage kernel of rows_per_block rows; stream_weights: bulk-copy
         weight streaming; slot_schedule: FP32 rows read their slots in the
-        halo's conflict-avoiding order (one operator, 4/8/16 tracers)."""
-        flags = (self.TILE_STREAM_WEIGHTS if stream_weights else 0) | (self.TILE_SLOT_SCHEDULE if slot_schedule else 0)
+        halo's conflict-avoiding order (one operator, 4/8/16 tracers);
+        prefetch: upcoming chunks of weights and indices asked of L2."""
+        flags = ((self.TILE_STREAM_WEIGHTS if stream_weights else 0) | (self.TILE_SLOT_SCHEDULE if slot_schedule else 0) |
+                 (self.TILE_PREFETCH if prefetch else 0))
         self.ctx.check(self.ctx.L.rbffd_pde_set_tiled_shape(self.h, rows_per_block, lanes, flags), "set_tiled_shape")
 
     def getTileFlags(self):

@@ -22,6 +22,10 @@ __host__ __device__ __forceinline__ size_t sell_elem(int i, int s, int nc) { ret
 
 __device__ __forceinline__ int4 ld_idx4(const int* p) { return __ldg(reinterpret_cast<const int4*>(p)); }
 
+// Ask the memory system to bring the line holding p into L2 (no register,
+// no wait): issued a few chunks ahead of the loads that will use it.
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ void ld_w4(const float* p, float (&w)[4])
 {
     float4 t = __ldg(reinterpret_cast<const float4*>(p));

@@ -36,6 +36,7 @@ struct Shape {
     int tile = 0;  // rows per block with the halo staged in shared memory; 0 = gather from global memory
     int tma = 0;   // tiled kernel that streams weights and indices into shared memory with bulk copies
     int sched = 0; // tiled, FP32, one operator: each row reads its slots in the halo's conflict-avoiding schedule
+    int pf = 0;    // tiled, one lane per row: upcoming chunks of weights and indices prefetched into L2
 };
 
 // Device status word of a context: kernels whose waits are bounded write a

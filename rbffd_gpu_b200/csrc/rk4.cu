@@ -210,7 +210,15 @@ struct TileParams {
     int N32;                       // rows of the sliced ELL arrays (N rounded up to 32)
 };
 
-template <typename T, int VEC, int G, int KIND, bool HV>
+// Chunks ahead that the prefetching variant of k_stage_tile asks L2 for.
+constexpr int TILE_PF_DIST = 2;
+
+// PF > 0: while working on chunk c, one lane per 128-byte line of a chunk's
+// weights asks L2 for chunk c + PF * G (weights and local indices).  It pays
+// where the weight stream comes from HBM and the kernel waits on it (FP64
+// multi-tracer stages); where the weights stay in L2 the extra instructions
+// cost more, so the autotuner decides.
+template <typename T, int VEC, int G, int KIND, bool HV, int PF = 0>
 __global__ void __launch_bounds__(1024) k_stage_tile(StageParams<T> p, TileParams tp)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -235,9 +243,20 @@ __global__ void __launch_bounds__(1024) k_stage_tile(StageParams<T> p, TileParam
 #pragma unroll
     for (int v = 0; v < VEC; v++) d0[v] = d1[v] = d2[v] = T(0);
     if (active) {
+        constexpr int RPL = 128 / (4 * (int)sizeof(T));  // rows per 128-byte line of one chunk
+        const bool lead = PF > 0 && lr == 0 && (i % RPL) == 0;
 #pragma unroll 2
         for (int c = g; c < p.nc; c += G) {
             const size_t o = sell_off(i, c, p.nc);
+            if (PF > 0 && lead && c + PF * G < p.nc) {
+                const size_t q = sell_off(i, c + PF * G, p.nc);
+                prefetch_l2(p.w0 + q);
+                if (KIND == KIND_ADVECT) {
+                    prefetch_l2(p.w1 + q);
+                    if (HV) prefetch_l2(p.w2 + q);
+                }
+                prefetch_l2(tp.lidx + q);
+            }
             const ushort4 l4 = __ldg(reinterpret_cast<const ushort4*>(tp.lidx + o));
             const int ll[4] = {l4.x, l4.y, l4.z, l4.w};
             T wa[4], wb[4], wc[4];
@@ -471,6 +490,7 @@ struct TileGeom {
     int vec = 1, vpn = 1, G = 1, threads = 0;
     int tma = 0, halo_bytes = 0, stage_bytes = 0;
     int sched = -1;  // index of the halo's slot schedule the rows read (-1: stencil order)
+    int pf = 0;      // L2 prefetch of upcoming chunks
     size_t smem = 0;
 };
 
@@ -546,6 +566,10 @@ static bool tile_geom(rbffd_pde* P, Shape sh, TileGeom* tg)
             return false;
         t.sched = log2_rows(Pw);
     }
+    if (sh.pf) {
+        if (t.G != 1 || sh.tma || sh.sched) return false;
+        t.pf = 1;
+    }
     if (sh.tma) {
         if (t.G != 1) return false;
         const int K = P->kind == KIND_HEAT ? 1 : (P->use_hv ? 3 : 2);
@@ -565,6 +589,12 @@ template <typename T, int VEC, int KIND, bool HV>
 static void launch_tile_v(const StageParams<T>& p, const TileParams& tp, const TileGeom& t, cudaStream_t s)
 {
     const int nb = t.h->nblocks;
+    if (t.pf) {
+        cudaFuncSetAttribute(k_stage_tile<T, VEC, 1, KIND, HV, TILE_PF_DIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)t.smem);
+        k_stage_tile<T, VEC, 1, KIND, HV, TILE_PF_DIST><<<nb, t.threads, t.smem, s>>>(p, tp);
+        return;
+    }
     switch (t.G) {
     case 1:
         cudaFuncSetAttribute(k_stage_tile<T, VEC, 1, KIND, HV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem);
@@ -720,6 +750,8 @@ static Shape autotune(rbffd_pde* P)
         Shape c{1, 0, R, 1};  // weights and indices streamed by bulk copies
         TileGeom tg;
         if (tile_geom(P, c, &tg)) cands.push_back(c);
+        Shape cp{1, 0, R, 0, 0, 1};  // upcoming chunks prefetched into L2
+        if (tile_geom(P, cp, &tg)) cands.push_back(cp);
         if (sched_rows(P) && pde_sched_prepare(P, R) == RBFFD_OK) {  // rows in the conflict-avoiding slot order
             Shape cs{1, 0, R, 0, 1};
             if (tile_geom(P, cs, &tg)) cands.push_back(cs);
@@ -760,9 +792,9 @@ static Shape autotune(rbffd_pde* P)
         }
         if (log)
             fprintf(stderr,
-                    "[rbffd tune] kind=%d hv=%d dtype=%d T=%d N=%d n_pad=%d lanes=%d block=%d tile=%d tma=%d sched=%d%s: "
-                    "%.2f us\n",
-                    P->kind, P->use_hv, P->dtype, P->T, P->g->N, P->g->n_pad, c.lanes, c.block, c.tile, c.tma, c.sched,
+                    "[rbffd tune] kind=%d hv=%d dtype=%d T=%d N=%d n_pad=%d lanes=%d block=%d tile=%d tma=%d sched=%d "
+                    "pf=%d%s: %.2f us\n",
+                    P->kind, P->use_hv, P->dtype, P->T, P->g->N, P->g->n_pad, c.lanes, c.block, c.tile, c.tma, c.sched, c.pf,
                     full_steps ? " (full steps)" : "", 1e3f * ms / launches);
         return ms / launches;
     };
@@ -1118,19 +1150,20 @@ extern "C" int rbffd_pde_set_tiled_shape(rbffd_pde* P, int rows_per_block, int l
     if (!P) return RBFFD_ERR_INVALID;
     if (rows_per_block < 32 || rows_per_block > 1024 || rows_per_block % 32 || !(lanes == 1 || lanes == 2 || lanes == 4))
         return set_error(P->ctx, RBFFD_ERR_INVALID, "rows_per_block must be a multiple of 32, lanes 1, 2 or 4");
-    if (flags & ~(RBFFD_TILE_STREAM_WEIGHTS | RBFFD_TILE_SLOT_SCHEDULE))
+    if (flags & ~(RBFFD_TILE_STREAM_WEIGHTS | RBFFD_TILE_SLOT_SCHEDULE | RBFFD_TILE_PREFETCH))
         return set_error(P->ctx, RBFFD_ERR_INVALID, "unknown tiled-shape flags 0x%x", flags);
-    const bool stream_weights = flags & RBFFD_TILE_STREAM_WEIGHTS, sched = flags & RBFFD_TILE_SLOT_SCHEDULE;
-    if ((stream_weights || sched) && lanes != 1)
-        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights and slot schedules use one lane per row");
-    if (stream_weights && sched)
-        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights and a slot schedule do not combine");
+    const bool stream_weights = flags & RBFFD_TILE_STREAM_WEIGHTS, sched = flags & RBFFD_TILE_SLOT_SCHEDULE,
+               pf = flags & RBFFD_TILE_PREFETCH;
+    if ((stream_weights || sched || pf) && lanes != 1)
+        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights, slot schedules and prefetch use one lane per row");
+    if ((int)stream_weights + (int)sched + (int)pf > 1)
+        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights, a slot schedule and prefetch do not combine");
     cudaSetDevice(P->ctx->device);
     const Halo* h = nullptr;
     int rc = grid_halo(P->g, rows_per_block, &h);
     if (rc) return rc;
     if (sched && (rc = pde_sched_prepare(P, rows_per_block))) return rc;
-    Shape c{lanes, 0, rows_per_block, stream_weights ? 1 : 0, sched ? 1 : 0};
+    Shape c{lanes, 0, rows_per_block, stream_weights ? 1 : 0, sched ? 1 : 0, pf ? 1 : 0};
     TileGeom tg;
     if (!tile_geom(P, c, &tg))
         return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "tiled shape (%d rows, %d lanes) does not fit this PDE",
@@ -1150,7 +1183,8 @@ extern "C" int rbffd_pde_get_tiling(rbffd_pde* P, int* rows_per_block)
 extern "C" int rbffd_pde_get_tile_flags(rbffd_pde* P, int* flags)
 {
     if (!P || !flags) return RBFFD_ERR_INVALID;
-    *flags = (P->shape.tma ? RBFFD_TILE_STREAM_WEIGHTS : 0) | (P->shape.sched ? RBFFD_TILE_SLOT_SCHEDULE : 0);
+    *flags = (P->shape.tma ? RBFFD_TILE_STREAM_WEIGHTS : 0) | (P->shape.sched ? RBFFD_TILE_SLOT_SCHEDULE : 0) |
+             (P->shape.pf ? RBFFD_TILE_PREFETCH : 0);
     return RBFFD_OK;
 }
 
@@ -1203,7 +1237,7 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
         if (full > 0) {
             if (!P->gexec || P->g_dt != dt || P->g_steps != chunk || P->g_shape.lanes != sh.lanes ||
                 P->g_shape.block != sh.block || P->g_shape.tile != sh.tile || P->g_shape.tma != sh.tma ||
-                P->g_shape.sched != sh.sched) {
+                P->g_shape.sched != sh.sched || P->g_shape.pf != sh.pf) {
                 if (P->gexec) {
                     cudaGraphExecDestroy(P->gexec);
                     P->gexec = nullptr;

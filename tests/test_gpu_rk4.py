@@ -163,7 +163,9 @@ def test_heat_fp32_tolerance_and_exact_decay(heat):
 
 @pytest.mark.parametrize("dtype,tol,tiled", [(R.F64, 0.0, None), (R.F32, 1e-5, None), (R.F64, 0.0, (64, 1)),
                                              (R.F64, 1e-12, (32, 4)), (R.F32, 1e-5, (128, 2)),
-                                             (R.F64, 0.0, (64, 1, True)), (R.F32, 1e-5, (128, 1, True))])
+                                             (R.F64, 0.0, (64, 1, True)), (R.F32, 1e-5, (128, 1, True)),
+                                             (R.F64, 0.0, (64, 1, False, False, True)),
+                                             (R.F32, 1e-5, (128, 1, False, False, True))])
 def test_multi_tracer_advection(bell, dtype, tol, tiled):
     T = 16
     rng = np.random.default_rng(4)
@@ -259,7 +261,8 @@ def test_autotuner_leaves_the_state_untouched(heat, dtype):
     tuned.close()
     forced = R.HeatSphere(grid, der, 1.0, dtype=dtype)
     if rows > 0:
-        forced.setTiledShape(rows, lanes, stream_weights=bool(flags & 1), slot_schedule=bool(flags & 2))
+        forced.setTiledShape(rows, lanes, stream_weights=bool(flags & 1), slot_schedule=bool(flags & 2),
+                             prefetch=bool(flags & 4))
     else:
         forced.setShape(lanes, block)
     forced.fillInitialConditions(heat["u0"])
