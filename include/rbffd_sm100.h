@@ -86,6 +86,23 @@ int rbffd_nodes_fibonacci(int N, uint64_t seed, double* xyz);
  * k-d tree of external/kdtree/KDTree.h:407-433.  st[N][n].  *ties (optional)
  * receives the number of stencils whose distance list had an exact tie. */
 int rbffd_stencils_knn(const double* xyz, int N, int n, int* st, int* ties, int nthreads);
+/* Grid::generateStencils(st_generator_t) (src/grids/grid_interface.cpp:514-536)
+ * for the reference's default generator and its k-d tree, in the caller's
+ * numbering, with the grid's max_st_radius:
+ *   RBFFD_ST_BRUTE_FORCE: Grid::generateStencilsBruteForce
+ *     (grid_interface.cpp:637-686): nodes by squared distance, equal
+ *     distances in decreasing node number (its std::set with a `<=`
+ *     comparator, grid_interface.h:442-461) -- a duplicate point with a
+ *     higher number then comes before the centre, as in the reference;
+ *   RBFFD_ST_KDTREE: the lists of rbffd_stencils_knn.
+ * Each list stops at the first node whose distance is not below max_radius
+ * (DBL_MAX: the reference's default, no trimming); st_len[N] receives the
+ * lengths and the rest of each row is the centre (padding).  Searched over a
+ * cell grid, not O(N^2).  RBFFD_ERR_INVALID for max_radius <= 0 (the
+ * reference's stencils would all be empty). */
+enum { RBFFD_ST_BRUTE_FORCE = 0, RBFFD_ST_KDTREE = 1 };
+int rbffd_stencils_generate(const double* xyz, int N, int n, int method, double max_radius, int* st, int* st_len,
+                            int* ties, int nthreads);
 /* The same stencils (identical lists and tie count) computed on ctx's device:
  * the host bins the points into a uniform cell grid, one warp per node
  * searches the surrounding cells.  Replaces the same reference call

@@ -75,6 +75,7 @@ def ref_lib(name):
         if L is not None and name == "ref_grid":
             L.ref_stencils_hash.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             _dp, ctypes.c_double, _dp, _ip, _ip]
+            L.ref_stencils_generate.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _ip, _ip]
         if L is not None and name == "ref_norms":
             L.ref_sol_norms.argtypes = [_dp, _dp, ctypes.c_int, _dp]
             L.ref_sol_norms.restype = None
@@ -354,6 +355,23 @@ def ref_stencils_hash(xyz, n, dims=(10, 10, 10), extents=None, max_radius=1.7976
     key = {tuple(p): i for i, p in enumerate(xyz.tolist())}
     order = np.array([key[tuple(p)] for p in xs.tolist()], dtype=np.int32)
     return order, st, ln
+
+
+def ref_stencils_generate(xyz, n, method, max_radius=1.7976931348623157e308):
+    """The reference's own Grid::generateStencilsBruteForce (method 0) or
+    generateStencilsKDTree (method 1) with max_st_radius trimming (compiled
+    into oracle/_ref/libref_grid.so): (stencils [N][n] padded with -1,
+    stencil lengths), in the caller's numbering."""
+    L = ref_lib("ref_grid")
+    if L is None:
+        return None
+    xyz = _c(xyz, np.float64)
+    N = len(xyz)
+    st = np.zeros((N, n), dtype=np.int32)
+    ln = np.zeros(N, dtype=np.int32)
+    if L.ref_stencils_generate(_p(xyz), N, n, int(method), float(max_radius), _p(st, _ip), _p(ln, _ip)):
+        raise RuntimeError("ref_stencils_generate")
+    return st, ln
 
 
 def alt_sfc(xyz, wx, wy, wz):

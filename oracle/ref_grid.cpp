@@ -46,3 +46,29 @@ extern "C" int ref_stencils_hash(const double* xyz, int N, int n, int nbx, int n
     }
     return 0;
 }
+
+// The reference's own Grid::generateStencilsBruteForce (method 0,
+// grid_interface.cpp:637-686) and Grid::generateStencilsKDTree (method 1,
+// grid_interface.cpp:688-725), both trimming at max_st_radius; the grid keeps
+// the caller's numbering.  st[N][n] padded with -1.
+extern "C" int ref_stencils_generate(const double* xyz, int N, int n, int method, double max_radius, int* st,
+                                     int* st_len)
+{
+    std::streambuf* old = std::cout.rdbuf();
+    std::ostringstream sink;
+    std::cout.rdbuf(sink.rdbuf());
+    std::vector<NodeType> nodes(N);
+    for (int i = 0; i < N; i++) nodes[i] = NodeType(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    HashGrid g(nodes);
+    g.refreshExtents();
+    g.setMaxStencilSize(n);
+    g.setRadius(max_radius);
+    g.generateStencils(method == 0 ? Grid::ST_BRUTE_FORCE : Grid::ST_KDTREE);
+    std::cout.rdbuf(old);
+    for (int i = 0; i < N; i++) {
+        StencilType& s = g.getStencil(i);
+        st_len[i] = (int)s.size();
+        for (int j = 0; j < n; j++) st[(size_t)i * n + j] = j < (int)s.size() ? (int)s[j] : -1;
+    }
+    return 0;
+}

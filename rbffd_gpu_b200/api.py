@@ -77,6 +77,24 @@ def knn_stencils(xyz, n, nthreads=0, return_ties=False):
     return (st, ties.value) if return_ties else st
 
 
+ST_BRUTE_FORCE, ST_KDTREE, ST_HASH = 0, 1, 2  # Grid::st_generator_t (grid_interface.h:37)
+
+
+def generate_stencils(xyz, n, method=ST_BRUTE_FORCE, max_radius=1.7976931348623157e308, nthreads=0):
+    """Grid::generateStencils with the reference's default brute-force
+    generator or its k-d tree, and max_st_radius trimming: (stencils [N][n],
+    lengths [N]), padding the centre.  Host only; ST_HASH is stencils_hash."""
+    xyz = _f64(xyz)
+    N = xyz.shape[0]
+    st = np.zeros((N, n), dtype=np.int32)
+    ln = np.zeros(N, dtype=np.int32)
+    rc = _lib.load().rbffd_stencils_generate(_dp(xyz), N, n, int(method), float(max_radius), _ip(st), _ip(ln), None,
+                                             nthreads)
+    if rc:
+        raise RbffdError(rc, "rbffd_stencils_generate")
+    return st, ln
+
+
 def write_weights_file(filename, stencils, w, st_len=None, binary=True):
     """The reference's weight file (Matrix Market, text or binary form) for
     weights w [N][n_pad] of stencils [N][n_pad]; host only."""

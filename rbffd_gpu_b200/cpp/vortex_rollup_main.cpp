@@ -13,9 +13,10 @@
 // USE_HYPERVISCOSITY, START_TIME, END_TIME, DT, MAX_NUM_ITERS,
 // LOCAL_SOL_DUMP_FREQUENCY, MAX_LOCAL_REL_ERROR, USE_EIG_DT and
 // DERIVATIVE_EIGENVALUE_TEST (eigenvalues of the operator; dt is lowered to
-// the suggested step when USE_EIG_DT=1), plus STENCIL_GENERATOR (hash, the
-// default, with NS_NB_X/Y/Z; or kdtree), POLY_DEG, DTYPE (64 or 32), SEED and
-// OUTPUT (file for the final solution, N doubles in node order).
+// the suggested step when USE_EIG_DT=1), STENCIL_GEN_TYPE (0 brute force,
+// 1 k-d tree, 2 hash grid with NS_NB_X/Y/Z -- the driver's default,
+// main.cpp:123-164), plus POLY_DEG, DTYPE (64 or 32), SEED and OUTPUT (file
+// for the final solution, N doubles in node order).
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -52,14 +53,18 @@ int main(int argc, char** argv)
     const int dtype = num("DTYPE", 64) == 32 ? RBFFD_F32 : RBFFD_F64;
 
     // nodes: Fibonacci spiral under a seeded rotation; stencils from the
-    // hash-grid generator (renumbering the nodes by cell) or the k-d tree
+    // brute-force or k-d tree generator, or the hash grid (which renumbers
+    // the nodes by cell)
     std::vector<double> xyz(3 * (size_t)N);
     check(nullptr, rbffd_nodes_fibonacci(N, (uint64_t)num("SEED", 1), xyz.data()), "nodes");
     std::vector<int> st((size_t)N * n), len(N, n);
-    const std::string generator = cfg.count("STENCIL_GENERATOR") ? cfg["STENCIL_GENERATOR"] : "hash";
-    if (generator == "kdtree") {
-        check(nullptr, rbffd_stencils_knn(xyz.data(), N, n, st.data(), nullptr, 0), "stencils");
-    } else if (generator == "hash") {
+    const int gen = (int)num("STENCIL_GEN_TYPE", 2);
+    if (gen == 0 || gen == 1) {
+        check(nullptr,
+              rbffd_stencils_generate(xyz.data(), N, n, gen == 0 ? RBFFD_ST_BRUTE_FORCE : RBFFD_ST_KDTREE, DBL_MAX,
+                                      st.data(), len.data(), nullptr, 0),
+              "stencils");
+    } else if (gen == 2) {
         std::vector<int> order(N);
         check(nullptr,
               rbffd_stencils_hash(xyz.data(), N, n, (int)num("NS_NB_X", 10), (int)num("NS_NB_Y", 10),
@@ -70,7 +75,7 @@ int main(int argc, char** argv)
             for (int c = 0; c < 3; c++) renumbered[3 * (size_t)k + c] = xyz[3 * (size_t)order[k] + c];
         xyz.swap(renumbered);
     } else {
-        std::fprintf(stderr, "STENCIL_GENERATOR must be hash or kdtree\n");
+        std::fprintf(stderr, "STENCIL_GEN_TYPE must be 0, 1 or 2\n");
         return 2;
     }
     std::vector<Vec3> nodes(N);

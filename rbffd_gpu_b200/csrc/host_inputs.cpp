@@ -14,6 +14,7 @@
 //   rbffd_exact_sph_heat   -- heat on the unit sphere: sum c_lm e^{-l(l+1)t} Y_lm.
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -102,9 +103,22 @@ static inline double dist2(const double* a, const double* b)
     return d;
 }
 
-extern "C" int rbffd_stencils_knn(const double* xyz, int N, int n, int* st, int* ties, int nthreads)
+// Exact n-nearest search over a uniform cell grid, shared by the k-d tree and
+// brute-force generators (method RBFFD_ST_KDTREE / RBFFD_ST_BRUTE_FORCE).
+// Shells of cells are added until the n-th squared distance is below the
+// searched reach, so every node tied with the n-th is a candidate.  Order:
+// k-d tree (squared distance, index), the centre first if a duplicate point
+// sorted ahead of it; brute force (squared distance, decreasing index), as
+// the reference's std::set with a `<=` comparator leaves equal keys
+// (grid_interface.h:442-461).  Each list is cut at the first entry whose
+// distance sqrt(d2) is not below max_radius (grid_interface.cpp:676, 716);
+// the rest is padding (the centre).
+static int stencils_cell_search(const double* xyz, int N, int n, int method, double max_radius, int* st,
+                                int* st_len, int* ties, int nthreads)
 {
     if (!xyz || !st || N <= 0 || n <= 0 || n > N) return RBFFD_ERR_INVALID;
+    if (method != RBFFD_ST_KDTREE && method != RBFFD_ST_BRUTE_FORCE) return RBFFD_ERR_INVALID;
+    if (!(max_radius > 0.0)) return RBFFD_ERR_INVALID;  // every stencil would be empty
     // Uniform cell grid over the bounding box; cell edge ~ half the radius
     // expected to hold n points on the unit sphere.
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -177,19 +191,41 @@ extern "C" int rbffd_stencils_knn(const double* xyz, int N, int n, int* st, int*
             failed.store(1);
             return;
         }
-        std::sort(cand.begin(), cand.end());  // (distance, index): closest first
+        if (method == RBFFD_ST_KDTREE)
+            std::sort(cand.begin(), cand.end());  // (distance, index): closest first
+        else
+            std::sort(cand.begin(), cand.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+                return a.first < b.first || (a.first == b.first && a.second > b.second);
+            });
         int* out = st + (size_t)i * n;
-        for (int k = 0; k < n; k++) out[k] = cand[k].second;
-        if (out[0] != i) {
+        int len = n;
+        for (int k = 0; k < n; k++) {
+            out[k] = cand[k].second;
+            if (len == n && !(std::sqrt(cand[k].first) < max_radius)) len = k;
+        }
+        if (method == RBFFD_ST_KDTREE && out[0] != i) {
             // duplicate point at distance 0 sorted ahead of the centre: put the centre first
             for (int k = 1; k < n; k++)
                 if (out[k] == i) { std::swap(out[0], out[k]); break; }
         }
+        for (int k = len; k < n; k++) out[k] = i;
+        if (st_len) st_len[i] = len;
         for (int k = 0; k + 1 < (int)cand.size() && k < n; k++)
             if (cand[k].first == cand[k + 1].first) { tie_count.fetch_add(1); break; }
     });
     if (ties) *ties = tie_count.load();
     return failed.load() ? RBFFD_ERR_INVALID : RBFFD_OK;
+}
+
+extern "C" int rbffd_stencils_knn(const double* xyz, int N, int n, int* st, int* ties, int nthreads)
+{
+    return stencils_cell_search(xyz, N, n, RBFFD_ST_KDTREE, DBL_MAX, st, nullptr, ties, nthreads);
+}
+
+extern "C" int rbffd_stencils_generate(const double* xyz, int N, int n, int method, double max_radius, int* st,
+                                       int* st_len, int* ties, int nthreads)
+{
+    return stencils_cell_search(xyz, N, n, method, max_radius, st, st_len, ties, nthreads);
 }
 
 extern "C" int rbffd_exact_cosine_bell(int N, const double* xyz, double a, double* h)

@@ -93,16 +93,17 @@ def test_vortex_driver_is_built_and_exits_like_the_reference_on_error():
 
 
 @pytest.mark.gpu
-def test_vortex_rollup_driver_matches_python_path(tmp_path):
+@pytest.mark.parametrize("gen", [2, 0])
+def test_vortex_rollup_driver_matches_python_path(tmp_path, gen):
     """The C++ vortex roll-up driver (RBFFD_CUDA + VortexRollup_CUDA, one
-    advance per iteration, hash-grid stencils, the eigenvalue check of the
-    d/dlambda operator) and the Python view of the same C ABI give the same
-    solution, and it tracks the exact roll-up."""
+    advance per iteration, hash-grid or brute-force stencils, the eigenvalue
+    check of the d/dlambda operator) and the Python view of the same C ABI
+    give the same solution, and it tracks the exact roll-up."""
     N, n, dt, t_end = 4096, 31, 0.01, 0.3
     out = tmp_path / "h.bin"
     args = ["GRID_SIZE=%d" % N, "STENCIL_SIZE=%d" % n, "EPSILON_C1=0.09375", "EPSILON_C2=0", "HV_K=4",
             "HV_GAMMA=1e-3", "POLY_DEG=2", "DT=%g" % dt, "END_TIME=%g" % t_end, "LOCAL_SOL_DUMP_FREQUENCY=10",
-            "DERIVATIVE_EIGENVALUE_TEST=1", "OUTPUT=%s" % out]
+            "DERIVATIVE_EIGENVALUE_TEST=1", "STENCIL_GEN_TYPE=%d" % gen, "OUTPUT=%s" % out]
     r = subprocess.run([VORTEX] + args, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert "Suggested max_dt based on eigenvalues" in r.stdout
@@ -110,8 +111,11 @@ def test_vortex_rollup_driver_matches_python_path(tmp_path):
     h_cpp = np.fromfile(out, dtype=np.float64)
     ctx = R.Context(0)
     xyz = R.fibonacci_nodes(N, 1)
-    order, st, _ = R.stencils_hash(xyz, n)
-    xyz = xyz[order]
+    if gen == 2:
+        order, st, _ = R.stencils_hash(xyz, n)
+        xyz = xyz[order]
+    else:
+        st, _ = R.generate_stencils(xyz, n, R.ST_BRUTE_FORCE)
     grid = R.Grid(ctx, xyz, st)
     der = R.RBFFD(R.LAMBDA, grid, 2)
     der.setUseHyperviscosity(1)
