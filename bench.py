@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--profile-multitracer", default=None, metavar="ROWS,LANES",
                     help="16-tracer vortex case on N=163842, n=101 (weights > L2), 3 un-graphed RK4 steps with the "
                          "tiled shape ROWS,LANES (0,0 = global-memory gathers; further fields: f = FP32 fused "
-                         "operator, s = conflict-avoiding slot schedule), for ncu captures")
+                         "operator, s = conflict-avoiding slot schedule, d = FP64), for ncu captures")
     ap.add_argument("--profile-serving", type=int, default=0, metavar="K",
                     help="serving stage kernels: K + K requests on two N=163842 grids, 3 RK4 steps, for ncu")
     ap.add_argument("--profile-heat-hbm", action="store_true",
@@ -1030,6 +1030,7 @@ def run_profile_multitracer(spec):
     rows, lanes = int(fields[0]), int(fields[1])
     fused = "f" in fields[2:]
     sched = "s" in fields[2:]
+    fp64 = "d" in fields[2:]
     N, n, T = 163842, 101, 16
     xyz = R.fibonacci_nodes(N, 4)
     st = R.knn_stencils(xyz, n)
@@ -1043,7 +1044,7 @@ def run_profile_multitracer(spec):
     der.setHVScalars(4, 1e-3)
     der.setPolynomialDegree(2)
     der.computeAllWeightsForAllStencils()
-    pde = R.Advection(grid, der, cu, cv, True, dtype=R.F32, ntracers=T)
+    pde = R.Advection(grid, der, cu, cv, True, dtype=R.F64 if fp64 else R.F32, ntracers=T)
     if fused:
         pde.setFusedOperator(True)
     if rows > 0:
