@@ -24,6 +24,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -74,6 +75,46 @@ private:
 typedef std::vector<int> StencilType;  // src/common_typedefs.h:16
 
 // Nodes and stencils resident on the device.
+// Grid::generateStencils(st_max_size, st_generator_t) (grid_interface.h:37,
+// 166-167): stencils of max_st_size nodes for a node list, with the
+// reference's max_st_radius (DBL_MAX: none).  ST_HASH renumbers the nodes by
+// cell, as the reference's hash generator re-sorts its grid: the node list is
+// replaced by the renumbered one.
+enum st_generator_t { ST_BRUTE_FORCE = 0, ST_KDTREE = 1, ST_HASH = 2 };
+inline std::vector<StencilType> generateStencils(std::vector<Vec3>& nodes, unsigned max_st_size,
+                                                 st_generator_t generator = ST_BRUTE_FORCE,
+                                                 double max_st_radius = DBL_MAX, int ns_nx = 10, int ns_ny = 10,
+                                                 int ns_nz = 10)
+{
+    const int N = (int)nodes.size(), n = (int)max_st_size;
+    std::vector<double> xyz(3 * (size_t)N);
+    for (int i = 0; i < N; i++) {
+        xyz[3 * (size_t)i] = nodes[i].x;
+        xyz[3 * (size_t)i + 1] = nodes[i].y;
+        xyz[3 * (size_t)i + 2] = nodes[i].z;
+    }
+    std::vector<int> st((size_t)N * n), len(N);
+    if (generator == ST_HASH) {
+        std::vector<int> order(N);
+        check(nullptr,
+              rbffd_stencils_hash(xyz.data(), N, n, ns_nx, ns_ny, ns_nz, nullptr, max_st_radius, order.data(),
+                                  st.data(), len.data()),
+              "generateStencils");
+        std::vector<Vec3> renumbered(N);
+        for (int k = 0; k < N; k++) renumbered[k] = nodes[order[k]];
+        nodes.swap(renumbered);
+    } else {
+        check(nullptr,
+              rbffd_stencils_generate(xyz.data(), N, n,
+                                      generator == ST_KDTREE ? RBFFD_ST_KDTREE : RBFFD_ST_BRUTE_FORCE, max_st_radius,
+                                      st.data(), len.data(), nullptr, 0),
+              "generateStencils");
+    }
+    std::vector<StencilType> out(N);
+    for (int i = 0; i < N; i++) out[i].assign(st.begin() + (size_t)i * n, st.begin() + (size_t)i * n + len[i]);
+    return out;
+}
+
 class Grid_CUDA {
 public:
     Grid_CUDA(Context& ctx, const std::vector<Vec3>& nodes, const std::vector<StencilType>& stencils,

@@ -54,35 +54,22 @@ int main(int argc, char** argv)
 
     // nodes: Fibonacci spiral under a seeded rotation; stencils from the
     // brute-force or k-d tree generator, or the hash grid (which renumbers
-    // the nodes by cell)
+    // the nodes by cell), as Grid::generateStencils makes them
     std::vector<double> xyz(3 * (size_t)N);
     check(nullptr, rbffd_nodes_fibonacci(N, (uint64_t)num("SEED", 1), xyz.data()), "nodes");
-    std::vector<int> st((size_t)N * n), len(N, n);
     const int gen = (int)num("STENCIL_GEN_TYPE", 2);
-    if (gen == 0 || gen == 1) {
-        check(nullptr,
-              rbffd_stencils_generate(xyz.data(), N, n, gen == 0 ? RBFFD_ST_BRUTE_FORCE : RBFFD_ST_KDTREE, DBL_MAX,
-                                      st.data(), len.data(), nullptr, 0),
-              "stencils");
-    } else if (gen == 2) {
-        std::vector<int> order(N);
-        check(nullptr,
-              rbffd_stencils_hash(xyz.data(), N, n, (int)num("NS_NB_X", 10), (int)num("NS_NB_Y", 10),
-                                  (int)num("NS_NB_Z", 10), nullptr, DBL_MAX, order.data(), st.data(), len.data()),
-              "stencils");
-        std::vector<double> renumbered(3 * (size_t)N);
-        for (int k = 0; k < N; k++)
-            for (int c = 0; c < 3; c++) renumbered[3 * (size_t)k + c] = xyz[3 * (size_t)order[k] + c];
-        xyz.swap(renumbered);
-    } else {
+    if (gen < 0 || gen > 2) {
         std::fprintf(stderr, "STENCIL_GEN_TYPE must be 0, 1 or 2\n");
         return 2;
     }
     std::vector<Vec3> nodes(N);
-    std::vector<StencilType> stencils(N);
+    for (int i = 0; i < N; i++) nodes[i] = Vec3{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+    std::vector<StencilType> stencils = generateStencils(nodes, n, (st_generator_t)gen, DBL_MAX, (int)num("NS_NB_X", 10),
+                                                         (int)num("NS_NB_Y", 10), (int)num("NS_NB_Z", 10));
     for (int i = 0; i < N; i++) {
-        nodes[i] = Vec3{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
-        stencils[i].assign(st.begin() + (size_t)i * n, st.begin() + (size_t)i * n + len[i]);
+        xyz[3 * i] = nodes[i].x;
+        xyz[3 * i + 1] = nodes[i].y;
+        xyz[3 * i + 2] = nodes[i].z;
     }
 
     Context ctx(0);
