@@ -71,6 +71,25 @@ def dist_env():
     return ws, rank, local
 
 
+def replicas_max(x, ws, device="cuda"):
+    """Max over the ranks of one figure per replica (a device time, a host
+    time): the job is as slow as its slowest replica.  One all-reduce of one
+    scalar; every rank calls it at the same point."""
+    if ws == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_rate(units_per_replica, ws, seconds):
+    """Whole-job rate of ws replicas that each processed units_per_replica in
+    at most `seconds` (weak scaling: per-GPU work fixed)."""
+    return float(units_per_replica) * ws / seconds
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -254,13 +273,9 @@ def run_ours(args):
     torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     clk = clocks.stop()
-    tot_ms = float(sum(step_ms))
-    if ws > 1:
-        tt = torch.tensor([tot_ms], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        tot_ms = float(tt.item())
-    node_updates = float(N) * steps * args.steps * ws
-    value = node_updates / (tot_ms * 1e-3)
+    tot_ms = replicas_max(float(sum(step_ms)), ws)
+    node_updates = float(N) * steps * args.steps * ws  # all replicas
+    value = replicas_rate(float(N) * steps * args.steps, ws, tot_ms * 1e-3)
     launches = 4 * steps * args.steps  # one fused stage kernel per RK4 stage
     per_launch_s = tot_ms * 1e-3 / launches
     shape = pde.getShape()  # (lanes per row, threads per block, rows per halo tile or 0), chosen by the autotuner
@@ -295,11 +310,7 @@ def run_ours(args):
         import ctypes
         pde_e2e.ctx.check(pde_e2e.ctx.L.rbffd_pde_get_state(pde_e2e.h, oh.ctypes.data_as(ctypes.POINTER(
             ctypes.c_double))), "get_state")  # device -> host (pinned)
-    e2e_s = time.perf_counter() - t
-    if ws > 1:
-        tt = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = replicas_max(time.perf_counter() - t, ws)
     e2e_value = node_updates / e2e_s
     extras = {}
     if not args.no_extras and rank == 0:
