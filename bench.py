@@ -313,10 +313,10 @@ def run_ours(args):
     e2e_s = replicas_max(time.perf_counter() - t, ws)
     e2e_value = node_updates / e2e_s
     extras = {}
-    if not args.no_extras and rank == 0:
+    if not args.no_extras and ws == 1:  # the other configurations: a one-GPU report
         extras = bench_extras(R, torch, ctx, grid, der, pde, u0, xyz, st, coeffs)
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if ws == 1 and not args.no_cpu_baseline:  # the host-core baseline: rank 0 at N = 1 only
         w64 = der.getWeights(R.LSFC)
         cps, nth, secs = cpu_baseline_heat(st, w64, u0, 1500)
         cpu = {"value": cps, "unit": "node-updates/s", "cores": nth, "kind": "port",
