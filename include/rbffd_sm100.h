@@ -108,6 +108,10 @@ int rbffd_stencils_generate(const double* xyz, int N, int n, int method, double 
  * searches the surrounding cells.  Replaces the same reference call
  * (grid_interface.cpp:688-725, KDTree.h:407-433); n <= 255. */
 int rbffd_stencils_knn_gpu(rbffd_ctx* ctx, const double* xyz, int N, int n, int* st, int* ties);
+/* rbffd_stencils_generate on ctx's device (both generators, max_radius, the
+ * same lists and lengths); n <= 255. */
+int rbffd_stencils_generate_gpu(rbffd_ctx* ctx, const double* xyz, int N, int n, int method, double max_radius,
+                                int* st, int* st_len, int* ties);
 /* Hash-grid stencils as the reference's cosine-bell experiment generates
  * them: Grid::generateStencilsHash (src/grids/grid_interface.cpp:733-966,
  * called at tests/experiments/cosine_bell_on_sphere/main.cpp:197-200).  Not

@@ -95,6 +95,17 @@ def generate_stencils(xyz, n, method=ST_BRUTE_FORCE, max_radius=1.79769313486231
     return st, ln
 
 
+def generate_stencils_gpu(ctx, xyz, n, method=ST_BRUTE_FORCE, max_radius=1.7976931348623157e308):
+    """generate_stencils on ctx's device (identical lists and lengths)."""
+    xyz = _f64(xyz)
+    N = xyz.shape[0]
+    st = np.zeros((N, n), dtype=np.int32)
+    ln = np.zeros(N, dtype=np.int32)
+    ctx.check(ctx.L.rbffd_stencils_generate_gpu(ctx.h, _dp(xyz), N, n, int(method), float(max_radius), _ip(st), _ip(ln),
+                                                None), "rbffd_stencils_generate_gpu")
+    return st, ln
+
+
 def write_weights_file(filename, stencils, w, st_len=None, binary=True):
     """The reference's weight file (Matrix Market, text or binary form) for
     weights w [N][n_pad] of stencils [N][n_pad]; host only."""

@@ -21,9 +21,15 @@
 // (R times the smallest cell edge): as in the host search, a smaller n-th
 // distance proves no unvisited point can enter; otherwise the next shell is
 // added.
+//
+// The same search serves the reference's default brute-force generator
+// (Grid::generateStencilsBruteForce, grid_interface.cpp:637-686): there equal
+// distances fall in decreasing index (DESC), with no centre swap; both cut a
+// list at the first node not closer than max_st_radius.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <vector>
 
@@ -46,14 +52,16 @@ __device__ __forceinline__ int cell_coord(const CellGrid& G, double p, int a)
     return max(0, min(G.dims[a] - 1, c));
 }
 
+template <bool DESC>
 __device__ __forceinline__ bool pair_less(double da, int ia, double db, int ib)
 {
-    return da < db || (da == db && ia < ib);
+    return da < db || (da == db && (DESC ? ia > ib : ia < ib));
 }
 
 // Sort the first cnt (<= KNN_CAP) entries of (d, id) ascending by distance,
-// then index: a bitonic network over the next power of two, the slots beyond
-// cnt padded with (+inf, INT_MAX).  One warp.
+// then index (descending with DESC): a bitonic network over the next power of
+// two, the slots beyond cnt padded with +inf distances.  One warp.
+template <bool DESC>
 __device__ void warp_bitonic_sort(double* d, int* id, int cnt, int lane)
 {
     int S = 32;
@@ -69,7 +77,8 @@ __device__ void warp_bitonic_sort(double* d, int* id, int cnt, int lane)
                 const int p = t ^ j;
                 if (p > t) {
                     const bool up = (t & k) == 0;
-                    const bool sw = up ? pair_less(d[p], id[p], d[t], id[t]) : pair_less(d[t], id[t], d[p], id[p]);
+                    const bool sw = up ? pair_less<DESC>(d[p], id[p], d[t], id[t])
+                                       : pair_less<DESC>(d[t], id[t], d[p], id[p]);
                     if (sw) {
                         const double td = d[t];
                         d[t] = d[p];
@@ -84,9 +93,10 @@ __device__ void warp_bitonic_sort(double* d, int* id, int cnt, int lane)
         }
 }
 
+template <bool DESC>
 __global__ void __launch_bounds__(32 * KNN_WARPS)
-k_knn(const double4* __restrict__ pts, const int* __restrict__ start, CellGrid G, int N, int n,
-      int* __restrict__ st, int* __restrict__ tie)
+k_knn(const double4* __restrict__ pts, const int* __restrict__ start, CellGrid G, int N, int n, double max_radius,
+      int* __restrict__ st, int* __restrict__ st_len, int* __restrict__ tie)
 {
     __shared__ double sd[KNN_WARPS][KNN_CAP];
     __shared__ int si[KNN_WARPS][KNN_CAP];
@@ -114,7 +124,7 @@ k_knn(const double4* __restrict__ pts, const int* __restrict__ start, CellGrid G
                     const int t0 = start[cell], t1 = start[cell + 1];
                     for (int t = t0; t < t1; t += 32) {
                         if (cnt + 32 > KNN_CAP) {  // full: keep the best n + 1
-                            warp_bitonic_sort(d, id, cnt, lane);
+                            warp_bitonic_sort<DESC>(d, id, cnt, lane);
                             cnt = n + 1;
                         }
                         const bool have = t + lane < t1;
@@ -134,24 +144,34 @@ k_knn(const double4* __restrict__ pts, const int* __restrict__ start, CellGrid G
             }
         }
         if (cnt >= n) {
-            warp_bitonic_sort(d, id, cnt, lane);
+            warp_bitonic_sort<DESC>(d, id, cnt, lane);
             cnt = min(cnt, n + 1);
             const double reach = R * G.minh;  // every unvisited point is farther than this
             if (d[n - 1] < reach * reach || R == maxr) break;
         }
     }
-    // d/id hold the sorted best min(cnt, n + 1) candidates
+    // d/id hold the sorted best min(cnt, n + 1) candidates; the list stops at
+    // the first one not closer than max_radius (the rest: the centre)
+    int len = n;
+    if (lane == 0)
+        for (int k = 0; k < n; k++)
+            if (!(sqrt(d[k]) < max_radius)) {
+                len = k;
+                break;
+            }
+    len = __shfl_sync(0xffffffffu, len, 0);
     int* out = st + (size_t)qi * n;
-    for (int k = lane; k < n; k += 32) out[k] = id[k];
+    for (int k = lane; k < n; k += 32) out[k] = k < len ? id[k] : qi;
     __syncwarp();
     if (lane == 0) {
         int first = -1;  // the centre's slot (the lowest if listed twice)
-        for (int k = 0; k < n && first < 0; k++)
+        for (int k = 0; k < len && first < 0; k++)
             if (id[k] == qi) first = k;
-        if (first > 0) {  // a duplicate point at distance 0 sorted ahead of the centre
+        if (!DESC && first > 0) {  // k-d tree lists: a duplicate at distance 0 sorted ahead of the centre
             out[first] = out[0];
             out[0] = qi;
         }
+        if (st_len) st_len[qi] = len;
         int t = 0;
         for (int k = 0; k + 1 < cnt && k < n; k++)
             if (d[k] == d[k + 1]) {
@@ -164,9 +184,12 @@ k_knn(const double4* __restrict__ pts, const int* __restrict__ start, CellGrid G
 
 }  // namespace
 
-extern "C" int rbffd_stencils_knn_gpu(rbffd_ctx* ctx, const double* xyz, int N, int n, int* st, int* ties)
+static int stencils_gpu(rbffd_ctx* ctx, const double* xyz, int N, int n, int method, double max_radius, int* st,
+                        int* st_len, int* ties)
 {
     if (!ctx || !xyz || !st || N <= 0 || n <= 0 || n > N) return RBFFD_ERR_INVALID;
+    if (method != RBFFD_ST_KDTREE && method != RBFFD_ST_BRUTE_FORCE) return RBFFD_ERR_INVALID;
+    if (!(max_radius > 0.0)) return RBFFD_ERR_INVALID;
     if (n > KNN_MAX_N) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "stencil size %d above %d", n, KNN_MAX_N);
     cudaSetDevice(ctx->device);
     // the host search's cell grid (host_inputs.cpp)
@@ -207,37 +230,56 @@ extern "C" int rbffd_stencils_knn_gpu(rbffd_ctx* ctx, const double* xyz, int N, 
         }
     }
     double4* d_pts = nullptr;
-    int *d_start = nullptr, *d_st = nullptr, *d_tie = nullptr;
+    int *d_start = nullptr, *d_st = nullptr, *d_tie = nullptr, *d_len = nullptr;
     const size_t b_pts = (size_t)N * sizeof(double4), b_start = (ncell + 1) * sizeof(int),
                  b_st = (size_t)N * n * sizeof(int), b_tie = (size_t)N * sizeof(int);
     int rc;
     if ((rc = dev_alloc(ctx, (void**)&d_pts, b_pts)) || (rc = dev_alloc(ctx, (void**)&d_start, b_start)) ||
-        (rc = dev_alloc(ctx, (void**)&d_st, b_st)) || (rc = dev_alloc(ctx, (void**)&d_tie, b_tie))) {
+        (rc = dev_alloc(ctx, (void**)&d_st, b_st)) || (rc = dev_alloc(ctx, (void**)&d_tie, b_tie)) ||
+        (st_len && (rc = dev_alloc(ctx, (void**)&d_len, b_tie)))) {
         dev_free(ctx, d_pts, b_pts);
         dev_free(ctx, d_start, b_start);
         dev_free(ctx, d_st, b_st);
+        dev_free(ctx, d_tie, b_tie);
         return rc;
     }
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaMemcpyAsync(d_pts, pts.data(), b_pts, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_start, start.data(), b_start, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
-        k_knn<<<(N + KNN_WARPS - 1) / KNN_WARPS, 32 * KNN_WARPS, 0, s>>>(d_pts, d_start, G, N, n, d_st, d_tie);
+        const unsigned nb = (unsigned)((N + KNN_WARPS - 1) / KNN_WARPS);
+        if (method == RBFFD_ST_BRUTE_FORCE)
+            k_knn<true><<<nb, 32 * KNN_WARPS, 0, s>>>(d_pts, d_start, G, N, n, max_radius, d_st, d_len, d_tie);
+        else
+            k_knn<false><<<nb, 32 * KNN_WARPS, 0, s>>>(d_pts, d_start, G, N, n, max_radius, d_st, d_len, d_tie);
         e = cudaGetLastError();
     }
     std::vector<int> tie(N);
     if (e == cudaSuccess) e = cudaMemcpyAsync(st, d_st, b_st, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(tie.data(), d_tie, b_tie, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && st_len) e = cudaMemcpyAsync(st_len, d_len, b_tie, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     dev_free(ctx, d_pts, b_pts);
     dev_free(ctx, d_start, b_start);
     dev_free(ctx, d_st, b_st);
     dev_free(ctx, d_tie, b_tie);
-    if (e != cudaSuccess) return cuda_error(ctx, e, "rbffd_stencils_knn_gpu");
+    dev_free(ctx, d_len, b_tie);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "stencils on the device");
     if (ties) {
         long long t = 0;
         for (int i = 0; i < N; i++) t += tie[i];
         *ties = (int)t;
     }
     return RBFFD_OK;
+}
+
+extern "C" int rbffd_stencils_knn_gpu(rbffd_ctx* ctx, const double* xyz, int N, int n, int* st, int* ties)
+{
+    return stencils_gpu(ctx, xyz, N, n, RBFFD_ST_KDTREE, DBL_MAX, st, nullptr, ties);
+}
+
+extern "C" int rbffd_stencils_generate_gpu(rbffd_ctx* ctx, const double* xyz, int N, int n, int method,
+                                           double max_radius, int* st, int* st_len, int* ties)
+{
+    return stencils_gpu(ctx, xyz, N, n, method, max_radius, st, st_len, ties);
 }

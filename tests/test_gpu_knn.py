@@ -45,3 +45,26 @@ def test_knn_gpu_rejects_bad_sizes(ctx):
         R.knn_stencils_gpu(ctx, xyz, 256)
     with pytest.raises(R.RbffdError):
         R.knn_stencils_gpu(ctx, xyz, 301)
+
+
+@pytest.mark.parametrize("method", [R.ST_BRUTE_FORCE, R.ST_KDTREE])
+@pytest.mark.parametrize("max_radius", [1.7976931348623157e308, 0.06])
+def test_generators_on_device_equal_host(ctx, method, max_radius):
+    """Both reference generators (brute-force order, k-d tree) with and without
+    the stencil radius: device lists and lengths equal the host's."""
+    xyz = R.fibonacci_nodes(20000, 9)
+    st, ln = R.generate_stencils_gpu(ctx, xyz, 31, method, max_radius)
+    hs, hl = R.generate_stencils(xyz, 31, method, max_radius)
+    assert np.array_equal(ln, hl) and np.array_equal(st, hs)
+    if max_radius < 1.0:
+        assert ln.min() < 31
+
+
+def test_brute_force_ties_on_device(ctx):
+    g = np.arange(8, dtype=np.float64)
+    xyz = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3) * 0.1
+    xyz = np.vstack([xyz, xyz[100:101]])  # and a duplicated point
+    for method in (R.ST_BRUTE_FORCE, R.ST_KDTREE):
+        st, ln = R.generate_stencils_gpu(ctx, xyz, 27, method)
+        hs, hl = R.generate_stencils(xyz, 27, method)
+        assert np.array_equal(st, hs) and np.array_equal(ln, hl)
