@@ -312,9 +312,6 @@ def run_ours(args):
             ctypes.c_double))), "get_state")  # device -> host (pinned)
     e2e_s = replicas_max(time.perf_counter() - t, ws)
     e2e_value = node_updates / e2e_s
-    extras = {}
-    if not args.no_extras and ws == 1:  # the other configurations: a one-GPU report
-        extras = bench_extras(R, torch, ctx, grid, der, pde, u0, xyz, st, coeffs)
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:  # the host-core baseline: rank 0 at N = 1 only
         w64 = der.getWeights(R.LSFC)
@@ -323,6 +320,9 @@ def run_ours(args):
                "sample": "1500 RK4 steps (3 runs of the 500-step workload) on the N=%d, n=%d grid, %.1f s; FP64 "
                          "oracle restatement of advanceRungeKutta4 + applyWeightsForDeriv, OpenMP over rows" % (
                              N, n, secs)}
+    extras = {}
+    if not args.no_extras and ws == 1:  # the other configurations: a one-GPU report
+        extras = bench_extras(R, torch, ctx, grid, der, pde, u0, xyz, st, coeffs)
     if rank == 0:
         line = {
             "metric": "rk4_node_updates_per_s", "value": value, "unit": "node-updates/s", "n_gpus": ws,
@@ -354,6 +354,15 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def guarded(fn, *a, **kw):
+    """Run one extra measurement; an extra that fails is reported as an error
+    entry and the headline line is still printed."""
+    try:
+        return fn(*a, **kw)
+    except Exception as e:  # noqa: BLE001 -- any failure of an extra is data, not a crash
+        return {"error": "%s: %s" % (type(e).__name__, e)}
+
+
 def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
     """FP64 and plain-path variants of the same workload, and errors."""
     W = WORKLOAD
@@ -373,31 +382,38 @@ def bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs):
         ctx.synchronize()
         return N * steps * reps / (e0.elapsed_time(e1) * 1e-3)
 
-    out["serving"] = bench_serving(R, torch, ctx)  # first: the stream's timing is sensitive to host stalls
-    p64 = R.HeatSphere(grid, der, 1.0, dtype=R.F64)
-    out["fp64_fused_graph"] = timed(p64, graph=True, asynchronous=True)
-    pplain = R.HeatSphere(grid, der, 1.0, dtype=R.F64)
-    out["fp64_plain_unfused"] = timed(pplain, reps=1, unfused=True)
-    out["fp32_fused_graph"] = timed(pde32, graph=True, asynchronous=True)
-    out["fused_fp32_over_plain_fp64"] = out["fp32_fused_graph"] / out["fp64_plain_unfused"]
-    # accuracy after the full 500 steps: FP32 vs FP64 (same weights), FP64 vs exact
-    p64.fillInitialConditions(u0)
-    p64.advance(R.RK4, dt, steps, graph=True)
-    pde32.fillInitialConditions(u0)
-    pde32.advance(R.RK4, dt, steps, graph=True)
-    u64, u32 = p64.getLocalSolution(), pde32.getLocalSolution()
-    ex = R.exact_sph_heat(xyz, W["lmax"], coeffs, steps * dt)
-    out["rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64))
-    out["rel_l2_fp64_vs_exact"] = float(np.linalg.norm(u64 - ex) / np.linalg.norm(ex))
-    out["shape_fp32"] = pde32.getShape()
-    p64.close()
-    pplain.close()
-    out["multitracer"] = bench_multitracer(R, torch, ctx)
-    out["weights"] = bench_weights(R, torch, ctx)
-    out["cosine_bell"] = bench_cosine_bell(R, torch, ctx)
-    out["eigenvalues"] = bench_eigenvalues(R, ctx)
-    out["node_order"] = bench_node_order(R, torch, ctx, xyz, st, u0)
-    out["heat_hbm_bound"] = bench_heat_hbm_bound(R, torch, ctx)
+    out["serving"] = guarded(bench_serving, R, torch, ctx)  # first: the stream's timing is sensitive to host stalls
+
+    def heat_variants():
+        res = {}
+        p64 = R.HeatSphere(grid, der, 1.0, dtype=R.F64)
+        res["fp64_fused_graph"] = timed(p64, graph=True, asynchronous=True)
+        pplain = R.HeatSphere(grid, der, 1.0, dtype=R.F64)
+        res["fp64_plain_unfused"] = timed(pplain, reps=1, unfused=True)
+        res["fp32_fused_graph"] = timed(pde32, graph=True, asynchronous=True)
+        res["fused_fp32_over_plain_fp64"] = res["fp32_fused_graph"] / res["fp64_plain_unfused"]
+        # accuracy after the full 500 steps: FP32 vs FP64 (same weights), FP64 vs exact
+        p64.fillInitialConditions(u0)
+        p64.advance(R.RK4, dt, steps, graph=True)
+        pde32.fillInitialConditions(u0)
+        pde32.advance(R.RK4, dt, steps, graph=True)
+        u64, u32 = p64.getLocalSolution(), pde32.getLocalSolution()
+        ex = R.exact_sph_heat(xyz, W["lmax"], coeffs, steps * dt)
+        res["rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64))
+        res["rel_l2_fp64_vs_exact"] = float(np.linalg.norm(u64 - ex) / np.linalg.norm(ex))
+        res["shape_fp32"] = pde32.getShape()
+        p64.close()
+        pplain.close()
+        return res
+
+    hv = guarded(heat_variants)
+    out.update(hv if "error" not in hv else {"heat_variants": hv})
+    out["multitracer"] = guarded(bench_multitracer, R, torch, ctx)
+    out["weights"] = guarded(bench_weights, R, torch, ctx)
+    out["cosine_bell"] = guarded(bench_cosine_bell, R, torch, ctx)
+    out["eigenvalues"] = guarded(bench_eigenvalues, R, ctx)
+    out["node_order"] = guarded(bench_node_order, R, torch, ctx, xyz, st, u0)
+    out["heat_hbm_bound"] = guarded(bench_heat_hbm_bound, R, torch, ctx)
     return out
 
 

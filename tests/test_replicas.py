@@ -62,3 +62,9 @@ def test_reference_arm_runs_on_rank_zero_only():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
                         "--steps", "1", "--warmup", "1"], env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_a_failing_extra_is_reported_not_raised():
+    out = bench.guarded(lambda: 1 / 0)
+    assert out == {"error": "ZeroDivisionError: division by zero"}
+    assert bench.guarded(lambda a, b=0: a + b, 2, b=3) == 5
