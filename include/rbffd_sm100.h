@@ -400,11 +400,15 @@ int rbffd_pde_set_fused_operator(rbffd_pde* pde, int on);
  * different grids, stencil sizes and right-hand sides share the device, and
  * requests on the same grid share one read of its weights and indices.
  * Requests admitted while others run join at the next step boundary.  Each
- * request's sums run over its stencil in order with the arithmetic of
+ * request's sums run over its own stencil with the arithmetic of
  * rbffd_pde_advance with one lane per row, so its result does not depend on
- * what else is in the batch (FP64 results equal the one-lane
- * rbffd_pde_advance result bit for bit; FP32 results equal the FP32
- * one-lane result). */
+ * what else is in the batch.  FP64 requests sum in stencil order and equal
+ * the one-lane rbffd_pde_advance result bit for bit; FP32 requests sum in a
+ * fixed per-grid slot order chosen against shared-memory bank conflicts (and
+ * FP32 advection uses one fused operator), so they are within FP32 rounding
+ * of the one-lane FP32 result.  The server's threads build per-grid tables on
+ * demand: while it holds requests on a grid, the caller uses that grid from
+ * no other thread. */
 typedef struct rbffd_server rbffd_server;
 
 typedef struct rbffd_request {
