@@ -180,6 +180,18 @@ public:
     };
     typedef unsigned int DerTypes;
     enum DataType { FP32 = RBFFD_F32, FP64 = RBFFD_F64 };
+    // RBFFD::WeightType (rbffd.h:89): the direct solve is the one implemented
+    enum WeightType { Direct = 0, ContourSVD = 1 };
+    // derTypeStr of rbffd.cpp:40-58, by DerType bit
+    static const char* derTypeStr(DerType which)
+    {
+        static const char* names[16] = {"x",    "y",        "z",        "lapl",     "r",        "hv",
+                                        "lambda", "theta",  "Lsfc",     "Xsfc",     "Ysfc",     "Zsfc",
+                                        "Alt_Xsfc", "Alt_Ysfc", "Alt_Zsfc", "interp"};
+        for (int b = 0; b < 16; b++)
+            if ((unsigned)which == (1u << b)) return names[b];
+        return "unknown";
+    }
 
     // RBFFD(DerTypes typesToCompute, Grid* grid, int dim_num, int rank=0) (rbffd.h:192)
     RBFFD_CUDA(DerTypes typesToCompute, Grid_CUDA* grid, int dim_num, int rank = 0)
@@ -249,8 +261,16 @@ public:
         computedTypes |= X | Y | Z | alt;
         return true;
     }
+    // rbffd.h:247-253.  Condition numbers are not computed on the device; the
+    // flag is kept so reference drivers run unchanged.
+    void setComputeConditionNumber(bool tf) { computeCondNums = tf; }
+    bool getComputeConditionNumber() const { return computeCondNums; }
+    void setWeightType(WeightType type) { weightMethod = type; }
     void computeAllWeightsForAllStencils()
     {
+        if (weightMethod != Direct)
+            check(nullptr, RBFFD_ERR_UNSUPPORTED,
+                  "computeAllWeightsForAllStencils: ContourSVD weights are not built (WeightType Direct only)");
         adjustForSFCTypes();
         rbffd_weight_params p;
         p.der_types = computedTypes;
@@ -305,6 +325,41 @@ public:
               "loadFromFile");
         setWeights(which, w);
         return 0;
+    }
+    // RBFFD::writeAllWeightsToFile / loadAllWeightsFromFile (rbffd.cpp:1212-1250):
+    // every computed type, one file each named base_<derTypeStr>.mtx (ASCII)
+    // or .bmtx (binary).  The reference derives base from its grid and
+    // parameters (getFileDetailString); here the caller names it.  load
+    // returns the number of types whose file could not be read, as the
+    // reference sums loadFromFile's error codes, and keeps the weights it
+    // could read.
+    std::string getFilename(DerType which, const std::string& base = "weights_rbffd") const
+    {
+        return base + "_" + derTypeStr(which) + (asciiWeights ? ".mtx" : ".bmtx");
+    }
+    void writeAllWeightsToFile(const std::string& base = "weights_rbffd")
+    {
+        for (int b = 0; b < 16; b++)
+            if (computedTypes & (1u << b)) writeToFile((DerType)(1u << b), getFilename((DerType)(1u << b), base));
+    }
+    int loadAllWeightsFromFile(const std::string& base = "weights_rbffd")
+    {
+        int err = 0;
+        for (int b = 0; b < 16; b++) {
+            if (!(computedTypes & (1u << b))) continue;
+            const DerType t = (DerType)(1u << b);
+            std::vector<double> w((size_t)grid_ref.getStencilsSize() * grid_ref.getMaxStencilSize());
+            const int rc = rbffd_weights_file_read(getFilename(t, base).c_str(), asciiWeights ? 0 : 1,
+                                                   (int)grid_ref.getStencilsSize(), (int)grid_ref.getMaxStencilSize(),
+                                                   grid_ref.paddedStencils().data(), grid_ref.stencilLengths().data(),
+                                                   w.data());
+            if (rc) {
+                err += 1;
+                continue;
+            }
+            setWeights(t, w);
+        }
+        return err;
     }
 
     // -- eigenvalue stability check (rbffd.h:91-100,281,412-417; rbffd.cpp:703-873) --
@@ -392,6 +447,8 @@ protected:
     std::vector<int> deg_rows;
     int dtype = RBFFD_F64;
     int asciiWeights = 0;  // binary weight files unless setAsciiWeights(1)
+    bool computeCondNums = false;
+    WeightType weightMethod = Direct;
     EigenvalueOutput cachedEigenvalues = {};
     bool eigenvalues_computed = false;
 };
