@@ -101,6 +101,13 @@ int rbffd_stencils_knn(const double* xyz, int N, int n, int* st, int* ties, int 
  * cell grid, not O(N^2).  RBFFD_ERR_INVALID for max_radius <= 0 (the
  * reference's stencils would all be empty). */
 enum { RBFFD_ST_BRUTE_FORCE = 0, RBFFD_ST_KDTREE = 1 };
+/* RBFFD::setVariableEpsilon (src/rbffd/rbffd.cpp:1378-1420, Sarler 2006
+ * form): eps[st[i][0]] = 1 / (alpha * r_max(i)), r_max the distance from the
+ * centre to the stencil's last node.  st_len NULL: every stencil n_pad long.
+ * eps[N] entries of nodes that are no stencil's centre are left as given.
+ * Host only. */
+int rbffd_variable_epsilon(int N, const double* xyz, int n_pad, const int* st, const int* st_len, double alpha,
+                           double* eps);
 int rbffd_stencils_generate(const double* xyz, int N, int n, int method, double max_radius, int* st, int* st_len,
                             int* ties, int nthreads);
 /* The same stencils (identical lists and tie count) computed on ctx's device:

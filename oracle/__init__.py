@@ -374,6 +374,20 @@ def ref_stencils_generate(xyz, n, method, max_radius=1.7976931348623157e308):
     return st, ln
 
 
+def variable_epsilon(xyz, st, st_len, alpha, eps):
+    """RBFFD::setVariableEpsilon, VARIABLE_EPS_TYPE 1 (src/rbffd/rbffd.cpp:1389,
+    1411-1416) with Grid::computeStencilRadii's max radius
+    (src/grids/grid_interface.cpp:556-557): eps[centre] = 1 / (alpha * |x_last
+    - x_centre|), the magnitude summed x, y, z left to right."""
+    eps = np.array(eps, dtype=np.float64, copy=True)
+    for i in range(st.shape[0]):
+        ln = st.shape[1] if st_len is None else int(st_len[i])
+        c, last = int(st[i, 0]), int(st[i, ln - 1])
+        d = xyz[last] - xyz[c]
+        eps[c] = 1.0 / (alpha * np.sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]))
+    return eps
+
+
 def alt_sfc(xyz, wx, wy, wz):
     """ALT_XSFC, ALT_YSFC, ALT_ZSFC from the X, Y, Z weights: the projection
     (I - x x^T) at each stencil centre, left to right without fused

@@ -58,6 +58,7 @@ PROTOTYPES = {
     "rbffd_nodes_fibonacci": (c_int, [c_int, c_uint64, dp]),
     "rbffd_stencils_knn": (c_int, [dp, c_int, c_int, ip, ip, c_int]),
     "rbffd_stencils_generate": (c_int, [dp, c_int, c_int, c_int, c_double, ip, ip, ip, c_int]),
+    "rbffd_variable_epsilon": (c_int, [c_int, dp, c_int, ip, ip, c_double, dp]),
     "rbffd_stencils_generate_gpu": (c_int, [c_void_p, dp, c_int, c_int, c_int, c_double, ip, ip, ip]),
     "rbffd_stencils_knn_gpu": (c_int, [c_void_p, dp, c_int, c_int, ip, ip]),
     "rbffd_exact_cosine_bell": (c_int, [c_int, dp, c_double, dp]),

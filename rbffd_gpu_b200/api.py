@@ -106,6 +106,20 @@ def generate_stencils_gpu(ctx, xyz, n, method=ST_BRUTE_FORCE, max_radius=1.79769
     return st, ln
 
 
+def variable_epsilon(xyz, stencils, st_len, alpha, eps=None):
+    """RBFFD::setVariableEpsilon's per-stencil eps (rbffd.cpp:1378-1420):
+    eps[centre] = 1 / (alpha * distance to the stencil's last node); entries
+    of eps (default ones) at nodes that centre no stencil are kept.  Host only."""
+    xyz, st = _f64(xyz), _i32(stencils)
+    N, n_pad = st.shape
+    out = np.ones(len(xyz)) if eps is None else np.array(eps, dtype=np.float64, copy=True)
+    rc = _lib.load().rbffd_variable_epsilon(N, _dp(xyz), n_pad, _ip(st), None if st_len is None else _ip(_i32(st_len)),
+                                            float(alpha), _dp(out))
+    if rc:
+        raise RbffdError(rc, "rbffd_variable_epsilon")
+    return out
+
+
 def write_weights_file(filename, stencils, w, st_len=None, binary=True):
     """The reference's weight file (Matrix Market, text or binary form) for
     weights w [N][n_pad] of stencils [N][n_pad]; host only."""
@@ -384,6 +398,13 @@ class RBFFD:
 
     def setEpsilonByParameters(self, c1, c2):
         self.setEpsilon(c1 * np.sqrt(self.grid.getGlobalNodeListSize()) - c2)
+
+    def setVariableEpsilon(self, alpha=1.0, beta=1.0):
+        """rbffd.cpp:1378-1420 (Sarler 2006): eps at each centre =
+        1 / (alpha * distance to the stencil's last node); beta is unused
+        there, as in the reference."""
+        g = self.grid
+        self.var_epsilon = variable_epsilon(g.nodes, g.stencils, g.st_len, alpha, self.var_epsilon)
 
     def setPolynomialDegree(self, deg, deg_per_row=None):
         """Beyond the reference (which fixes np = 1): -1 none, 0 constant, 1..4."""

@@ -229,6 +229,17 @@ public:
         setEpsilon(c1 * std::sqrt((double)grid_ref.getGlobalNodeListSize()) - c2);
     }
     // the reference's per-stencil-size table for the cosine bell (rbffd.h:300-345)
+    // rbffd.h:376-380, rbffd.cpp:1378-1420 (Sarler 2006): eps at each centre =
+    // 1 / (alpha * distance to the stencil's last node); beta unused there too
+    void setVariableEpsilon(double alpha = 1.0, double beta = 1.0)
+    {
+        (void)beta;
+        check(nullptr,
+              rbffd_variable_epsilon((int)grid_ref.getStencilsSize(), grid_ref.coordinates().data(),
+                                     (int)grid_ref.getMaxStencilSize(), grid_ref.paddedStencils().data(),
+                                     grid_ref.stencilLengths().data(), alpha, var_epsilon.data()),
+              "setVariableEpsilon");
+    }
     void setEpsilonByStencilSize()
     {
         double c1, c2;

@@ -661,3 +661,25 @@ extern "C" int rbffd_sol_norms(const double* sol, const double* exact, int n, do
     out[5] = rel(li, lid);
     return RBFFD_OK;
 }
+
+// RBFFD::setVariableEpsilon (src/rbffd/rbffd.cpp:1378-1420, its
+// VARIABLE_EPS_TYPE 1, Sarler 2006): eps at each stencil's centre =
+// 1 / (alpha * r_max), r_max the distance from the centre to the stencil's
+// last node (Grid::computeStencilRadii, grid_interface.cpp:556-557), as
+// Vec3d::magnitude of the difference: sqrt(dx*dx + dy*dy + dz*dz).
+extern "C" int rbffd_variable_epsilon(int N, const double* xyz, int n_pad, const int* st, const int* st_len,
+                                      double alpha, double* eps)
+{
+    if (N <= 0 || !xyz || n_pad <= 0 || !st || !eps || alpha == 0.0) return RBFFD_ERR_INVALID;
+    for (int i = 0; i < N; i++) {
+        const int len = st_len ? st_len[i] : n_pad;
+        if (len < 1 || len > n_pad) return RBFFD_ERR_INVALID;
+        const int c = st[(size_t)i * n_pad], last = st[(size_t)i * n_pad + len - 1];
+        if (c < 0 || c >= N || last < 0 || last >= N) return RBFFD_ERR_INVALID;
+        const double dx = xyz[3 * (size_t)last] - xyz[3 * (size_t)c];
+        const double dy = xyz[3 * (size_t)last + 1] - xyz[3 * (size_t)c + 1];
+        const double dz = xyz[3 * (size_t)last + 2] - xyz[3 * (size_t)c + 2];
+        eps[c] = 1. / (alpha * std::sqrt(dx * dx + dy * dy + dz * dz));
+    }
+    return RBFFD_OK;
+}

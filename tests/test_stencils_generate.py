@@ -76,3 +76,18 @@ def test_duplicate_point_order():
     assert bf[5, 0] == 300 and bf[5, 1] == 5
     kd, _ = R.generate_stencils(xyz, 12, R.ST_KDTREE)
     assert kd[5, 0] == 5 and kd[300, 0] == 300
+
+
+def test_variable_epsilon_equals_oracle():
+    """RBFFD::setVariableEpsilon (Sarler 2006 form) on ragged stencils:
+    1 / (alpha * distance to the last node), bit for bit with the oracle."""
+    xyz = R.fibonacci_nodes(1200, 4)
+    st, ln = R.generate_stencils(xyz, 31, R.ST_KDTREE, 0.11)
+    for alpha in (1.0, 0.37):
+        got = R.variable_epsilon(xyz, st, ln, alpha)
+        assert np.array_equal(got, O.variable_epsilon(xyz, st, ln, alpha, np.ones(len(xyz))))
+    full = R.knn_stencils(xyz, 17)
+    assert np.array_equal(R.variable_epsilon(xyz, full, None, 2.0),
+                          O.variable_epsilon(xyz, full, None, 2.0, np.ones(len(xyz))))
+    with pytest.raises(R.RbffdError):
+        R.variable_epsilon(xyz, st, ln, 0.0)
