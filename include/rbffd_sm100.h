@@ -335,7 +335,9 @@ enum rbffd_advance_flags {
 };
 /* nsteps classical RK4 steps of size dt: TimeDependentPDE::advance(RK4, dt)
  * (src/pdes/time_dependent_pde.cpp:53-73,172-304), nsteps times.
- * scheme must be 2 (TimeDependentPDE::RK4). */
+ * scheme must be 2 (TimeDependentPDE::RK4); EULER (0) and MIDPOINT (1) return
+ * RBFFD_ERR_UNSUPPORTED, as the reference's GPU class compiles them out and
+ * exits on them (TimeDependentPDE_CL::advance, time_dependent_pde_cl.cpp:350-375). */
 int rbffd_pde_advance(rbffd_pde* pde, int scheme, double dt, int nsteps, int flags);
 /* Heat-equation RK4 that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that cannot let a library allocate on the
