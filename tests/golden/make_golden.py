@@ -1,0 +1,72 @@
+"""Writes tests/golden/reference_outputs.npz: outputs of the reference's own
+code, compiled from its sources into oracle/_ref/ (oracle/build.py), on small
+seeded inputs.  The tests in tests/test_golden.py check the oracle and the
+product's host functions against these arrays without needing the reference
+tree.  Run from the repository root where the reference tree is present:
+
+    python tests/golden/make_golden.py
+
+Contents (all from the reference's code):
+  rbf_*      RBF_Gaussian eval/derivatives/Laplacians/hyperviscosity
+             (src/rbffd/rbfs/rbf_gaussian.h) at seeded (which, eps, dim, d, k)
+  sph_*      cart2sph (src/utils/geom/cart2sph.cpp) of 200 Fibonacci nodes
+  kd_*       KDTree::k_closest_points lists (external/kdtree/KDTree.h), 600 nodes, n = 17
+  bf_*       Grid::generateStencilsBruteForce, 400 nodes, n = 15, with max_st_radius 0.2
+  hash_*     Grid::generateStencilsHash, 600 nodes, n = 20, 8x12x6 overlay (order, stencils, lengths)
+  norms_*    norms.cpp l1/l2/linf with calcSolNorms' relative rule on seeded vectors
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+import oracle as O  # noqa: E402
+import rbffd_gpu_b200 as R  # noqa: E402
+
+
+def main():
+    L = O.ref_lib("ref_rbf")
+    if L is None or O.ref_lib("ref_kdtree") is None or O.ref_lib("ref_grid") is None or \
+            O.ref_lib("ref_norms") is None:
+        sys.exit("the reference libraries are not built (python -c 'import oracle.build as b; b.build()')")
+    out = {}
+    rng = np.random.default_rng(2024)
+    args, vals = [], []
+    for which in range(9):
+        for _ in range(40):
+            d = rng.normal(size=3) * rng.choice([1e-3, 1e-1, 0.5])
+            eps = rng.uniform(0.5, 9.0)
+            dim = int(rng.integers(1, 4))
+            k = int(rng.integers(0, 9))
+            args.append([which, eps, dim, d[0], d[1], d[2], k])
+            vals.append(L.ref_rbf(which, eps, dim, *d, k))
+    out["rbf_args"] = np.array(args)
+    out["rbf_vals"] = np.array(vals)
+    xyz = R.fibonacci_nodes(200, 11)
+    sph = []
+    for p in xyz:
+        t, ph, r = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        L.ref_cart2sph(*p, ctypes.byref(t), ctypes.byref(ph), ctypes.byref(r))
+        sph.append([t.value, ph.value])
+    out["sph_xyz"], out["sph_vals"] = xyz, np.array(sph)
+    xyz = R.fibonacci_nodes(600, 12)
+    out["kd_xyz"], out["kd_st"] = xyz, O.ref_knn(xyz, 17)[0]
+    xyz = R.fibonacci_nodes(400, 13)
+    st, ln = O.ref_stencils_generate(xyz, 15, 0, 0.2)
+    out["bf_xyz"], out["bf_st"], out["bf_len"] = xyz, st, ln
+    xyz = R.fibonacci_nodes(600, 14)
+    order, st, ln = O.ref_stencils_hash(xyz, 20, (8, 12, 6))
+    out["hash_xyz"], out["hash_order"], out["hash_st"], out["hash_len"] = xyz, order, st, ln
+    sol = rng.normal(size=(4, 300))
+    exact = sol + 1e-3 * rng.normal(size=(4, 300))
+    exact[3] = 0.0  # the calcSolNorms rule for exact norms below 1e-10
+    out["norms_sol"], out["norms_exact"] = sol, exact
+    out["norms_vals"] = np.array([O.ref_sol_norms(sol[i], exact[i]) for i in range(4)])
+    np.savez_compressed(os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_outputs.npz"), **out)
+
+
+if __name__ == "__main__":
+    main()
