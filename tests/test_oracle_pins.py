@@ -180,3 +180,25 @@ def test_heat_oracle_tracks_exact_spectral_decay():
     u = O.rk4_heat(st, None, W[O.LSFC], u0, dt, steps)
     ex = R.exact_sph_heat(xyz, lmax, c, dt * steps)
     assert rel_l2(u, ex) < 1e-4
+
+
+@pytest.mark.parametrize("deg", [0, 2])
+def test_cosine_bell_returns_after_one_revolution(deg):
+    """The cosine-bell experiment's known answer (exact_advection.h:37-53;
+    main.cpp:517-532): after one revolution (1000 RK4 steps of 1036.8 s) the
+    solution is the initial bell again, within the experiment's
+    MAX_GLOBAL_REL_ERROR = 1.0 (test.conf:50).  Here on 4096 seeded nodes,
+    n = 31, eps = 6, hyperviscosity -1e-3 N^-4 Delta^4, with the reference's
+    constant basis (deg 0) and degree 2; the error is about 8e-2."""
+    from tests.helpers import cosine_bell_setup
+    N, n = 4096, 31
+    xyz, st = sphere_problem(N, n, 1)
+    p = cosine_bell_setup()
+    types = O.LAMBDA | O.THETA | O.HV
+    W = O.weights(xyz, st, None, 6.0, types, dim=2, poly_deg=deg, hv_k=4, hv_scale=-1e-3 * N ** -4.0)
+    cu, cv = O.cosine_bell_coeffs(xyz, a=p["a"], alpha=p["alpha"], u0=p["u0"])
+    h0 = R.exact_cosine_bell(xyz)
+    h = O.rk4_advect(st, None, W[O.LAMBDA], W[O.THETA], W[O.HV], cu, cv, h0, p["dt"], 1000)
+    err = rel_l2(h, h0)
+    assert err < 1.0  # the reference experiment's threshold
+    assert err < 0.1
