@@ -202,3 +202,17 @@ def test_cosine_bell_returns_after_one_revolution(deg):
     err = rel_l2(h, h0)
     assert err < 1.0  # the reference experiment's threshold
     assert err < 0.1
+
+
+def test_vortex_rollup_tracks_exact_solution():
+    """The vortex roll-up experiment's known answer (exact_rollup.h:25-50):
+    the oracle's RK4 of f = -w(theta) D_lambda h + HV h on 4096 seeded nodes
+    (n = 31, eps = 6, dt = 0.01, 50 steps) stays close to the exact roll-up."""
+    N, n = 4096, 31
+    xyz, st = sphere_problem(N, n, 4)
+    types = O.LAMBDA | O.HV
+    W = O.weights(xyz, st, None, 6.0, types, dim=2, poly_deg=2, hv_k=4, hv_scale=-1e-3 * N ** -4.0)
+    h0 = O.exact_vortex_rollup(xyz, 0.0)
+    w = O.vortex_rollup_w(xyz)
+    h = O.rk4_advect(st, None, W[O.LAMBDA], W[O.LAMBDA], W[O.HV], w, np.zeros(N), h0, 0.01, 50)
+    assert rel_l2(h, O.exact_vortex_rollup(xyz, 0.5)) < 0.1
