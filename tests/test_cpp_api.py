@@ -134,3 +134,36 @@ def test_vortex_rollup_driver_matches_python_path(tmp_path, gen):
     ctx.close()
     assert rel_l2(h_cpp, h_py) < 1e-12  # same kernels; the autotuned lane split may differ per process
     assert rel_l2(h_cpp, R.exact_vortex_rollup(xyz, steps * dt)) < 0.1
+
+
+def test_reference_driver_calls_compile(tmp_path):
+    """The reference drivers' calls on the C++ classes compile against the
+    header (-Wall -Werror): stencil generation, the shape-parameter setters,
+    weight type, condition-number flag and the all-types weight files.  The
+    program only builds the calls; run without arguments it touches no GPU."""
+    src = tmp_path / "calls.cpp"
+    src.write_text(
+        '#include "rbffd_cuda.hpp"\n'
+        "using namespace rbffd_sm100;\n"
+        "static int drive() {\n"
+        "  std::vector<Vec3> nodes(100, Vec3{1.0, 0.0, 0.0});\n"
+        "  std::vector<StencilType> st = generateStencils(nodes, 9, ST_KDTREE, 0.5);\n"
+        "  Context ctx(0);\n"
+        "  Grid_CUDA grid(ctx, nodes, st);\n"
+        "  RBFFD_CUDA der(RBFFD_CUDA::LAMBDA | RBFFD_CUDA::THETA | RBFFD_CUDA::HV, &grid, 2);\n"
+        "  der.setWeightType(RBFFD_CUDA::Direct);\n"
+        "  der.setComputeConditionNumber(true);\n"
+        "  der.setVariableEpsilon(0.5);\n"
+        "  der.setEpsilonByParameters(0.035, 0.1);\n"
+        "  if (der.loadAllWeightsFromFile(\"w\")) der.computeAllWeightsForAllStencils();\n"
+        "  der.writeAllWeightsToFile(\"w\");\n"
+        "  return (int)der.getFilename(RBFFD_CUDA::LAMBDA, \"w\").size();\n"
+        "}\n"
+        "int main(int argc, char**) { return argc > 99 ? drive() : 0; }\n")
+    exe = tmp_path / "calls"
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I" + os.path.join(ROOT, "include"),
+                        "-I" + HEADER_DIR, str(src), "-L" + os.path.dirname(_lib.LIB_PATH), "-lrbffd_sm100",
+                        "-Wl,-rpath," + os.path.dirname(_lib.LIB_PATH), "-o", str(exe)], capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
+    assert subprocess.run([str(exe)]).returncode == 0
