@@ -91,3 +91,23 @@ def test_variable_epsilon_equals_oracle():
                           O.variable_epsilon(xyz, full, None, 2.0, np.ones(len(xyz))))
     with pytest.raises(R.RbffdError):
         R.variable_epsilon(xyz, st, ln, 0.0)
+
+
+def test_generator_argument_checks():
+    """Invalid calls return RBFFD_ERR_INVALID (the C ABI never exits)."""
+    from rbffd_gpu_b200 import _lib
+    L = _lib.load()
+    xyz = R.fibonacci_nodes(50, 1)
+    st = np.zeros((50, 5), dtype=np.int32)
+    ln = np.zeros(50, dtype=np.int32)
+    dp = xyz.ctypes.data_as(_lib.dp)
+    ip, lp = st.ctypes.data_as(_lib.ip), ln.ctypes.data_as(_lib.ip)
+    assert L.rbffd_stencils_generate(dp, 50, 5, 7, 1.0, ip, lp, None, 0) == -1      # unknown method
+    assert L.rbffd_stencils_generate(dp, 50, 5, 0, -1.0, ip, lp, None, 0) == -1     # radius <= 0
+    assert L.rbffd_stencils_generate(dp, 50, 51, 0, 1.0, ip, lp, None, 0) == -1     # n > N
+    assert L.rbffd_stencils_generate(None, 50, 5, 0, 1.0, ip, lp, None, 0) == -1    # no nodes
+    assert L.rbffd_stencils_generate(dp, 50, 5, 0, 1.0, ip, None, None, 0) == 0     # lengths optional
+    bad = np.full((50, 5), 60, dtype=np.int32)
+    eps = np.ones(50)
+    assert L.rbffd_variable_epsilon(50, dp, 5, bad.ctypes.data_as(_lib.ip), None, 1.0,
+                                    eps.ctypes.data_as(_lib.dp)) == -1              # index out of range
