@@ -9,7 +9,7 @@ import pytest
 import oracle as O
 import rbffd_gpu_b200 as R
 
-pytestmark = pytest.mark.skipif(O.ref_lib("ref_grid") is None, reason="reference sources not built")
+needs_ref = pytest.mark.skipif(O.ref_lib("ref_grid") is None, reason="reference sources not built")
 
 
 def _compare(xyz, n, method, max_radius=1.7976931348623157e308):
@@ -22,6 +22,7 @@ def _compare(xyz, n, method, max_radius=1.7976931348623157e308):
     return st, ln
 
 
+@needs_ref
 @pytest.mark.parametrize("method", [R.ST_BRUTE_FORCE, R.ST_KDTREE])
 @pytest.mark.parametrize("N,n,seed", [(800, 17, 1), (1500, 31, 2), (600, 50, 3)])
 def test_sphere_nodes(method, N, n, seed):
@@ -30,6 +31,7 @@ def test_sphere_nodes(method, N, n, seed):
     assert (ln == n).all() and (st[:, 0] == np.arange(N)).all()
 
 
+@needs_ref
 @pytest.mark.parametrize("method", [R.ST_BRUTE_FORCE, R.ST_KDTREE])
 def test_radius_trimming(method):
     xyz = R.fibonacci_nodes(1000, 5)
@@ -39,6 +41,7 @@ def test_radius_trimming(method):
     assert ln.min() < 31  # the largest radius still trims some stencils
 
 
+@needs_ref
 def test_brute_force_ties_in_decreasing_index():
     """A cubic lattice: every node has many neighbours at equal distance. The
     brute-force generator keeps the higher node numbers first among equal
@@ -66,6 +69,7 @@ def test_invalid_radius():
         R.generate_stencils(R.fibonacci_nodes(100, 1), 9, R.ST_BRUTE_FORCE, 0.0)
 
 
+@needs_ref
 def test_duplicate_point_order():
     """A duplicated node: the brute-force generator puts the copy with the
     higher number first, ahead of the centre, as the reference does; the k-d
