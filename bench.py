@@ -10,9 +10,14 @@ n = 50, RBFFD::setEpsilonByStencilSize, gives eps h = 0.155 where the systems
 reach kappa ~ 1e15 and rounding in the weights seeds a growing mode within
 500 steps), initial condition a sum of spherical
 harmonics of degree <= 20 with N(0,1) seeded coefficients, 500 RK4 steps of
-dt = 1e-6 per benchmark step, FP32 state/weights/accumulation (FP64 reported
-beside it).  Metric: RK4 node-updates/s (one node advanced one full RK4
-step).
+dt = 1e-6 per benchmark step.  The headline is FP64 state, weights and
+accumulation -- the reference's arithmetic -- with FP32 reported beside it
+under "fp32" and both errors against the FP64 oracle under "accuracy".
+Metric: RK4 node-updates/s (one node advanced one full RK4 step).
+
+--impl reference times the reference's CPU implementation of the path (the
+FP64 oracle restatement, all host threads) on the same workload, built
+without the product library, and prints the same config.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -47,6 +52,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="setup plus 25 un-graphed RK4 steps with the autotuned kernel shape, for ncu captures")
+    ap.add_argument("--profile-dtype", default="f64", choices=["f64", "f32"],
+                    help="arithmetic of the --profile / --profile-tile run (default: FP64, the headline's)")
     ap.add_argument("--profile-tile", type=int, default=0, metavar="ROWS",
                     help="as --profile, with the halo-tiled stage kernel of ROWS rows and one lane per row forced "
                          "(no autotuning)")
@@ -159,8 +166,32 @@ def setup_problem():
     return xyz, st, u0, eps, c
 
 
+def setup_problem_reference():
+    """The same grid and initial state built without the product library:
+    the oracle's restatement of the seeded Fibonacci nodes (equal bit for bit
+    to the product's), the reference's own k-d tree for the stencils (equal to
+    the product's lists), the oracle's spherical-harmonic sum for u0."""
+    import oracle as O
+    W = WORKLOAD
+    xyz = O.fibonacci_nodes(W["N"], W["seed"])
+    st, st_src = O.knn_for_baseline(xyz, W["n"])
+    c = np.random.default_rng(W["seed"]).standard_normal((W["lmax"] + 1) ** 2)
+    u0 = O.sph_heat(xyz, W["lmax"], c, 0.0)
+    return xyz, st, u0, heat_eps(W["N"]), c, st_src
+
+
 def heat_eps(N):
     return 0.25 / np.sqrt(4.0 * np.pi / N)
+
+
+def workload_config(ws):
+    """The workload as both arms print it (identical dicts)."""
+    W = WORKLOAD
+    return {"workload": W["name"], "nodes": W["N"], "stencil": W["n"], "poly_deg": W["deg"], "operator": "LSFC",
+            "rk4_steps": W["steps"], "dt": W["dt"], "eps": heat_eps(W["N"]), "ic_lmax": W["lmax"], "seed": W["seed"],
+            "arithmetic": "FP64 weights, state and accumulation",
+            "parallelism": "replicas" if ws > 1 else "single",
+            "l2_flush": "GPU arm: a 256 MiB buffer is written between timed steps; CPU arm: none (host caches)"}
 
 
 def stage_bytes(n, wbytes, sbytes, ibytes=4):
@@ -171,50 +202,134 @@ def stage_bytes(n, wbytes, sbytes, ibytes=4):
     return n * wbytes + ibytes * n + 4 * sbytes
 
 
-def cpu_baseline_heat(st, w_lsfc, u0, steps):
+def cpu_oracle_heat(st, w_lsfc, u0, runs):
+    """The FP64 oracle's RK4 over the whole 500-step workload, `runs` times
+    from u0, on all host threads: (node-updates/s, threads, seconds, final state)."""
     import oracle as O
     nth = O.max_threads()
     t = time.perf_counter()
-    O.rk4_heat(st, None, w_lsfc, u0, WORKLOAD["dt"], steps, nthreads=nth)
+    for _ in range(runs):
+        u = O.rk4_heat(st, None, w_lsfc, u0, WORKLOAD["dt"], WORKLOAD["steps"], nthreads=nth)
     dt = time.perf_counter() - t
-    return WORKLOAD["N"] * steps / dt, nth, dt
+    return WORKLOAD["N"] * WORKLOAD["steps"] * runs / dt, nth, dt, u
 
 
 def run_reference(args):
+    """The reference's CPU implementation of the path on the host cores: the
+    FP64 oracle restatement of RBFFD::computeAllWeightsForAllStencils (setup,
+    untimed), TimeDependentPDE::advanceRungeKutta4 and applyWeightsForDeriv,
+    OpenMP over stencil rows.  Each benchmark step is the whole workload (500
+    RK4 steps from u0).  Nothing here loads the product library."""
     ws, rank, _ = dist_env()
     if ws > 1 and rank != 0:
         return
     import oracle as O
-    xyz, st, u0, eps, _ = setup_problem()
+    xyz, st, u0, eps, _, st_src = setup_problem_reference()
     nth = O.max_threads()
     t0 = time.perf_counter()
     W = O.weights(xyz, st, None, eps, O.LSFC, dim=2, poly_deg=WORKLOAD["deg"], nthreads=nth)[O.LSFC]
     t_w = time.perf_counter() - t0
-    sample = 10  # RK4 steps per benchmark step: a bounded sample of the 500-step workload
-    u = u0
+    steps, dt = WORKLOAD["steps"], WORKLOAD["dt"]
     for _ in range(args.warmup):
-        O.rk4_heat(st, None, W, u, WORKLOAD["dt"], 1, nthreads=nth)
+        O.rk4_heat(st, None, W, u0, dt, steps, nthreads=nth)
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
-        O.rk4_heat(st, None, W, u, WORKLOAD["dt"], sample, nthreads=nth)
+        O.rk4_heat(st, None, W, u0, dt, steps, nthreads=nth)
         times.append(time.perf_counter() - t)
     tot = sum(times)
-    value = WORKLOAD["N"] * sample * args.steps / tot
+    value = WORKLOAD["N"] * steps * args.steps / tot
     line = {
         "impl": "reference", "metric": "rk4_node_updates_per_s", "value": value, "unit": "node-updates/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD["name"], "nodes": WORKLOAD["N"], "stencil": WORKLOAD["n"],
-                   "poly_deg": WORKLOAD["deg"], "l2_flush": "working set re-read from host memory"},
+        "config": workload_config(ws),
         "cpu_baseline": {"value": value, "unit": "node-updates/s", "cores": nth, "kind": "port",
-                         "sample": "%d of the 500 RK4 steps per benchmark step on the full N=%d grid; FP64 oracle "
-                                   "restatement of TimeDependentPDE::advanceRungeKutta4 + applyWeightsForDeriv, "
-                                   "OpenMP over stencil rows (weights setup %.1f s, untimed)" % (
-                                       sample, WORKLOAD["N"], t_w)},
+                         "sample": "the whole workload per benchmark step (%d RK4 steps from u0, N=%d, n=%d); FP64 "
+                                   "oracle restatement of TimeDependentPDE::advanceRungeKutta4 + applyWeightsForDeriv, "
+                                   "OpenMP over stencil rows; grid from the oracle's nodes and the %s, weights by the "
+                                   "oracle (setup %.1f s, untimed)" % (steps, WORKLOAD["N"], WORKLOAD["n"], st_src,
+                                                                        t_w)},
         "e2e": {"value": value, "unit": "node-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def timed_heat_steps(torch, ctx, pde, nsteps, flush, ws, clocks=None):
+    """K benchmark steps of the whole 500-step workload on `pde` (inputs
+    resident, graphed RK4 steps), each bracketed by CUDA events on the
+    library's stream with the L2 flush written before it; a barrier and a
+    synchronize on both sides.  Returns the max over ranks of the summed
+    device time (ms) and the per-step times."""
+    import rbffd_gpu_b200 as R
+    W = WORKLOAD
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    if clocks is not None:
+        clocks.start()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    evs = []
+    with torch.cuda.stream(stream):
+        for _ in range(nsteps):
+            flush.fill_(1.0)  # write a buffer larger than L2 between timed steps
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pde.advance(R.RK4, W["dt"], W["steps"], graph=True, asynchronous=True)
+            e1.record(stream)
+            evs.append((e0, e1))
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    step_ms = [x.elapsed_time(y) for x, y in evs]
+    return replicas_max(float(sum(step_ms)), ws), step_ms
+
+
+def e2e_heat(R, ctx, pde, u0, nsteps, ws):
+    """The workload through the C ABI with host buffers: every benchmark step
+    copies u0 from pinned host memory to the device, advances 500 graphed RK4
+    steps and reads the state back into pinned host memory.  Host wall time,
+    max over ranks."""
+    import ctypes
+    import torch
+    W = WORKLOAD
+    u_host = torch.from_numpy(u0.copy()).pin_memory()
+    out_host = torch.empty(W["N"], dtype=torch.float64).pin_memory()
+    uh, oh = u_host.numpy(), out_host.numpy()
+    pde.fillInitialConditions(uh)
+    pde.advance(R.RK4, W["dt"], W["steps"], graph=True)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(nsteps):
+        pde.fillInitialConditions(uh)  # host -> device (pinned)
+        pde.advance(R.RK4, W["dt"], W["steps"], graph=True)
+        ctx.check(ctx.L.rbffd_pde_get_state(pde.h, oh.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                  "get_state")  # device -> host (pinned)
+    return replicas_max(time.perf_counter() - t, ws), oh.copy()
+
+
+def stage_kernel_name(shape, tname):
+    if shape[2] > 0:
+        return "k_stage_tile<%s,HEAT> (halo tile of %d rows, 16-bit local indices)" % (tname, shape[2])
+    return "k_stage_scalar<%s,HEAT> (%d lane(s) per row)" % (tname, shape[0])
+
+
+def stage_traffic(tag, tiled):
+    """DRAM bytes per stage launch from the committed ncu summary, or None."""
+    tp = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if not os.path.exists(tp):
+        return None
+    try:
+        return json.load(open(tp)).get("heat_%s%s_dram_bytes_per_launch" % (tag, "_tile" if tiled else ""))
+    except (OSError, ValueError):
+        return None
+
+
+def rel_err(x, ref):
+    d = x - ref
+    return float(np.linalg.norm(d) / np.linalg.norm(ref)), float(np.abs(d).max() / np.abs(ref).max())
 
 
 def run_ours(args):
@@ -242,112 +357,101 @@ def run_ours(args):
     t = time.perf_counter()
     der.computeAllWeightsForAllStencils()  # second call: tuned shapes, warm caches
     t_weights2 = time.perf_counter() - t
-    pde = R.HeatSphere(grid, der, 1.0, dtype=R.F32)
-    pde.fillInitialConditions(u0)
-    stream = torch.cuda.ExternalStream(ctx.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
-    def one_step():
-        pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
-
-    for _ in range(max(3, args.warmup)):
-        one_step()
-    ctx.synchronize()
-    # ---- timed region (device time, CUDA events on the library's stream) ----
-    clocks = ClockSampler(local)
-    clocks.start()
-    if ws > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    ctx.synchronize()
-    evs = []
-    with torch.cuda.stream(stream):
-        for _ in range(args.steps):
-            flush.fill_(1.0)  # write a buffer larger than L2 between timed steps
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            one_step()
-            e1.record(stream)
-            evs.append((e0, e1))
-    ctx.synchronize()
-    torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    clk = clocks.stop()
-    tot_ms = replicas_max(float(sum(step_ms)), ws)
-    node_updates = float(N) * steps * args.steps * ws  # all replicas
-    value = replicas_rate(float(N) * steps * args.steps, ws, tot_ms * 1e-3)
-    launches = 4 * steps * args.steps  # one fused stage kernel per RK4 stage
-    per_launch_s = tot_ms * 1e-3 / launches
-    shape = pde.getShape()  # (lanes per row, threads per block, rows per halo tile or 0), chosen by the autotuner
-    tiled = shape[2] > 0
-    kernel_name = ("k_stage_tile<float,HEAT> (halo tile of %d rows, 16-bit local indices)" % shape[2] if tiled else
-                   "k_stage_scalar<float,HEAT> (%d lane(s) per row)" % shape[0])
-    bytes_launch = N * stage_bytes(n, 4, 4, 2 if tiled else 4)
-    achieved = bytes_launch / per_launch_s / 1e9
     peak, peak_kind = load_peaks()
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get("heat_f32_tile_dram_bytes_per_launch" if tiled else
-                                              "heat_f32_dram_bytes_per_launch")
-        except (OSError, ValueError):
-            traffic = None
-    # ---- end to end through the C ABI with host buffers ----
-    u_host = torch.from_numpy(u0.copy()).pin_memory()
-    out_host = torch.empty(N, dtype=torch.float64).pin_memory()
-    uh = u_host.numpy()
-    oh = out_host.numpy()
-    pde_e2e = R.HeatSphere(grid, der, 1.0, dtype=R.F32)
-    pde_e2e.fillInitialConditions(uh)
-    pde_e2e.advance(R.RK4, dt, steps, graph=True)
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        pde_e2e.fillInitialConditions(uh)  # host -> device (pinned)
-        pde_e2e.advance(R.RK4, dt, steps, graph=True)
-        pde_e2e.ctx.check(0)
-        import ctypes
-        pde_e2e.ctx.check(pde_e2e.ctx.L.rbffd_pde_get_state(pde_e2e.h, oh.ctypes.data_as(ctypes.POINTER(
-            ctypes.c_double))), "get_state")  # device -> host (pinned)
-    e2e_s = replicas_max(time.perf_counter() - t, ws)
-    e2e_value = node_updates / e2e_s
+    warm = max(3, args.warmup)
+    res = {}
+    # FP64 (the headline: the reference's arithmetic) and FP32 beside it, same protocol.
+    for tag, dtype, wb in (("fp64", R.F64, 8), ("fp32", R.F32, 4)):
+        pde = R.HeatSphere(grid, der, 1.0, dtype=dtype)
+        pde.fillInitialConditions(u0)
+        for _ in range(warm):
+            pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
+        ctx.synchronize()
+        clocks = ClockSampler(local)
+        tot_ms, step_ms = timed_heat_steps(torch, ctx, pde, args.steps, flush, ws, clocks)
+        clk = clocks.stop()
+        launches = 4 * steps * args.steps  # one fused stage kernel per RK4 stage
+        per_launch_s = tot_ms * 1e-3 / launches
+        shape = pde.getShape()  # (lanes per row, threads per block, rows per halo tile or 0): the autotuner's pick
+        tiled = shape[2] > 0
+        bytes_launch = N * stage_bytes(n, wb, wb, 2 if tiled else 4)
+        achieved = bytes_launch / per_launch_s / 1e9
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, dt, steps, graph=True)
+        res[tag] = {
+            "value": replicas_rate(float(N) * steps * args.steps, ws, tot_ms * 1e-3), "ms_per_step": tot_ms / args.steps,
+            "launches": launches, "clocks": clk, "shape": shape, "u_final": pde.getLocalSolution(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": stage_traffic(tag.replace("fp", "f"), tiled), "peak_kind": peak_kind,
+                         "kernel": stage_kernel_name(shape, "double" if wb == 8 else "float") +
+                         ", fused SpMV + RHS + RK4 stage", "shape": shape, "algorithmic_bytes_per_launch": bytes_launch,
+                         "l2_resident": True,
+                         "note": "per-launch time = timed region / launches (includes graph launch gaps). The %s "
+                                 "weights and indices (%.1f MB) stay in the 126 MB L2 across the 2000 launches of "
+                                 "a benchmark step (the L2 flush runs between benchmark steps), so this rate is "
+                                 "L2-fed and can exceed the HBM copy peak; hbm_bound_case is the same kernel where "
+                                 "it cannot stay in L2" % (tag.upper(), N * n * (wb + (2 if tiled else 4)) / 1e6)}}
+        if tag == "fp64":
+            e2e_s, e2e_out = e2e_heat(R, ctx, pde, u0, args.steps, ws)
+            res[tag]["e2e"] = float(N) * steps * args.steps * ws / e2e_s
+            res[tag]["e2e_equals_device"] = bool(np.array_equal(e2e_out, res[tag]["u_final"]))
+        else:
+            e2e_s, _ = e2e_heat(R, ctx, pde, u0, args.steps, ws)
+            res[tag]["e2e"] = float(N) * steps * args.steps * ws / e2e_s
+        pde.close()
+    h = res["fp64"]
     cpu = None
-    if ws == 1 and not args.no_cpu_baseline:  # the host-core baseline: rank 0 at N = 1 only
+    accuracy = {}
+    if ws == 1 and not args.no_cpu_baseline:  # the host-core baseline and the FP64 oracle: rank 0 at N = 1 only
         w64 = der.getWeights(R.LSFC)
-        cps, nth, secs = cpu_baseline_heat(st, w64, u0, 1500)
+        cps, nth, secs, u_ref = cpu_oracle_heat(st, w64, u0, 3)
         cpu = {"value": cps, "unit": "node-updates/s", "cores": nth, "kind": "port",
-               "sample": "1500 RK4 steps (3 runs of the 500-step workload) on the N=%d, n=%d grid, %.1f s; FP64 "
-                         "oracle restatement of advanceRungeKutta4 + applyWeightsForDeriv, OpenMP over rows" % (
-                             N, n, secs)}
+               "sample": "the 500-step workload 3 times (1500 RK4 steps) on the N=%d, n=%d grid, %.1f s; FP64 "
+                         "oracle restatement of advanceRungeKutta4 + applyWeightsForDeriv, OpenMP over rows, on the "
+                         "device's FP64 weights" % (N, n, secs)}
+        ex = R.exact_sph_heat(xyz, W["lmax"], coeffs, steps * dt)
+        for tag in ("fp64", "fp32"):
+            l2, linf = rel_err(res[tag]["u_final"], u_ref)
+            accuracy["%s_vs_fp64_oracle" % tag] = {"rel_l2": l2, "rel_linf": linf}
+        accuracy["fp64_bit_exact_vs_oracle"] = bool(np.array_equal(res["fp64"]["u_final"], u_ref))
+        l2, linf = rel_err(res["fp64"]["u_final"], ex)
+        accuracy["fp64_vs_exact"] = {"rel_l2": l2, "rel_linf": linf}
+        accuracy["note"] = ("after the 500 RK4 steps; oracle = FP64 CPU restatement of the reference's RK4 and SpMV "
+                            "on the same weights; exact = the spherical-harmonic solution")
     extras = {}
     if not args.no_extras and ws == 1:  # the other configurations: a one-GPU report
-        extras = bench_extras(R, torch, ctx, grid, der, pde, u0, xyz, st, coeffs)
+        pde32 = R.HeatSphere(grid, der, 1.0, dtype=R.F32)
+        extras = bench_extras(R, torch, ctx, grid, der, pde32, u0, xyz, st, coeffs)
+        pde32.close()
+    hbm = extras.get("heat_hbm_bound", {}) if isinstance(extras, dict) else {}
+    if isinstance(hbm, dict) and "n50_fp64" in hbm:
+        h["roofline"]["hbm_bound_case"] = dict(hbm["n50_fp64"], workload="heat_sphere_N655362_n50_deg3 (FP64)")
+    if isinstance(hbm, dict) and "n50_fp32" in hbm:
+        res["fp32"]["roofline"]["hbm_bound_case"] = dict(hbm["n50_fp32"], workload="heat_sphere_N655362_n50_deg3 (FP32)")
     if rank == 0:
+        f32 = res["fp32"]
         line = {
-            "metric": "rk4_node_updates_per_s", "value": value, "unit": "node-updates/s", "n_gpus": ws,
-            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": tot_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": W["name"], "nodes": N, "stencil": n, "poly_deg": W["deg"], "rk4_steps_per_step": steps,
-                       "dt": dt, "eps": eps, "parallelism": "replicas" if ws > 1 else "single",
-                       "l2_flush": "256 MiB buffer written between timed steps"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": kernel_name + ", fused SpMV + RHS + RK4 stage", "shape": shape,
-                         "algorithmic_bytes_per_launch": bytes_launch,
-                         "note": "per-launch time = timed region / launches (includes graph launch gaps); "
-                                 "FP32 weights+indices (65.5 MB) fit the 126 MB L2"},
+            "metric": "rk4_node_updates_per_s", "value": h["value"], "unit": "node-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": warm, "ms_per_step": h["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(ws),
+            "roofline": h["roofline"],
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "node-updates/s", "h2d_bytes_per_step": N * 8,
+            "e2e": {"value": h["e2e"], "unit": "node-updates/s", "h2d_bytes_per_step": N * 8,
                     "d2h_bytes_per_step": N * 8},
-            "gpu_launches": launches,
-            "clocks": clk,
+            "gpu_launches": h["launches"],
+            "clocks": h["clocks"],
+            "accuracy": accuracy,
+            "fp32": {"value": f32["value"], "unit": "node-updates/s", "ms_per_step": f32["ms_per_step"],
+                     "e2e": f32["e2e"], "dtype": "f32", "shape": f32["shape"], "clocks": f32["clocks"],
+                     "roofline": f32["roofline"],
+                     "note": "FP32 weights, state and accumulation on the same grid and weights (rounded from FP64), "
+                             "same timing protocol; errors against the FP64 oracle under accuracy"},
             "weights_setup_s": {"first_call": t_weights, "tuned": t_weights2},
             "extras": extras,
         }
         print(json.dumps(line), flush=True)
-    pde.close()
-    pde_e2e.close()
     grid.close()
     ctx.close()
     if ws > 1:
@@ -1030,7 +1134,7 @@ def bench_serving(R, torch, ctx):
     }
 
 
-def run_profile(tile_rows=0):
+def run_profile(tile_rows=0, dtype="f64"):
     import rbffd_gpu_b200 as R
     xyz, st, u0, eps, _ = setup_problem()
     ctx = R.Context(0)
@@ -1039,7 +1143,7 @@ def run_profile(tile_rows=0):
     der.setEpsilon(eps)
     der.setPolynomialDegree(WORKLOAD["deg"])
     der.computeAllWeightsForAllStencils()
-    pde = R.HeatSphere(grid, der, 1.0, dtype=R.F32)
+    pde = R.HeatSphere(grid, der, 1.0, dtype=R.F64 if dtype == "f64" else R.F32)
     if tile_rows:
         pde.setTiledShape(tile_rows, 1)
     pde.fillInitialConditions(u0)
@@ -1174,7 +1278,7 @@ def main():
     elif args.profile_multitracer:
         run_profile_multitracer(args.profile_multitracer)
     elif args.profile or args.profile_tile:
-        run_profile(args.profile_tile)
+        run_profile(args.profile_tile, args.profile_dtype)
     elif args.impl == "reference":
         run_reference(args)
     else:

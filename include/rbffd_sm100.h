@@ -348,11 +348,13 @@ int rbffd_pde_advance(rbffd_pde* pde, int scheme, double dt, int nsteps, int fla
  * u_t = kappa * LSFC u on the grid's Laplace-Beltrami weights (computed or
  * set beforehand).  A copy of the state in the grid's internal node order and
  * the three RK4 stage buffers live in one fixed 8 MiB array inside the
- * library, reserved on each GPU when the library's device code is loaded
- * there and held until the process exits: grids above 262144 nodes
- * (FP64) or 524288 nodes (FP32) are rejected with RBFFD_ERR_INVALID.  The
- * first call on a device looks up that array's device address, so make it
- * before any stream capture.  All calls on a device share the array and
+ * library.  rbffd_ctx_create loads this path's device code on its GPU, which
+ * reserves the array there (held until the process exits); so a host that
+ * reserves nearly all GPU memory for its own pool creates its context first,
+ * and no call of this entry point then takes device memory, the first one
+ * included.  Grids above 262144 nodes (FP64) or 524288 nodes (FP32) are
+ * rejected with RBFFD_ERR_INVALID.  Every call looks up the array's device
+ * address (cudaGetSymbolAddress, no allocation).  All calls on a device share the array and
  * leave their stage values in it: calls that overlap on the GPU race and
  * must be serialised by the caller.  Runs on the context stream and returns
  * after the steps complete. */

@@ -54,6 +54,10 @@ def lib():
                                      _dp, ctypes.c_double, ctypes.c_int, ctypes.c_int]
         L.orc_rk4_heat.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, ctypes.c_double, ctypes.c_int, _dp,
                                    ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.orc_set_fused.argtypes = [ctypes.c_int]
+        L.orc_set_fused.restype = None
+        L.orc_nodes_fibonacci.argtypes = [ctypes.c_int, ctypes.c_uint64, _dp]
+        L.orc_sph_heat.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, _dp]
         _LIB = L
     return _LIB
 
@@ -79,10 +83,39 @@ def ref_lib(name):
         if L is not None and name == "ref_norms":
             L.ref_sol_norms.argtypes = [_dp, _dp, ctypes.c_int, _dp]
             L.ref_sol_norms.restype = None
+        if L is not None and name == "ref_rbffd":
+            L.ref_rbffd_create.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_int, ctypes.c_double, ctypes.c_int, _ip,
+                                           ctypes.POINTER(ctypes.c_void_p)]
+            L.ref_rbffd_destroy.argtypes = [ctypes.c_void_p]
+            L.ref_rbffd_destroy.restype = None
+            L.ref_rbffd_weights.argtypes = [ctypes.c_void_p, ctypes.c_uint, _dp]
+            L.ref_rbffd_system.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+            L.ref_rbffd_apply.argtypes = [ctypes.c_void_p, ctypes.c_uint, _dp, _dp, ctypes.c_int, ctypes.c_int]
+            L.ref_rbffd_rk4.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]
+            L.ref_exact_advection.argtypes = [_dp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp]
+            L.ref_exact_advection.restype = None
         if L is not None and name == "ref_mmio":
             L.ref_mm_write_header.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
             L.ref_mm_read_header.argtypes = [ctypes.c_char_p, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_long)]
     return _REF[name]
+
+
+class reference_arithmetic:
+    """Within this block the oracle's time-stepping arithmetic (SpMV, RK4
+    axpys, advection right-hand side) rounds every product and every sum, in
+    the reference's source order: the arithmetic of the reference as its own
+    build compiles it (x86-64, no FMA).  Outside it, each of those
+    multiply-adds is fused: the device kernels' FP64 arithmetic."""
+
+    def __enter__(self):
+        lib().orc_set_fused(0)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_fused(1)
+        return False
 
 
 def _c(a, dt):
@@ -197,6 +230,42 @@ def ref_knn(xyz, k):
     if L.ref_knn(_p(xyz), N, k, _p(idx, _ip), _p(d)) != 0:
         raise RuntimeError("reference kd-tree returned a short list")
     return idx, d
+
+
+def fibonacci_nodes(N, seed):
+    """The benchmark's seeded Fibonacci-sphere nodes (N x 3), restated here so
+    the CPU arm builds its grid without the product library."""
+    xyz = np.zeros((N, 3))
+    if lib().orc_nodes_fibonacci(N, seed, _p(xyz)) != 0:
+        raise ValueError("orc_nodes_fibonacci: bad arguments")
+    return xyz
+
+
+def sph_heat(xyz, lmax, coeffs, t, kappa=1.0):
+    """sum c_lm exp(-kappa l(l+1) t) Y_lm on the unit sphere (real orthonormal
+    harmonics, coefficients ordered l, m = -l..l): the heat workload's initial
+    state (t = 0) and exact solution."""
+    xyz = _c(xyz, np.float64)
+    coeffs = _c(coeffs, np.float64)
+    if coeffs.size != (lmax + 1) ** 2:
+        raise ValueError("need (lmax+1)^2 coefficients")
+    u = np.zeros(xyz.shape[0])
+    if lib().orc_sph_heat(xyz.shape[0], _p(xyz), lmax, _p(coeffs), kappa, t, _p(u)) != 0:
+        raise ValueError("orc_sph_heat failed")
+    return u
+
+
+def knn_for_baseline(xyz, k):
+    """k-nearest stencils for the CPU arm: the reference's own k-d tree
+    (external/kdtree/KDTree.h compiled in oracle/_ref) when it was built,
+    else scipy's k-d tree (same lists wherever no two distances tie).
+    Returns (stencils, source)."""
+    r = ref_knn(xyz, k)
+    if r is not None:
+        return r[0], "reference k-d tree (external/kdtree/KDTree.h)"
+    from scipy.spatial import cKDTree
+    _, idx = cKDTree(xyz).query(xyz, k)
+    return idx.astype(np.int32), "scipy cKDTree"
 
 
 def cart2sph(x, y, z):
@@ -436,4 +505,76 @@ def exact_vortex_rollup(xyz, t):
     for i, (x, y, z) in enumerate(np.asarray(xyz).tolist()):
         rho = 3.0 * math.cos(math.atan2(z, math.sqrt(x * x + y * y)))
         out[i] = 1.0 - math.tanh((rho / 5.0) * math.sin(math.atan2(y, x) - w[i] * t))
+    return out
+
+
+class RefRBFFD:
+    """The reference's own RBFFD / TimeDependentPDE / CosineBell / VortexRollup,
+    compiled from its sources into oracle/_ref/libref_rbffd.so (see
+    oracle/ref_rbffd.cpp): a problem built as the cosine-bell experiment
+    builds it on one rank (k-d tree stencils, one subdomain, RBFFD with
+    ONE_MONOMIAL: the constant is the only polynomial term)."""
+
+    KIND_COSINE_BELL, KIND_HEAT, KIND_VORTEX = 0, 1, 2
+
+    @staticmethod
+    def available():
+        return ref_lib("ref_rbffd") is not None
+
+    def __init__(self, xyz, n, der_types, eps, dim=2, hv_k=4, hv_gamma=8e-4, use_hv=False):
+        self.L = ref_lib("ref_rbffd")
+        if self.L is None:
+            raise RuntimeError("oracle/_ref/libref_rbffd.so is not built (needs the reference tree)")
+        self.xyz = _c(xyz, np.float64)
+        self.N, self.n = self.xyz.shape[0], n
+        self.stencils = np.zeros((self.N, n), dtype=np.int32)
+        h = ctypes.c_void_p()
+        rc = self.L.ref_rbffd_create(_p(self.xyz), self.N, n, der_types, dim, eps, hv_k, hv_gamma,
+                                     1 if use_hv else 0, _p(self.stencils, _ip), ctypes.byref(h))
+        if rc != 0:
+            raise RuntimeError("the reference's RBFFD set-up failed")
+        self.h = h
+
+    def weights(self, der_type):
+        """Stored weights: N x (n + 1), the stencil weights then the constant's."""
+        w = np.zeros((self.N, self.n + 1))
+        if self.L.ref_rbffd_weights(self.h, der_type, _p(w)) != 0:
+            raise RuntimeError("no weights of type 0x%x" % der_type)
+        return w
+
+    def system(self, st_index, n_types):
+        """(LHS, RHS) of one stencil from getStencilLHS / getStencilMultiRHS."""
+        m = self.n + 1
+        A = np.zeros(m * m)
+        B = np.zeros(m * n_types)
+        self.L.ref_rbffd_system(self.h, st_index, _p(A), _p(B))
+        return A.reshape(m, m).T.copy(), B.reshape(n_types, m).T.copy()
+
+    def apply(self, der_type, u, start=0, count=0):
+        u = _c(u, np.float64)
+        d = np.zeros(self.N)
+        self.L.ref_rbffd_apply(self.h, der_type, _p(u), _p(d), start, count)
+        return d
+
+    def rk4(self, kind, u, dt, nsteps, a=1.0, alpha=np.pi / 2, revolution=1036800.0, use_hv=True):
+        u = np.array(u, dtype=np.float64)
+        if self.L.ref_rbffd_rk4(self.h, kind, a, alpha, revolution, 1 if use_hv else 0, dt, nsteps, _p(u)) != 0:
+            raise RuntimeError("ref_rbffd_rk4")
+        return u
+
+    def close(self):
+        if self.h:
+            self.L.ref_rbffd_destroy(self.h)
+            self.h = None
+
+
+def ref_exact_advection(xyz, a=1.0, t=0.0):
+    """ExactAdvection (tests/experiments/cosine_bell_on_sphere/exact_advection.h)
+    compiled from the reference, at the nodes; None without the library."""
+    L = ref_lib("ref_rbffd")
+    if L is None:
+        return None
+    xyz = _c(xyz, np.float64)
+    out = np.zeros(xyz.shape[0])
+    L.ref_exact_advection(_p(xyz), xyz.shape[0], a, t, _p(out))
     return out

@@ -15,17 +15,38 @@
 * ``oracle/_ref/libref_mmio.so`` -- the reference's own ``external/nist/mmio.cpp``
   (the Matrix Market header of its weight files).
 
-The reference's full RBFFD class (``src/rbffd/rbffd.cpp``) needs Armadillo,
-LAPACK, MPI and Boost, none of which exist here, so it is treated as
-unbuildable; ``oracle.c`` restates it instead.  The ``_ref`` libraries are
-built only where the reference tree exists and travel prebuilt elsewhere.
+* ``oracle/_ref/libref_rbffd.so`` -- the reference's own hot path through
+  ``oracle/ref_rbffd.cpp``: ``src/rbffd/rbffd.cpp`` (weights, getStencilLHS/RHS,
+  applyWeightsForDeriv), ``src/pdes/{pde,time_dependent_pde}.cpp`` (RK4),
+  ``src/pdes/hyperbolic/{cosine_bell,vortex_rollup}.cpp``, ``src/grids/{grid_interface,
+  domain}.cpp`` and their utilities, unmodified, against ``oracle/shim/armadillo``
+  (dense matrices; ``arma::solve`` as partial-pivot LU) and ``oracle/shim/mpi.h``
+  (one rank).  ``oracle.c`` is checked against it bit for bit.
+
+The ``_ref`` libraries are built only where the reference tree exists and
+travel prebuilt elsewhere.
 """
 import os
 import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("RBFFD_REFERENCE_ROOT", "/root/reference")
+# The reference checkout: RBFFD_REFERENCE_ROOT if set, else a directory named
+# "reference" beside the repository's own directory.  Where neither exists the
+# reference pieces are skipped (their prebuilt libraries are used as they are).
+REF = os.environ.get("RBFFD_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+
+
+# The reference's hot path compiled as a whole (oracle/ref_rbffd.cpp): RBFFD,
+# PDE / TimeDependentPDE, CosineBell, VortexRollup and what they need.
+REF_CORE_SOURCES = [
+    "src/rbffd/rbffd.cpp", "src/grids/grid_interface.cpp", "src/grids/domain.cpp", "src/pdes/pde.cpp",
+    "src/pdes/time_dependent_pde.cpp", "src/pdes/hyperbolic/cosine_bell.cpp", "src/pdes/hyperbolic/vortex_rollup.cpp",
+    "src/utils/comm/communicator.cpp", "src/utils/comm/mpisendable.cpp", "src/utils/norms.cpp", "src/utils/random.cpp",
+    "src/utils/geom/cart2sph.cpp", "external/nist/mmio.cpp", "external/timers/timer_eb.cpp",
+    "external/graphics_lib/utilities/Vec3d.cpp", "external/graphics_lib/utilities/CVec3.cpp",
+    "external/graphics_lib/utilities/Vec3i.cpp",
+]
 
 
 def _newer(target, sources):
@@ -100,6 +121,24 @@ def build_ref(force=False):
                        nm_src[0], nm_src[1], os.path.join(REF, "src/utils/random.cpp"), os.path.join(util, "Vec3d.cpp"),
                        "-o", nm])
     built.append(nm)
+    rb2 = os.path.join(outdir, "libref_rbffd.so")
+    rb2_src = [os.path.join(HERE, "ref_rbffd.cpp")] + [os.path.join(REF, f) for f in REF_CORE_SOURCES]
+    if force or _newer(rb2, rb2_src + [os.path.join(HERE, "shim", "armadillo"), os.path.join(HERE, "shim", "mpi.h")]):
+        # The reference's own flags (CMakeLists.txt:130-140, common/LINUX_CONFIG.cmake:23): g++ -O3
+        # -ftree-vectorize for x86-64 with no -march, so no FMA contraction.  Two additions: -std=gnu++14
+        # (its headers use dynamic exception specifications, removed in C++17, and it needs the C++11
+        # pow(double, int) its tests were pinned with), and -fno-unswitch-loops: with GCC 13.3 at -O3 the
+        # loop unswitching of getStencilRHS's per-node switch sends DerType HV to the default branch
+        # ("deriv type 32 is not supported yet"); the option changes no arithmetic.
+        _run(["g++", "-std=gnu++14", "-O3", "-ftree-vectorize", "-fno-unswitch-loops", "-DNDEBUG", "-DUSE_KDTREE",
+              "-DUSE_DOUBLE_VEC3", "-fPIC", "-shared", "-w", "-include", "ctime", "-include", "cstdio",
+              "-I" + os.path.join(HERE, "shim")] +
+             ["-I" + os.path.join(REF, d) for d in ("src", "src/rbffd", "src/grids", "src/utils", "src/pdes",
+                                                    "external/kdtree", "external/timers", "external/nist",
+                                                    "external/graphics_lib/utilities",
+                                                    "tests/experiments/cosine_bell_on_sphere")] +
+             rb2_src + ["-Wl,--no-undefined", "-o", rb2])
+    built.append(rb2)
     mm = os.path.join(outdir, "libref_mmio.so")
     mm_src = [os.path.join(HERE, "ref_mmio.cpp"), os.path.join(REF, "external/nist/mmio.cpp")]
     if force or _newer(mm, mm_src):

@@ -19,13 +19,21 @@
  *   - TimeDependentPDE::advanceRungeKutta4  src/pdes/time_dependent_pde.cpp:172-304
  *
  * Floating-point model.  Compiled with -ffp-contract=off so every expression
- * is evaluated exactly as written.  Where the reference, compiled by GCC with
- * its default -ffp-contract=fast on an FMA-capable host, would fuse a
- * multiply-add (the SpMV accumulation, the RK4 axpys, the advection RHS, the
- * LU updates) this file writes fma() explicitly, so the model is pinned and
- * repeatable.  The RBF kernel evaluations are written without fma, operand
- * order as in rbf_gaussian.h (checked against the header itself, compiled
- * from the reference sources, by tests/test_oracle_pins.py).
+ * is evaluated exactly as written.  Two models of the multiply-adds on the
+ * time-stepping path (the SpMV accumulation, the RK4 axpys, the advection
+ * right-hand side), selected by orc_set_fused():
+ *   fused (default) -- each such multiply-add is one fma(), the arithmetic of
+ *     the device kernels' FP64 path (one rounding per multiply-add);
+ *   plain (orc_set_fused(0)) -- a rounded product, then a rounded sum, in the
+ *     reference's source order: the arithmetic of the reference as its own
+ *     build compiles it (CMakeLists.txt:130-140: g++ -O3 -ftree-vectorize for
+ *     x86-64 without -march, which has no FMA instruction), checked bit for
+ *     bit against the reference's RBFFD, TimeDependentPDE and CosineBell
+ *     compiled from their sources (oracle/ref_rbffd.cpp, tests/test_ref_core.py).
+ * The LU updates are always fused (the shim's arma::solve is the same code).
+ * The RBF kernel evaluations are written without fma, operand order as in
+ * rbf_gaussian.h (checked against the header itself, compiled from the
+ * reference sources, by tests/test_oracle_pins.py).
  *
  * Polynomial augmentation.  poly_deg = 0 is the reference build
  * (ONE_MONOMIAL, np = 1, rbffd.cpp:1,230-234; constant row of the RHS is 0
@@ -499,10 +507,20 @@ int orc_assemble(const double* xyz, const int* st, int n, int deg, double eps, u
 /* ------------------------------------------------------------------ */
 /* applyWeightsForDeriv (rbffd.cpp:669-688): deriv[i] = sum_s w[i][s]*u[st_i[s]],
  * s in stencil order; accumulation fused (fma).  u and deriv are [N][T].      */
+static int g_fused = 1;
+
+/* 1: fused multiply-adds on the time-stepping path (the device's FP64
+ * arithmetic); 0: plain products and sums (the reference's own build). */
+void orc_set_fused(int fused) { g_fused = fused ? 1 : 0; }
+int orc_get_fused(void) { return g_fused; }
+
+/* a*b + c in the selected model */
+static inline double madd(double a, double b, double c) { return g_fused ? fma(a, b, c) : a * b + c; }
+
 static inline double row_dot(const double* w, const int* s, int n, const double* u, int T, int t)
 {
     double der = 0.0;
-    for (int k = 0; k < n; k++) der = fma(w[k], u[(size_t)s[k] * T + t], der);
+    for (int k = 0; k < n; k++) der = madd(w[k], u[(size_t)s[k] * T + t], der);
     return der;
 }
 
@@ -560,7 +578,8 @@ static void eval_rhs(const rhs_t* R, const double* x, double* f)
             if (R->kind == 1) {
                 double dl = row_dot(R->w0 + (size_t)i * R->n_pad, s, n, x, R->T, t);
                 double dt = row_dot(R->w1 + (size_t)i * R->n_pad, s, n, x, R->T, t);
-                v = -fma(R->cu[i], dl, R->cv[i] * dt);
+                /* -((vel_u/a) * dh_dlambda + (vel_v/a) * dh_dtheta), cosine_bell.cpp:51 */
+                v = -madd(R->cu[i], dl, R->cv[i] * dt);
                 if (R->w2) v = v + row_dot(R->w2 + (size_t)i * R->n_pad, s, n, x, R->T, t);
             } else {
                 v = R->kappa * row_dot(R->w0 + (size_t)i * R->n_pad, s, n, x, R->T, t);
@@ -581,14 +600,17 @@ static int rk4(const rhs_t* R, double* u, double dt, int nsteps, int nthreads)
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
     for (int step = 0; step < nsteps; step++) {
+        /* s = u + 0.5*dt*(k + 0): time_dependent_pde.cpp:201-250 (the forcing
+         * term f is 0, and k + 0. == k for every non-zero k) */
         eval_rhs(R, u, k1);
-        for (size_t i = 0; i < L; i++) s[i] = fma(0.5 * dt, k1[i], u[i]);
+        for (size_t i = 0; i < L; i++) s[i] = madd(0.5 * dt, k1[i], u[i]);
         eval_rhs(R, s, k2);
-        for (size_t i = 0; i < L; i++) s[i] = fma(0.5 * dt, k2[i], u[i]);
+        for (size_t i = 0; i < L; i++) s[i] = madd(0.5 * dt, k2[i], u[i]);
         eval_rhs(R, s, k3);
-        for (size_t i = 0; i < L; i++) s[i] = fma(dt, k3[i], u[i]);
+        for (size_t i = 0; i < L; i++) s[i] = madd(dt, k3[i], u[i]);
         eval_rhs(R, s, k4);
-        for (size_t i = 0; i < L; i++) u[i] = fma(dt / 6., k1[i] + 2. * k2[i] + 2. * k3[i] + k4[i], u[i]);
+        /* u + (dt/6.)*(k1 + 2k2 + 2k3 + k4), :280-282 (2.*k is exact) */
+        for (size_t i = 0; i < L; i++) u[i] = madd(dt / 6., k1[i] + 2. * k2[i] + 2. * k3[i] + k4[i], u[i]);
     }
     free(s); free(k1); free(k2); free(k3); free(k4);
     return 0;
@@ -622,4 +644,109 @@ int orc_max_threads(void)
 void orc_cart2sph(double x, double y, double z, double* theta, double* phi)
 {
     cart2sph(x, y, z, theta, phi);
+}
+
+/* ------------------------------------------------------------------------
+ * Synthetic workload inputs for the CPU arm of the benchmark, so that it
+ * builds its grid and initial state without the product library.  The
+ * reference's maximum-determinant node files are not distributed; these are
+ * the seeded stand-ins the benchmark uses on both arms.
+ *
+ * orc_nodes_fibonacci: the Fibonacci spiral z_i = 1 - (2i+1)/N,
+ * phi_i = i*pi*(3 - sqrt 5), turned by a uniform random rotation drawn from
+ * three splitmix64 uniforms (Shoemake's unit quaternion), each point
+ * renormalised onto the unit sphere.
+ * ------------------------------------------------------------------------ */
+static uint64_t sm64_next(uint64_t* s)
+{
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static double sm64_unit(uint64_t* s) { return (double)(sm64_next(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+int orc_nodes_fibonacci(int N, uint64_t seed, double* xyz)
+{
+    if (N <= 0 || !xyz) return -1;
+    uint64_t s = seed;
+    double a = sm64_unit(&s), b = sm64_unit(&s), c = sm64_unit(&s);
+    const double tau = 6.283185307179586476925286766559;
+    /* unit quaternion (qw; qx, qy, qz) */
+    double qx = sqrt(1.0 - a) * sin(tau * b), qy = sqrt(1.0 - a) * cos(tau * b);
+    double qz = sqrt(a) * sin(tau * c), qw = sqrt(a) * cos(tau * c);
+    double M[3][3];
+    M[0][0] = 1 - 2 * (qy * qy + qz * qz); M[0][1] = 2 * (qx * qy - qz * qw); M[0][2] = 2 * (qx * qz + qy * qw);
+    M[1][0] = 2 * (qx * qy + qz * qw); M[1][1] = 1 - 2 * (qx * qx + qz * qz); M[1][2] = 2 * (qy * qz - qx * qw);
+    M[2][0] = 2 * (qx * qz - qy * qw); M[2][1] = 2 * (qy * qz + qx * qw); M[2][2] = 1 - 2 * (qx * qx + qy * qy);
+    const double ga = 3.14159265358979323846264338327950288 * (3.0 - sqrt(5.0));
+    for (int i = 0; i < N; i++) {
+        double zi = 1.0 - (2.0 * i + 1.0) / N;
+        double ri = 1.0 - zi * zi;
+        ri = sqrt(ri > 0.0 ? ri : 0.0);
+        double ph = ga * (double)i;
+        double p0 = ri * cos(ph), p1 = ri * sin(ph), p2 = zi;
+        double q[3];
+        for (int r = 0; r < 3; r++) q[r] = M[r][0] * p0 + M[r][1] * p1 + M[r][2] * p2;
+        double len = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+        for (int r = 0; r < 3; r++) xyz[3 * (size_t)i + r] = q[r] / len;
+    }
+    return 0;
+}
+
+/* orc_sph_heat: u(x, t) = sum_{l <= lmax, |m| <= l} c_lm exp(-kappa l(l+1) t) Y_lm(x)
+ * with real orthonormal spherical harmonics, coefficients ordered (l, m = -l..l):
+ * Y_l0 = P_l0(cos colat), Y_lm = sqrt 2 P_l|m|(cos colat) cos(m lon) for m > 0 and
+ * sin(|m| lon) for m < 0, P the fully normalised associated Legendre functions
+ * (Condon-Shortley phase) from the standard three-term recurrences.  The exact
+ * solution of u_t = kappa * Laplace-Beltrami(u) on the unit sphere. */
+int orc_sph_heat(int N, const double* xyz, int lmax, const double* coef, double kappa, double t, double* u)
+{
+    if (N < 0 || !xyz || !coef || !u || lmax < 0 || lmax > 200) return -1;
+    const double PI = 3.14159265358979323846264338327950288;
+    int L1 = lmax + 1;
+    double* dec = (double*)malloc(sizeof(double) * L1);
+    if (!dec) return -2;
+    for (int l = 0; l <= lmax; l++) dec[l] = exp(-kappa * l * (l + 1.0) * t);
+    int bad = 0;
+#pragma omp parallel
+    {
+        double* P = (double*)malloc(sizeof(double) * L1 * L1);
+        if (!P) {
+#pragma omp atomic write
+            bad = 1;
+        }
+#pragma omp for schedule(static)
+        for (int i = 0; i < N; i++) {
+            if (!P) continue;
+            double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
+            double sc = sqrt(x * x + y * y), cc = z, lon = atan2(y, x);
+            P[0] = sqrt(1.0 / (4.0 * PI));
+            for (int m = 1; m <= lmax; m++)
+                P[m * L1 + m] = -sqrt((2.0 * m + 1.0) / (2.0 * m)) * sc * P[(m - 1) * L1 + (m - 1)];
+            for (int m = 0; m < lmax; m++) P[(m + 1) * L1 + m] = sqrt(2.0 * m + 3.0) * cc * P[m * L1 + m];
+            for (int m = 0; m <= lmax; m++)
+                for (int l = m + 2; l <= lmax; l++) {
+                    double al = sqrt((4.0 * l * l - 1.0) / ((double)l * l - (double)m * m));
+                    double bl = sqrt(((l - 1.0) * (l - 1.0) - (double)m * m) / (4.0 * (l - 1.0) * (l - 1.0) - 1.0));
+                    P[l * L1 + m] = al * (cc * P[(l - 1) * L1 + m] - bl * P[(l - 2) * L1 + m]);
+                }
+            double sum = 0.0;
+            int k = 0;
+            for (int l = 0; l <= lmax; l++) {
+                double part = 0.0;
+                for (int m = -l; m <= l; m++, k++) {
+                    int am = m < 0 ? -m : m;
+                    double y_lm = m == 0 ? P[l * L1] : sqrt(2.0) * P[l * L1 + am] * (m > 0 ? cos(am * lon) : sin(am * lon));
+                    part += coef[k] * y_lm;
+                }
+                sum += dec[l] * part;
+            }
+            u[i] = sum;
+        }
+        free(P);
+    }
+    free(dec);
+    return bad ? -2 : 0;
 }

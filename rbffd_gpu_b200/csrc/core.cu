@@ -125,7 +125,7 @@ extern "C" int rbffd_ctx_create(int device, rbffd_ctx** out)
     }
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
     if (cudaMalloc((void**)&c->d_status, sizeof(int)) != cudaSuccess ||
-        cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
+        cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess || noalloc_preload() != RBFFD_OK) {
         cudaGetLastError();
         if (c->d_status) cudaFree(c->d_status);
         cudaStreamDestroy(c->stream);
@@ -719,6 +719,15 @@ int grid_to_internal(rbffd_grid* g, const void* src, void* dst, int T, int elem_
 int grid_to_caller(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s)
 {
     return grid_permute(g, src, dst, T, elem_bytes, s, 0);
+}
+
+int grid_permute_preload()
+{
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, k_permute<unsigned long long>) != cudaSuccess ||
+        cudaFuncGetAttributes(&a, k_permute<unsigned int>) != cudaSuccess)
+        return RBFFD_ERR_CUDA;
+    return RBFFD_OK;
 }
 
 extern "C" int rbffd_grid_nbytes(const rbffd_grid* g, size_t* bytes)

@@ -85,6 +85,10 @@ struct rbffd_grid {
 // grid's internal order (device arrays, on stream s).
 int grid_to_internal(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s);
 int grid_to_caller(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s);
+// Load (under lazy module loading) the device code of the permutation
+// kernels / of the allocation-free heat RK4 path on the current device.
+int grid_permute_preload();
+int noalloc_preload();
 
 // Row blocks of R consecutive internal rows with their halo: the unique nodes
 // their stencils reference.  A block's kernel stages the halo's values in

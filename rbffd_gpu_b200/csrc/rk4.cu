@@ -1282,8 +1282,12 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
 // device.  rbffd_heat_rk4_noalloc serves them: the caller passes the state
 // vector in its own device memory; the copy of the state in the grid's
 // internal node order and the three stage buffers RK4 needs live in the
-// file-scope array below, reserved when this library's device code is loaded
-// on a GPU and held until the process exits.
+// file-scope array below.  rbffd_ctx_create loads the device code this path
+// uses (this array, the stage kernels, the permutation kernels) on the
+// context's GPU, so the array is reserved then and held until the process
+// exits, and no call of this entry point loads a module (which would take
+// device memory) even under the CUDA runtime's lazy loading.  A caller that
+// reserves the GPU's memory for its own pool creates its context first.
 //
 // Limits and sharing: NOALLOC_MAX_NODES nodes in FP64 (twice that in FP32);
 // larger grids are rejected.  Every call on a device uses the same array, so
@@ -1294,23 +1298,32 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
 constexpr int NOALLOC_MAX_NODES = 262144;
 static __device__ __align__(256) double g_noalloc_scratch[4 * NOALLOC_MAX_NODES];  // 8 MiB per GPU
 
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[128];  // device address of g_noalloc_scratch, per device ordinal
-
 // The host-side name g_noalloc_scratch is not a device address: the address a
-// kernel may use is looked up once per device, with that device current.
+// kernel may use is looked up with the context's device current, on every
+// call (cheap, allocates nothing), so a context recreated after a
+// cudaDeviceReset -- where the module reloads at a new address -- is served
+// its current address.
 static int noalloc_scratch(rbffd_ctx* ctx, void** out)
 {
-    if (ctx->device < 0 || ctx->device >= 128) return set_error(ctx, RBFFD_ERR_INVALID, "device ordinal out of range");
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[ctx->device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return cuda_error(ctx, e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
-        g_noalloc_ptr[ctx->device] = p;
-    }
-    *out = g_noalloc_ptr[ctx->device];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return cuda_error(ctx, e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
+    *out = p;
     return RBFFD_OK;
+}
+
+// Called by rbffd_ctx_create with the context's device current: loads the
+// allocation-free path's device code (see above).  cudaFuncGetAttributes
+// loads a kernel; cudaGetSymbolAddress loads the array's module.
+int noalloc_preload()
+{
+    void* p = nullptr;
+    cudaFuncAttributes a;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess ||
+        cudaFuncGetAttributes(&a, k_stage_scalar<double, KIND_HEAT, false, 1>) != cudaSuccess ||
+        cudaFuncGetAttributes(&a, k_stage_scalar<float, KIND_HEAT, false, 1>) != cudaSuccess)
+        return RBFFD_ERR_CUDA;
+    return grid_permute_preload();
 }
 
 // u: the state in the grid's internal order (a region of the scratch array)

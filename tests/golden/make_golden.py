@@ -14,6 +14,10 @@ Contents (all from the reference's code):
   bf_*       Grid::generateStencilsBruteForce, 400 nodes, n = 15, with max_st_radius 0.2
   hash_*     Grid::generateStencilsHash, 600 nodes, n = 20, 8x12x6 overlay (order, stencils, lengths)
   norms_*    norms.cpp l1/l2/linf with calcSolNorms' relative rule on seeded vectors
+  core_*     the reference's RBFFD + CosineBell + TimeDependentPDE (oracle/ref_rbffd.cpp):
+             300 nodes, n = 13, eps = 0.4 / h, LAMBDA, THETA, HV (k = 4, gamma = 1e-3, dim 2):
+             k-d tree stencils, the stored weights (n + 1 per row), applyWeightsForDeriv of a
+             smooth field per operator, and the cosine bell after 1 and 5 RK4 steps of 1036.8 s
 """
 import ctypes
 import os
@@ -30,7 +34,7 @@ import rbffd_gpu_b200 as R  # noqa: E402
 def main():
     L = O.ref_lib("ref_rbf")
     if L is None or O.ref_lib("ref_kdtree") is None or O.ref_lib("ref_grid") is None or \
-            O.ref_lib("ref_norms") is None:
+            O.ref_lib("ref_norms") is None or not O.RefRBFFD.available():
         sys.exit("the reference libraries are not built (python -c 'import oracle.build as b; b.build()')")
     out = {}
     rng = np.random.default_rng(2024)
@@ -65,6 +69,20 @@ def main():
     exact[3] = 0.0  # the calcSolNorms rule for exact norms below 1e-10
     out["norms_sol"], out["norms_exact"] = sol, exact
     out["norms_vals"] = np.array([O.ref_sol_norms(sol[i], exact[i]) for i in range(4)])
+    N, n = 300, 13
+    xyz = R.fibonacci_nodes(N, 21)
+    ref = O.RefRBFFD(xyz, n, O.LAMBDA | O.THETA, 0.4 / np.sqrt(4 * np.pi / N), dim=2, hv_k=4, hv_gamma=1e-3,
+                     use_hv=True)
+    out["core_xyz"], out["core_st"] = xyz, ref.stencils
+    u = np.sin(3 * xyz[:, 0]) + xyz[:, 1] * xyz[:, 2]
+    for name, t in (("lambda", O.LAMBDA), ("theta", O.THETA), ("hv", O.HV)):
+        out["core_w_" + name] = ref.weights(t)
+        out["core_apply_" + name] = ref.apply(t, u)
+    h0 = R.exact_cosine_bell(xyz)
+    out["core_h0"] = h0
+    out["core_rk4_1"] = ref.rk4(O.RefRBFFD.KIND_COSINE_BELL, h0, 1036.8, 1)
+    out["core_rk4_5"] = ref.rk4(O.RefRBFFD.KIND_COSINE_BELL, h0, 1036.8, 5)
+    ref.close()
     np.savez_compressed(os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_outputs.npz"), **out)
 
 

@@ -52,3 +52,27 @@ def test_sol_norms_equal_reference_outputs(row):
     got = R.sol_norms(GOLDEN["norms_sol"][row], GOLDEN["norms_exact"][row])
     keys = ("l1", "l1_rel", "l2", "l2_rel", "linf", "linf_rel")
     assert np.array_equal(np.array([got[k] for k in keys]), GOLDEN["norms_vals"][row])
+
+
+def test_oracle_core_equals_reference_outputs():
+    """The reference's RBFFD weights, applyWeightsForDeriv and CosineBell RK4
+    (src/rbffd/rbffd.cpp, src/pdes/time_dependent_pde.cpp,
+    src/pdes/hyperbolic/cosine_bell.cpp, compiled from its sources) on 300
+    nodes: the oracle with the constant basis and the reference's arithmetic
+    (oracle.reference_arithmetic) reproduces them bit for bit."""
+    xyz, st = GOLDEN["core_xyz"], GOLDEN["core_st"]
+    N, n = st.shape
+    assert np.array_equal(R.knn_stencils(xyz, n), st)
+    W = O.weights(xyz, st, None, 0.4 / np.sqrt(4 * np.pi / N), O.LAMBDA | O.THETA | O.HV, dim=2, poly_deg=0,
+                  hv_k=4, hv_scale=-1e-3 * float(N) ** -4.0)
+    u = np.sin(3 * xyz[:, 0]) + xyz[:, 1] * xyz[:, 2]
+    with O.reference_arithmetic():
+        for name, t in (("lambda", O.LAMBDA), ("theta", O.THETA), ("hv", O.HV)):
+            assert np.array_equal(W[t], GOLDEN["core_w_" + name][:, :n]), name
+            assert np.array_equal(O.apply(st, None, W[t], u), GOLDEN["core_apply_" + name]), name
+        h0 = GOLDEN["core_h0"]
+        assert np.array_equal(R.exact_cosine_bell(xyz), h0)
+        cu, cv = O.cosine_bell_coeffs(xyz, 1.0, np.pi / 2, 2 * np.pi / 1036800.0)
+        for k in (1, 5):
+            got = O.rk4_advect(st, None, W[O.LAMBDA], W[O.THETA], W[O.HV], cu, cv, h0, 1036.8, k)
+            assert np.array_equal(got, GOLDEN["core_rk4_%d" % k]), k

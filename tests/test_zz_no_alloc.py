@@ -13,6 +13,10 @@ larger than its fixed array are refused.
 This file is named so that pytest collects it last.
 """
 import ctypes
+import json
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -95,3 +99,56 @@ def test_noalloc_rejects_grids_beyond_its_fixed_scratch(ctx):
     assert rc == -1
     assert b"at most 262144" in ctx.L.rbffd_ctx_last_error(ctx.h)
     grid.close()
+
+
+_FRESH = r"""
+import ctypes, json, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import torch
+import rbffd_gpu_b200 as R
+
+ctx = R.Context(0)  # loads the allocation-free path's device code on this GPU
+
+
+def heat_grid(N, seed):
+    xyz = R.fibonacci_nodes(N, seed)
+    grid = R.Grid(ctx, xyz, R.knn_stencils(xyz, 31))
+    der = R.RBFFD(R.LSFC, grid, 2)
+    der.setEpsilon(0.25 / np.sqrt(4 * np.pi / N))
+    der.setPolynomialDegree(2)
+    der.computeAllWeightsForAllStencils()
+    u = torch.tensor(R.exact_sph_heat(xyz, 4, np.ones(25), 0.0), dtype=torch.float64, device="cuda")
+    return grid, der, u
+
+
+def call(grid, u):
+    ctx.check(ctx.L.rbffd_heat_rk4_noalloc(grid.h, R.F64, 1.0, 1e-5, 3, ctypes.c_void_p(u.data_ptr())), "noalloc")
+
+
+free = []
+g1, d1, u1 = heat_grid(4096, 1)
+torch.cuda.synchronize()
+free.append(ctx.mem_info()[1])
+call(g1, u1)  # the first call on this device in this process
+free.append(ctx.mem_info()[1])
+g2, d2, u2 = heat_grid(10242, 3)  # a new grid, allocated before the next reading
+torch.cuda.synchronize()
+free.append(ctx.mem_info()[1])
+call(g2, u2)
+free.append(ctx.mem_info()[1])
+print(json.dumps(free))
+"""
+
+
+def test_noalloc_takes_no_device_memory_in_a_fresh_process():
+    """In a process of its own (nothing else has run): once the context
+    exists, neither the first call of the entry point nor a later call on a
+    new grid changes the GPU's free memory (cudaMemGetInfo) -- no allocation,
+    and no module loaded by the call."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _FRESH, root], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    f0, f1, f2, f3 = json.loads(r.stdout.strip().splitlines()[-1])
+    assert f1 == f0, "first call changed free device memory by %d bytes" % (f0 - f1)
+    assert f3 == f2, "second call changed free device memory by %d bytes" % (f2 - f3)
