@@ -76,6 +76,23 @@ int rbffd_ctx_synchronize(rbffd_ctx* ctx);
 int rbffd_ctx_mem_info(rbffd_ctx* ctx, size_t* held, size_t* free_bytes, size_t* total_bytes);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own work after ours. */
 int rbffd_ctx_stream(rbffd_ctx* ctx, void** stream);
+/* FP64 arithmetic of the derivative application and time stepping.
+ *   RBFFD_ARITH_FUSED (default): every multiply-add of the SpMV, the
+ *     right-hand side and the RK4 update is one fused multiply-add;
+ *   RBFFD_ARITH_UNFUSED: every such multiply-add is a rounded product, then a
+ *     rounded sum, in the reference's source order -- the arithmetic of the
+ *     reference's RBFFD::applyWeightsForDeriv (rbffd.cpp:669-688),
+ *     CosineBell::solve (cosine_bell.cpp:47-57), VortexRollup::solve and
+ *     TimeDependentPDE::advanceRungeKutta4 (time_dependent_pde.cpp:172-304) as
+ *     the reference's own build compiles them (g++ -O3 for x86-64, which has no
+ *     FMA instruction): with it the device's FP64 results equal that build's
+ *     bit for bit.  One lane per stencil row, gathers from global memory.
+ * The context's setting applies to FP64 rbffd_apply / rbffd_apply_dev calls
+ * and to FP64 one-tracer PDEs created after it; rbffd_pde_set_arithmetic sets
+ * one PDE's (FP64, one tracer).  FP32 paths are unaffected. */
+enum { RBFFD_ARITH_FUSED = 0, RBFFD_ARITH_UNFUSED = 1 };
+int rbffd_ctx_set_arithmetic(rbffd_ctx* ctx, int arith);
+int rbffd_ctx_get_arithmetic(rbffd_ctx* ctx, int* arith);
 
 /* ---- host-side inputs (no GPU) ----------------------------------------- */
 /* N Fibonacci-spiral points on the unit sphere under a seeded uniform random
@@ -263,6 +280,24 @@ int rbffd_eig_classify(const double* re, int n, double zero_tol, rbffd_eig_outpu
 #define RBFFD_EIG_MAX_N 16384
 int rbffd_eigenvalues(rbffd_grid* grid, unsigned der_type, int use_hv, double* eig_re, double* eig_im,
                       rbffd_eig_output* out, double* max_neg_eig);
+/* The rightmost eigenvalues (largest real part) of the operator der_type
+ * (+ RBFFD_HV when use_hv) on grids too large for the dense check: the
+ * stability question of RBFFD::computeEigenvalues (rbffd.cpp:703-873) -- any
+ * eigenvalue with positive real part? -- answered by implicitly restarted
+ * Arnoldi on the device's FP64 sliced-ELL operator (basis of ncv vectors,
+ * classical Gram-Schmidt with reorthogonalisation, exact shifts, a seeded
+ * start vector).  Writes the nev rightmost Ritz values (re, im; rightmost
+ * first) and their residual estimates; *nconv of them met
+ * |h_{m+1,m}| |e_m^T y| <= tol * max(|theta|, 1e-3 |theta_max|).  nev >= 1,
+ * nev + 2 <= ncv <= 256, ncv < N. */
+int rbffd_eigen_rightmost(rbffd_grid* grid, unsigned der_type, int use_hv, int nev, int ncv, double tol,
+                          int max_restarts, unsigned long long seed, double* re, double* im, double* ritz_resid,
+                          int* nconv, int* restarts, int* matvecs);
+/* Eigenvalues of a real upper Hessenberg n x n matrix (row-major), by the
+ * shifted QR algorithm in complex arithmetic (the projected problem of
+ * rbffd_eigen_rightmost); host only.  RBFFD_ERR_UNSUPPORTED if it does not
+ * converge. */
+int rbffd_hessenberg_eigenvalues(int n, const double* H, double* re, double* im);
 
 /* ---- apply (derivative evaluation) ------------------------------------- */
 /* deriv[i] = sum_s w[i][s] * u[st_i[s]] for i in [start, start+count):
@@ -359,6 +394,13 @@ int rbffd_pde_advance(rbffd_pde* pde, int scheme, double dt, int nsteps, int fla
  * must be serialised by the caller.  Runs on the context stream and returns
  * after the steps complete. */
 int rbffd_heat_rk4_noalloc(rbffd_grid* grid, int dtype, double kappa, double dt, int nsteps, void* u_dev);
+/* The FP64 arithmetic of this PDE (RBFFD_ARITH_*, see rbffd_ctx_set_arithmetic);
+ * RBFFD_ARITH_UNFUSED needs an FP64 one-tracer PDE (else RBFFD_ERR_UNSUPPORTED)
+ * and fixes the stage kernel to one lane per row (set_shape may still pick the
+ * block size; tiled shapes are refused).  Setting RBFFD_ARITH_FUSED returns the
+ * PDE to the autotuned shape. */
+int rbffd_pde_set_arithmetic(rbffd_pde* pde, int arith);
+int rbffd_pde_get_arithmetic(rbffd_pde* pde, int* arith);
 /* Kernel-shape choice for this PDE's stage kernel (lanes per stencil row and
  * threads per block); 0 = autotuned. */
 int rbffd_pde_set_shape(rbffd_pde* pde, int lanes_per_row, int block_threads);

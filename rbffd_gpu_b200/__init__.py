@@ -8,11 +8,11 @@ by the tests and the benchmark.  The C++ view for drop-in use is in
 rbffd_gpu_b200/cpp/.
 """
 from .api import (  # noqa: F401
-    F32, F64, X, Y, Z, LAPL, R, HV, LAMBDA, THETA, LSFC, XSFC, YSFC, ZSFC, INTERP, ALT_XSFC, ALT_YSFC, ALT_ZSFC, RK4,
+    F32, F64, ARITH_FUSED, ARITH_UNFUSED, X, Y, Z, LAPL, R, HV, LAMBDA, THETA, LSFC, XSFC, YSFC, ZSFC, INTERP, ALT_XSFC, ALT_YSFC, ALT_ZSFC, RK4,
     RbffdError, Context, Grid, RBFFD, TimeDependentPDE, CosineBell, HeatSphere, Advection, VortexRollup,
     vortex_rollup_coefficients, exact_vortex_rollup, sol_norms,
     fibonacci_nodes, knn_stencils, knn_stencils_gpu, generate_stencils, generate_stencils_gpu, variable_epsilon, ST_BRUTE_FORCE, ST_KDTREE, ST_HASH,
     write_weights_file, read_weights_file, exact_cosine_bell,
-    exact_sph_heat, device_count, version, eig_classify, node_order, stencils_hash, ORDER_MORTON, ORDER_RCM, ORDER_GIVEN,
+    exact_sph_heat, device_count, version, eig_classify, hessenberg_eigenvalues, node_order, stencils_hash, ORDER_MORTON, ORDER_RCM, ORDER_GIVEN,
     Server, heat_params, cosine_bell_params, ERR_OOM, ERR_TIMEOUT, ERR_BUDGET, ERR_CANCELLED,
 )

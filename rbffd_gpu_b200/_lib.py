@@ -55,6 +55,8 @@ PROTOTYPES = {
     "rbffd_ctx_synchronize": (c_int, [c_void_p]),
     "rbffd_ctx_mem_info": (c_int, [c_void_p, P(c_size_t), P(c_size_t), P(c_size_t)]),
     "rbffd_ctx_stream": (c_int, [c_void_p, P(c_void_p)]),
+    "rbffd_ctx_set_arithmetic": (c_int, [c_void_p, c_int]),
+    "rbffd_ctx_get_arithmetic": (c_int, [c_void_p, ip]),
     "rbffd_nodes_fibonacci": (c_int, [c_int, c_uint64, dp]),
     "rbffd_stencils_knn": (c_int, [dp, c_int, c_int, ip, ip, c_int]),
     "rbffd_stencils_generate": (c_int, [dp, c_int, c_int, c_int, c_double, ip, ip, ip, c_int]),
@@ -80,6 +82,9 @@ PROTOTYPES = {
     "rbffd_weights_file_read": (c_int, [c_char_p, c_int, c_int, c_int, ip, ip, dp]),
     "rbffd_eig_classify": (c_int, [dp, c_int, c_double, c_void_p, dp]),
     "rbffd_eigenvalues": (c_int, [c_void_p, c_uint, c_int, dp, dp, c_void_p, dp]),
+    "rbffd_eigen_rightmost": (c_int, [c_void_p, c_uint, c_int, c_int, c_int, c_double, c_int, ctypes.c_ulonglong, dp,
+                                      dp, dp, ip, ip, ip]),
+    "rbffd_hessenberg_eigenvalues": (c_int, [c_int, dp, dp, dp]),
     "rbffd_apply": (c_int, [c_void_p, c_uint, c_int, c_uint, c_uint, dp, dp]),
     "rbffd_apply_dev": (c_int, [c_void_p, c_uint, c_int, c_int, c_void_p, c_void_p]),
     "rbffd_batched_gesv_dev": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
@@ -91,6 +96,8 @@ PROTOTYPES = {
     "rbffd_pde_get_time": (c_int, [c_void_p, dp]),
     "rbffd_pde_advance": (c_int, [c_void_p, c_int, c_double, c_int, c_int]),
     "rbffd_pde_set_shape": (c_int, [c_void_p, c_int, c_int]),
+    "rbffd_pde_set_arithmetic": (c_int, [c_void_p, c_int]),
+    "rbffd_pde_get_arithmetic": (c_int, [c_void_p, ip]),
     "rbffd_pde_set_fused_operator": (c_int, [c_void_p, c_int]),
     "rbffd_pde_set_tiled_shape": (c_int, [c_void_p, c_int, c_int, c_int]),
     "rbffd_pde_get_tiling": (c_int, [c_void_p, ip]),

@@ -14,6 +14,9 @@ import numpy as np
 from . import _lib
 
 F32, F64 = 0, 1
+# FP64 arithmetic of the apply and time-stepping kernels (rbffd_ctx_set_arithmetic):
+# fused multiply-adds (default), or rounded products then sums, the reference build's arithmetic
+ARITH_FUSED, ARITH_UNFUSED = 0, 1
 X, Y, Z, LAPL, R, HV, LAMBDA, THETA = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20, 0x40, 0x80
 LSFC, XSFC, YSFC, ZSFC, INTERP = 0x100, 0x200, 0x400, 0x800, 0x8000
 ALT_XSFC, ALT_YSFC, ALT_ZSFC = 0x1000, 0x2000, 0x4000
@@ -216,6 +219,18 @@ def node_order(method, xyz=None, stencils=None, st_len=None):
     return order
 
 
+def hessenberg_eigenvalues(H):
+    """Eigenvalues of a real upper Hessenberg matrix (the Arnoldi check's
+    projected problem; shifted QR in complex arithmetic, host only)."""
+    H = _f64(H)
+    n = H.shape[0]
+    re, im = np.zeros(n), np.zeros(n)
+    rc = _lib.load().rbffd_hessenberg_eigenvalues(n, _dp(H), _dp(re), _dp(im))
+    if rc:
+        raise RbffdError(rc, "rbffd_hessenberg_eigenvalues")
+    return re + 1j * im
+
+
 def eig_output_dict(o):
     return {k: getattr(o, k) for k, _ in _lib.EigOutput._fields_}
 
@@ -289,6 +304,17 @@ class Context:
         held, free, total = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t()
         self.check(self.L.rbffd_ctx_mem_info(self.h, ctypes.byref(held), ctypes.byref(free), ctypes.byref(total)))
         return held.value, free.value, total.value
+
+    def setArithmetic(self, arith):
+        """FP64 arithmetic of rbffd_apply* calls and of FP64 one-tracer PDEs
+        created afterwards: ARITH_FUSED, or ARITH_UNFUSED (the reference's own
+        build: a rounded product, then a rounded sum)."""
+        self.check(self.L.rbffd_ctx_set_arithmetic(self.h, arith), "set_arithmetic")
+
+    def getArithmetic(self):
+        a = ctypes.c_int()
+        self.check(self.L.rbffd_ctx_get_arithmetic(self.h, ctypes.byref(a)))
+        return a.value
 
     def stream(self):
         s = ctypes.c_void_p()
@@ -489,6 +515,22 @@ class RBFFD:
             raise RbffdError(-1, "computeEigenvalues: eigenvalues of both signs or more than one zero: %r" % res)
         return (ret.value, re + 1j * im) if return_eigenvalues else ret.value
 
+    def computeRightmostEigenvalues(self, which, nev=6, ncv=40, tol=1e-8, max_restarts=3000, seed=1):
+        """The nev rightmost eigenvalues of `which` (+ HV when hyperviscosity
+        is on) by implicitly restarted Arnoldi on the device's sparse operator
+        (rbffd_eigen_rightmost): the stability verdict of computeEigenvalues
+        for grids too large for the dense check.  Returns a dict with the
+        eigenvalues (complex, rightmost first), their residual estimates, how
+        many converged, restarts and operator applications."""
+        g = self.grid
+        re, im, rs = np.zeros(nev), np.zeros(nev), np.zeros(nev)
+        nconv, restarts, mv = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        g.ctx.check(g.ctx.L.rbffd_eigen_rightmost(g.h, which, int(bool(self.useHyperviscosity)), nev, ncv, tol,
+                                                  max_restarts, seed, _dp(re), _dp(im), _dp(rs), ctypes.byref(nconv),
+                                                  ctypes.byref(restarts), ctypes.byref(mv)), "rbffd_eigen_rightmost")
+        return {"eigenvalues": re + 1j * im, "residual_estimates": rs, "nconv": nconv.value,
+                "restarts": restarts.value, "matvecs": mv.value}
+
     def getEigenvalues(self):
         if getattr(self, "cachedEigenvalues", None) is None:
             self.computeEigenvalues(LAPL, False)
@@ -581,6 +623,16 @@ class TimeDependentPDE:
 
     def setShape(self, lanes_per_row=0, block_threads=0):
         self.ctx.check(self.ctx.L.rbffd_pde_set_shape(self.h, lanes_per_row, block_threads), "set_shape")
+
+    def setArithmetic(self, arith):
+        """ARITH_UNFUSED (FP64, one tracer): the reference build's arithmetic,
+        one lane per stencil row; ARITH_FUSED: fused multiply-adds, autotuned shape."""
+        self.ctx.check(self.ctx.L.rbffd_pde_set_arithmetic(self.h, arith), "set_arithmetic")
+
+    def getArithmetic(self):
+        a = ctypes.c_int()
+        self.ctx.check(self.ctx.L.rbffd_pde_get_arithmetic(self.h, ctypes.byref(a)))
+        return a.value
 
     def getShape(self):
         """(lanes per row, threads per block, rows per tiled block or 0)."""
@@ -688,11 +740,15 @@ class Server:
         self.h = h
         self._out = {}
 
-    def submit(self, grid, params, u0, dt, nsteps, cu=None, cv=None):
-        """Queue a request; returns its id.  Raises RbffdError on a refused request."""
+    def submit(self, grid, params, u0, dt, nsteps, cu=None, cv=None, out=None):
+        """Queue a request; returns its id.  Raises RbffdError on a refused request.
+        out: a float64 array of grid.N values that receives the result (by
+        default a new one, returned by result())."""
         u = _f64(u0)
         assert u.shape == (grid.N,)
-        out = np.zeros(grid.N)
+        if out is None:
+            out = np.zeros(grid.N)
+        assert out.dtype == np.float64 and out.shape == (grid.N,) and out.flags.c_contiguous
         keep = [u, out]
         if cu is not None:
             a, b = _f64(cu), _f64(cv)

@@ -312,6 +312,7 @@ extern "C" int rbffd_grid_destroy(rbffd_grid* g)
     rbffd_ctx* ctx = g->ctx;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    weights_work_free(g);
     size_t wsz = (size_t)g->N32 * g->n4;
     for (int t = 0; t < 16; t++) {
         dev_free(ctx, g->d_w64[t], wsz * sizeof(double));
@@ -887,7 +888,9 @@ extern "C" int rbffd_weights_get(rbffd_grid* g, unsigned der_type, double* w)
 // accumulation order is the reference's (s = 0 .. n-1, rbffd.cpp:680-684) and
 // FP64 results equal those of a fused-multiply-add CPU loop.
 
-template <typename T, int G>
+// PLAIN: each multiply-add rounded twice, product then sum (madd, ell.cuh):
+// the reference's own build, whose x86-64 flags have no FMA.
+template <typename T, int G, bool PLAIN = false>
 __global__ void __launch_bounds__(256) k_ell_apply(const int* __restrict__ idx, const T* __restrict__ w, int nc,
                                                    const T* __restrict__ u, T* __restrict__ out, int start, int count,
                                                    int T_tr)
@@ -904,10 +907,10 @@ __global__ void __launch_bounds__(256) k_ell_apply(const int* __restrict__ idx, 
             int4 j = ld_idx4(idx + o);
             T wv[4];
             ld_w4(w + o, wv);
-            acc = fma_rn<T>(wv[0], __ldg(u + (size_t)j.x * T_tr + t), acc);
-            acc = fma_rn<T>(wv[1], __ldg(u + (size_t)j.y * T_tr + t), acc);
-            acc = fma_rn<T>(wv[2], __ldg(u + (size_t)j.z * T_tr + t), acc);
-            acc = fma_rn<T>(wv[3], __ldg(u + (size_t)j.w * T_tr + t), acc);
+            acc = madd<T, PLAIN>(wv[0], __ldg(u + (size_t)j.x * T_tr + t), acc);
+            acc = madd<T, PLAIN>(wv[1], __ldg(u + (size_t)j.y * T_tr + t), acc);
+            acc = madd<T, PLAIN>(wv[2], __ldg(u + (size_t)j.z * T_tr + t), acc);
+            acc = madd<T, PLAIN>(wv[3], __ldg(u + (size_t)j.w * T_tr + t), acc);
         }
     }
     acc = group_sum<G>(acc);
@@ -940,6 +943,33 @@ int grid_apply_dev(rbffd_grid* g, int op, int dtype, int T_tr, const void* u, vo
         launch_apply<float>(g, g->d_w32[op], (const float*)u, (float*)out, start, count, T_tr, G, s);
     }
     RBFFD_CUDA_TRY(g->ctx, cudaGetLastError());
+    return RBFFD_OK;
+}
+
+int grid_apply_dev_plain(rbffd_grid* g, int op, int T_tr, const double* u, double* out, int start, int count,
+                         cudaStream_t s)
+{
+    if (!g->d_w64[op]) return set_error(g->ctx, RBFFD_ERR_STATE, "weights of operator bit %d not computed", op);
+    long long threads = (long long)count * T_tr;
+    int nb = (int)((threads + 255) / 256);
+    k_ell_apply<double, 1, true><<<nb, 256, 0, s>>>(g->d_idx, g->d_w64[op], g->nc, u, out, start, count, T_tr);
+    RBFFD_CUDA_TRY(g->ctx, cudaGetLastError());
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_ctx_set_arithmetic(rbffd_ctx* ctx, int arith)
+{
+    if (!ctx) return RBFFD_ERR_INVALID;
+    if (arith != RBFFD_ARITH_FUSED && arith != RBFFD_ARITH_UNFUSED)
+        return set_error(ctx, RBFFD_ERR_INVALID, "unknown arithmetic %d", arith);
+    ctx->arith = arith;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_ctx_get_arithmetic(rbffd_ctx* ctx, int* arith)
+{
+    if (!ctx || !arith) return RBFFD_ERR_INVALID;
+    *arith = ctx->arith;
     return RBFFD_OK;
 }
 
@@ -984,7 +1014,8 @@ extern "C" int rbffd_apply(rbffd_grid* g, unsigned der_type, int dtype, unsigned
     if (e == cudaSuccess) rc = grid_to_internal(g, du, dd, 1, 8, s);
     if (e == cudaSuccess && rc == RBFFD_OK) {
         if (dtype == RBFFD_F64) {
-            rc = grid_apply_dev(g, op, dtype, 1, dd, du, 0, N, 1, s);
+            rc = ctx->arith == RBFFD_ARITH_UNFUSED ? grid_apply_dev_plain(g, op, 1, dd, du, 0, N, s)
+                                                   : grid_apply_dev(g, op, dtype, 1, dd, du, 0, N, 1, s);
         } else {
             k_d2f<<<(N + 255) / 256, 256, 0, s>>>(dd, fu, N);
             rc = grid_apply_dev(g, op, dtype, 1, fu, fd, 0, N, 1, s);
@@ -1024,7 +1055,10 @@ extern "C" int rbffd_apply_dev(rbffd_grid* g, unsigned der_type, int dtype, int 
     }
     cudaStream_t s = ctx->stream;
     rc = grid_to_internal(g, u_dev, tin, ntracers, es, s);
-    if (rc == RBFFD_OK) rc = grid_apply_dev(g, op, dtype, ntracers, tin, tout, 0, g->N, 1, s);
+    if (rc == RBFFD_OK)
+        rc = dtype == RBFFD_F64 && ctx->arith == RBFFD_ARITH_UNFUSED
+                 ? grid_apply_dev_plain(g, op, ntracers, (const double*)tin, (double*)tout, 0, g->N, s)
+                 : grid_apply_dev(g, op, dtype, ntracers, tin, tout, 0, g->N, 1, s);
     if (rc == RBFFD_OK) rc = grid_to_caller(g, tout, deriv_dev, ntracers, es, s);
     cudaError_t e = cudaStreamSynchronize(s);
     dev_free(ctx, tin, bytes);

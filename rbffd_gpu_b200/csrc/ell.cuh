@@ -90,6 +90,16 @@ struct Ar<float> {
     static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
 };
 
+// a*b + c with one rounding (PLAIN = false: the fused multiply-add), or with
+// two, product then sum (PLAIN = true: the arithmetic of a CPU build without
+// FMA instructions, such as the reference's own x86-64 build).
+template <typename T, bool PLAIN>
+__device__ __forceinline__ T madd(T a, T b, T c)
+{
+    if (PLAIN) return Ar<T>::add(Ar<T>::mul(a, b), c);
+    return Ar<T>::fma(a, b, c);
+}
+
 // Sum of G lanes' partial values (lanes of a group are consecutive in the warp).
 template <int G, typename T>
 __device__ __forceinline__ T group_sum(T v)

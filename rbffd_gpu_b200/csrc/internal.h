@@ -37,6 +37,8 @@ struct Shape {
     int tma = 0;   // tiled kernel that streams weights and indices into shared memory with bulk copies
     int sched = 0; // tiled, FP32, one operator: each row reads its slots in the halo's conflict-avoiding schedule
     int pf = 0;    // tiled, one lane per row: upcoming chunks of weights and indices prefetched into L2
+    int plain = 0; // FP64, one tracer, one lane per row, global gathers: the reference build's arithmetic
+                   // (every multiply-add a rounded product, then a rounded sum; RBFFD_ARITH_UNFUSED)
 };
 
 // Device status word of a context: kernels whose waits are bounded write a
@@ -53,6 +55,7 @@ struct rbffd_ctx {
     std::mutex mu;
     std::map<TuneKey, Shape> tuned;  // autotuner results per problem shape
     int* d_status = nullptr;         // DEV_STATUS_* written by kernels with bounded waits
+    int arith = 0;                   // RBFFD_ARITH_*: FP64 arithmetic of rbffd_apply* and of new FP64 PDEs
 };
 
 // Read and clear the context's device status; RBFFD_ERR_TIMEOUT if a kernel gave up waiting.
@@ -78,13 +81,18 @@ struct rbffd_grid {
     std::vector<int> h_iperm;      // caller's node index -> internal row
     std::vector<int> h_len;        // stencil lengths, internal order
     std::map<int, struct Halo*> halos;  // per rows-per-block R, built on first use
+    struct WeightsWork* ww = nullptr;   // the weight solver's device workspace and captured launch (weights.cu)
     size_t bytes = 0;
 };
+void weights_work_free(rbffd_grid* g);
 
 // Move [N][T] values (elem_bytes each) between the caller's node order and the
 // grid's internal order (device arrays, on stream s).
 int grid_to_internal(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s);
 int grid_to_caller(rbffd_grid* g, const void* src, void* dst, int T, int elem_bytes, cudaStream_t s);
+// FP64 ELL apply with plain (unfused) multiply-adds, one lane per row (core.cu).
+int grid_apply_dev_plain(rbffd_grid* g, int op, int T_tr, const double* u, double* out, int start, int count,
+                         cudaStream_t s);
 // Load (under lazy module loading) the device code of the permutation
 // kernels / of the allocation-free heat RK4 path on the current device.
 int grid_permute_preload();
@@ -157,6 +165,7 @@ struct rbffd_pde {
     double t = 0.0;
     Shape shape;
     bool forced = false;
+    int arith = 0;  // RBFFD_ARITH_*
     cudaGraphExec_t gexec = nullptr;
     double g_dt = 0.0;
     int g_steps = 0;

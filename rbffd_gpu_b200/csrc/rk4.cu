@@ -51,14 +51,16 @@ struct StageParams {
     int N, nc, T_tr, stage;  // nc: 4-slot chunks per row (sliced ELL, ell.cuh)
 };
 
-// Right-hand side and the stage update for one (row, tracer) value.
-template <typename T, int KIND, bool HV>
+// Right-hand side and the stage update for one (row, tracer) value.  PLAIN:
+// every multiply-add rounded twice (madd, ell.cuh), the reference build's
+// arithmetic; otherwise fused.
+template <typename T, int KIND, bool HV, bool PLAIN = false>
 __device__ __forceinline__ void stage_update(const StageParams<T>& p, int i, size_t e, T d0, T d1, T d2, T cu, T cv)
 {
     T f;
     if (KIND == KIND_ADVECT) {
         // CosineBell::solve: f = -((vel_u/a) * dlambda + (vel_v/a) * dtheta) (+ hv), cosine_bell.cpp:47-57
-        f = -Ar<T>::fma(cu, d0, Ar<T>::mul(cv, d1));
+        f = -madd<T, PLAIN>(cu, d0, Ar<T>::mul(cv, d1));
         if (HV) f = Ar<T>::add(f, d2);
     } else {
         f = Ar<T>::mul(p.kappa, d0);
@@ -67,22 +69,22 @@ __device__ __forceinline__ void stage_update(const StageParams<T>& p, int i, siz
     switch (p.stage) {
     case 0:
         p.acc[e] = f;
-        p.xnext[e] = Ar<T>::fma(p.c, f, ui);
+        p.xnext[e] = madd<T, PLAIN>(p.c, f, ui);
         break;
     case 1:
     case 2:
         p.acc[e] = Ar<T>::add(p.acc[e], Ar<T>::mul(T(2), f));
-        p.xnext[e] = Ar<T>::fma(p.c, f, ui);
+        p.xnext[e] = madd<T, PLAIN>(p.c, f, ui);
         break;
     default:
-        p.u[e] = Ar<T>::fma(p.c, Ar<T>::add(p.acc[e], f), ui);
+        p.u[e] = madd<T, PLAIN>(p.c, Ar<T>::add(p.acc[e], f), ui);
         break;
     }
 }
 
 // Single tracer, G lanes per row; lane g handles the 4-slot chunks g, g+G, ...
 // With G == 1 the slots are accumulated in stencil order.
-template <typename T, int KIND, bool HV, int G>
+template <typename T, int KIND, bool HV, int G, bool PLAIN = false>
 __global__ void __launch_bounds__(512) k_stage_scalar(StageParams<T> p)
 {
     int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -98,15 +100,15 @@ __global__ void __launch_bounds__(512) k_stage_scalar(StageParams<T> p)
         T w[4];
         ld_w4(p.w0 + o, w);
 #pragma unroll
-        for (int k = 0; k < 4; k++) d0 = Ar<T>::fma(w[k], x[k], d0);
+        for (int k = 0; k < 4; k++) d0 = madd<T, PLAIN>(w[k], x[k], d0);
         if (KIND == KIND_ADVECT) {
             ld_w4(p.w1 + o, w);
 #pragma unroll
-            for (int k = 0; k < 4; k++) d1 = Ar<T>::fma(w[k], x[k], d1);
+            for (int k = 0; k < 4; k++) d1 = madd<T, PLAIN>(w[k], x[k], d1);
             if (HV) {
                 ld_w4(p.w2 + o, w);
 #pragma unroll
-                for (int k = 0; k < 4; k++) d2 = Ar<T>::fma(w[k], x[k], d2);
+                for (int k = 0; k < 4; k++) d2 = madd<T, PLAIN>(w[k], x[k], d2);
             }
         }
     }
@@ -123,7 +125,7 @@ __global__ void __launch_bounds__(512) k_stage_scalar(StageParams<T> p)
         cu = p.cu[i];
         cv = p.cv[i];
     }
-    stage_update<T, KIND, HV>(p, i, (size_t)i, d0, d1, d2, cu, cv);
+    stage_update<T, KIND, HV, PLAIN>(p, i, (size_t)i, d0, d1, d2, cu, cv);
 }
 
 // Multiple tracers: state [N][T_tr]; VEC consecutive tracers per lane, loaded
@@ -218,13 +220,16 @@ constexpr int TILE_PF_DIST = 2;
 // where the weight stream comes from HBM and the kernel waits on it (FP64
 // multi-tracer stages); where the weights stay in L2 the extra instructions
 // cost more, so the autotuner decides.
-template <typename T, int VEC, int G, int KIND, bool HV, int PF = 0>
+// NV > 0: the vectors per node (T_tr / VEC) known at compile time, so node
+// offsets in shared memory and state indices are shifts, not multiplies.
+template <typename T, int VEC, int G, int KIND, bool HV, int PF = 0, int NV = 0>
 __global__ void __launch_bounds__(1024) k_stage_tile(StageParams<T> p, TileParams tp)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sx = reinterpret_cast<T*>(smem_raw);
     typedef typename VecT<T, VEC>::type V;
-    const int vpn = p.T_tr / VEC;  // vectors per node (= lanes per tracer group of a row)
+    const int vpn = NV > 0 ? NV : p.T_tr / VEC;  // vectors per node (= lanes per tracer group of a row)
+    const int ntr = NV > 0 ? NV * VEC : p.T_tr;
     const int L = vpn * G;         // threads per row
     const int b = blockIdx.x;
     const int h0 = __ldg(tp.ptr + b), hn = __ldg(tp.ptr + b + 1) - h0;
@@ -232,7 +237,7 @@ __global__ void __launch_bounds__(1024) k_stage_tile(StageParams<T> p, TileParam
         const int h = e / vpn, v = e - h * vpn;
         const int node = __ldg(tp.nodes + h0 + h);
         reinterpret_cast<V*>(sx)[(size_t)h * vpn + v] =
-            __ldg(reinterpret_cast<const V*>(p.x + (size_t)node * p.T_tr) + v);
+            __ldg(reinterpret_cast<const V*>(p.x + (size_t)node * ntr) + v);
     }
     __syncthreads();
     const int lr = threadIdx.x % L, rl = threadIdx.x / L;
@@ -301,7 +306,7 @@ __global__ void __launch_bounds__(1024) k_stage_tile(StageParams<T> p, TileParam
     }
 #pragma unroll
     for (int v = 0; v < VEC; v++)
-        stage_update<T, KIND, HV>(p, i, (size_t)i * p.T_tr + (size_t)tv * VEC + v, d0[v], d1[v], d2[v], cu, cv);
+        stage_update<T, KIND, HV>(p, i, (size_t)i * ntr + (size_t)tv * VEC + v, d0[v], d1[v], d2[v], cu, cv);
 }
 
 // Tiled stage kernel with bulk-copy streaming.  Same per-row arithmetic as
@@ -430,7 +435,7 @@ __global__ void __launch_bounds__(1024) k_stage_tma(StageParams<T> p, TileParams
 }
 
 // Unfused right-hand side + stage update from per-operator outputs (the plain path).
-template <typename T, int KIND, bool HV>
+template <typename T, int KIND, bool HV, bool PLAIN = false>
 __global__ void k_rhs_axpy(StageParams<T> p, const T* __restrict__ d0, const T* __restrict__ d1, const T* __restrict__ d2)
 {
     size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -441,7 +446,7 @@ __global__ void k_rhs_axpy(StageParams<T> p, const T* __restrict__ d0, const T* 
         cu = p.cu[i];
         cv = p.cv[i];
     }
-    stage_update<T, KIND, HV>(p, i, e, d0[e], KIND == KIND_ADVECT ? d1[e] : T(0), HV ? d2[e] : T(0), cu, cv);
+    stage_update<T, KIND, HV, PLAIN>(p, i, e, d0[e], KIND == KIND_ADVECT ? d1[e] : T(0), HV ? d2[e] : T(0), cu, cv);
 }
 
 // ---------------------------------------------------------------------------
@@ -595,6 +600,23 @@ static void launch_tile_v(const StageParams<T>& p, const TileParams& tp, const T
         k_stage_tile<T, VEC, 1, KIND, HV, TILE_PF_DIST><<<nb, t.threads, t.smem, s>>>(p, tp);
         return;
     }
+    // one lane per row with the common node widths: compile-time vectors per node
+    if (t.G == 1 && (t.vpn == 1 || t.vpn == 4 || t.vpn == 8)) {
+        if (t.vpn == 1) {
+            cudaFuncSetAttribute(k_stage_tile<T, VEC, 1, KIND, HV, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)t.smem);
+            k_stage_tile<T, VEC, 1, KIND, HV, 0, 1><<<nb, t.threads, t.smem, s>>>(p, tp);
+        } else if (t.vpn == 4) {
+            cudaFuncSetAttribute(k_stage_tile<T, VEC, 1, KIND, HV, 0, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)t.smem);
+            k_stage_tile<T, VEC, 1, KIND, HV, 0, 4><<<nb, t.threads, t.smem, s>>>(p, tp);
+        } else {
+            cudaFuncSetAttribute(k_stage_tile<T, VEC, 1, KIND, HV, 0, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)t.smem);
+            k_stage_tile<T, VEC, 1, KIND, HV, 0, 8><<<nb, t.threads, t.smem, s>>>(p, tp);
+        }
+        return;
+    }
     switch (t.G) {
     case 1:
         cudaFuncSetAttribute(k_stage_tile<T, VEC, 1, KIND, HV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem);
@@ -645,6 +667,12 @@ static void launch_stage_t(rbffd_pde* P, const StageParams<T>& p, Shape sh, cuda
         return;
     }
     int B = sh.block > 0 ? sh.block : 256;
+    if constexpr (std::is_same<T, double>::value) {
+        if (sh.plain) {  // the reference build's arithmetic: one tracer, one lane per row
+            k_stage_scalar<T, KIND, HV, 1, true><<<(P->g->N + B - 1) / B, B, 0, s>>>(p);
+            return;
+        }
+    }
     if (P->T == 1) {
         int G = sh.lanes > 0 ? sh.lanes : 1;
         long long threads = (long long)P->g->N * G;
@@ -688,13 +716,17 @@ static void launch_stage_any(rbffd_pde* P, int stage, double dt, Shape sh, cudaS
         launch_stage<float>(P, stage, dt, sh, s);
 }
 
-template <typename T>
-static int unfused_stage(rbffd_pde* P, int stage, double dt, cudaStream_t s)
+template <typename T, bool PLAIN>
+static int unfused_stage_t(rbffd_pde* P, int stage, double dt, cudaStream_t s)
 {
     int nops = P->kind == KIND_HEAT ? 1 : (P->use_hv ? 3 : 2);
     for (int k = 0; k < nops; k++) {
         StageParams<T> p = make_params<T>(P, stage, dt);
-        int rc = grid_apply_dev(P->g, P->op[k], P->dtype, P->T, p.x, P->d[k], 0, P->g->N, 1, s);
+        int rc;
+        if constexpr (PLAIN)
+            rc = grid_apply_dev_plain(P->g, P->op[k], P->T, p.x, (double*)P->d[k], 0, P->g->N, s);
+        else
+            rc = grid_apply_dev(P->g, P->op[k], P->dtype, P->T, p.x, P->d[k], 0, P->g->N, 1, s);
         if (rc) return rc;
     }
     StageParams<T> p = make_params<T>(P, stage, dt);
@@ -702,12 +734,20 @@ static int unfused_stage(rbffd_pde* P, int stage, double dt, cudaStream_t s)
     int nb = (int)((n + 255) / 256);
     const T *d0 = (const T*)P->d[0], *d1 = (const T*)P->d[1], *d2 = (const T*)P->d[2];
     if (P->kind == KIND_HEAT)
-        k_rhs_axpy<T, KIND_HEAT, false><<<nb, 256, 0, s>>>(p, d0, d1, d2);
+        k_rhs_axpy<T, KIND_HEAT, false, PLAIN><<<nb, 256, 0, s>>>(p, d0, d1, d2);
     else if (P->use_hv)
-        k_rhs_axpy<T, KIND_ADVECT, true><<<nb, 256, 0, s>>>(p, d0, d1, d2);
+        k_rhs_axpy<T, KIND_ADVECT, true, PLAIN><<<nb, 256, 0, s>>>(p, d0, d1, d2);
     else
-        k_rhs_axpy<T, KIND_ADVECT, false><<<nb, 256, 0, s>>>(p, d0, d1, d2);
+        k_rhs_axpy<T, KIND_ADVECT, false, PLAIN><<<nb, 256, 0, s>>>(p, d0, d1, d2);
     return RBFFD_OK;
+}
+
+template <typename T>
+static int unfused_stage(rbffd_pde* P, int stage, double dt, cudaStream_t s)
+{
+    if constexpr (std::is_same<T, double>::value)
+        if (P->arith == RBFFD_ARITH_UNFUSED) return unfused_stage_t<double, true>(P, stage, dt, s);
+    return unfused_stage_t<T, false>(P, stage, dt, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -1040,6 +1080,9 @@ extern "C" int rbffd_pde_create(rbffd_grid* g, const rbffd_pde_params* prm, rbff
         }
     RBFFD_CUDA_TRY(ctx, cudaMemsetAsync(P->u, 0, n, s));
     RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    // the context's FP64 arithmetic (rbffd_ctx_set_arithmetic) for PDEs it applies to
+    if (ctx->arith == RBFFD_ARITH_UNFUSED && P->dtype == RBFFD_F64 && P->T == 1)
+        rbffd_pde_set_arithmetic(P, RBFFD_ARITH_UNFUSED);
     *out = P;
     return RBFFD_OK;
 }
@@ -1124,16 +1167,45 @@ extern "C" int rbffd_pde_get_time(rbffd_pde* P, double* t)
 extern "C" int rbffd_pde_set_shape(rbffd_pde* P, int lanes, int block)
 {
     if (!P) return RBFFD_ERR_INVALID;
+    if (!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16)) return RBFFD_ERR_INVALID;
+    if (!(block == 0 || block == 64 || block == 128 || block == 256 || block == 512)) return RBFFD_ERR_INVALID;
+    if (P->arith == RBFFD_ARITH_UNFUSED) {  // one lane per row in stencil order; only the block size is free
+        if (lanes > 1)
+            return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "the unfused (reference) arithmetic uses one lane per row");
+        P->shape = Shape{1, block ? block : 256};
+        P->shape.plain = 1;
+        P->forced = true;
+        return RBFFD_OK;
+    }
     if (lanes == 0 && block == 0) {
         P->forced = false;
         P->shape = Shape{};
         return RBFFD_OK;
     }
-    if (!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16)) return RBFFD_ERR_INVALID;
-    if (!(block == 0 || block == 64 || block == 128 || block == 256 || block == 512)) return RBFFD_ERR_INVALID;
     if (P->T > 1 && lanes > 1) return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "lanes per row apply to one tracer only");
     P->shape = Shape{lanes ? lanes : 1, block ? block : 256, 0};
     P->forced = true;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_set_arithmetic(rbffd_pde* P, int arith)
+{
+    if (!P) return RBFFD_ERR_INVALID;
+    if (arith != RBFFD_ARITH_FUSED && arith != RBFFD_ARITH_UNFUSED)
+        return set_error(P->ctx, RBFFD_ERR_INVALID, "unknown arithmetic %d", arith);
+    if (arith == RBFFD_ARITH_UNFUSED && (P->dtype != RBFFD_F64 || P->T != 1))
+        return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "the unfused (reference) arithmetic is FP64 with one tracer");
+    P->arith = arith;
+    P->forced = false;
+    P->shape = Shape{};
+    if (arith == RBFFD_ARITH_UNFUSED) return rbffd_pde_set_shape(P, 1, 256);
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_pde_get_arithmetic(rbffd_pde* P, int* arith)
+{
+    if (!P || !arith) return RBFFD_ERR_INVALID;
+    *arith = P->arith;
     return RBFFD_OK;
 }
 
@@ -1148,6 +1220,8 @@ extern "C" int rbffd_pde_get_shape(rbffd_pde* P, int* lanes, int* block)
 extern "C" int rbffd_pde_set_tiled_shape(rbffd_pde* P, int rows_per_block, int lanes, int flags)
 {
     if (!P) return RBFFD_ERR_INVALID;
+    if (P->arith == RBFFD_ARITH_UNFUSED)
+        return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "the unfused (reference) arithmetic gathers from global memory");
     if (rows_per_block < 32 || rows_per_block > 1024 || rows_per_block % 32 || !(lanes == 1 || lanes == 2 || lanes == 4))
         return set_error(P->ctx, RBFFD_ERR_INVALID, "rows_per_block must be a multiple of 32, lanes 1, 2 or 4");
     if (flags & ~(RBFFD_TILE_STREAM_WEIGHTS | RBFFD_TILE_SLOT_SCHEDULE | RBFFD_TILE_PREFETCH))
@@ -1237,7 +1311,7 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
         if (full > 0) {
             if (!P->gexec || P->g_dt != dt || P->g_steps != chunk || P->g_shape.lanes != sh.lanes ||
                 P->g_shape.block != sh.block || P->g_shape.tile != sh.tile || P->g_shape.tma != sh.tma ||
-                P->g_shape.sched != sh.sched || P->g_shape.pf != sh.pf) {
+                P->g_shape.sched != sh.sched || P->g_shape.pf != sh.pf || P->g_shape.plain != sh.plain) {
                 if (P->gexec) {
                     cudaGraphExecDestroy(P->gexec);
                     P->gexec = nullptr;

@@ -45,6 +45,16 @@ constexpr int MAX_WARPS = 8;   // per team
 constexpr int MAX_M = 160;     // largest system (stencil + polynomial terms)
 constexpr int ELIM_CHUNKS = (MAX_M + MAX_K + 31) / 32;  // 32-column chunks of a row
 
+constexpr int MAX_CLASSES = 24;  // system sizes in one persistent launch
+
+// One system size in the persistent launch: its rows are rows[rows_off ..
+// rows_off + nrows), solved `teams` at a time per CTA by teams of `team`
+// threads, each holding its system at row stride lda in `stride` doubles of
+// shared memory; its work units are numbered from unit0.
+struct WClass {
+    int m, lda, team, teams, stride, blocked, rows_off, nrows, unit0;
+};
+
 struct WParams {
     const double4* xyz;
     const int* idx;
@@ -54,9 +64,12 @@ struct WParams {
     const int* rows;
     double* w[MAX_K];
     int* status;  // min(row) + 1 over rows with a zero pivot, INT_MAX if none
+    int* work;    // next work unit (the persistent launch's counter, zeroed before it)
     double eps_uniform, hv_scale;
     int n4, n_pad, deg_uniform, nrows, K, m, dim, hv_k, team_stride;  // n4: row stride; team_stride: doubles per team
     int opbit[MAX_K];
+    int nclasses, nunits;
+    WClass cls[MAX_CLASSES];
 };
 
 struct Team {
@@ -302,11 +315,12 @@ __device__ void team_pivot_column0(const Team& T, const double* a, int m, int ld
 }
 
 // Returns 0, or k + 1 when the pivot column at step k is exactly zero (dgetrf's INFO).
-__device__ int team_eliminate(const Team& T, double* a, int m, int K, double* cand_v, int* cand_r)
+// a: m rows of ld = m + K columns at row stride lda (>= ld).
+__device__ int team_eliminate(const Team& T, double* a, int m, int K, int lda, double* cand_v, int* cand_r)
 {
     const int ld = m + K;
     const int nw = T.nwarps(), w = T.warp(), lane = T.lane();
-    team_pivot_column0(T, a, m, ld, cand_v, cand_r);
+    team_pivot_column0(T, a, m, lda, cand_v, cand_r);
     T.sync();
     for (int k = 0; k < m; k++) {
         // reduce the per-warp candidates (every thread, identical result)
@@ -320,15 +334,15 @@ __device__ int team_eliminate(const Team& T, double* a, int m, int K, double* ca
         if (!(bv > 0.0)) return k + 1;  // exactly zero (or NaN) pivot column
         if (p != k)
             for (int j = k + T.tid; j < ld; j += T.size) {
-                double t = a[k * ld + j];
-                a[k * ld + j] = a[p * ld + j];
-                a[p * ld + j] = t;
+                double t = a[k * lda + j];
+                a[k * lda + j] = a[p * lda + j];
+                a[p * lda + j] = t;
             }
         T.sync();
-        const double piv = a[k * ld + k];
+        const double piv = a[k * lda + k];
         // the multipliers of all rows at once, one division per thread, kept in
         // column k (where LAPACK keeps L; nothing reads it afterwards)
-        for (int i = k + 1 + T.tid; i < m; i += T.size) a[i * ld + k] = a[i * ld + k] / piv;
+        for (int i = k + 1 + T.tid; i < m; i += T.size) a[i * lda + k] = a[i * lda + k] / piv;
         T.sync();
         // rows split across warps, columns across lanes (column k+1+lane+32c);
         // each lane keeps its columns of the pivot row in registers for the
@@ -337,14 +351,14 @@ __device__ int team_eliminate(const Team& T, double* a, int m, int K, double* ca
 #pragma unroll
         for (int c = 0; c < ELIM_CHUNKS; c++) {
             const int j = k + 1 + lane + 32 * c;
-            pr[c] = j < ld ? a[k * ld + j] : 0.0;
+            pr[c] = j < ld ? a[k * lda + j] : 0.0;
         }
         double nbv = -1.0;
         int nbr = INT_MAX;
 #pragma unroll 2
         for (int i = k + 1 + w; i < m; i += nw) {
-            const double l = a[i * ld + k];
-            double* ai = a + (size_t)i * ld;
+            const double l = a[i * lda + k];
+            double* ai = a + (size_t)i * lda;
 #pragma unroll
             for (int c = 0; c < ELIM_CHUNKS; c++) {
                 const int j = k + 1 + lane + 32 * c;
@@ -367,20 +381,158 @@ __device__ int team_eliminate(const Team& T, double* a, int m, int K, double* ca
     return 0;
 }
 
-// Column-oriented back substitution (dtrsm upper, non-unit), one warp per RHS column.
-__device__ void team_back_substitute(const Team& T, double* a, int m, int K)
+// Pivot candidates of column k over rows [k, m): one per warp, first maximum.
+__device__ void team_column_candidates(const Team& T, const double* a, int lda, int k, int m, double* cand_v,
+                                       int* cand_r)
 {
-    const int ld = m + K;
+    double bv = -1.0;
+    int br = INT_MAX;
+    for (int i = k + T.tid; i < m; i += T.size) {
+        const double v = fabs(a[i * lda + k]);
+        if (v > bv) { bv = v; br = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+        if (ov > bv || (ov == bv && orr < br)) { bv = ov; br = orr; }
+    }
+    if (T.lane() == 0) {
+        cand_v[T.warp()] = bv;
+        cand_r[T.warp()] = br;
+    }
+}
+
+// Blocked elimination with delayed trailing updates, the same arithmetic as
+// team_eliminate (and so as dgetf2): every element receives its updates
+// a_ij <- fma(-l_ik, u_kj, a_ij) in ascending k, with the same multipliers
+// (divisions by the same pivots) and the same first-maximum pivots; only the
+// moment an update is applied changes.  Panels of PB columns, as LAPACK's
+// dgetrf blocks them: within a panel, step k swaps whole rows and updates the
+// panel's columns of the rows below k only (every row's trailing columns then
+// lack the same panel steps, so swapping them is consistent); after the panel,
+// the panel rows' trailing columns are solved against the unit lower triangle
+// of the panel, column by column, in ascending step order (dtrsm), and the
+// rows below receive the panel's delayed updates at once as a register-tiled
+// rank-PB product (each warp: 8 rows x 32 lanes x up to 4 column groups held in
+// registers, the L values broadcast, the U row read once per row tile), so the
+// trailing matrix is read and written once per panel instead of once per step.
+template <int PB>
+__device__ int team_eliminate_blocked(const Team& T, double* a, int m, int K, int lda, double* cand_v, int* cand_r)
+{
+    const int ncols = m + K;
+    const int nw = T.nwarps(), w = T.warp(), lane = T.lane();
+    for (int k0 = 0; k0 < m; k0 += PB) {
+        const int kend = min(k0 + PB, m);
+        team_column_candidates(T, a, lda, k0, m, cand_v, cand_r);
+        T.sync();
+        for (int k = k0; k < kend; k++) {
+            double bv = cand_v[0];
+            int p = cand_r[0];
+            for (int q = 1; q < nw; q++) {
+                const double v = cand_v[q];
+                const int r = cand_r[q];
+                if (v > bv || (v == bv && r < p)) { bv = v; p = r; }
+            }
+            if (!(bv > 0.0)) return k + 1;
+            if (p != k)
+                for (int j = T.tid; j < ncols; j += T.size) {
+                    const double t = a[k * lda + j];
+                    a[k * lda + j] = a[p * lda + j];
+                    a[p * lda + j] = t;
+                }
+            T.sync();
+            const double piv = a[k * lda + k];
+            for (int i = k + 1 + T.tid; i < m; i += T.size) a[i * lda + k] = a[i * lda + k] / piv;
+            T.sync();
+            // rows k+1..m-1 x the panel's columns k+1..kend-1
+            const int wa = kend - k - 1;
+            const int na = (m - k - 1) * wa;
+            double nbv = -1.0;
+            int nbr = INT_MAX;
+            for (int e = T.tid; e < na; e += T.size) {
+                const int i = k + 1 + e / wa, j = k + 1 + e % wa;
+                const double v = __fma_rn(-a[i * lda + k], a[k * lda + j], a[i * lda + j]);
+                a[i * lda + j] = v;
+                if (j == k + 1) {
+                    const double av = fabs(v);
+                    if (av > nbv || (av == nbv && i < nbr)) { nbv = av; nbr = i; }
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, nbv, o);
+                const int orr = __shfl_xor_sync(0xffffffffu, nbr, o);
+                if (ov > nbv || (ov == nbv && orr < nbr)) { nbv = ov; nbr = orr; }
+            }
+            if (lane == 0) {
+                cand_v[w] = nbv;
+                cand_r[w] = nbr;
+            }
+            T.sync();
+        }
+        // U: the panel rows' trailing columns, one column per thread, steps in order
+        for (int j = kend + T.tid; j < ncols; j += T.size)
+            for (int r = k0 + 1; r < kend; r++) {
+                double v = a[r * lda + j];
+                for (int pp = k0; pp < r; pp++) v = __fma_rn(-a[r * lda + pp], a[pp * lda + j], v);
+                a[r * lda + j] = v;
+            }
+        T.sync();
+        if (kend >= m) break;
+        // delayed rank-(kend-k0) update of rows kend..m-1, columns kend..ncols-1
+        const int nr = m - kend;
+        const int ntiles = (nr + 7) >> 3;
+        for (int cb = kend; cb < ncols; cb += 128) {
+            for (int rt = w; rt < ntiles; rt += nw) {
+                const int i0 = kend + rt * 8;
+                double acc[8][4];
+#pragma unroll
+                for (int r = 0; r < 8; r++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const int i = i0 + r, j = cb + lane + 32 * c;
+                        acc[r][c] = (i < m && j < ncols) ? a[i * lda + j] : 0.0;
+                    }
+                for (int pp = k0; pp < kend; pp++) {
+                    double u[4], l[8];
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const int j = cb + lane + 32 * c;
+                        u[c] = j < ncols ? a[pp * lda + j] : 0.0;
+                    }
+#pragma unroll
+                    for (int r = 0; r < 8; r++) l[r] = (i0 + r < m) ? a[(i0 + r) * lda + pp] : 0.0;
+#pragma unroll
+                    for (int r = 0; r < 8; r++)
+#pragma unroll
+                        for (int c = 0; c < 4; c++) acc[r][c] = __fma_rn(-l[r], u[c], acc[r][c]);
+                }
+#pragma unroll
+                for (int r = 0; r < 8; r++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const int i = i0 + r, j = cb + lane + 32 * c;
+                        if (i < m && j < ncols) a[i * lda + j] = acc[r][c];
+                    }
+            }
+        }
+        T.sync();
+    }
+    return 0;
+}
+
+// Column-oriented back substitution (dtrsm upper, non-unit), one warp per RHS column.
+__device__ void team_back_substitute(const Team& T, double* a, int m, int K, int lda)
+{
     for (int c = T.warp(); c < K; c += T.nwarps()) {
         const int col = m + c;
         for (int k = m - 1; k >= 0; k--) {
             double xk = 0.0;
             if (T.lane() == 0) {
-                xk = a[k * ld + col] / a[k * ld + k];
-                a[k * ld + col] = xk;
+                xk = a[k * lda + col] / a[k * lda + k];
+                a[k * lda + col] = xk;
             }
             xk = __shfl_sync(0xffffffffu, xk, 0);
-            for (int i = T.lane(); i < k; i += 32) a[i * ld + col] = __fma_rn(-xk, a[i * ld + k], a[i * ld + col]);
+            for (int i = T.lane(); i < k; i += 32) a[i * lda + col] = __fma_rn(-xk, a[i * lda + k], a[i * lda + col]);
             __syncwarp();
         }
     }
@@ -389,15 +541,16 @@ __device__ void team_back_substitute(const Team& T, double* a, int m, int K)
 
 // ---------------------------------------------------------------------------
 
-// Team assembly of the augmented system [A | B] of stencil r into a (m x (m+K)).
-// xs: scratch for the stencil's coordinates; fr: 7 doubles of scratch (tangent frame).
-// Returns m.  Ends with a team barrier.
-__device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, double* xs, double* fr, int& n_out)
+// Team assembly of the augmented system [A | B] of stencil r into a (m rows of
+// m + K columns at row stride ld).  xs: scratch for the stencil's coordinates;
+// fr: 7 doubles of scratch (tangent frame).  Returns m.  Ends with a team barrier.
+__device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, double* xs, double* fr, int& n_out,
+                             int ld)
 {
     const int n = P.len[r];
     const int deg = P.deg ? P.deg[r] : P.deg_uniform;
     const int np = poly_size(deg);
-    const int m = n + np, K = P.K, ld = m + K;
+    const int m = n + np, K = P.K;
     const double eps = P.eps ? P.eps[r] : P.eps_uniform;  // var_epsilon[stencil[0]]
     const double eps2 = eps * eps;
     for (int q = T.tid; q < n; q += T.size) {
@@ -420,12 +573,19 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
         }
         fr[6] = s2 > 0.0 ? sqrt(s2) : 1.0;
     }
-    // Phi block: ar(j, i) = phi(x_i - x_j)   (rbffd.cpp:943-966)
-    for (int e = T.tid; e < n * n; e += T.size) {
-        int j = e / n, i = e - j * n;
+    // Phi block: ar(j, i) = phi(x_i - x_j)   (rbffd.cpp:943-966).  Symmetric to
+    // the last bit (x_j - x_i squares to the same r^2), so each pair j <= i is
+    // evaluated once and written to both places: n(n+1)/2 exponentials.
+    for (int e = T.tid; e < n * (n + 1) / 2; e += T.size) {
+        int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);  // e = i(i+1)/2 + j, 0 <= j <= i
+        while (i * (i + 1) / 2 > e) i--;
+        while ((i + 1) * (i + 2) / 2 <= e) i++;
+        const int j = e - i * (i + 1) / 2;
         double dx = xs[3 * i] - xs[3 * j], dy = xs[3 * i + 1] - xs[3 * j + 1], dz = xs[3 * i + 2] - xs[3 * j + 2];
         double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-        a[j * ld + i] = g_eval(eps2, r2);
+        const double v = g_eval(eps2, r2);
+        a[j * ld + i] = v;
+        a[i * ld + j] = v;
     }
     T.sync();  // frame visible
     const double* e1 = fr;
@@ -476,37 +636,60 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
     return m;
 }
 
-// Per-team shared memory: [a: m x (m+K)] [xs: 3 n_pad] [frame: 8] [cand_v: MAX_WARPS] [cand_r: MAX_WARPS ints]
-__global__ void __launch_bounds__(512) k_weights(WParams P, int team_size)
+// One system end to end by one team: assemble, eliminate (blocked or not),
+// back-substitute, store the weights of row r.  a: the team's shared memory,
+// [a: m rows at stride lda] [xs: 3 n_pad] [frame: 8] [cand_v: MAX_WARPS]
+// [cand_r: MAX_WARPS ints].
+__device__ void team_solve(const Team& T, const WParams& P, int r, double* a, int m, int lda, int blocked)
 {
-    extern __shared__ double smem[];
-    Team T;
-    T.size = team_size;
-    T.id = threadIdx.x / team_size;
-    T.tid = threadIdx.x % team_size;
-    const int teams_per_cta = blockDim.x / team_size;
-    double* a = smem + (size_t)T.id * P.team_stride;
-    double* xs = a + (size_t)P.m * (P.m + P.K);
+    double* xs = a + (size_t)m * lda;
     double* fr = xs + 3 * P.n_pad;
     double* cand_v = fr + 8;
     int* cand_r = (int*)(cand_v + MAX_WARPS);
     const int K = P.K;
-    for (int t = blockIdx.x * teams_per_cta + T.id; t < P.nrows; t += gridDim.x * teams_per_cta) {
-        const int r = P.rows[t];
-        int n;
-        const int m = team_assemble(T, P, r, a, xs, fr, n);
-        const int ld = m + K;
-        const bool ok = team_eliminate(T, a, m, K, cand_v, cand_r) == 0;
-        if (ok) team_back_substitute(T, a, m, K);
-        if (!ok && T.tid == 0) atomicMin(P.status, r + 1);
-        // store: weights[type][r][j] = W(j, col) * scale (rbffd.cpp:300-306), row r of the sliced ELL
-        for (int e = T.tid; e < K * P.n4; e += T.size) {
-            int c = e / P.n4, j = e - c * P.n4;
-            double scale = P.opbit[c] == RBFFD_HV ? P.hv_scale : 1.0;
-            double v = (j < n) ? (ok ? a[j * ld + m + c] * scale : __longlong_as_double(0x7ff8000000000000ll)) : 0.0;
-            P.w[c][sell_elem(r, j, P.n4 >> 2)] = v;
-        }
-        T.sync();
+    int n;
+    team_assemble(T, P, r, a, xs, fr, n, lda);
+    const int st = blocked ? team_eliminate_blocked<8>(T, a, m, K, lda, cand_v, cand_r)
+                           : team_eliminate(T, a, m, K, lda, cand_v, cand_r);
+    const bool ok = st == 0;
+    if (ok) team_back_substitute(T, a, m, K, lda);
+    if (!ok && T.tid == 0) atomicMin(P.status, r + 1);
+    // store: weights[type][r][j] = W(j, col) * scale (rbffd.cpp:300-306), row r of the sliced ELL
+    for (int e = T.tid; e < K * P.n4; e += T.size) {
+        int c = e / P.n4, j = e - c * P.n4;
+        double scale = P.opbit[c] == RBFFD_HV ? P.hv_scale : 1.0;
+        double v = (j < n) ? (ok ? a[j * lda + m + c] * scale : __longlong_as_double(0x7ff8000000000000ll)) : 0.0;
+        P.w[c][sell_elem(r, j, P.n4 >> 2)] = v;
+    }
+    T.sync();
+}
+
+// The whole batch in one persistent launch.  Work units are numbered class
+// by class (classes in decreasing system size, so the largest systems start
+// first); a unit is teams_per_cta systems of one class, one per team of the
+// CTA.  Each CTA takes the next unit from a global counter until none is
+// left, splits itself into that class's teams and solves.
+__global__ void __launch_bounds__(256) k_weights_all(WParams P)
+{
+    extern __shared__ double smem[];
+    __shared__ int s_unit;
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = atomicAdd(P.work, 1);
+        __syncthreads();
+        const int u = s_unit;
+        __syncthreads();
+        if (u >= P.nunits) break;
+        int c = 0;
+        while (c + 1 < P.nclasses && u >= P.cls[c + 1].unit0) c++;
+        const WClass C = P.cls[c];
+        Team T;
+        T.size = C.team;
+        T.id = threadIdx.x / C.team;
+        T.tid = threadIdx.x % C.team;
+        const int t = (u - C.unit0) * C.teams + T.id;
+        if (T.id < C.teams && t < C.nrows)
+            team_solve(T, P, P.rows[C.rows_off + t], smem + (size_t)T.id * C.stride, C.m, C.lda, C.blocked);
+        __syncthreads();  // every team done with the shared memory before the next unit
     }
 }
 
@@ -525,7 +708,7 @@ __global__ void __launch_bounds__(512) k_assemble(WParams P, int team_size, doub
     const size_t sz = (size_t)P.m * (P.m + P.K);
     for (int t = blockIdx.x * teams_per_cta + T.id; t < P.nrows; t += gridDim.x * teams_per_cta) {
         int n;
-        team_assemble(T, P, P.rows[t], a, xs, fr, n);
+        team_assemble(T, P, P.rows[t], a, xs, fr, n, P.m + P.K);
         for (size_t e = T.tid; e < sz; e += T.size) out[(size_t)t * sz + e] = a[e];
         T.sync();
     }
@@ -533,7 +716,7 @@ __global__ void __launch_bounds__(512) k_assemble(WParams P, int team_size, doub
 
 // Plain batched solve: A [batch][m][m], B [batch][m][nrhs] row-major, X -> B.
 __global__ void __launch_bounds__(512) k_gesv(double* A, double* B, int* info, int m, int K, int batch, int team_size,
-                                              int team_stride)
+                                              int team_stride, int blocked)
 {
     extern __shared__ double smem[];
     Team T;
@@ -551,17 +734,19 @@ __global__ void __launch_bounds__(512) k_gesv(double* A, double* B, int* info, i
         for (int e = T.tid; e < m * m; e += T.size) a[(e / m) * ld + e % m] = Ab[e];
         for (int e = T.tid; e < m * K; e += T.size) a[(e / K) * ld + m + e % K] = Bb[e];
         T.sync();
-        const int st = team_eliminate(T, a, m, K, cand_v, cand_r);
-        if (st == 0) team_back_substitute(T, a, m, K);
+        const int st = blocked ? team_eliminate_blocked<8>(T, a, m, K, ld, cand_v, cand_r)
+                               : team_eliminate(T, a, m, K, ld, cand_v, cand_r);
+        if (st == 0) team_back_substitute(T, a, m, K, ld);
         if (T.tid == 0) info[b] = st;
         for (int e = T.tid; e < m * K; e += T.size) Bb[e] = a[(e / K) * ld + m + e % K];
         T.sync();
     }
 }
 
-size_t team_bytes_w(int m, int K, int n_pad)
+size_t team_bytes_w(int m, int K, int n_pad, int lda = 0)
 {
-    return ((size_t)m * (m + K) + 3 * (size_t)n_pad + 8 + 2 * MAX_WARPS) * sizeof(double);
+    if (lda == 0) lda = m + K;
+    return ((size_t)m * lda + 3 * (size_t)n_pad + 8 + 2 * MAX_WARPS) * sizeof(double);
 }
 
 int max_smem_optin(rbffd_ctx* ctx)
@@ -571,45 +756,120 @@ int max_smem_optin(rbffd_ctx* ctx)
     return v;
 }
 
+constexpr int W_CTA = 256;  // threads per CTA of the persistent launch
+
+// A class's team shape: team width (teams per CTA = W_CTA / team) and the elimination.
 struct WShape {
-    int team, block;
+    int team, blocked;
 };
 
 }  // namespace
 
-// Candidate team shapes for a bucket: (team width, CTA threads) such that the
-// teams fit the shared memory of one CTA.
-static std::vector<WShape> w_candidates(int m, size_t team_bytes, int smem_max)
+// Row stride of a class's systems: m + K rounded up to odd, so a column walk
+// (pivot search, multipliers) touches 32 different bank pairs.
+static int class_lda(int m, int K) { return (m + K) | 1; }
+
+static size_t class_stride_bytes(int m, int K, int n_pad)
+{
+    return (team_bytes_w(m, K, n_pad, class_lda(m, K)) + 127) / 128 * 128;
+}
+
+// Candidate shapes of a class: teams whose shared memory fits one CTA.
+static std::vector<WShape> w_candidates(int m, size_t stride_bytes, int smem_max)
 {
     std::vector<WShape> out;
     const int teams[4] = {32, 64, 128, 256};
-    const int blocks[3] = {128, 256, 512};
-    for (int tw : teams)
-        for (int b : blocks) {
-            if (b < tw || b / tw > 15) continue;
-            if (tw > 32 * MAX_WARPS) continue;
-            if ((size_t)(b / tw) * team_bytes > (size_t)smem_max) continue;
-            if (m <= 40 && tw > 64) continue;  // small systems: narrow teams only
-            out.push_back(WShape{tw, b});
-        }
+    for (int tw : teams) {
+        if ((size_t)(W_CTA / tw) * stride_bytes > (size_t)smem_max) continue;
+        if (m <= 40 && tw > 64) continue;   // small systems: narrow teams only
+        if (m > 96 && tw < 128) continue;   // large systems: wide teams only
+        out.push_back(WShape{tw, 0});
+        if (m >= 24) out.push_back(WShape{tw, 1});
+    }
     return out;
 }
 
-static int launch_weights(rbffd_ctx* ctx, const WParams& P, WShape sh, size_t team_bytes, int nrows_cap)
+// The per-grid device workspace of the weight solver, kept between calls so a
+// captured launch can be replayed: row list, degrees, epsilons, status, counter.
+struct WeightsWork {
+    int* d_rows = nullptr;
+    int* d_deg = nullptr;
+    double* d_eps = nullptr;
+    int* d_status = nullptr;  // [0] status, [1] work counter
+    size_t bytes = 0;
+    cudaGraphExec_t gexec = nullptr;
+    WParams gparams;  // the parameters the graph was captured with
+    size_t gsmem = 0;
+    int ggrid = 0;
+};
+
+void weights_work_free(rbffd_grid* g)
 {
-    WParams Q = P;
-    if (nrows_cap > 0) Q.nrows = std::min(Q.nrows, nrows_cap);
-    int teams_per_cta = sh.block / sh.team;
-    size_t smem = (size_t)teams_per_cta * team_bytes;
-    RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(k_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_weights, sh.block, smem));
-    if (per_sm < 1) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "weight kernel shape does not fit an SM");
-    int need = (Q.nrows + teams_per_cta - 1) / teams_per_cta;
-    int grid = std::max(1, std::min(need, per_sm * ctx->sm_count));
-    k_weights<<<grid, sh.block, smem, ctx->stream>>>(Q, sh.team);
-    RBFFD_CUDA_TRY(ctx, cudaGetLastError());
+    WeightsWork* W = g->ww;
+    if (!W) return;
+    rbffd_ctx* ctx = g->ctx;
+    if (W->gexec) cudaGraphExecDestroy(W->gexec);
+    dev_free(ctx, W->d_rows, (size_t)g->N * sizeof(int));
+    dev_free(ctx, W->d_deg, (size_t)g->N * sizeof(int));
+    dev_free(ctx, W->d_eps, (size_t)g->N * sizeof(double));
+    dev_free(ctx, W->d_status, 2 * sizeof(int));
+    delete W;
+    g->ww = nullptr;
+}
+
+static int weights_work(rbffd_grid* g, WeightsWork** out)
+{
+    if (!g->ww) {
+        rbffd_ctx* ctx = g->ctx;
+        WeightsWork* W = new (std::nothrow) WeightsWork();
+        if (!W) return set_error(ctx, RBFFD_ERR_OOM, "weights workspace");
+        g->ww = W;
+        int rc;
+        if ((rc = dev_alloc(ctx, (void**)&W->d_rows, (size_t)g->N * sizeof(int))) ||
+            (rc = dev_alloc(ctx, (void**)&W->d_deg, (size_t)g->N * sizeof(int))) ||
+            (rc = dev_alloc(ctx, (void**)&W->d_eps, (size_t)g->N * sizeof(double))) ||
+            (rc = dev_alloc(ctx, (void**)&W->d_status, 2 * sizeof(int)))) {
+            weights_work_free(g);
+            return rc;
+        }
+    }
+    *out = g->ww;
     return RBFFD_OK;
+}
+
+// Shared memory, CTAs per SM and grid of a persistent launch over P's classes.
+static int persistent_geometry(rbffd_ctx* ctx, const WParams& P, size_t* smem, int* grid)
+{
+    size_t sm = 0;
+    for (int c = 0; c < P.nclasses; c++)
+        sm = std::max(sm, (size_t)P.cls[c].teams * P.cls[c].stride * sizeof(double));
+    RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(k_weights_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int per_sm = 0;
+    RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_weights_all, W_CTA, sm));
+    if (per_sm < 1) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "weight kernel shape does not fit an SM");
+    *smem = sm;
+    *grid = std::max(1, std::min(P.nunits, per_sm * ctx->sm_count));
+    return RBFFD_OK;
+}
+
+// Zero the counter and launch (what the graph holds).
+static void enqueue_persistent(const WParams& P, size_t smem, int grid, cudaStream_t s)
+{
+    cudaMemsetAsync(P.work, 0, sizeof(int), s);
+    k_weights_all<<<grid, W_CTA, smem, s>>>(P);
+}
+
+// Fill in the classes' shapes and unit numbering (cls[].team/blocked set).
+static void number_units(WParams& P)
+{
+    int u = 0;
+    for (int c = 0; c < P.nclasses; c++) {
+        WClass& C = P.cls[c];
+        C.teams = W_CTA / C.team;
+        C.unit0 = u;
+        u += (C.nrows + C.teams - 1) / C.teams;
+    }
+    P.nunits = u;
 }
 
 constexpr unsigned ALT_BITS = RBFFD_ALT_XSFC | RBFFD_ALT_YSFC | RBFFD_ALT_ZSFC;
@@ -673,15 +933,18 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
                 return set_error(ctx, RBFFD_ERR_INVALID, "deg_per_row[%d] = %d outside [-1, 4]", i, deg_per_row[i]);
             deg[g->h_iperm[i]] = deg_per_row[i];  // internal row order
         }
-    // buckets by system size m
-    std::map<int, std::vector<int>> buckets;
+    // classes by system size m, largest first
+    std::map<int, std::vector<int>, std::greater<int>> buckets;
     for (int i = 0; i < N; i++) {
         int np = poly_size(deg[i]);
         buckets[g->h_len[i] + np].push_back(i);
     }
+    if ((int)buckets.size() > MAX_CLASSES)
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "%d different system sizes (at most %d)", (int)buckets.size(),
+                         MAX_CLASSES);
     int smem_max = max_smem_optin(ctx);
     for (auto& kv : buckets)
-        if (team_bytes_w(kv.first, K, g->n_pad) > (size_t)smem_max)
+        if (class_stride_bytes(kv.first, K, g->n_pad) > (size_t)smem_max)
             return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "system size %d with %d operators exceeds shared memory", kv.first, K);
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
@@ -691,67 +954,54 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
         if ((rc = grid_alloc_w64(g, op))) return rc;
         P.w[c] = g->d_w64[op];
     }
-    // device inputs
-    int *d_rows = nullptr, *d_deg = nullptr, *d_status = nullptr;
-    double* d_eps = nullptr;
-    size_t b_rows = (size_t)N * sizeof(int);
-    auto cleanup = [&]() {
-        dev_free(ctx, d_rows, b_rows);
-        dev_free(ctx, d_deg, b_rows);
-        dev_free(ctx, d_status, sizeof(int));
-        dev_free(ctx, d_eps, (size_t)N * sizeof(double));
-    };
-    if ((rc = dev_alloc(ctx, (void**)&d_rows, b_rows)) || (rc = dev_alloc(ctx, (void**)&d_deg, b_rows)) ||
-        (rc = dev_alloc(ctx, (void**)&d_status, sizeof(int))) ||
-        (eps && (rc = dev_alloc(ctx, (void**)&d_eps, (size_t)N * sizeof(double))))) {
-        cleanup();
-        return rc;
-    }
+    WeightsWork* W = nullptr;
+    if ((rc = weights_work(g, &W))) return rc;
     std::vector<int> rows;
     rows.reserve(N);
     for (auto& kv : buckets) rows.insert(rows.end(), kv.second.begin(), kv.second.end());
-    int status0 = INT_MAX;
-    cudaError_t e = cudaMemcpyAsync(d_rows, rows.data(), b_rows, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_deg, deg.data(), b_rows, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_status, &status0, sizeof(int), cudaMemcpyHostToDevice, s);
+    const int status0[2] = {INT_MAX, 0};
+    cudaError_t e = cudaMemcpyAsync(W->d_rows, rows.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(W->d_deg, deg.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(W->d_status, status0, 2 * sizeof(int), cudaMemcpyHostToDevice, s);
     std::vector<double> eps_int;
     if (eps) {
         eps_int.resize(N);
         for (int i = 0; i < N; i++) eps_int[i] = eps[g->h_perm[i]];  // internal row order
     }
     if (e == cudaSuccess && eps)
-        e = cudaMemcpyAsync(d_eps, eps_int.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
+        e = cudaMemcpyAsync(W->d_eps, eps_int.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // host vectors above go out of scope after this block
-    if (e != cudaSuccess) {
-        cleanup();
-        return cuda_error(ctx, e, "rbffd_weights_compute upload");
-    }
+    if (e != cudaSuccess) return cuda_error(ctx, e, "rbffd_weights_compute upload");
     P.xyz = g->d_xyz;
     P.idx = g->d_idx;
     P.len = g->d_len;
-    P.eps = d_eps;
+    P.eps = eps ? W->d_eps : nullptr;
     P.eps_uniform = eps_uniform;
-    P.deg = d_deg;
+    P.deg = W->d_deg;
     P.deg_uniform = prm->poly_deg;
-    P.status = d_status;
+    P.rows = W->d_rows;
+    P.nrows = N;
+    P.status = W->d_status;
+    P.work = W->d_status + 1;
     P.n4 = g->n4;
     P.n_pad = g->n_pad;
     P.dim = prm->dim;
     P.hv_k = prm->hv_k;
     double hvN = prm->hv_nodes > 0 ? prm->hv_nodes : (double)N;
     P.hv_scale = -prm->hv_gamma * pow(hvN, -(double)prm->hv_k);
-    size_t off = 0;
+    // classes, each with its tuned team shape
+    int off = 0;
+    P.nclasses = 0;
     for (auto& kv : buckets) {
-        int m = kv.first;
-        int cnt = (int)kv.second.size();
-        WParams Q = P;
-        Q.rows = d_rows + off;
-        Q.nrows = cnt;
-        Q.m = m;
-        size_t tb = team_bytes_w(m, K, g->n_pad);
-        tb = (tb + 127) / 128 * 128;  // keep teams 128-byte aligned
-        Q.team_stride = (int)(tb / sizeof(double));
-        TuneKey key{100 + K, m, g->n_pad, 0, 0};
+        WClass& C = P.cls[P.nclasses++];
+        C.m = kv.first;
+        C.lda = class_lda(C.m, K);
+        const size_t sb = class_stride_bytes(C.m, K, g->n_pad);
+        C.stride = (int)(sb / sizeof(double));
+        C.rows_off = off;
+        C.nrows = (int)kv.second.size();
+        off += C.nrows;
+        TuneKey key{200 + K, C.m, g->n_pad, 0, 0};
         WShape best{0, 0};
         {
             std::lock_guard<std::mutex> lk(ctx->mu);
@@ -759,22 +1009,31 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
             if (it != ctx->tuned.end()) best = WShape{it->second.lanes, it->second.block};
         }
         if (best.team == 0) {
-            std::vector<WShape> cands = w_candidates(m, tb, smem_max);
-            if (cands.empty()) {
-                cleanup();
-                return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "no kernel shape fits system size %d", m);
-            }
+            std::vector<WShape> cands = w_candidates(C.m, sb, smem_max);
+            if (cands.empty()) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "no kernel shape fits system size %d", C.m);
             best = cands[0];
-            if (cands.size() > 1 && cnt >= 2048) {
-                // time each shape on a prefix of the bucket (outputs are rewritten by the full launch)
+            if (cands.size() > 1 && C.nrows >= 2048) {
+                // time each shape on a prefix of the class (outputs are rewritten by the full launch)
                 cudaEvent_t e0, e1;
                 cudaEventCreate(&e0);
                 cudaEventCreate(&e1);
                 float best_ms = 1e30f;
-                int cap = std::min(cnt, 8 * ctx->sm_count * 8);
-                for (const WShape& c : cands) {
+                for (const WShape& cs : cands) {
+                    WParams Q = P;
+                    Q.nclasses = 1;
+                    Q.cls[0] = C;
+                    Q.cls[0].team = cs.team;
+                    Q.cls[0].blocked = cs.blocked;
+                    Q.cls[0].nrows = std::min(C.nrows, 16 * ctx->sm_count * (W_CTA / cs.team));
+                    number_units(Q);
+                    size_t smem;
+                    int grid;
+                    if (persistent_geometry(ctx, Q, &smem, &grid) != RBFFD_OK) {
+                        cudaGetLastError();
+                        continue;
+                    }
                     cudaEventRecord(e0, s);
-                    if (launch_weights(ctx, Q, c, tb, cap) != RBFFD_OK) continue;
+                    enqueue_persistent(Q, smem, grid, s);
                     cudaEventRecord(e1, s);
                     if (cudaEventSynchronize(e1) != cudaSuccess) {
                         cudaGetLastError();
@@ -782,27 +1041,54 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
                     }
                     float ms = 0;
                     cudaEventElapsedTime(&ms, e0, e1);
+                    ms /= (float)Q.cls[0].nrows;
                     if (ms < best_ms) {
                         best_ms = ms;
-                        best = c;
+                        best = cs;
                     }
                 }
                 cudaEventDestroy(e0);
                 cudaEventDestroy(e1);
             }
             std::lock_guard<std::mutex> lk(ctx->mu);
-            ctx->tuned[key] = Shape{best.team, best.block};
+            ctx->tuned[key] = Shape{best.team, best.blocked};
         }
-        if ((rc = launch_weights(ctx, Q, best, tb, 0))) {
-            cleanup();
-            return rc;
-        }
-        off += cnt;
+        C.team = best.team;
+        C.blocked = best.blocked;
     }
+    number_units(P);
+    // the whole batch: one persistent launch, captured in a CUDA graph and
+    // replayed while the parameters stay the same
+    size_t smem;
+    int grid;
+    if ((rc = persistent_geometry(ctx, P, &smem, &grid))) return rc;
+    if (!W->gexec || memcmp(&W->gparams, &P, sizeof P) != 0 || W->gsmem != smem || W->ggrid != grid) {
+        if (W->gexec) {
+            cudaGraphExecDestroy(W->gexec);
+            W->gexec = nullptr;
+        }
+        cudaGraph_t graph;
+        RBFFD_CUDA_TRY(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        enqueue_persistent(P, smem, grid, s);
+        e = cudaStreamEndCapture(s, &graph);
+        if (e != cudaSuccess) return cuda_error(ctx, e, "weights graph capture");
+        e = cudaGraphInstantiate(&W->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            W->gexec = nullptr;
+            return cuda_error(ctx, e, "weights graph instantiate");
+        }
+        W->gparams = P;
+        W->gsmem = smem;
+        W->ggrid = grid;
+    }
+    e = cudaMemcpyAsync(W->d_status, status0, 2 * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaGraphLaunch(W->gexec, s);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "rbffd_weights_compute launch");
+    int* d_status = W->d_status;
     int status = INT_MAX;
     e = cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cleanup();
     if (e != cudaSuccess) return cuda_error(ctx, e, "rbffd_weights_compute");
     if (status != INT_MAX)
         return set_error(ctx, RBFFD_ERR_SINGULAR, "stencil %d: zero pivot in the weight system",
@@ -843,8 +1129,9 @@ extern "C" int rbffd_batched_gesv_dev(rbffd_ctx* ctx, int m, int nrhs, int batch
     int per_sm = 0;
     RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gesv, block, smem));
     int grid = std::max(1, std::min((batch + teams - 1) / teams, std::max(1, per_sm) * ctx->sm_count));
+    // blocked elimination above 40 unknowns (the same arithmetic, fewer passes over the trailing matrix)
     k_gesv<<<grid, block, smem, ctx->stream>>>((double*)A, (double*)B, (int*)info, m, nrhs, batch, team,
-                                                (int)(tb / sizeof(double)));
+                                                (int)(tb / sizeof(double)), m > 40 ? 1 : 0);
     RBFFD_CUDA_TRY(ctx, cudaGetLastError());
     RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return RBFFD_OK;

@@ -158,3 +158,60 @@ def test_eigenvalue_errors():
 
 
 R_EIG_MAX = 16384
+
+
+def test_hessenberg_eigenvalues_match_lapack():
+    """The Arnoldi check's projected eigenproblem (host, shifted QR in complex
+    arithmetic) against LAPACK (numpy) on random Hessenberg matrices of the
+    sizes the check uses, scaled and shifted."""
+    rng = np.random.default_rng(5)
+    for n in (1, 2, 3, 8, 40, 64, 120):
+        for trial in range(6):
+            H = np.triu(rng.standard_normal((n, n)), -1) * 10.0 ** rng.uniform(-6, 6)
+            ev, ref = R.hessenberg_eigenvalues(H), np.linalg.eigvals(H)
+            assert _set_distance(ev, ref) <= 1e-10 * max(np.abs(ref).max(), 1e-300), (n, trial)
+    with pytest.raises(R.RbffdError):
+        R.hessenberg_eigenvalues(np.zeros((0, 0)))
+
+
+def _rightmost_case(ctx, N, n, types, eps, deg, hv):
+    xyz = R.fibonacci_nodes(N, 1)
+    st = R.knn_stencils(xyz, n)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(types, grid, 2)
+    if hv:
+        der.setUseHyperviscosity(1)
+        der.setHVScalars(4, 1e-3)
+    der.setEpsilon(eps)
+    der.setPolynomialDegree(deg)
+    der.computeAllWeightsForAllStencils()
+    return grid, der
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a GPU")
+@pytest.mark.parametrize("case", ["advection_hv", "heat"])
+def test_rightmost_eigenvalues_match_the_dense_check(case):
+    """Arnoldi on the sparse operator against every eigenvalue of the dense
+    check: the rightmost Ritz values equal the rightmost eigenvalues to 1e-7
+    of the spectral radius, and the stability verdict (sign of the largest
+    real part beyond the 1e-8 band) agrees."""
+    ctx = R.Context(0)
+    if case == "advection_hv":  # unstable: positive real parts (the cosine bell at eps = 6)
+        grid, der = _rightmost_case(ctx, 4096, 31, R.LAMBDA, 6.0, 2, True)
+        which, nev = R.LAMBDA, 5
+    else:  # stable: the constant mode at 0, the rest negative
+        grid, der = _rightmost_case(ctx, 2562, 31, R.LSFC, 0.25 * np.sqrt(2562 / (4 * np.pi)), 2, False)
+        which, nev = R.LSFC, 4
+    _, dense = der.computeEigenvalues(which, return_eigenvalues=True)
+    dense = dense[np.argsort(-dense.real)]
+    rho = np.abs(dense).max()
+    out = der.computeRightmostEigenvalues(which, nev=nev, ncv=40, tol=1e-9)
+    ev = out["eigenvalues"]
+    assert out["nconv"] >= nev - 1, out
+    top = ev[:nev - 1]  # the last wanted value may sit in a cluster; the others are pinned
+    assert _set_distance(top, dense[:len(top) + 2]) <= 1e-7 * rho, (top, dense[:nev + 1])
+    assert abs(ev[0].real - dense[0].real) <= 1e-7 * rho
+    assert (ev[0].real > 1e-8) == (dense[0].real > 1e-8)
+    grid.close()
+    ctx.close()

@@ -348,3 +348,27 @@ def test_slot_schedule_refused_where_it_does_not_apply(bell, heat):
         pde.setTiledShape(128, 1, stream_weights=True, slot_schedule=True)
     assert e.value.status == -1
     pde.close()
+
+
+@pytest.mark.slow
+def test_heat_benchmark_grid_parity(ctx):
+    """The benchmark's own heat configuration: N = 163842, n = 50, degree 3,
+    eps h = 0.25, the whole 500-step workload.  FP64 with one lane per row
+    equals the oracle bit for bit; FP64 with the autotuned shape within 1e-12;
+    FP32 (autotuned) within 1e-5 of the FP64 oracle (rel. L2)."""
+    N, n, steps, dt = 163842, 50, 500, 1e-6
+    xyz = R.fibonacci_nodes(N, 2)
+    st = R.knn_stencils(xyz, n)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(R.LSFC, grid, 2)
+    der.setEpsilon(0.25 / np.sqrt(4 * np.pi / N))
+    der.setPolynomialDegree(3)
+    der.computeAllWeightsForAllStencils()
+    W = der.getWeights(R.LSFC)
+    u0 = R.exact_sph_heat(xyz, 20, np.random.default_rng(2).standard_normal(441), 0.0)
+    ref = O.rk4_heat(st, None, W, u0, dt, steps, nthreads=O.max_threads())
+    h = dict(grid=grid, der=der, u0=u0)
+    assert np.array_equal(_gpu_heat(h, steps, dt, shape=(1, 256), graph=True), ref)
+    assert rel_l2(_gpu_heat(h, steps, dt, shape=None, graph=True), ref) <= 1e-12
+    assert rel_l2(_gpu_heat(h, steps, dt, dtype=R.F32, shape=None, graph=True), ref) <= 1e-5
+    grid.close()

@@ -106,12 +106,15 @@ def test_elimination_bit_exact_random(ctx, m, nrhs):
         assert np.array_equal(X[k], O.lu_solve(A[k], B[k]))
 
 
-def test_elimination_reports_zero_pivot(ctx):
-    A = np.eye(6)[None].repeat(2, axis=0)
-    A[1, :, 3] = 0.0  # column 3 exactly zero: zero pivot at step 3
-    B = np.ones((2, 6, 1))
+@pytest.mark.parametrize("m,col", [(6, 3), (60, 45), (116, 8)])
+def test_elimination_reports_zero_pivot(ctx, m, col):
+    """A zero pivot column, in the unblocked (m <= 40) and the blocked
+    elimination (a panel's first and a later column)."""
+    A = np.eye(m)[None].repeat(2, axis=0)
+    A[1, :, col] = 0.0  # column `col` exactly zero: zero pivot at that step
+    B = np.ones((2, m, 1))
     _, info = _gesv_dev(ctx, A, B)
-    assert info[0] == 0 and info[1] == 4
+    assert info[0] == 0 and info[1] == col + 1
 
 
 def test_weights_match_oracle_cosine_bell_setup(ctx):
