@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--profile-multitracer", default=None, metavar="ROWS,LANES",
                     help="16-tracer vortex case on N=163842, n=101 (weights > L2), 3 un-graphed RK4 steps with the "
                          "tiled shape ROWS,LANES (0,0 = global-memory gathers; further fields: f = FP32 fused "
-                         "operator, s = conflict-avoiding slot schedule, d = FP64), for ncu captures")
+                         "operator, s = conflict-avoiding slot schedule, p = register-pipelined weight stream, "
+                         "d = FP64), for ncu captures")
     ap.add_argument("--profile-serving", type=int, default=0, metavar="K",
                     help="serving stage kernels: K + K requests on two N=163842 grids, 3 RK4 steps, for ncu")
     ap.add_argument("--profile-heat-hbm", action="store_true",
@@ -1236,6 +1237,7 @@ def run_profile_multitracer(spec):
     fused = "f" in fields[2:]
     sched = "s" in fields[2:]
     fp64 = "d" in fields[2:]
+    pipe = "p" in fields[2:]
     N, n, T = 163842, 101, 16
     xyz = R.fibonacci_nodes(N, 4)
     st = R.knn_stencils(xyz, n)
@@ -1253,7 +1255,7 @@ def run_profile_multitracer(spec):
     if fused:
         pde.setFusedOperator(True)
     if rows > 0:
-        pde.setTiledShape(rows, lanes, slot_schedule=sched)
+        pde.setTiledShape(rows, lanes, slot_schedule=sched, pipeline=pipe)
     else:
         pde.setShape(1, 256)
     pde.fillInitialConditions(u0)

@@ -420,14 +420,19 @@ int rbffd_pde_get_shape(rbffd_pde* pde, int* lanes_per_row, int* block_threads);
  *     each row's FP32 summation order;
  *   RBFFD_TILE_PREFETCH: the block's lanes ask L2 for the weights and indices
  *     of chunks a few steps ahead (pays where the weight stream comes from
- *     HBM); the arithmetic is unchanged.
- * At most one of the three.  (flags = 1, the former stream_weights argument,
- * keeps its meaning.)
+ *     HBM); the arithmetic is unchanged;
+ *   RBFFD_TILE_PIPELINE: PDEs that stream one operator (heat, or a fused
+ *     advection operator) with 1, 4, 8 or 16 (FP32) / 1, 8, 16 (FP64) values
+ *     per node: each lane keeps the local indices and weights of its row's
+ *     next four chunks in flight in registers; the arithmetic is unchanged.
+ * At most one of the first three; RBFFD_TILE_PIPELINE combines with
+ * RBFFD_TILE_SLOT_SCHEDULE only.  (flags = 1, the former stream_weights
+ * argument, keeps its meaning.)
  * Returns RBFFD_ERR_UNSUPPORTED if the staged data do not fit shared memory
  * or the flags do not apply to the PDE.
  * get_tiling reports 0 when the stage kernel gathers from global memory;
  * get_tile_flags the flags of the shape in use (set or autotuned). */
-enum { RBFFD_TILE_STREAM_WEIGHTS = 1, RBFFD_TILE_SLOT_SCHEDULE = 2, RBFFD_TILE_PREFETCH = 4 };
+enum { RBFFD_TILE_STREAM_WEIGHTS = 1, RBFFD_TILE_SLOT_SCHEDULE = 2, RBFFD_TILE_PREFETCH = 4, RBFFD_TILE_PIPELINE = 8 };
 int rbffd_pde_set_tiled_shape(rbffd_pde* pde, int rows_per_block, int lanes, int flags);
 int rbffd_pde_get_tiling(rbffd_pde* pde, int* rows_per_block);
 int rbffd_pde_get_tile_flags(rbffd_pde* pde, int* flags);

@@ -39,6 +39,7 @@ struct Shape {
     int pf = 0;    // tiled, one lane per row: upcoming chunks of weights and indices prefetched into L2
     int plain = 0; // FP64, one tracer, one lane per row, global gathers: the reference build's arithmetic
                    // (every multiply-add a rounded product, then a rounded sum; RBFFD_ARITH_UNFUSED)
+    int pipe = 0;  // tiled, one operator, one lane group per row: weights and indices pipelined in registers
 };
 
 // Device status word of a context: kernels whose waits are bounded write a

@@ -309,6 +309,77 @@ __global__ void __launch_bounds__(1024) k_stage_tile(StageParams<T> p, TileParam
         stage_update<T, KIND, HV>(p, i, (size_t)i * ntr + (size_t)tv * VEC + v, d0[v], d1[v], d2[v], cu, cv);
 }
 
+// Tiled stage kernel with the weight and index stream software-pipelined in
+// registers: one operator (heat, or a fused advection operator), one lane
+// group of NV lanes per row, each lane keeping the local indices and weights
+// of its row's next RD chunks in flight while it works on the current one
+// (loads issued RD chunks ahead, a ring of registers indexed statically by an
+// unrolled loop).  The per-row arithmetic -- chunks in order, slots in order,
+// the same fused multiply-adds -- is k_stage_tile's with G = 1, so the results
+// are the same bits.
+template <typename T, int VEC, int NV, int RD>
+__global__ void __launch_bounds__(1024) k_stage_tile_pipe(StageParams<T> p, TileParams tp)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sx = reinterpret_cast<T*>(smem_raw);
+    typedef typename VecT<T, VEC>::type V;
+    constexpr int ntr = NV * VEC;
+    const int b = blockIdx.x;
+    const int h0 = __ldg(tp.ptr + b), hn = __ldg(tp.ptr + b + 1) - h0;
+    for (int e = threadIdx.x; e < hn * NV; e += blockDim.x) {
+        const int h = e / NV, v = e - h * NV;
+        const int node = __ldg(tp.nodes + h0 + h);
+        reinterpret_cast<V*>(sx)[(size_t)h * NV + v] = __ldg(reinterpret_cast<const V*>(p.x + (size_t)node * ntr) + v);
+    }
+    __syncthreads();
+    const int tv = threadIdx.x % NV, rl = threadIdx.x / NV;
+    const int i = __ldg(tp.rows + b) + rl;
+    if (i >= __ldg(tp.rows + b + 1)) return;
+    const int nc = p.nc;
+    const size_t o0 = sell_off(i, 0, nc);  // chunk c of row i sits at o0 + 128 c (sliced ELL)
+    T d0[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; v++) d0[v] = T(0);
+    ushort4 lq[RD];
+    T wq[RD][4];
+#pragma unroll
+    for (int r = 0; r < RD; r++)
+        if (r < nc) {
+            lq[r] = __ldg(reinterpret_cast<const ushort4*>(tp.lidx + o0 + 128 * (size_t)r));
+            ld_w4(p.w0 + o0 + 128 * (size_t)r, wq[r]);
+        }
+    for (int c0 = 0; c0 < nc; c0 += RD) {
+#pragma unroll
+        for (int r = 0; r < RD; r++) {
+            const int c = c0 + r;
+            if (c < nc) {
+                const ushort4 l4 = lq[r];
+                T w[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) w[k] = wq[r][k];
+                if (c + RD < nc) {
+                    const size_t o = o0 + 128 * (size_t)(c + RD);
+                    lq[r] = __ldg(reinterpret_cast<const ushort4*>(tp.lidx + o));
+                    ld_w4(p.w0 + o, wq[r]);
+                }
+                const int ll[4] = {l4.x, l4.y, l4.z, l4.w};
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    T xj[VEC];
+                    const V t = reinterpret_cast<const V*>(sx)[(size_t)ll[k] * NV + tv];
+                    memcpy(xj, &t, sizeof(V));
+#pragma unroll
+                    for (int v = 0; v < VEC; v++) d0[v] = Ar<T>::fma(w[k], xj[v], d0[v]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < VEC; v++)
+        stage_update<T, KIND_HEAT, false>(p, i, (size_t)i * ntr + (size_t)tv * VEC + v, d0[v], T(0), T(0), T(0),
+                                          T(0));
+}
+
 // Tiled stage kernel with bulk-copy streaming.  Same per-row arithmetic as
 // k_stage_tile with one chunk lane per row, but the block's weights and local
 // indices -- in the sliced layout one contiguous run per operator per 32-row
@@ -496,6 +567,7 @@ struct TileGeom {
     int tma = 0, halo_bytes = 0, stage_bytes = 0;
     int sched = -1;  // index of the halo's slot schedule the rows read (-1: stencil order)
     int pf = 0;      // L2 prefetch of upcoming chunks
+    int pipe = 0;    // k_stage_tile_pipe: weights and indices pipelined in registers
     size_t smem = 0;
 };
 
@@ -575,6 +647,12 @@ static bool tile_geom(rbffd_pde* P, Shape sh, TileGeom* tg)
         if (t.G != 1 || sh.tma || sh.sched) return false;
         t.pf = 1;
     }
+    if (sh.pipe) {  // one operator streamed, one lane group per row, a compile-time node width
+        if (t.G != 1 || sh.tma || sh.pf || !(P->kind == KIND_HEAT || P->fused) ||
+            !(t.vpn == 1 || t.vpn == 4 || t.vpn == 8))
+            return false;
+        t.pipe = 1;
+    }
     if (sh.tma) {
         if (t.G != 1) return false;
         const int K = P->kind == KIND_HEAT ? 1 : (P->use_hv ? 3 : 2);
@@ -633,6 +711,28 @@ static void launch_tile_v(const StageParams<T>& p, const TileParams& tp, const T
     }
 }
 
+// Depth of the register pipeline of k_stage_tile_pipe (chunks in flight per lane).
+constexpr int PIPE_RD = 4;
+
+template <typename T, int VEC>
+static void launch_pipe_v(const StageParams<T>& p, const TileParams& tp, const TileGeom& t, cudaStream_t s)
+{
+    const int nb = t.h->nblocks;
+    if (t.vpn == 1) {
+        cudaFuncSetAttribute(k_stage_tile_pipe<T, VEC, 1, PIPE_RD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)t.smem);
+        k_stage_tile_pipe<T, VEC, 1, PIPE_RD><<<nb, t.threads, t.smem, s>>>(p, tp);
+    } else if (t.vpn == 4) {
+        cudaFuncSetAttribute(k_stage_tile_pipe<T, VEC, 4, PIPE_RD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)t.smem);
+        k_stage_tile_pipe<T, VEC, 4, PIPE_RD><<<nb, t.threads, t.smem, s>>>(p, tp);
+    } else {
+        cudaFuncSetAttribute(k_stage_tile_pipe<T, VEC, 8, PIPE_RD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)t.smem);
+        k_stage_tile_pipe<T, VEC, 8, PIPE_RD><<<nb, t.threads, t.smem, s>>>(p, tp);
+    }
+}
+
 template <typename T, int VEC, int KIND, bool HV>
 static void launch_tma_v(const StageParams<T>& p, const TileParams& tp, const TileGeom& t, int* status, cudaStream_t s)
 {
@@ -651,7 +751,17 @@ static void launch_stage_t(rbffd_pde* P, const StageParams<T>& p, Shape sh, cuda
             StageParams<T> ps = p;
             ps.w0 = (const T*)P->ws;
             tp.lidx = tg.h->d_lidx_s[tg.sched];
-            launch_tile_v<T, VV, KIND, HV>(ps, tp, tg, s);
+            if (tg.pipe)
+                launch_pipe_v<T, VV>(ps, tp, tg, s);
+            else
+                launch_tile_v<T, VV, KIND, HV>(ps, tp, tg, s);
+            return;
+        }
+        if (tg.pipe) {
+            if (tg.vec == 1)
+                launch_pipe_v<T, 1>(p, tp, tg, s);
+            else
+                launch_pipe_v<T, VV>(p, tp, tg, s);
             return;
         }
         if (tg.tma) {
@@ -792,8 +902,13 @@ static Shape autotune(rbffd_pde* P)
         if (tile_geom(P, c, &tg)) cands.push_back(c);
         Shape cp{1, 0, R, 0, 0, 1};  // upcoming chunks prefetched into L2
         if (tile_geom(P, cp, &tg)) cands.push_back(cp);
+        Shape cq{1, 0, R};  // weights and indices pipelined in registers
+        cq.pipe = 1;
+        if (tile_geom(P, cq, &tg)) cands.push_back(cq);
         if (sched_rows(P) && pde_sched_prepare(P, R) == RBFFD_OK) {  // rows in the conflict-avoiding slot order
             Shape cs{1, 0, R, 0, 1};
+            if (tile_geom(P, cs, &tg)) cands.push_back(cs);
+            cs.pipe = 1;
             if (tile_geom(P, cs, &tg)) cands.push_back(cs);
         }
     }
@@ -1224,20 +1339,24 @@ extern "C" int rbffd_pde_set_tiled_shape(rbffd_pde* P, int rows_per_block, int l
         return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "the unfused (reference) arithmetic gathers from global memory");
     if (rows_per_block < 32 || rows_per_block > 1024 || rows_per_block % 32 || !(lanes == 1 || lanes == 2 || lanes == 4))
         return set_error(P->ctx, RBFFD_ERR_INVALID, "rows_per_block must be a multiple of 32, lanes 1, 2 or 4");
-    if (flags & ~(RBFFD_TILE_STREAM_WEIGHTS | RBFFD_TILE_SLOT_SCHEDULE | RBFFD_TILE_PREFETCH))
+    if (flags & ~(RBFFD_TILE_STREAM_WEIGHTS | RBFFD_TILE_SLOT_SCHEDULE | RBFFD_TILE_PREFETCH | RBFFD_TILE_PIPELINE))
         return set_error(P->ctx, RBFFD_ERR_INVALID, "unknown tiled-shape flags 0x%x", flags);
     const bool stream_weights = flags & RBFFD_TILE_STREAM_WEIGHTS, sched = flags & RBFFD_TILE_SLOT_SCHEDULE,
-               pf = flags & RBFFD_TILE_PREFETCH;
-    if ((stream_weights || sched || pf) && lanes != 1)
-        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights, slot schedules and prefetch use one lane per row");
-    if ((int)stream_weights + (int)sched + (int)pf > 1)
-        return set_error(P->ctx, RBFFD_ERR_INVALID, "streamed weights, a slot schedule and prefetch do not combine");
+               pf = flags & RBFFD_TILE_PREFETCH, pipe = flags & RBFFD_TILE_PIPELINE;
+    if ((stream_weights || sched || pf || pipe) && lanes != 1)
+        return set_error(P->ctx, RBFFD_ERR_INVALID,
+                         "streamed weights, slot schedules, prefetch and the register pipeline use one lane per row");
+    if ((int)stream_weights + (int)sched + (int)pf > 1 || (pipe && (stream_weights || pf)))
+        return set_error(P->ctx, RBFFD_ERR_INVALID,
+                         "streamed weights, a slot schedule and prefetch do not combine; the register pipeline "
+                         "combines with a slot schedule only");
     cudaSetDevice(P->ctx->device);
     const Halo* h = nullptr;
     int rc = grid_halo(P->g, rows_per_block, &h);
     if (rc) return rc;
     if (sched && (rc = pde_sched_prepare(P, rows_per_block))) return rc;
     Shape c{lanes, 0, rows_per_block, stream_weights ? 1 : 0, sched ? 1 : 0, pf ? 1 : 0};
+    c.pipe = pipe ? 1 : 0;
     TileGeom tg;
     if (!tile_geom(P, c, &tg))
         return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "tiled shape (%d rows, %d lanes) does not fit this PDE",
@@ -1258,7 +1377,7 @@ extern "C" int rbffd_pde_get_tile_flags(rbffd_pde* P, int* flags)
 {
     if (!P || !flags) return RBFFD_ERR_INVALID;
     *flags = (P->shape.tma ? RBFFD_TILE_STREAM_WEIGHTS : 0) | (P->shape.sched ? RBFFD_TILE_SLOT_SCHEDULE : 0) |
-             (P->shape.pf ? RBFFD_TILE_PREFETCH : 0);
+             (P->shape.pf ? RBFFD_TILE_PREFETCH : 0) | (P->shape.pipe ? RBFFD_TILE_PIPELINE : 0);
     return RBFFD_OK;
 }
 
@@ -1311,7 +1430,8 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
         if (full > 0) {
             if (!P->gexec || P->g_dt != dt || P->g_steps != chunk || P->g_shape.lanes != sh.lanes ||
                 P->g_shape.block != sh.block || P->g_shape.tile != sh.tile || P->g_shape.tma != sh.tma ||
-                P->g_shape.sched != sh.sched || P->g_shape.pf != sh.pf || P->g_shape.plain != sh.plain) {
+                P->g_shape.sched != sh.sched || P->g_shape.pf != sh.pf || P->g_shape.plain != sh.plain ||
+                P->g_shape.pipe != sh.pipe) {
                 if (P->gexec) {
                     cudaGraphExecDestroy(P->gexec);
                     P->gexec = nullptr;

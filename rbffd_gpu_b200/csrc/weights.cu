@@ -381,6 +381,97 @@ __device__ int team_eliminate(const Team& T, double* a, int m, int K, int lda, d
     return 0;
 }
 
+// Unblocked elimination with one team barrier per step.  Rows are not
+// swapped in memory: perm (2 m ints, two buffers) maps a logical row to its
+// physical row, and step k writes the next map while it reads the current
+// one; the pivot candidates are double-buffered the same way.  Each warp
+// forms the multiplier of each of its rows itself (every lane divides) and
+// updates the row against the pivot row held in registers.  The arithmetic --
+// pivots, multipliers, the fma sequence of every element -- is
+// team_eliminate's; only where a row lives changes.  On return the final map
+// is perm + (m & 1) * m (logical row k at physical row map[k]).
+__device__ int team_eliminate_perm(const Team& T, double* a, int m, int K, int lda, double* cand_v, int* cand_r,
+                                   int* perm)
+{
+    const int ld = m + K;
+    const int nw = T.nwarps(), w = T.warp(), lane = T.lane();
+    for (int i = T.tid; i < m; i += T.size) perm[i] = i;
+    team_pivot_column0(T, a, m, lda, cand_v, cand_r);  // candidates buffer 0
+    T.sync();
+    for (int k = 0; k < m; k++) {
+        const int par = k & 1;
+        const double* cv = cand_v + par * MAX_WARPS;
+        const int* cr = cand_r + par * MAX_WARPS;
+        double bv = cv[0];
+        int p = cr[0];
+        for (int q = 1; q < nw; q++) {
+            const double v = cv[q];
+            const int r = cr[q];
+            if (v > bv || (v == bv && r < p)) { bv = v; p = r; }
+        }
+        if (!(bv > 0.0)) return k + 1;
+        const int* P = perm + par * m;
+        int* Q = perm + (par ^ 1) * m;
+        for (int i = T.tid; i < m; i += T.size) Q[i] = i == k ? P[p] : (i == p ? P[k] : P[i]);
+        const int prow = P[p];  // the pivot's physical row
+        const double piv = a[prow * lda + k];
+        double pr[ELIM_CHUNKS];
+#pragma unroll
+        for (int c = 0; c < ELIM_CHUNKS; c++) {
+            const int j = k + 1 + lane + 32 * c;
+            pr[c] = j < ld ? a[prow * lda + j] : 0.0;
+        }
+        double nbv = -1.0;
+        int nbr = INT_MAX;
+#pragma unroll 2
+        for (int i = k + 1 + w; i < m; i += nw) {
+            double* ai = a + (size_t)(i == p ? P[k] : P[i]) * lda;
+            const double l = ai[k] / piv;
+#pragma unroll
+            for (int c = 0; c < ELIM_CHUNKS; c++) {
+                const int j = k + 1 + lane + 32 * c;
+                if (j < ld) {
+                    const double v = __fma_rn(-l, pr[c], ai[j]);
+                    ai[j] = v;
+                    if (c == 0 && lane == 0) {
+                        const double av = fabs(v);
+                        if (av > nbv) { nbv = av; nbr = i; }
+                    }
+                }
+            }
+        }
+        if (lane == 0) {
+            cand_v[(par ^ 1) * MAX_WARPS + w] = nbv;
+            cand_r[(par ^ 1) * MAX_WARPS + w] = nbr;
+        }
+        T.sync();
+    }
+    return 0;
+}
+
+// Back substitution of team_back_substitute for rows placed by the map F.
+__device__ void team_back_substitute_perm(const Team& T, double* a, int m, int K, int lda, const int* F)
+{
+    for (int c = T.warp(); c < K; c += T.nwarps()) {
+        const int col = m + c;
+        for (int k = m - 1; k >= 0; k--) {
+            const int rk = F[k];
+            double xk = 0.0;
+            if (T.lane() == 0) {
+                xk = a[rk * lda + col] / a[rk * lda + k];
+                a[rk * lda + col] = xk;
+            }
+            xk = __shfl_sync(0xffffffffu, xk, 0);
+            for (int i = T.lane(); i < k; i += 32) {
+                const int ri = F[i];
+                a[ri * lda + col] = __fma_rn(-xk, a[ri * lda + k], a[ri * lda + col]);
+            }
+            __syncwarp();
+        }
+    }
+    T.sync();
+}
+
 // Pivot candidates of column k over rows [k, m): one per warp, first maximum.
 __device__ void team_column_candidates(const Team& T, const double* a, int lda, int k, int m, double* cand_v,
                                        int* cand_r)
@@ -636,29 +727,41 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
     return m;
 }
 
-// One system end to end by one team: assemble, eliminate (blocked or not),
-// back-substitute, store the weights of row r.  a: the team's shared memory,
-// [a: m rows at stride lda] [xs: 3 n_pad] [frame: 8] [cand_v: MAX_WARPS]
-// [cand_r: MAX_WARPS ints].
-__device__ void team_solve(const Team& T, const WParams& P, int r, double* a, int m, int lda, int blocked)
+// The elimination variants a size class can use (same arithmetic, same results).
+enum { ELIM_UNBLOCKED = 0, ELIM_BLOCKED = 1, ELIM_PERM = 2 };
+
+// One system end to end by one team: assemble, eliminate, back-substitute,
+// store the weights of row r.  a: the team's shared memory,
+// [a: m rows at stride lda] [xs: 3 n_pad] [frame: 8] [cand_v: 2 MAX_WARPS]
+// [cand_r: 2 MAX_WARPS ints] [perm: 2 m ints].
+__device__ void team_solve(const Team& T, const WParams& P, int r, double* a, int m, int lda, int mode)
 {
     double* xs = a + (size_t)m * lda;
     double* fr = xs + 3 * P.n_pad;
     double* cand_v = fr + 8;
-    int* cand_r = (int*)(cand_v + MAX_WARPS);
+    int* cand_r = (int*)(cand_v + 2 * MAX_WARPS);
+    int* perm = cand_r + 2 * MAX_WARPS;
     const int K = P.K;
     int n;
     team_assemble(T, P, r, a, xs, fr, n, lda);
-    const int st = blocked ? team_eliminate_blocked<8>(T, a, m, K, lda, cand_v, cand_r)
-                           : team_eliminate(T, a, m, K, lda, cand_v, cand_r);
+    const int st = mode == ELIM_BLOCKED ? team_eliminate_blocked<8>(T, a, m, K, lda, cand_v, cand_r)
+                   : mode == ELIM_PERM  ? team_eliminate_perm(T, a, m, K, lda, cand_v, cand_r, perm)
+                                        : team_eliminate(T, a, m, K, lda, cand_v, cand_r);
     const bool ok = st == 0;
-    if (ok) team_back_substitute(T, a, m, K, lda);
+    const int* F = perm + (m & 1) * m;  // ELIM_PERM: where each logical row lives
+    if (ok) {
+        if (mode == ELIM_PERM)
+            team_back_substitute_perm(T, a, m, K, lda, F);
+        else
+            team_back_substitute(T, a, m, K, lda);
+    }
     if (!ok && T.tid == 0) atomicMin(P.status, r + 1);
     // store: weights[type][r][j] = W(j, col) * scale (rbffd.cpp:300-306), row r of the sliced ELL
     for (int e = T.tid; e < K * P.n4; e += T.size) {
         int c = e / P.n4, j = e - c * P.n4;
         double scale = P.opbit[c] == RBFFD_HV ? P.hv_scale : 1.0;
-        double v = (j < n) ? (ok ? a[j * lda + m + c] * scale : __longlong_as_double(0x7ff8000000000000ll)) : 0.0;
+        const int rj = mode == ELIM_PERM && j < n ? F[j] : j;
+        double v = (j < n) ? (ok ? a[rj * lda + m + c] * scale : __longlong_as_double(0x7ff8000000000000ll)) : 0.0;
         P.w[c][sell_elem(r, j, P.n4 >> 2)] = v;
     }
     T.sync();
@@ -727,18 +830,29 @@ __global__ void __launch_bounds__(512) k_gesv(double* A, double* B, int* info, i
     const int ld = m + K;
     double* a = smem + (size_t)T.id * team_stride;
     double* cand_v = a + (size_t)m * ld;
-    int* cand_r = (int*)(cand_v + MAX_WARPS);
+    int* cand_r = (int*)(cand_v + 2 * MAX_WARPS);
+    int* perm = cand_r + 2 * MAX_WARPS;
+    const int* F = perm + (m & 1) * m;
     for (int b = blockIdx.x * teams_per_cta + T.id; b < batch; b += gridDim.x * teams_per_cta) {
         const double* Ab = A + (size_t)b * m * m;
         double* Bb = B + (size_t)b * m * K;
         for (int e = T.tid; e < m * m; e += T.size) a[(e / m) * ld + e % m] = Ab[e];
         for (int e = T.tid; e < m * K; e += T.size) a[(e / K) * ld + m + e % K] = Bb[e];
         T.sync();
-        const int st = blocked ? team_eliminate_blocked<8>(T, a, m, K, ld, cand_v, cand_r)
-                               : team_eliminate(T, a, m, K, ld, cand_v, cand_r);
-        if (st == 0) team_back_substitute(T, a, m, K, ld);
+        const int st = blocked == ELIM_BLOCKED ? team_eliminate_blocked<8>(T, a, m, K, ld, cand_v, cand_r)
+                       : blocked == ELIM_PERM  ? team_eliminate_perm(T, a, m, K, ld, cand_v, cand_r, perm)
+                                               : team_eliminate(T, a, m, K, ld, cand_v, cand_r);
+        if (st == 0) {
+            if (blocked == ELIM_PERM)
+                team_back_substitute_perm(T, a, m, K, ld, F);
+            else
+                team_back_substitute(T, a, m, K, ld);
+        }
         if (T.tid == 0) info[b] = st;
-        for (int e = T.tid; e < m * K; e += T.size) Bb[e] = a[(e / K) * ld + m + e % K];
+        for (int e = T.tid; e < m * K; e += T.size) {
+            const int row = e / K;
+            Bb[e] = a[(blocked == ELIM_PERM ? F[row] : row) * ld + m + e % K];
+        }
         T.sync();
     }
 }
@@ -746,7 +860,8 @@ __global__ void __launch_bounds__(512) k_gesv(double* A, double* B, int* info, i
 size_t team_bytes_w(int m, int K, int n_pad, int lda = 0)
 {
     if (lda == 0) lda = m + K;
-    return ((size_t)m * lda + 3 * (size_t)n_pad + 8 + 2 * MAX_WARPS) * sizeof(double);
+    // a, xs, frame, cand_v (2 MAX_WARPS), cand_r (2 MAX_WARPS ints), perm (2 m ints)
+    return ((size_t)m * lda + 3 * (size_t)n_pad + 8 + 2 * MAX_WARPS + MAX_WARPS + (size_t)m) * sizeof(double);
 }
 
 int max_smem_optin(rbffd_ctx* ctx)
@@ -783,8 +898,9 @@ static std::vector<WShape> w_candidates(int m, size_t stride_bytes, int smem_max
         if ((size_t)(W_CTA / tw) * stride_bytes > (size_t)smem_max) continue;
         if (m <= 40 && tw > 64) continue;   // small systems: narrow teams only
         if (m > 96 && tw < 128) continue;   // large systems: wide teams only
-        out.push_back(WShape{tw, 0});
-        if (m >= 24) out.push_back(WShape{tw, 1});
+        out.push_back(WShape{tw, ELIM_UNBLOCKED});
+        out.push_back(WShape{tw, ELIM_PERM});
+        if (m >= 24) out.push_back(WShape{tw, ELIM_BLOCKED});
     }
     return out;
 }
@@ -1116,7 +1232,7 @@ extern "C" int rbffd_batched_gesv_dev(rbffd_ctx* ctx, int m, int nrhs, int batch
     if (!ctx || !A || !B || !info || m < 1 || m > 160 || nrhs < 1 || nrhs > 16 || batch < 0) return RBFFD_ERR_INVALID;
     if (batch == 0) return RBFFD_OK;
     cudaSetDevice(ctx->device);
-    size_t tb = ((size_t)m * (m + nrhs) + 2 * MAX_WARPS) * sizeof(double);
+    size_t tb = ((size_t)m * (m + nrhs) + 2 * MAX_WARPS + MAX_WARPS + m) * sizeof(double);  // a, candidates, map
     tb = (tb + 127) / 128 * 128;
     int smem_max = max_smem_optin(ctx);
     if (tb > (size_t)smem_max) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "system %d x %d exceeds shared memory", m, m);
@@ -1129,9 +1245,11 @@ extern "C" int rbffd_batched_gesv_dev(rbffd_ctx* ctx, int m, int nrhs, int batch
     int per_sm = 0;
     RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gesv, block, smem));
     int grid = std::max(1, std::min((batch + teams - 1) / teams, std::max(1, per_sm) * ctx->sm_count));
-    // blocked elimination above 40 unknowns (the same arithmetic, fewer passes over the trailing matrix)
+    // the three eliminations (the same arithmetic): row swaps up to 40 unknowns, a row map from 41 to 96,
+    // blocked above
     k_gesv<<<grid, block, smem, ctx->stream>>>((double*)A, (double*)B, (int*)info, m, nrhs, batch, team,
-                                                (int)(tb / sizeof(double)), m > 40 ? 1 : 0);
+                                                (int)(tb / sizeof(double)),
+                                                m <= 40 ? ELIM_UNBLOCKED : (m <= 96 ? ELIM_PERM : ELIM_BLOCKED));
     RBFFD_CUDA_TRY(ctx, cudaGetLastError());
     RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return RBFFD_OK;

@@ -372,3 +372,55 @@ def test_heat_benchmark_grid_parity(ctx):
     assert rel_l2(_gpu_heat(h, steps, dt, shape=None, graph=True), ref) <= 1e-12
     assert rel_l2(_gpu_heat(h, steps, dt, dtype=R.F32, shape=None, graph=True), ref) <= 1e-5
     grid.close()
+
+
+@pytest.mark.parametrize("dtype,ntr", [(R.F64, 1), (R.F64, 8), (R.F64, 16), (R.F32, 1), (R.F32, 4), (R.F32, 16)])
+def test_register_pipelined_tile_heat(heat, dtype, ntr):
+    """The tiled kernel with the weight and index stream pipelined in
+    registers (RBFFD_TILE_PIPELINE): the same bits as the plain tiled kernel
+    with one lane group per row, for every node width it serves; FP64 equals
+    the oracle bit for bit."""
+    rng = np.random.default_rng(40 + ntr)
+    u0 = heat["u0"] if ntr == 1 else heat["u0"][:, None] * (1.0 + 0.1 * rng.random((1, ntr)))
+    steps, dt = 30, 1e-6
+
+    def run(pipe, rows=128):
+        pde = R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=dtype, ntracers=ntr)
+        pde.setTiledShape(rows, 1, pipeline=pipe)
+        assert pde.getTileFlags() == (R.TimeDependentPDE.TILE_PIPELINE if pipe else 0)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, dt, steps, graph=True)
+        out = pde.getLocalSolution()
+        pde.close()
+        return out
+
+    piped = run(True)
+    assert np.array_equal(piped, run(False))
+    assert np.array_equal(run(True, 64), piped)
+    if dtype == R.F64:
+        assert np.array_equal(piped, O.rk4_heat(heat["st"], None, heat["W"][O.LSFC], u0, dt, steps))
+
+
+def test_register_pipelined_tile_fused_advection_with_schedule(bell):
+    """16-tracer FP32 advection on its fused operator, rows in the slot
+    schedule: the pipelined kernel gives the plain scheduled kernel's bits; a
+    three-operator PDE refuses the pipeline."""
+    T = 16
+    rng = np.random.default_rng(8)
+    cen = rng.normal(size=(T, 3))
+    cen /= np.linalg.norm(cen, axis=1)[:, None]
+    u0 = np.exp(-8.0 * ((bell["xyz"][:, None, :] - cen[None, :, :]) ** 2).sum(2))
+    outs = []
+    for pipe in (True, False):
+        pde = R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=R.F32, ntracers=T)
+        pde.setFusedOperator(True)
+        pde.setTiledShape(128, 1, slot_schedule=True, pipeline=pipe)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, bell["p"]["dt"], 10, graph=True)
+        outs.append(pde.getLocalSolution())
+        pde.close()
+    assert np.array_equal(outs[0], outs[1])
+    p3 = R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=R.F32, ntracers=T)
+    with pytest.raises(R.RbffdError):
+        p3.setTiledShape(128, 1, pipeline=True)
+    p3.close()

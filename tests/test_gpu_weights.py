@@ -95,7 +95,9 @@ def test_elimination_bit_exact_on_identical_systems(ctx, deg):
         assert np.array_equal(X[k], O.lu_solve(A[k], B[k]))
 
 
-@pytest.mark.parametrize("m,nrhs", [(1, 1), (7, 2), (32, 3), (33, 1), (100, 4), (126, 3), (160, 2)])
+# sizes that reach each elimination: row swaps (m <= 40), a row map (41-96), blocked (> 96)
+@pytest.mark.parametrize("m,nrhs", [(1, 1), (7, 2), (32, 3), (33, 1), (41, 3), (67, 1), (96, 2), (100, 4), (126, 3),
+                                    (160, 2)])
 def test_elimination_bit_exact_random(ctx, m, nrhs):
     rng = np.random.default_rng(m)
     A = rng.normal(size=(9, m, m))
