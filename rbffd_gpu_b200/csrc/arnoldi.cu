@@ -378,6 +378,7 @@ extern "C" int rbffd_eigen_rightmost(rbffd_grid* g, unsigned der_type, int use_h
     int j0 = 0, nmv = 0, kk = nev, it = 0;
     std::vector<cd> th;
     std::vector<double> est;
+    double scale = 0.0;  // largest |Ritz value|: the spectral scale of the convergence test
     bool converged = false;
     for (it = 0; it < max_restarts; it++) {
         // extend the factorisation from j0 to m columns
@@ -406,7 +407,7 @@ extern "C" int rbffd_eigen_rightmost(rbffd_grid* g, unsigned der_type, int use_h
         if (!hess_eigs(m, Hsq.data(), th))
             return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "the projected eigenproblem did not converge");
         std::stable_sort(th.begin(), th.end(), [](const cd& a, const cd& b) { return a.real() > b.real(); });
-        double scale = 0.0;
+        scale = 0.0;
         for (const cd& t : th) scale = std::max(scale, std::abs(t));
         kk = nev;
         // keep a complex pair together
@@ -489,9 +490,9 @@ extern "C" int rbffd_eigen_rightmost(rbffd_grid* g, unsigned der_type, int use_h
         im[i] = th[i].imag();
         if (ritz_resid) ritz_resid[i] = i < (int)est.size() ? est[i] : 0.0;
     }
-    int nc = 0;
+    int nc = 0;  // the loop's own test
     for (int i = 0; i < nout && i < (int)est.size(); i++)
-        if (est[i] <= tol * std::max(std::abs(th[i]), 1e-3 * std::abs(th[0]) + 1e-300)) nc++;
+        if (est[i] <= tol * std::max(std::abs(th[i]), 1e-3 * scale)) nc++;
     if (nconv) *nconv = nc;
     if (restarts) *restarts = it;
     if (matvecs) *matvecs = nmv;
