@@ -422,17 +422,29 @@ int rbffd_pde_get_shape(rbffd_pde* pde, int* lanes_per_row, int* block_threads);
  *     of chunks a few steps ahead (pays where the weight stream comes from
  *     HBM); the arithmetic is unchanged;
  *   RBFFD_TILE_PIPELINE: PDEs that stream one operator (heat, or a fused
- *     advection operator) with 1, 4, 8 or 16 (FP32) / 1, 8, 16 (FP64) values
- *     per node: each lane keeps the local indices and weights of its row's
- *     next four chunks in flight in registers; the arithmetic is unchanged.
+ *     advection operator) with 1, 4, 8, 16 or 32 (FP32) / 1, 2, 4, 8 or 16
+ *     (FP64) values per node: each lane keeps the local indices and weights of
+ *     its row's next four chunks in flight in registers; the arithmetic is
+ *     unchanged;
+ *   RBFFD_TILE_DOUBLE_BUFFER: the same PDEs: a persistent grid (as many
+ *     blocks as fit on the device) whose blocks walk the tiles and copy the
+ *     next tile's node values into a second shared-memory buffer (cp.async)
+ *     while they compute the current one; the arithmetic is unchanged.
+ *     Refused where a block's halo exceeds 8 nodes per row.
  * At most one of the first three; RBFFD_TILE_PIPELINE combines with
- * RBFFD_TILE_SLOT_SCHEDULE only.  (flags = 1, the former stream_weights
- * argument, keeps its meaning.)
+ * RBFFD_TILE_SLOT_SCHEDULE only, RBFFD_TILE_DOUBLE_BUFFER with none.
+ * (flags = 1, the former stream_weights argument, keeps its meaning.)
  * Returns RBFFD_ERR_UNSUPPORTED if the staged data do not fit shared memory
  * or the flags do not apply to the PDE.
  * get_tiling reports 0 when the stage kernel gathers from global memory;
  * get_tile_flags the flags of the shape in use (set or autotuned). */
-enum { RBFFD_TILE_STREAM_WEIGHTS = 1, RBFFD_TILE_SLOT_SCHEDULE = 2, RBFFD_TILE_PREFETCH = 4, RBFFD_TILE_PIPELINE = 8 };
+enum {
+    RBFFD_TILE_STREAM_WEIGHTS = 1,
+    RBFFD_TILE_SLOT_SCHEDULE = 2,
+    RBFFD_TILE_PREFETCH = 4,
+    RBFFD_TILE_PIPELINE = 8,
+    RBFFD_TILE_DOUBLE_BUFFER = 16
+};
 int rbffd_pde_set_tiled_shape(rbffd_pde* pde, int rows_per_block, int lanes, int flags);
 int rbffd_pde_get_tiling(rbffd_pde* pde, int* rows_per_block);
 int rbffd_pde_get_tile_flags(rbffd_pde* pde, int* flags);

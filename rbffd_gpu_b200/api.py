@@ -645,22 +645,25 @@ class TimeDependentPDE:
         """FP32 advection: one fused operator -(cu Wl + cv Wt) + Whv per stage."""
         self.ctx.check(self.ctx.L.rbffd_pde_set_fused_operator(self.h, int(bool(on))), "set_fused_operator")
 
-    TILE_STREAM_WEIGHTS, TILE_SLOT_SCHEDULE, TILE_PREFETCH, TILE_PIPELINE = 1, 2, 4, 8
+    TILE_STREAM_WEIGHTS, TILE_SLOT_SCHEDULE, TILE_PREFETCH, TILE_PIPELINE, TILE_DOUBLE_BUFFER = 1, 2, 4, 8, 16
 
     def setTiledShape(self, rows_per_block, lanes=1, stream_weights=False, slot_schedule=False, prefetch=False,
-                      pipeline=False):
+                      pipeline=False, double_buffer=False):
         """Tiled stage kernel of rows_per_block rows; stream_weights: bulk-copy
         weight streaming; slot_schedule: FP32 rows read their slots in the
         halo's conflict-avoiding order (one operator, 4/8/16 tracers);
         prefetch: upcoming chunks of weights and indices asked of L2;
         pipeline: one operator streamed, the next chunks' weights and indices
-        kept in flight in registers (combines with slot_schedule)."""
+        kept in flight in registers (combines with slot_schedule);
+        double_buffer: one operator streamed by a persistent grid that copies
+        the next tile's halo in while it computes the current one."""
         flags = ((self.TILE_STREAM_WEIGHTS if stream_weights else 0) | (self.TILE_SLOT_SCHEDULE if slot_schedule else 0) |
-                 (self.TILE_PREFETCH if prefetch else 0) | (self.TILE_PIPELINE if pipeline else 0))
+                 (self.TILE_PREFETCH if prefetch else 0) | (self.TILE_PIPELINE if pipeline else 0) |
+                 (self.TILE_DOUBLE_BUFFER if double_buffer else 0))
         self.ctx.check(self.ctx.L.rbffd_pde_set_tiled_shape(self.h, rows_per_block, lanes, flags), "set_tiled_shape")
 
     def getTileFlags(self):
-        """Flags of the tiled shape in use: TILE_STREAM_WEIGHTS | TILE_SLOT_SCHEDULE."""
+        """Flags of the tiled shape in use (TILE_* bits)."""
         f = ctypes.c_int()
         self.ctx.check(self.ctx.L.rbffd_pde_get_tile_flags(self.h, ctypes.byref(f)))
         return f.value

@@ -40,6 +40,8 @@ struct Shape {
     int plain = 0; // FP64, one tracer, one lane per row, global gathers: the reference build's arithmetic
                    // (every multiply-add a rounded product, then a rounded sum; RBFFD_ARITH_UNFUSED)
     int pipe = 0;  // tiled, one operator, one lane group per row: weights and indices pipelined in registers
+    int db = 0;    // tiled, one operator, one lane group per row: persistent blocks, next tile's halo copied in
+                   // (cp.async) while the current one is computed
 };
 
 // Device status word of a context: kernels whose waits are bounded write a

@@ -380,6 +380,107 @@ __global__ void __launch_bounds__(1024) k_stage_tile_pipe(StageParams<T> p, Tile
                                           T(0));
 }
 
+// Asynchronous global -> shared copies of one node record's vector (16, 8 or
+// 4 bytes; cp.async), committed as a group and waited for by group count.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_vec(void* smem_dst, const void* gsrc)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    if (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(gsrc), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Halo slots a thread stages per tile in k_stage_tile_db (max halo x NV / threads, rounded up).
+constexpr int DB_SLOTS = 8;
+
+// Persistent tiled stage kernel for one streamed operator (heat, or a fused
+// advection operator), one lane group of NV lanes per row: each block takes
+// tiles b = blockIdx.x, blockIdx.x + gridDim.x, ... and keeps two halo
+// buffers, so the node values of its next tile are copied in (cp.async, 16
+// bytes per lane) while it works on the current one; the node indices of the
+// tile after that are loaded into registers a tile ahead, so issuing the
+// copies never waits on them.  The per-row arithmetic is k_stage_tile's with
+// G = 1 (chunks and slots in order, the same fused multiply-adds), so the
+// results are the same bits.
+template <typename T, int VEC, int NV>
+__global__ void __launch_bounds__(1024) k_stage_tile_db(StageParams<T> p, TileParams tp, int nblocks, int buf_vecs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    typedef typename VecT<T, VEC>::type V;
+    constexpr int ntr = NV * VEC;
+    V* const buf0 = reinterpret_cast<V*>(smem_raw);  // buffer k of the two at buf0 + k * buf_vecs
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int nodes_next[DB_SLOTS];  // node of each of this thread's halo slots, for the tile to be copied next
+    auto load_nodes = [&](int tb) {
+        if (tb >= nblocks) return;
+        const int h0 = __ldg(tp.ptr + tb), hn = __ldg(tp.ptr + tb + 1) - h0;
+#pragma unroll
+        for (int q = 0; q < DB_SLOTS; q++) {
+            const int e = tid + q * nt;
+            nodes_next[q] = e < hn * NV ? __ldg(tp.nodes + h0 + e / NV) : -1;
+        }
+    };
+    auto issue = [&](int tb, V* dst) {  // copies of tile tb's halo (node indices from nodes_next)
+        if (tb < nblocks) {
+#pragma unroll
+            for (int q = 0; q < DB_SLOTS; q++) {
+                const int e = tid + q * nt;
+                if (nodes_next[q] >= 0)
+                    cp_async_vec<sizeof(V)>(dst + e, reinterpret_cast<const V*>(p.x + (size_t)nodes_next[q] * ntr) +
+                                                         (e % NV));
+            }
+        }
+        cp_async_commit();  // an empty group past the last tile keeps the group count regular
+    };
+    int b = blockIdx.x;
+    load_nodes(b);
+    issue(b, buf0);
+    load_nodes(b + gridDim.x);
+    const int tv = tid % NV, rl = tid / NV;
+    const int nc = p.nc;
+    for (int it = 0; b < nblocks; it++, b += gridDim.x) {
+        issue(b + gridDim.x, buf0 + ((it + 1) & 1) * (size_t)buf_vecs);
+        load_nodes(b + 2 * gridDim.x);
+        cp_async_wait<1>();  // this thread's copies of tile b have landed
+        __syncthreads();     // ... and everyone's
+        const V* sx = buf0 + (it & 1) * (size_t)buf_vecs;
+        const int i = __ldg(tp.rows + b) + rl;
+        if (i < __ldg(tp.rows + b + 1)) {
+            T d0[VEC];
+#pragma unroll
+            for (int v = 0; v < VEC; v++) d0[v] = T(0);
+            const size_t o0 = sell_off(i, 0, nc);
+#pragma unroll 2
+            for (int c = 0; c < nc; c++) {
+                const size_t o = o0 + 128 * (size_t)c;
+                const ushort4 l4 = __ldg(reinterpret_cast<const ushort4*>(tp.lidx + o));
+                const int ll[4] = {l4.x, l4.y, l4.z, l4.w};
+                T w[4];
+                ld_w4(p.w0 + o, w);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    T xj[VEC];
+                    const V t = sx[(size_t)ll[k] * NV + tv];
+                    memcpy(xj, &t, sizeof(V));
+#pragma unroll
+                    for (int v = 0; v < VEC; v++) d0[v] = Ar<T>::fma(w[k], xj[v], d0[v]);
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < VEC; v++)
+                stage_update<T, KIND_HEAT, false>(p, i, (size_t)i * ntr + (size_t)tv * VEC + v, d0[v], T(0), T(0),
+                                                  T(0), T(0));
+        }
+        __syncthreads();  // tile b's buffer is free for the copies issued next iteration
+    }
+    cp_async_wait<0>();
+}
+
 // Tiled stage kernel with bulk-copy streaming.  Same per-row arithmetic as
 // k_stage_tile with one chunk lane per row, but the block's weights and local
 // indices -- in the sliced layout one contiguous run per operator per 32-row
@@ -568,6 +669,7 @@ struct TileGeom {
     int sched = -1;  // index of the halo's slot schedule the rows read (-1: stencil order)
     int pf = 0;      // L2 prefetch of upcoming chunks
     int pipe = 0;    // k_stage_tile_pipe: weights and indices pipelined in registers
+    int db = 0;      // k_stage_tile_db: persistent blocks with two halo buffers
     size_t smem = 0;
 };
 
@@ -649,9 +751,16 @@ static bool tile_geom(rbffd_pde* P, Shape sh, TileGeom* tg)
     }
     if (sh.pipe) {  // one operator streamed, one lane group per row, a compile-time node width
         if (t.G != 1 || sh.tma || sh.pf || !(P->kind == KIND_HEAT || P->fused) ||
-            !(t.vpn == 1 || t.vpn == 4 || t.vpn == 8))
+            !(t.vpn == 1 || t.vpn == 2 || t.vpn == 4 || t.vpn == 8))
             return false;
         t.pipe = 1;
+    }
+    if (sh.db) {  // as pipe, and every block's halo within DB_SLOTS copies per thread
+        if (t.G != 1 || sh.tma || sh.pf || sh.pipe || !(P->kind == KIND_HEAT || P->fused) ||
+            !(t.vpn == 1 || t.vpn == 2 || t.vpn == 4 || t.vpn == 8) || t.h->max_halo > DB_SLOTS * sh.tile)
+            return false;
+        t.db = 1;
+        t.smem *= 2;
     }
     if (sh.tma) {
         if (t.G != 1) return false;
@@ -722,6 +831,10 @@ static void launch_pipe_v(const StageParams<T>& p, const TileParams& tp, const T
         cudaFuncSetAttribute(k_stage_tile_pipe<T, VEC, 1, PIPE_RD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)t.smem);
         k_stage_tile_pipe<T, VEC, 1, PIPE_RD><<<nb, t.threads, t.smem, s>>>(p, tp);
+    } else if (t.vpn == 2) {
+        cudaFuncSetAttribute(k_stage_tile_pipe<T, VEC, 2, PIPE_RD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)t.smem);
+        k_stage_tile_pipe<T, VEC, 2, PIPE_RD><<<nb, t.threads, t.smem, s>>>(p, tp);
     } else if (t.vpn == 4) {
         cudaFuncSetAttribute(k_stage_tile_pipe<T, VEC, 4, PIPE_RD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)t.smem);
@@ -731,6 +844,38 @@ static void launch_pipe_v(const StageParams<T>& p, const TileParams& tp, const T
                              (int)t.smem);
         k_stage_tile_pipe<T, VEC, 8, PIPE_RD><<<nb, t.threads, t.smem, s>>>(p, tp);
     }
+}
+
+// Persistent grid of k_stage_tile_db: as many blocks as fit on the device at
+// once (occupancy x SMs), at most one per tile.
+template <typename T, int VEC, int NV>
+static void launch_db_nv(const StageParams<T>& p, const TileParams& tp, const TileGeom& t, int device, cudaStream_t s)
+{
+    auto kern = k_stage_tile_db<T, VEC, NV>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem);
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, t.threads, t.smem);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int nb = t.h->nblocks;
+    const int grid = std::max(1, std::min(nb, std::max(per_sm, 1) * sms));
+    kern<<<grid, t.threads, t.smem, s>>>(p, tp, nb, (int)(t.smem / 2 / sizeof(typename VecT<T, VEC>::type)));
+}
+
+template <typename T, int VEC>
+static void launch_db_v(const StageParams<T>& p, const TileParams& tp, const TileGeom& t, int device, cudaStream_t s)
+{
+    if constexpr (VEC == 1) {  // one value per node
+        launch_db_nv<T, 1, 1>(p, tp, t, device, s);
+        return;
+    }
+    if (t.vpn == 1)
+        launch_db_nv<T, VEC, 1>(p, tp, t, device, s);
+    else if (t.vpn == 2)
+        launch_db_nv<T, VEC, 2>(p, tp, t, device, s);
+    else if (t.vpn == 4)
+        launch_db_nv<T, VEC, 4>(p, tp, t, device, s);
+    else
+        launch_db_nv<T, VEC, 8>(p, tp, t, device, s);
 }
 
 template <typename T, int VEC, int KIND, bool HV>
@@ -755,6 +900,13 @@ static void launch_stage_t(rbffd_pde* P, const StageParams<T>& p, Shape sh, cuda
                 launch_pipe_v<T, VV>(ps, tp, tg, s);
             else
                 launch_tile_v<T, VV, KIND, HV>(ps, tp, tg, s);
+            return;
+        }
+        if (tg.db) {
+            if (tg.vec == 1)
+                launch_db_v<T, 1>(p, tp, tg, P->ctx->device, s);
+            else
+                launch_db_v<T, VV>(p, tp, tg, P->ctx->device, s);
             return;
         }
         if (tg.pipe) {
@@ -905,6 +1057,9 @@ static Shape autotune(rbffd_pde* P)
         Shape cq{1, 0, R};  // weights and indices pipelined in registers
         cq.pipe = 1;
         if (tile_geom(P, cq, &tg)) cands.push_back(cq);
+        Shape cd{1, 0, R};  // persistent blocks, next tile's halo copied in during the current one
+        cd.db = 1;
+        if (tile_geom(P, cd, &tg)) cands.push_back(cd);
         if (sched_rows(P) && pde_sched_prepare(P, R) == RBFFD_OK) {  // rows in the conflict-avoiding slot order
             Shape cs{1, 0, R, 0, 1};
             if (tile_geom(P, cs, &tg)) cands.push_back(cs);
@@ -1339,13 +1494,18 @@ extern "C" int rbffd_pde_set_tiled_shape(rbffd_pde* P, int rows_per_block, int l
         return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "the unfused (reference) arithmetic gathers from global memory");
     if (rows_per_block < 32 || rows_per_block > 1024 || rows_per_block % 32 || !(lanes == 1 || lanes == 2 || lanes == 4))
         return set_error(P->ctx, RBFFD_ERR_INVALID, "rows_per_block must be a multiple of 32, lanes 1, 2 or 4");
-    if (flags & ~(RBFFD_TILE_STREAM_WEIGHTS | RBFFD_TILE_SLOT_SCHEDULE | RBFFD_TILE_PREFETCH | RBFFD_TILE_PIPELINE))
+    if (flags & ~(RBFFD_TILE_STREAM_WEIGHTS | RBFFD_TILE_SLOT_SCHEDULE | RBFFD_TILE_PREFETCH | RBFFD_TILE_PIPELINE |
+                  RBFFD_TILE_DOUBLE_BUFFER))
         return set_error(P->ctx, RBFFD_ERR_INVALID, "unknown tiled-shape flags 0x%x", flags);
     const bool stream_weights = flags & RBFFD_TILE_STREAM_WEIGHTS, sched = flags & RBFFD_TILE_SLOT_SCHEDULE,
-               pf = flags & RBFFD_TILE_PREFETCH, pipe = flags & RBFFD_TILE_PIPELINE;
-    if ((stream_weights || sched || pf || pipe) && lanes != 1)
+               pf = flags & RBFFD_TILE_PREFETCH, pipe = flags & RBFFD_TILE_PIPELINE,
+               db = flags & RBFFD_TILE_DOUBLE_BUFFER;
+    if ((stream_weights || sched || pf || pipe || db) && lanes != 1)
         return set_error(P->ctx, RBFFD_ERR_INVALID,
-                         "streamed weights, slot schedules, prefetch and the register pipeline use one lane per row");
+                         "streamed weights, slot schedules, prefetch, the register pipeline and double-buffered "
+                         "halos use one lane per row");
+    if (db && (stream_weights || sched || pf || pipe))
+        return set_error(P->ctx, RBFFD_ERR_INVALID, "double-buffered halos combine with no other tiled-shape flag");
     if ((int)stream_weights + (int)sched + (int)pf > 1 || (pipe && (stream_weights || pf)))
         return set_error(P->ctx, RBFFD_ERR_INVALID,
                          "streamed weights, a slot schedule and prefetch do not combine; the register pipeline "
@@ -1357,6 +1517,7 @@ extern "C" int rbffd_pde_set_tiled_shape(rbffd_pde* P, int rows_per_block, int l
     if (sched && (rc = pde_sched_prepare(P, rows_per_block))) return rc;
     Shape c{lanes, 0, rows_per_block, stream_weights ? 1 : 0, sched ? 1 : 0, pf ? 1 : 0};
     c.pipe = pipe ? 1 : 0;
+    c.db = db ? 1 : 0;
     TileGeom tg;
     if (!tile_geom(P, c, &tg))
         return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "tiled shape (%d rows, %d lanes) does not fit this PDE",
@@ -1377,7 +1538,8 @@ extern "C" int rbffd_pde_get_tile_flags(rbffd_pde* P, int* flags)
 {
     if (!P || !flags) return RBFFD_ERR_INVALID;
     *flags = (P->shape.tma ? RBFFD_TILE_STREAM_WEIGHTS : 0) | (P->shape.sched ? RBFFD_TILE_SLOT_SCHEDULE : 0) |
-             (P->shape.pf ? RBFFD_TILE_PREFETCH : 0) | (P->shape.pipe ? RBFFD_TILE_PIPELINE : 0);
+             (P->shape.pf ? RBFFD_TILE_PREFETCH : 0) | (P->shape.pipe ? RBFFD_TILE_PIPELINE : 0) |
+             (P->shape.db ? RBFFD_TILE_DOUBLE_BUFFER : 0);
     return RBFFD_OK;
 }
 
@@ -1431,7 +1593,7 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
             if (!P->gexec || P->g_dt != dt || P->g_steps != chunk || P->g_shape.lanes != sh.lanes ||
                 P->g_shape.block != sh.block || P->g_shape.tile != sh.tile || P->g_shape.tma != sh.tma ||
                 P->g_shape.sched != sh.sched || P->g_shape.pf != sh.pf || P->g_shape.plain != sh.plain ||
-                P->g_shape.pipe != sh.pipe) {
+                P->g_shape.pipe != sh.pipe || P->g_shape.db != sh.db) {
                 if (P->gexec) {
                     cudaGraphExecDestroy(P->gexec);
                     P->gexec = nullptr;

@@ -401,6 +401,100 @@ def test_register_pipelined_tile_heat(heat, dtype, ntr):
         assert np.array_equal(piped, O.rk4_heat(heat["st"], None, heat["W"][O.LSFC], u0, dt, steps))
 
 
+@pytest.mark.parametrize("dtype,ntr", [(R.F64, 1), (R.F64, 2), (R.F64, 4), (R.F64, 16), (R.F32, 1), (R.F32, 8),
+                                       (R.F32, 16)])
+def test_double_buffered_tile_heat(heat, dtype, ntr):
+    """The persistent tiled kernel that copies the next tile's halo in while
+    it computes the current one (RBFFD_TILE_DOUBLE_BUFFER): the same bits as
+    the plain tiled kernel for every node width it serves; FP64 equals the
+    oracle bit for bit; it combines with no other tiled-shape flag."""
+    rng = np.random.default_rng(60 + ntr)
+    u0 = heat["u0"] if ntr == 1 else heat["u0"][:, None] * (1.0 + 0.1 * rng.random((1, ntr)))
+    steps, dt = 30, 1e-6
+
+    def run(db, rows=128):
+        pde = R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=dtype, ntracers=ntr)
+        pde.setTiledShape(rows, 1, double_buffer=db)
+        assert pde.getTileFlags() == (R.TimeDependentPDE.TILE_DOUBLE_BUFFER if db else 0)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, dt, steps, graph=True)
+        out = pde.getLocalSolution()
+        pde.close()
+        return out
+
+    db = run(True)
+    assert np.array_equal(db, run(False))
+    assert np.array_equal(run(True, 64), db)
+    if dtype == R.F64:
+        assert np.array_equal(db, O.rk4_heat(heat["st"], None, heat["W"][O.LSFC], u0, dt, steps))
+    pde = R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=dtype, ntracers=ntr)
+    with pytest.raises(R.RbffdError):
+        pde.setTiledShape(128, 1, pipeline=True, double_buffer=True)
+    with pytest.raises(R.RbffdError):
+        pde.setTiledShape(128, 2, double_buffer=True)
+    pde.close()
+
+
+@pytest.mark.parametrize("dtype,ntr", [(R.F64, 16), (R.F32, 32)])
+def test_double_buffered_tile_walks_several_tiles_per_block(ctx, dtype, ntr):
+    """A grid of 40962 nodes in 64-row tiles with 16 (FP64) / 32 (FP32) values
+    per node has more tiles than the persistent grid has blocks, so each block
+    walks several tiles through both halo buffers: the same bits as the plain
+    tiled kernel and the register-pipelined one, with and without a graph."""
+    N, n = 40962, 50
+    xyz = R.fibonacci_nodes(N, 2)
+    st = R.knn_stencils(xyz, n)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(R.LSFC, grid, 2)
+    der.setEpsilon(0.25 / np.sqrt(4 * np.pi / N))
+    der.setPolynomialDegree(3)
+    der.computeAllWeightsForAllStencils()
+    rng = np.random.default_rng(9)
+    u0 = R.exact_sph_heat(xyz, 12, rng.standard_normal(169), 0.0)[:, None] * (1.0 + 0.1 * rng.random((1, ntr)))
+    steps, dt = 12, 1e-7
+
+    def run(graph, **flags):
+        pde = R.HeatSphere(grid, der, 1.0, dtype=dtype, ntracers=ntr)
+        pde.setTiledShape(64, 1, **flags)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, dt, steps, graph=graph)
+        out = pde.getLocalSolution()
+        pde.close()
+        return out
+
+    db = run(True, double_buffer=True)
+    assert np.isfinite(db).all()
+    assert np.array_equal(db, run(True))
+    assert np.array_equal(db, run(True, pipeline=True))
+    assert np.array_equal(db, run(False, double_buffer=True))
+    grid.close()
+
+
+def test_double_buffered_tile_fused_advection(bell):
+    """16-tracer FP32 advection on its fused operator: the double-buffered
+    persistent kernel gives the plain tiled kernel's bits; a three-operator
+    PDE refuses it."""
+    T = 16
+    rng = np.random.default_rng(18)
+    cen = rng.normal(size=(T, 3))
+    cen /= np.linalg.norm(cen, axis=1)[:, None]
+    u0 = np.exp(-8.0 * ((bell["xyz"][:, None, :] - cen[None, :, :]) ** 2).sum(2))
+    outs = []
+    for db in (True, False):
+        pde = R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=R.F32, ntracers=T)
+        pde.setFusedOperator(True)
+        pde.setTiledShape(128, 1, double_buffer=db)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, bell["p"]["dt"], 10, graph=True)
+        outs.append(pde.getLocalSolution())
+        pde.close()
+    assert np.array_equal(outs[0], outs[1])
+    p3 = R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=R.F32, ntracers=T)
+    with pytest.raises(R.RbffdError):
+        p3.setTiledShape(128, 1, double_buffer=True)
+    p3.close()
+
+
 def test_register_pipelined_tile_fused_advection_with_schedule(bell):
     """16-tracer FP32 advection on its fused operator, rows in the slot
     schedule: the pipelined kernel gives the plain scheduled kernel's bits; a
