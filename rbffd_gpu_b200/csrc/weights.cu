@@ -248,13 +248,13 @@ __device__ double hv_p_k(double eps2r2, int dim, int k)
     return pm1;
 }
 
-// RHS entry for node j (rbffd.cpp:375-503); diff = x0 - xj.
-__device__ double rhs_rbf(unsigned bit, const double* x0, const double* xj, double eps, double eps2, int dim, int hv_k,
-                          double lam_i, double th_i, double lam_j, double th_j)
+// RHS entry for node j (rbffd.cpp:375-503); dx, dy, dz = x0 - xj, r2 its
+// squared length and phi = g_eval(eps2, r2) (one evaluation shared by the
+// operators of a node); eps_2k = pow(eps, 2 hv_k) (per stencil).
+__device__ double rhs_rbf(unsigned bit, const double* x0, const double* xj, double eps2, int dim, int hv_k,
+                          double eps_2k, double lam_i, double th_i, double lam_j, double th_j, double dx, double dy,
+                          double dz, double r2, double phi)
 {
-    double dx = x0[0] - xj[0], dy = x0[1] - xj[1], dz = x0[2] - xj[2];
-    double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-    double phi = g_eval(eps2, r2);
     double rdr = -2. * eps2 * phi;  // rderiv_over_r
     switch (bit) {
     case RBFFD_X: return -2. * (dx * eps2) * phi;
@@ -285,7 +285,7 @@ __device__ double rhs_rbf(unsigned bit, const double* x0, const double* xj, doub
         int ax = bit == RBFFD_XSFC ? 0 : (bit == RBFFD_YSFC ? 1 : 2);
         return (x0[ax] * xTx - xj[ax]) * rdr;
     }
-    case RBFFD_HV: return pow(eps, 2 * hv_k) * hv_p_k(eps2 * r2, dim, hv_k) * phi;
+    case RBFFD_HV: return eps_2k * hv_p_k(eps2 * r2, dim, hv_k) * phi;
     default: return 0.;  // ALT_*: rbffd.cpp:490-494
     }
 }
@@ -311,6 +311,85 @@ __device__ void team_pivot_column0(const Team& T, const double* a, int m, int ld
     if (T.lane() == 0) {
         cand_v[T.warp()] = bv;
         cand_r[T.warp()] = br;
+    }
+}
+
+// Rows i = i0, i0 + stride, ... (< m) of a warp updated at step k against
+// the pivot row's columns k+1 .. ld-1, held in registers as NCH 32-column
+// chunks (column k+1+lane+32c in pr[c]; the last chunk may be partial):
+// a_ij <- fma(-l_i, u_kj, a_ij) with l_i from mult(i) and the row's storage
+// from row(i).  Two rows per pass, their loads issued before either row's
+// stores.  Lane 0, whose first column is k+1, tracks the first maximum
+// |a_i,k+1| over the rows in order (the next step's pivot candidates).
+template <int NCH, typename RowF, typename MulF>
+__device__ __forceinline__ void warp_rows_update(int k, int ld, int m, int i0, int stride, int lane, const double* pr,
+                                                 RowF row, MulF mult, double& nbv, int& nbr)
+{
+    const int j0 = k + 1 + lane;
+    bool in[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) in[c] = c < NCH - 1 || j0 + 32 * c < ld;
+    for (int i = i0; i < m; i += 2 * stride) {
+        const int i2 = i + stride;
+        const bool two = i2 < m;
+        double* a1 = row(i) + j0;
+        double* a2 = two ? row(i2) + j0 : a1;
+        const double l1 = mult(i);
+        const double l2 = two ? mult(i2) : 0.0;
+        double x1[NCH], x2[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            x1[c] = in[c] ? a1[32 * c] : 0.0;
+            x2[c] = in[c] && two ? a2[32 * c] : 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            x1[c] = __fma_rn(-l1, pr[c], x1[c]);
+            x2[c] = __fma_rn(-l2, pr[c], x2[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            if (in[c]) a1[32 * c] = x1[c];
+            if (in[c] && two) a2[32 * c] = x2[c];
+        }
+        if (lane == 0) {
+            const double v1 = fabs(x1[0]);
+            if (v1 > nbv) { nbv = v1; nbr = i; }
+            if (two) {
+                const double v2 = fabs(x2[0]);
+                if (v2 > nbv) { nbv = v2; nbr = i2; }
+            }
+        }
+    }
+}
+
+// The pivot row's columns k+1 .. ld-1 (NCH chunks) into registers, then the
+// warp's rows; NCH = number of 32-column chunks from column k+1 (at most
+// ELIM_CHUNKS).
+template <int NCH, typename RowF, typename MulF>
+__device__ __forceinline__ void warp_step(int k, int ld, int m, int i0, int stride, int lane, const double* prow,
+                                          RowF row, MulF mult, double& nbv, int& nbr)
+{
+    double pr[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        const int j = k + 1 + lane + 32 * c;
+        pr[c] = j < ld ? prow[j] : 0.0;
+    }
+    warp_rows_update<NCH>(k, ld, m, i0, stride, lane, pr, row, mult, nbv, nbr);
+}
+
+template <typename RowF, typename MulF>
+__device__ __forceinline__ void warp_step_any(int k, int ld, int m, int i0, int stride, int lane, const double* prow,
+                                              RowF row, MulF mult, double& nbv, int& nbr)
+{
+    switch ((ld - k - 1 + 31) >> 5) {  // columns k+1 .. ld-1 (at least one: K >= 1)
+    case 1: warp_step<1>(k, ld, m, i0, stride, lane, prow, row, mult, nbv, nbr); break;
+    case 2: warp_step<2>(k, ld, m, i0, stride, lane, prow, row, mult, nbv, nbr); break;
+    case 3: warp_step<3>(k, ld, m, i0, stride, lane, prow, row, mult, nbv, nbr); break;
+    case 4: warp_step<4>(k, ld, m, i0, stride, lane, prow, row, mult, nbv, nbr); break;
+    case 5: warp_step<5>(k, ld, m, i0, stride, lane, prow, row, mult, nbv, nbr); break;
+    default: warp_step<ELIM_CHUNKS>(k, ld, m, i0, stride, lane, prow, row, mult, nbv, nbr); break;
     }
 }
 
@@ -344,34 +423,12 @@ __device__ int team_eliminate(const Team& T, double* a, int m, int K, int lda, d
         // column k (where LAPACK keeps L; nothing reads it afterwards)
         for (int i = k + 1 + T.tid; i < m; i += T.size) a[i * lda + k] = a[i * lda + k] / piv;
         T.sync();
-        // rows split across warps, columns across lanes (column k+1+lane+32c);
-        // each lane keeps its columns of the pivot row in registers for the
-        // step; lane 0's first column is k+1, where it tracks the next pivot
-        double pr[ELIM_CHUNKS];
-#pragma unroll
-        for (int c = 0; c < ELIM_CHUNKS; c++) {
-            const int j = k + 1 + lane + 32 * c;
-            pr[c] = j < ld ? a[k * lda + j] : 0.0;
-        }
+        // rows split across warps, columns across lanes
         double nbv = -1.0;
         int nbr = INT_MAX;
-#pragma unroll 2
-        for (int i = k + 1 + w; i < m; i += nw) {
-            const double l = a[i * lda + k];
-            double* ai = a + (size_t)i * lda;
-#pragma unroll
-            for (int c = 0; c < ELIM_CHUNKS; c++) {
-                const int j = k + 1 + lane + 32 * c;
-                if (j < ld) {
-                    const double v = __fma_rn(-l, pr[c], ai[j]);
-                    ai[j] = v;
-                    if (c == 0 && lane == 0) {
-                        const double av = fabs(v);
-                        if (av > nbv) { nbv = av; nbr = i; }
-                    }
-                }
-            }
-        }
+        warp_step_any(
+            k, ld, m, k + 1 + w, nw, lane, a + (size_t)k * lda, [&](int i) { return a + (size_t)i * lda; },
+            [&](int i) { return a[(size_t)i * lda + k]; }, nbv, nbr);
         if (lane == 0) {
             cand_v[w] = nbv;
             cand_r[w] = nbr;
@@ -379,6 +436,68 @@ __device__ int team_eliminate(const Team& T, double* a, int m, int K, int lda, d
         T.sync();
     }
     return 0;
+}
+
+// The row-map elimination's update of a warp's rows at step k (NCH chunks
+// of the pivot row from column k+1): the rows k+1+w, k+1+w+nw, ... in
+// batches of 32, lane t finding the physical row of the batch's row t and
+// dividing for its multiplier (the divisions side by side), then the rows
+// two at a time with their row and multiplier broadcast, both rows' loads
+// issued before their stores.  Lane 0 tracks the first maximum of column k+1.
+template <int NCH>
+__device__ __forceinline__ void perm_rows_update(double* a, int lda, int k, int ld, int m, int w, int nw, int lane,
+                                                 int p, const int* P, const double* prow, double piv, double& nbv,
+                                                 int& nbr)
+{
+    const int j0 = k + 1 + lane;
+    double pr[NCH];
+    bool in[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        in[c] = c < NCH - 1 || j0 + 32 * c < ld;
+        pr[c] = in[c] ? prow[j0 + 32 * c] : 0.0;
+    }
+    for (int i0 = k + 1 + w; i0 < m; i0 += 32 * nw) {
+        const int it = i0 + lane * nw;
+        int phys = 0;
+        double lt = 0.0;
+        if (it < m) {
+            phys = it == p ? P[k] : P[it];
+            lt = a[(size_t)phys * lda + k] / piv;
+        }
+        const int cnt = min(32, (m - i0 + nw - 1) / nw);
+        for (int t = 0; t < cnt; t += 2) {
+            const bool two = t + 1 < cnt;
+            const int r1 = __shfl_sync(0xffffffffu, phys, t), r2 = __shfl_sync(0xffffffffu, phys, t + 1);
+            const double l1 = __shfl_sync(0xffffffffu, lt, t), l2 = __shfl_sync(0xffffffffu, lt, t + 1);
+            double* a1 = a + (size_t)r1 * lda + j0;
+            double* a2 = two ? a + (size_t)r2 * lda + j0 : a1;
+            double x1[NCH], x2[NCH];
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                x1[c] = in[c] ? a1[32 * c] : 0.0;
+                x2[c] = in[c] && two ? a2[32 * c] : 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                x1[c] = __fma_rn(-l1, pr[c], x1[c]);
+                x2[c] = __fma_rn(-l2, pr[c], x2[c]);
+            }
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                if (in[c]) a1[32 * c] = x1[c];
+                if (in[c] && two) a2[32 * c] = x2[c];
+            }
+            if (lane == 0) {
+                const double v1 = fabs(x1[0]);
+                if (v1 > nbv) { nbv = v1; nbr = i0 + t * nw; }
+                if (two) {
+                    const double v2 = fabs(x2[0]);
+                    if (v2 > nbv) { nbv = v2; nbr = i0 + (t + 1) * nw; }
+                }
+            }
+        }
+    }
 }
 
 // Unblocked elimination with one team barrier per step.  Rows are not
@@ -415,30 +534,17 @@ __device__ int team_eliminate_perm(const Team& T, double* a, int m, int K, int l
         for (int i = T.tid; i < m; i += T.size) Q[i] = i == k ? P[p] : (i == p ? P[k] : P[i]);
         const int prow = P[p];  // the pivot's physical row
         const double piv = a[prow * lda + k];
-        double pr[ELIM_CHUNKS];
-#pragma unroll
-        for (int c = 0; c < ELIM_CHUNKS; c++) {
-            const int j = k + 1 + lane + 32 * c;
-            pr[c] = j < ld ? a[prow * lda + j] : 0.0;
-        }
         double nbv = -1.0;
         int nbr = INT_MAX;
-#pragma unroll 2
-        for (int i = k + 1 + w; i < m; i += nw) {
-            double* ai = a + (size_t)(i == p ? P[k] : P[i]) * lda;
-            const double l = ai[k] / piv;
-#pragma unroll
-            for (int c = 0; c < ELIM_CHUNKS; c++) {
-                const int j = k + 1 + lane + 32 * c;
-                if (j < ld) {
-                    const double v = __fma_rn(-l, pr[c], ai[j]);
-                    ai[j] = v;
-                    if (c == 0 && lane == 0) {
-                        const double av = fabs(v);
-                        if (av > nbv) { nbv = av; nbr = i; }
-                    }
-                }
-            }
+        switch ((ld - k - 1 + 31) >> 5) {
+        case 1: perm_rows_update<1>(a, lda, k, ld, m, w, nw, lane, p, P, a + (size_t)prow * lda, piv, nbv, nbr); break;
+        case 2: perm_rows_update<2>(a, lda, k, ld, m, w, nw, lane, p, P, a + (size_t)prow * lda, piv, nbv, nbr); break;
+        case 3: perm_rows_update<3>(a, lda, k, ld, m, w, nw, lane, p, P, a + (size_t)prow * lda, piv, nbv, nbr); break;
+        case 4: perm_rows_update<4>(a, lda, k, ld, m, w, nw, lane, p, P, a + (size_t)prow * lda, piv, nbv, nbr); break;
+        case 5: perm_rows_update<5>(a, lda, k, ld, m, w, nw, lane, p, P, a + (size_t)prow * lda, piv, nbv, nbr); break;
+        default:
+            perm_rows_update<ELIM_CHUNKS>(a, lda, k, ld, m, w, nw, lane, p, P, a + (size_t)prow * lda, piv, nbv, nbr);
+            break;
         }
         if (lane == 0) {
             cand_v[(par ^ 1) * MAX_WARPS + w] = nbv;
@@ -447,29 +553,6 @@ __device__ int team_eliminate_perm(const Team& T, double* a, int m, int K, int l
         T.sync();
     }
     return 0;
-}
-
-// Back substitution of team_back_substitute for rows placed by the map F.
-__device__ void team_back_substitute_perm(const Team& T, double* a, int m, int K, int lda, const int* F)
-{
-    for (int c = T.warp(); c < K; c += T.nwarps()) {
-        const int col = m + c;
-        for (int k = m - 1; k >= 0; k--) {
-            const int rk = F[k];
-            double xk = 0.0;
-            if (T.lane() == 0) {
-                xk = a[rk * lda + col] / a[rk * lda + k];
-                a[rk * lda + col] = xk;
-            }
-            xk = __shfl_sync(0xffffffffu, xk, 0);
-            for (int i = T.lane(); i < k; i += 32) {
-                const int ri = F[i];
-                a[ri * lda + col] = __fma_rn(-xk, a[ri * lda + k], a[ri * lda + col]);
-            }
-            __syncwarp();
-        }
-    }
-    T.sync();
 }
 
 // Pivot candidates of column k over rows [k, m): one per warp, first maximum.
@@ -611,21 +694,57 @@ __device__ int team_eliminate_blocked(const Team& T, double* a, int m, int K, in
     return 0;
 }
 
-// Column-oriented back substitution (dtrsm upper, non-unit), one warp per RHS column.
-__device__ void team_back_substitute(const Team& T, double* a, int m, int K, int lda)
+// Column-oriented back substitution (dtrsm upper, non-unit), one warp per
+// right-hand side: x_k = b_k / u_kk for k = m-1 .. 0, then b_i <- fma(-x_k,
+// u_ik, b_i) for i < k.  Lane l keeps b_i of rows i = l + 32 q in registers
+// (q < BS, m <= 32 BS); every lane divides row k's value by the diagonal and
+// lane k mod 32's quotient is broadcast, so a step's critical path is one
+// division, one shuffle and one fma.  Row storage from row(i) (the identity,
+// or the row map of the row-map elimination).  The solution replaces the
+// right-hand side.
+template <int BS, typename RowF>
+__device__ void back_substitute_bs(const Team& T, int m, int K, RowF row)
 {
+    const int lane = T.lane();
     for (int c = T.warp(); c < K; c += T.nwarps()) {
         const int col = m + c;
-        for (int k = m - 1; k >= 0; k--) {
-            double xk = 0.0;
-            if (T.lane() == 0) {
-                xk = a[k * lda + col] / a[k * lda + k];
-                a[k * lda + col] = xk;
-            }
-            xk = __shfl_sync(0xffffffffu, xk, 0);
-            for (int i = T.lane(); i < k; i += 32) a[i * lda + col] = __fma_rn(-xk, a[i * lda + k], a[i * lda + col]);
-            __syncwarp();
+        double b[BS];
+        double* ri[BS];
+#pragma unroll
+        for (int q = 0; q < BS; q++) {
+            const int i = lane + 32 * q;
+            ri[q] = row(i < m ? i : 0);
+            b[q] = i < m ? ri[q][col] : 0.0;
         }
+        for (int k = m - 1; k >= 0; k--) {
+            const int qk = k >> 5, lk = k & 31;
+            double bk = b[0];
+#pragma unroll
+            for (int q = 1; q < BS; q++)
+                if (q == qk) bk = b[q];
+            const double xk = __shfl_sync(0xffffffffu, bk / row(k)[k], lk);
+#pragma unroll
+            for (int q = 0; q < BS; q++) {
+                const int i = lane + 32 * q;
+                if (i < k) b[q] = __fma_rn(-xk, ri[q][k], b[q]);
+                if (i == k) b[q] = xk;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < BS; q++)
+            if (lane + 32 * q < m) ri[q][col] = b[q];
+    }
+}
+
+template <typename RowF>
+__device__ void team_back_substitute_rows(const Team& T, double* a, int m, int K, RowF row)
+{
+    switch ((m + 31) >> 5) {
+    case 1: back_substitute_bs<1>(T, m, K, row); break;
+    case 2: back_substitute_bs<2>(T, m, K, row); break;
+    case 3: back_substitute_bs<3>(T, m, K, row); break;
+    case 4: back_substitute_bs<4>(T, m, K, row); break;
+    default: back_substitute_bs<(MAX_M + 31) / 32>(T, m, K, row); break;
     }
     T.sync();
 }
@@ -650,25 +769,33 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
         xs[3 * q + 1] = v.y;
         xs[3 * q + 2] = v.z;
     }
+    if (T.tid == 0) fr[7] = 0.0;  // max_j |x_j - c|^2, gathered below
     T.sync();
     const double x0[3] = {xs[0], xs[1], xs[2]};
     const double lam_i = atan2(x0[1], x0[0]), th_i = atan2(x0[2], sqrt(x0[0] * x0[0] + x0[1] * x0[1]));
-    if (deg >= 2 && T.tid == 0) {
-        fr[0] = -sin(lam_i); fr[1] = cos(lam_i); fr[2] = 0.0;
-        fr[3] = -sin(th_i) * cos(lam_i); fr[4] = -sin(th_i) * sin(lam_i); fr[5] = cos(th_i);
+    if (deg >= 2) {
+        if (T.tid == 0) {
+            fr[0] = -sin(lam_i); fr[1] = cos(lam_i); fr[2] = 0.0;
+            fr[3] = -sin(th_i) * cos(lam_i); fr[4] = -sin(th_i) * sin(lam_i); fr[5] = cos(th_i);
+        }
+        // the largest squared distance from the centre: a maximum, so any
+        // order of the comparisons gives the same value; non-negative doubles
+        // order as their bit patterns, so the team combines with an integer max
         double s2 = 0.0;
-        for (int j = 0; j < n; j++) {
+        for (int j = T.tid; j < n; j += T.size) {
             double dx = xs[3 * j] - x0[0], dy = xs[3 * j + 1] - x0[1], dz = xs[3 * j + 2] - x0[2];
             double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
             s2 = fmax(s2, r2);
         }
-        fr[6] = s2 > 0.0 ? sqrt(s2) : 1.0;
+        for (int o = 16; o > 0; o >>= 1) s2 = fmax(s2, __shfl_xor_sync(0xffffffffu, s2, o));
+        if (T.lane() == 0)
+            atomicMax(reinterpret_cast<unsigned long long*>(fr + 7), (unsigned long long)__double_as_longlong(s2));
     }
     // Phi block: ar(j, i) = phi(x_i - x_j)   (rbffd.cpp:943-966).  Symmetric to
     // the last bit (x_j - x_i squares to the same r^2), so each pair j <= i is
     // evaluated once and written to both places: n(n+1)/2 exponentials.
     for (int e = T.tid; e < n * (n + 1) / 2; e += T.size) {
-        int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);  // e = i(i+1)/2 + j, 0 <= j <= i
+        int i = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);  // e = i(i+1)/2 + j, 0 <= j <= i (estimate, corrected below)
         while (i * (i + 1) / 2 > e) i--;
         while ((i + 1) * (i + 2) / 2 <= e) i++;
         const int j = e - i * (i + 1) / 2;
@@ -678,10 +805,10 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
         a[j * ld + i] = v;
         a[i * ld + j] = v;
     }
-    T.sync();  // frame visible
+    T.sync();  // frame and distance visible
     const double* e1 = fr;
     const double* e2 = fr + 3;
-    const double s = fr[6];
+    const double s = fr[7] > 0.0 ? sqrt(fr[7]) : 1.0;
     // polynomial border and zero block
     for (int e = T.tid; e < np * n; e += T.size) {
         int q = e / n, i = e - q * n;
@@ -702,13 +829,26 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
         a[i * ld + (n + q)] = v;
     }
     for (int e = T.tid; e < np * np; e += T.size) a[(n + e / np) * ld + n + e % np] = 0.0;
-    // right-hand sides, one column per operator in bit order (rbffd.cpp:106-125)
+    // right-hand sides, one column per operator in bit order (rbffd.cpp:106-125);
+    // a node's kernel value is evaluated once for all operators, its angles
+    // only when an operator needs them
+    bool angles = false;
+    for (int c = 0; c < K; c++) angles |= P.opbit[c] == RBFFD_LAMBDA || P.opbit[c] == RBFFD_THETA;
+    const double eps_2k = pow(eps, 2 * P.hv_k);
     for (int j = T.tid; j < m; j += T.size) {
         if (j < n) {
             const double* xj = xs + 3 * j;
-            double lam_j = atan2(xj[1], xj[0]), th_j = atan2(xj[2], sqrt(xj[0] * xj[0] + xj[1] * xj[1]));
+            double lam_j = 0.0, th_j = 0.0;
+            if (angles) {
+                lam_j = atan2(xj[1], xj[0]);
+                th_j = atan2(xj[2], sqrt(xj[0] * xj[0] + xj[1] * xj[1]));
+            }
+            const double dx = x0[0] - xj[0], dy = x0[1] - xj[1], dz = x0[2] - xj[2];
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            const double phi = g_eval(eps2, r2);
             for (int c = 0; c < K; c++)
-                a[j * ld + m + c] = rhs_rbf(P.opbit[c], x0, xj, eps, eps2, P.dim, P.hv_k, lam_i, th_i, lam_j, th_j);
+                a[j * ld + m + c] = rhs_rbf(P.opbit[c], x0, xj, eps2, P.dim, P.hv_k, eps_2k, lam_i, th_i, lam_j, th_j,
+                                            dx, dy, dz, r2, phi);
         } else {
             for (int c = 0; c < K; c++) {
                 double v = 0.0;
@@ -751,9 +891,9 @@ __device__ void team_solve(const Team& T, const WParams& P, int r, double* a, in
     const int* F = perm + (m & 1) * m;  // ELIM_PERM: where each logical row lives
     if (ok) {
         if (mode == ELIM_PERM)
-            team_back_substitute_perm(T, a, m, K, lda, F);
+            team_back_substitute_rows(T, a, m, K, [&](int i) { return a + (size_t)F[i] * lda; });
         else
-            team_back_substitute(T, a, m, K, lda);
+            team_back_substitute_rows(T, a, m, K, [&](int i) { return a + (size_t)i * lda; });
     }
     if (!ok && T.tid == 0) atomicMin(P.status, r + 1);
     // store: weights[type][r][j] = W(j, col) * scale (rbffd.cpp:300-306), row r of the sliced ELL
@@ -767,31 +907,33 @@ __device__ void team_solve(const Team& T, const WParams& P, int r, double* a, in
     T.sync();
 }
 
-// The whole batch in one persistent launch.  Work units are numbered class
-// by class (classes in decreasing system size, so the largest systems start
-// first); a unit is teams_per_cta systems of one class, one per team of the
-// CTA.  Each CTA takes the next unit from a global counter until none is
-// left, splits itself into that class's teams and solves.
-__global__ void __launch_bounds__(256) k_weights_all(WParams P)
+// One size class in one persistent launch (the classes of a call run as a
+// sequence of such launches, each with the shared memory and the resident
+// CTAs its own systems allow).  A work unit is teams_per_cta systems of the
+// class, one per team of the CTA; each CTA takes the next unit from the
+// class's counter until none is left, splits itself into the class's teams
+// and solves.  MODE is the class's elimination, so each variant is compiled
+// with only its own registers (the unblocked and row-map eliminations fit
+// four CTAs of 256 threads on an SM, the register-tiled blocked one two).
+template <int MODE>
+__global__ void __launch_bounds__(256, MODE == ELIM_BLOCKED ? 2 : 3) k_weights_class(WParams P)
 {
     extern __shared__ double smem[];
     __shared__ int s_unit;
+    const WClass C = P.cls[0];
+    Team T;
+    T.size = C.team;
+    T.id = threadIdx.x / C.team;
+    T.tid = threadIdx.x % C.team;
     for (;;) {
         if (threadIdx.x == 0) s_unit = atomicAdd(P.work, 1);
         __syncthreads();
         const int u = s_unit;
         __syncthreads();
         if (u >= P.nunits) break;
-        int c = 0;
-        while (c + 1 < P.nclasses && u >= P.cls[c + 1].unit0) c++;
-        const WClass C = P.cls[c];
-        Team T;
-        T.size = C.team;
-        T.id = threadIdx.x / C.team;
-        T.tid = threadIdx.x % C.team;
-        const int t = (u - C.unit0) * C.teams + T.id;
+        const int t = u * C.teams + T.id;
         if (T.id < C.teams && t < C.nrows)
-            team_solve(T, P, P.rows[C.rows_off + t], smem + (size_t)T.id * C.stride, C.m, C.lda, C.blocked);
+            team_solve(T, P, P.rows[C.rows_off + t], smem + (size_t)T.id * C.stride, C.m, C.lda, MODE);
         __syncthreads();  // every team done with the shared memory before the next unit
     }
 }
@@ -844,9 +986,9 @@ __global__ void __launch_bounds__(512) k_gesv(double* A, double* B, int* info, i
                                                : team_eliminate(T, a, m, K, ld, cand_v, cand_r);
         if (st == 0) {
             if (blocked == ELIM_PERM)
-                team_back_substitute_perm(T, a, m, K, ld, F);
+                team_back_substitute_rows(T, a, m, K, [&](int i) { return a + (size_t)F[i] * ld; });
             else
-                team_back_substitute(T, a, m, K, ld);
+                team_back_substitute_rows(T, a, m, K, [&](int i) { return a + (size_t)i * ld; });
         }
         if (T.tid == 0) info[b] = st;
         for (int e = T.tid; e < m * K; e += T.size) {
@@ -911,12 +1053,10 @@ struct WeightsWork {
     int* d_rows = nullptr;
     int* d_deg = nullptr;
     double* d_eps = nullptr;
-    int* d_status = nullptr;  // [0] status, [1] work counter
+    int* d_status = nullptr;  // [0] status, [1 + c] work counter of class c
     size_t bytes = 0;
     cudaGraphExec_t gexec = nullptr;
-    WParams gparams;  // the parameters the graph was captured with
-    size_t gsmem = 0;
-    int ggrid = 0;
+    WParams gparams;  // the parameters the graph was captured with (each class's launch follows from them)
 };
 
 void weights_work_free(rbffd_grid* g)
@@ -928,7 +1068,7 @@ void weights_work_free(rbffd_grid* g)
     dev_free(ctx, W->d_rows, (size_t)g->N * sizeof(int));
     dev_free(ctx, W->d_deg, (size_t)g->N * sizeof(int));
     dev_free(ctx, W->d_eps, (size_t)g->N * sizeof(double));
-    dev_free(ctx, W->d_status, 2 * sizeof(int));
+    dev_free(ctx, W->d_status, (1 + MAX_CLASSES) * sizeof(int));
     delete W;
     g->ww = nullptr;
 }
@@ -944,7 +1084,7 @@ static int weights_work(rbffd_grid* g, WeightsWork** out)
         if ((rc = dev_alloc(ctx, (void**)&W->d_rows, (size_t)g->N * sizeof(int))) ||
             (rc = dev_alloc(ctx, (void**)&W->d_deg, (size_t)g->N * sizeof(int))) ||
             (rc = dev_alloc(ctx, (void**)&W->d_eps, (size_t)g->N * sizeof(double))) ||
-            (rc = dev_alloc(ctx, (void**)&W->d_status, 2 * sizeof(int)))) {
+            (rc = dev_alloc(ctx, (void**)&W->d_status, (1 + MAX_CLASSES) * sizeof(int)))) {
             weights_work_free(g);
             return rc;
         }
@@ -953,39 +1093,71 @@ static int weights_work(rbffd_grid* g, WeightsWork** out)
     return RBFFD_OK;
 }
 
-// Shared memory, CTAs per SM and grid of a persistent launch over P's classes.
+// The kernel of an elimination mode.
+static void (*class_kernel(int mode))(WParams)
+{
+    return mode == ELIM_BLOCKED ? k_weights_class<ELIM_BLOCKED>
+           : mode == ELIM_PERM  ? k_weights_class<ELIM_PERM>
+                                : k_weights_class<ELIM_UNBLOCKED>;
+}
+
+// Shared memory and grid of the persistent launch of a one-class P (cls[0]):
+// as many CTAs as fit on the device at once, at most one per work unit.
 static int persistent_geometry(rbffd_ctx* ctx, const WParams& P, size_t* smem, int* grid)
 {
-    size_t sm = 0;
-    for (int c = 0; c < P.nclasses; c++)
-        sm = std::max(sm, (size_t)P.cls[c].teams * P.cls[c].stride * sizeof(double));
-    RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(k_weights_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const WClass& C = P.cls[0];
+    const size_t sm = (size_t)C.teams * C.stride * sizeof(double);
+    auto kern = class_kernel(C.blocked);
+    RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int per_sm = 0;
-    RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_weights_all, W_CTA, sm));
+    RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W_CTA, sm));
     if (per_sm < 1) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "weight kernel shape does not fit an SM");
     *smem = sm;
     *grid = std::max(1, std::min(P.nunits, per_sm * ctx->sm_count));
     return RBFFD_OK;
 }
 
-// Zero the counter and launch (what the graph holds).
+// Each mode's kernel allowed the largest dynamic shared memory of the classes
+// that use it (the attribute is per kernel, and a captured or replayed launch
+// needs it to cover its own size).
+static int class_smem_attributes(rbffd_ctx* ctx, const WParams* Q, const size_t* smem, int n)
+{
+    for (int mode : {ELIM_UNBLOCKED, ELIM_BLOCKED, ELIM_PERM}) {
+        size_t mx = 0;
+        for (int c = 0; c < n; c++)
+            if (Q[c].cls[0].blocked == mode) mx = std::max(mx, smem[c]);
+        if (mx)
+            RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(class_kernel(mode), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)mx));
+    }
+    return RBFFD_OK;
+}
+
+// Zero the class's counter and launch (what the graph holds, class by class).
 static void enqueue_persistent(const WParams& P, size_t smem, int grid, cudaStream_t s)
 {
     cudaMemsetAsync(P.work, 0, sizeof(int), s);
-    k_weights_all<<<grid, W_CTA, smem, s>>>(P);
+    class_kernel(P.cls[0].blocked)<<<grid, W_CTA, smem, s>>>(P);
 }
 
-// Fill in the classes' shapes and unit numbering (cls[].team/blocked set).
+// Shape a one-class P: its teams per CTA and work units (cls[0].team/blocked set).
 static void number_units(WParams& P)
 {
-    int u = 0;
-    for (int c = 0; c < P.nclasses; c++) {
-        WClass& C = P.cls[c];
-        C.teams = W_CTA / C.team;
-        C.unit0 = u;
-        u += (C.nrows + C.teams - 1) / C.teams;
-    }
-    P.nunits = u;
+    WClass& C = P.cls[0];
+    C.teams = W_CTA / C.team;
+    C.unit0 = 0;
+    P.nunits = (C.nrows + C.teams - 1) / C.teams;
+}
+
+// The one-class parameters of class c of P, counting on counter c.
+static WParams class_params(const WParams& P, int c, int* counters)
+{
+    WParams Q = P;
+    Q.nclasses = 1;
+    Q.cls[0] = P.cls[c];
+    Q.work = counters + c;
+    number_units(Q);
+    return Q;
 }
 
 constexpr unsigned ALT_BITS = RBFFD_ALT_XSFC | RBFFD_ALT_YSFC | RBFFD_ALT_ZSFC;
@@ -1141,6 +1313,7 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
                     Q.cls[0].team = cs.team;
                     Q.cls[0].blocked = cs.blocked;
                     Q.cls[0].nrows = std::min(C.nrows, 16 * ctx->sm_count * (W_CTA / cs.team));
+                    Q.work = W->d_status + 1;
                     number_units(Q);
                     size_t smem;
                     int grid;
@@ -1172,20 +1345,24 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
         C.team = best.team;
         C.blocked = best.blocked;
     }
-    number_units(P);
-    // the whole batch: one persistent launch, captured in a CUDA graph and
-    // replayed while the parameters stay the same
-    size_t smem;
-    int grid;
-    if ((rc = persistent_geometry(ctx, P, &smem, &grid))) return rc;
-    if (!W->gexec || memcmp(&W->gparams, &P, sizeof P) != 0 || W->gsmem != smem || W->ggrid != grid) {
+    // the whole batch: one persistent launch per class, largest systems first,
+    // captured in a CUDA graph and replayed while the parameters stay the same
+    WParams Qc[MAX_CLASSES];
+    size_t smem_c[MAX_CLASSES];
+    int grid_c[MAX_CLASSES];
+    for (int c = 0; c < P.nclasses; c++) {
+        Qc[c] = class_params(P, c, W->d_status + 1);
+        if ((rc = persistent_geometry(ctx, Qc[c], &smem_c[c], &grid_c[c]))) return rc;
+    }
+    if ((rc = class_smem_attributes(ctx, Qc, smem_c, P.nclasses))) return rc;
+    if (!W->gexec || memcmp(&W->gparams, &P, sizeof P) != 0) {
         if (W->gexec) {
             cudaGraphExecDestroy(W->gexec);
             W->gexec = nullptr;
         }
         cudaGraph_t graph;
         RBFFD_CUDA_TRY(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        enqueue_persistent(P, smem, grid, s);
+        for (int c = 0; c < P.nclasses; c++) enqueue_persistent(Qc[c], smem_c[c], grid_c[c], s);
         e = cudaStreamEndCapture(s, &graph);
         if (e != cudaSuccess) return cuda_error(ctx, e, "weights graph capture");
         e = cudaGraphInstantiate(&W->gexec, graph, 0);
@@ -1195,8 +1372,6 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
             return cuda_error(ctx, e, "weights graph instantiate");
         }
         W->gparams = P;
-        W->gsmem = smem;
-        W->ggrid = grid;
     }
     e = cudaMemcpyAsync(W->d_status, status0, 2 * sizeof(int), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaGraphLaunch(W->gexec, s);
