@@ -67,8 +67,9 @@ def parse():
     ap.add_argument("--profile-heat-hbm", action="store_true",
                     help="the heat stage where it is HBM-bound: N=655362, FP32 n=50 then FP64 n=101, halo tiles of "
                          "128 rows, 3 un-graphed RK4 steps each (12 launches each), for ncu")
-    ap.add_argument("--profile-weights", type=int, default=0, metavar="N",
-                    help="batched weights (the 1e6-stencil mix at N stencils): a tuned call, then one more, for ncu")
+    ap.add_argument("--profile-weights", default=None, metavar="N[,METHOD]",
+                    help="batched weights (the 1e6-stencil mix at N stencils): a tuned call, then one more, for ncu; "
+                         "METHOD: auto (default), unblocked, blocked, row_map, registers")
     return ap.parse_args()
 
 
@@ -1313,13 +1314,19 @@ def run_profile_heat_hbm():
     print("profile run done")
 
 
-def run_profile_weights(N):
+def run_profile_weights(spec):
     """The batched-weights mix (n over {17, 31, 50, 101} with degrees 1-4,
     eps ~ U[2, 8], XSFC/YSFC/ZSFC) on N stencils: the tuned call, then one
-    more (the launches to capture)."""
+    more (the launches to capture).  spec: "N" or "N,method" with method one
+    of auto, unblocked, blocked, row_map, registers (the elimination)."""
     import rbffd_gpu_b200 as R
     C = WEIGHTS
+    fields = str(spec).split(",")
+    N = int(fields[0])
+    method = {"auto": R.ELIM_AUTO, "unblocked": R.ELIM_UNBLOCKED, "blocked": R.ELIM_BLOCKED,
+              "row_map": R.ELIM_ROW_MAP, "registers": R.ELIM_REGISTERS}[fields[1] if len(fields) > 1 else "auto"]
     ctx = R.Context(0)
+    ctx.setWeightsElimination(method)
     xyz = R.fibonacci_nodes(N, C["seed"])
     full = R.knn_stencils(xyz, max(C["sizes"]))
     rng = np.random.default_rng(C["seed"])

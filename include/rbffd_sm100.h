@@ -227,6 +227,22 @@ typedef struct rbffd_weight_params {
  * zero pivot (first failing row in last_error). */
 int rbffd_weights_compute(rbffd_grid* grid, const rbffd_weight_params* params, const double* eps, double eps_uniform,
                           const int* deg_per_row);
+/* Elimination used by rbffd_weights_compute on this context (no reference
+ * counterpart: the reference calls LAPACK through arma::solve).  Every
+ * method performs dgetf2's arithmetic (first-maximum partial pivoting,
+ * multipliers by division, fused updates in step order) and gives the same
+ * weights bit for bit; they differ in where the system lives:
+ *   RBFFD_ELIM_AUTO       the autotuner picks per system size (default);
+ *   RBFFD_ELIM_UNBLOCKED  shared memory, one pass over the trailing rows per step;
+ *   RBFFD_ELIM_BLOCKED    shared memory, panels of 8 steps with register-tiled updates;
+ *   RBFFD_ELIM_ROW_MAP    shared memory, rows never swapped (a row map), one barrier per step;
+ *   RBFFD_ELIM_REGISTERS  the rows in registers of one CTA (m <= 128 and m + K <= 128).
+ * A method that does not apply to a system size leaves that size to the
+ * autotuner. */
+enum { RBFFD_ELIM_AUTO = 0, RBFFD_ELIM_UNBLOCKED = 1, RBFFD_ELIM_BLOCKED = 2, RBFFD_ELIM_ROW_MAP = 3,
+       RBFFD_ELIM_REGISTERS = 4 };
+int rbffd_weights_set_elimination(rbffd_ctx* ctx, int method);
+int rbffd_weights_get_elimination(rbffd_ctx* ctx, int* method);
 /* The assembled augmented systems [A | B] (m x (m+K), row-major, K = number
  * of selected operators) of the listed stencils, as the weight solver builds
  * them before elimination: RBFFD::getStencilLHS + getStencilMultiRHS

@@ -8,7 +8,7 @@ by the tests and the benchmark.  The C++ view for drop-in use is in
 rbffd_gpu_b200/cpp/.
 """
 from .api import (  # noqa: F401
-    F32, F64, ARITH_FUSED, ARITH_UNFUSED, X, Y, Z, LAPL, R, HV, LAMBDA, THETA, LSFC, XSFC, YSFC, ZSFC, INTERP, ALT_XSFC, ALT_YSFC, ALT_ZSFC, RK4,
+    F32, F64, ARITH_FUSED, ARITH_UNFUSED, ELIM_AUTO, ELIM_UNBLOCKED, ELIM_BLOCKED, ELIM_ROW_MAP, ELIM_REGISTERS, X, Y, Z, LAPL, R, HV, LAMBDA, THETA, LSFC, XSFC, YSFC, ZSFC, INTERP, ALT_XSFC, ALT_YSFC, ALT_ZSFC, RK4,
     RbffdError, Context, Grid, RBFFD, TimeDependentPDE, CosineBell, HeatSphere, Advection, VortexRollup,
     vortex_rollup_coefficients, exact_vortex_rollup, sol_norms,
     fibonacci_nodes, knn_stencils, knn_stencils_gpu, generate_stencils, generate_stencils_gpu, variable_epsilon, ST_BRUTE_FORCE, ST_KDTREE, ST_HASH,

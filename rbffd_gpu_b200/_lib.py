@@ -76,6 +76,8 @@ PROTOTYPES = {
     "rbffd_grid_nbytes": (c_int, [c_void_p, P(c_size_t)]),
     "rbffd_weights_compute": (c_int, [c_void_p, P(WeightParams), dp, c_double, ip]),
     "rbffd_weights_assemble": (c_int, [c_void_p, P(WeightParams), dp, c_double, ip, ip, c_int, dp]),
+    "rbffd_weights_set_elimination": (c_int, [c_void_p, c_int]),
+    "rbffd_weights_get_elimination": (c_int, [c_void_p, ip]),
     "rbffd_weights_set": (c_int, [c_void_p, c_uint, dp]),
     "rbffd_weights_get": (c_int, [c_void_p, c_uint, dp]),
     "rbffd_weights_file_write": (c_int, [c_char_p, c_int, c_int, c_int, ip, ip, dp]),

@@ -17,6 +17,7 @@ F32, F64 = 0, 1
 # FP64 arithmetic of the apply and time-stepping kernels (rbffd_ctx_set_arithmetic):
 # fused multiply-adds (default), or rounded products then sums, the reference build's arithmetic
 ARITH_FUSED, ARITH_UNFUSED = 0, 1
+ELIM_AUTO, ELIM_UNBLOCKED, ELIM_BLOCKED, ELIM_ROW_MAP, ELIM_REGISTERS = 0, 1, 2, 3, 4
 X, Y, Z, LAPL, R, HV, LAMBDA, THETA = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20, 0x40, 0x80
 LSFC, XSFC, YSFC, ZSFC, INTERP = 0x100, 0x200, 0x400, 0x800, 0x8000
 ALT_XSFC, ALT_YSFC, ALT_ZSFC = 0x1000, 0x2000, 0x4000
@@ -314,6 +315,17 @@ class Context:
     def getArithmetic(self):
         a = ctypes.c_int()
         self.check(self.L.rbffd_ctx_get_arithmetic(self.h, ctypes.byref(a)))
+        return a.value
+
+    def setWeightsElimination(self, method):
+        """Elimination of the batched weight solves on this context: ELIM_AUTO
+        (autotuned per system size), ELIM_UNBLOCKED, ELIM_BLOCKED, ELIM_ROW_MAP
+        or ELIM_REGISTERS; every method gives the same weights bit for bit."""
+        self.check(self.L.rbffd_weights_set_elimination(self.h, method), "set_elimination")
+
+    def getWeightsElimination(self):
+        a = ctypes.c_int()
+        self.check(self.L.rbffd_weights_get_elimination(self.h, ctypes.byref(a)))
         return a.value
 
     def stream(self):

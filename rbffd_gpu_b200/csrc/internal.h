@@ -59,6 +59,7 @@ struct rbffd_ctx {
     std::map<TuneKey, Shape> tuned;  // autotuner results per problem shape
     int* d_status = nullptr;         // DEV_STATUS_* written by kernels with bounded waits
     int arith = 0;                   // RBFFD_ARITH_*: FP64 arithmetic of rbffd_apply* and of new FP64 PDEs
+    int weights_elim = 0;            // RBFFD_ELIM_*: elimination of the weight solves (0: autotuned)
 };
 
 // Read and clear the context's device status; RBFFD_ERR_TIMEOUT if a kernel gave up waiting.

@@ -555,24 +555,112 @@ __device__ int team_eliminate_perm(const Team& T, double* a, int m, int K, int l
     return 0;
 }
 
-// Pivot candidates of column k over rows [k, m): one per warp, first maximum.
-__device__ void team_column_candidates(const Team& T, const double* a, int lda, int k, int m, double* cand_v,
-                                       int* cand_r)
+// Warp-wide first maximum: the largest v, ties to the smaller index i.
+__device__ __forceinline__ void warp_argmax_index(double& v, int& i)
 {
-    double bv = -1.0;
-    int br = INT_MAX;
-    for (int i = k + T.tid; i < m; i += T.size) {
-        const double v = fabs(a[i * lda + k]);
-        if (v > bv) { bv = v; br = i; }
-    }
     for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-        const int orr = __shfl_xor_sync(0xffffffffu, br, o);
-        if (ov > bv || (ov == bv && orr < br)) { bv = ov; br = orr; }
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+        if (ov > v || (ov == v && oi < i)) {
+            v = ov;
+            i = oi;
+        }
     }
-    if (T.lane() == 0) {
-        cand_v[T.warp()] = bv;
-        cand_r[T.warp()] = br;
+}
+
+// The panel of columns k0 .. k0+pw-1 (pw <= 8) over rows k0 .. m-1, factored
+// by one warp in registers with dgetf2's steps: lane l holds rows
+// k0 + l + 32 t (t < TS), the panel's 8 columns each.  Step k = k0 + s:
+// first maximum |a_ik| over rows i >= k (smaller row on ties), the rows k and
+// p exchanged across the panel's columns (the multipliers of earlier steps
+// included, as dgetf2 swaps whole rows), multipliers a_ik / a_kk, then
+// a_ij <- fma(-l_i, u_kj, a_ij) on the panel's later columns.  Pivot rows
+// go to piv_rows[s].  Returns 0, or k + 1 at an exactly zero pivot column.
+template <int TS>
+__device__ int warp_panel(double* a, int lda, int m, int k0, int pw, int lane, int* piv_rows)
+{
+    double v[TS][8];
+#pragma unroll
+    for (int t = 0; t < TS; t++) {
+        const int i = k0 + lane + 32 * t;
+#pragma unroll
+        for (int c = 0; c < 8; c++) v[t][c] = (i < m && c < pw) ? a[(size_t)i * lda + k0 + c] : 0.0;
+    }
+    int info = 0;
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+        if (s >= pw) break;
+        const int k = k0 + s;
+        double bv = -1.0;
+        int bi = INT_MAX;
+#pragma unroll
+        for (int t = 0; t < TS; t++) {
+            const int i = k0 + lane + 32 * t;
+            if (i >= k && i < m) {
+                const double x = fabs(v[t][s]);
+                if (x > bv) {
+                    bv = x;
+                    bi = i;
+                }
+            }
+        }
+        warp_argmax_index(bv, bi);
+        if (!(bv > 0.0)) {
+            info = k + 1;  // exactly zero (or NaN) pivot column
+            break;
+        }
+        if (lane == 0) piv_rows[s] = bi;
+        const int pl = (bi - k0) & 31, pt = (bi - k0) >> 5;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const double xk = __shfl_sync(0xffffffffu, v[0][c], s);  // row k: lane s, slot 0
+            double y = v[0][c];
+#pragma unroll
+            for (int t = 1; t < TS; t++)
+                if (t == pt) y = v[t][c];
+            const double xp = __shfl_sync(0xffffffffu, y, pl);  // row p
+            if (lane == s) v[0][c] = xp;
+#pragma unroll
+            for (int t = 0; t < TS; t++)
+                if (t == pt && lane == pl) v[t][c] = xk;
+        }
+        const double piv = __shfl_sync(0xffffffffu, v[0][s], s);
+#pragma unroll
+        for (int t = 0; t < TS; t++) {
+            const int i = k0 + lane + 32 * t;
+            if (i > k && i < m) v[t][s] = v[t][s] / piv;
+        }
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            if (c > s && c < pw) {
+                const double u = __shfl_sync(0xffffffffu, v[0][c], s);
+#pragma unroll
+                for (int t = 0; t < TS; t++) {
+                    const int i = k0 + lane + 32 * t;
+                    if (i > k && i < m) v[t][c] = __fma_rn(-v[t][s], u, v[t][c]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < TS; t++) {
+        const int i = k0 + lane + 32 * t;
+        if (i < m)
+#pragma unroll
+            for (int c = 0; c < 8; c++)
+                if (c < pw) a[(size_t)i * lda + k0 + c] = v[t][c];
+    }
+    return info;
+}
+
+__device__ int warp_panel_any(double* a, int lda, int m, int k0, int pw, int lane, int* piv_rows)
+{
+    switch ((m - k0 + 31) >> 5) {
+    case 1: return warp_panel<1>(a, lda, m, k0, pw, lane, piv_rows);
+    case 2: return warp_panel<2>(a, lda, m, k0, pw, lane, piv_rows);
+    case 3: return warp_panel<3>(a, lda, m, k0, pw, lane, piv_rows);
+    case 4: return warp_panel<4>(a, lda, m, k0, pw, lane, piv_rows);
+    default: return warp_panel<(MAX_M + 31) / 32>(a, lda, m, k0, pw, lane, piv_rows);
     }
 }
 
@@ -580,76 +668,48 @@ __device__ void team_column_candidates(const Team& T, const double* a, int lda, 
 // team_eliminate (and so as dgetf2): every element receives its updates
 // a_ij <- fma(-l_ik, u_kj, a_ij) in ascending k, with the same multipliers
 // (divisions by the same pivots) and the same first-maximum pivots; only the
-// moment an update is applied changes.  Panels of PB columns, as LAPACK's
-// dgetrf blocks them: within a panel, step k swaps whole rows and updates the
-// panel's columns of the rows below k only (every row's trailing columns then
-// lack the same panel steps, so swapping them is consistent); after the panel,
-// the panel rows' trailing columns are solved against the unit lower triangle
-// of the panel, column by column, in ascending step order (dtrsm), and the
-// rows below receive the panel's delayed updates at once as a register-tiled
-// rank-PB product (each warp: 8 rows x 32 lanes x up to 4 column groups held in
-// registers, the L values broadcast, the U row read once per row tile), so the
-// trailing matrix is read and written once per panel instead of once per step.
+// moment an update is applied changes.  Panels of 8 columns, as LAPACK's
+// dgetrf blocks them: warp 0 factors the panel in registers (warp_panel, no
+// team barrier inside); then every thread takes trailing columns, applies
+// the panel's row exchanges to each in order (dlaswp) and solves the panel
+// rows against the panel's unit lower triangle (dtrsm, steps in order); then
+// the rows below take the panel's delayed updates at once as a
+// register-tiled rank-8 product (each warp: 8 rows x 32 lanes x up to 4
+// column groups held in registers, the L values broadcast, the U row read
+// once per row tile).  Three team barriers per panel.
+// cand_r: scratch of at least 9 ints (status, 8 pivot rows).
 template <int PB>
 __device__ int team_eliminate_blocked(const Team& T, double* a, int m, int K, int lda, double* cand_v, int* cand_r)
 {
+    static_assert(PB == 8, "warp_panel holds 8 columns");
     const int ncols = m + K;
     const int nw = T.nwarps(), w = T.warp(), lane = T.lane();
+    int* piv_rows = cand_r + 1;
     for (int k0 = 0; k0 < m; k0 += PB) {
-        const int kend = min(k0 + PB, m);
-        team_column_candidates(T, a, lda, k0, m, cand_v, cand_r);
-        T.sync();
-        for (int k = k0; k < kend; k++) {
-            double bv = cand_v[0];
-            int p = cand_r[0];
-            for (int q = 1; q < nw; q++) {
-                const double v = cand_v[q];
-                const int r = cand_r[q];
-                if (v > bv || (v == bv && r < p)) { bv = v; p = r; }
-            }
-            if (!(bv > 0.0)) return k + 1;
-            if (p != k)
-                for (int j = T.tid; j < ncols; j += T.size) {
-                    const double t = a[k * lda + j];
-                    a[k * lda + j] = a[p * lda + j];
-                    a[p * lda + j] = t;
-                }
-            T.sync();
-            const double piv = a[k * lda + k];
-            for (int i = k + 1 + T.tid; i < m; i += T.size) a[i * lda + k] = a[i * lda + k] / piv;
-            T.sync();
-            // rows k+1..m-1 x the panel's columns k+1..kend-1
-            const int wa = kend - k - 1;
-            const int na = (m - k - 1) * wa;
-            double nbv = -1.0;
-            int nbr = INT_MAX;
-            for (int e = T.tid; e < na; e += T.size) {
-                const int i = k + 1 + e / wa, j = k + 1 + e % wa;
-                const double v = __fma_rn(-a[i * lda + k], a[k * lda + j], a[i * lda + j]);
-                a[i * lda + j] = v;
-                if (j == k + 1) {
-                    const double av = fabs(v);
-                    if (av > nbv || (av == nbv && i < nbr)) { nbv = av; nbr = i; }
-                }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, nbv, o);
-                const int orr = __shfl_xor_sync(0xffffffffu, nbr, o);
-                if (ov > nbv || (ov == nbv && orr < nbr)) { nbv = ov; nbr = orr; }
-            }
-            if (lane == 0) {
-                cand_v[w] = nbv;
-                cand_r[w] = nbr;
-            }
-            T.sync();
+        const int kend = min(k0 + PB, m), pw = kend - k0;
+        if (w == 0) {
+            const int info = warp_panel_any(a, lda, m, k0, pw, lane, piv_rows);
+            if (lane == 0) cand_r[0] = info;
         }
-        // U: the panel rows' trailing columns, one column per thread, steps in order
-        for (int j = kend + T.tid; j < ncols; j += T.size)
-            for (int r = k0 + 1; r < kend; r++) {
-                double v = a[r * lda + j];
-                for (int pp = k0; pp < r; pp++) v = __fma_rn(-a[r * lda + pp], a[pp * lda + j], v);
-                a[r * lda + j] = v;
+        T.sync();
+        const int info = cand_r[0];
+        if (info) return info;
+        // trailing columns: the panel's row exchanges in order, then the panel rows (U), one column per thread
+        for (int j = kend + T.tid; j < ncols; j += T.size) {
+            for (int q = 0; q < pw; q++) {
+                const int p = piv_rows[q];
+                if (p != k0 + q) {
+                    const double t = a[(size_t)(k0 + q) * lda + j];
+                    a[(size_t)(k0 + q) * lda + j] = a[(size_t)p * lda + j];
+                    a[(size_t)p * lda + j] = t;
+                }
             }
+            for (int r = k0 + 1; r < kend; r++) {
+                double v = a[(size_t)r * lda + j];
+                for (int pp = k0; pp < r; pp++) v = __fma_rn(-a[(size_t)r * lda + pp], a[(size_t)pp * lda + j], v);
+                a[(size_t)r * lda + j] = v;
+            }
+        }
         T.sync();
         if (kend >= m) break;
         // delayed rank-(kend-k0) update of rows kend..m-1, columns kend..ncols-1
@@ -751,18 +811,28 @@ __device__ void team_back_substitute_rows(const Team& T, double* a, int m, int K
 
 // ---------------------------------------------------------------------------
 
-// Team assembly of the augmented system [A | B] of stencil r into a (m rows of
-// m + K columns at row stride ld).  xs: scratch for the stencil's coordinates;
-// fr: 7 doubles of scratch (tangent frame).  Returns m.  Ends with a team barrier.
-__device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, double* xs, double* fr, int& n_out,
-                             int ld)
+// The per-stencil quantities of an assembly: sizes, shape parameter, centre,
+// its angles, the tangent frame (e1 = fr[0..2], e2 = fr[3..5]) and scale s.
+struct SysInputs {
+    int n, deg, np, m;
+    double eps, eps2, eps_2k, lam_i, th_i, s;
+    double x0[3];
+    bool angles;  // an operator needs the nodes' longitude and latitude
+};
+
+// Team step 1 of an assembly: the stencil's node coordinates into xs, the
+// tangent frame and the largest squared distance from the centre into fr.
+// Ends with a team barrier (xs and fr visible).
+__device__ SysInputs team_inputs(const Team& T, const WParams& P, int r, double* xs, double* fr)
 {
-    const int n = P.len[r];
-    const int deg = P.deg ? P.deg[r] : P.deg_uniform;
-    const int np = poly_size(deg);
-    const int m = n + np, K = P.K;
-    const double eps = P.eps ? P.eps[r] : P.eps_uniform;  // var_epsilon[stencil[0]]
-    const double eps2 = eps * eps;
+    SysInputs S;
+    S.n = P.len[r];
+    S.deg = P.deg ? P.deg[r] : P.deg_uniform;
+    S.np = poly_size(S.deg);
+    S.m = S.n + S.np;
+    S.eps = P.eps ? P.eps[r] : P.eps_uniform;  // var_epsilon[stencil[0]]
+    S.eps2 = S.eps * S.eps;
+    const int n = S.n;
     for (int q = T.tid; q < n; q += T.size) {
         double4 v = P.xyz[P.idx[sell_elem(r, q, P.n4 >> 2)]];
         xs[3 * q] = v.x;
@@ -771,12 +841,16 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
     }
     if (T.tid == 0) fr[7] = 0.0;  // max_j |x_j - c|^2, gathered below
     T.sync();
-    const double x0[3] = {xs[0], xs[1], xs[2]};
-    const double lam_i = atan2(x0[1], x0[0]), th_i = atan2(x0[2], sqrt(x0[0] * x0[0] + x0[1] * x0[1]));
-    if (deg >= 2) {
+    const double* x0 = xs;
+    S.x0[0] = x0[0];
+    S.x0[1] = x0[1];
+    S.x0[2] = x0[2];
+    S.lam_i = atan2(x0[1], x0[0]);
+    S.th_i = atan2(x0[2], sqrt(x0[0] * x0[0] + x0[1] * x0[1]));
+    if (S.deg >= 2) {
         if (T.tid == 0) {
-            fr[0] = -sin(lam_i); fr[1] = cos(lam_i); fr[2] = 0.0;
-            fr[3] = -sin(th_i) * cos(lam_i); fr[4] = -sin(th_i) * sin(lam_i); fr[5] = cos(th_i);
+            fr[0] = -sin(S.lam_i); fr[1] = cos(S.lam_i); fr[2] = 0.0;
+            fr[3] = -sin(S.th_i) * cos(S.lam_i); fr[4] = -sin(S.th_i) * sin(S.lam_i); fr[5] = cos(S.th_i);
         }
         // the largest squared distance from the centre: a maximum, so any
         // order of the comparisons gives the same value; non-negative doubles
@@ -791,75 +865,122 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
         if (T.lane() == 0)
             atomicMax(reinterpret_cast<unsigned long long*>(fr + 7), (unsigned long long)__double_as_longlong(s2));
     }
-    // Phi block: ar(j, i) = phi(x_i - x_j)   (rbffd.cpp:943-966).  Symmetric to
-    // the last bit (x_j - x_i squares to the same r^2), so each pair j <= i is
-    // evaluated once and written to both places: n(n+1)/2 exponentials.
+    S.angles = false;
+    for (int c = 0; c < P.K; c++) S.angles |= P.opbit[c] == RBFFD_LAMBDA || P.opbit[c] == RBFFD_THETA;
+    S.eps_2k = pow(S.eps, 2 * P.hv_k);
+    T.sync();  // frame and distance visible
+    S.s = fr[7] > 0.0 ? sqrt(fr[7]) : 1.0;
+    return S;
+}
+
+// Phi entry of nodes i >= j: phi(x_i - x_j)   (rbffd.cpp:943-966).
+__device__ __forceinline__ double phi_pair(const double* xs, int i, int j, double eps2)
+{
+    double dx = xs[3 * i] - xs[3 * j], dy = xs[3 * i + 1] - xs[3 * j + 1], dz = xs[3 * i + 2] - xs[3 * j + 2];
+    double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    return g_eval(eps2, r2);
+}
+
+// Polynomial border entry: basis function q at node i.
+__device__ __forceinline__ double poly_entry(const SysInputs& S, const double* xs, const double* fr, int q, int i)
+{
+    if (S.deg >= 2) {
+        const double* e1 = fr;
+        const double* e2 = fr + 3;
+        int pa, pb;
+        tangent_exp(q, pa, pb);
+        double dx = xs[3 * i] - S.x0[0], dy = xs[3 * i + 1] - S.x0[1], dz = xs[3 * i + 2] - S.x0[2];
+        double u = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, e1[0]), __dmul_rn(dy, e1[1])), __dmul_rn(dz, e1[2])), S.s);
+        double w = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, e2[0]), __dmul_rn(dy, e2[1])), __dmul_rn(dz, e2[2])), S.s);
+        return ipow(u, pa) * ipow(w, pb);
+    }
+    int pa, pb, pc;
+    basis_exp(q, pa, pb, pc);
+    return ipow(xs[3 * i], pa) * ipow(xs[3 * i + 1], pb) * ipow(xs[3 * i + 2], pc);
+}
+
+// The node quantities a right-hand-side entry of node j < n needs: its
+// angles (when an operator needs them), x0 - x_j, its squared length, phi.
+struct NodeTerms {
+    double lam_j, th_j, dx, dy, dz, r2, phi;
+};
+
+__device__ __forceinline__ NodeTerms node_terms(const SysInputs& S, const double* xj)
+{
+    NodeTerms t;
+    t.lam_j = 0.0;
+    t.th_j = 0.0;
+    if (S.angles) {
+        t.lam_j = atan2(xj[1], xj[0]);
+        t.th_j = atan2(xj[2], sqrt(xj[0] * xj[0] + xj[1] * xj[1]));
+    }
+    t.dx = S.x0[0] - xj[0];
+    t.dy = S.x0[1] - xj[1];
+    t.dz = S.x0[2] - xj[2];
+    t.r2 = __dadd_rn(__dadd_rn(__dmul_rn(t.dx, t.dx), __dmul_rn(t.dy, t.dy)), __dmul_rn(t.dz, t.dz));
+    t.phi = g_eval(S.eps2, t.r2);
+    return t;
+}
+
+// Right-hand-side entry of operator c at node j < n.
+__device__ __forceinline__ double rhs_node(const WParams& P, const SysInputs& S, const double* xj, const NodeTerms& t,
+                                           int c)
+{
+    return rhs_rbf(P.opbit[c], S.x0, xj, S.eps2, P.dim, P.hv_k, S.eps_2k, S.lam_i, S.th_i, t.lam_j, t.th_j, t.dx, t.dy,
+                   t.dz, t.r2, t.phi);
+}
+
+// Right-hand-side entry of operator c at polynomial row j >= n.
+__device__ __forceinline__ double rhs_poly(const WParams& P, const SysInputs& S, const double* fr, int j, int c)
+{
+    double v = 0.0;
+    if (S.deg == 1) v = poly_row(P.opbit[c], j - S.n, S.x0, P.dim, P.hv_k, S.lam_i, S.th_i);
+    if (S.deg >= 2) {
+        int pa, pb;
+        tangent_exp(j - S.n, pa, pb);
+        v = tangent_row(P.opbit[c], pa, pb, fr, fr + 3, S.s, P.dim, P.hv_k);
+    }
+    return v;
+}
+
+// Team assembly of the augmented system [A | B] of stencil r into a (m rows of
+// m + K columns at row stride ld).  xs: scratch for the stencil's coordinates;
+// fr: 8 doubles of scratch (tangent frame, distance).  Returns m.  Ends with a
+// team barrier.
+__device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, double* xs, double* fr, int& n_out,
+                             int ld)
+{
+    const SysInputs S = team_inputs(T, P, r, xs, fr);
+    const int n = S.n, np = S.np, m = S.m, K = P.K;
+    // Phi block: symmetric to the last bit (x_j - x_i squares to the same
+    // r^2), so each pair j <= i is evaluated once and written to both places:
+    // n(n+1)/2 exponentials.
     for (int e = T.tid; e < n * (n + 1) / 2; e += T.size) {
         int i = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);  // e = i(i+1)/2 + j, 0 <= j <= i (estimate, corrected below)
         while (i * (i + 1) / 2 > e) i--;
         while ((i + 1) * (i + 2) / 2 <= e) i++;
         const int j = e - i * (i + 1) / 2;
-        double dx = xs[3 * i] - xs[3 * j], dy = xs[3 * i + 1] - xs[3 * j + 1], dz = xs[3 * i + 2] - xs[3 * j + 2];
-        double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-        const double v = g_eval(eps2, r2);
+        const double v = phi_pair(xs, i, j, S.eps2);
         a[j * ld + i] = v;
         a[i * ld + j] = v;
     }
-    T.sync();  // frame and distance visible
-    const double* e1 = fr;
-    const double* e2 = fr + 3;
-    const double s = fr[7] > 0.0 ? sqrt(fr[7]) : 1.0;
     // polynomial border and zero block
     for (int e = T.tid; e < np * n; e += T.size) {
         int q = e / n, i = e - q * n;
-        double v;
-        if (deg >= 2) {
-            int pa, pb;
-            tangent_exp(q, pa, pb);
-            double dx = xs[3 * i] - x0[0], dy = xs[3 * i + 1] - x0[1], dz = xs[3 * i + 2] - x0[2];
-            double u = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, e1[0]), __dmul_rn(dy, e1[1])), __dmul_rn(dz, e1[2])), s);
-            double w = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, e2[0]), __dmul_rn(dy, e2[1])), __dmul_rn(dz, e2[2])), s);
-            v = ipow(u, pa) * ipow(w, pb);
-        } else {
-            int pa, pb, pc;
-            basis_exp(q, pa, pb, pc);
-            v = ipow(xs[3 * i], pa) * ipow(xs[3 * i + 1], pb) * ipow(xs[3 * i + 2], pc);
-        }
+        const double v = poly_entry(S, xs, fr, q, i);
         a[(n + q) * ld + i] = v;
         a[i * ld + (n + q)] = v;
     }
     for (int e = T.tid; e < np * np; e += T.size) a[(n + e / np) * ld + n + e % np] = 0.0;
     // right-hand sides, one column per operator in bit order (rbffd.cpp:106-125);
-    // a node's kernel value is evaluated once for all operators, its angles
-    // only when an operator needs them
-    bool angles = false;
-    for (int c = 0; c < K; c++) angles |= P.opbit[c] == RBFFD_LAMBDA || P.opbit[c] == RBFFD_THETA;
-    const double eps_2k = pow(eps, 2 * P.hv_k);
+    // a node's kernel value is evaluated once for all operators
     for (int j = T.tid; j < m; j += T.size) {
         if (j < n) {
             const double* xj = xs + 3 * j;
-            double lam_j = 0.0, th_j = 0.0;
-            if (angles) {
-                lam_j = atan2(xj[1], xj[0]);
-                th_j = atan2(xj[2], sqrt(xj[0] * xj[0] + xj[1] * xj[1]));
-            }
-            const double dx = x0[0] - xj[0], dy = x0[1] - xj[1], dz = x0[2] - xj[2];
-            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            const double phi = g_eval(eps2, r2);
-            for (int c = 0; c < K; c++)
-                a[j * ld + m + c] = rhs_rbf(P.opbit[c], x0, xj, eps2, P.dim, P.hv_k, eps_2k, lam_i, th_i, lam_j, th_j,
-                                            dx, dy, dz, r2, phi);
+            const NodeTerms t = node_terms(S, xj);
+            for (int c = 0; c < K; c++) a[j * ld + m + c] = rhs_node(P, S, xj, t, c);
         } else {
-            for (int c = 0; c < K; c++) {
-                double v = 0.0;
-                if (deg == 1) v = poly_row(P.opbit[c], j - n, x0, P.dim, P.hv_k, lam_i, th_i);
-                if (deg >= 2) {
-                    int pa, pb;
-                    tangent_exp(j - n, pa, pb);
-                    v = tangent_row(P.opbit[c], pa, pb, e1, e2, s, P.dim, P.hv_k);
-                }
-                a[j * ld + m + c] = v;
-            }
+            for (int c = 0; c < K; c++) a[j * ld + m + c] = rhs_poly(P, S, fr, j, c);
         }
     }
     T.sync();
@@ -868,7 +989,7 @@ __device__ int team_assemble(const Team& T, const WParams& P, int r, double* a, 
 }
 
 // The elimination variants a size class can use (same arithmetic, same results).
-enum { ELIM_UNBLOCKED = 0, ELIM_BLOCKED = 1, ELIM_PERM = 2 };
+enum { ELIM_UNBLOCKED = 0, ELIM_BLOCKED = 1, ELIM_PERM = 2, ELIM_REG = 3 };
 
 // One system end to end by one team: assemble, eliminate, back-substitute,
 // store the weights of row r.  a: the team's shared memory,
@@ -905,6 +1026,226 @@ __device__ void team_solve(const Team& T, const WParams& P, int r, double* a, in
         P.w[c][sell_elem(r, j, P.n4 >> 2)] = v;
     }
     T.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Register-resident elimination: one system per CTA of NW warps.  Warp w
+// holds the physical rows w + NW q (q < R) in registers, lane l the columns
+// l + 32 c (c < C), loaded from the system team_assemble stages in shared
+// memory.  Rows never move:
+// every row keeps its logical position (dgetf2's row order after its swaps)
+// in lane q of its warp, so ties in the pivot search go to the smaller
+// position as in dgetf2.  Step k, after the one block barrier:
+//   every warp reduces the NW published candidates (first maximum |a_ik|,
+//   smaller position on ties) and reads the winner's published row (the
+//   pivot row, columns in its lanes); the pivot row takes position k and the
+//   row at position k the pivot's; the pivot leaves the active set;
+//   lane q divides its row's column-k value (gathered at the end of step k-1)
+//   by the pivot, and the active rows take a_ij <- fma(-l_i, u_kj, a_ij);
+//   lane q then gathers its row's column-(k+1) value, the warp finds its
+//   candidate for step k+1 and publishes it with its row's values
+//   (double-buffered by step parity).
+// The multipliers, pivots and the fma sequence of every element are
+// dgetf2's, so the result is team_eliminate's bit for bit.  The finished rows
+// (U and the transformed right-hand sides) are written to shared memory in
+// position order for the back substitution.  Valid for m <= NW R and
+// m + K <= 32 C.
+template <int NW, int R, int C>
+struct RegElim {
+    static constexpr int THREADS = NW * 32;
+    // shared memory: U [m x lda] | xs [3 n_pad] | fr [8] | rows [2][NW][32 C] | cand_v [2][NW] |
+    // cand_pos [2][NW] ints | cand_row [2][NW] ints
+    static size_t smem_bytes(int m, int lda, int n_pad)
+    {
+        return ((size_t)m * lda + 3 * (size_t)n_pad + 8 + 2 * (size_t)NW * 32 * C + 2 * NW + 2 * NW) * sizeof(double);
+    }
+};
+
+__device__ __forceinline__ void argmax_first(double& v, int& pos, int& who)
+{
+    // warp-wide maximum of v, ties to the smaller pos (then any who)
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int op = __shfl_xor_sync(0xffffffffu, pos, o);
+        const int ow = __shfl_xor_sync(0xffffffffu, who, o);
+        if (ov > v || (ov == v && op < pos)) {
+            v = ov;
+            pos = op;
+            who = ow;
+        }
+    }
+}
+
+template <int NW, int R, int C>
+__device__ __forceinline__ int reg_eliminate(double (&A)[R][C], int m, int ld, int w, int lane, int& mypos, double* rows,
+                             double* cand_v, int* cand_p, int* cand_r)
+{
+    unsigned act = 0;
+#pragma unroll
+    for (int q = 0; q < R; q++)
+        if (w + NW * q < m) act |= 1u << q;
+    mypos = w + NW * lane;  // lane q: the position of row w + NW q (its own index to begin with)
+    double num = 0.0;       // lane q: row q's value in the column of the current step
+    // candidates of column 0, published in buffer 0
+    {
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            const double t = __shfl_sync(0xffffffffu, A[q][0], 0);
+            if (lane == q) num = t;
+        }
+        const bool live = lane < R && ((act >> lane) & 1) && fabs(num) >= 0.0;  // NaN never a candidate
+        double v = live ? fabs(num) : -1.0;
+        int pos = live ? mypos : INT_MAX, who = lane;
+        argmax_first(v, pos, who);
+        if (lane == 0) {
+            cand_v[w] = v;
+            cand_p[w] = pos;
+            cand_r[w] = w + NW * who;
+        }
+        if (v >= 0.0) {
+#pragma unroll
+            for (int q = 0; q < R; q++)
+                if (q == who)
+#pragma unroll
+                    for (int c = 0; c < C; c++) rows[(size_t)w * 32 * C + lane + 32 * c] = A[q][c];
+        }
+    }
+    __syncthreads();
+    for (int k = 0; k < m; k++) {
+        const int par = k & 1;
+        // the pivot: first maximum over the warps' candidates
+        double gv = lane < NW ? cand_v[par * NW + lane] : -1.0;
+        int gpos = lane < NW ? cand_p[par * NW + lane] : INT_MAX, gw = lane;
+        argmax_first(gv, gpos, gw);
+        if (!(gv > 0.0)) return k + 1;  // exactly zero (or NaN) pivot column
+        const int grow = cand_r[par * NW + gw];
+        const double* prow = rows + ((size_t)par * NW + gw) * 32 * C;
+        double pr[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) pr[c] = prow[lane + 32 * c];
+        const double piv = prow[k];
+        // positions after dgetf2's swap of positions k and gpos; the pivot row leaves the active set
+        if (lane < R) {
+            if (w + NW * lane == grow)
+                mypos = k;
+            else if (mypos == k)
+                mypos = gpos;
+        }
+        if (w == gw) act &= ~(1u << (grow / NW));
+        // multipliers (lane q: row q), then the updates of the active rows
+        const double lq = num / piv;
+        const int c0 = (k + 1) >> 5;  // chunks below c0 hold only columns <= k
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            if ((act >> q) & 1) {
+                const double l = __shfl_sync(0xffffffffu, lq, q);
+#pragma unroll
+                for (int c = 0; c < C; c++)
+                    if (c >= c0) A[q][c] = __fma_rn(-l, pr[c], A[q][c]);
+            }
+        }
+        // candidates of column k + 1, published in the other buffer
+        if (k + 1 < m) {
+            const int kc = (k + 1) >> 5, kl = (k + 1) & 31;
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                double x = A[q][0];
+#pragma unroll
+                for (int c = 1; c < C; c++)
+                    if (kc == c) x = A[q][c];
+                const double t = __shfl_sync(0xffffffffu, x, kl);
+                if (lane == q) num = t;
+            }
+            const bool live = lane < R && ((act >> lane) & 1) && fabs(num) >= 0.0;  // NaN never a candidate
+            double v = live ? fabs(num) : -1.0;
+            int pos = live ? mypos : INT_MAX, who = lane;
+            argmax_first(v, pos, who);
+            const int nb = par ^ 1;
+            if (lane == 0) {
+                cand_v[nb * NW + w] = v;
+                cand_p[nb * NW + w] = pos;
+                cand_r[nb * NW + w] = w + NW * who;
+            }
+            if (v >= 0.0) {
+                double* dst = rows + ((size_t)nb * NW + w) * 32 * C;
+#pragma unroll
+                for (int q = 0; q < R; q++)
+                    if (q == who)
+#pragma unroll
+                        for (int c = 0; c < C; c++) dst[lane + 32 * c] = A[q][c];
+            }
+        }
+        __syncthreads();
+    }
+    return 0;
+}
+
+// The register-resident solve of a class: per system, the inputs, the
+// entries into registers, the elimination, the rows into shared memory in
+// position order, the back substitution and the store of team_solve.
+template <int NW, int R, int C>
+__global__ void __launch_bounds__(NW * 32, NW == 16 ? 1 : 2) k_weights_reg(WParams P)
+{
+    extern __shared__ double smem[];
+    __shared__ int s_unit;
+    const WClass Cc = P.cls[0];
+    const int m = Cc.m, lda = Cc.lda, K = P.K, ld = m + K;
+    double* U = smem;
+    double* xs = U + (size_t)m * lda;
+    double* fr = xs + 3 * P.n_pad;
+    double* rows = fr + 8;
+    double* cand_v = rows + 2 * NW * 32 * C;
+    int* cand_p = (int*)(cand_v + 2 * NW);
+    int* cand_r = cand_p + 2 * NW;
+    Team T;
+    T.size = NW * 32;
+    T.id = 0;
+    T.tid = threadIdx.x;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = atomicAdd(P.work, 1);
+        __syncthreads();
+        const int u = s_unit;
+        __syncthreads();
+        if (u >= P.nunits) break;
+        const int r = P.rows[Cc.rows_off + u];
+        int n;
+        team_assemble(T, P, r, U, xs, fr, n, lda);  // staged in shared memory, then into registers
+        double A[R][C];
+#pragma unroll
+        for (int q = 0; q < R; q++)
+#pragma unroll
+            for (int c = 0; c < C; c++) {
+                const int row = w + NW * q, col = lane + 32 * c;
+                A[q][c] = (row < m && col < ld) ? U[(size_t)row * lda + col] : 0.0;
+            }
+        __syncthreads();  // every row read before the rows are written back in position order
+        int mypos;
+        const int st = reg_eliminate<NW, R, C>(A, m, ld, w, lane, mypos, rows, cand_v, cand_p, cand_r);
+        const bool ok = st == 0;
+        if (ok) {
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                const int row = w + NW * q;
+                const int pos = __shfl_sync(0xffffffffu, mypos, q);
+                if (row < m)
+#pragma unroll
+                    for (int c = 0; c < C; c++)
+                        if (lane + 32 * c < ld) U[(size_t)pos * lda + lane + 32 * c] = A[q][c];
+            }
+            __syncthreads();
+            team_back_substitute_rows(T, U, m, K, [&](int i) { return U + (size_t)i * lda; });
+        }
+        if (!ok && threadIdx.x == 0) atomicMin(P.status, r + 1);
+        for (int e = threadIdx.x; e < K * P.n4; e += T.size) {
+            const int c = e / P.n4, j = e - c * P.n4;
+            const double scale = P.opbit[c] == RBFFD_HV ? P.hv_scale : 1.0;
+            const double v = (j < n) ? (ok ? U[(size_t)j * lda + m + c] * scale : __longlong_as_double(0x7ff8000000000000ll))
+                                     : 0.0;
+            P.w[c][sell_elem(r, j, P.n4 >> 2)] = v;
+        }
+        __syncthreads();
+    }
 }
 
 // One size class in one persistent launch (the classes of a call run as a
@@ -1032,7 +1373,7 @@ static size_t class_stride_bytes(int m, int K, int n_pad)
 }
 
 // Candidate shapes of a class: teams whose shared memory fits one CTA.
-static std::vector<WShape> w_candidates(int m, size_t stride_bytes, int smem_max)
+static std::vector<WShape> w_candidates(int m, int K, int n_pad, size_t stride_bytes, int smem_max)
 {
     std::vector<WShape> out;
     const int teams[4] = {32, 64, 128, 256};
@@ -1044,6 +1385,12 @@ static std::vector<WShape> w_candidates(int m, size_t stride_bytes, int smem_max
         out.push_back(WShape{tw, ELIM_PERM});
         if (m >= 24) out.push_back(WShape{tw, ELIM_BLOCKED});
     }
+    // register-resident elimination (one system per CTA of 256 or 512 threads), last: measured slower
+    const int lda = class_lda(m, K);
+    if (m <= 64 && m + K <= 64 && RegElim<8, 8, 2>::smem_bytes(m, lda, n_pad) <= (size_t)smem_max)
+        out.push_back(WShape{RegElim<8, 8, 2>::THREADS, ELIM_REG});
+    else if (m <= 128 && m + K <= 128 && RegElim<16, 8, 4>::smem_bytes(m, lda, n_pad) <= (size_t)smem_max)
+        out.push_back(WShape{RegElim<16, 8, 4>::THREADS, ELIM_REG});
     return out;
 }
 
@@ -1093,7 +1440,7 @@ static int weights_work(rbffd_grid* g, WeightsWork** out)
     return RBFFD_OK;
 }
 
-// The kernel of an elimination mode.
+// The kernel of a shared-memory elimination mode.
 static void (*class_kernel(int mode))(WParams)
 {
     return mode == ELIM_BLOCKED ? k_weights_class<ELIM_BLOCKED>
@@ -1101,34 +1448,54 @@ static void (*class_kernel(int mode))(WParams)
                                 : k_weights_class<ELIM_UNBLOCKED>;
 }
 
+// Register-resident shapes: 16 warps x 8 rows x 4 column chunks (m <= 128,
+// m + K <= 128) and 8 warps x 8 rows x 2 chunks (m <= 64, m + K <= 64).
+using RegL = RegElim<16, 8, 4>;
+using RegS = RegElim<8, 8, 2>;
+static bool reg_small(int m, int K) { return m <= 64 && m + K <= 64; }
+
+// Kernel, threads per CTA and dynamic shared memory of a one-class P's launch.
+struct ClassLaunch {
+    void (*kern)(WParams);
+    int threads;
+    size_t smem;
+};
+
+static ClassLaunch class_launch(const WParams& P)
+{
+    const WClass& C = P.cls[0];
+    if (C.blocked == ELIM_REG) {
+        if (reg_small(C.m, P.K)) return {k_weights_reg<8, 8, 2>, RegS::THREADS, RegS::smem_bytes(C.m, C.lda, P.n_pad)};
+        return {k_weights_reg<16, 8, 4>, RegL::THREADS, RegL::smem_bytes(C.m, C.lda, P.n_pad)};
+    }
+    return {class_kernel(C.blocked), W_CTA, (size_t)C.teams * C.stride * sizeof(double)};
+}
+
 // Shared memory and grid of the persistent launch of a one-class P (cls[0]):
 // as many CTAs as fit on the device at once, at most one per work unit.
 static int persistent_geometry(rbffd_ctx* ctx, const WParams& P, size_t* smem, int* grid)
 {
-    const WClass& C = P.cls[0];
-    const size_t sm = (size_t)C.teams * C.stride * sizeof(double);
-    auto kern = class_kernel(C.blocked);
-    RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const ClassLaunch L = class_launch(P);
+    RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(L.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
     int per_sm = 0;
-    RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W_CTA, sm));
+    RBFFD_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.kern, L.threads, L.smem));
     if (per_sm < 1) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "weight kernel shape does not fit an SM");
-    *smem = sm;
+    *smem = L.smem;
     *grid = std::max(1, std::min(P.nunits, per_sm * ctx->sm_count));
     return RBFFD_OK;
 }
 
-// Each mode's kernel allowed the largest dynamic shared memory of the classes
-// that use it (the attribute is per kernel, and a captured or replayed launch
+// Each kernel allowed the largest dynamic shared memory of the classes that
+// use it (the attribute is per kernel, and a captured or replayed launch
 // needs it to cover its own size).
 static int class_smem_attributes(rbffd_ctx* ctx, const WParams* Q, const size_t* smem, int n)
 {
-    for (int mode : {ELIM_UNBLOCKED, ELIM_BLOCKED, ELIM_PERM}) {
+    for (int c = 0; c < n; c++) {
+        const auto kern = class_launch(Q[c]).kern;
         size_t mx = 0;
-        for (int c = 0; c < n; c++)
-            if (Q[c].cls[0].blocked == mode) mx = std::max(mx, smem[c]);
-        if (mx)
-            RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(class_kernel(mode), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)mx));
+        for (int d = 0; d < n; d++)
+            if (class_launch(Q[d]).kern == kern) mx = std::max(mx, smem[d]);
+        RBFFD_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx));
     }
     return RBFFD_OK;
 }
@@ -1136,15 +1503,16 @@ static int class_smem_attributes(rbffd_ctx* ctx, const WParams* Q, const size_t*
 // Zero the class's counter and launch (what the graph holds, class by class).
 static void enqueue_persistent(const WParams& P, size_t smem, int grid, cudaStream_t s)
 {
+    const ClassLaunch L = class_launch(P);
     cudaMemsetAsync(P.work, 0, sizeof(int), s);
-    class_kernel(P.cls[0].blocked)<<<grid, W_CTA, smem, s>>>(P);
+    L.kern<<<grid, L.threads, smem, s>>>(P);
 }
 
 // Shape a one-class P: its teams per CTA and work units (cls[0].team/blocked set).
 static void number_units(WParams& P)
 {
     WClass& C = P.cls[0];
-    C.teams = W_CTA / C.team;
+    C.teams = C.blocked == ELIM_REG ? 1 : W_CTA / C.team;  // register-resident: one system per CTA
     C.unit0 = 0;
     P.nunits = (C.nrows + C.teams - 1) / C.teams;
 }
@@ -1289,7 +1657,13 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
         C.rows_off = off;
         C.nrows = (int)kv.second.size();
         off += C.nrows;
-        TuneKey key{200 + K, C.m, g->n_pad, 0, 0};
+        // a forced elimination (rbffd_weights_set_elimination) narrows the candidates to its own shapes
+        const int forced = ctx->weights_elim == RBFFD_ELIM_UNBLOCKED ? ELIM_UNBLOCKED
+                           : ctx->weights_elim == RBFFD_ELIM_BLOCKED ? ELIM_BLOCKED
+                           : ctx->weights_elim == RBFFD_ELIM_ROW_MAP ? ELIM_PERM
+                           : ctx->weights_elim == RBFFD_ELIM_REGISTERS ? ELIM_REG
+                                                                      : -1;
+        TuneKey key{200 + K, C.m, g->n_pad, forced + 1, 0};
         WShape best{0, 0};
         {
             std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1297,7 +1671,13 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
             if (it != ctx->tuned.end()) best = WShape{it->second.lanes, it->second.block};
         }
         if (best.team == 0) {
-            std::vector<WShape> cands = w_candidates(C.m, sb, smem_max);
+            std::vector<WShape> cands = w_candidates(C.m, K, g->n_pad, sb, smem_max);
+            if (forced >= 0) {  // the forced elimination where it applies to this size, else all shapes
+                std::vector<WShape> f;
+                for (const WShape& cs : cands)
+                    if (cs.blocked == forced) f.push_back(cs);
+                if (!f.empty()) cands = f;
+            }
             if (cands.empty()) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "no kernel shape fits system size %d", C.m);
             best = cands[0];
             if (cands.size() > 1 && C.nrows >= 2048) {
@@ -1312,7 +1692,8 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
                     Q.cls[0] = C;
                     Q.cls[0].team = cs.team;
                     Q.cls[0].blocked = cs.blocked;
-                    Q.cls[0].nrows = std::min(C.nrows, 16 * ctx->sm_count * (W_CTA / cs.team));
+                    Q.cls[0].nrows =
+                        std::min(C.nrows, 16 * ctx->sm_count * (cs.blocked == ELIM_REG ? 1 : W_CTA / cs.team));
                     Q.work = W->d_status + 1;
                     number_units(Q);
                     size_t smem;
@@ -1399,6 +1780,23 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
             if ((rc = grid_make_f32(g, oa[k]))) return rc;
     }
     RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_weights_set_elimination(rbffd_ctx* ctx, int method)
+{
+    if (!ctx) return RBFFD_ERR_INVALID;
+    if (method < RBFFD_ELIM_AUTO || method > RBFFD_ELIM_REGISTERS)
+        return set_error(ctx, RBFFD_ERR_INVALID, "unknown elimination %d", method);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->weights_elim = method;
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_weights_get_elimination(rbffd_ctx* ctx, int* method)
+{
+    if (!ctx || !method) return RBFFD_ERR_INVALID;
+    *method = ctx->weights_elim;
     return RBFFD_OK;
 }
 

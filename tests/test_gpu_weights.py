@@ -196,3 +196,89 @@ def test_alt_sfc_operators(ctx):
     b = der.applyWeightsForDeriv(R.XSFC, f)
     assert rel_l2(a, b) < 1e-2
     grid.close()
+
+
+METHODS = (R.ELIM_AUTO, R.ELIM_UNBLOCKED, R.ELIM_BLOCKED, R.ELIM_ROW_MAP, R.ELIM_REGISTERS)
+
+
+def _weights_by_method(ctx, xyz, full, lens, degs, eps, types, methods=METHODS):
+    grid = R.Grid(ctx, xyz, full, st_len=lens)
+    out = {}
+    try:
+        for meth in methods:
+            ctx.setWeightsElimination(meth)
+            assert ctx.getWeightsElimination() == meth
+            der = R.RBFFD(types, grid, 2)
+            der.setEpsilon(eps)
+            der.setPolynomialDegree(1, deg_per_row=degs)
+            der.computeAllWeightsForAllStencils()
+            out[meth] = {t: der.getWeights(t) for t in (R.XSFC, R.YSFC, R.ZSFC)}
+    finally:
+        ctx.setWeightsElimination(R.ELIM_AUTO)
+        grid.close()
+    return out
+
+
+def test_weights_every_elimination_same_bits(ctx):
+    """The batched mix (n in {17, 31, 50, 101}, degrees 1-4: m = 21, 37, 60,
+    116) solved with each elimination -- shared-memory unblocked, blocked
+    panels, row map, and the rows held in registers -- gives the same weights
+    bit for bit, and they differentiate like the oracle's."""
+    N = 6000
+    xyz = R.fibonacci_nodes(N, 5)
+    full = R.knn_stencils(xyz, 101)
+    rng = np.random.default_rng(5)
+    sizes = np.array([17, 31, 50, 101])
+    pick = rng.integers(0, 4, N)
+    lens = sizes[pick].astype(np.int32)
+    degs = (pick + 1).astype(np.int32)
+    eps = rng.uniform(10.0, 16.0, N)
+    types = R.XSFC | R.YSFC | R.ZSFC
+    W = _weights_by_method(ctx, xyz, full, lens, degs, eps, types)
+    for meth in METHODS[1:]:
+        for t in (R.XSFC, R.YSFC, R.ZSFC):
+            assert np.array_equal(W[meth][t], W[R.ELIM_AUTO][t]), (meth, t)
+    Wo = O.weights(xyz, full, lens, eps, O.XSFC | O.YSFC | O.ZSFC, dim=2, deg_per_row=degs)
+    f = np.sin(2 * xyz[:, 0] + xyz[:, 1]) * np.cos(xyz[:, 2])
+    for t in (R.XSFC, R.YSFC, R.ZSFC):
+        assert rel_l2(O.apply(full, lens, W[R.ELIM_REGISTERS][t], f), O.apply(full, lens, Wo[t], f)) < 1e-6
+
+
+@pytest.mark.parametrize("n,deg", [(110, 4), (51, 3)])
+def test_register_elimination_at_its_size_limits(ctx, n, deg):
+    """The register-resident shapes at their largest systems: m = 125 with
+    three right-hand sides fills 4 column chunks of 16 warps x 8 rows exactly
+    (m + K = 128); m = 61 fills the 8-warp shape's 2 chunks (m + K = 64).
+    Same bits as the shared-memory elimination."""
+    N = 3000
+    xyz = R.fibonacci_nodes(N, 6)
+    full = R.knn_stencils(xyz, n)
+    lens = np.full(N, n, dtype=np.int32)
+    degs = np.full(N, deg, dtype=np.int32)
+    eps = np.random.default_rng(6).uniform(8.0, 12.0, N)
+    W = _weights_by_method(ctx, xyz, full, lens, degs, eps, R.XSFC | R.YSFC | R.ZSFC,
+                           methods=(R.ELIM_UNBLOCKED, R.ELIM_REGISTERS))
+    for t in (R.XSFC, R.YSFC, R.ZSFC):
+        assert np.isfinite(W[R.ELIM_REGISTERS][t]).all()
+        assert np.array_equal(W[R.ELIM_REGISTERS][t], W[R.ELIM_UNBLOCKED][t]), t
+
+
+@pytest.mark.parametrize("meth", METHODS[1:])
+def test_weights_singular_stencil_reported(ctx, meth):
+    """A stencil that lists a node twice has two equal rows: every
+    elimination meets an exactly zero pivot and the call reports it."""
+    N, n = 2048, 31
+    xyz = R.fibonacci_nodes(N, 7)
+    st = R.knn_stencils(xyz, n)
+    st[100, 7] = st[100, 6]
+    grid = R.Grid(ctx, xyz, st)
+    ctx.setWeightsElimination(meth)
+    try:
+        der = R.RBFFD(R.XSFC, grid, 2)
+        der.setEpsilon(10.0)
+        der.setPolynomialDegree(2)
+        with pytest.raises(R.RbffdError):
+            der.computeAllWeightsForAllStencils()
+    finally:
+        ctx.setWeightsElimination(R.ELIM_AUTO)
+        grid.close()
