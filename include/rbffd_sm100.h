@@ -464,14 +464,16 @@ enum {
 int rbffd_pde_set_tiled_shape(rbffd_pde* pde, int rows_per_block, int lanes, int flags);
 int rbffd_pde_get_tiling(rbffd_pde* pde, int* rows_per_block);
 int rbffd_pde_get_tile_flags(rbffd_pde* pde, int* flags);
-/* FP32 advection with time-independent coefficients: replace the three
+/* Advection with time-independent coefficients: replace the three
  * operators of each stage (CosineBell::solve's Dlambda, Dtheta and HV,
  * cosine_bell.cpp:47-57) by one fused operator
  * Wf = -(cu W_lambda + cv W_theta) + W_hv, formed once in FP64 from the FP64
- * weights and rounded to FP32, so a stage streams one weight array instead of
- * three (beyond the reference; results within FP32 rounding of the
- * three-operator path, not bit-identical).  on = 0 returns to three
- * operators.  RBFFD_ERR_UNSUPPORTED for heat or FP64 PDEs. */
+ * weights and rounded to the PDE's dtype, so a stage streams one weight array
+ * instead of three (beyond the reference; results within the dtype's rounding
+ * of the three-operator path, not bit-identical: FP64 PDEs that must keep the
+ * reference's operation order stay on three operators).  on = 0 returns to
+ * three operators.  RBFFD_ERR_UNSUPPORTED for heat PDEs and for PDEs in the
+ * unfused (reference) arithmetic. */
 int rbffd_pde_set_fused_operator(rbffd_pde* pde, int on);
 
 /* ---- serving: persistent request loop with continuous batching --------- *

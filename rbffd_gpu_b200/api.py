@@ -654,7 +654,8 @@ class TimeDependentPDE:
         return a.value, b.value, r.value
 
     def setFusedOperator(self, on=True):
-        """FP32 advection: one fused operator -(cu Wl + cv Wt) + Whv per stage."""
+        """Advection: one fused operator -(cu Wl + cv Wt) + Whv per stage (formed
+        in FP64, rounded to the PDE's dtype; not in the unfused arithmetic)."""
         self.ctx.check(self.ctx.L.rbffd_pde_set_fused_operator(self.h, int(bool(on))), "set_fused_operator")
 
     TILE_STREAM_WEIGHTS, TILE_SLOT_SCHEDULE, TILE_PREFETCH, TILE_PIPELINE, TILE_DOUBLE_BUFFER = 1, 2, 4, 8, 16

@@ -151,10 +151,10 @@ struct rbffd_pde {
     int op[3] = {-1, -1, -1};
     void *u = nullptr, *xa = nullptr, *xb = nullptr, *acc = nullptr;
     void *cu = nullptr, *cv = nullptr;
-    // FP32 advection with one fused operator -(cu W_lambda + cv W_theta) + W_hv
-    // (sliced ELL, formed in FP64 and rounded once): the stages stream one
-    // weight array instead of three
-    float* wf = nullptr;
+    // Advection with one fused operator -(cu W_lambda + cv W_theta) + W_hv
+    // (sliced ELL, formed in FP64, rounded once to the PDE's dtype): the
+    // stages stream one weight array instead of three
+    void* wf = nullptr;  // in the PDE's dtype
     bool fused = false;
     // The one FP32 operator the stages stream (wf, or the grid's FP32 copy)
     // in the slot schedule of halo ws_R for ws_P rows per wavefront; remade

@@ -696,7 +696,7 @@ static int pde_sched_prepare(rbffd_pde* P, int R)
     const Halo* h = nullptr;
     int rc = grid_halo_schedule(g, R, Pw, &h);
     if (rc) return rc;
-    const float* src = P->fused ? P->wf : g->d_w32[P->op[0]];
+    const float* src = P->fused ? (const float*)P->wf : g->d_w32[P->op[0]];
     const unsigned ver = P->fused ? 0u : g->w32_ver[P->op[0]];
     if (!src) return set_error(ctx, RBFFD_ERR_STATE, "no FP32 weights for the slot schedule");
     if (!P->ws) {
@@ -1214,17 +1214,18 @@ static void pde_free(rbffd_pde* P)
     dev_free(ctx, P->stage64, (size_t)P->g->N * P->T * 8);
     dev_free(ctx, P->cu, (size_t)P->g->N * es);
     dev_free(ctx, P->cv, (size_t)P->g->N * es);
-    dev_free(ctx, P->wf, (size_t)P->g->N32 * P->g->n4 * sizeof(float));
+    dev_free(ctx, P->wf, (size_t)P->g->N32 * P->g->n4 * (P->dtype == RBFFD_F64 ? sizeof(double) : sizeof(float)));
     dev_free(ctx, P->ws, (size_t)P->g->N32 * P->g->n4 * sizeof(float));
     delete P;
 }
 
-// Fused advection operator of an FP32 PDE, row by row over the padded rows
-// (padding rows and slots 0): Wf = -(cu W_lambda + cv W_theta) (+ W_hv) in
-// FP64 from the FP64 weights and the PDE's FP32 coefficients, rounded once.
-__global__ void k_fuse_operator(float* __restrict__ wf, const double* __restrict__ wl, const double* __restrict__ wt,
-                                const double* __restrict__ wh, const float* __restrict__ cu,
-                                const float* __restrict__ cv, int N, int rows, int nc)
+// Fused advection operator, row by row over the padded rows (padding rows
+// and slots 0): Wf = -(cu W_lambda + cv W_theta) (+ W_hv) in FP64 from the
+// FP64 weights and the PDE's coefficients (in its dtype T), rounded once to T.
+template <typename T>
+__global__ void k_fuse_operator(T* __restrict__ wf, const double* __restrict__ wl, const double* __restrict__ wt,
+                                const double* __restrict__ wh, const T* __restrict__ cu, const T* __restrict__ cv,
+                                int N, int rows, int nc)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
@@ -1233,7 +1234,7 @@ __global__ void k_fuse_operator(float* __restrict__ wf, const double* __restrict
         const size_t o = sell_elem(i, s, nc);
         double w = -__fma_rn(a, wl[o], __dmul_rn(c, wt[o]));
         if (wh) w = __dadd_rn(w, wh[o]);
-        wf[o] = i < N ? __double2float_rn(w) : 0.0f;
+        wf[o] = i < N ? (T)w : T(0);
     }
 }
 
@@ -1249,20 +1250,29 @@ extern "C" int rbffd_pde_set_fused_operator(rbffd_pde* P, int on)
         P->fused = false;
         return RBFFD_OK;
     }
-    if (P->kind != KIND_ADVECT || P->dtype != RBFFD_F32)
-        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a fused operator is built for FP32 advection only");
+    if (P->kind != KIND_ADVECT)
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a fused operator is built for advection only");
+    if (P->arith == RBFFD_ARITH_UNFUSED)
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "the unfused (reference) arithmetic keeps the three operators");
     if (P->fused) return RBFFD_OK;
     rbffd_grid* g = P->g;
     cudaSetDevice(ctx->device);
-    const size_t bytes = (size_t)g->N32 * g->n4 * sizeof(float);
+    const bool f64 = P->dtype == RBFFD_F64;
+    const size_t bytes = (size_t)g->N32 * g->n4 * (f64 ? sizeof(double) : sizeof(float));
     if (!P->wf) {
         int rc = dev_alloc(ctx, (void**)&P->wf, bytes);
         if (rc) return rc;
         P->bytes += bytes;
     }
-    k_fuse_operator<<<(g->N32 + 127) / 128, 128, 0, ctx->stream>>>(
-        P->wf, g->d_w64[P->op[0]], g->d_w64[P->op[1]], P->op[2] >= 0 ? g->d_w64[P->op[2]] : nullptr,
-        (const float*)P->cu, (const float*)P->cv, g->N, g->N32, g->nc);
+    const double* wh = P->op[2] >= 0 ? g->d_w64[P->op[2]] : nullptr;
+    if (f64)
+        k_fuse_operator<double><<<(g->N32 + 127) / 128, 128, 0, ctx->stream>>>(
+            (double*)P->wf, g->d_w64[P->op[0]], g->d_w64[P->op[1]], wh, (const double*)P->cu, (const double*)P->cv,
+            g->N, g->N32, g->nc);
+    else
+        k_fuse_operator<float><<<(g->N32 + 127) / 128, 128, 0, ctx->stream>>>(
+            (float*)P->wf, g->d_w64[P->op[0]], g->d_w64[P->op[1]], wh, (const float*)P->cu, (const float*)P->cv,
+            g->N, g->N32, g->nc);
     RBFFD_CUDA_TRY(ctx, cudaGetLastError());
     P->ws_src = nullptr;  // a scheduled copy of the previous operator is stale
     if (P->gexec) {
@@ -1465,6 +1475,8 @@ extern "C" int rbffd_pde_set_arithmetic(rbffd_pde* P, int arith)
         return set_error(P->ctx, RBFFD_ERR_INVALID, "unknown arithmetic %d", arith);
     if (arith == RBFFD_ARITH_UNFUSED && (P->dtype != RBFFD_F64 || P->T != 1))
         return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "the unfused (reference) arithmetic is FP64 with one tracer");
+    if (arith == RBFFD_ARITH_UNFUSED && P->fused)
+        return set_error(P->ctx, RBFFD_ERR_UNSUPPORTED, "the unfused (reference) arithmetic keeps the three operators");
     P->arith = arith;
     P->forced = false;
     P->shape = Shape{};

@@ -294,6 +294,19 @@ __device__ double rhs_rbf(unsigned bit, const double* x0, const double* xj, doub
 // Team elimination on the augmented row-major matrix a (m x ld, ld = m + K).
 // cand_v / cand_r: one pivot candidate per warp.  Returns false on a zero pivot.
 
+// Warp-wide first maximum: the largest v, ties to the smaller index i.
+__device__ __forceinline__ void warp_argmax_index(double& v, int& i)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+        if (ov > v || (ov == v && oi < i)) {
+            v = ov;
+            i = oi;
+        }
+    }
+}
+
 __device__ void team_pivot_column0(const Team& T, const double* a, int m, int ld, double* cand_v, int* cand_r)
 {
     // candidates for step 0: rows handled warp-strided, first maximum kept
@@ -394,41 +407,49 @@ __device__ __forceinline__ void warp_step_any(int k, int ld, int m, int i0, int 
 }
 
 // Returns 0, or k + 1 when the pivot column at step k is exactly zero (dgetrf's INFO).
-// a: m rows of ld = m + K columns at row stride lda (>= ld).
-__device__ int team_eliminate(const Team& T, double* a, int m, int K, int lda, double* cand_v, int* cand_r)
+// a: m rows of ld = m + K columns at row stride lda (>= ld); lbuf: m doubles
+// of scratch.  Two team barriers per step: after the barrier every thread
+// reduces the warps' candidates (lanes in parallel) to the pivot row p, reads
+// the pivot a_pk, exchanges rows k and p beyond column k and forms the
+// multipliers into lbuf (row p's from the old a_kk, which the exchange would
+// have moved there; column k itself is not written); after the next barrier
+// the warps update their rows and publish the candidates of column k+1, and
+// a_kk takes the pivot (the U diagonal the back substitution reads).  The
+// same divisions, pivots and fma sequence as dgetf2.
+__device__ int team_eliminate(const Team& T, double* a, int m, int K, int lda, double* cand_v, int* cand_r,
+                              double* lbuf)
 {
     const int ld = m + K;
     const int nw = T.nwarps(), w = T.warp(), lane = T.lane();
     team_pivot_column0(T, a, m, lda, cand_v, cand_r);
     T.sync();
     for (int k = 0; k < m; k++) {
-        // reduce the per-warp candidates (every thread, identical result)
+        // the warps' candidates, first maximum (every warp, identical result)
         double bv = cand_v[0];
         int p = cand_r[0];
-        for (int q = 1; q < nw; q++) {
-            double v = cand_v[q];
-            int r = cand_r[q];
-            if (v > bv || (v == bv && r < p)) { bv = v; p = r; }
+        if (nw > 1) {
+            bv = lane < nw ? cand_v[lane] : -1.0;
+            p = lane < nw ? cand_r[lane] : INT_MAX;
+            warp_argmax_index(bv, p);
         }
         if (!(bv > 0.0)) return k + 1;  // exactly zero (or NaN) pivot column
+        const double piv = a[(size_t)p * lda + k];
         if (p != k)
-            for (int j = k + T.tid; j < ld; j += T.size) {
-                double t = a[k * lda + j];
-                a[k * lda + j] = a[p * lda + j];
-                a[p * lda + j] = t;
+            for (int j = k + 1 + T.tid; j < ld; j += T.size) {
+                const double t = a[(size_t)k * lda + j];
+                a[(size_t)k * lda + j] = a[(size_t)p * lda + j];
+                a[(size_t)p * lda + j] = t;
             }
+        for (int i = k + 1 + T.tid; i < m; i += T.size)
+            lbuf[i] = (i == p ? a[(size_t)k * lda + k] : a[(size_t)i * lda + k]) / piv;
         T.sync();
-        const double piv = a[k * lda + k];
-        // the multipliers of all rows at once, one division per thread, kept in
-        // column k (where LAPACK keeps L; nothing reads it afterwards)
-        for (int i = k + 1 + T.tid; i < m; i += T.size) a[i * lda + k] = a[i * lda + k] / piv;
-        T.sync();
+        if (T.tid == 0) a[(size_t)k * lda + k] = piv;
         // rows split across warps, columns across lanes
         double nbv = -1.0;
         int nbr = INT_MAX;
         warp_step_any(
             k, ld, m, k + 1 + w, nw, lane, a + (size_t)k * lda, [&](int i) { return a + (size_t)i * lda; },
-            [&](int i) { return a[(size_t)i * lda + k]; }, nbv, nbr);
+            [&](int i) { return lbuf[i]; }, nbv, nbr);
         if (lane == 0) {
             cand_v[w] = nbv;
             cand_r[w] = nbr;
@@ -553,19 +574,6 @@ __device__ int team_eliminate_perm(const Team& T, double* a, int m, int K, int l
         T.sync();
     }
     return 0;
-}
-
-// Warp-wide first maximum: the largest v, ties to the smaller index i.
-__device__ __forceinline__ void warp_argmax_index(double& v, int& i)
-{
-    for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-        if (ov > v || (ov == v && oi < i)) {
-            v = ov;
-            i = oi;
-        }
-    }
 }
 
 // The panel of columns k0 .. k0+pw-1 (pw <= 8) over rows k0 .. m-1, factored
@@ -1007,7 +1015,7 @@ __device__ void team_solve(const Team& T, const WParams& P, int r, double* a, in
     team_assemble(T, P, r, a, xs, fr, n, lda);
     const int st = mode == ELIM_BLOCKED ? team_eliminate_blocked<8>(T, a, m, K, lda, cand_v, cand_r)
                    : mode == ELIM_PERM  ? team_eliminate_perm(T, a, m, K, lda, cand_v, cand_r, perm)
-                                        : team_eliminate(T, a, m, K, lda, cand_v, cand_r);
+                                        : team_eliminate(T, a, m, K, lda, cand_v, cand_r, (double*)perm);
     const bool ok = st == 0;
     const int* F = perm + (m & 1) * m;  // ELIM_PERM: where each logical row lives
     if (ok) {
@@ -1324,7 +1332,7 @@ __global__ void __launch_bounds__(512) k_gesv(double* A, double* B, int* info, i
         T.sync();
         const int st = blocked == ELIM_BLOCKED ? team_eliminate_blocked<8>(T, a, m, K, ld, cand_v, cand_r)
                        : blocked == ELIM_PERM  ? team_eliminate_perm(T, a, m, K, ld, cand_v, cand_r, perm)
-                                               : team_eliminate(T, a, m, K, ld, cand_v, cand_r);
+                                               : team_eliminate(T, a, m, K, ld, cand_v, cand_r, (double*)perm);
         if (st == 0) {
             if (blocked == ELIM_PERM)
                 team_back_substitute_rows(T, a, m, K, [&](int i) { return a + (size_t)F[i] * ld; });

@@ -228,13 +228,46 @@ def test_fused_advection_operator_fp32(bell, ntr, shape):
     assert np.array_equal(run(fused_then_off=True, fused=False), run(fused=False))
 
 
+@pytest.mark.parametrize("ntr", [1, 16])
+def test_fused_operator_fp64(bell, ntr):
+    """FP64 advection on its fused operator (formed in FP64, one weight array
+    per stage): within FP64 rounding of the three-operator path (itself within
+    rounding of the oracle)."""
+    rng = np.random.default_rng(80 + ntr)
+    u0 = bell["h0"] if ntr == 1 else bell["h0"][:, None] * (1.0 + 0.1 * rng.random((1, ntr)))
+    steps = 20
+
+    def run(fused):
+        pde = R.Advection(bell["grid"], bell["der"], bell["cu"], bell["cv"], True, dtype=R.F64, ntracers=ntr)
+        if fused:
+            pde.setFusedOperator(True)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, bell["p"]["dt"], steps, graph=True)
+        out = pde.getLocalSolution()
+        pde.close()
+        return out
+
+    three = run(False)
+    assert rel_l2(run(True), three) <= 1e-12
+    if ntr == 1:
+        assert rel_l2(three, _oracle_bell(bell, steps)) <= 1e-14
+
+
 def test_fused_operator_errors(bell, heat):
+    """The reference's (unfused) arithmetic keeps the three operators either
+    way round; heat has no operator to fuse."""
     pde = R.CosineBell(bell["grid"], bell["der"], bell["p"]["a"], bell["p"]["alpha"], bell["p"]["T"], True,
                        dtype=R.F64)
+    pde.setArithmetic(R.ARITH_UNFUSED)
     with pytest.raises(R.RbffdError) as e:
         pde.setFusedOperator(True)
     assert e.value.status == -5
     pde.setFusedOperator(False)  # off is always accepted
+    pde.setArithmetic(R.ARITH_FUSED)
+    pde.setFusedOperator(True)
+    with pytest.raises(R.RbffdError) as e:
+        pde.setArithmetic(R.ARITH_UNFUSED)
+    assert e.value.status == -5
     pde.close()
     hp = R.HeatSphere(heat["grid"], heat["der"], 1.0, dtype=R.F32)
     with pytest.raises(R.RbffdError) as e:
