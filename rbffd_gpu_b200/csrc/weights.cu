@@ -427,10 +427,19 @@ __device__ int team_eliminate(const Team& T, double* a, int m, int K, int lda, d
         // the warps' candidates, first maximum (every warp, identical result)
         double bv = cand_v[0];
         int p = cand_r[0];
-        if (nw > 1) {
+        if (nw > 1) {  // lanes 0 .. nw-1 (a power of two) combine by butterfly, lane 0's result broadcast
             bv = lane < nw ? cand_v[lane] : -1.0;
             p = lane < nw ? cand_r[lane] : INT_MAX;
-            warp_argmax_index(bv, p);
+            for (int o = 1; o < nw; o <<= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int op = __shfl_xor_sync(0xffffffffu, p, o);
+                if (ov > bv || (ov == bv && op < p)) {
+                    bv = ov;
+                    p = op;
+                }
+            }
+            bv = __shfl_sync(0xffffffffu, bv, 0);
+            p = __shfl_sync(0xffffffffu, p, 0);
         }
         if (!(bv > 0.0)) return k + 1;  // exactly zero (or NaN) pivot column
         const double piv = a[(size_t)p * lda + k];
