@@ -1617,6 +1617,10 @@ extern "C" int rbffd_weights_compute(rbffd_grid* g, const rbffd_weight_params* p
                          MAX_CLASSES);
     int smem_max = max_smem_optin(ctx);
     for (auto& kv : buckets)
+        if (kv.first > MAX_M)
+            return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "system size %d (stencil + polynomial terms) exceeds %d",
+                             kv.first, MAX_M);
+    for (auto& kv : buckets)
         if (class_stride_bytes(kv.first, K, g->n_pad) > (size_t)smem_max)
             return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "system size %d with %d operators exceeds shared memory", kv.first, K);
     cudaSetDevice(ctx->device);
