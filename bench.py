@@ -806,7 +806,8 @@ def bench_cosine_bell(R, torch, ctx):
     order).  At the configuration's eps = 0.035 sqrt(N) the operator has
     growing modes on these nodes (reported over a short horizon); a full
     revolution uses eps = 6, with the degree-2 basis and with the reference's
-    own basis {1} (np = 1, m = 32)."""
+    own basis {1} (np = 1, m = 32).  The same runs again through the
+    cluster-resident path (every step in one thread-block-cluster launch)."""
     import oracle as O
     C = COSINE_BELL
     N, n = C["N"], C["n"]
@@ -834,20 +835,27 @@ def bench_cosine_bell(R, torch, ctx):
         for t, w in W.items():
             der.setWeights(t, w)
         res = {"eps": eps, "steps": steps, "poly_deg": deg, "system_size_m": n + O.lib().orc_poly_size(deg)}
-        for dname, dtype in (("fp64", R.F64), ("fp32", R.F32)):
+        for dname, dtype, resident in (("fp64", R.F64, False), ("fp32", R.F32, False),
+                                       ("fp64_resident", R.F64, True), ("fp32_resident", R.F32, True)):
             pde = R.CosineBell(grid, der, a, alpha, T, True, dtype=dtype)
-            pde.setShape(1, 256)
+            how = dict(resident=True) if resident else dict(graph=True)
+            if not resident:
+                pde.setShape(1, 256)
             pde.fillInitialConditions(h0)
-            pde.advance(R.RK4, dt, 10, graph=True)  # warm-up (graph instantiation)
+            pde.advance(R.RK4, dt, 10, **how)  # warm-up (graph instantiation / resident halo)
             pde.fillInitialConditions(h0)
             ctx.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
+            pde.advance(R.RK4, dt, steps, asynchronous=True, **how)
             e1.record(stream)
             ctx.synchronize()
             res[dname] = {"h": pde.getLocalSolution(), "node_updates_per_s": N * steps / (e0.elapsed_time(e1) * 1e-3)}
             pde.close()
+        # all steps in one cluster launch: the one-lane kernels' arithmetic, so the same bits
+        for dname in ("fp64", "fp32"):
+            hr = res[dname + "_resident"].pop("h")
+            res[dname + "_resident"]["equals_one_lane_graphed_bitwise"] = bool(np.array_equal(hr, res[dname]["h"]))
         t = time.perf_counter()
         h_or = O.rk4_advect(st, None, W[R.LAMBDA], W[R.THETA], W[R.HV], cu, cv, h0, dt, steps, nthreads=1)
         cpu_s = time.perf_counter() - t

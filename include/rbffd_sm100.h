@@ -382,7 +382,17 @@ enum rbffd_advance_flags {
                                     launches and a host synchronisation after every step,
                                     the structure of TimeDependentPDE_CL::advanceRK4
                                     (time_dependent_pde_cl.cpp:496-537) */
-    RBFFD_ADVANCE_ASYNC = 0x4    /* return without waiting for the device */
+    RBFFD_ADVANCE_ASYNC = 0x4,   /* return without waiting for the device */
+    RBFFD_ADVANCE_RESIDENT = 0x8 /* one tracer, small grids: all steps in one launch of a 16-CTA
+                                    thread-block cluster that keeps the weights, stencils and
+                                    state in its shared memory (each CTA copies its halo of
+                                    the stage input from the other CTAs through distributed
+                                    shared memory, then gathers locally; a cluster barrier
+                                    per stage);
+                                    the one-lane-per-row kernels' arithmetic, fused or unfused
+                                    per the PDE's arithmetic.  RBFFD_ERR_UNSUPPORTED when the
+                                    grid's weights do not fit 16 CTAs' shared memory (about
+                                    N x n x operators x 8 bytes <= 3.3 MB in FP64) */
 };
 /* nsteps classical RK4 steps of size dt: TimeDependentPDE::advance(RK4, dt)
  * (src/pdes/time_dependent_pde.cpp:53-73,172-304), nsteps times.

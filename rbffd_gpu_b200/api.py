@@ -23,7 +23,7 @@ LSFC, XSFC, YSFC, ZSFC, INTERP = 0x100, 0x200, 0x400, 0x800, 0x8000
 ALT_XSFC, ALT_YSFC, ALT_ZSFC = 0x1000, 0x2000, 0x4000
 EULER, MIDPOINT, RK4 = 0, 1, 2  # TimeDependentPDE::TimeScheme (time_dependent_pde.h:20)
 
-ADVANCE_GRAPH, ADVANCE_UNFUSED, ADVANCE_ASYNC = 0x1, 0x2, 0x4
+ADVANCE_GRAPH, ADVANCE_UNFUSED, ADVANCE_ASYNC, ADVANCE_RESIDENT = 0x1, 0x2, 0x4, 0x8
 RHS_COSINE_BELL, RHS_HEAT, RHS_ADVECTION = 1, 2, 3
 
 
@@ -600,9 +600,13 @@ class TimeDependentPDE:
         """PDE::checkGlobalError (pde.h:130-147): on one rank, checkLocalError."""
         return self.checkLocalError(exact, rel_err_max)
 
-    def advance(self, which=RK4, delta_t=1.0, nsteps=1, graph=False, unfused=False, asynchronous=False):
+    def advance(self, which=RK4, delta_t=1.0, nsteps=1, graph=False, unfused=False, asynchronous=False,
+                resident=False):
+        """nsteps RK4 steps (rbffd_pde_advance); resident: all steps in one
+        launch of a thread-block cluster holding the operator and state in its
+        shared memory (one tracer, small grids)."""
         flags = (ADVANCE_GRAPH if graph else 0) | (ADVANCE_UNFUSED if unfused else 0) | (
-            ADVANCE_ASYNC if asynchronous else 0)
+            ADVANCE_ASYNC if asynchronous else 0) | (ADVANCE_RESIDENT if resident else 0)
         self.ctx.check(self.ctx.L.rbffd_pde_advance(self.h, which, delta_t, nsteps, flags), "rbffd_pde_advance")
 
     def checkLocalError(self, exact, rel_err_max=-1.0):

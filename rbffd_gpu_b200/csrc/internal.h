@@ -85,6 +85,12 @@ struct rbffd_grid {
     std::vector<int> h_iperm;      // caller's node index -> internal row
     std::vector<int> h_len;        // stencil lengths, internal order
     std::map<int, struct Halo*> halos;  // per rows-per-block R, built on first use
+    // Halo of the cluster-resident RK4 layout (res_C CTAs of res_R rows; rk4.cu):
+    // per CTA res_H positions, each the owning CTA << 10 | local row of a node its
+    // rows read, and each stencil slot's position.  Built on first use.
+    int res_R = 0, res_C = 0, res_H = 0;
+    unsigned short* d_res_nodes = nullptr;  // [res_C][res_H]
+    unsigned short* d_res_lidx = nullptr;   // [res_C][n4][res_R]
     struct WeightsWork* ww = nullptr;   // the weight solver's device workspace and captured launch (weights.cu)
     size_t bytes = 0;
 };

@@ -20,6 +20,7 @@
 // FP64 arithmetic uses explicit round-to-nearest intrinsics so the order of
 // operations is fixed: with one lane per row the result equals a CPU loop
 // that fuses the same multiply-adds.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -126,6 +127,148 @@ __global__ void __launch_bounds__(512) k_stage_scalar(StageParams<T> p)
         cv = p.cv[i];
     }
     stage_update<T, KIND, HV, PLAIN>(p, i, (size_t)i, d0, d1, d2, cu, cv);
+}
+
+// ---------------------------------------------------------------------------
+// Cluster-resident RK4: every step of an advance in one launch of one
+// thread-block cluster of C CTAs.  CTA q holds rows q R .. q R + R-1 (one
+// thread per row): the rows' weights of every operator, their stencils as
+// positions in the CTA's halo (the unique nodes its rows read, each named by
+// its owning CTA and local row, 4 + 10 bits) in shared memory for the whole
+// launch, and its rows of u, the two stage inputs and the accumulator.  A
+// stage first copies the halo's values of the stage input from the owning
+// CTAs' shared memory (distributed shared memory: one load per halo node,
+// all in flight together), then every row sums its slots in stencil order
+// from the local copy and applies stage_update, the per-stage kernels'
+// arithmetic, so the result is k_stage_scalar's with one lane per row bit for
+// bit; a cluster barrier separates the stages.  u is read at the start and
+// written back at the end.
+constexpr int RES_MAX_CLUSTER = 16;
+
+template <typename T>
+struct ResidentParams {
+    const unsigned short* hnodes;  // [C][H]: halo node of each position, owner << 10 | local row
+    const unsigned short* lidx;    // [C][n4][R]: halo position of each stencil slot
+    const T* w[3];                 // the operators streamed (sliced ELL)
+    const T* cu;
+    const T* cv;
+    T* u;                          // state, internal order
+    T c[4];                        // dt/2, dt/2, dt, dt/6 (rounded to T as the per-stage launches do)
+    T kappa;
+    int N, nc, R, K, H, nsteps;
+};
+
+template <typename T, int KIND, bool HV, bool PLAIN>
+__global__ void __launch_bounds__(1024) k_rk4_cluster(ResidentParams<T> rp)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int R = rp.R, n4 = 4 * rp.nc, K = rp.K, H = rp.H;
+    T* ws = reinterpret_cast<T*>(smem_raw);  // [K][n4][R]
+    T* xs = ws + (size_t)K * n4 * R;           // u, xa, xb, acc, cu, cv: [6][R]
+    T* us = xs;
+    T* xa = xs + R;
+    T* xb = xs + 2 * R;
+    T* acc = xs + 3 * R;
+    T* cus = xs + 4 * R;
+    T* cvs = xs + 5 * R;
+    T* hx = xs + 6 * R;                                                    // [H] halo values of the stage input
+    unsigned short* hn = reinterpret_cast<unsigned short*>(hx + H);        // [H]
+    unsigned short* lx = hn + H;                                           // [n4][R]
+    const int q = (int)cl.block_rank(), r = threadIdx.x;
+    const int i = q * R + r;
+    const bool active = i < rp.N;
+    for (int h = r; h < H; h += R) hn[h] = rp.hnodes[(size_t)q * H + h];
+    for (int sl = 0; sl < n4; sl++) {
+        const size_t o = active ? sell_elem(i, sl, rp.nc) : 0;
+        lx[(size_t)sl * R + r] = rp.lidx[((size_t)q * n4 + sl) * R + r];
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            if (k < K) ws[((size_t)k * n4 + sl) * R + r] = active ? rp.w[k][o] : T(0);
+    }
+    us[r] = active ? rp.u[i] : T(0);
+    xa[r] = xb[r] = acc[r] = T(0);
+    cus[r] = active && KIND == KIND_ADVECT ? rp.cu[i] : T(0);
+    cvs[r] = active && KIND == KIND_ADVECT ? rp.cv[i] : T(0);
+    cl.sync();
+    StageParams<T> p = {};
+    p.kappa = rp.kappa;
+    p.u = us;
+    p.acc = acc;
+    for (int step = 0; step < rp.nsteps; step++)
+        for (int stage = 0; stage < 4; stage++) {
+            T* src = stage == 0 ? us : (stage == 2 ? xb : xa);
+            p.xnext = stage == 0 ? xa : (stage == 1 ? xb : (stage == 2 ? xa : nullptr));
+            p.c = stage == 0 ? rp.c[0] : (stage == 1 ? rp.c[1] : (stage == 2 ? rp.c[2] : rp.c[3]));
+            p.stage = stage;
+            for (int h = r; h < H; h += R) {
+                const unsigned v = hn[h];
+                hx[h] = cl.map_shared_rank(src, (int)(v >> 10))[v & 1023u];
+            }
+            __syncthreads();
+            if (active) {
+                T d0 = T(0), d1 = T(0), d2 = T(0);
+                for (int c4 = 0; c4 < n4; c4 += 4) {
+                    T xj[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) xj[k] = hx[lx[(size_t)(c4 + k) * R + r]];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const size_t e = (size_t)(c4 + k) * R + r;
+                        d0 = madd<T, PLAIN>(ws[e], xj[k], d0);
+                        if (KIND == KIND_ADVECT) {
+                            d1 = madd<T, PLAIN>(ws[(size_t)n4 * R + e], xj[k], d1);
+                            if (HV) d2 = madd<T, PLAIN>(ws[(size_t)2 * n4 * R + e], xj[k], d2);
+                        }
+                    }
+                }
+                stage_update<T, KIND, HV, PLAIN>(p, i, (size_t)r, d0, d1, d2, cus[r], cvs[r]);
+            }
+            cl.sync();
+        }
+    if (active) rp.u[i] = us[r];
+}
+
+// Shared memory of k_rk4_cluster for R rows per CTA and H halo positions.
+template <typename T>
+static size_t resident_smem(int K, int n4, int R, int H)
+{
+    return ((size_t)K * n4 * R + 6 * (size_t)R + H) * sizeof(T) + ((size_t)n4 * R + H) * sizeof(unsigned short);
+}
+
+template <typename T, int KIND, bool HV, bool PLAIN>
+static int launch_resident_t(rbffd_pde* P, const ResidentParams<T>& rp, int C, size_t smem, cudaStream_t s,
+                             bool check_only)
+{
+    rbffd_ctx* ctx = P->ctx;
+    auto kern = k_rk4_cluster<T, KIND, HV, PLAIN>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "cluster-resident RK4: kernel attributes refused");
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C, 1, 1);
+    cfg.blockDim = dim3(rp.R, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) != cudaSuccess || nclusters < 1) {
+        cudaGetLastError();
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "cluster-resident RK4: a cluster of %d CTAs with %zu bytes "
+                         "of shared memory each does not fit", C, smem);
+    }
+    if (check_only) return RBFFD_OK;
+    RBFFD_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, kern, rp));
+    return RBFFD_OK;
 }
 
 // Multiple tracers: state [N][T_tr]; VEC consecutive tracers per lane, loaded
@@ -1561,6 +1704,126 @@ static void run_steps(rbffd_pde* P, double dt, int nsteps, Shape sh)
         for (int st = 0; st < 4; st++) launch_stage_any(P, st, dt, sh, P->ctx->stream);
 }
 
+// The cluster-resident layout's halos (C CTAs of R rows), built on the host
+// from the device's stencil array the first time the layout is used.
+static int resident_halo(rbffd_grid* g, int R, int C)
+{
+    if (g->res_R == R && g->res_C == C) return RBFFD_OK;
+    rbffd_ctx* ctx = g->ctx;
+    const int N = g->N, nc = g->nc, n4 = g->n4;
+    std::vector<int> idx((size_t)g->N32 * n4);
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    RBFFD_CUDA_TRY(ctx, cudaMemcpy(idx.data(), g->d_idx, idx.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<std::vector<int>> halo(C);
+    int H = 1;
+    for (int q = 0; q < C; q++) {
+        std::vector<int>& v = halo[q];
+        for (int i = q * R; i < std::min(N, q * R + R); i++)
+            for (int sl = 0; sl < n4; sl++) v.push_back(idx[sell_elem(i, sl, nc)]);
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        H = std::max(H, (int)v.size());
+    }
+    std::vector<unsigned short> nodes((size_t)C * H, 0), lidx((size_t)C * n4 * R, 0);
+    for (int q = 0; q < C; q++) {
+        const std::vector<int>& v = halo[q];
+        for (size_t h = 0; h < v.size(); h++) nodes[(size_t)q * H + h] = (unsigned short)(((v[h] / R) << 10) | (v[h] % R));
+        for (int i = q * R; i < std::min(N, q * R + R); i++)
+            for (int sl = 0; sl < n4; sl++) {
+                const int j = idx[sell_elem(i, sl, nc)];
+                lidx[((size_t)q * n4 + sl) * R + (i - q * R)] =
+                    (unsigned short)(std::lower_bound(v.begin(), v.end(), j) - v.begin());
+            }
+    }
+    dev_free(ctx, g->d_res_nodes, (size_t)g->res_C * g->res_H * sizeof(unsigned short));
+    dev_free(ctx, g->d_res_lidx, (size_t)g->res_C * n4 * g->res_R * sizeof(unsigned short));
+    g->d_res_nodes = g->d_res_lidx = nullptr;
+    g->res_R = g->res_C = g->res_H = 0;
+    int rc = dev_alloc(ctx, (void**)&g->d_res_nodes, nodes.size() * sizeof(unsigned short));
+    if (!rc) rc = dev_alloc(ctx, (void**)&g->d_res_lidx, lidx.size() * sizeof(unsigned short));
+    if (rc) {
+        dev_free(ctx, g->d_res_nodes, nodes.size() * sizeof(unsigned short));
+        g->d_res_nodes = nullptr;
+        return rc;
+    }
+    RBFFD_CUDA_TRY(ctx, cudaMemcpy(g->d_res_nodes, nodes.data(), nodes.size() * sizeof(unsigned short),
+                                   cudaMemcpyHostToDevice));
+    RBFFD_CUDA_TRY(ctx, cudaMemcpy(g->d_res_lidx, lidx.data(), lidx.size() * sizeof(unsigned short),
+                                   cudaMemcpyHostToDevice));
+    g->res_R = R;
+    g->res_C = C;
+    g->res_H = H;
+    return RBFFD_OK;
+}
+
+// nsteps RK4 steps in one cluster-resident launch (k_rk4_cluster), one
+// tracer; check_only: report whether the PDE fits without launching.
+template <typename T>
+static int advance_resident_t(rbffd_pde* P, double dt, int nsteps, cudaStream_t s, bool check_only)
+{
+    rbffd_ctx* ctx = P->ctx;
+    rbffd_grid* g = P->g;
+    const bool heat = P->kind == KIND_HEAT || P->fused;
+    const int K = heat ? 1 : (P->use_hv ? 3 : 2);
+    const int C = std::min(RES_MAX_CLUSTER, (g->N + 31) / 32), n4 = 4 * g->nc;
+    const int R = ((g->N + C - 1) / C + 31) / 32 * 32;
+    if (R > 1024)
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "cluster-resident RK4: %d nodes exceed %d CTAs of 1024 rows",
+                         g->N, C);
+    int rc = resident_halo(g, R, C);
+    if (rc) return rc;
+    const size_t smem = resident_smem<T>(K, n4, R, g->res_H);
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+    if (smem > (size_t)optin)
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED,
+                         "cluster-resident RK4: %zu bytes of weights, halo and state per CTA exceed shared memory",
+                         smem);
+    ResidentParams<T> rp;
+    for (int k = 0; k < 3; k++)
+        rp.w[k] = k < K ? (P->fused ? (const T*)P->wf
+                                    : (std::is_same<T, double>::value ? (const T*)g->d_w64[P->op[k]]
+                                                                      : (const T*)g->d_w32[P->op[k]]))
+                        : nullptr;
+    rp.cu = (const T*)P->cu;
+    rp.cv = (const T*)P->cv;
+    rp.u = (T*)P->u;
+    static const double cfac[4] = {0.5, 0.5, 1.0, 0.0};
+    for (int st = 0; st < 4; st++) rp.c[st] = (T)(st == 3 ? dt / 6. : cfac[st] * dt);
+    rp.kappa = P->fused ? T(1) : (T)P->kappa;
+    rp.N = g->N;
+    rp.nc = g->nc;
+    rp.R = R;
+    rp.K = K;
+    rp.H = g->res_H;
+    rp.hnodes = g->d_res_nodes;
+    rp.lidx = g->d_res_lidx;
+    rp.nsteps = nsteps;
+    const bool plain = P->arith == RBFFD_ARITH_UNFUSED;
+    if (heat)
+        return plain ? launch_resident_t<T, KIND_HEAT, false, true>(P, rp, C, smem, s, check_only)
+                     : launch_resident_t<T, KIND_HEAT, false, false>(P, rp, C, smem, s, check_only);
+    if (P->use_hv)
+        return plain ? launch_resident_t<T, KIND_ADVECT, true, true>(P, rp, C, smem, s, check_only)
+                     : launch_resident_t<T, KIND_ADVECT, true, false>(P, rp, C, smem, s, check_only);
+    return plain ? launch_resident_t<T, KIND_ADVECT, false, true>(P, rp, C, smem, s, check_only)
+                 : launch_resident_t<T, KIND_ADVECT, false, false>(P, rp, C, smem, s, check_only);
+}
+
+static int advance_resident(rbffd_pde* P, double dt, int nsteps, int flags)
+{
+    rbffd_ctx* ctx = P->ctx;
+    if (P->T != 1) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "cluster-resident RK4 serves one tracer");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int rc = P->dtype == RBFFD_F64 ? advance_resident_t<double>(P, dt, nsteps, s, false)
+                                         : advance_resident_t<float>(P, dt, nsteps, s, false);
+    if (rc) return rc;
+    P->t += dt * nsteps;
+    if (!(flags & RBFFD_ADVANCE_ASYNC)) RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    return RBFFD_OK;
+}
+
 extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps, int flags)
 {
     if (!P) return RBFFD_ERR_INVALID;
@@ -1568,6 +1831,7 @@ extern "C" int rbffd_pde_advance(rbffd_pde* P, int scheme, double dt, int nsteps
     if (scheme != 2) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "time scheme %d (only RK4 = 2)", scheme);
     if (nsteps < 0) return set_error(ctx, RBFFD_ERR_INVALID, "nsteps < 0");
     if (nsteps == 0) return RBFFD_OK;
+    if (flags & RBFFD_ADVANCE_RESIDENT) return advance_resident(P, dt, nsteps, flags);
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
     if (flags & RBFFD_ADVANCE_UNFUSED) {
