@@ -439,11 +439,12 @@ int rbffd_pde_get_shape(rbffd_pde* pde, int* lanes_per_row, int* block_threads);
  *     streamed into shared memory by asynchronous bulk copies (TMA), several
  *     stages ahead; its waits are bounded and a timeout is reported by
  *     rbffd_pde_advance as RBFFD_ERR_TIMEOUT;
- *   RBFFD_TILE_SLOT_SCHEDULE: FP32 PDEs that stream one operator (heat, or a
- *     fused advection operator) with 4, 8 or 16 tracers: each row reads its
- *     slots in an order chosen so that the rows sharing a shared-memory
- *     wavefront read different bank groups (fewer bank conflicts).  Changes
- *     each row's FP32 summation order;
+ *   RBFFD_TILE_SLOT_SCHEDULE: FP32 PDEs with 4, 8 or 16 tracers (heat, a
+ *     fused advection operator, or the two or three advection operators,
+ *     each kept in the same order): each row reads its slots in an order
+ *     chosen so that the rows sharing a shared-memory wavefront read
+ *     different bank groups (fewer bank conflicts).  Changes each row's FP32
+ *     summation order;
  *   RBFFD_TILE_PREFETCH: the block's lanes ask L2 for the weights and indices
  *     of chunks a few steps ahead (pays where the weight stream comes from
  *     HBM); the arithmetic is unchanged;

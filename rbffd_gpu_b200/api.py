@@ -668,7 +668,8 @@ class TimeDependentPDE:
                       pipeline=False, double_buffer=False):
         """Tiled stage kernel of rows_per_block rows; stream_weights: bulk-copy
         weight streaming; slot_schedule: FP32 rows read their slots in the
-        halo's conflict-avoiding order (one operator, 4/8/16 tracers);
+        halo's conflict-avoiding order (4/8/16 tracers; every streamed
+        operator in that order);
         prefetch: upcoming chunks of weights and indices asked of L2;
         pipeline: one operator streamed, the next chunks' weights and indices
         kept in flight in registers (combines with slot_schedule);

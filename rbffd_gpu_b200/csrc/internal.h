@@ -162,13 +162,13 @@ struct rbffd_pde {
     // stages stream one weight array instead of three
     void* wf = nullptr;  // in the PDE's dtype
     bool fused = false;
-    // The one FP32 operator the stages stream (wf, or the grid's FP32 copy)
-    // in the slot schedule of halo ws_R for ws_P rows per wavefront; remade
-    // when its source changes (ws_src, ws_ver)
-    float* ws = nullptr;
+    // The FP32 operators the stages stream (wf, or the grid's FP32 copies of
+    // the one to three operators) in the slot schedule of halo ws_R for ws_P
+    // rows per wavefront; each remade when its source changes (ws_src, ws_ver)
+    float* ws[3] = {nullptr, nullptr, nullptr};
     int ws_R = 0, ws_P = 0;
-    const void* ws_src = nullptr;
-    unsigned ws_ver = 0;
+    const void* ws_src[3] = {nullptr, nullptr, nullptr};
+    unsigned ws_ver[3] = {0, 0, 0};
     void *d[3] = {nullptr, nullptr, nullptr};  // unfused path: one output per operator
     double* stage64 = nullptr;                  // FP64 staging for host state copies of an FP32 PDE
     double kappa = 1.0;

@@ -818,43 +818,53 @@ struct TileGeom {
 
 // Rows per 16-byte-load wavefront of the FP32 tiled kernel with one lane group
 // per row: 128 bytes / (T * 4)-byte node records (8, 4 or 2 for T = 4, 8, 16),
-// or 0 where a slot schedule does not apply (one operator streamed, FP32,
-// four values per vector).
+// or 0 where a slot schedule does not apply (FP32, four values per vector).
 static int sched_rows(const rbffd_pde* P)
 {
-    if (P->dtype != RBFFD_F32 || !(P->kind == KIND_HEAT || P->fused)) return 0;
+    if (P->dtype != RBFFD_F32) return 0;
     return P->T == 4 ? 8 : (P->T == 8 ? 4 : (P->T == 16 ? 2 : 0));
+}
+
+// Operators a stage streams: one for heat and the fused advection operator,
+// two or three (hyperviscosity) for advection.
+static int streamed_operators(const rbffd_pde* P)
+{
+    return (P->kind == KIND_HEAT || P->fused) ? 1 : (P->use_hv ? 3 : 2);
 }
 
 static int log2_rows(int Pw) { return Pw == 2 ? 1 : (Pw == 4 ? 2 : 3); }
 
-// The halo schedule of R rows per block and the PDE's operator in its slot
+// The halo schedule of R rows per block and the PDE's operators in its slot
 // order (P->ws), made or refreshed before launches that read them.
 static int pde_sched_prepare(rbffd_pde* P, int R)
 {
     rbffd_grid* g = P->g;
     rbffd_ctx* ctx = P->ctx;
     const int Pw = sched_rows(P);
-    if (!Pw) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a slot schedule needs FP32, one operator and 4, 8 or 16 tracers");
+    if (!Pw) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a slot schedule needs FP32 and 4, 8 or 16 tracers");
     const Halo* h = nullptr;
     int rc = grid_halo_schedule(g, R, Pw, &h);
     if (rc) return rc;
-    const float* src = P->fused ? (const float*)P->wf : g->d_w32[P->op[0]];
-    const unsigned ver = P->fused ? 0u : g->w32_ver[P->op[0]];
-    if (!src) return set_error(ctx, RBFFD_ERR_STATE, "no FP32 weights for the slot schedule");
-    if (!P->ws) {
-        const size_t bytes = (size_t)g->N32 * g->n4 * sizeof(float);
-        if ((rc = dev_alloc(ctx, (void**)&P->ws, bytes))) return rc;
-        P->bytes += bytes;
-        P->ws_src = nullptr;
+    const size_t bytes = (size_t)g->N32 * g->n4 * sizeof(float);
+    const int K = streamed_operators(P);
+    const bool fresh_layout = P->ws_R != R || P->ws_P != Pw;
+    for (int k = 0; k < K; k++) {
+        const float* src = P->fused ? (const float*)P->wf : g->d_w32[P->op[k]];
+        const unsigned ver = P->fused ? 0u : g->w32_ver[P->op[k]];
+        if (!src) return set_error(ctx, RBFFD_ERR_STATE, "no FP32 weights for the slot schedule");
+        if (!P->ws[k]) {
+            if ((rc = dev_alloc(ctx, (void**)&P->ws[k], bytes))) return rc;
+            P->bytes += bytes;
+            P->ws_src[k] = nullptr;
+        }
+        if (fresh_layout || P->ws_src[k] != src || P->ws_ver[k] != ver) {
+            if ((rc = grid_schedule_weights(g, src, h->d_slot_s[log2_rows(Pw)], P->ws[k], ctx->stream))) return rc;
+            P->ws_src[k] = src;
+            P->ws_ver[k] = ver;
+        }
     }
-    if (P->ws_R != R || P->ws_P != Pw || P->ws_src != src || P->ws_ver != ver) {
-        if ((rc = grid_schedule_weights(g, src, h->d_slot_s[log2_rows(Pw)], P->ws, ctx->stream))) return rc;
-        P->ws_R = R;
-        P->ws_P = Pw;
-        P->ws_src = src;
-        P->ws_ver = ver;
-    }
+    P->ws_R = R;
+    P->ws_P = Pw;
     return RBFFD_OK;
 }
 
@@ -883,9 +893,11 @@ static bool tile_geom(rbffd_pde* P, Shape sh, TileGeom* tg)
     t.smem = (size_t)t.h->max_halo * P->T * es;
     if (sh.sched) {  // prepared by pde_sched_prepare for this block size
         const int Pw = sched_rows(P);
-        if (!Pw || t.G != 1 || t.vec != 4 || sh.tma || !P->ws || P->ws_R != sh.tile || P->ws_P != Pw ||
+        if (!Pw || t.G != 1 || t.vec != 4 || sh.tma || P->ws_R != sh.tile || P->ws_P != Pw ||
             !t.h->d_lidx_s[log2_rows(Pw)])
             return false;
+        for (int k = 0; k < streamed_operators(P); k++)
+            if (!P->ws[k]) return false;
         t.sched = log2_rows(Pw);
     }
     if (sh.pf) {
@@ -1035,9 +1047,11 @@ static void launch_stage_t(rbffd_pde* P, const StageParams<T>& p, Shape sh, cuda
     if (tile_geom(P, sh, &tg)) {
         TileParams tp{tg.h->d_ptr, tg.h->d_nodes, tg.h->d_lidx, tg.h->d_rows, tg.h->R, P->g->N32};
         constexpr int VV = std::is_same<T, float>::value ? 4 : 2;
-        if (tg.sched >= 0) {  // slot-scheduled rows: local indices and the one operator in that order
+        if (tg.sched >= 0) {  // slot-scheduled rows: local indices and the operators in that order
             StageParams<T> ps = p;
-            ps.w0 = (const T*)P->ws;
+            ps.w0 = (const T*)P->ws[0];
+            ps.w1 = (const T*)P->ws[1];
+            ps.w2 = (const T*)P->ws[2];
             tp.lidx = tg.h->d_lidx_s[tg.sched];
             if (tg.pipe)
                 launch_pipe_v<T, VV>(ps, tp, tg, s);
@@ -1358,7 +1372,7 @@ static void pde_free(rbffd_pde* P)
     dev_free(ctx, P->cu, (size_t)P->g->N * es);
     dev_free(ctx, P->cv, (size_t)P->g->N * es);
     dev_free(ctx, P->wf, (size_t)P->g->N32 * P->g->n4 * (P->dtype == RBFFD_F64 ? sizeof(double) : sizeof(float)));
-    dev_free(ctx, P->ws, (size_t)P->g->N32 * P->g->n4 * sizeof(float));
+    for (int k = 0; k < 3; k++) dev_free(ctx, P->ws[k], (size_t)P->g->N32 * P->g->n4 * sizeof(float));
     delete P;
 }
 
@@ -1417,7 +1431,7 @@ extern "C" int rbffd_pde_set_fused_operator(rbffd_pde* P, int on)
             (float*)P->wf, g->d_w64[P->op[0]], g->d_w64[P->op[1]], wh, (const float*)P->cu, (const float*)P->cv,
             g->N, g->N32, g->nc);
     RBFFD_CUDA_TRY(ctx, cudaGetLastError());
-    P->ws_src = nullptr;  // a scheduled copy of the previous operator is stale
+    P->ws_src[0] = nullptr;  // a scheduled copy of the previous operator is stale
     if (P->gexec) {
         cudaGraphExecDestroy(P->gexec);
         P->gexec = nullptr;
