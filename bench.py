@@ -70,6 +70,9 @@ def parse():
     ap.add_argument("--profile-weights", default=None, metavar="N[,METHOD]",
                     help="batched weights (the 1e6-stencil mix at N stencils): a tuned call, then one more, for ncu; "
                          "METHOD: auto (default), unblocked, blocked, row_map, registers")
+    ap.add_argument("--profile-resident", default=None, choices=["f64", "f32"],
+                    help="the 4096-node cosine bell (n=31, hyperviscosity, eps=6) in one cluster-resident launch "
+                         "of 200 RK4 steps, after one warm-up launch, for ncu")
     return ap.parse_args()
 
 
@@ -1327,6 +1330,31 @@ def run_profile_heat_hbm():
     print("profile run done")
 
 
+def run_profile_resident(dtype):
+    import rbffd_gpu_b200 as R
+    C = COSINE_BELL
+    N, n = C["N"], C["n"]
+    xyz = R.fibonacci_nodes(N, C["seed"])
+    st = R.knn_stencils(xyz, n)
+    types = R.LAMBDA | R.THETA | R.HV
+    ctx = R.Context(0)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(types, grid, 2)
+    der.setEpsilon(C["eps_stable"])
+    der.setPolynomialDegree(C["deg"])
+    der.setHVScalars(C["hv_k"], C["gamma"])
+    der.computeAllWeightsForAllStencils()
+    pde = R.CosineBell(grid, der, 1.0, np.pi / 2, C["T"], True, dtype=R.F64 if dtype == "f64" else R.F32)
+    pde.fillInitialConditions(R.exact_cosine_bell(xyz))
+    dt = C["T"] / C["steps"]
+    pde.advance(R.RK4, dt, 10, resident=True)   # warm-up: the halo is built, the module loaded
+    pde.advance(R.RK4, dt, 200, resident=True)  # the captured launch
+    print("profile run done")
+    pde.close()
+    grid.close()
+    ctx.close()
+
+
 def run_profile_weights(spec):
     """The batched-weights mix (n over {17, 31, 50, 101} with degrees 1-4,
     eps ~ U[2, 8], XSFC/YSFC/ZSFC) on N stencils: the tuned call, then one
@@ -1393,6 +1421,8 @@ def main():
         run_profile_serving(args.profile_serving)
     elif args.profile_weights:
         run_profile_weights(args.profile_weights)
+    elif args.profile_resident:
+        run_profile_resident(args.profile_resident)
     elif args.profile_heat_hbm:
         run_profile_heat_hbm()
     elif args.profile_multitracer:

@@ -323,8 +323,7 @@ extern "C" int rbffd_grid_destroy(rbffd_grid* g)
     dev_free(ctx, g->d_len, (size_t)g->N * sizeof(int));
     dev_free(ctx, g->d_perm, (size_t)g->N * sizeof(int));
     dev_free(ctx, g->d_xyz, (size_t)g->N * sizeof(double4));
-    dev_free(ctx, g->d_res_nodes, (size_t)g->res_C * g->res_H * sizeof(unsigned short));
-    dev_free(ctx, g->d_res_lidx, (size_t)g->res_C * g->n4 * g->res_R * sizeof(unsigned short));
+    resident_free(g);
     for (auto& kv : g->halos) {
         Halo* h = kv.second;
         dev_free(ctx, h->d_ptr, (size_t)(h->nblocks + 1) * sizeof(int));

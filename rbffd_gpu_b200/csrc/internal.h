@@ -85,16 +85,19 @@ struct rbffd_grid {
     std::vector<int> h_iperm;      // caller's node index -> internal row
     std::vector<int> h_len;        // stencil lengths, internal order
     std::map<int, struct Halo*> halos;  // per rows-per-block R, built on first use
-    // Halo of the cluster-resident RK4 layout (res_C CTAs of res_R rows; rk4.cu):
-    // per CTA res_H positions, each the owning CTA << 10 | local row of a node its
-    // rows read, and each stencil slot's position.  Built on first use.
-    int res_R = 0, res_C = 0, res_H = 0;
-    unsigned short* d_res_nodes = nullptr;  // [res_C][res_H]
+    // The cluster-resident RK4 layout (res_C CTAs of res_R rows; rk4.cu): per
+    // CTA a halo of at most res_H nodes, each stencil slot's halo position, and
+    // each row's push list (consumer CTA << 12 | halo position).  Built on first use.
+    int res_R = 0, res_C = 0, res_H = 0, res_P = 0;
+    int* d_res_pptr = nullptr;              // [res_C][res_R + 1] push-list ranges
+    unsigned short* d_res_pdst = nullptr;   // [res_C][res_P]
     unsigned short* d_res_lidx = nullptr;   // [res_C][n4][res_R]
     struct WeightsWork* ww = nullptr;   // the weight solver's device workspace and captured launch (weights.cu)
     size_t bytes = 0;
 };
 void weights_work_free(rbffd_grid* g);
+// Free the cluster-resident layout of a grid (rk4.cu).
+void resident_free(rbffd_grid* g);
 
 // Move [N][T] values (elem_bytes each) between the caller's node order and the
 // grid's internal order (device arrays, on stream s).

@@ -133,21 +133,23 @@ __global__ void __launch_bounds__(512) k_stage_scalar(StageParams<T> p)
 // Cluster-resident RK4: every step of an advance in one launch of one
 // thread-block cluster of C CTAs.  CTA q holds rows q R .. q R + R-1 (one
 // thread per row): the rows' weights of every operator, their stencils as
-// positions in the CTA's halo (the unique nodes its rows read, each named by
-// its owning CTA and local row, 4 + 10 bits) in shared memory for the whole
-// launch, and its rows of u, the two stage inputs and the accumulator.  A
-// stage first copies the halo's values of the stage input from the owning
-// CTAs' shared memory (distributed shared memory: one load per halo node,
-// all in flight together), then every row sums its slots in stencil order
-// from the local copy and applies stage_update, the per-stage kernels'
-// arithmetic, so the result is k_stage_scalar's with one lane per row bit for
-// bit; a cluster barrier separates the stages.  u is read at the start and
-// written back at the end.
+// positions in the CTA's halo (the unique nodes its rows read, each held by
+// its owning CTA and local row) in shared memory for the whole launch, and
+// its rows of u, the two stage inputs and the accumulator.  Every row sums
+// its slots in stencil order from the CTA's halo buffer and applies
+// stage_update, the per-stage kernels' arithmetic, so the result is
+// k_stage_scalar's with one lane per row bit for bit; it then stores its new
+// value straight into the other halo buffer of every CTA whose halo holds the
+// row (distributed shared memory; a host-built push list per row), and one
+// cluster barrier (release / acquire) separates the stages: stage s reads
+// halo buffer s mod 2 and fills buffer s + 1 mod 2.  u is read at the start
+// and written back at the end.
 constexpr int RES_MAX_CLUSTER = 16;
 
 template <typename T>
 struct ResidentParams {
-    const unsigned short* hnodes;  // [C][H]: halo node of each position, owner << 10 | local row
+    const int* pptr;               // [C][R + 1]: each row's range in pdst
+    const unsigned short* pdst;    // [C][P]: halo positions a row's value goes to, consumer CTA << 12 | position
     const unsigned short* lidx;    // [C][n4][R]: halo position of each stencil slot
     const T* w[3];                 // the operators streamed (sliced ELL)
     const T* cu;
@@ -155,16 +157,24 @@ struct ResidentParams {
     T* u;                          // state, internal order
     T c[4];                        // dt/2, dt/2, dt, dt/6 (rounded to T as the per-stage launches do)
     T kappa;
-    int N, nc, R, K, H, nsteps;
+    int N, nc, R, K, H, P, nsteps;
 };
 
-template <typename T, int KIND, bool HV, bool PLAIN>
-__global__ void __launch_bounds__(1024) k_rk4_cluster(ResidentParams<T> rp)
+// Body of the cluster-resident kernels.  NCR = 0: each row's weights and halo
+// positions in shared memory (any stencil size); NCR > 0: stencils of exactly
+// NCR 4-slot chunks with the row's weights and halo positions in registers for
+// the whole launch (at most 256 rows per CTA), so a slot costs one
+// shared-memory load (the halo value) instead of up to four.
+template <typename T, int KIND, bool HV, bool PLAIN, int NCR>
+__device__ __forceinline__ void rk4_cluster_body(const ResidentParams<T>& rp)
 {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int R = rp.R, n4 = 4 * rp.nc, K = rp.K, H = rp.H;
+    constexpr int KC = KIND == KIND_HEAT ? 1 : (HV ? 3 : 2);
+    constexpr int N4R = 4 * NCR;
+    const int R = rp.R, n4 = NCR > 0 ? N4R : 4 * rp.nc, H = rp.H, P = rp.P;
+    const int K = NCR > 0 ? 0 : rp.K;          // operators kept in shared memory
     T* ws = reinterpret_cast<T*>(smem_raw);  // [K][n4][R]
     T* xs = ws + (size_t)K * n4 * R;           // u, xa, xb, acc, cu, cv: [6][R]
     T* us = xs;
@@ -173,24 +183,51 @@ __global__ void __launch_bounds__(1024) k_rk4_cluster(ResidentParams<T> rp)
     T* acc = xs + 3 * R;
     T* cus = xs + 4 * R;
     T* cvs = xs + 5 * R;
-    T* hx = xs + 6 * R;                                                    // [H] halo values of the stage input
-    unsigned short* hn = reinterpret_cast<unsigned short*>(hx + H);        // [H]
-    unsigned short* lx = hn + H;                                           // [n4][R]
+    T* hb0 = xs + 6 * R;                                                  // [2][H] halo buffers
+    T* hb1 = hb0 + H;
+    unsigned short* pd = reinterpret_cast<unsigned short*>(hb1 + H);     // [P] this CTA's push list
+    unsigned short* lx = pd + P;                                          // [n4][R] (NCR = 0)
     const int q = (int)cl.block_rank(), r = threadIdx.x;
     const int i = q * R + r;
     const bool active = i < rp.N;
-    for (int h = r; h < H; h += R) hn[h] = rp.hnodes[(size_t)q * H + h];
-    for (int sl = 0; sl < n4; sl++) {
-        const size_t o = active ? sell_elem(i, sl, rp.nc) : 0;
-        lx[(size_t)sl * R + r] = rp.lidx[((size_t)q * n4 + sl) * R + r];
+    T wr[NCR > 0 ? KC : 1][NCR > 0 ? N4R : 1];
+    unsigned lr[NCR > 0 ? N4R / 2 : 1];  // two 16-bit halo positions per register
+    for (int e = r; e < P; e += R) pd[e] = rp.pdst[(size_t)q * P + e];
+    const int pb = rp.pptr[(size_t)q * (R + 1) + r], pe = rp.pptr[(size_t)q * (R + 1) + r + 1];
+    if constexpr (NCR > 0) {
 #pragma unroll
-        for (int k = 0; k < 3; k++)
-            if (k < K) ws[((size_t)k * n4 + sl) * R + r] = active ? rp.w[k][o] : T(0);
+        for (int sl = 0; sl < N4R; sl++) {
+            const size_t o = active ? sell_elem(i, sl, NCR) : 0;
+            const unsigned v = rp.lidx[((size_t)q * N4R + sl) * R + r];
+            if (sl % 2 == 0)
+                lr[sl / 2] = v;
+            else
+                lr[sl / 2] |= v << 16;
+#pragma unroll
+            for (int k = 0; k < KC; k++) wr[k][sl] = active ? rp.w[k][o] : T(0);
+        }
+    } else {
+        for (int sl = 0; sl < n4; sl++) {
+            const size_t o = active ? sell_elem(i, sl, rp.nc) : 0;
+            lx[(size_t)sl * R + r] = rp.lidx[((size_t)q * n4 + sl) * R + r];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                if (k < K) ws[((size_t)k * n4 + sl) * R + r] = active ? rp.w[k][o] : T(0);
+        }
     }
-    us[r] = active ? rp.u[i] : T(0);
+    const T u0 = active ? rp.u[i] : T(0);
+    us[r] = u0;
     xa[r] = xb[r] = acc[r] = T(0);
     cus[r] = active && KIND == KIND_ADVECT ? rp.cu[i] : T(0);
     cvs[r] = active && KIND == KIND_ADVECT ? rp.cv[i] : T(0);
+    cl.sync();  // every CTA of the cluster runs: its shared memory may be written
+    auto push = [&](T* buf, T value) {
+        for (int e = pb; e < pe; e++) {
+            const unsigned v = pd[e];
+            cl.map_shared_rank(buf, (int)(v >> 12))[v & 4095u] = value;
+        }
+    };
+    push(hb0, u0);
     cl.sync();
     StageParams<T> p = {};
     p.kappa = rp.kappa;
@@ -198,51 +235,100 @@ __global__ void __launch_bounds__(1024) k_rk4_cluster(ResidentParams<T> rp)
     p.acc = acc;
     for (int step = 0; step < rp.nsteps; step++)
         for (int stage = 0; stage < 4; stage++) {
-            T* src = stage == 0 ? us : (stage == 2 ? xb : xa);
+            const T* hin = (stage & 1) ? hb1 : hb0;
             p.xnext = stage == 0 ? xa : (stage == 1 ? xb : (stage == 2 ? xa : nullptr));
             p.c = stage == 0 ? rp.c[0] : (stage == 1 ? rp.c[1] : (stage == 2 ? rp.c[2] : rp.c[3]));
             p.stage = stage;
-            for (int h = r; h < H; h += R) {
-                const unsigned v = hn[h];
-                hx[h] = cl.map_shared_rank(src, (int)(v >> 10))[v & 1023u];
-            }
-            __syncthreads();
             if (active) {
                 T d0 = T(0), d1 = T(0), d2 = T(0);
-                for (int c4 = 0; c4 < n4; c4 += 4) {
-                    T xj[4];
+                if constexpr (NCR > 0) {
 #pragma unroll
-                    for (int k = 0; k < 4; k++) xj[k] = hx[lx[(size_t)(c4 + k) * R + r]];
+                    for (int c4 = 0; c4 < N4R; c4 += 4) {
+                        T xj[4];
 #pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        const size_t e = (size_t)(c4 + k) * R + r;
-                        d0 = madd<T, PLAIN>(ws[e], xj[k], d0);
-                        if (KIND == KIND_ADVECT) {
-                            d1 = madd<T, PLAIN>(ws[(size_t)n4 * R + e], xj[k], d1);
-                            if (HV) d2 = madd<T, PLAIN>(ws[(size_t)2 * n4 * R + e], xj[k], d2);
+                        for (int k = 0; k < 4; k++) xj[k] = hin[(lr[(c4 + k) / 2] >> (16 * ((c4 + k) % 2))) & 0xFFFFu];
+#pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            d0 = madd<T, PLAIN>(wr[0][c4 + k], xj[k], d0);
+                            if constexpr (KC > 1) d1 = madd<T, PLAIN>(wr[KC > 1 ? 1 : 0][c4 + k], xj[k], d1);
+                            if constexpr (KC > 2) d2 = madd<T, PLAIN>(wr[KC > 2 ? 2 : 0][c4 + k], xj[k], d2);
+                        }
+                    }
+                } else {
+                    for (int c4 = 0; c4 < n4; c4 += 4) {
+                        T xj[4];
+#pragma unroll
+                        for (int k = 0; k < 4; k++) xj[k] = hin[lx[(size_t)(c4 + k) * R + r]];
+#pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            const size_t e = (size_t)(c4 + k) * R + r;
+                            d0 = madd<T, PLAIN>(ws[e], xj[k], d0);
+                            if (KIND == KIND_ADVECT) {
+                                d1 = madd<T, PLAIN>(ws[(size_t)n4 * R + e], xj[k], d1);
+                                if (HV) d2 = madd<T, PLAIN>(ws[(size_t)2 * n4 * R + e], xj[k], d2);
+                            }
                         }
                     }
                 }
                 stage_update<T, KIND, HV, PLAIN>(p, i, (size_t)r, d0, d1, d2, cus[r], cvs[r]);
+                push((stage & 1) ? hb0 : hb1, stage == 3 ? us[r] : p.xnext[r]);  // the next stage's input
             }
             cl.sync();
         }
     if (active) rp.u[i] = us[r];
 }
 
-// Shared memory of k_rk4_cluster for R rows per CTA and H halo positions.
-template <typename T>
-static size_t resident_smem(int K, int n4, int R, int H)
+template <typename T, int KIND, bool HV, bool PLAIN>
+__global__ void __launch_bounds__(1024) k_rk4_cluster(ResidentParams<T> rp)
 {
-    return ((size_t)K * n4 * R + 6 * (size_t)R + H) * sizeof(T) + ((size_t)n4 * R + H) * sizeof(unsigned short);
+    rk4_cluster_body<T, KIND, HV, PLAIN, 0>(rp);
+}
+
+// Register-resident weights: one CTA of at most 256 threads per SM, up to 255 registers each.
+template <typename T, int KIND, bool HV, bool PLAIN, int NCR>
+__global__ void __launch_bounds__(256, 1) k_rk4_cluster_rw(ResidentParams<T> rp)
+{
+    rk4_cluster_body<T, KIND, HV, PLAIN, NCR>(rp);
+}
+
+// Stencil chunk counts with a register-resident variant, and the register
+// budget of a row's weights (32-bit registers).
+constexpr int RES_RW_NC0 = 8, RES_RW_NC1 = 13, RES_RW_MAX_REGS = 192;
+
+template <typename T, int KIND, bool HV>
+constexpr bool res_rw_fits(int ncr)
+{
+    return (KIND == KIND_HEAT ? 1 : (HV ? 3 : 2)) * 4 * ncr * (int)sizeof(T) / 4 <= RES_RW_MAX_REGS;
+}
+
+// The kernel for ncr chunks held in registers (0, or a combination over the
+// register budget: weights in shared memory).
+template <typename T, int KIND, bool HV, bool PLAIN, int NCR>
+static void (*res_kernel())(ResidentParams<T>)
+{
+    if constexpr (NCR > 0 && res_rw_fits<T, KIND, HV>(NCR))
+        return k_rk4_cluster_rw<T, KIND, HV, PLAIN, NCR>;
+    else
+        return k_rk4_cluster<T, KIND, HV, PLAIN>;
+}
+
+// Shared memory of k_rk4_cluster for R rows per CTA, H halo positions, P push
+// entries and K operators of n4 slots in shared memory.
+template <typename T>
+static size_t resident_smem(int K, int n4, int R, int H, int P)
+{
+    return ((size_t)K * n4 * R + 6 * (size_t)R + 2 * (size_t)H) * sizeof(T) +
+           ((size_t)(K ? n4 : 0) * R + P) * sizeof(unsigned short);
 }
 
 template <typename T, int KIND, bool HV, bool PLAIN>
 static int launch_resident_t(rbffd_pde* P, const ResidentParams<T>& rp, int C, size_t smem, cudaStream_t s,
-                             bool check_only)
+                             bool check_only, int ncr)
 {
     rbffd_ctx* ctx = P->ctx;
-    auto kern = k_rk4_cluster<T, KIND, HV, PLAIN>;
+    auto kern = ncr == RES_RW_NC0   ? res_kernel<T, KIND, HV, PLAIN, RES_RW_NC0>()
+                : ncr == RES_RW_NC1 ? res_kernel<T, KIND, HV, PLAIN, RES_RW_NC1>()
+                                    : res_kernel<T, KIND, HV, PLAIN, 0>();
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
@@ -1718,8 +1804,21 @@ static void run_steps(rbffd_pde* P, double dt, int nsteps, Shape sh)
         for (int st = 0; st < 4; st++) launch_stage_any(P, st, dt, sh, P->ctx->stream);
 }
 
-// The cluster-resident layout's halos (C CTAs of R rows), built on the host
-// from the device's stencil array the first time the layout is used.
+// The cluster-resident layout (C CTAs of R rows), built on the host from the
+// device's stencil array the first time it is used: each CTA's halo (the
+// sorted unique nodes its rows read), each stencil slot's halo position, and
+// each row's push list (the CTAs and halo positions its value goes to).
+void resident_free(rbffd_grid* g)
+{
+    rbffd_ctx* ctx = g->ctx;
+    dev_free(ctx, g->d_res_pptr, (size_t)g->res_C * (g->res_R + 1) * sizeof(int));
+    dev_free(ctx, g->d_res_pdst, (size_t)g->res_C * g->res_P * sizeof(unsigned short));
+    dev_free(ctx, g->d_res_lidx, (size_t)g->res_C * g->n4 * g->res_R * sizeof(unsigned short));
+    g->d_res_pptr = nullptr;
+    g->d_res_pdst = g->d_res_lidx = nullptr;
+    g->res_R = g->res_C = g->res_H = g->res_P = 0;
+}
+
 static int resident_halo(rbffd_grid* g, int R, int C)
 {
     if (g->res_R == R && g->res_C == C) return RBFFD_OK;
@@ -1738,10 +1837,12 @@ static int resident_halo(rbffd_grid* g, int R, int C)
         v.erase(std::unique(v.begin(), v.end()), v.end());
         H = std::max(H, (int)v.size());
     }
-    std::vector<unsigned short> nodes((size_t)C * H, 0), lidx((size_t)C * n4 * R, 0);
+    if (H > 4096) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "cluster-resident RK4: a CTA's halo exceeds 4096 nodes");
+    std::vector<unsigned short> lidx((size_t)C * n4 * R, 0);
+    std::vector<std::vector<unsigned short>> dst((size_t)C * R);  // push targets of each row
     for (int q = 0; q < C; q++) {
         const std::vector<int>& v = halo[q];
-        for (size_t h = 0; h < v.size(); h++) nodes[(size_t)q * H + h] = (unsigned short)(((v[h] / R) << 10) | (v[h] % R));
+        for (size_t h = 0; h < v.size(); h++) dst[v[h]].push_back((unsigned short)((q << 12) | (int)h));
         for (int i = q * R; i < std::min(N, q * R + R); i++)
             for (int sl = 0; sl < n4; sl++) {
                 const int j = idx[sell_elem(i, sl, nc)];
@@ -1749,24 +1850,42 @@ static int resident_halo(rbffd_grid* g, int R, int C)
                     (unsigned short)(std::lower_bound(v.begin(), v.end(), j) - v.begin());
             }
     }
-    dev_free(ctx, g->d_res_nodes, (size_t)g->res_C * g->res_H * sizeof(unsigned short));
-    dev_free(ctx, g->d_res_lidx, (size_t)g->res_C * n4 * g->res_R * sizeof(unsigned short));
-    g->d_res_nodes = g->d_res_lidx = nullptr;
-    g->res_R = g->res_C = g->res_H = 0;
-    int rc = dev_alloc(ctx, (void**)&g->d_res_nodes, nodes.size() * sizeof(unsigned short));
+    int Pm = 1;
+    for (int q = 0; q < C; q++) {
+        int cnt = 0;
+        for (int r = 0; r < R; r++) cnt += (int)dst[(size_t)q * R + r].size();
+        Pm = std::max(Pm, cnt);
+    }
+    std::vector<int> pptr((size_t)C * (R + 1), 0);
+    std::vector<unsigned short> pdst((size_t)C * Pm, 0);
+    for (int q = 0; q < C; q++) {
+        int e = 0;
+        for (int r = 0; r < R; r++) {
+            pptr[(size_t)q * (R + 1) + r] = e;
+            for (unsigned short d : dst[(size_t)q * R + r]) pdst[(size_t)q * Pm + e++] = d;
+        }
+        pptr[(size_t)q * (R + 1) + R] = e;
+    }
+    resident_free(g);
+    int rc = dev_alloc(ctx, (void**)&g->d_res_pptr, pptr.size() * sizeof(int));
+    if (!rc) rc = dev_alloc(ctx, (void**)&g->d_res_pdst, pdst.size() * sizeof(unsigned short));
     if (!rc) rc = dev_alloc(ctx, (void**)&g->d_res_lidx, lidx.size() * sizeof(unsigned short));
     if (rc) {
-        dev_free(ctx, g->d_res_nodes, nodes.size() * sizeof(unsigned short));
-        g->d_res_nodes = nullptr;
+        dev_free(ctx, g->d_res_pptr, pptr.size() * sizeof(int));
+        dev_free(ctx, g->d_res_pdst, pdst.size() * sizeof(unsigned short));
+        g->d_res_pptr = nullptr;
+        g->d_res_pdst = nullptr;
         return rc;
     }
-    RBFFD_CUDA_TRY(ctx, cudaMemcpy(g->d_res_nodes, nodes.data(), nodes.size() * sizeof(unsigned short),
+    RBFFD_CUDA_TRY(ctx, cudaMemcpy(g->d_res_pptr, pptr.data(), pptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+    RBFFD_CUDA_TRY(ctx, cudaMemcpy(g->d_res_pdst, pdst.data(), pdst.size() * sizeof(unsigned short),
                                    cudaMemcpyHostToDevice));
     RBFFD_CUDA_TRY(ctx, cudaMemcpy(g->d_res_lidx, lidx.data(), lidx.size() * sizeof(unsigned short),
                                    cudaMemcpyHostToDevice));
     g->res_R = R;
     g->res_C = C;
     g->res_H = H;
+    g->res_P = Pm;
     return RBFFD_OK;
 }
 
@@ -1786,7 +1905,13 @@ static int advance_resident_t(rbffd_pde* P, double dt, int nsteps, cudaStream_t 
                          g->N, C);
     int rc = resident_halo(g, R, C);
     if (rc) return rc;
-    const size_t smem = resident_smem<T>(K, n4, R, g->res_H);
+    // weights and halo positions in registers where the stencil size has a variant and the budget allows
+    const int ncr =
+        (R <= 256 && (g->nc == RES_RW_NC0 || g->nc == RES_RW_NC1) && K * n4 * (int)sizeof(T) / 4 <= RES_RW_MAX_REGS)
+            ? g->nc
+            : 0;
+    const size_t smem =
+        ncr ? resident_smem<T>(0, 0, R, g->res_H, g->res_P) : resident_smem<T>(K, n4, R, g->res_H, g->res_P);
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
     if (smem > (size_t)optin)
@@ -1810,18 +1935,20 @@ static int advance_resident_t(rbffd_pde* P, double dt, int nsteps, cudaStream_t 
     rp.R = R;
     rp.K = K;
     rp.H = g->res_H;
-    rp.hnodes = g->d_res_nodes;
+    rp.P = g->res_P;
+    rp.pptr = g->d_res_pptr;
+    rp.pdst = g->d_res_pdst;
     rp.lidx = g->d_res_lidx;
     rp.nsteps = nsteps;
     const bool plain = P->arith == RBFFD_ARITH_UNFUSED;
     if (heat)
-        return plain ? launch_resident_t<T, KIND_HEAT, false, true>(P, rp, C, smem, s, check_only)
-                     : launch_resident_t<T, KIND_HEAT, false, false>(P, rp, C, smem, s, check_only);
+        return plain ? launch_resident_t<T, KIND_HEAT, false, true>(P, rp, C, smem, s, check_only, ncr)
+                     : launch_resident_t<T, KIND_HEAT, false, false>(P, rp, C, smem, s, check_only, ncr);
     if (P->use_hv)
-        return plain ? launch_resident_t<T, KIND_ADVECT, true, true>(P, rp, C, smem, s, check_only)
-                     : launch_resident_t<T, KIND_ADVECT, true, false>(P, rp, C, smem, s, check_only);
-    return plain ? launch_resident_t<T, KIND_ADVECT, false, true>(P, rp, C, smem, s, check_only)
-                 : launch_resident_t<T, KIND_ADVECT, false, false>(P, rp, C, smem, s, check_only);
+        return plain ? launch_resident_t<T, KIND_ADVECT, true, true>(P, rp, C, smem, s, check_only, ncr)
+                     : launch_resident_t<T, KIND_ADVECT, true, false>(P, rp, C, smem, s, check_only, ncr);
+    return plain ? launch_resident_t<T, KIND_ADVECT, false, true>(P, rp, C, smem, s, check_only, ncr)
+                 : launch_resident_t<T, KIND_ADVECT, false, false>(P, rp, C, smem, s, check_only, ncr);
 }
 
 static int advance_resident(rbffd_pde* P, double dt, int nsteps, int flags)

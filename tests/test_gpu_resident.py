@@ -1,6 +1,6 @@
 """Cluster-resident RK4 (RBFFD_ADVANCE_RESIDENT): every step in one launch of
-a thread-block cluster (up to 16 CTAs) holding the weights, stencils, halos
-and state in shared memory.  It performs the one-lane-per-row kernels'
+a thread-block cluster (up to 16 CTAs) holding the weights (in registers for
+31- and 50-node stencils), stencils, halos and state on chip.  It performs the one-lane-per-row kernels'
 arithmetic, so it must give their bits (and, in FP64, the oracle's)."""
 import numpy as np
 import pytest
@@ -86,6 +86,28 @@ def test_resident_heat(ctx):
         pde.close()
     assert np.array_equal(outs[0], outs[1])
     assert np.array_equal(outs[0], O.rk4_heat(st, None, W, u0, 1e-5, 25))
+    grid.close()
+
+
+def test_resident_weights_in_shared_memory(ctx):
+    """37-node stencils (10 chunks: no register-resident variant), so the
+    weights stay in shared memory: FP64 advection equals the oracle bit for
+    bit, FP32 with hyperviscosity equals the one-lane kernels."""
+    N, n = 4096, 37
+    xyz, st = sphere_problem(N, n, 6)
+    types = O.LAMBDA | O.THETA | O.HV
+    W = O.weights(xyz, st, None, 6.0, types, dim=2, poly_deg=2, hv_k=4, hv_scale=-1e-3 * N ** -4.0)
+    grid = R.Grid(ctx, xyz, st)
+    der = R.RBFFD(types, grid, 2)
+    for t, w in W.items():
+        der.setWeights(t, w)
+    p = cosine_bell_setup()
+    b = dict(grid=grid, der=der, p=p, h0=R.exact_cosine_bell(xyz))
+    res, _ = _run(b, R.F64, True, 20, hv=False)
+    cu, cv = O.cosine_bell_coeffs(xyz, a=p["a"], alpha=p["alpha"], u0=p["u0"])
+    assert np.array_equal(res, O.rk4_advect(st, None, W[O.LAMBDA], W[O.THETA], None, cu, cv, b["h0"], p["dt"], 20))
+    res, _ = _run(b, R.F32, True, 20, hv=True)
+    assert np.array_equal(res, _run(b, R.F32, False, 20, hv=True)[0])
     grid.close()
 
 
