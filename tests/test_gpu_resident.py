@@ -111,10 +111,11 @@ def test_resident_weights_in_shared_memory(ctx):
     grid.close()
 
 
-@pytest.mark.parametrize("N", [40, 1000])
+@pytest.mark.parametrize("N", [40, 1000, 2562])
 def test_resident_small_and_ragged_grids(ctx, N):
     """N = 40: a cluster of 2 CTAs, the second with 8 rows; N = 1000: 16 CTAs
-    of 64 rows, the last with 40.  Equal to the oracle bit for bit."""
+    of 64 rows, the last with 40; N = 2562: 16 CTAs of 192 rows, the last two
+    without rows.  Equal to the oracle bit for bit."""
     n = 10
     xyz = R.fibonacci_nodes(N, 11)
     st = R.knn_stencils(xyz, n)
