@@ -504,8 +504,12 @@ int rbffd_pde_set_fused_operator(rbffd_pde* pde, int on);
  * what else is in the batch.  FP64 requests sum in stencil order and equal
  * the one-lane rbffd_pde_advance result bit for bit; FP32 requests sum in a
  * fixed per-grid slot order chosen against shared-memory bank conflicts (and
- * FP32 advection uses one fused operator), so they are within FP32 rounding
- * of the one-lane FP32 result.  The server's threads build per-grid tables on
+ * FP32 advection uses one fused operator), and FP32 requests add each step's
+ * increment to the state with a compensated sum (the rounding lost in u +
+ * increment carried into the next step, the result read out as u minus that
+ * compensation), so long runs of small steps stay close to the FP64 result:
+ * closer than the one-lane FP32 result, from which they differ within FP32
+ * rounding.  The server's threads build per-grid tables on
  * demand: while it holds requests on a grid, the caller uses that grid from
  * no other thread. */
 typedef struct rbffd_server rbffd_server;

@@ -5,8 +5,9 @@
 //
 // Banks.  Requests on the same grid with the same right-hand side (kind,
 // hyperviscosity, advection field) and dtype share a bank: state arrays u,
-// xa, xb, acc with room for BANK_W_F32 (FP32) or BANK_W_F64 (FP64) values per
-// node (one for requests with their own per-node coefficients), in the grid's
+// xa, xb, acc (FP32: and comp, below) with room for BANK_W_F32 (FP32) or
+// BANK_W_F64 (FP64) values per node (one for requests with their own per-node
+// coefficients), in the grid's
 // internal node order, plus the bank's advection coefficients.  The K
 // requests of a bank occupy columns 0..K-1 of an interleaved [N][W] layout
 // whose row stride W is K rounded up to a power of two; a stage kernel row
@@ -16,6 +17,14 @@
 // lone request runs on the plain [N] layout.  When requests join or leave,
 // the bank is repacked at the next step boundary (u into the free xa buffer
 // at the new stride, then the two are swapped).
+//
+// FP32 banks keep a compensated state: a request's RK4 step moves u by a
+// small fraction of itself, and rounding u + increment to FP32 every step
+// drops most of the increment's bits (over 2000 steps of a serving-sized
+// heat solve the FP32 state drifted 2e-5 from FP64).  Stage 3 therefore adds
+// the increment with Knuth's TwoSum and keeps minus the lost part in a
+// per-value compensation array that the next step adds back; a result is read
+// out as u - comp.  Stages 0-2 and the gathers are unchanged.
 //
 // FP32 advection banks fuse their right-hand side into one operator: the
 // velocity field is steady and the same for every column, so
@@ -92,6 +101,7 @@ struct BankDesc {
     T* xa;
     T* xb;
     T* acc;
+    T* comp;  // FP32 banks: [N][W] compensation of u's rounding (nullptr: none)
     T c[4][BANK_W_MAX];  // per column: dt/2, dt/2, dt, dt/6 (0 for free columns)
     T kappa[BANK_W_MAX];
     // row blocks and halos of the grid (tiled launches)
@@ -151,9 +161,11 @@ __device__ __forceinline__ void bank_stage_update(const BankDesc<T>& B, int i, i
     const bool adv = B.kind == KIND_ADVECT;
     const T cu = adv ? B.cu[i] : T(0), cv = adv ? B.cv[i] : T(0);
     const size_t row = (size_t)i * W;
-    T ui[W], ac[W], out[W];
+    T ui[W], ac[W], out[W], cm[W];
     ldw<T, W>(B.u + row, ui, false);
     if (stage > 0) ldw<T, W>(B.acc + row, ac, false);
+    const bool comp = stage == 3 && B.comp != nullptr;
+    if (comp) ldw<T, W>(B.comp + row, cm, false);
 #pragma unroll
     for (int v = 0; v < W; v++) {
         T f;
@@ -170,6 +182,15 @@ __device__ __forceinline__ void bank_stage_update(const BankDesc<T>& B, int i, i
         } else if (stage < 3) {
             ac[v] = Ar<T>::add(ac[v], Ar<T>::mul(T(2), f));
             out[v] = Ar<T>::fma(c, f, ui[v]);
+        } else if (comp) {
+            // compensated update: the increment is small against u, so rounding u + inc
+            // loses most of its bits; cm holds minus what each step's sum lost (the exact
+            // rounding error of the sum, by Knuth's TwoSum) and the next step adds it back
+            const T y = Ar<T>::sub(Ar<T>::mul(c, Ar<T>::add(ac[v], f)), cm[v]);
+            out[v] = Ar<T>::add(ui[v], y);
+            const T yb = Ar<T>::sub(out[v], ui[v]);
+            const T lost = Ar<T>::add(Ar<T>::sub(ui[v], Ar<T>::sub(out[v], yb)), Ar<T>::sub(y, yb));
+            cm[v] = -lost;
         } else {
             out[v] = Ar<T>::fma(c, Ar<T>::add(ac[v], f), ui[v]);
         }
@@ -179,6 +200,7 @@ __device__ __forceinline__ void bank_stage_update(const BankDesc<T>& B, int i, i
         stw<T, W>((stage == 1 ? B.xb : B.xa) + row, out);
     } else {
         stw<T, W>(B.u + row, out);
+        if (comp) stw<T, W>(B.comp + row, cm);
     }
 }
 
@@ -325,10 +347,14 @@ __global__ void k_repack(Repack<T> a)
 
 // A request's column, back to FP64 in the caller's node order.
 template <typename T>
-__global__ void k_column_out(const T* u, int W, int col, double* __restrict__ io, const int* __restrict__ perm, int N)
+__global__ void k_column_out(const T* u, const T* comp, int W, int col, double* __restrict__ io,
+                             const int* __restrict__ perm, int N)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < N) io[perm[i]] = (double)u[(size_t)i * W + col];
+    if (i >= N) return;
+    const size_t e = (size_t)i * W + col;
+    // with a compensation, u - comp is the state to twice the precision of T
+    io[perm[i]] = comp ? (double)u[e] - (double)comp[e] : (double)u[e];
 }
 
 // Fused advection operator of a bank, row by row over the padded rows (sliced
@@ -382,6 +408,7 @@ struct Bank {
     int Wcap = 1;  // values per node the arrays hold
     int op[3] = {-1, -1, -1};
     void *u = nullptr, *xa = nullptr, *xb = nullptr, *acc = nullptr, *cu = nullptr, *cv = nullptr;
+    void* comp = nullptr;  // FP32 banks: compensation of u's rounding, [N][Wcap]
     void* wf = nullptr;  // fused advection operator (FP32 advection banks), sliced ELL
     const Halo* halo = nullptr;  // the grid's row blocks of SEG_ROWS rows (nullptr: untiled)
     // FP32 tiled banks read the halo's conflict-avoiding slot schedule: local
@@ -416,7 +443,8 @@ size_t bank_bytes(const rbffd_grid* g, const rbffd_pde_params& p)
 {
     const size_t es = state_bytes(p), N = (size_t)g->N;
     const size_t rhs = p.rhs_kind == RBFFD_RHS_HEAT ? 0 : (bank_fused(p) ? fused_bytes(g) : 2 * N * es);
-    return 4 * N * bank_capacity(p) * es + rhs;
+    const int arrays = p.dtype == RBFFD_F32 ? 5 : 4;  // u, xa, xb, acc (and FP32: the compensation)
+    return arrays * N * bank_capacity(p) * es + rhs;
 }
 
 bool bank_fits(const Bank& b, const Request& r)
@@ -493,10 +521,11 @@ void bank_free_memory(rbffd_ctx* ctx, Bank& b)
     dev_free(ctx, b.xa, n);
     dev_free(ctx, b.xb, n);
     dev_free(ctx, b.acc, n);
+    dev_free(ctx, b.comp, n);
     dev_free(ctx, b.cu, nc);
     dev_free(ctx, b.cv, nc);
     dev_free(ctx, b.wf, fused_bytes(b.grid));
-    b.u = b.xa = b.xb = b.acc = b.cu = b.cv = b.wf = nullptr;
+    b.u = b.xa = b.xb = b.acc = b.comp = b.cu = b.cv = b.wf = nullptr;
 }
 
 // Device arrays of a new bank for request r (zeroed state, advection
@@ -529,7 +558,7 @@ int bank_create(rbffd_server* S, const Request& r, Bank& b)
         if (b.dtype == RBFFD_F32 && !g->d_w32[b.op[k]] && (rc = grid_make_f32(g, b.op[k]))) return rc;
     const size_t es = state_bytes(p), n = (size_t)g->N * b.Wcap * es;
     if ((rc = dev_alloc(ctx, &b.u, n)) || (rc = dev_alloc(ctx, &b.xa, n)) || (rc = dev_alloc(ctx, &b.xb, n)) ||
-        (rc = dev_alloc(ctx, &b.acc, n))) {
+        (rc = dev_alloc(ctx, &b.acc, n)) || (b.dtype == RBFFD_F32 && (rc = dev_alloc(ctx, &b.comp, n)))) {
         bank_free_memory(ctx, b);
         return rc;
     }
@@ -550,6 +579,7 @@ int bank_create(rbffd_server* S, const Request& r, Bank& b)
     if (e == cudaSuccess) e = cudaMemsetAsync(b.xa, 0, n, S->astream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b.xb, 0, n, S->astream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b.acc, 0, n, S->astream);
+    if (e == cudaSuccess && b.comp) e = cudaMemsetAsync(b.comp, 0, n, S->astream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(S->astream);
     if (e != cudaSuccess) {
         bank_free_memory(ctx, b);
@@ -731,6 +761,7 @@ void fill_desc(BankDesc<T>& d, const Bank& b, int block0)
     d.xa = (T*)b.xa;
     d.xb = (T*)b.xb;
     d.acc = (T*)b.acc;
+    d.comp = (T*)b.comp;
     for (int v = 0; v < BANK_W_MAX; v++) {
         const Request* r = v < b.W ? b.cols[v] : nullptr;
         const bool on = r != nullptr;
@@ -958,6 +989,15 @@ void bank_repack(Bank& b, cudaStream_t s)
     }
     k_repack<T><<<(a.N + 255) / 256, 256, 0, s>>>(a);
     std::swap(b.u, b.xa);
+    if (b.comp) {  // the compensation follows its column into xb (also free between steps); joiners start at 0
+        Repack<T> ac = a;
+        ac.dst = (T*)b.xb;
+        ac.src = (const T*)b.comp;
+        for (int c = 0; c < BANK_W_MAX; c++)
+            if (ac.from[c] == FROM_IO) ac.from[c] = FROM_ZERO;
+        k_repack<T><<<(a.N + 255) / 256, 256, 0, s>>>(ac);
+        std::swap(b.comp, b.xb);
+    }
     b.W = W;
     b.cols.assign(W, nullptr);
     for (int c = 0; c < K; c++) {
@@ -972,7 +1012,8 @@ void column_out(const Request& r, cudaStream_t s)
 {
     const Bank& b = *r.bank;
     const int N = b.grid->N;
-    k_column_out<T><<<(N + 255) / 256, 256, 0, s>>>((const T*)b.u, b.W, r.col, r.d_io, b.grid->d_perm, N);
+    k_column_out<T><<<(N + 255) / 256, 256, 0, s>>>((const T*)b.u, (const T*)b.comp, b.W, r.col, r.d_io,
+                                                    b.grid->d_perm, N);
 }
 
 // A batch of steps in flight.  Requests that finish with it leave the banks

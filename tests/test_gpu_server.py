@@ -4,8 +4,10 @@
   time_dependent_pde.cpp:172-304) bit for bit, heat and cosine bell;
 * every request's result is identical alone and in a mix of grids, stencil
   sizes, right-hand sides, dtypes and step counts with staggered arrivals;
-  FP32 heat results equal the one-lane rbffd_pde_advance result, FP32
-  advection (one fused operator per bank) is within 1e-5 of the FP64 oracle;
+  FP32 heat results are within FP32 rounding of the one-lane rbffd_pde_advance
+  result, FP32 advection (one fused operator per bank) is within 1e-5 of the
+  FP64 oracle; FP32 banks keep a compensated state, so long runs of small
+  steps stay close to FP64;
 * admission: a request that can never fit the HBM budget is refused at
   submission; a budget with room for one request runs them one at a time;
 * cancellation (pending and active), injected admission failures, malformed
@@ -180,6 +182,37 @@ def test_served_fp32_heat_against_oracle_and_pde_path(ctx, grids):
     assert not np.array_equal(served, ref32)  # the scheduled order is in use
 
 
+def test_served_fp32_long_heat_keeps_its_small_increments(ctx, grids):
+    """2000 small heat steps (each moves the state by about 1e-4 of itself):
+    rounding u + increment to FP32 every step loses most of the increment's
+    bits, and the FP32 PDE path drifts by 1.6e-6 from the FP64 result; the
+    FP32 banks carry each step's lost part into the next (compensated sum)
+    and stay within 2e-7 of it, 40x closer."""
+    g = grids[1]
+    u0 = _heat_u0(g, 3)
+    dt, steps = 1e-6, 2000
+
+    def pde_run(dtype):
+        pde = R.HeatSphere(g["grid"], g["der"], 1.0, dtype=dtype)
+        pde.setShape(1, 128)
+        pde.fillInitialConditions(u0)
+        pde.advance(R.RK4, dt, steps, graph=True)
+        out = pde.getLocalSolution()
+        pde.close()
+        return out
+
+    ref, plain32 = pde_run(R.F64), pde_run(R.F32)
+    srv = R.Server(ctx)
+    try:
+        rid = srv.submit(g["grid"], R.heat_params(1.0, R.F32), u0, dt, steps)
+        assert srv.wait(rid) == 0
+        served = srv.result(rid)
+    finally:
+        srv.stop()
+    assert rel_l2(served, ref) < 2e-7
+    assert rel_l2(plain32, ref) > 5 * rel_l2(served, ref)
+
+
 def test_served_fp32_advection_fused_operator(ctx, grids):
     """FP32 advection banks apply one fused operator per bank,
     Wf = -(cu W_lambda + cv W_theta) + W_hv formed in FP64 and rounded once to
@@ -233,8 +266,9 @@ def test_wait_idle_means_every_request_is_done(ctx, grids):
 
 
 def _need_fp32_heat(N):
-    """Device bytes of a new FP32 heat bank (u, xa, xb, acc of 8 columns) and one I/O buffer."""
-    return N * (4 * 8 * 4 + 8)
+    """Device bytes of a new FP32 heat bank (u, xa, xb, acc and the compensation
+    of u, 8 columns each) and one I/O buffer."""
+    return N * (5 * 8 * 4 + 8)
 
 
 def test_request_that_can_never_fit_is_refused(ctx, grids):
