@@ -367,8 +367,10 @@ def run_ours(args):
     warm = max(3, args.warmup)
     res = {}
     # FP64 (the headline: the reference's arithmetic) and FP32 beside it, same protocol.
-    for tag, dtype, wb in (("fp64", R.F64, 8), ("fp32", R.F32, 4)):
+    for tag, dtype, wb in (("fp64", R.F64, 8), ("fp32", R.F32, 4), ("fp32_compensated", R.F32, 4)):
         pde = R.HeatSphere(grid, der, 1.0, dtype=dtype)
+        if tag == "fp32_compensated":
+            pde.setCompensatedState(True)
         pde.fillInitialConditions(u0)
         for _ in range(warm):
             pde.advance(R.RK4, dt, steps, graph=True, asynchronous=True)
@@ -388,7 +390,7 @@ def run_ours(args):
             "value": replicas_rate(float(N) * steps * args.steps, ws, tot_ms * 1e-3), "ms_per_step": tot_ms / args.steps,
             "launches": launches, "clocks": clk, "shape": shape, "u_final": pde.getLocalSolution(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": stage_traffic(tag.replace("fp", "f"), tiled), "peak_kind": peak_kind,
+                         "traffic": stage_traffic(tag[:4].replace("fp", "f"), tiled), "peak_kind": peak_kind,
                          "kernel": stage_kernel_name(shape, "double" if wb == 8 else "float") +
                          ", fused SpMV + RHS + RK4 stage", "shape": shape, "algorithmic_bytes_per_launch": bytes_launch,
                          "l2_resident": True,
@@ -416,7 +418,7 @@ def run_ours(args):
                          "oracle restatement of advanceRungeKutta4 + applyWeightsForDeriv, OpenMP over rows, on the "
                          "device's FP64 weights" % (N, n, secs)}
         ex = R.exact_sph_heat(xyz, W["lmax"], coeffs, steps * dt)
-        for tag in ("fp64", "fp32"):
+        for tag in ("fp64", "fp32", "fp32_compensated"):
             l2, linf = rel_err(res[tag]["u_final"], u_ref)
             accuracy["%s_vs_fp64_oracle" % tag] = {"rel_l2": l2, "rel_linf": linf}
         accuracy["fp64_bit_exact_vs_oracle"] = bool(np.array_equal(res["fp64"]["u_final"], u_ref))
@@ -453,6 +455,13 @@ def run_ours(args):
                      "roofline": f32["roofline"],
                      "note": "FP32 weights, state and accumulation on the same grid and weights (rounded from FP64), "
                              "same timing protocol; errors against the FP64 oracle under accuracy"},
+            "fp32_compensated": {
+                "value": res["fp32_compensated"]["value"], "unit": "node-updates/s",
+                "ms_per_step": res["fp32_compensated"]["ms_per_step"], "e2e": res["fp32_compensated"]["e2e"],
+                "dtype": "f32", "shape": res["fp32_compensated"]["shape"],
+                "note": "as fp32, with the state's update compensated (rbffd_pde_set_compensated_state: each step's "
+                        "rounding of u + increment carried into the next; one more FP32 array read and written in "
+                        "stage 3); error against the FP64 oracle under accuracy"},
             "weights_setup_s": {"first_call": t_weights, "tuned": t_weights2},
             "extras": extras,
         }

@@ -486,6 +486,19 @@ int rbffd_pde_get_tile_flags(rbffd_pde* pde, int* flags);
  * three operators.  RBFFD_ERR_UNSUPPORTED for heat PDEs and for PDEs in the
  * unfused (reference) arithmetic. */
 int rbffd_pde_set_fused_operator(rbffd_pde* pde, int on);
+/* FP32 PDEs: keep the state with a compensated update (beyond the reference,
+ * which steps in FP64 only).  An RK4 step moves u by a small fraction of
+ * itself, and rounding u + increment to FP32 every step drops most of the
+ * increment's bits: over thousands of small steps the FP32 state drifts from
+ * the FP64 one by far more than one rounding.  With on = 1 stage 3 adds the
+ * increment with an exact two-sum and keeps minus the lost part in an extra
+ * N x ntracers FP32 array, added back by the next step; rbffd_pde_get_state
+ * returns u - that correction (computed in FP64); set_state clears it.  Costs
+ * one more FP32 read and write per value and step.  The weights, gathers,
+ * sums and stages 0-2 stay FP32 as before.  on = 0 frees the array.
+ * RBFFD_ERR_UNSUPPORTED for FP64 PDEs; every stepping path applies it except
+ * RBFFD_ADVANCE_RESIDENT, which refuses a PDE that has it on. */
+int rbffd_pde_set_compensated_state(rbffd_pde* pde, int on);
 
 /* ---- serving: persistent request loop with continuous batching --------- *
  * No counterpart in the reference, whose drivers run one PDE per process

@@ -101,6 +101,7 @@ PROTOTYPES = {
     "rbffd_pde_set_arithmetic": (c_int, [c_void_p, c_int]),
     "rbffd_pde_get_arithmetic": (c_int, [c_void_p, ip]),
     "rbffd_pde_set_fused_operator": (c_int, [c_void_p, c_int]),
+    "rbffd_pde_set_compensated_state": (c_int, [c_void_p, c_int]),
     "rbffd_pde_set_tiled_shape": (c_int, [c_void_p, c_int, c_int, c_int]),
     "rbffd_pde_get_tiling": (c_int, [c_void_p, ip]),
     "rbffd_pde_get_tile_flags": (c_int, [c_void_p, ip]),

@@ -662,6 +662,13 @@ class TimeDependentPDE:
         in FP64, rounded to the PDE's dtype; not in the unfused arithmetic)."""
         self.ctx.check(self.ctx.L.rbffd_pde_set_fused_operator(self.h, int(bool(on))), "set_fused_operator")
 
+    def setCompensatedState(self, on=True):
+        """FP32 PDEs: add each RK4 increment to the state with an exact two-sum
+        and carry the rounding it lost into the next step (one more FP32 array),
+        so long runs of small steps do not drift from FP64; getLocalSolution
+        returns the state minus that correction (rbffd_pde_set_compensated_state)."""
+        self.ctx.check(self.ctx.L.rbffd_pde_set_compensated_state(self.h, int(bool(on))), "set_compensated_state")
+
     TILE_STREAM_WEIGHTS, TILE_SLOT_SCHEDULE, TILE_PREFETCH, TILE_PIPELINE, TILE_DOUBLE_BUFFER = 1, 2, 4, 8, 16
 
     def setTiledShape(self, rows_per_block, lanes=1, stream_weights=False, slot_schedule=False, prefetch=False,

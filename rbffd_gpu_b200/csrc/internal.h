@@ -165,6 +165,10 @@ struct rbffd_pde {
     // stages stream one weight array instead of three
     void* wf = nullptr;  // in the PDE's dtype
     bool fused = false;
+    // FP32 compensated state (rbffd_pde_set_compensated_state): [N][T] floats,
+    // minus the rounding each step's u + increment lost; nullptr: off
+    void* comp = nullptr;
+    bool tuning = false;  // the autotuner's dt = 0 steps run: stage 3 leaves comp alone
     // The FP32 operators the stages stream (wf, or the grid's FP32 copies of
     // the one to three operators) in the slot schedule of halo ws_R for ws_P
     // rows per wavefront; each remade when its source changes (ws_src, ws_ver)

@@ -50,6 +50,7 @@ struct StageParams {
     T c;          // dt/2, dt/2, dt, dt/6 for stages 0..3
     T kappa;
     int N, nc, T_tr, stage;  // nc: 4-slot chunks per row (sliced ELL, ell.cuh)
+    T* comp = nullptr;       // stage 3 of an FP32 PDE with a compensated state: minus what u lost
 };
 
 // Right-hand side and the stage update for one (row, tracer) value.  PLAIN:
@@ -78,7 +79,18 @@ __device__ __forceinline__ void stage_update(const StageParams<T>& p, int i, siz
         p.xnext[e] = madd<T, PLAIN>(p.c, f, ui);
         break;
     default:
-        p.u[e] = madd<T, PLAIN>(p.c, Ar<T>::add(p.acc[e], f), ui);
+        if (!std::is_same<T, double>::value && p.comp) {
+            // compensated: add the increment with Knuth's TwoSum and keep minus the part
+            // the rounded sum lost; the next step adds it back (u - comp is the state)
+            const T y = Ar<T>::sub(Ar<T>::mul(p.c, Ar<T>::add(p.acc[e], f)), p.comp[e]);
+            const T s = Ar<T>::add(ui, y);
+            const T yb = Ar<T>::sub(s, ui);
+            const T lost = Ar<T>::add(Ar<T>::sub(ui, Ar<T>::sub(s, yb)), Ar<T>::sub(y, yb));
+            p.u[e] = s;
+            p.comp[e] = -lost;
+        } else {
+            p.u[e] = madd<T, PLAIN>(p.c, Ar<T>::add(p.acc[e], f), ui);
+        }
         break;
     }
 }
@@ -883,6 +895,7 @@ static StageParams<T> make_params(rbffd_pde* P, int stage, double dt)
     p.xnext = stage == 0 ? xa : (stage == 1 ? xb : (stage == 2 ? xa : nullptr));
     p.u = u;
     p.acc = (T*)P->acc;
+    p.comp = stage == 3 && !P->tuning ? (T*)P->comp : nullptr;
     p.N = g->N;
     p.nc = g->nc;
     p.T_tr = P->T;
@@ -1273,6 +1286,12 @@ static Shape autotune(rbffd_pde* P)
         auto it = ctx->tuned.find(key);
         if (it != ctx->tuned.end()) return it->second;
     }
+    // tuning steps (dt = 0, state saved and restored) leave a compensated state's correction alone
+    struct TuningFlag {
+        rbffd_pde* P;
+        explicit TuningFlag(rbffd_pde* q) : P(q) { P->tuning = true; }
+        ~TuningFlag() { P->tuning = false; }
+    } tuning_flag(P);
     std::vector<Shape> cands;
     const int blocks[3] = {128, 256, 512};
     if (P->T == 1) {
@@ -1459,6 +1478,7 @@ static void pde_free(rbffd_pde* P)
     dev_free(ctx, P->cv, (size_t)P->g->N * es);
     dev_free(ctx, P->wf, (size_t)P->g->N32 * P->g->n4 * (P->dtype == RBFFD_F64 ? sizeof(double) : sizeof(float)));
     for (int k = 0; k < 3; k++) dev_free(ctx, P->ws[k], (size_t)P->g->N32 * P->g->n4 * sizeof(float));
+    dev_free(ctx, P->comp, (size_t)P->g->N * P->T * sizeof(float));
     delete P;
 }
 
@@ -1523,6 +1543,37 @@ extern "C" int rbffd_pde_set_fused_operator(rbffd_pde* P, int on)
         P->gexec = nullptr;
     }
     P->fused = true;
+    return RBFFD_OK;
+}
+
+// FP32 state with a compensated update: a per-value FP32 array holds minus
+// the part of u + increment that each step's rounding lost (Knuth's TwoSum in
+// stage 3 of the per-stage kernels), added back by the next step; the state
+// read out is u - comp.  Off: the array is freed and the plain update returns.
+extern "C" int rbffd_pde_set_compensated_state(rbffd_pde* P, int on)
+{
+    if (!P) return RBFFD_ERR_INVALID;
+    rbffd_ctx* ctx = P->ctx;
+    const size_t bytes = (size_t)P->g->N * P->T * sizeof(float);
+    if (on && P->dtype != RBFFD_F32)
+        return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a compensated state is for FP32 PDEs (FP64 rounds 2^29 times finer)");
+    if (!on == !P->comp) return RBFFD_OK;
+    cudaSetDevice(ctx->device);
+    if (P->gexec) {  // captured launches carry the array's address
+        cudaGraphExecDestroy(P->gexec);
+        P->gexec = nullptr;
+    }
+    if (!on) {
+        RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        dev_free(ctx, P->comp, bytes);
+        P->comp = nullptr;
+        P->bytes -= bytes;
+        return RBFFD_OK;
+    }
+    int rc = dev_alloc(ctx, &P->comp, bytes);
+    if (rc) return rc;
+    P->bytes += bytes;
+    RBFFD_CUDA_TRY(ctx, cudaMemsetAsync(P->comp, 0, bytes, ctx->stream));
     return RBFFD_OK;
 }
 
@@ -1629,6 +1680,13 @@ __global__ void k_from_f(const float* __restrict__ a, double* __restrict__ b, si
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = (double)a[i];
 }
+// b = a - c in FP64 (a compensated FP32 state and its correction)
+__global__ void k_from_f_compensated(const float* __restrict__ a, const float* __restrict__ c, double* __restrict__ b,
+                                     size_t n)
+{
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (double)a[i] - (double)c[i];
+}
 
 extern "C" int rbffd_pde_set_state(rbffd_pde* P, const double* u)
 {
@@ -1647,6 +1705,7 @@ extern "C" int rbffd_pde_set_state(rbffd_pde* P, const double* u)
         k_to_dtype_f<<<(int)((n + 255) / 256), 256, 0, s>>>(P->stage64, (float*)P->xb, n);
         RBFFD_CUDA_TRY(ctx, cudaGetLastError());
         if ((rc = grid_to_internal(P->g, P->xb, P->u, P->T, 4, s))) return rc;
+        if (P->comp) RBFFD_CUDA_TRY(ctx, cudaMemsetAsync(P->comp, 0, n * sizeof(float), s));
     }
     RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     return RBFFD_OK;
@@ -1665,7 +1724,13 @@ extern "C" int rbffd_pde_get_state(rbffd_pde* P, double* u)
         RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(u, P->xa, n * 8, cudaMemcpyDeviceToHost, s));
     } else {
         if ((rc = grid_to_caller(P->g, P->u, P->xb, P->T, 4, s))) return rc;
-        k_from_f<<<(int)((n + 255) / 256), 256, 0, s>>>((const float*)P->xb, P->stage64, n);
+        if (P->comp) {  // u - comp, the compensated state
+            if ((rc = grid_to_caller(P->g, P->comp, P->xa, P->T, 4, s))) return rc;
+            k_from_f_compensated<<<(int)((n + 255) / 256), 256, 0, s>>>((const float*)P->xb, (const float*)P->xa,
+                                                                         P->stage64, n);
+        } else {
+            k_from_f<<<(int)((n + 255) / 256), 256, 0, s>>>((const float*)P->xb, P->stage64, n);
+        }
         RBFFD_CUDA_TRY(ctx, cudaGetLastError());
         RBFFD_CUDA_TRY(ctx, cudaMemcpyAsync(u, P->stage64, n * 8, cudaMemcpyDeviceToHost, s));
     }
@@ -1955,6 +2020,7 @@ static int advance_resident(rbffd_pde* P, double dt, int nsteps, int flags)
 {
     rbffd_ctx* ctx = P->ctx;
     if (P->T != 1) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "cluster-resident RK4 serves one tracer");
+    if (P->comp) return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "cluster-resident RK4 keeps no compensated state");
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
     const int rc = P->dtype == RBFFD_F64 ? advance_resident_t<double>(P, dt, nsteps, s, false)
