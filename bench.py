@@ -750,11 +750,14 @@ def bench_multitracer(R, torch, ctx):
     t_weights = time.perf_counter() - t
     stream = torch.cuda.ExternalStream(ctx.stream())
     res = {}
-    for dtype, fused in ((R.F32, True), (R.F64, False), ("fp32_three_operators", False), ("fp64_fused", True)):
+    for dtype, fused in ((R.F32, True), (R.F64, False), ("fp32_three_operators", False), ("fp64_fused", True),
+                         ("fp32_compensated", True)):
         pde = R.Advection(grid, der, cu, cv, True, dtype=R.F64 if dtype in (R.F64, "fp64_fused") else R.F32,
                           ntracers=T)
         if fused:
             pde.setFusedOperator(True)  # steady velocity: one fused operator per stage (K = 1 streamed)
+        if dtype == "fp32_compensated":
+            pde.setCompensatedState(True)
         pde.fillInitialConditions(u0)
         pde.advance(R.RK4, dt, 25, graph=True)
         pde.fillInitialConditions(u0)
@@ -772,7 +775,8 @@ def bench_multitracer(R, torch, ctx):
     out = {"workload": C["name"], "weights_setup_s": t_weights}
     for dtype, tag, wb, sb, K in ((R.F32, "fp32", 4, 4, 1), (R.F64, "fp64", 8, 8, 3),
                                   ("fp32_three_operators", "fp32_three_operators", 4, 4, 3),
-                                  ("fp64_fused", "fp64_fused", 8, 8, 1)):
+                                  ("fp64_fused", "fp64_fused", 8, 8, 1),
+                                  ("fp32_compensated", "fp32_compensated", 4, 4, 1)):
         secs = res[dtype][1]
         per_launch = secs / (4 * steps)
         ib = 2 if res[dtype][2][2] > 0 else 4  # 16-bit local indices in the halo-tiled kernels
@@ -797,6 +801,10 @@ def bench_multitracer(R, torch, ctx):
                                                        np.linalg.norm(u64))
     out["rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64))
     out["rel_l2_fp64_fused_vs_fp64"] = float(np.linalg.norm(res["fp64_fused"][0] - u64) / np.linalg.norm(u64))
+    out["rel_l2_fp32_compensated_vs_fp64"] = float(np.linalg.norm(res["fp32_compensated"][0] - u64) /
+                                                   np.linalg.norm(u64))
+    out["fp32_compensated"]["note"] = ("the fp32 row with the state's update compensated "
+                                       "(rbffd_pde_set_compensated_state; its bytes are not in the roofline)")
     out["fp64_fused"]["note"] = ("FP64 with the fused operator formed in FP64 (one weight array per stage); the "
                                  "fp64 row keeps the reference's three operators and operation order")
     out["rel_linf_fp32_vs_fp64"] = float(np.abs(u32 - u64).max() / np.abs(u64).max())
