@@ -998,7 +998,8 @@ def bench_weights(R, torch, ctx):
 
 SERVING = dict(name="serving_poisson200_4096", requests=4096, stream=4096, rate=200.0, seed=5,
                sizes=(2562, 10242, 40962, 163842, 655362), stencils=(31, 50, 101), steps=(100, 2000),
-               heat_deg={31: 2, 50: 3, 101: 4}, hbm_fraction=0.8, plain_per_class=2, states_per_grid=4)
+               heat_deg={31: 2, 50: 3, 101: 4}, hbm_fraction=0.8, plain_per_class=2, states_per_grid=4,
+               sjf_max_active=512)
 
 
 def serving_hv_gamma(N, n):
@@ -1155,37 +1156,44 @@ def bench_serving(R, torch, ctx):
         seen[r["cls"]] = cnt + 1
     heat32 = R.heat_params(1.0, R.F32)
     adv32 = R.cosine_bell_params(bell["a"], bell["alpha"], bell["T"], True, dtype=R.F32)
-    # warm-up: one short request per grid and kind (module load, slot buffers)
+
+    def serve(srv, keep_sampled):
+        """Warm the server up (one short request per grid and kind: module load,
+        slot buffers), then submit the stream at its arrival times and wait for
+        all of it; returns ids, makespan, stats before and after, latencies."""
+        for key, g in grids.items():
+            for p in (heat32, adv32):
+                srv.submit(g["grid"], p, np.zeros(key[0]), 1e-9, 2, out=g["sink"])
+        srv.wait_idle(120)
+        s0 = srv.stats()
+        # (the submitting thread is this interpreter: no cyclic-GC pauses meanwhile)
+        import gc
+        gc.collect()
+        gc.disable()
+        ids = []
+        t_start = time.perf_counter()
+        for r in reqs:
+            delay = r["t"] - (time.perf_counter() - t_start)
+            if delay > 0:
+                time.sleep(delay)
+            g = grids[(r["N"], r["n"])]
+            ids.append(srv.submit(g["grid"], heat32 if r["heat"] else adv32, r["u0"], r["dt"], r["steps"],
+                                  out=None if (keep_sampled and r["sampled"]) else g["sink"]))
+        srv.wait_idle(1800)
+        makespan = time.perf_counter() - t_start
+        gc.enable()
+        s1 = srv.stats()
+        lat, queue = [], []
+        for rid in ids:
+            done, status, l_s, q_s = srv.poll(rid)
+            assert done and status == 0, status
+            lat.append(l_s)
+            queue.append(q_s)
+        return ids, makespan, s0, s1, lat, queue
+
+    # ---- the stream, admitted in arrival order ----
     srv = R.Server(ctx, hbm_fraction=C["hbm_fraction"])
-    for key, g in grids.items():
-        for p in (heat32, adv32):
-            srv.submit(g["grid"], p, np.zeros(key[0]), 1e-9, 2, out=g["sink"])
-    srv.wait_idle(120)
-    s0 = srv.stats()
-    # ---- the stream: submit at the arrival times, wait for all results ----
-    # (the submitting thread is this interpreter: no cyclic-GC pauses meanwhile)
-    import gc
-    gc.collect()
-    gc.disable()
-    ids = []
-    t_start = time.perf_counter()
-    for r in reqs:
-        delay = r["t"] - (time.perf_counter() - t_start)
-        if delay > 0:
-            time.sleep(delay)
-        g = grids[(r["N"], r["n"])]
-        ids.append(srv.submit(g["grid"], heat32 if r["heat"] else adv32, r["u0"], r["dt"], r["steps"],
-                              out=None if r["sampled"] else g["sink"]))
-    srv.wait_idle(1800)
-    makespan = time.perf_counter() - t_start
-    gc.enable()
-    s1 = srv.stats()
-    lat, queue = [], []
-    for rid in ids:
-        done, status, l_s, q_s = srv.poll(rid)
-        assert done and status == 0, status
-        lat.append(l_s)
-        queue.append(q_s)
+    ids, makespan, s0, s1, lat, queue = serve(srv, True)
     work = float(sum(r["N"] * r["steps"] for r in reqs))
     # ---- plain FP64, one request at a time, for real on the stratified sample ----
     plain_s, plain_work, errs, err_detail = {}, {}, [], []
@@ -1207,6 +1215,10 @@ def bench_serving(R, torch, ctx):
         errs.append(float(np.linalg.norm(out - ref) / np.linalg.norm(ref)))
         err_detail.append((errs[-1], k, r["heat"], r["N"], r["n"], r["steps"], float(np.abs(ref).max())))
         pde.close()
+    srv.stop()
+    # ---- the same stream with at most sjf_max_active requests admitted, least work first ----
+    srv = R.Server(ctx, hbm_fraction=C["hbm_fraction"], max_active=C["sjf_max_active"], admission="shortest")
+    _, sjf_makespan, t0s, t1s, sjf_lat, sjf_queue = serve(srv, False)
     srv.stop()
     step_s = {c: plain_s[c] / plain_work[c] for c in plain_s}  # per RK4 step of each class, from real runs
     cpu = serving_cpu_baseline(R, reqs, grids, bell, os.cpu_count() or 1)
@@ -1256,6 +1268,17 @@ def bench_serving(R, torch, ctx):
                       "with their own step counts; each stream request's service time = its steps x its "
                       "class's measured time per step; served first come, first served on the same "
                       "arrivals" % C["plain_per_class"]},
+        "served_fp32_shortest_first": {
+            "node_updates_per_s": work / sjf_makespan, "makespan_s": sjf_makespan,
+            "gpu_busy_node_updates_per_s": (t1s["node_updates"] - t0s["node_updates"]) /
+                                           (t1s["gpu_busy_s"] - t0s["gpu_busy_s"]),
+            "latency_p50_s": float(np.percentile(sjf_lat, 50)), "latency_p99_s": float(np.percentile(sjf_lat, 99)),
+            "queue_p50_s": float(np.percentile(sjf_queue, 50)), "queue_p99_s": float(np.percentile(sjf_queue, 99)),
+            "max_active": t1s["max_active_seen"],
+            "note": "the same stream and server with at most %d requests admitted at once, the waiting request "
+                    "with the least work (nodes x padded stencil size x steps) admitted next "
+                    "(rbffd_server_set_admission_order); results equal the arrival-order run's" %
+                    C["sjf_max_active"]},
         "served_over_plain": served_rate / plain_rate,
         "cpu_baseline_processes": cpu,
         "rel_l2_served_fp32_vs_plain_fp64": {"max": max(errs), "median": float(np.median(errs)),

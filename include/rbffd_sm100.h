@@ -554,6 +554,17 @@ typedef struct rbffd_server_stats {
 /* Start the loop on ctx's device.  hbm_fraction in (0, 1]; max_active <= 0
  * means no slot limit. */
 int rbffd_server_start(rbffd_ctx* ctx, double hbm_fraction, int max_active, rbffd_server** out);
+/* Which waiting request the admission thread takes next when a slot or
+ * memory frees up (beyond the reference, which has no server):
+ *   RBFFD_ADMIT_ARRIVAL (default): arrival order;
+ *   RBFFD_ADMIT_SHORTEST: the request with the least work left to do (grid
+ *     nodes x padded stencil size x steps), ties in arrival order.  With a
+ *     max_active limit on an overloaded stream, short requests overtake long
+ *     ones, which lowers the median latency; a long request waits while
+ *     shorter ones keep arriving.
+ * Takes effect for the next admission; results are the same either way. */
+enum { RBFFD_ADMIT_ARRIVAL = 0, RBFFD_ADMIT_SHORTEST = 1 };
+int rbffd_server_set_admission_order(rbffd_server* srv, int order);
 /* Queue a request; *id identifies it.  Returns RBFFD_ERR_BUDGET when the
  * request alone could never fit the budget, RBFFD_ERR_INVALID /
  * RBFFD_ERR_STATE / RBFFD_ERR_UNSUPPORTED for a malformed request. */

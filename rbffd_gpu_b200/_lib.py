@@ -115,6 +115,7 @@ PROTOTYPES = {
     "rbffd_server_cancel": (c_int, [c_void_p, c_uint64]),
     "rbffd_server_get_stats": (c_int, [c_void_p, P(ServerStats)]),
     "rbffd_server_pause": (c_int, [c_void_p, c_int]),
+    "rbffd_server_set_admission_order": (c_int, [c_void_p, c_int]),
     "rbffd_server_inject_admission_failures": (c_int, [c_void_p, c_int]),
     "rbffd_server_stop": (c_int, [c_void_p]),
 }

@@ -764,12 +764,24 @@ class Server:
     state, dt and a step count) are admitted against an HBM budget and advanced
     together, one launch per RK4 stage over all active requests."""
 
-    def __init__(self, ctx, hbm_fraction=0.8, max_active=0):
+    ADMIT_ARRIVAL, ADMIT_SHORTEST = 0, 1
+
+    def __init__(self, ctx, hbm_fraction=0.8, max_active=0, admission="arrival"):
+        """admission: "arrival" (waiting requests admitted in arrival order) or
+        "shortest" (least work first; rbffd_server_set_admission_order)."""
+        if admission not in ("arrival", "shortest"):
+            raise ValueError("admission must be 'arrival' or 'shortest'")
         self.ctx, self.L = ctx, ctx.L
         h = ctypes.c_void_p()
         ctx.check(self.L.rbffd_server_start(ctx.h, hbm_fraction, max_active, ctypes.byref(h)), "rbffd_server_start")
         self.h = h
         self._out = {}
+        if admission != "arrival":
+            self.setAdmissionOrder(admission)
+
+    def setAdmissionOrder(self, admission):
+        order = {"arrival": self.ADMIT_ARRIVAL, "shortest": self.ADMIT_SHORTEST}[admission]
+        self.ctx.check(self.L.rbffd_server_set_admission_order(self.h, order), "rbffd_server_set_admission_order")
 
     def submit(self, grid, params, u0, dt, nsteps, cu=None, cv=None, out=None):
         """Queue a request; returns its id.  Raises RbffdError on a refused request.

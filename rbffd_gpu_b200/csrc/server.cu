@@ -41,7 +41,8 @@
 // int32 indices, and gathers that never leave the SM.
 //
 // Two host threads per server:
-//   * admission (admission_loop), in arrival order: a request gets a free
+//   * admission (admission_loop), in arrival order (or least work first,
+//     rbffd_server_set_admission_order): a request gets a free
 //     column of a matching bank, or a new bank, while the context's device
 //     memory plus what the request adds stays within the HBM budget and fewer
 //     than max_active requests are admitted (idle banks are freed first,
@@ -468,6 +469,7 @@ struct rbffd_server {
     cudaEvent_t ev_tab = nullptr;    // the last bank tables copied to the device
     size_t budget = 0;
     int max_active = 0;
+    int order = RBFFD_ADMIT_ARRIVAL;  // which pending request admission takes next (S->mu)
     std::mutex mu;  // guards everything below up to the stepping-thread state
     std::condition_variable cv_work;   // the stepping thread waits for admitted requests
     std::condition_variable cv_admit;  // the admission thread waits for requests, columns or memory
@@ -620,10 +622,33 @@ int bank_create(rbffd_server* S, const Request& r, Bank& b)
     return RBFFD_OK;
 }
 
-// Admission thread.  In arrival order, each pending request gets a column of a
-// matching bank (a new bank when none has room and the budget allows; idle
-// banks are freed first, oldest first) and an I/O buffer holding its initial
-// state, then moves to the ready list.  Runs beside the stepping thread, so
+// The pending request admission takes next (S->mu held, queue not empty):
+// the first, or with RBFFD_ADMIT_SHORTEST the one with the least work
+// (nodes x padded stencil size x steps; the first of equals).
+std::shared_ptr<Request> next_pending(rbffd_server* S)
+{
+    if (S->order != RBFFD_ADMIT_SHORTEST) return S->pending.front();
+    auto work = [](const Request& r) { return (double)r.p.grid->N * r.p.grid->n4 * r.p.nsteps; };
+    auto best = S->pending.begin();
+    for (auto it = S->pending.begin(); it != S->pending.end(); ++it)
+        if (work(**it) < work(**best)) best = it;
+    return *best;
+}
+
+// Remove r from the pending queue (S->mu held).
+void drop_pending(rbffd_server* S, const std::shared_ptr<Request>& r)
+{
+    for (auto it = S->pending.begin(); it != S->pending.end(); ++it)
+        if (*it == r) {
+            S->pending.erase(it);
+            return;
+        }
+}
+
+// Admission thread.  In admission order (arrival, or least work first), each
+// pending request gets a column of a matching bank (a new bank when none has
+// room and the budget allows; idle banks are freed first, oldest first) and
+// an I/O buffer holding its initial state, then moves to the ready list.  Runs beside the stepping thread, so
 // allocation and the upload overlap the running batches.
 void admission_loop(rbffd_server* S)
 {
@@ -647,10 +672,10 @@ void admission_loop(rbffd_server* S)
             S->cv_admit.wait(lk);
             continue;
         }
-        std::shared_ptr<Request> r = S->pending.front();
+        std::shared_ptr<Request> r = next_pending(S);
         if (S->inject_fail > 0) {
             S->inject_fail--;
-            S->pending.pop_front();
+            drop_pending(S, r);
             finish_request(*r, set_error(S->ctx, RBFFD_ERR_OOM, "injected admission failure"));
             S->st.failed++;
             S->cv_done.notify_all();
@@ -684,7 +709,7 @@ void admission_loop(rbffd_server* S)
                 S->cv_admit.wait(lk);
                 continue;
             }
-            S->pending.pop_front();
+            drop_pending(S, r);
             finish_request(*r, set_error(S->ctx, RBFFD_ERR_BUDGET,
                                          "request needing %zu bytes does not fit the budget of %zu bytes", need,
                                          S->budget));
@@ -716,7 +741,7 @@ void admission_loop(rbffd_server* S)
         }
         if (rc != RBFFD_OK && fresh) bank_free_memory(S->ctx, *fresh);  // no-op after a failed bank_create
         lk.lock();
-        S->pending.pop_front();  // still r: only this thread removes from the queue
+        drop_pending(S, r);  // still queued: only this thread removes from the queue
         if (rc != RBFFD_OK) {
             S->owned -= std::min(S->owned, need);
             if (bank && --bank->members == 0) bank->idle_since = Clock::now();
@@ -1386,6 +1411,15 @@ extern "C" int rbffd_server_get_stats(rbffd_server* S, rbffd_server_stats* out)
     out->pending = (long long)S->pending.size();
     out->active = (long long)(S->active.size() + S->ready.size()) + S->finishing;
     out->held_bytes = (double)ctx_held(S->ctx);
+    return RBFFD_OK;
+}
+
+extern "C" int rbffd_server_set_admission_order(rbffd_server* S, int order)
+{
+    if (!S || (order != RBFFD_ADMIT_ARRIVAL && order != RBFFD_ADMIT_SHORTEST)) return RBFFD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->order = order;
+    S->cv_admit.notify_all();
     return RBFFD_OK;
 }
 

@@ -308,6 +308,46 @@ def test_budget_for_one_request_serialises_admission(ctx, grids):
     pde.close()
 
 
+def test_shortest_first_admission(ctx, grids):
+    """One slot, least work first: the request admitted at once runs first,
+    then the waiting ones in order of work (grid nodes x stencil size x
+    steps), whatever their arrival order; each result is the one it gets in
+    arrival order."""
+    g = grids[0]
+    steps = [30, 40, 10, 20]
+    u0 = [_heat_u0(g, k) for k in range(len(steps))]
+    outs = {}
+    for admission in ("arrival", "shortest"):
+        srv = R.Server(ctx, max_active=1, admission=admission)
+        try:
+            srv.pause(True)
+            ids, t_sub = [], []
+            for u, k in zip(u0, steps):
+                t_sub.append(time.perf_counter())
+                ids.append(srv.submit(g["grid"], R.heat_params(1.0, R.F32), u, 1e-5, k))
+            srv.pause(False)
+            srv.wait_idle(60)
+            done_at = []
+            for rid, t in zip(ids, t_sub):
+                done, status, lat, _ = srv.poll(rid)
+                assert done and status == 0
+                done_at.append(t + lat)
+            outs[admission] = [srv.result(rid) for rid in ids]
+        finally:
+            srv.stop()
+        order = [int(k) for k in np.argsort(done_at)]
+        if admission == "shortest":
+            # the first request takes the free slot as it arrives (unless the admission thread
+            # first sees all four), then the waiting ones by work: 10, 20, 40 steps
+            assert order in ([0, 2, 3, 1], [2, 3, 0, 1])
+        else:
+            assert order == [0, 1, 2, 3]
+    for a, b in zip(outs["arrival"], outs["shortest"]):
+        assert np.array_equal(a, b)
+    with pytest.raises(ValueError):
+        R.Server(ctx, admission="longest")
+
+
 def test_cancel_pending_and_active(ctx, grids):
     g = grids[0]
     srv = R.Server(ctx, max_active=1)
