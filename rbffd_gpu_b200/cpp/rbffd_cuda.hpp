@@ -492,6 +492,8 @@ public:
         return u;
     }
     void setTime(double t) { check(ctx(), rbffd_pde_set_time(h_, t), "setTime"); }
+    // FP32 PDEs: carry each step's rounding of u + increment into the next (rbffd_pde_set_compensated_state)
+    void setCompensatedState(bool on) { check(ctx(), rbffd_pde_set_compensated_state(h_, on ? 1 : 0), "setCompensatedState"); }
     // PDE::checkLocalError (pde.h:120-127): the solution's error norms against
     // exact values, printed as the reference prints them (no boundary nodes on
     // the sphere); a high error is reported, never fatal.  Returns the norms
@@ -686,6 +688,11 @@ public:
     }
     int wait(uint64_t id, double timeout_s = 600.0) { return rbffd_server_wait(h_, id, timeout_s); }
     void waitIdle(double timeout_s = 600.0) { check(ctx_.handle(), rbffd_server_wait_idle(h_, timeout_s), "wait_idle"); }
+    // RBFFD_ADMIT_ARRIVAL or RBFFD_ADMIT_SHORTEST (least work first)
+    void setAdmissionOrder(int order)
+    {
+        check(ctx_.handle(), rbffd_server_set_admission_order(h_, order), "set_admission_order");
+    }
     rbffd_server_stats stats()
     {
         rbffd_server_stats s;
