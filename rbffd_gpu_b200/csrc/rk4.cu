@@ -1559,12 +1559,12 @@ extern "C" int rbffd_pde_set_compensated_state(rbffd_pde* P, int on)
         return set_error(ctx, RBFFD_ERR_UNSUPPORTED, "a compensated state is for FP32 PDEs (FP64 rounds 2^29 times finer)");
     if (!on == !P->comp) return RBFFD_OK;
     cudaSetDevice(ctx->device);
+    RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));  // no launch of the old setting still running
     if (P->gexec) {  // captured launches carry the array's address
         cudaGraphExecDestroy(P->gexec);
         P->gexec = nullptr;
     }
     if (!on) {
-        RBFFD_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
         dev_free(ctx, P->comp, bytes);
         P->comp = nullptr;
         P->bytes -= bytes;
