@@ -65,6 +65,7 @@ def test_null_handles_are_rejected():
     assert L.rbffd_pde_destroy(None) == -1
     assert L.rbffd_pde_advance(None, 2, 1.0, 1, 0) == -1
     assert L.rbffd_apply(None, 1, 1, 0, 1, None, None) == -1
+    assert L.rbffd_pde_set_compensated_state(None, 1) == -1
 
 
 def test_fibonacci_nodes_are_unit_and_seeded():
@@ -119,6 +120,9 @@ def test_server_rejects_null_handles():
     assert L.rbffd_server_stop(None) == -1
     assert L.rbffd_server_cancel(None, 1) == -1
     assert L.rbffd_server_wait_idle(None, 1.0) == -1
+    assert L.rbffd_server_set_admission_order(None, 1) == -1
+    with pytest.raises(ValueError):
+        R.Server(None, admission="longest")  # checked before any call into the library
 
 
 def test_ctypes_structs_match_the_header_layout(tmp_path):
