@@ -999,7 +999,7 @@ def bench_weights(R, torch, ctx):
 SERVING = dict(name="serving_poisson200_4096", requests=4096, stream=4096, rate=200.0, seed=5,
                sizes=(2562, 10242, 40962, 163842, 655362), stencils=(31, 50, 101), steps=(100, 2000),
                heat_deg={31: 2, 50: 3, 101: 4}, hbm_fraction=0.8, plain_per_class=2, states_per_grid=4,
-               sjf_max_active=512)
+               sjf_max_active=256)
 
 
 def serving_hv_gamma(N, n):
